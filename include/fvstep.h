@@ -1,0 +1,205 @@
+/*
+ * fvstep.h -- C-ABI of the B200 explicit finite-volume step (Schemi drop-in).
+ *
+ * One opaque handle owns one case: a structured parallelepiped mesh held on one GPU,
+ * its conserved state in structure-of-arrays FP64 storage, and one CUDA stream.
+ * Every entry point returns an int status whose values are the reference's `errors`
+ * enumeration (Schemi/enumerations/errorsEnum.hpp:15-30): 0 = noErrors.
+ *
+ * Reference interfaces replaced by this boundary (paths inside the Schemi project):
+ *   fv_create    <- main's factory/mesh/phase set-up: Schemi/main/Schemi.cpp:269-278,597-639,
+ *                   abstractFlowSolver::createFlowSolver (src/interfaces/abstractFlowSolver.cpp:25-71),
+ *                   abstractLimiter::createLimiter (src/interfaces/abstractLimiter.cpp:35-113),
+ *                   abstractMixtureThermodynamics::createThermodynamics
+ *                   (src/interfaces/abstractMixtureThermodynamics.cpp:32-159)
+ *   fv_upload    <- phaseInitialization derived fields (src/thermodynamics/phaseInitialization.cpp:1827-1885)
+ *                   fed with the restart set c_k, v, p (fieldsOutput/output_N/<field>.dat)
+ *   fv_step      <- abstractStepSolver::calculateStep (headers/abstractStepSolver.hpp:108) as
+ *                   implemented by secondOrderStepSolver (src/solverStages/secondOrderStepSolver.cpp:48-93)
+ *                   with Advection() (src/Advections/Advection.cpp:20-513), followed by main's
+ *                   CFL block (Schemi/main/Schemi.cpp:802-835)
+ *   fv_run       <- main's time loop (Schemi/main/Schemi.cpp:664-670,767-940) incl. the last-step clamp
+ *   fv_download  <- structForOutput::collectParallelData + output::dataOutput field set
+ *                   (src/service/output.cpp:14-308), in internal cell order (x fastest)
+ *   fv_batch_*   <- no reference counterpart (the reference runs one case per process)
+ *   fv_adjoint_* <- no reference counterpart (the reference has no adjoint)
+ */
+#ifndef SCHEMI_B200_FVSTEP_H_
+#define SCHEMI_B200_FVSTEP_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FV_ABI_VERSION 1
+#define FV_MAX_SPECIES 4
+
+typedef int fv_status;
+
+/* errors enum of the reference (errorsEnum.hpp:15-30). */
+enum fv_error_code {
+    FV_OK = 0,
+    FV_ERR_RIEMANN = 1,           /* RiemannSolverError: NaN wave speeds (HLLCSolver.cpp:385-388) */
+    FV_ERR_NEGATIVE_T = 2,        /* negativeTemperatureError */
+    FV_ERR_TOO_BIG_OUTPUT = 3,
+    FV_ERR_SYSTEM = 4,            /* systemError: CUDA failures, bad handle */
+    FV_ERR_BOUNDARY = 5,          /* boundaryConditionError */
+    FV_ERR_CUBIC = 6,
+    FV_ERR_POSITIVENESS = 7,
+    FV_ERR_MPI = 8,
+    FV_ERR_FIELD_INIT = 9,
+    FV_ERR_MESH = 10,             /* meshGenerationError */
+    FV_ERR_INIT = 11,             /* initialisationError: invalid configuration */
+    FV_ERR_NAN = 12               /* NaNError: non-finite state detected after a step */
+};
+
+/* Equation of state: names of abstractMixtureThermodynamics.cpp:39-43. */
+enum fv_eos { FV_EOS_IDEAL = 0, FV_EOS_VAN_DER_WAALS = 1 };
+
+/* Flux solver: names of abstractFlowSolver.cpp:29-35 that this build implements. */
+enum fv_flux { FV_FLUX_HLLC = 0, FV_FLUX_HLL = 1 };
+
+/* Limiter: values of typeOfTVDLimiterEnum.hpp (factory names abstractLimiter.cpp:39-53). */
+enum fv_limiter {
+    FV_LIM_ZERO = 0, FV_LIM_MINMOD = 1, FV_LIM_VANLEER = 2, FV_LIM_LINEAR = 3,
+    FV_LIM_VANALBADA = 4, FV_LIM_HQUICK = 5, FV_LIM_VANLEER2 = 6, FV_LIM_SUPERBEE = 7,
+    FV_LIM_VANALBADA2 = 8, FV_LIM_MINMOD2 = 9, FV_LIM_SWEBY = 10, FV_LIM_KOREN = 11,
+    FV_LIM_KOREN2 = 12, FV_LIM_UTCDFS = 13, FV_LIM_SCHMIDTMANN = 14
+};
+
+/* Boundary-condition types: values of boundaryConditionTypesEnum.hpp:15-34.
+ * FV_BC_PERIODIC has no counterpart in the reference (it offers no periodic patch); it must be
+ * set on both patches of an axis for every field. */
+enum fv_bc {
+    FV_BC_FREE = 1, FV_BC_SLIP = 2, FV_BC_FIXED_CELL = 3, FV_BC_FIXED_SURFACE = 4,
+    FV_BC_PERIODIC = 100
+};
+
+/* Patch order of the task files (#Tail, #Point, #Bottom, #Right, #Left, #Top):
+ * tail = x-min, point = x-max, bottom = z-min, right = y-min, left = y-max, top = z-max
+ * (mesh.cpp:350-420, 781-860, 1572-1760). */
+enum fv_patch {
+    FV_PATCH_TAIL = 0, FV_PATCH_POINT = 1, FV_PATCH_BOTTOM = 2,
+    FV_PATCH_RIGHT = 3, FV_PATCH_LEFT = 4, FV_PATCH_TOP = 5
+};
+
+/* Arithmetic of the step.  F64: everything in FP64.  F32_FLUX: reconstruction, EOS
+ * closures and face fluxes in FP32; conserved variables stored and accumulated in FP64. */
+enum fv_precision { FV_PREC_F64 = 0, FV_PREC_F32_FLUX = 1 };
+
+/* Chemistry source (per-cell, after the advection step). */
+enum fv_chemistry { FV_CHEM_NONE = 0, FV_CHEM_A_B_2C = 1 };
+
+typedef struct fv_config {
+    int dims;                 /* 1, 2 or 3 (#Dimensions_of_the_task) */
+    int n[3];                 /* cells per direction (#Number_of_cells_in_direction) */
+    double L[3];              /* parallelepiped radius-vector (#Radius-vector...); origin at 0 */
+    int n_species;            /* 1..FV_MAX_SPECIES (#Number_of_components) */
+    double R;                 /* universal gas constant value (SI / "1" / CGS / CGmS) */
+    double M[FV_MAX_SPECIES];   /* molar masses (sub_k.txt #Molar_mass) */
+    double Cv[FV_MAX_SPECIES];  /* molar isochoric heat capacities */
+    double Tc[FV_MAX_SPECIES];  /* critical temperatures (van der Waals) */
+    double Pc[FV_MAX_SPECIES];  /* critical pressures (van der Waals) */
+    int eos;                  /* fv_eos */
+    int flux;                 /* fv_flux */
+    int limiter;              /* fv_limiter */
+    int precision;            /* fv_precision */
+    double courant;           /* #Courant_number */
+    double min_timestep;      /* #Minimal_timestep (also the first time step) */
+    int courant_only;         /* 1 when #Source_timestep_correction is "Courant" */
+    int gravity;              /* g.txt #Free_fall_acceleration_flag */
+    double g[3];              /* free-fall acceleration */
+    double g_delta[3];        /* #Acceleration_growth (g += g_delta*dt after each step) */
+    /* Boundary conditions per patch (fv_patch) and per field. */
+    int bc_conc[6][FV_MAX_SPECIES];
+    double bc_conc_value[6][FV_MAX_SPECIES];
+    int bc_vel[6];
+    double bc_vel_value[6][3];
+    int bc_p[6];
+    double bc_p_value[6];
+    /* Chemistry: one-step A + B -> 2C, rate = A * c_A * c_B * exp(-Ea_R / T),
+     * heat release q per mol of reaction (species 0, 1 -> 2). */
+    int chemistry;            /* fv_chemistry */
+    double chem_A;
+    double chem_Ea_R;
+    double chem_q;
+    int chem_substeps;        /* backward-Euler sub-steps per dt (>=1) */
+} fv_config;
+
+/* Field indices of fv_download / fv_upload arrays (n_cells doubles each, x fastest).
+ * Upload takes the restart set: c_1..c_N, v_x, v_y, v_z, p  (N+4 arrays). */
+enum fv_field {
+    FV_F_CONC = 0,            /* c_1..c_N occupy FV_F_CONC + k */
+    FV_F_VX = FV_MAX_SPECIES, FV_F_VY, FV_F_VZ, FV_F_P,
+    FV_F_RHO_K,               /* rho_1..rho_N occupy FV_F_RHO_K + k */
+    FV_F_RHO = FV_F_RHO_K + FV_MAX_SPECIES,
+    FV_F_MX, FV_F_MY, FV_F_MZ, FV_F_E, FV_F_UV, FV_F_T, FV_F_SONIC,
+    FV_F_COUNT
+};
+
+typedef struct fv_handle fv_handle;
+
+typedef struct fv_run_stats {
+    double time;              /* simulated time reached */
+    double dt_next;           /* time step that would be used next */
+    long long steps;          /* steps taken in this call */
+    float device_ms;          /* device time of the call (CUDA events on the handle's stream) */
+} fv_run_stats;
+
+int fv_abi_version(void);
+
+/* Validates cfg, builds geometry tables and allocates device memory on the current device. */
+fv_status fv_create(const fv_config* cfg, fv_handle** out);
+void fv_destroy(fv_handle* h);
+const char* fv_last_error(const fv_handle* h);
+
+/* Host arrays (n_cells each): c_1..c_N, v_x, v_y, v_z, p.  Derives rho_k, rho, m, E as
+ * phaseInitialization.cpp:1827-1885 does, and sets time = 0, dt = min_timestep. */
+fv_status fv_upload(fv_handle* h, const double* const* prim);
+
+/* Same, from device pointers (no host copy). */
+fv_status fv_upload_device(fv_handle* h, const double* const* prim_dev);
+
+/* One step with the handle's current dt (first call: min_timestep), then the CFL block:
+ * dt_next = max(min(Courant / max_i((|v_i| + c_i) / minEdge_i), dtSource), minTimestep).
+ * Writes the dt used and the new dt.  No clamp to an end time. */
+fv_status fv_step(fv_handle* h, double* dt_used, double* dt_next);
+
+/* Runs main's time loop on the device until time >= t_end (or max_steps), with the
+ * last-step clamp dt = t_end - time.  Steps are launched in CUDA-graph chunks; the host
+ * synchronises once per chunk. */
+fv_status fv_run(fv_handle* h, double t_end, long long max_steps, fv_run_stats* stats);
+
+/* Output set (fv_field order).  out[f] may be NULL to skip field f. */
+fv_status fv_download(fv_handle* h, double* const* out);
+
+/* Time and time step held by the handle. */
+fv_status fv_get_time(const fv_handle* h, double* time, double* dt);
+fv_status fv_set_time(fv_handle* h, double time, double dt);
+
+/* Conserved state (rho_1..rho_N, rho, m_x..m_D, E) as device pointers, SoA, n_cells each. */
+fv_status fv_state_device(fv_handle* h, double** fields, int* n_fields, long long* n_cells);
+
+/* Synchronises the handle's stream. */
+fv_status fv_sync(fv_handle* h);
+
+/* ---- Batched ensemble: many independent cases advanced by one persistent kernel ---- */
+typedef struct fv_batch fv_batch;
+
+typedef struct fv_batch_stats {
+    long long cell_updates;   /* sum over cases of cells x steps */
+    long long steps_max;      /* largest step count of any case */
+    long long launches;       /* kernel launches issued */
+    float device_ms;          /* device time of the run */
+} fv_batch_stats;
+
+/* All handles must share dims, n_species, eos, flux, limiter and precision. */
+fv_status fv_batch_create(fv_handle* const* cases, int n_cases, fv_batch** out);
+fv_status fv_batch_run(fv_batch* b, const double* t_end, long long max_steps, fv_batch_stats* stats);
+void fv_batch_destroy(fv_batch* b);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SCHEMI_B200_FVSTEP_H_ */

@@ -1,0 +1,1183 @@
+/*
+ * fv_oracle.cpp -- TEST INFRASTRUCTURE: FP64 CPU restatement of Schemi's explicit
+ * finite-volume step, used only as the checker of the CUDA path (parity tests, smoke
+ * check, CPU baseline of the bench).  Never linked into the product.
+ *
+ * It restates, on a structured parallelepiped, the algorithm of the reference (paths are
+ * inside the Schemi project):
+ *   mesh geometry          src/dataStructures/mesh.cpp:34-86 (normals, weights), :296-500 (1D),
+ *                          :522-1200 (2D), :1205-1900 (3D)
+ *   Gauss gradient         templates/gradient.hpp:19-58, linear interpolation
+ *                          templates/linearInterpolate.hpp:43-80
+ *   TVD limiter (r-ratio)  src/limiters/TVDLimiter.cpp:12-125 (vector), :127-272 (tensor)
+ *   limiter functions      src/limiters/<name>Limiter.cpp (xiR = 2/(1+r) forms)
+ *   reconstruction+closure src/Advections/Advection.cpp:114-387
+ *   Hancock predictor      src/Advections/HancockStage.cpp:10-448, headers/HancockStage.hpp:22-95
+ *   HLLC / HLL fluxes      src/RiemannSolvers/HLLCSolver.cpp:13-406, HLLSolver.cpp:13-318
+ *   update                 src/Advections/Advection.cpp:414-505, templates/divergence.hpp:61-96
+ *   CFL block + time loop  main/Schemi.cpp:641-670, 767-940
+ *   EOS                    src/thermodynamics/mixtureIdeal.cpp, idealFluid.cpp:13-60,
+ *                          mixtureVanDerWaals.cpp:19-58,88-146,309-397, vanDerWaalsFluid.cpp:14-75
+ *   boundary values        headers/boundaryConditionValue.hpp:34-515, src/boundary/slipFunction.cpp
+ * The operation order of every floating-point expression follows the reference so that the
+ * restatement reproduces the reference binary to round-off.  Periodic patches and the
+ * A+B->2C chemistry have no reference counterpart; they follow the same conventions.
+ * Compiled with -ffp-contract=off (the reference build has no FMA).
+ */
+#include "fv_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+namespace {
+
+constexpr double kStab = 5 * std::numeric_limits<double>::epsilon(); // globalConstants.hpp:33
+constexpr double kTwoThirds = 2. / 3.;
+constexpr double kVeryBig = 1E-3 * std::numeric_limits<double>::max(); // globalConstants.hpp:35
+
+struct V3 {
+    double x[3];
+};
+struct T9 {
+    double x[9];
+};
+
+inline V3 v3(double a, double b, double c) { return V3{{a, b, c}}; }
+inline V3 vadd(const V3& a, const V3& b) { return v3(b.x[0] + a.x[0], b.x[1] + a.x[1], b.x[2] + a.x[2]); }
+inline V3 vsub(const V3& a, const V3& b) { return v3(a.x[0] - b.x[0], a.x[1] - b.x[1], a.x[2] - b.x[2]); }
+inline V3 vmul(const V3& a, double s) { return v3(a.x[0] * s, a.x[1] * s, a.x[2] * s); }
+inline V3 vdiv(const V3& a, double s) { return v3(a.x[0] / s, a.x[1] / s, a.x[2] / s); }
+// vector::operator& (vector.cpp:109-119): ((0 + a0 b0) + a1 b1) + a2 b2
+inline double vdot(const V3& a, const V3& b) {
+    double r = 0;
+    r += a.x[0] * b.x[0];
+    r += a.x[1] * b.x[1];
+    r += a.x[2] * b.x[2];
+    return r;
+}
+inline V3 vcross(const V3& a, const V3& b) {
+    return v3(a.x[1] * b.x[2] - a.x[2] * b.x[1], -(a.x[0] * b.x[2] - a.x[2] * b.x[0]),
+              a.x[0] * b.x[1] - a.x[1] * b.x[0]);
+}
+// Scaled 3-argument hypot with the semantics of the reference build's std::hypot(x, y, z):
+// a = the largest magnitude, result a * sqrt((x/a)^2 + (y/a)^2 + (z/a)^2).
+inline double mag3(const V3& v) {
+    double x = std::fabs(v.x[0]), y = std::fabs(v.x[1]), z = std::fabs(v.x[2]);
+    double a = x < y ? (y < z ? z : y) : (x < z ? z : x);
+    if (a == 0) return 0;
+    return a * std::sqrt((x / a) * (x / a) + (y / a) * (y / a) + (z / a) * (z / a));
+}
+// vector * vector (vector.cpp:94-107): T[3i+j] = a_i b_j
+inline T9 outer(const V3& a, const V3& b) {
+    T9 t;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) t.x[3 * i + j] = a.x[i] * b.x[j];
+    return t;
+}
+// tensor & vector (tensor.cpp:163-176)
+inline V3 tdot(const T9& t, const V3& v) {
+    return v3(t.x[0] * v.x[0] + t.x[1] * v.x[1] + t.x[2] * v.x[2],
+              t.x[3] * v.x[0] + t.x[4] * v.x[1] + t.x[5] * v.x[2],
+              t.x[6] * v.x[0] + t.x[7] * v.x[1] + t.x[8] * v.x[2]);
+}
+inline T9 tmul(const T9& t, double s) {
+    T9 r;
+    for (int i = 0; i < 9; ++i) r.x[i] = t.x[i] * s;
+    return r;
+}
+
+// ------------------------------------------------------------------ limiter functions
+// phi(r, xiR) with xiR = 2 / (1 + r), src/limiters/<name>Limiter.cpp (the "calculate" forms).
+double limiterPhi(int lim, double r, double xiR) {
+    switch (lim) {
+    case FV_LIM_ZERO: return 0;  // zeroLimiter.cpp returns a zero gradient
+    case FV_LIM_MINMOD:          // minmodLimiter.cpp:14-27
+        if (r <= 0.) return 0;
+        if (r <= 1.) return r;
+        return std::min(1.0, xiR);
+    case FV_LIM_VANLEER:         // vanLeerLimiter.cpp:14-25
+        if (r < 0.) return 0;
+        return std::min(2 * r / (1 + r), xiR);
+    case FV_LIM_LINEAR: return 1;  // linearLimiter.cpp returns the gradient unchanged
+    case FV_LIM_VANALBADA:       // vanAlbadaLimiter.cpp:15-28
+        if (r <= 0.) return 0;
+        return std::min((r * r + r) / (1 + r * r), xiR);
+    case FV_LIM_HQUICK:
+        if (r <= 0.) return 0;
+        return std::min(4 * r / (3 + r), xiR);
+    case FV_LIM_VANLEER2: {
+        if (r <= 0.) return 0;
+        const double denom = 1 + r;
+        return std::min(4 * r / (denom * denom), 2 * xiR);
+    }
+    case FV_LIM_SUPERBEE:        // superbeeLimiter.cpp:14-29
+        if (r <= 0.) return 0;
+        if (r <= 0.5) return 2 * r;
+        if (r <= 1.) return r;
+        return std::min({r, 2.0, xiR});
+    case FV_LIM_VANALBADA2:
+        if (r <= 0.) return 0;
+        return std::min(2 * r / (1 + r * r), 2 * xiR);
+    case FV_LIM_MINMOD2:
+        if (r <= 0.) return 0;
+        return std::min({1.0, 4 * r / (1 + r), 2 * xiR});
+    case FV_LIM_SWEBY: {
+        const double b = 2.0;  // SwebyLimiter.hpp:17
+        if (r <= 0.) return 0;
+        return std::min({std::min(1.0, b * r), std::min(b, r), b * xiR});
+    }
+    case FV_LIM_KOREN:
+        if (r <= 0) return 0;
+        return std::min(std::min({2 * r, (1 + 2 * r) / 3, 2.0}), 2 * xiR);
+    case FV_LIM_KOREN2:
+        if (r <= 0) return std::min(0.0, std::max(-kTwoThirds, (1 + 2 * r) / 3));
+        return std::min({2 * kTwoThirds * r, std::min((1 + 2 * r) / 3, 2.0), 2 * xiR});
+    case FV_LIM_UTCDFS:
+        if (r < -1) return r * (r + 1) / (r * r + 1);
+        if ((r >= -1) && (r < 0)) return 0;
+        if ((r >= 0) && (r < 0.5)) return r * r * r - 2 * (r * r) + 2 * r;
+        if ((r >= 0.5) && (r < 2)) return 0.75 * r + 0.25;
+        return std::min((2 * (r * r) - 2 * r - 9.0 / 4.0) / (r * r - r - 1), 2 * xiR);
+    case FV_LIM_SCHMIDTMANN: {
+        const double alpha = 1, beta = 2, gamma = 1.5;  // SchmidtmannLimiter.hpp:17
+        const double phiO3 = (2 + r) / 3;
+        return std::min(std::max(0.0, std::min(phiO3, std::max(-alpha * r, std::min({beta * r, phiO3, gamma})))),
+                        2 * xiR);
+    }
+    }
+    return 0;
+}
+
+// ------------------------------------------------------------------ geometry
+struct Face {
+    V3 rC, N;
+    double S;
+    int own, nei;      // nei = -1 on a boundary patch
+    int patch;         // fv_patch of a boundary face, -1 inner, or patch of the wrapped face (periodic)
+    V3 neiShift;       // translation applied to the neighbour centre across a periodic patch
+    double wOwn, wNei;
+};
+
+struct Cell {
+    V3 rC;
+    double V;
+    double minLS;      // 1 / min edge (Schemi.cpp:648-662)
+    int faces[6];
+    int nFaces;
+    int nb[6];         // neighbour cells (mesh.cpp "Set environment cells" order)
+    V3 nbShift[6];
+    int nNb;
+};
+
+struct Mix {
+    int N;
+    int eos;
+    double R;
+    double M[FV_MAX_SPECIES], Cv[FV_MAX_SPECIES];
+    double a[FV_MAX_SPECIES][FV_MAX_SPECIES], b[FV_MAX_SPECIES][FV_MAX_SPECIES];
+
+    // calcMolarFrac (fractionCalculation.cpp:36-44) and the mixture sums
+    void mixParams(const double* c, double& CvMix, double& aMix, double& bMix, double& MMix) const {
+        double X[FV_MAX_SPECIES];
+        for (int k = 0; k < N; ++k) X[k] = c[k + 1] / c[0];
+        CvMix = 0;
+        MMix = 0;
+        for (int k = 0; k < N; ++k) {
+            CvMix += X[k] * Cv[k];
+            MMix += X[k] * M[k];
+        }
+        aMix = 0;
+        bMix = 0;
+        if (eos == FV_EOS_VAN_DER_WAALS)
+            for (int k = 0; k < N; ++k)
+                for (int l = 0; l < N; ++l) {
+                    aMix += X[k] * X[l] * a[k][l];
+                    bMix += X[k] * X[l] * b[k][l];
+                }
+    }
+    double pFromUv(const double* c, double Uv) const {
+        double Cvm, am, bm, Mm;
+        mixParams(c, Cvm, am, bm, Mm);
+        const double g1 = R / Cvm;
+        if (eos == FV_EOS_IDEAL) return g1 * Uv;  // idealFluid.cpp:13-17
+        const double acc = am * (c[0] * c[0]);   // vanDerWaalsFluid.cpp:14-21
+        return g1 * (Uv + acc) / (1 - c[0] * bm) - acc;
+    }
+    double UvFromp(const double* c, double p) const {
+        double Cvm, am, bm, Mm;
+        mixParams(c, Cvm, am, bm, Mm);
+        const double g1 = R / Cvm;
+        if (eos == FV_EOS_IDEAL) return p / g1;  // idealFluid.cpp:19-23
+        const double acc = am * (c[0] * c[0]);   // vanDerWaalsFluid.cpp:23-30
+        return (p + acc) * (1 - c[0] * bm) / g1 - acc;
+    }
+    double TFromUv(const double* c, double Uv) const {
+        double Cvm, am, bm, Mm;
+        mixParams(c, Cvm, am, bm, Mm);
+        if (eos == FV_EOS_IDEAL) return Uv / ((c[0] + kStab) * Cvm);  // idealFluid.cpp:37-41
+        return (Uv + am * (c[0] * c[0])) / ((c[0] + kStab) * Cvm);    // vanDerWaalsFluid.cpp:44-48
+    }
+    double dpdUv(const double* c) const {
+        double Cvm, am, bm, Mm;
+        mixParams(c, Cvm, am, bm, Mm);
+        const double g1 = R / Cvm;
+        if (eos == FV_EOS_IDEAL) return g1;
+        return g1 / (1 - c[0] * bm);  // vanDerWaalsFluid.cpp:71-75
+    }
+    // sqSonicSpeed = dpdrho + dpdUv * (Uv + p) / rho (mixtureIdeal.cpp, mixtureVanDerWaals.cpp:390-397)
+    double sqSonicSpeed(const double* c, double rho, double Uv, double p) const {
+        double Cvm, am, bm, Mm;
+        mixParams(c, Cvm, am, bm, Mm);
+        const double g1 = R / Cvm;
+        if (eos == FV_EOS_IDEAL) return 0 + g1 * (Uv + p) / rho;
+        const double m_cb = 1 - c[0] * bm;  // vanDerWaalsFluid.cpp:57-69
+        const double ac = am * c[0];
+        const double dpdrho = (g1 * (2 * ac / m_cb - bm * (Uv + ac * c[0]) / (m_cb * m_cb)) - 2 * ac) / Mm;
+        const double dUv = g1 / m_cb;
+        return dpdrho + dUv * (Uv + p) / rho;
+    }
+};
+
+// Face-side state (owner or neighbour side of one face)
+struct FState {
+    double c[FV_MAX_SPECIES + 1];    // c[0] = total
+    double rho[FV_MAX_SPECIES + 1];  // rho[0] = mixture density
+    V3 v, m;
+    double E, Uv, p;
+};
+
+}  // namespace
+
+struct fvo_case {
+    fv_config cfg;
+    int N, D;
+    int n[3];
+    long long nCells;
+    std::vector<Cell> cells;
+    std::vector<Face> faces;
+    Mix mix;
+    // cell state (homogeneousPhase<cubicCell>)
+    std::vector<double> c[FV_MAX_SPECIES + 1], rho[FV_MAX_SPECIES + 1];
+    std::vector<V3> v, m;
+    std::vector<double> E, Uv, p;
+    double time = 0, dt = 0;
+    V3 g{};
+    std::string err;
+};
+
+namespace {
+
+// ---------------------------------------------------------------- boundary values
+int bcType(const fvo_case& cs, int field, int k, int patch) {
+    // field 0: concentration k, 1: velocity, 2: pressure
+    if (field == 0) return cs.cfg.bc_conc[patch][k];
+    if (field == 1) return cs.cfg.bc_vel[patch];
+    return cs.cfg.bc_p[patch];
+}
+
+// boundaryConditionValueSurface for scalars (boundaryConditionValue.hpp:34-66)
+double bcSurfaceS(const fvo_case& cs, double in, int field, int k, int patch) {
+    const int t = bcType(cs, field, k, patch);
+    const double val = field == 0 ? cs.cfg.bc_conc_value[patch][k] : cs.cfg.bc_p_value[patch];
+    switch (t) {
+    case FV_BC_FREE: return in;
+    case FV_BC_SLIP: return in;  // slipFunction(scalar) is the identity
+    case FV_BC_FIXED_CELL: return (in + val) * 0.5;
+    case FV_BC_FIXED_SURFACE: return val;
+    }
+    return in;
+}
+// boundaryConditionValueCell for scalars (boundaryConditionValue.hpp:279-300)
+double bcCellS(const fvo_case& cs, double in, int field, int k, int patch, bool& bad) {
+    const int t = bcType(cs, field, k, patch);
+    const double val = field == 0 ? cs.cfg.bc_conc_value[patch][k] : cs.cfg.bc_p_value[patch];
+    switch (t) {
+    case FV_BC_FREE: return in;
+    case FV_BC_SLIP: return in;
+    case FV_BC_FIXED_CELL: return val;
+    case FV_BC_FIXED_SURFACE: bad = true; return in;  // the reference throws boundaryConditionError
+    }
+    return in;
+}
+// slipFunction(vector): v - (v & n) n  (slipFunction.cpp:21-25)
+V3 slipV(const V3& v, const V3& n) { return vsub(v, vmul(n, vdot(v, n))); }
+
+V3 bcSurfaceV(const fvo_case& cs, const V3& in, int patch, const V3& N) {
+    const int t = cs.cfg.bc_vel[patch];
+    const V3 val = v3(cs.cfg.bc_vel_value[patch][0], cs.cfg.bc_vel_value[patch][1], cs.cfg.bc_vel_value[patch][2]);
+    switch (t) {
+    case FV_BC_FREE: return in;
+    case FV_BC_SLIP: return slipV(in, N);
+    case FV_BC_FIXED_CELL: return vmul(vadd(in, val), 0.5);
+    case FV_BC_FIXED_SURFACE: return val;
+    }
+    return in;
+}
+V3 bcCellV(const fvo_case& cs, const V3& in, int patch, const V3& N, bool& bad) {
+    const int t = cs.cfg.bc_vel[patch];
+    const V3 val = v3(cs.cfg.bc_vel_value[patch][0], cs.cfg.bc_vel_value[patch][1], cs.cfg.bc_vel_value[patch][2]);
+    switch (t) {
+    case FV_BC_FREE: return in;
+    case FV_BC_SLIP: return vsub(vmul(slipV(in, N), 2), in);  // boundaryConditionValue.hpp:291-294
+    case FV_BC_FIXED_CELL: return val;
+    case FV_BC_FIXED_SURFACE: bad = true; return in;
+    }
+    return in;
+}
+
+// ---------------------------------------------------------------- geometry builder
+struct Quad {
+    V3 r00, rX0, r0Y, rXY;
+};
+
+void finishFace(Face& f, const Quad& q, const std::vector<Cell>& cells) {
+    f.rC = vdiv(vadd(vadd(vadd(q.r00, q.rX0), q.r0Y), q.rXY), 4.);
+    f.S = mag3(vsub(q.rX0, q.r00)) * mag3(vsub(q.r0Y, q.r00));
+    // mesh.cpp:34-53
+    const V3 V1 = vsub(q.rX0, q.r00), V2 = vsub(q.r0Y, q.r00);
+    V3 Nn = vcross(V1, V2);
+    Nn = vdiv(Nn, mag3(Nn));
+    const V3 cs = vsub(f.rC, cells[f.own].rC);
+    if (vdot(cs, Nn) < 0.) Nn = vmul(Nn, -1.);
+    f.N = Nn;
+}
+
+bool buildMesh(fvo_case& cs) {
+    const fv_config& cf = cs.cfg;
+    const int D = cf.dims;
+    const int nx = cf.n[0], ny = D >= 2 ? cf.n[1] : 1, nz = D >= 3 ? cf.n[2] : 1;
+    cs.n[0] = nx; cs.n[1] = ny; cs.n[2] = nz;
+    cs.nCells = (long long)nx * ny * nz;
+    const double Lx = cf.L[0], Ly = cf.L[1], Lz = cf.L[2];
+    const double dx = Lx / nx, dy = Ly / ny, dz = Lz / nz;
+    auto X = [&](int i) { return 0.0 + dx * (double)(std::size_t)i; };
+    auto Y = [&](int j) { return D >= 2 ? 0.0 + dy * (double)(std::size_t)j : (j == 0 ? 0.0 : Ly); };
+    auto Z = [&](int k) { return D >= 3 ? 0.0 + dz * (double)(std::size_t)k : (k == 0 ? 0.0 : Lz); };
+    auto cellId = [&](int i, int j, int k) { return (int)(i + (long long)nx * (j + (long long)ny * k)); };
+
+    cs.cells.resize(cs.nCells);
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                Cell& c = cs.cells[cellId(i, j, k)];
+                const double xa = X(i), xb = X(i + 1), ya = Y(j), yb = Y(j + 1), za = Z(k), zb = Z(k + 1);
+                const V3 r000 = v3(xa, ya, za), rX00 = v3(xb, ya, za), r0Y0 = v3(xa, yb, za), rXY0 = v3(xb, yb, za);
+                const V3 r00Z = v3(xa, ya, zb), rX0Z = v3(xb, ya, zb), r0YZ = v3(xa, yb, zb), rXYZ = v3(xb, yb, zb);
+                V3 s = vadd(r000, rX00);
+                s = vadd(s, r0Y0); s = vadd(s, rXY0); s = vadd(s, r00Z); s = vadd(s, rX0Z); s = vadd(s, r0YZ); s = vadd(s, rXYZ);
+                c.rC = vdiv(s, 8.);
+                const double e1 = mag3(vsub(rX00, r000)), e2 = mag3(vsub(r0Y0, r000)), e3 = mag3(vsub(r00Z, r000));
+                c.V = e1 * e2 * e3;
+                c.minLS = 1. / std::min(std::min(e1, e2), e3);
+                c.nFaces = 0;
+                c.nNb = 0;
+            }
+
+    const bool perX = cf.bc_vel[FV_PATCH_TAIL] == FV_BC_PERIODIC;
+    const bool perY = D >= 2 && cf.bc_vel[FV_PATCH_RIGHT] == FV_BC_PERIODIC;
+    const bool perZ = D >= 3 && cf.bc_vel[FV_PATCH_BOTTOM] == FV_BC_PERIODIC;
+
+    // Faces.  Per cell the face list follows mesh.cpp: [x-, x+, y+, y-, z-, z+].
+    // xFace[i][j][k] for i in [0, nx], yFace[i][j][k] for j in [0, ny], zFace for k in [0, nz].
+    std::vector<int> xF((size_t)(nx + 1) * ny * nz), yF, zF;
+    if (D >= 2) yF.resize((size_t)nx * (ny + 1) * nz);
+    if (D >= 3) zF.resize((size_t)nx * ny * (nz + 1));
+    auto xIdx = [&](int i, int j, int k) { return (size_t)i + (size_t)(nx + 1) * (j + (size_t)ny * k); };
+    auto yIdx = [&](int i, int j, int k) { return (size_t)i + (size_t)nx * (j + (size_t)(ny + 1) * k); };
+    auto zIdx = [&](int i, int j, int k) { return (size_t)i + (size_t)nx * (j + (size_t)ny * k); };
+
+    // x faces
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i <= nx; ++i) {
+                Face f{};
+                double Xf;
+                if (i == 0) Xf = 0.0 + 0.;
+                else if (i == nx) Xf = 0.0 + Lx;
+                else Xf = X(i);
+                Quad q;
+                if (D == 1) {
+                    q = {v3(Xf, 0., 0.), v3(Xf, 0., Lz), v3(Xf, Ly, 0.), v3(Xf, Ly, Lz)};
+                } else if (D == 2) {
+                    q = {v3(Xf, Y(j), 0.), v3(Xf, Y(j), Lz), v3(Xf, Y(j + 1), 0.), v3(Xf, Y(j + 1), Lz)};
+                } else {
+                    q = {v3(Xf, Y(j), Z(k)), v3(Xf, Y(j), Z(k + 1)), v3(Xf, Y(j + 1), Z(k)), v3(Xf, Y(j + 1), Z(k + 1))};
+                }
+                f.neiShift = v3(0, 0, 0);
+                if (i == 0) {
+                    if (perX) { xF[xIdx(i, j, k)] = -1; continue; }  // created as the x-max face
+                    f.own = cellId(0, j, k); f.nei = -1; f.patch = FV_PATCH_TAIL;
+                } else if (i == nx) {
+                    if (perX) {
+                        f.own = cellId(nx - 1, j, k); f.nei = cellId(0, j, k); f.patch = FV_PATCH_POINT;
+                        f.neiShift = v3(Lx, 0, 0);
+                    } else {
+                        f.own = cellId(nx - 1, j, k); f.nei = -1; f.patch = FV_PATCH_POINT;
+                    }
+                } else {
+                    f.own = cellId(i - 1, j, k); f.nei = cellId(i, j, k); f.patch = -1;
+                }
+                finishFace(f, q, cs.cells);
+                xF[xIdx(i, j, k)] = (int)cs.faces.size();
+                cs.faces.push_back(f);
+            }
+    if (perX)
+        for (int k = 0; k < nz; ++k)
+            for (int j = 0; j < ny; ++j) xF[xIdx(0, j, k)] = xF[xIdx(nx, j, k)];
+    // y faces
+    if (D >= 2) {
+        for (int k = 0; k < nz; ++k)
+            for (int j = 0; j <= ny; ++j)
+                for (int i = 0; i < nx; ++i) {
+                    Face f{};
+                    f.neiShift = v3(0, 0, 0);
+                    Quad q;
+                    const double za = D >= 3 ? Z(k) : 0., zb = D >= 3 ? Z(k + 1) : Lz;
+                    if (j == 0 || j == ny) {
+                        const double Yf = j == 0 ? 0.0 + 0. : 0.0 + Ly;
+                        // mesh.cpp:781-860 (right / left patches)
+                        q = {v3(X(i), Yf, za), v3(X(i), Yf, zb), v3(X(i + 1), Yf, za), v3(X(i + 1), Yf, zb)};
+                    } else {
+                        const double Yf = Y(j);
+                        // mesh.cpp:689-732 (inner y faces)
+                        q = {v3(X(i), Yf, za), v3(X(i + 1), Yf, za), v3(X(i), Yf, zb), v3(X(i + 1), Yf, zb)};
+                    }
+                    if (j == 0) {
+                        if (perY) { yF[yIdx(i, j, k)] = -1; continue; }
+                        f.own = cellId(i, 0, k); f.nei = -1; f.patch = FV_PATCH_RIGHT;
+                    } else if (j == ny) {
+                        if (perY) {
+                            f.own = cellId(i, ny - 1, k); f.nei = cellId(i, 0, k); f.patch = FV_PATCH_LEFT;
+                            f.neiShift = v3(0, Ly, 0);
+                        } else {
+                            f.own = cellId(i, ny - 1, k); f.nei = -1; f.patch = FV_PATCH_LEFT;
+                        }
+                    } else {
+                        f.own = cellId(i, j - 1, k); f.nei = cellId(i, j, k); f.patch = -1;
+                    }
+                    finishFace(f, q, cs.cells);
+                    yF[yIdx(i, j, k)] = (int)cs.faces.size();
+                    cs.faces.push_back(f);
+                }
+        if (perY)
+            for (int k = 0; k < nz; ++k)
+                for (int i = 0; i < nx; ++i) yF[yIdx(i, 0, k)] = yF[yIdx(i, ny, k)];
+    }
+    // z faces
+    if (D >= 3) {
+        for (int k = 0; k <= nz; ++k)
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) {
+                    Face f{};
+                    f.neiShift = v3(0, 0, 0);
+                    const double Zf = k == 0 ? 0.0 + 0. : (k == nz ? 0.0 + Lz : Z(k));
+                    const Quad q = {v3(X(i), Y(j), Zf), v3(X(i + 1), Y(j), Zf), v3(X(i), Y(j + 1), Zf),
+                                    v3(X(i + 1), Y(j + 1), Zf)};
+                    if (k == 0) {
+                        if (perZ) { zF[zIdx(i, j, k)] = -1; continue; }
+                        f.own = cellId(i, j, 0); f.nei = -1; f.patch = FV_PATCH_BOTTOM;
+                    } else if (k == nz) {
+                        if (perZ) {
+                            f.own = cellId(i, j, nz - 1); f.nei = cellId(i, j, 0); f.patch = FV_PATCH_TOP;
+                            f.neiShift = v3(0, 0, Lz);
+                        } else {
+                            f.own = cellId(i, j, nz - 1); f.nei = -1; f.patch = FV_PATCH_TOP;
+                        }
+                    } else {
+                        f.own = cellId(i, j, k - 1); f.nei = cellId(i, j, k); f.patch = -1;
+                    }
+                    finishFace(f, q, cs.cells);
+                    zF[zIdx(i, j, k)] = (int)cs.faces.size();
+                    cs.faces.push_back(f);
+                }
+        if (perZ)
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) zF[zIdx(i, j, 0)] = zF[zIdx(i, j, nz)];
+    }
+
+    // interpolation weights (mesh.cpp:55-86)
+    for (Face& f : cs.faces) {
+        if (f.nei >= 0) {
+            const double ownR = mag3(vsub(f.rC, cs.cells[f.own].rC));
+            const double neiR = mag3(vsub(f.rC, vadd(cs.cells[f.nei].rC, f.neiShift)));
+            const double sumR = ownR + neiR;
+            f.wOwn = neiR / sumR;
+            f.wNei = ownR / sumR;
+        } else {
+            f.wOwn = 1.0;
+            f.wNei = 0.0;
+        }
+    }
+
+    // per-cell face and neighbour lists
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                Cell& c = cs.cells[cellId(i, j, k)];
+                c.faces[c.nFaces++] = xF[xIdx(i, j, k)];
+                c.faces[c.nFaces++] = xF[xIdx(i + 1, j, k)];
+                if (D >= 2) {
+                    c.faces[c.nFaces++] = yF[yIdx(i, j + 1, k)];
+                    c.faces[c.nFaces++] = yF[yIdx(i, j, k)];
+                }
+                if (D >= 3) {
+                    c.faces[c.nFaces++] = zF[zIdx(i, j, k)];
+                    c.faces[c.nFaces++] = zF[zIdx(i, j, k + 1)];
+                }
+                // neighbours in order x-, x+, y-, y+, z-, z+ (mesh.cpp "Set environment cells")
+                auto addNb = [&](int ii, int jj, int kk, V3 sh) {
+                    c.nb[c.nNb] = cellId(ii, jj, kk);
+                    c.nbShift[c.nNb] = sh;
+                    c.nNb++;
+                };
+                if (i > 0) addNb(i - 1, j, k, v3(0, 0, 0));
+                else if (perX) addNb(nx - 1, j, k, v3(-Lx, 0, 0));
+                if (i < nx - 1) addNb(i + 1, j, k, v3(0, 0, 0));
+                else if (perX) addNb(0, j, k, v3(Lx, 0, 0));
+                if (D >= 2) {
+                    if (j > 0) addNb(i, j - 1, k, v3(0, 0, 0));
+                    else if (perY) addNb(i, ny - 1, k, v3(0, -Ly, 0));
+                    if (j < ny - 1) addNb(i, j + 1, k, v3(0, 0, 0));
+                    else if (perY) addNb(i, 0, k, v3(0, Ly, 0));
+                }
+                if (D >= 3) {
+                    if (k > 0) addNb(i, j, k - 1, v3(0, 0, 0));
+                    else if (perZ) addNb(i, j, nz - 1, v3(0, 0, -Lz));
+                    if (k < nz - 1) addNb(i, j, k + 1, v3(0, 0, 0));
+                    else if (perZ) addNb(i, j, 0, v3(0, 0, Lz));
+                }
+            }
+    return true;
+}
+
+// ---------------------------------------------------------------- gradients + limiter
+// Gauss gradient of a scalar cell field (gradient.hpp:19-58 with linearInterpolate.hpp:43-80)
+void gradScalar(const fvo_case& cs, const std::vector<double>& phi, int field, int k, std::vector<V3>& grad) {
+    const size_t nf = cs.faces.size();
+    std::vector<double> fv(nf);
+    for (size_t f = 0; f < nf; ++f) {
+        const Face& F = cs.faces[f];
+        if (F.nei >= 0) fv[f] = phi[F.own] * F.wOwn + phi[F.nei] * F.wNei;
+        else fv[f] = bcSurfaceS(cs, phi[F.own], field, k, F.patch);
+    }
+    grad.resize(cs.nCells);
+    for (long long i = 0; i < cs.nCells; ++i) {
+        const Cell& c = cs.cells[i];
+        V3 acc = v3(0, 0, 0);
+        for (int j = 0; j < c.nFaces; ++j) {
+            const Face& F = cs.faces[c.faces[j]];
+            const V3 n = (F.own == i) ? F.N : vmul(F.N, -1);
+            const V3 term = vmul(vmul(n, fv[c.faces[j]]), F.S);
+            acc.x[0] += term.x[0]; acc.x[1] += term.x[1]; acc.x[2] += term.x[2];
+        }
+        grad[i] = vdiv(acc, c.V);
+    }
+}
+
+void gradVector(const fvo_case& cs, const std::vector<V3>& phi, std::vector<T9>& grad) {
+    const size_t nf = cs.faces.size();
+    std::vector<V3> fv(nf);
+    for (size_t f = 0; f < nf; ++f) {
+        const Face& F = cs.faces[f];
+        if (F.nei >= 0) fv[f] = vadd(vmul(phi[F.own], F.wOwn), vmul(phi[F.nei], F.wNei));
+        else fv[f] = bcSurfaceV(cs, phi[F.own], F.patch, F.N);
+    }
+    grad.resize(cs.nCells);
+    for (long long i = 0; i < cs.nCells; ++i) {
+        const Cell& c = cs.cells[i];
+        T9 acc{};
+        for (int j = 0; j < c.nFaces; ++j) {
+            const Face& F = cs.faces[c.faces[j]];
+            const V3 n = (F.own == i) ? F.N : vmul(F.N, -1);
+            const T9 term = tmul(outer(fv[c.faces[j]], n), F.S);
+            for (int q = 0; q < 9; ++q) acc.x[q] += term.x[q];
+        }
+        T9 g;
+        for (int q = 0; q < 9; ++q) g.x[q] = acc.x[q] / c.V;
+        grad[i] = g;
+    }
+}
+
+// TVDLimiter for a scalar field (TVDLimiter.cpp:12-125)
+void tvdScalar(const fvo_case& cs, const std::vector<V3>& grad, const std::vector<double>& phi, int field, int k,
+               std::vector<V3>& out, bool& bad) {
+    out.resize(cs.nCells);
+    const int lim = cs.cfg.limiter;
+    for (long long i = 0; i < cs.nCells; ++i) {
+        const Cell& c = cs.cells[i];
+        V3 list[12];
+        int nl = 0;
+        for (int cx = 0; cx < c.nNb; ++cx) {
+            const V3 d = vsub(vadd(cs.cells[c.nb[cx]].rC, c.nbShift[cx]), c.rC);
+            const double dm = mag3(d);
+            const V3 dn = vdiv(d, dm);
+            V3 g;
+            for (int j = 0; j < 3; ++j) g.x[j] = (phi[c.nb[cx]] - phi[i]) / dm * dn.x[j];
+            list[nl++] = g;
+        }
+        if (c.nNb < c.nFaces) {
+            for (int j = 0; j < c.nFaces; ++j) {
+                const Face& F = cs.faces[c.faces[j]];
+                if (F.nei >= 0) continue;
+                const V3 d = vmul(vsub(F.rC, c.rC), 2);
+                const double dm = mag3(d);
+                const V3 dn = vdiv(d, dm);
+                const double b = bcCellS(cs, phi[i], field, k, F.patch, bad);
+                list[nl++] = v3((b - phi[i]) / dm * dn.x[0], (b - phi[i]) / dm * dn.x[1], (b - phi[i]) / dm * dn.x[2]);
+            }
+        }
+        V3 mn = list[0], mx = list[0];
+        for (int cx = 1; cx < nl; ++cx)
+            for (int j = 0; j < 3; ++j) {
+                mn.x[j] = std::min(mn.x[j], list[cx].x[j]);
+                mx.x[j] = std::max(mx.x[j], list[cx].x[j]);
+            }
+        V3 res;
+        for (int j = 0; j < 3; ++j) {
+            const double r = mn.x[j] / (mx.x[j] + kStab);
+            res.x[j] = limiterPhi(lim, r, 2 / (1 + r)) * grad[i].x[j];
+        }
+        if (lim == FV_LIM_ZERO) res = v3(0, 0, 0);
+        if (lim == FV_LIM_LINEAR) res = grad[i];
+        out[i] = res;
+    }
+}
+
+// TVDLimiter for the velocity (TVDLimiter.cpp:127-272).  Note the index convention: the
+// neighbour "gradients" are stored as [3*direction + component] while the Gauss gradient is
+// [3*component + direction]; the limiter multiplies them element by element.
+void tvdVector(const fvo_case& cs, const std::vector<T9>& grad, const std::vector<V3>& phi, std::vector<T9>& out,
+               bool& bad) {
+    out.resize(cs.nCells);
+    const int lim = cs.cfg.limiter;
+    for (long long i = 0; i < cs.nCells; ++i) {
+        const Cell& c = cs.cells[i];
+        T9 list[12];
+        int nl = 0;
+        for (int cx = 0; cx < c.nNb; ++cx) {
+            const V3 d = vsub(vadd(cs.cells[c.nb[cx]].rC, c.nbShift[cx]), c.rC);
+            const double dm = mag3(d);
+            const V3 dn = vdiv(d, dm);
+            const V3 dv = vsub(phi[c.nb[cx]], phi[i]);
+            T9 g;
+            for (int j = 0; j < 3; ++j)
+                for (int q = 0; q < 3; ++q) g.x[3 * j + q] = dv.x[q] / dm * dn.x[j];
+            list[nl++] = g;
+        }
+        if (c.nNb < c.nFaces) {
+            for (int j = 0; j < c.nFaces; ++j) {
+                const Face& F = cs.faces[c.faces[j]];
+                if (F.nei >= 0) continue;
+                const V3 d = vmul(vsub(F.rC, c.rC), 2);
+                const double dm = mag3(d);
+                const V3 dn = vdiv(d, dm);
+                const V3 b = bcCellV(cs, phi[i], F.patch, F.N, bad);
+                const V3 dv = vsub(b, phi[i]);
+                T9 g;
+                for (int jj = 0; jj < 3; ++jj)
+                    for (int q = 0; q < 3; ++q) g.x[3 * jj + q] = dv.x[q] / dm * dn.x[jj];
+                list[nl++] = g;
+            }
+        }
+        T9 mn = list[0], mx = list[0];
+        for (int cx = 1; cx < nl; ++cx)
+            for (int q = 0; q < 9; ++q) {
+                mn.x[q] = std::min(mn.x[q], list[cx].x[q]);
+                mx.x[q] = std::max(mx.x[q], list[cx].x[q]);
+            }
+        T9 res;
+        for (int q = 0; q < 9; ++q) {
+            const double r = mn.x[q] / (mx.x[q] + kStab);
+            res.x[q] = limiterPhi(lim, r, 2 / (1 + r)) * grad[i].x[q];
+        }
+        if (lim == FV_LIM_ZERO) res = T9{};
+        if (lim == FV_LIM_LINEAR) res = grad[i];
+        out[i] = res;
+    }
+}
+
+// closure of a reconstructed face state: Advection.cpp:238-303 (owner), :305-387 (neighbour)
+void closeFromPrimitive(const Mix& mx, FState& s) {
+    s.c[0] = 0;
+    s.rho[0] = 0;
+    for (int k = 1; k <= mx.N; ++k) {
+        s.c[0] += s.c[k];
+        s.rho[k] = s.c[k] * mx.M[k - 1];
+        s.rho[0] += s.rho[k];
+    }
+    s.Uv = mx.UvFromp(s.c, s.p);
+    s.m = vmul(s.v, s.rho[0]);
+    const double v2 = vdot(s.v, s.v);
+    s.E = s.Uv + s.rho[0] * v2 * 0.5 + 0.0;
+}
+
+// recalculation after the Hancock half step: HancockStage.cpp:177-224 / :248-306
+void closeFromConserved(const Mix& mx, FState& s) {
+    s.c[0] = 0;
+    for (int k = 1; k <= mx.N; ++k) {
+        s.c[k] = s.rho[k] / mx.M[k - 1];
+        s.c[0] += s.c[k];
+    }
+    s.v = vdiv(s.m, s.rho[0]);
+    const double v2 = vdot(s.v, s.v);
+    s.Uv = s.E - s.rho[0] * v2 * 0.5 - 0.0;
+    s.p = mx.pFromUv(s.c, s.Uv);
+}
+
+struct Flux {
+    V3 rho[FV_MAX_SPECIES + 1];
+    T9 m;
+    V3 E;
+};
+
+// HLLC (HLLCSolver.cpp:13-406) and HLL (HLLSolver.cpp:13-318) for one face; returns false
+// when no branch applies (NaN wave speeds).
+bool riemann(const fvo_case& cs, const FState& O, const FState& B, const V3& N, Flux& F) {
+    const Mix& mx = cs.mix;
+    const int NS = mx.N;
+    const double csO = std::sqrt(mx.sqSonicSpeed(O.c, O.rho[0], O.Uv, O.p) + kTwoThirds * 0.0 * (1. + mx.dpdUv(O.c)));
+    const double csN = std::sqrt(mx.sqSonicSpeed(B.c, B.rho[0], B.Uv, B.p) + kTwoThirds * 0.0 * (1. + mx.dpdUv(B.c)));
+    const double uO = vdot(O.v, N), uN = vdot(B.v, N);
+    const double tpO = kTwoThirds * 0.0, tpN = kTwoThirds * 0.0;
+    const double SO = std::min(uO - csO, uN - csN);
+    const double SN = std::max(uO + csO, uN + csN);
+    const V3 IN = N;  // tensor(1,0,0,0,1,0,0,0,1) & N
+    const V3 INe = v3(1 * N.x[0] + 0 * N.x[1] + 0 * N.x[2], 0 * N.x[0] + 1 * N.x[1] + 0 * N.x[2],
+                      0 * N.x[0] + 0 * N.x[1] + 1 * N.x[2]);
+    (void)IN;
+    if (cs.cfg.flux == FV_FLUX_HLLC) {
+        const double Sc = ((B.p + tpN) - (O.p + tpO) + O.rho[0] * uO * (SO - uO) - B.rho[0] * uN * (SN - uN)) /
+                          (O.rho[0] * (SO - uO) - B.rho[0] * (SN - uN));
+        const double POwnNei = 0.5 * ((O.p + tpO) + (B.p + tpN) + O.rho[0] * (SO - uO) * (Sc - uO) +
+                                      B.rho[0] * (SN - uN) * (Sc - uN));
+        if (SO >= 0) {
+            for (int k = 0; k <= NS; ++k) F.rho[k] = vmul(vmul(N, uO), O.rho[k]);
+            F.m = outer(vadd(vmul(O.m, uO), vmul(INe, O.p + tpO)), N);
+            F.E = vmul(N, uO * (O.E + O.p + tpO));
+        } else if (Sc >= 0) {
+            const double factor = SO - uO;
+            const double den = 1 / (SO - Sc);
+            double rs[FV_MAX_SPECIES + 1];
+            for (int k = 0; k <= NS; ++k) rs[k] = O.rho[k] * factor * den;
+            const V3 ms = vmul(vsub(vmul(O.m, factor), vmul(N, O.p + tpO - POwnNei)), den);
+            const double Es = (O.E * factor - (O.p + tpO) * uO + POwnNei * Sc) * den;
+            for (int k = 0; k <= NS; ++k) F.rho[k] = vmul(N, O.rho[k] * uO + SO * (rs[k] - O.rho[k]));
+            F.m = outer(vadd(vadd(vmul(O.m, uO), vmul(INe, O.p + tpO)), vmul(vsub(ms, O.m), SO)), N);
+            F.E = vmul(N, (O.E + O.p + tpO) * uO + SO * (Es - O.E));
+        } else if (SN > 0) {
+            const double factor = SN - uN;
+            const double den = 1 / (SN - Sc);
+            double rs[FV_MAX_SPECIES + 1];
+            for (int k = 0; k <= NS; ++k) rs[k] = B.rho[k] * factor * den;
+            const V3 ms = vmul(vsub(vmul(B.m, factor), vmul(N, B.p + tpN - POwnNei)), den);
+            const double Es = (B.E * factor - (B.p + tpN) * uN + POwnNei * Sc) * den;
+            for (int k = 0; k <= NS; ++k) F.rho[k] = vmul(N, B.rho[k] * uN + SN * (rs[k] - B.rho[k]));
+            F.m = outer(vadd(vadd(vmul(B.m, uN), vmul(INe, B.p + tpN)), vmul(vsub(ms, B.m), SN)), N);
+            F.E = vmul(N, (B.E + B.p + tpN) * uN + SN * (Es - B.E));
+        } else if (SN <= 0) {
+            for (int k = 0; k <= NS; ++k) F.rho[k] = vmul(vmul(N, uN), B.rho[k]);
+            F.m = outer(vadd(vmul(B.m, uN), vmul(INe, B.p + tpN)), N);
+            F.E = vmul(N, uN * (B.E + B.p + tpN));
+        } else {
+            return false;
+        }
+        return true;
+    }
+    // HLL
+    if (SO >= 0) {
+        for (int k = 0; k <= NS; ++k) F.rho[k] = vmul(N, uO * O.rho[k]);
+        F.m = outer(vadd(vmul(O.m, uO), vmul(INe, O.p + tpO)), N);
+        F.E = vmul(N, uO * (O.E + O.p + tpO));
+    } else if (SN > 0) {
+        const double den = 1 / (SN - SO);
+        for (int k = 0; k <= NS; ++k)
+            F.rho[k] = vmul(N, (SN * uO * O.rho[k] - SO * uN * B.rho[k] + SN * SO * (B.rho[k] - O.rho[k])) * den);
+        const V3 t1 = vmul(vadd(vmul(O.m, uO), vmul(N, O.p + tpO)), SN);
+        const V3 t2 = vmul(vadd(vmul(B.m, uN), vmul(N, B.p + tpN)), SO);
+        const V3 t3 = vmul(vsub(B.m, O.m), SN * SO);
+        F.m = outer(vmul(vadd(vsub(t1, t2), t3), den), N);
+        F.E = vmul(N, (SN * (uO * (O.E + O.p + tpO)) - SO * (uN * (B.E + B.p + tpN)) + SN * SO * (B.E - O.E)) * den);
+    } else if (SN <= 0) {
+        for (int k = 0; k <= NS; ++k) F.rho[k] = vmul(N, uN * B.rho[k]);
+        F.m = outer(vadd(vmul(B.m, uN), vmul(INe, B.p + tpN)), N);
+        F.E = vmul(N, uN * (B.E + B.p + tpN));
+    } else {
+        return false;
+    }
+    return true;
+}
+
+void cellPrimitivesFromConserved(fvo_case& cs, long long i) {
+    // Advection.cpp:455-479
+    const Mix& mx = cs.mix;
+    cs.c[0][i] = 0;
+    for (int k = 1; k <= mx.N; ++k) {
+        cs.c[k][i] = cs.rho[k][i] / mx.M[k - 1];
+        cs.c[0][i] += cs.c[k][i];
+    }
+    cs.v[i] = vdiv(cs.m[i], cs.rho[0][i]);
+    const double v2 = vdot(cs.v[i], cs.v[i]);
+    cs.Uv[i] = cs.E[i] - cs.rho[0][i] * v2 * 0.5 - 0.0;
+    double cc[FV_MAX_SPECIES + 1];
+    for (int k = 0; k <= mx.N; ++k) cc[k] = cs.c[k][i];
+    cs.p[i] = mx.pFromUv(cc, cs.Uv[i]);
+}
+
+int doStep(fvo_case& cs, double dt) {
+    const Mix& mx = cs.mix;
+    const int NS = mx.N;
+    const long long nc = cs.nCells;
+    const size_t nf = cs.faces.size();
+    bool bad = false;
+
+    // 1. limited gradients (Advection.cpp:58-79)
+    std::vector<V3> limC[FV_MAX_SPECIES + 1];
+    for (int k = 1; k <= NS; ++k) {
+        std::vector<V3> g;
+        gradScalar(cs, cs.c[k], 0, k - 1, g);
+        tvdScalar(cs, g, cs.c[k], 0, k - 1, limC[k], bad);
+    }
+    std::vector<T9> gv, limV;
+    gradVector(cs, cs.v, gv);
+    tvdVector(cs, gv, cs.v, limV, bad);
+    std::vector<V3> gp, limP;
+    gradScalar(cs, cs.p, 2, 0, gp);
+    tvdScalar(cs, gp, cs.p, 2, 0, limP, bad);
+
+    // 2. reconstruction (Advection.cpp:114-235) and closure
+    std::vector<FState> own(nf), nei(nf);
+    for (long long i = 0; i < nc; ++i) {
+        const Cell& c = cs.cells[i];
+        for (int j = 0; j < c.nFaces; ++j) {
+            const int fi = c.faces[j];
+            const Face& F = cs.faces[fi];
+            const V3 delta = vsub(F.rC, c.rC);
+            FState s{};
+            for (int k = 1; k <= NS; ++k) s.c[k] = vdot(limC[k][i], delta) + cs.c[k][i];
+            s.v = vadd(tdot(limV[i], delta), cs.v[i]);
+            s.p = vdot(limP[i], delta) + cs.p[i];
+            if (F.own == i) own[fi] = s;
+            else nei[fi] = s;
+        }
+    }
+    for (size_t f = 0; f < nf; ++f) {
+        closeFromPrimitive(mx, own[f]);
+        if (cs.faces[f].nei >= 0) closeFromPrimitive(mx, nei[f]);
+    }
+
+    // 3. Hancock half step (HancockStage.cpp:10-240)
+    const double halfTimestep = 0.5 * dt;
+    for (long long i = 0; i < nc; ++i) {
+        const Cell& c = cs.cells[i];
+        double divR[FV_MAX_SPECIES + 1];
+        for (int k = 0; k <= NS; ++k) {
+            double acc = 0;
+            for (int j = 0; j < c.nFaces; ++j) {
+                const Face& F = cs.faces[c.faces[j]];
+                const FState& s = (F.own == i) ? own[c.faces[j]] : nei[c.faces[j]];
+                const V3 n = (F.own == i) ? F.N : vmul(F.N, -1);
+                acc += vdot(vmul(s.v, s.rho[k]), n) * F.S;
+            }
+            divR[k] = acc / c.V;
+        }
+        V3 divM = v3(0, 0, 0);
+        double divE = 0;
+        for (int j = 0; j < c.nFaces; ++j) {
+            const Face& F = cs.faces[c.faces[j]];
+            const FState& s = (F.own == i) ? own[c.faces[j]] : nei[c.faces[j]];
+            const V3 n = (F.own == i) ? F.N : vmul(F.N, -1);
+            const V3 tm = vmul(vadd(tdot(outer(s.m, s.v), n), vmul(n, s.p + kTwoThirds * 0.0)), F.S);
+            divM.x[0] += tm.x[0]; divM.x[1] += tm.x[1]; divM.x[2] += tm.x[2];
+            divE += (vdot(vmul(s.v, s.E), n) + vdot(vmul(s.v, s.p + kTwoThirds * 0.0), n)) * F.S;
+        }
+        divM = vdiv(divM, c.V);
+        divE /= c.V;
+        for (int j = 0; j < c.nFaces; ++j) {
+            const Face& F = cs.faces[c.faces[j]];
+            FState& s = (F.own == i) ? own[c.faces[j]] : nei[c.faces[j]];
+            for (int k = 0; k <= NS; ++k) s.rho[k] -= divR[k] * halfTimestep;
+            const V3 dm = vmul(divM, halfTimestep);
+            s.m.x[0] -= dm.x[0]; s.m.x[1] -= dm.x[1]; s.m.x[2] -= dm.x[2];
+            s.E -= divE * halfTimestep;
+        }
+    }
+    for (size_t f = 0; f < nf; ++f) {
+        closeFromConserved(mx, own[f]);
+        const Face& F = cs.faces[f];
+        if (F.nei >= 0) {
+            closeFromConserved(mx, nei[f]);
+        } else {
+            // ghost neighbour state (HancockStage.cpp:324-446)
+            FState& s = nei[f];
+            s.c[0] = 0;
+            s.rho[0] = 0;
+            for (int k = 1; k <= NS; ++k) {
+                s.c[k] = bcCellS(cs, own[f].c[k], 0, k - 1, F.patch, bad);
+                s.rho[k] = s.c[k] * mx.M[k - 1];
+                s.c[0] += s.c[k];
+                s.rho[0] += s.rho[k];
+            }
+            s.v = bcCellV(cs, own[f].v, F.patch, F.N, bad);
+            s.m = vmul(s.v, s.rho[0]);
+            s.p = bcCellS(cs, own[f].p, 2, 0, F.patch, bad);
+            s.Uv = mx.UvFromp(s.c, s.p);
+            const double v2 = vdot(s.v, s.v);
+            s.E = s.Uv + s.rho[0] * v2 * 0.5 + 0.0;
+        }
+    }
+    if (bad) {
+        cs.err = "fixedValueSurface is not a valid cell boundary value";
+        return FV_ERR_BOUNDARY;
+    }
+
+    // 4. fluxes
+    std::vector<Flux> flux(nf);
+    for (size_t f = 0; f < nf; ++f)
+        if (!riemann(cs, own[f], nei[f], cs.faces[f].N, flux[f])) {
+            cs.err = "Fatal error in Riemann solver.";
+            return FV_ERR_RIEMANN;
+        }
+
+    // 5. update (Advection.cpp:414-505)
+    const V3 gvec = cs.g;
+    for (long long i = 0; i < nc; ++i) {
+        const Cell& c = cs.cells[i];
+        double dE = 0;
+        V3 dM = v3(0, 0, 0);
+        double dR[FV_MAX_SPECIES + 1];
+        for (int k = 0; k <= NS; ++k) dR[k] = 0;
+        for (int j = 0; j < c.nFaces; ++j) {
+            const int fi = c.faces[j];
+            const Face& F = cs.faces[fi];
+            const V3 n = (F.own == i) ? F.N : vmul(F.N, -1);
+            dE += vdot(flux[fi].E, n) * F.S;
+            const V3 tm = vmul(tdot(flux[fi].m, n), F.S);
+            dM.x[0] += tm.x[0]; dM.x[1] += tm.x[1]; dM.x[2] += tm.x[2];
+            for (int k = 0; k <= NS; ++k) dR[k] += vdot(flux[fi].rho[k], n) * F.S;
+        }
+        const double divE = dE / c.V;
+        const V3 divM = vdiv(dM, c.V);
+        const double rhoOld = cs.rho[0][i];
+        const V3 vOld = cs.v[i];
+        cs.E[i] -= divE * dt;
+        const V3 mdt = vmul(divM, dt);
+        cs.m[i].x[0] -= mdt.x[0]; cs.m[i].x[1] -= mdt.x[1]; cs.m[i].x[2] -= mdt.x[2];
+        if (cs.cfg.gravity) {
+            cs.E[i] += rhoOld * vdot(vOld, gvec) * dt;
+            const V3 gm = vmul(vmul(gvec, rhoOld), dt);
+            cs.m[i].x[0] += gm.x[0]; cs.m[i].x[1] += gm.x[1]; cs.m[i].x[2] += gm.x[2];
+        }
+        for (int k = 0; k <= NS; ++k) cs.rho[k][i] -= dR[k] / c.V * dt;
+    }
+    for (long long i = 0; i < nc; ++i) cellPrimitivesFromConserved(cs, i);
+    return FV_OK;
+}
+
+// main's CFL block (Schemi.cpp:807-833)
+double cflTimestep(const fvo_case& cs) {
+    double maxS = -std::numeric_limits<double>::infinity();
+    for (long long i = 0; i < cs.nCells; ++i) {
+        double cc[FV_MAX_SPECIES + 1];
+        for (int k = 0; k <= cs.N; ++k) cc[k] = cs.c[k][i];
+        const double sonic = std::sqrt(cs.mix.sqSonicSpeed(cc, cs.rho[0][i], cs.Uv[i], cs.p[i]));
+        double s = mag3(cs.v[i]) + sonic;
+        s *= cs.cells[i].minLS;
+        maxS = std::max(maxS, s);
+    }
+    double dt = cs.cfg.courant / maxS;
+    if (!cs.cfg.courant_only) dt = std::min(dt, kVeryBig);
+    dt = std::max(dt, cs.cfg.min_timestep);
+    return dt;
+}
+
+bool validate(const fv_config& cf, std::string& err) {
+    if (cf.dims < 1 || cf.dims > 3) { err = "dims must be 1, 2 or 3"; return false; }
+    for (int d = 0; d < cf.dims; ++d)
+        if (cf.n[d] < 1) { err = "cell counts must be positive"; return false; }
+    if (cf.n_species < 1 || cf.n_species > FV_MAX_SPECIES) { err = "n_species out of range"; return false; }
+    if (cf.eos != FV_EOS_IDEAL && cf.eos != FV_EOS_VAN_DER_WAALS) { err = "unknown equation of state"; return false; }
+    if (cf.flux != FV_FLUX_HLLC && cf.flux != FV_FLUX_HLL) { err = "unknown flux solver"; return false; }
+    if (cf.limiter < 0 || cf.limiter > FV_LIM_SCHMIDTMANN) { err = "unknown limiter"; return false; }
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+fvo_case* fvo_create(const fv_config* cfg, char* err, int err_len) {
+    std::string e;
+    if (!cfg || !validate(*cfg, e)) {
+        if (err && err_len > 0) snprintf(err, err_len, "%s", e.c_str());
+        return nullptr;
+    }
+    fvo_case* cs = new fvo_case();
+    cs->cfg = *cfg;
+    cs->N = cfg->n_species;
+    cs->D = cfg->dims;
+    buildMesh(*cs);
+    Mix& mx = cs->mix;
+    mx.N = cs->N;
+    mx.eos = cfg->eos;
+    mx.R = cfg->R;
+    for (int k = 0; k < mx.N; ++k) {
+        mx.M[k] = cfg->M[k];
+        mx.Cv[k] = cfg->Cv[k];
+    }
+    if (cfg->eos == FV_EOS_VAN_DER_WAALS) {
+        // mixtureVanDerWaals.cpp:33-52
+        for (int k = 0; k < mx.N; ++k) {
+            mx.b[k][k] = cfg->Tc[k] * mx.R / (8 * cfg->Pc[k]);
+            mx.a[k][k] = cfg->Pc[k] * mx.b[k][k] * mx.b[k][k] * 27;
+        }
+        for (int k = 0; k < mx.N; ++k)
+            for (int l = 0; l < mx.N; ++l)
+                if (k != l) {
+                    mx.b[k][l] = std::pow(0.5 * (std::cbrt(mx.b[k][k]) + std::cbrt(mx.b[l][l])), 3);
+                    mx.a[k][l] = std::sqrt(mx.a[k][k] * mx.a[l][l]);
+                }
+    }
+    for (int k = 0; k <= cs->N; ++k) {
+        cs->c[k].assign(cs->nCells, 0.0);
+        cs->rho[k].assign(cs->nCells, 0.0);
+    }
+    cs->v.assign(cs->nCells, v3(0, 0, 0));
+    cs->m.assign(cs->nCells, v3(0, 0, 0));
+    cs->E.assign(cs->nCells, 0.0);
+    cs->Uv.assign(cs->nCells, 0.0);
+    cs->p.assign(cs->nCells, 0.0);
+    cs->g = v3(cfg->g[0], cfg->g[1], cfg->g[2]);
+    cs->dt = cfg->min_timestep;
+    return cs;
+}
+
+void fvo_destroy(fvo_case* c) { delete c; }
+
+long long fvo_n_cells(const fvo_case* c) { return c ? c->nCells : 0; }
+
+int fvo_upload(fvo_case* cs, const double* const* prim) {
+    const int NS = cs->N;
+    const Mix& mx = cs->mix;
+    for (long long i = 0; i < cs->nCells; ++i) {
+        // phaseInitialization.cpp:1827-1885
+        cs->c[0][i] = 0;
+        for (int k = 1; k <= NS; ++k) {
+            cs->c[k][i] = prim[k - 1][i];
+            cs->c[0][i] += cs->c[k][i];
+        }
+        for (int k = 1; k <= NS; ++k) cs->rho[k][i] = cs->c[k][i] * mx.M[k - 1];
+        cs->rho[0][i] = 0;
+        for (int k = 1; k <= NS; ++k) cs->rho[0][i] += cs->rho[k][i];
+        cs->v[i] = v3(prim[NS][i], prim[NS + 1][i], prim[NS + 2][i]);
+        cs->p[i] = prim[NS + 3][i];
+        cs->m[i] = vmul(cs->v[i], cs->rho[0][i]);
+        double cc[FV_MAX_SPECIES + 1];
+        for (int k = 0; k <= NS; ++k) cc[k] = cs->c[k][i];
+        cs->Uv[i] = mx.UvFromp(cc, cs->p[i]);
+        const double v2 = vdot(cs->v[i], cs->v[i]);
+        cs->E[i] = cs->Uv[i] + cs->rho[0][i] * v2 * 0.5 + 0.0;
+    }
+    cs->time = 0;
+    cs->dt = cs->cfg.min_timestep;
+    cs->g = v3(cs->cfg.g[0], cs->cfg.g[1], cs->cfg.g[2]);
+    return FV_OK;
+}
+
+int fvo_step(fvo_case* cs, double* dt_used, double* dt_next) {
+    const double dt = cs->dt;
+    const int st = doStep(*cs, dt);
+    if (st != FV_OK) return st;
+    if (cs->cfg.gravity) {
+        cs->g = vadd(cs->g, vmul(v3(cs->cfg.g_delta[0], cs->cfg.g_delta[1], cs->cfg.g_delta[2]), dt));
+    }
+    cs->time += dt;
+    cs->dt = cflTimestep(*cs);
+    if (dt_used) *dt_used = dt;
+    if (dt_next) *dt_next = cs->dt;
+    return FV_OK;
+}
+
+int fvo_run(fvo_case* cs, double t_end, long long max_steps, double* time, long long* steps) {
+    long long n = 0;
+    cs->dt = std::min(cs->dt, t_end);
+    int st = FV_OK;
+    do {
+        if (n >= max_steps) break;
+        st = fvo_step(cs, nullptr, nullptr);
+        if (st != FV_OK) break;
+        ++n;
+        if ((cs->time + cs->dt) > t_end) cs->dt = t_end - cs->time;
+    } while (cs->time < t_end);
+    if (time) *time = cs->time;
+    if (steps) *steps = n;
+    return st;
+}
+
+int fvo_download(fvo_case* cs, double* const* out) {
+    const int NS = cs->N;
+    const Mix& mx = cs->mix;
+    for (long long i = 0; i < cs->nCells; ++i) {
+        double cc[FV_MAX_SPECIES + 1];
+        for (int k = 0; k <= NS; ++k) cc[k] = cs->c[k][i];
+        for (int k = 0; k < NS; ++k)
+            if (out[FV_F_CONC + k]) out[FV_F_CONC + k][i] = cs->c[k + 1][i];
+        if (out[FV_F_VX]) out[FV_F_VX][i] = cs->v[i].x[0];
+        if (out[FV_F_VY]) out[FV_F_VY][i] = cs->v[i].x[1];
+        if (out[FV_F_VZ]) out[FV_F_VZ][i] = cs->v[i].x[2];
+        if (out[FV_F_P]) out[FV_F_P][i] = cs->p[i];
+        for (int k = 0; k < NS; ++k)
+            if (out[FV_F_RHO_K + k]) out[FV_F_RHO_K + k][i] = cs->rho[k + 1][i];
+        if (out[FV_F_RHO]) out[FV_F_RHO][i] = cs->rho[0][i];
+        if (out[FV_F_MX]) out[FV_F_MX][i] = cs->m[i].x[0];
+        if (out[FV_F_MY]) out[FV_F_MY][i] = cs->m[i].x[1];
+        if (out[FV_F_MZ]) out[FV_F_MZ][i] = cs->m[i].x[2];
+        if (out[FV_F_E]) out[FV_F_E][i] = cs->E[i];
+        if (out[FV_F_UV]) out[FV_F_UV][i] = cs->Uv[i];
+        if (out[FV_F_T]) out[FV_F_T][i] = mx.TFromUv(cc, cs->Uv[i]);
+        if (out[FV_F_SONIC]) out[FV_F_SONIC][i] = std::sqrt(mx.sqSonicSpeed(cc, cs->rho[0][i], cs->Uv[i], cs->p[i]));
+    }
+    return FV_OK;
+}
+
+int fvo_get_time(const fvo_case* cs, double* time, double* dt) {
+    if (time) *time = cs->time;
+    if (dt) *dt = cs->dt;
+    return FV_OK;
+}
+
+int fvo_set_time(fvo_case* cs, double time, double dt) {
+    cs->time = time;
+    cs->dt = dt;
+    return FV_OK;
+}
+
+int fvo_get_conserved(const fvo_case* cs, double* const* out) {
+    const int NS = cs->N;
+    for (long long i = 0; i < cs->nCells; ++i) {
+        for (int k = 0; k < NS; ++k) out[k][i] = cs->rho[k + 1][i];
+        out[NS][i] = cs->rho[0][i];
+        for (int d = 0; d < cs->D; ++d) out[NS + 1 + d][i] = cs->m[i].x[d];
+        out[NS + 1 + cs->D][i] = cs->E[i];
+    }
+    return FV_OK;
+}
+
+int fvo_set_conserved(fvo_case* cs, const double* const* in) {
+    const int NS = cs->N;
+    for (long long i = 0; i < cs->nCells; ++i) {
+        for (int k = 0; k < NS; ++k) cs->rho[k + 1][i] = in[k][i];
+        cs->rho[0][i] = in[NS][i];
+        cs->m[i] = v3(0, 0, 0);
+        for (int d = 0; d < cs->D; ++d) cs->m[i].x[d] = in[NS + 1 + d][i];
+        cs->E[i] = in[NS + 1 + cs->D][i];
+        cellPrimitivesFromConserved(*cs, i);
+    }
+    return FV_OK;
+}
+
+}  // extern "C"

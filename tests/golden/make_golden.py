@@ -1,0 +1,93 @@
+"""Regenerates the golden fixtures in this directory by running the reference solver.
+
+The reference (Eicosane-2/Schemi) is compiled from its own sources by ``oracle/Makefile``
+(``make -C oracle ref``) into ``oracle/_ref/schemi_patched``; each case below is written as a
+task deck by ``schemi_b200.deck`` and fed to it through its restart reader.  The fixtures hold
+the reference's per-step outputs, so the parity tests need neither the reference sources nor
+the binary at run time.
+
+    python tests/golden/make_golden.py
+"""
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from schemi_b200 import cases  # noqa: E402
+from schemi_b200.case import BC, Case, PatchBC  # noqa: E402
+import oracle as O  # noqa: E402
+
+FIELDS = {"c1": "concentration_1", "c2": "concentration_2", "c3": "concentration_3", "vx": "velocity_x",
+          "vy": "velocity_y", "vz": "velocity_z", "p": "pressure", "rho": "density", "E": "total_energy",
+          "mx": "momentum_x", "my": "momentum_y"}
+
+
+def golden_cases():
+    """(name, case, prim, n_steps or None for a run to t_end, steps to keep)."""
+    out = []
+    c, p = cases.shock_tube_1d()
+    out.append(("shock_tube_1d_full", c, p, None, [1, 2, 10, 100, 500, "last"]))
+    c, p = cases.kelvin_helmholtz_2d(n=24, periodic=False)
+    out.append(("kh_slip_24_vanleer", c, p, 12, [1, 12]))
+    c, p = cases.kelvin_helmholtz_2d(n=24, periodic=False, limiter="Koren2")
+    out.append(("kh_slip_24_koren2", c, p, 10, [1, 10]))
+    c, p = cases.kelvin_helmholtz_2d(n=24, periodic=False, limiter="linear")
+    out.append(("kh_slip_24_linear", c, p, 10, [1, 10]))
+    c, p = cases.kelvin_helmholtz_2d(n=24, periodic=False)
+    c.flux = "HLL"
+    out.append(("kh_slip_24_hll", c, p, 10, [10]))
+    c, p = cases.rayleigh_taylor_2d(nx=16, ny=48, modes=4)
+    out.append(("rt_16x48_gravity", c, p, 10, [1, 10]))
+    c, p, _ = cases.richtmyer_meshkov(0, n=32)
+    c.precision = "f64"
+    out.append(("rm_32_superbee", c, p, 10, [1, 10]))
+    c3, p3 = cases.reacting_shear_3d(n=12, periodic=False)
+    n = 12
+    c = Case(dims=2, n=(n, n, 1), L=(1.0, 1.0, 1.0), species=c3.species, t_end=1.0, R_units="SI",
+             eos="vanDerWaals", limiter="vanLeer", name="vdw2d")
+    for k in ("tail", "point", "right", "left"):
+        c.bc[k] = PatchBC.uniform("slip", 3)
+    out.append(("vdw_2d_12", c, [a.reshape(n, n, n)[0].ravel() for a in p3], 10, [1, 10]))
+    c, p = cases.shock_tube_1d(n=100)
+    c.bc["tail"] = PatchBC([BC("fixedValueCell", 1.0), BC("fixedValueCell", 0.0)],
+                           BC("fixedValueCell", (0.2, 0.0, 0.0)), BC("fixedValueCell", 1.0))
+    c.bc["point"] = PatchBC([BC("slip"), BC("slip")], BC("slip"), BC("slip"))
+    out.append(("tube_fixedvalue_slip_100", c, p, 20, [1, 20]))
+    c, p = cases.shock_tube_1d(n=200)
+    c.flux, c.limiter = "HLL", "superbee"
+    out.append(("tube_hll_superbee_200", c, p, 30, [30]))
+    return out
+
+
+def main():
+    for name, case, prim, nsteps, keep in golden_cases():
+        if nsteps is not None:
+            oc = O.OracleCase(case)
+            oc.upload(prim)
+            for _ in range(nsteps):
+                oc.step()
+            case.t_end = oc.time()[0]
+        outs, times, wall = O.run_reference(case, prim, frequency_of_output=1)
+        idx = sorted(i for i in outs if i >= 2)
+        last = idx[-1]
+        data = {"n_steps": np.int64(len(idx)), "t_end": np.float64(case.t_end)}
+        for k in keep:
+            i = last if k == "last" else k + 1       # output_<s+1> holds the state after step s
+            step = len(idx) if k == "last" else k
+            r = outs[i]
+            data[f"time_{step}"] = np.float64(times[i])
+            for short, col in FIELDS.items():
+                if col in r:
+                    data[f"{short}_{step}"] = np.asarray(r[col], dtype=np.float64)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **data)
+        print(f"{name}: {len(idx)} steps, reference wall {wall:.2f} s")
+
+
+if __name__ == "__main__":
+    main()
