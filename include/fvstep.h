@@ -177,7 +177,9 @@ fv_status fv_download(fv_handle* h, double* const* out);
 fv_status fv_get_time(const fv_handle* h, double* time, double* dt);
 fv_status fv_set_time(fv_handle* h, double time, double dt);
 
-/* Conserved state (rho_1..rho_N, rho, m_x..m_D, E) as device pointers, SoA, n_cells each. */
+/* Conserved state (rho_1..rho_N, rho, m_x, m_y, m_z, E) as device pointers, SoA, n_cells each.
+ * A 1D/2D case whose restart set has no transverse velocity leaves the transverse momentum
+ * fields untouched (they stay zero). */
 fv_status fv_state_device(fv_handle* h, double** fields, int* n_fields, long long* n_cells);
 
 /* Synchronises the handle's stream. */

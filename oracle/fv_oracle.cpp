@@ -610,7 +610,7 @@ void tvdScalar(const fvo_case& cs, const std::vector<V3>& grad, const std::vecto
     const int lim = cs.cfg.limiter;
     for (long long i = 0; i < cs.nCells; ++i) {
         const Cell& c = cs.cells[i];
-        V3 list[12];
+        V3 list[12] = {};
         int nl = 0;
         for (int cx = 0; cx < c.nNb; ++cx) {
             const V3 d = vsub(vadd(cs.cells[c.nb[cx]].rC, c.nbShift[cx]), c.rC);
@@ -657,7 +657,7 @@ void tvdVector(const fvo_case& cs, const std::vector<T9>& grad, const std::vecto
     const int lim = cs.cfg.limiter;
     for (long long i = 0; i < cs.nCells; ++i) {
         const Cell& c = cs.cells[i];
-        T9 list[12];
+        T9 list[12] = {};
         int nl = 0;
         for (int cx = 0; cx < c.nNb; ++cx) {
             const V3 d = vsub(vadd(cs.cells[c.nb[cx]].rC, c.nbShift[cx]), c.rC);
@@ -856,7 +856,8 @@ int doStep(fvo_case& cs, double dt) {
         for (int j = 0; j < c.nFaces; ++j) {
             const int fi = c.faces[j];
             const Face& F = cs.faces[fi];
-            const V3 delta = vsub(F.rC, c.rC);
+            // across a periodic wrap face the neighbour-side cell sits one period further on
+            const V3 delta = (F.own == i) ? vsub(F.rC, c.rC) : vsub(F.rC, vadd(c.rC, F.neiShift));
             FState s{};
             for (int k = 1; k <= NS; ++k) s.c[k] = vdot(limC[k][i], delta) + cs.c[k][i];
             s.v = vadd(tdot(limV[i], delta), cs.v[i]);
@@ -1161,8 +1162,8 @@ int fvo_get_conserved(const fvo_case* cs, double* const* out) {
     for (long long i = 0; i < cs->nCells; ++i) {
         for (int k = 0; k < NS; ++k) out[k][i] = cs->rho[k + 1][i];
         out[NS][i] = cs->rho[0][i];
-        for (int d = 0; d < cs->D; ++d) out[NS + 1 + d][i] = cs->m[i].x[d];
-        out[NS + 1 + cs->D][i] = cs->E[i];
+        for (int d = 0; d < 3; ++d) out[NS + 1 + d][i] = cs->m[i].x[d];
+        out[NS + 4][i] = cs->E[i];
     }
     return FV_OK;
 }
@@ -1172,9 +1173,8 @@ int fvo_set_conserved(fvo_case* cs, const double* const* in) {
     for (long long i = 0; i < cs->nCells; ++i) {
         for (int k = 0; k < NS; ++k) cs->rho[k + 1][i] = in[k][i];
         cs->rho[0][i] = in[NS][i];
-        cs->m[i] = v3(0, 0, 0);
-        for (int d = 0; d < cs->D; ++d) cs->m[i].x[d] = in[NS + 1 + d][i];
-        cs->E[i] = in[NS + 1 + cs->D][i];
+        for (int d = 0; d < 3; ++d) cs->m[i].x[d] = in[NS + 1 + d][i];
+        cs->E[i] = in[NS + 4][i];
         cellPrimitivesFromConserved(*cs, i);
     }
     return FV_OK;

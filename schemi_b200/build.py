@@ -1,0 +1,87 @@
+"""Build recipe of the CUDA library ``schemi_b200/lib/libschemi_fv.so`` (sm_100a).
+
+    python -m schemi_b200.build            # or build() from Python
+
+Translation units:
+  csrc/fv_f64.cu   FP64 step kernels, --fmad=false (bit-exact with the reference build)
+  csrc/fv_f32.cu   FP32-flux step kernels
+  csrc/fv_capi.cu  C-ABI, upload/download/finalize kernels, device time loop (--fmad=false)
+  csrc/fv_batch.cu batched persistent ensemble kernel
+nvcc cross-compiles for sm_100a without a GPU.
+"""
+
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIBDIR = os.path.join(HERE, "lib")
+LIB = os.path.join(LIBDIR, "libschemi_fv.so")
+BUILD = os.path.join(HERE, "_build")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "--expt-relaxed-constexpr",
+          "-I", os.path.join(HERE, "..", "include")]
+UNITS = {
+    "fv_f64.cu": ["--fmad=false"],
+    "fv_f32.cu": [],
+    "fv_capi.cu": ["--fmad=false"],
+}
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _sources():
+    return [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".inc", ".h"))]
+
+
+def _stale(target: str, deps) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(verbose: bool = False, force: bool = False, extra_flags=None) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    os.makedirs(LIBDIR, exist_ok=True)
+    deps = _sources() + [os.path.join(HERE, "..", "include", "fvstep.h")]
+    units = dict(UNITS)
+    if os.path.exists(os.path.join(CSRC, "fv_batch.cu")):
+        units["fv_batch.cu"] = ["--fmad=false"]
+    objs = []
+    jobs = []
+    for unit, flags in units.items():
+        obj = os.path.join(BUILD, unit.replace(".cu", ".o"))
+        objs.append(obj)
+        if force or _stale(obj, deps):
+            cmd = [nvcc(), *ARCH, *COMMON, *flags, *(extra_flags or []), "-c", os.path.join(CSRC, unit), "-o", obj]
+            jobs.append(cmd)
+    with cf.ThreadPoolExecutor(max_workers=max(1, len(jobs))) as ex:
+        futs = [ex.submit(subprocess.run, cmd, capture_output=True, text=True) for cmd in jobs]
+        for cmd, fut in zip(jobs, futs):
+            res = fut.result()
+            if verbose or res.returncode != 0:
+                sys.stderr.write(" ".join(cmd) + "\n" + res.stdout + res.stderr)
+            if res.returncode != 0:
+                raise RuntimeError(f"nvcc failed for {cmd[-3]}")
+    if force or jobs or _stale(LIB, objs):
+        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError("link failed:\n" + res.stdout + res.stderr)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv, force="-f" in sys.argv))

@@ -38,8 +38,6 @@ PATCHES = ["tail", "point", "bottom", "right", "left", "top"]
 # which patches a task of dimension D uses (the others are "blank" in the task files)
 PATCHES_USED = {1: ["tail", "point"], 2: ["tail", "point", "right", "left"],
                 3: ["tail", "point", "bottom", "right", "left", "top"]}
-# conserved fields per cell, in device order
-# rho_1..rho_N, rho, m_x..m_D, E
 
 
 class fv_config_t(ctypes.Structure):
@@ -163,7 +161,8 @@ class Case:
 
     @property
     def n_conserved(self) -> int:
-        return self.n_species + 1 + self.dims + 1
+        """rho_1..rho_N, rho, m_x, m_y, m_z, E."""
+        return self.n_species + 5
 
     @property
     def R(self) -> float:

@@ -1,0 +1,855 @@
+// fv_capi.cu -- the C-ABI of include/fvstep.h: handle management, geometry tables, upload /
+// download, the device-resident time loop (CUDA graphs of step chunks) and error reporting.
+//
+// Built with --fmad=false: the upload kernel restates phaseInitialization.cpp:1827-1885 and the
+// finalize kernel the CFL block of Schemi.cpp:807-835 with the reference's rounding.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/fvstep.h"
+#include "fv_launch.cuh"
+
+using namespace fv;
+
+// ============================================================================ device kernels
+namespace {
+
+// phaseInitialization.cpp:1827-1885 for one cell
+template <int NS, int EOS>
+__global__ void k_upload(const StepParams P, const double* __restrict__ prim, double* __restrict__ U) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= P.ncell) return;
+    const long long s = P.stride;
+    double c[NS + 1], rho[NS + 1];
+    c[0] = 0;
+#pragma unroll
+    for (int k = 1; k <= NS; ++k) {
+        c[k] = prim[(k - 1) * s + i];
+        c[0] += c[k];
+    }
+#pragma unroll
+    for (int k = 1; k <= NS; ++k) rho[k] = c[k] * P.mix.M[k - 1];
+    rho[0] = 0;
+#pragma unroll
+    for (int k = 1; k <= NS; ++k) rho[0] += rho[k];
+    const double v[3] = {prim[NS * s + i], prim[(NS + 1) * s + i], prim[(NS + 2) * s + i]};
+    const double p = prim[(NS + 3) * s + i];
+    const double Uv = Mixture<double, NS, EOS>::UvFromp(P.mix, c, p);
+    double v2 = 0;
+    v2 += v[0] * v[0];
+    v2 += v[1] * v[1];
+    v2 += v[2] * v[2];
+    const double E = Uv + rho[0] * v2 * 0.5 + 0.0;
+#pragma unroll
+    for (int k = 1; k <= NS; ++k) U[(k - 1) * s + i] = rho[k];
+    U[NS * s + i] = rho[0];
+    for (int d = 0; d < 3; ++d) U[(NS + 1 + d) * s + i] = v[d] * rho[0];
+    U[(NS + 4) * s + i] = E;
+}
+
+// output set (fv_field order) of one cell; primitives from the restart set before step 1
+template <int NS, int EOS>
+__global__ void k_download(const StepParams P, const double* __restrict__ U, const double* __restrict__ prim0,
+                           const DevClock* __restrict__ ck, double* __restrict__ out) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= P.ncell) return;
+    const long long n = P.ncell, s = P.stride;
+    double c[NS + 1], v[3], p, rho0, rho[NS + 1], m[3], E;
+    const double* prim = ck->first ? prim0 : nullptr;
+    switch (P.dims) {
+    case 1: cellPrimitive<double, NS, EOS, 1>(P, U, prim, i, c, v, p, rho0, rho, m, E); break;
+    case 2: cellPrimitive<double, NS, EOS, 2>(P, U, prim, i, c, v, p, rho0, rho, m, E); break;
+    default: cellPrimitive<double, NS, EOS, 3>(P, U, prim, i, c, v, p, rho0, rho, m, E); break;
+    }
+    double Uv;
+    if (prim) {
+        Uv = Mixture<double, NS, EOS>::UvFromp(P.mix, c, p);
+    } else {
+        double v2 = 0;
+        v2 += v[0] * v[0];
+        v2 += v[1] * v[1];
+        v2 += v[2] * v[2];
+        Uv = E - rho0 * v2 * 0.5 - 0.0;
+    }
+    for (int k = 0; k < NS; ++k) out[(FV_F_CONC + k) * n + i] = c[k + 1];
+    out[FV_F_VX * n + i] = v[0];
+    out[FV_F_VY * n + i] = v[1];
+    out[FV_F_VZ * n + i] = v[2];
+    out[FV_F_P * n + i] = p;
+    for (int k = 0; k < NS; ++k) out[(FV_F_RHO_K + k) * n + i] = rho[k + 1];
+    out[FV_F_RHO * n + i] = rho0;
+    out[FV_F_MX * n + i] = m[0];
+    out[FV_F_MY * n + i] = m[1];
+    out[FV_F_MZ * n + i] = m[2];
+    out[FV_F_E * n + i] = E;
+    out[FV_F_UV * n + i] = Uv;
+    out[FV_F_T * n + i] = Mixture<double, NS, EOS>::TFromUv(P.mix, c, Uv);
+    out[FV_F_SONIC * n + i] = sqrt(Mixture<double, NS, EOS>::sqSonic(P.mix, c, rho0, Uv, p));
+}
+
+// flag |= (any transverse velocity component of the restart set is non-zero)
+__global__ void k_transverse(const StepParams P, const double* __restrict__ prim, int* flag) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= P.ncell) return;
+    bool nz = false;
+    for (int d = P.dims; d < 3; ++d) nz |= prim[(P.mix.ns + d) * P.stride + i] != 0.0;
+    if (nz) atomicOr(flag, 1);
+}
+
+}  // namespace
+
+namespace fv {
+// CFL block of Schemi.cpp:802-835 and the last-step clamp of :933-935.
+__global__ void k_finalize(const StepParams P, DevClock* ck, const double* __restrict__ blockMax, int nblocks) {
+    __shared__ double red[32];
+    if (ck->done) return;
+    double m = -1;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) m = smax(m, blockMax[b]);
+    m = blockMaxReduce<double>(m, red);
+    if (threadIdx.x != 0) return;
+    const double dtUsed = ck->dt;
+    double dtn = P.courant / m;
+    if (!P.courant_only) dtn = smin(dtn, kVeryBigD());
+    dtn = smax(dtn, P.min_dt);
+    if (P.gravity) {
+        for (int d = 0; d < 3; ++d) ck->g[d] += ck->g_delta[d] * dtUsed;
+    }
+    ck->time += dtUsed;
+    ck->steps += 1;
+    ck->first = 0;
+    ck->dt_used = dtUsed;
+    ck->dt_free = dtn;
+    if ((ck->time + dtn) > ck->t_end) dtn = ck->t_end - ck->time;
+    ck->dt = dtn;
+    if (!(ck->time < ck->t_end) || ck->err) ck->done = 1;
+}
+}  // namespace fv
+
+// ============================================================================ host side
+struct fv_handle {
+    fv_config cfg;
+    StepParams P;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double* U[2] = {nullptr, nullptr};
+    int cur = 0;
+    double* prim0 = nullptr;
+    DevClock* ck = nullptr;        // device clock
+    DevClock* ckHost = nullptr;    // pinned mirror
+    double* blockMax = nullptr;
+    long long blockMaxCap = 0;
+    double* geo = nullptr;         // all geometry tables
+    void* Pc = nullptr;            // generic scratch
+    void* FS = nullptr;
+    void* FL = nullptr;
+    GenericLayout L{};
+    double* outBuf = nullptr;      // download staging
+    int path = PATH_GENERIC;
+    MarchShape shape{128, 1, 32};
+    int nConserved = 0;
+    // graphs of step chunks, one per start buffer
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int graphSteps = 0;
+    std::string err;
+};
+
+namespace {
+
+const char* kNoHandle = "invalid handle";
+
+fv_status fail(fv_handle* h, int code, const std::string& msg) {
+    if (h) h->err = msg;
+    return code;
+}
+
+fv_status cudaFail(fv_handle* h, cudaError_t e, const char* what) {
+    return fail(h, FV_ERR_SYSTEM, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define FV_CUDA(h, call)                                      \
+    do {                                                      \
+        cudaError_t e_ = (call);                              \
+        if (e_ != cudaSuccess) return cudaFail((h), e_, #call); \
+    } while (0)
+
+// scaled hypot of one non-zero component (|x| exactly)
+double edge(double a, double b) { return std::fabs(b - a); }
+
+bool validate(const fv_config& c, std::string& e) {
+    if (c.dims < 1 || c.dims > 3) { e = "dims must be 1, 2 or 3"; return false; }
+    for (int d = 0; d < c.dims; ++d)
+        if (c.n[d] < 1) { e = "cell counts must be positive"; return false; }
+    for (int d = 0; d < 3; ++d)
+        if (!(c.L[d] > 0)) { e = "parallelepiped extents must be positive"; return false; }
+    if (c.n_species < 1 || c.n_species > FV_MAX_SPECIES) { e = "n_species must be 1..4"; return false; }
+    if (c.eos != FV_EOS_IDEAL && c.eos != FV_EOS_VAN_DER_WAALS) { e = "unknown equation of state"; return false; }
+    if (c.flux != FV_FLUX_HLLC && c.flux != FV_FLUX_HLL) { e = "unknown flux solver"; return false; }
+    if (c.limiter < 0 || c.limiter > FV_LIM_SCHMIDTMANN) { e = "unknown limiter"; return false; }
+    if (c.precision != FV_PREC_F64 && c.precision != FV_PREC_F32_FLUX) { e = "unknown precision"; return false; }
+    for (int k = 0; k < c.n_species; ++k)
+        if (!(c.M[k] > 0) || !(c.Cv[k] > 0)) { e = "molar mass and Cv must be positive"; return false; }
+    static const int lo[3] = {FV_PATCH_TAIL, FV_PATCH_RIGHT, FV_PATCH_BOTTOM};
+    static const int hi[3] = {FV_PATCH_POINT, FV_PATCH_LEFT, FV_PATCH_TOP};
+    for (int a = 0; a < c.dims; ++a) {
+        for (int side = 0; side < 2; ++side) {
+            const int p = side ? hi[a] : lo[a];
+            auto okType = [](int t) {
+                return t == FV_BC_FREE || t == FV_BC_SLIP || t == FV_BC_FIXED_CELL || t == FV_BC_FIXED_SURFACE ||
+                       t == FV_BC_PERIODIC;
+            };
+            if (!okType(c.bc_vel[p]) || !okType(c.bc_p[p])) { e = "unknown boundary condition type"; return false; }
+            for (int k = 0; k < c.n_species; ++k)
+                if (!okType(c.bc_conc[p][k])) { e = "unknown boundary condition type"; return false; }
+        }
+        const bool per = c.bc_vel[lo[a]] == FV_BC_PERIODIC;
+        auto allPer = [&](int p) {
+            if ((c.bc_vel[p] == FV_BC_PERIODIC) != per || (c.bc_p[p] == FV_BC_PERIODIC) != per) return false;
+            for (int k = 0; k < c.n_species; ++k)
+                if ((c.bc_conc[p][k] == FV_BC_PERIODIC) != per) return false;
+            return true;
+        };
+        if (!allPer(lo[a]) || !allPer(hi[a])) {
+            e = "a periodic axis needs periodic conditions for every field on both patches";
+            return false;
+        }
+        if (per && c.n[a] < 2) { e = "a periodic axis needs at least 2 cells"; return false; }
+    }
+    if (c.chemistry != FV_CHEM_NONE && c.chemistry != FV_CHEM_A_B_2C) { e = "unknown chemistry"; return false; }
+    if (c.chemistry == FV_CHEM_A_B_2C && c.n_species < 3) { e = "A+B->2C needs 3 species"; return false; }
+    return true;
+}
+
+// Per-axis geometry tables with the mesh generator's arithmetic (mesh.cpp:296-1900):
+// node coordinates 0 + d*i, cell centres as the 8-corner average, face centres as the
+// 4-corner average in the corner order of each face type.
+void buildGeometry(const fv_config& c, std::vector<double>& host, size_t off[3][5], int nAxis[3]) {
+    host.clear();
+    for (int a = 0; a < 3; ++a) {
+        const bool used = a < c.dims;
+        const int n = used ? c.n[a] : 1;
+        nAxis[a] = n;
+        const double L = c.L[a];
+        const double d = L / n;
+        auto node = [&](int i) -> double {
+            if (used) return 0.0 + d * (double)(size_t)i;
+            return i == 0 ? 0.0 : L;
+        };
+        // h
+        off[a][0] = host.size();
+        for (int i = 0; i < n; ++i) host.push_back(edge(node(i), node(i + 1)));
+        // cell centre: pattern x: a b a b a b a b ; y: a a b b a a b b ; z: a a a a b b b b
+        off[a][1] = host.size();
+        for (int i = 0; i < n; ++i) {
+            const double A = node(i), B = node(i + 1);
+            double seq[8];
+            for (int q = 0; q < 8; ++q) {
+                const int bit = a == 0 ? (q & 1) : (a == 1 ? ((q >> 1) & 1) : ((q >> 2) & 1));
+                seq[q] = bit ? B : A;
+            }
+            double s = seq[0] + seq[1];
+            for (int q = 2; q < 8; ++q) s = s + seq[q];
+            host.push_back(s / 8.);
+        }
+        // own-axis face centre: X at all four corners; X = 0 + 0., 0 + d*i, 0 + L
+        off[a][2] = host.size();
+        for (int i = 0; i <= n; ++i) {
+            double X;
+            if (i == 0) X = 0.0 + 0.;
+            else if (i == n) X = 0.0 + L;
+            else X = node(i);
+            double s = X + X;
+            s = s + X;
+            s = s + X;
+            host.push_back(s / 4.);
+        }
+        // transverse face-centre coordinates
+        off[a][3] = host.size();
+        for (int i = 0; i < n; ++i) {
+            const double A = node(i), B = node(i + 1);
+            double s = A + A;
+            s = s + B;
+            s = s + B;
+            host.push_back(s / 4.);
+        }
+        off[a][4] = host.size();
+        for (int i = 0; i < n; ++i) {
+            const double A = node(i), B = node(i + 1);
+            double s = A + B;
+            s = s + A;
+            s = s + B;
+            host.push_back(s / 4.);
+        }
+    }
+}
+
+template <int NS, int EOS>
+void launchUpload(fv_handle* h, const double* primDev) {
+    const int tpb = 256;
+    const unsigned g = (unsigned)((h->P.ncell + tpb - 1) / tpb);
+    k_upload<NS, EOS><<<g, tpb, 0, h->stream>>>(h->P, primDev, h->U[h->cur]);
+}
+template <int NS, int EOS>
+void launchDownload(fv_handle* h) {
+    const int tpb = 256;
+    const unsigned g = (unsigned)((h->P.ncell + tpb - 1) / tpb);
+    k_download<NS, EOS><<<g, tpb, 0, h->stream>>>(h->P, h->U[h->cur], h->prim0, h->ck, h->outBuf);
+}
+template <template <int, int> class F> struct Dispatch;
+
+void upload(fv_handle* h, const double* primDev) {
+    const int ns = h->cfg.n_species;
+    const bool vdw = h->cfg.eos == FV_EOS_VAN_DER_WAALS;
+    switch (ns) {
+    case 1: vdw ? launchUpload<1, 1>(h, primDev) : launchUpload<1, 0>(h, primDev); break;
+    case 2: vdw ? launchUpload<2, 1>(h, primDev) : launchUpload<2, 0>(h, primDev); break;
+    case 3: vdw ? launchUpload<3, 1>(h, primDev) : launchUpload<3, 0>(h, primDev); break;
+    default: vdw ? launchUpload<4, 1>(h, primDev) : launchUpload<4, 0>(h, primDev); break;
+    }
+}
+void download(fv_handle* h) {
+    const int ns = h->cfg.n_species;
+    const bool vdw = h->cfg.eos == FV_EOS_VAN_DER_WAALS;
+    switch (ns) {
+    case 1: vdw ? launchDownload<1, 1>(h) : launchDownload<1, 0>(h); break;
+    case 2: vdw ? launchDownload<2, 1>(h) : launchDownload<2, 0>(h); break;
+    case 3: vdw ? launchDownload<3, 1>(h) : launchDownload<3, 0>(h); break;
+    default: vdw ? launchDownload<4, 1>(h) : launchDownload<4, 0>(h); break;
+    }
+}
+
+void destroyGraphs(fv_handle* h) {
+    for (auto& g : h->graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    h->graphSteps = 0;
+}
+
+StepBuffers buffersFor(fv_handle* h, int from) {
+    StepBuffers B;
+    B.U = h->U[from];
+    B.Un = h->U[from ^ 1];
+    B.prim0 = h->prim0;
+    B.ck = h->ck;
+    B.blockMax = h->blockMax;
+    B.blockMaxCap = h->blockMaxCap;
+    B.Pc = h->Pc;
+    B.FS = h->FS;
+    B.FL = h->FL;
+    B.L = h->L;
+    return B;
+}
+
+long long stepBlocks(fv_handle* h) {
+    return h->path == PATH_MARCH ? marchBlocks(h->P, h->shape) : genericBlocks(h->P);
+}
+
+// enqueue step + finalize reading U[from]
+cudaError_t enqueueStep(fv_handle* h, int from) {
+    const StepBuffers B = buffersFor(h, from);
+    cudaError_t e = h->cfg.precision == FV_PREC_F64 ? launchStepF64(h->P, B, h->path, h->shape, h->stream)
+                                                     : launchStepF32(h->P, B, h->path, h->shape, h->stream);
+    if (e != cudaSuccess) return e;
+    k_finalize<<<1, 1024, 0, h->stream>>>(h->P, h->ck, h->blockMax, (int)stepBlocks(h));
+    return cudaGetLastError();
+}
+
+// Opt the chosen fused-march instantiation in to its dynamic shared memory; runs outside any
+// stream capture (a launch with null buffers and the legacy stream only configures).
+fv_status configureKernels(fv_handle* h) {
+    if (h->path != PATH_MARCH) return FV_OK;
+    StepBuffers B{};
+    cudaError_t e = h->cfg.precision == FV_PREC_F64 ? launchStepF64(h->P, B, PATH_MARCH, h->shape, nullptr)
+                                                     : launchStepF32(h->P, B, PATH_MARCH, h->shape, nullptr);
+    if (e != cudaSuccess) return cudaFail(h, e, "kernel configuration");
+    return FV_OK;
+}
+
+fv_status ensureScratch(fv_handle* h) {
+    const long long nb = std::max(marchBlocks(h->P, h->shape), genericBlocks(h->P));
+    if (nb > h->blockMaxCap) {
+        if (h->blockMax) cudaFree(h->blockMax);
+        FV_CUDA(h, cudaMalloc(&h->blockMax, sizeof(double) * nb));
+        h->blockMaxCap = nb;
+    }
+    if (configureKernels(h) != FV_OK) return FV_ERR_SYSTEM;
+    if (h->path == PATH_GENERIC && !h->FS) {
+        const size_t tsz = h->cfg.precision == FV_PREC_F64 ? sizeof(double) : sizeof(float);
+        const int ns = h->cfg.n_species;
+        const int nff = 2 * (ns + 1) + 10;
+        const int nfl = ns + 1 + 3 + 1;
+        FV_CUDA(h, cudaMalloc(&h->Pc, tsz * (ns + 4) * h->P.ncell));
+        FV_CUDA(h, cudaMalloc(&h->FS, tsz * 2 * nff * h->L.nfaces));
+        FV_CUDA(h, cudaMalloc(&h->FL, tsz * nfl * h->L.nfaces));
+    }
+    return FV_OK;
+}
+
+int choosePath(const fv_config& c) {
+    if (c.dims < 2) return PATH_GENERIC;
+    for (int a = 0; a < c.dims; ++a)
+        if (c.n[a] < 2) return PATH_GENERIC;
+    return limiterZeroForNonPositiveR(c.limiter) ? PATH_MARCH : PATH_GENERIC;
+}
+
+MarchShape defaultShape(const fv_config& c) {
+    if (c.dims == 2) return MarchShape{128, 1, 32};
+    return MarchShape{32, 8, 32};
+}
+
+fv_status readClock(fv_handle* h) {
+    FV_CUDA(h, cudaMemcpyAsync(h->ckHost, h->ck, sizeof(DevClock), cudaMemcpyDeviceToHost, h->stream));
+    FV_CUDA(h, cudaStreamSynchronize(h->stream));
+    return FV_OK;
+}
+
+fv_status clockError(fv_handle* h) {
+    const int e = h->ckHost->err;
+    if (!e) return FV_OK;
+    switch (e) {
+    case FV_ERR_RIEMANN: return fail(h, e, "Fatal error in Riemann solver.");
+    case FV_ERR_BOUNDARY: return fail(h, e, "fixedValueSurface is not a valid cell boundary value");
+    default: return fail(h, e, "device error");
+    }
+}
+
+}  // namespace
+
+// ============================================================================ C ABI
+extern "C" {
+
+int fv_abi_version(void) { return FV_ABI_VERSION; }
+
+const char* fv_last_error(const fv_handle* h) { return h ? h->err.c_str() : kNoHandle; }
+
+fv_status fv_create(const fv_config* cfg, fv_handle** out) {
+    if (!cfg || !out) return FV_ERR_INIT;
+    *out = nullptr;
+    std::string e;
+    if (!validate(*cfg, e)) {
+        fprintf(stderr, "fv_create: %s\n", e.c_str());
+        return FV_ERR_INIT;
+    }
+    fv_handle* h = new (std::nothrow) fv_handle();
+    if (!h) return FV_ERR_SYSTEM;
+    h->cfg = *cfg;
+    cudaError_t ce = cudaGetDevice(&h->device);
+    if (ce != cudaSuccess) {
+        delete h;
+        fprintf(stderr, "fv_create: no CUDA device: %s\n", cudaGetErrorString(ce));
+        return FV_ERR_SYSTEM;
+    }
+    StepParams& P = h->P;
+    memset(&P, 0, sizeof(P));
+    P.dims = cfg->dims;
+    for (int a = 0; a < 3; ++a) {
+        P.n[a] = a < cfg->dims ? cfg->n[a] : 1;
+        P.ext[a] = cfg->L[a];
+    }
+    P.periodic[0] = cfg->bc_vel[FV_PATCH_TAIL] == FV_BC_PERIODIC;
+    P.periodic[1] = cfg->dims >= 2 && cfg->bc_vel[FV_PATCH_RIGHT] == FV_BC_PERIODIC;
+    P.periodic[2] = cfg->dims >= 3 && cfg->bc_vel[FV_PATCH_BOTTOM] == FV_BC_PERIODIC;
+    P.ncell = (long long)P.n[0] * P.n[1] * P.n[2];
+    P.stride = P.ncell;
+    P.limiter = cfg->limiter;
+    P.flux = cfg->flux;
+    P.gravity = cfg->gravity;
+    P.courant_only = cfg->courant_only;
+    P.courant = cfg->courant;
+    P.min_dt = cfg->min_timestep;
+    MixParams& mp = P.mix;
+    mp.ns = cfg->n_species;
+    mp.eos_kind = cfg->eos;
+    mp.R = cfg->R;
+    for (int k = 0; k < cfg->n_species; ++k) {
+        mp.M[k] = cfg->M[k];
+        mp.Cv[k] = cfg->Cv[k];
+    }
+    if (cfg->eos == FV_EOS_VAN_DER_WAALS) {
+        // mixtureVanDerWaals.cpp:33-52
+        for (int k = 0; k < cfg->n_species; ++k) {
+            mp.b[k][k] = cfg->Tc[k] * mp.R / (8 * cfg->Pc[k]);
+            mp.a[k][k] = cfg->Pc[k] * mp.b[k][k] * mp.b[k][k] * 27;
+        }
+        for (int k = 0; k < cfg->n_species; ++k)
+            for (int l = 0; l < cfg->n_species; ++l)
+                if (k != l) {
+                    mp.b[k][l] = std::pow(0.5 * (std::cbrt(mp.b[k][k]) + std::cbrt(mp.b[l][l])), 3);
+                    mp.a[k][l] = std::sqrt(mp.a[k][k] * mp.a[l][l]);
+                }
+    }
+    for (int p = 0; p < 6; ++p) {
+        for (int k = 0; k < FV_MAX_SPECIES; ++k) {
+            P.bc.conc[p][k] = cfg->bc_conc[p][k];
+            P.bc.conc_value[p][k] = cfg->bc_conc_value[p][k];
+        }
+        P.bc.vel[p] = cfg->bc_vel[p];
+        for (int d = 0; d < 3; ++d) P.bc.vel_value[p][d] = cfg->bc_vel_value[p][d];
+        P.bc.p[p] = cfg->bc_p[p];
+        P.bc.p_value[p] = cfg->bc_p_value[p];
+    }
+    h->nConserved = cfg->n_species + 5;
+    P.nmom = cfg->dims;
+    h->path = choosePath(*cfg);
+    h->shape = defaultShape(*cfg);
+
+    // generic face layout
+    long long base = 0;
+    for (int a = 0; a < 3; ++a) {
+        h->L.faceBase[a] = base;
+        if (a < cfg->dims) {
+            long long cnt = P.n[a] + 1;
+            for (int b = 0; b < 3; ++b)
+                if (b != a) cnt *= P.n[b];
+            base += cnt;
+        }
+    }
+    h->L.nfaces = base;
+
+    std::vector<double> geo;
+    size_t off[3][5];
+    int nAxis[3];
+    buildGeometry(*cfg, geo, off, nAxis);
+
+    auto bail = [&](cudaError_t e2, const char* what) {
+        fprintf(stderr, "fv_create: %s: %s\n", what, cudaGetErrorString(e2));
+        fv_destroy(h);
+        return FV_ERR_SYSTEM;
+    };
+    if ((ce = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(ce, "stream");
+    if ((ce = cudaEventCreate(&h->ev0)) != cudaSuccess) return bail(ce, "event");
+    if ((ce = cudaEventCreate(&h->ev1)) != cudaSuccess) return bail(ce, "event");
+    const size_t stateBytes = sizeof(double) * h->nConserved * P.ncell;
+    for (int b = 0; b < 2; ++b)
+        if ((ce = cudaMalloc(&h->U[b], stateBytes)) != cudaSuccess) return bail(ce, "state");
+    if ((ce = cudaMalloc(&h->prim0, sizeof(double) * (cfg->n_species + 4) * P.ncell)) != cudaSuccess)
+        return bail(ce, "restart set");
+    if ((ce = cudaMalloc(&h->ck, sizeof(DevClock))) != cudaSuccess) return bail(ce, "clock");
+    if ((ce = cudaMallocHost(&h->ckHost, sizeof(DevClock))) != cudaSuccess) return bail(ce, "clock mirror");
+    if ((ce = cudaMalloc(&h->geo, sizeof(double) * geo.size())) != cudaSuccess) return bail(ce, "geometry");
+    if ((ce = cudaMemcpy(h->geo, geo.data(), sizeof(double) * geo.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return bail(ce, "geometry copy");
+    for (int a = 0; a < 3; ++a) {
+        P.geo.h[a] = h->geo + off[a][0];
+        P.geo.cc[a] = h->geo + off[a][1];
+        P.geo.fpos[a] = h->geo + off[a][2];
+        P.geo.aabb[a] = h->geo + off[a][3];
+        P.geo.abab[a] = h->geo + off[a][4];
+    }
+    memset(h->ckHost, 0, sizeof(DevClock));
+    h->ckHost->dt = cfg->min_timestep;
+    h->ckHost->dt_free = cfg->min_timestep;
+    h->ckHost->t_end = std::numeric_limits<double>::infinity();
+    h->ckHost->first = 1;
+    for (int d = 0; d < 3; ++d) {
+        h->ckHost->g[d] = cfg->g[d];
+        h->ckHost->g_delta[d] = cfg->g_delta[d];
+    }
+    if ((ce = cudaMemcpy(h->ck, h->ckHost, sizeof(DevClock), cudaMemcpyHostToDevice)) != cudaSuccess)
+        return bail(ce, "clock copy");
+    if (ensureScratch(h) != FV_OK) {
+        fprintf(stderr, "fv_create: %s\n", h->err.c_str());
+        fv_destroy(h);
+        return FV_ERR_SYSTEM;
+    }
+    *out = h;
+    return FV_OK;
+}
+
+void fv_destroy(fv_handle* h) {
+    if (!h) return;
+    destroyGraphs(h);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (auto& u : h->U)
+        if (u) cudaFree(u);
+    if (h->prim0) cudaFree(h->prim0);
+    if (h->ck) cudaFree(h->ck);
+    if (h->ckHost) cudaFreeHost(h->ckHost);
+    if (h->blockMax) cudaFree(h->blockMax);
+    if (h->geo) cudaFree(h->geo);
+    if (h->Pc) cudaFree(h->Pc);
+    if (h->FS) cudaFree(h->FS);
+    if (h->FL) cudaFree(h->FL);
+    if (h->outBuf) cudaFree(h->outBuf);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+// Carry all three momentum components when the restart set has a transverse velocity.
+static fv_status setMomentumComponents(fv_handle* h) {
+    int nmom = h->cfg.dims;
+    if (h->cfg.dims < 3) {
+        FV_CUDA(h, cudaMemsetAsync(&h->ck->pad, 0, sizeof(int), h->stream));
+        const unsigned g = (unsigned)((h->P.ncell + 255) / 256);
+        k_transverse<<<g, 256, 0, h->stream>>>(h->P, h->prim0, &h->ck->pad);
+        FV_CUDA(h, cudaGetLastError());
+        int flag = 0;
+        FV_CUDA(h, cudaMemcpyAsync(&flag, &h->ck->pad, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        FV_CUDA(h, cudaStreamSynchronize(h->stream));
+        if (flag) nmom = 3;
+    }
+    if (nmom != h->P.nmom) {
+        h->P.nmom = nmom;
+        destroyGraphs(h);
+    }
+    return FV_OK;
+}
+
+static fv_status resetClock(fv_handle* h) {
+    DevClock& c = *h->ckHost;
+    memset(&c, 0, sizeof(DevClock));
+    c.dt = h->cfg.min_timestep;
+    c.dt_free = h->cfg.min_timestep;
+    c.t_end = std::numeric_limits<double>::infinity();
+    c.first = 1;
+    for (int d = 0; d < 3; ++d) {
+        c.g[d] = h->cfg.g[d];
+        c.g_delta[d] = h->cfg.g_delta[d];
+    }
+    FV_CUDA(h, cudaMemcpyAsync(h->ck, h->ckHost, sizeof(DevClock), cudaMemcpyHostToDevice, h->stream));
+    return FV_OK;
+}
+
+fv_status fv_upload_device(fv_handle* h, const double* const* prim_dev) {
+    if (!h || !prim_dev) return FV_ERR_INIT;
+    const int nf = h->cfg.n_species + 4;
+    const long long n = h->P.ncell;
+    for (int f = 0; f < nf; ++f)
+        FV_CUDA(h, cudaMemcpyAsync(h->prim0 + f * n, prim_dev[f], sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                                   h->stream));
+    h->cur = 0;
+    fv_status st = setMomentumComponents(h);
+    if (st != FV_OK) return st;
+    upload(h, h->prim0);
+    FV_CUDA(h, cudaGetLastError());
+    st = resetClock(h);
+    if (st != FV_OK) return st;
+    FV_CUDA(h, cudaStreamSynchronize(h->stream));
+    return FV_OK;
+}
+
+fv_status fv_upload(fv_handle* h, const double* const* prim) {
+    if (!h || !prim) return FV_ERR_INIT;
+    const int nf = h->cfg.n_species + 4;
+    const long long n = h->P.ncell;
+    for (int f = 0; f < nf; ++f)
+        FV_CUDA(h, cudaMemcpyAsync(h->prim0 + f * n, prim[f], sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+    h->cur = 0;
+    fv_status st = setMomentumComponents(h);
+    if (st != FV_OK) return st;
+    upload(h, h->prim0);
+    FV_CUDA(h, cudaGetLastError());
+    st = resetClock(h);
+    if (st != FV_OK) return st;
+    FV_CUDA(h, cudaStreamSynchronize(h->stream));
+    return FV_OK;
+}
+
+fv_status fv_step(fv_handle* h, double* dt_used, double* dt_next) {
+    if (!h) return FV_ERR_INIT;
+    // single steps are never clamped to an end time
+    h->ckHost->t_end = std::numeric_limits<double>::infinity();
+    FV_CUDA(h, cudaMemcpyAsync(&h->ck->t_end, &h->ckHost->t_end, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    FV_CUDA(h, cudaMemsetAsync(&h->ck->done, 0, sizeof(int), h->stream));
+    FV_CUDA(h, enqueueStep(h, h->cur));
+    h->cur ^= 1;
+    fv_status st = readClock(h);
+    if (st != FV_OK) return st;
+    if (dt_used) *dt_used = h->ckHost->dt_used;
+    if (dt_next) *dt_next = h->ckHost->dt;
+    return clockError(h);
+}
+
+fv_status fv_run(fv_handle* h, double t_end, long long max_steps, fv_run_stats* stats) {
+    if (!h) return FV_ERR_INIT;
+    fv_status st = readClock(h);
+    if (st != FV_OK) return st;
+    const long long steps0 = h->ckHost->steps;
+    // main: mesh_.setTimestep(std::min(mesh_.timestep(), timeOfCalculation)) before the loop
+    DevClock& c = *h->ckHost;
+    c.t_end = t_end;
+    c.done = !(c.time < t_end);
+    c.dt = std::min(c.dt_free, t_end - c.time);
+    FV_CUDA(h, cudaMemcpyAsync(h->ck, h->ckHost, sizeof(DevClock), cudaMemcpyHostToDevice, h->stream));
+    const int chunk = 32;  // steps per graph
+    if (h->graphSteps != chunk) {
+        destroyGraphs(h);
+        for (int start = 0; start < 2; ++start) {
+            cudaGraph_t g;
+            FV_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+            int from = start;
+            for (int s = 0; s < chunk; ++s) {
+                cudaError_t e = enqueueStep(h, from);
+                if (e != cudaSuccess) {
+                    cudaStreamEndCapture(h->stream, &g);
+                    return cudaFail(h, e, "step capture");
+                }
+                from ^= 1;
+            }
+            FV_CUDA(h, cudaStreamEndCapture(h->stream, &g));
+            FV_CUDA(h, cudaGraphInstantiate(&h->graph[start], g, 0));
+            cudaGraphDestroy(g);
+        }
+        h->graphSteps = chunk;
+    }
+    FV_CUDA(h, cudaEventRecord(h->ev0, h->stream));
+    long long done = 0;
+    while (!c.done && done < max_steps) {
+        const long long left = max_steps - done;
+        if (left >= chunk) {
+            // a graph of `chunk` steps; steps after the end time are no-ops that leave the
+            // state in place, so the current buffer follows the executed step count
+            FV_CUDA(h, cudaGraphLaunch(h->graph[h->cur], h->stream));
+        } else {
+            int from = h->cur;
+            for (long long s = 0; s < left; ++s) {
+                FV_CUDA(h, enqueueStep(h, from));
+                from ^= 1;
+            }
+        }
+        const long long before = c.steps;
+        st = readClock(h);
+        if (st != FV_OK) return st;
+        const long long executed = c.steps - before;
+        if (executed & 1) h->cur ^= 1;
+        done += (left >= chunk) ? chunk : left;
+        if (c.err) break;
+    }
+    FV_CUDA(h, cudaEventRecord(h->ev1, h->stream));
+    FV_CUDA(h, cudaEventSynchronize(h->ev1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    if (stats) {
+        stats->time = c.time;
+        stats->dt_next = c.dt;
+        stats->steps = c.steps - steps0;
+        stats->device_ms = ms;
+    }
+    return clockError(h);
+}
+
+fv_status fv_download(fv_handle* h, double* const* out) {
+    if (!h || !out) return FV_ERR_INIT;
+    const long long n = h->P.ncell;
+    if (!h->outBuf) FV_CUDA(h, cudaMalloc(&h->outBuf, sizeof(double) * FV_F_COUNT * n));
+    download(h);
+    FV_CUDA(h, cudaGetLastError());
+    for (int f = 0; f < FV_F_COUNT; ++f) {
+        if (!out[f]) continue;
+        const bool species = (f >= FV_F_CONC && f < FV_F_CONC + FV_MAX_SPECIES) ||
+                             (f >= FV_F_RHO_K && f < FV_F_RHO_K + FV_MAX_SPECIES);
+        if (species) {
+            const int k = f >= FV_F_RHO_K ? f - FV_F_RHO_K : f - FV_F_CONC;
+            if (k >= h->cfg.n_species) continue;
+        }
+        FV_CUDA(h, cudaMemcpyAsync(out[f], h->outBuf + f * n, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+    }
+    FV_CUDA(h, cudaStreamSynchronize(h->stream));
+    return FV_OK;
+}
+
+fv_status fv_get_time(const fv_handle* hc, double* time, double* dt) {
+    fv_handle* h = const_cast<fv_handle*>(hc);
+    if (!h) return FV_ERR_INIT;
+    fv_status st = readClock(h);
+    if (st != FV_OK) return st;
+    if (time) *time = h->ckHost->time;
+    if (dt) *dt = h->ckHost->dt;
+    return FV_OK;
+}
+
+fv_status fv_set_time(fv_handle* h, double time, double dt) {
+    if (!h) return FV_ERR_INIT;
+    fv_status st = readClock(h);
+    if (st != FV_OK) return st;
+    h->ckHost->time = time;
+    h->ckHost->dt = dt;
+    h->ckHost->dt_free = dt;
+    FV_CUDA(h, cudaMemcpyAsync(h->ck, h->ckHost, sizeof(DevClock), cudaMemcpyHostToDevice, h->stream));
+    FV_CUDA(h, cudaStreamSynchronize(h->stream));
+    return FV_OK;
+}
+
+fv_status fv_state_device(fv_handle* h, double** fields, int* n_fields, long long* n_cells) {
+    if (!h) return FV_ERR_INIT;
+    if (n_fields) *n_fields = h->nConserved;
+    if (n_cells) *n_cells = h->P.ncell;
+    if (fields)
+        for (int f = 0; f < h->nConserved; ++f) fields[f] = h->U[h->cur] + f * h->P.stride;
+    return FV_OK;
+}
+
+fv_status fv_sync(fv_handle* h) {
+    if (!h) return FV_ERR_INIT;
+    FV_CUDA(h, cudaStreamSynchronize(h->stream));
+    return FV_OK;
+}
+
+// ---- introspection used by the tests and the bench (no reference counterpart)
+int fv_step_path(const fv_handle* h) { return h ? h->path : -1; }
+
+fv_status fv_set_march_shape(fv_handle* h, int bx, int by, int rows) {
+    if (!h) return FV_ERR_INIT;
+    MarchShape s{bx, by, rows};
+    if (!marchShapeSupported(h->cfg.dims, s) || rows < 1) return fail(h, FV_ERR_INIT, "unsupported march shape");
+    h->shape = s;
+    destroyGraphs(h);
+    return ensureScratch(h);
+}
+
+fv_status fv_force_generic(fv_handle* h) {
+    if (!h) return FV_ERR_INIT;
+    h->path = PATH_GENERIC;
+    destroyGraphs(h);
+    return ensureScratch(h);
+}
+
+// Time `iters` launches of one step kernel (no finalize, state untouched) for the shape.
+fv_status fv_time_step_kernel(fv_handle* h, int iters, float* ms_per_step) {
+    if (!h || iters < 1) return FV_ERR_INIT;
+    const StepBuffers B = buffersFor(h, h->cur);
+    // use the second buffer as the output; U[cur] is unchanged
+    FV_CUDA(h, cudaEventRecord(h->ev0, h->stream));
+    for (int i = 0; i < iters; ++i) {
+        cudaError_t e = h->cfg.precision == FV_PREC_F64 ? launchStepF64(h->P, B, h->path, h->shape, h->stream)
+                                                         : launchStepF32(h->P, B, h->path, h->shape, h->stream);
+        if (e != cudaSuccess) return cudaFail(h, e, "step launch");
+    }
+    FV_CUDA(h, cudaEventRecord(h->ev1, h->stream));
+    FV_CUDA(h, cudaEventSynchronize(h->ev1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    *ms_per_step = ms / iters;
+    return FV_OK;
+}
+
+}  // extern "C"
+
+// ============================================================================ shapes
+namespace fv {
+long long marchBlocks(const StepParams& P, const MarchShape& s) {
+    if (P.dims < 2) return 0;
+    const long long gx = (P.n[0] + s.bx - 3) / (s.bx - 2);
+    if (P.dims == 2) return gx * ((P.n[1] + s.rows - 1) / s.rows);
+    const long long gy = (P.n[1] + s.by - 3) / (s.by - 2);
+    return gx * gy * ((P.n[2] + s.rows - 1) / s.rows);
+}
+long long genericBlocks(const StepParams& P) { return (P.ncell + 127) / 128; }
+bool marchShapeSupported(int dims, const MarchShape& s) {
+    if (dims == 2) return s.by == 1 && (s.bx == 64 || s.bx == 128 || s.bx == 256);
+    if (dims == 3) return (s.bx == 32 && (s.by == 8 || s.by == 16)) || (s.bx == 64 && s.by == 8);
+    return false;
+}
+}  // namespace fv

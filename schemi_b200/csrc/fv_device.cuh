@@ -1,0 +1,432 @@
+// fv_device.cuh -- device-side physics of the explicit finite-volume step.
+//
+// Point functions of the reference's step, written for registers: mixture EOS, limiter
+// functions, face-state closures, boundary ghost values and the HLLC / HLL fluxes.  Each
+// expression keeps the reference's operation order (paths inside the Schemi project):
+//   EOS          src/thermodynamics/mixtureIdeal.cpp, idealFluid.cpp:13-60,
+//                mixtureVanDerWaals.cpp:88-146,309-397, vanDerWaalsFluid.cpp:14-75
+//   limiters     src/limiters/<name>Limiter.cpp
+//   closures     src/Advections/Advection.cpp:238-387, HancockStage.cpp:177-306
+//   ghosts       headers/boundaryConditionValue.hpp:279-300, src/boundary/slipFunction.cpp:21-25
+//   HLLC / HLL   src/RiemannSolvers/HLLCSolver.cpp:52-403, HLLSolver.cpp:52-300
+// so that the FP64 instantiation, compiled without FMA contraction, reproduces the reference
+// bit for bit.  The FP32 instantiation is the "FP32 flux" arithmetic of the fast path.
+//
+// Normals of the structured mesh are exact signed unit vectors along an axis, so a normal is
+// carried as (axis, sign) and v & N reduces to sign * v[axis] exactly.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/fvstep.h"
+
+namespace fv {
+
+constexpr int MAXS = FV_MAX_SPECIES;
+
+// constants of globalConstants.hpp:22-35
+__host__ __device__ constexpr double kStabD() { return 5 * 2.220446049250313080847e-16; }
+__host__ __device__ constexpr double kVeryBigD() { return 1E-3 * 1.7976931348623157e308; }
+
+template <typename T> struct Num;
+template <> struct Num<double> {
+    __device__ static double stab() { return kStabD(); }
+    __device__ static double sqrt_(double x) { return sqrt(x); }
+    __device__ static double abs_(double x) { return fabs(x); }
+};
+template <> struct Num<float> {
+    __device__ static float stab() { return 5.0f * 1.1920929e-07f; }
+    __device__ static float sqrt_(float x) { return sqrtf(x); }
+    __device__ static float abs_(float x) { return fabsf(x); }
+};
+
+// std::min / std::max semantics (first argument wins ties and unordered comparisons)
+template <typename T> __device__ __forceinline__ T smin(T a, T b) { return (b < a) ? b : a; }
+template <typename T> __device__ __forceinline__ T smax(T a, T b) { return (a < b) ? b : a; }
+
+// Scaled 3-argument hypot with the semantics of the reference build's std::hypot(x, y, z).
+template <typename T> __device__ __forceinline__ T mag3(T x, T y, T z) {
+    x = Num<T>::abs_(x); y = Num<T>::abs_(y); z = Num<T>::abs_(z);
+    const T a = x < y ? (y < z ? z : y) : (x < z ? z : x);
+    if (a == T(0)) return T(0);
+    const T xa = x / a, ya = y / a, za = z / a;
+    return a * Num<T>::sqrt_(xa * xa + ya * ya + za * za);
+}
+
+// ------------------------------------------------------------------ mixture parameters
+struct MixParams {
+    int ns;        // number of species
+    int eos_kind;  // fv_eos
+    double R;
+    double M[MAXS];
+    double Cv[MAXS];
+    double a[MAXS][MAXS];
+    double b[MAXS][MAXS];
+};
+
+template <typename T, int NS, int EOS>
+struct Mixture {
+    // X_k = c_k / c_0 ; Cv_mix = sum X_k Cv_k (fractionCalculation.cpp:36-44, mixtureIdeal.cpp)
+    __device__ __forceinline__ static void params(const MixParams& mp, const T* c, T& g1, T& am, T& bm, T& Mm) {
+        T X[NS];
+#pragma unroll
+        for (int k = 0; k < NS; ++k) X[k] = c[k + 1] / c[0];
+        T Cvm = 0;
+        Mm = 0;
+#pragma unroll
+        for (int k = 0; k < NS; ++k) {
+            Cvm += X[k] * T(mp.Cv[k]);
+            Mm += X[k] * T(mp.M[k]);
+        }
+        g1 = T(mp.R) / Cvm;
+        am = 0;
+        bm = 0;
+        if (EOS == FV_EOS_VAN_DER_WAALS) {
+#pragma unroll
+            for (int k = 0; k < NS; ++k)
+#pragma unroll
+                for (int l = 0; l < NS; ++l) {
+                    am += X[k] * X[l] * T(mp.a[k][l]);
+                    bm += X[k] * X[l] * T(mp.b[k][l]);
+                }
+        }
+    }
+    __device__ __forceinline__ static T pFromUv(const MixParams& mp, const T* c, T Uv) {
+        T g1, am, bm, Mm;
+        params(mp, c, g1, am, bm, Mm);
+        if (EOS == FV_EOS_IDEAL) return g1 * Uv;
+        const T acc = am * (c[0] * c[0]);
+        return g1 * (Uv + acc) / (T(1) - c[0] * bm) - acc;
+    }
+    __device__ __forceinline__ static T UvFromp(const MixParams& mp, const T* c, T p) {
+        T g1, am, bm, Mm;
+        params(mp, c, g1, am, bm, Mm);
+        if (EOS == FV_EOS_IDEAL) return p / g1;
+        const T acc = am * (c[0] * c[0]);
+        return (p + acc) * (T(1) - c[0] * bm) / g1 - acc;
+    }
+    __device__ __forceinline__ static T TFromUv(const MixParams& mp, const T* c, T Uv) {
+        T g1, am, bm, Mm;
+        params(mp, c, g1, am, bm, Mm);
+        const T Cvm = T(mp.R) / g1;  // only used for output; not bit-matched
+        if (EOS == FV_EOS_IDEAL) return Uv / ((c[0] + Num<T>::stab()) * Cvm);
+        return (Uv + am * (c[0] * c[0])) / ((c[0] + Num<T>::stab()) * Cvm);
+    }
+    // sqSonicSpeed = dpdrho + dpdUv * (Uv + p) / rho
+    __device__ __forceinline__ static T sqSonic(const MixParams& mp, const T* c, T rho, T Uv, T p) {
+        T g1, am, bm, Mm;
+        params(mp, c, g1, am, bm, Mm);
+        if (EOS == FV_EOS_IDEAL) return T(0) + g1 * (Uv + p) / rho;
+        const T m_cb = T(1) - c[0] * bm;
+        const T ac = am * c[0];
+        const T dpdrho = (g1 * (T(2) * ac / m_cb - bm * (Uv + ac * c[0]) / (m_cb * m_cb)) - T(2) * ac) / Mm;
+        const T dUv = g1 / m_cb;
+        return dpdrho + dUv * (Uv + p) / rho;
+    }
+};
+
+// ------------------------------------------------------------------ limiter functions
+template <typename T> __device__ __forceinline__ T limiterPhi(int lim, T r, T xiR) {
+    const T one = 1, two = 2;
+    switch (lim) {
+    case FV_LIM_ZERO: return 0;
+    case FV_LIM_MINMOD:
+        if (r <= T(0)) return 0;
+        if (r <= one) return r;
+        return smin(one, xiR);
+    case FV_LIM_VANLEER:
+        if (r < T(0)) return 0;
+        return smin(two * r / (one + r), xiR);
+    case FV_LIM_LINEAR: return one;
+    case FV_LIM_VANALBADA:
+        if (r <= T(0)) return 0;
+        return smin((r * r + r) / (one + r * r), xiR);
+    case FV_LIM_HQUICK:
+        if (r <= T(0)) return 0;
+        return smin(T(4) * r / (T(3) + r), xiR);
+    case FV_LIM_VANLEER2: {
+        if (r <= T(0)) return 0;
+        const T denom = one + r;
+        return smin(T(4) * r / (denom * denom), two * xiR);
+    }
+    case FV_LIM_SUPERBEE:
+        if (r <= T(0)) return 0;
+        if (r <= T(0.5)) return two * r;
+        if (r <= one) return r;
+        return smin(smin(r, two), xiR);
+    case FV_LIM_VANALBADA2:
+        if (r <= T(0)) return 0;
+        return smin(two * r / (one + r * r), two * xiR);
+    case FV_LIM_MINMOD2:
+        if (r <= T(0)) return 0;
+        return smin(smin(one, T(4) * r / (one + r)), two * xiR);
+    case FV_LIM_SWEBY: {
+        const T b = 2;
+        if (r <= T(0)) return 0;
+        return smin(smin(smin(one, b * r), smin(b, r)), b * xiR);
+    }
+    case FV_LIM_KOREN:
+        if (r <= T(0)) return 0;
+        return smin(smin(smin(two * r, (one + two * r) / T(3)), two), two * xiR);
+    case FV_LIM_KOREN2: {
+        const T tt = T(2. / 3.);
+        if (r <= T(0)) return smin(T(0), smax(-tt, (one + two * r) / T(3)));
+        return smin(smin(two * tt * r, smin((one + two * r) / T(3), two)), two * xiR);
+    }
+    case FV_LIM_UTCDFS:
+        if (r < T(-1)) return r * (r + one) / (r * r + one);
+        if ((r >= T(-1)) && (r < T(0))) return 0;
+        if ((r >= T(0)) && (r < T(0.5))) return r * r * r - two * (r * r) + two * r;
+        if ((r >= T(0.5)) && (r < two)) return T(0.75) * r + T(0.25);
+        return smin((two * (r * r) - two * r - T(9.0 / 4.0)) / (r * r - r - one), two * xiR);
+    case FV_LIM_SCHMIDTMANN: {
+        const T alpha = 1, beta = 2, gamma = 1.5;
+        const T phiO3 = (two + r) / T(3);
+        return smin(smax(T(0), smin(phiO3, smax(-alpha * r, smin(smin(beta * r, phiO3), gamma)))), two * xiR);
+    }
+    }
+    return 0;
+}
+
+// True when phi(r) == 0 for every r <= 0: on a multi-dimensional structured mesh the r-ratio
+// of every gradient component is <= 0 (transverse neighbours contribute an exact 0 to the
+// component-wise min/max of TVDLimiter.cpp:103-119), so these limiters give zero slopes and
+// the reconstruction is piecewise constant.
+__host__ __device__ inline bool limiterZeroForNonPositiveR(int lim) {
+    switch (lim) {
+    case FV_LIM_LINEAR: case FV_LIM_KOREN2: case FV_LIM_UTCDFS: case FV_LIM_SCHMIDTMANN: return false;
+    default: return true;
+    }
+}
+
+// ------------------------------------------------------------------ face states
+// One side of one face: primitives + conserved + sound speed.
+template <typename T, int NS>
+struct FaceState {
+    T c[NS + 1];    // c[0] = total concentration
+    T rho[NS + 1];  // rho[0] = mixture density (evolved separately)
+    T v[3], m[3];
+    T E, Uv, p, cs;
+};
+
+// Closure of a reconstructed primitive state (Advection.cpp:238-303 / :305-387).
+template <typename T, int NS, int EOS>
+__device__ __forceinline__ void closeFromPrimitive(const MixParams& mp, FaceState<T, NS>& s) {
+    s.c[0] = 0;
+    s.rho[0] = 0;
+#pragma unroll
+    for (int k = 1; k <= NS; ++k) {
+        s.c[0] += s.c[k];
+        s.rho[k] = s.c[k] * T(mp.M[k - 1]);
+        s.rho[0] += s.rho[k];
+    }
+    s.Uv = Mixture<T, NS, EOS>::UvFromp(mp, s.c, s.p);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) s.m[d] = s.v[d] * s.rho[0];
+    T v2 = 0;
+    v2 += s.v[0] * s.v[0];
+    v2 += s.v[1] * s.v[1];
+    v2 += s.v[2] * s.v[2];
+    s.E = s.Uv + s.rho[0] * v2 * T(0.5) + T(0);
+}
+
+// Recalculation from conserved face values (HancockStage.cpp:177-224, Advection.cpp:455-479).
+template <typename T, int NS, int EOS>
+__device__ __forceinline__ void closeFromConserved(const MixParams& mp, FaceState<T, NS>& s) {
+    s.c[0] = 0;
+#pragma unroll
+    for (int k = 1; k <= NS; ++k) {
+        s.c[k] = s.rho[k] / T(mp.M[k - 1]);
+        s.c[0] += s.c[k];
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) s.v[d] = s.m[d] / s.rho[0];
+    T v2 = 0;
+    v2 += s.v[0] * s.v[0];
+    v2 += s.v[1] * s.v[1];
+    v2 += s.v[2] * s.v[2];
+    s.Uv = s.E - s.rho[0] * v2 * T(0.5) - T(0);
+    s.p = Mixture<T, NS, EOS>::pFromUv(mp, s.c, s.Uv);
+}
+
+// Sound speed of HLLCSolver.cpp:26-50 with zero turbulent energy.
+template <typename T, int NS, int EOS>
+__device__ __forceinline__ void soundSpeed(const MixParams& mp, FaceState<T, NS>& s) {
+    s.cs = Num<T>::sqrt_(Mixture<T, NS, EOS>::sqSonic(mp, s.c, s.rho[0], s.Uv, s.p) + T(0));
+}
+
+// ------------------------------------------------------------------ boundary conditions
+struct BCParams {
+    int conc[6][MAXS];
+    double conc_value[6][MAXS];
+    int vel[6];
+    double vel_value[6][3];
+    int p[6];
+    double p_value[6];
+};
+
+// boundaryConditionValueCell for a scalar (free / slip -> value, fixedValueCell -> fixed value)
+template <typename T> __device__ __forceinline__ T ghostScalar(int type, double fixed, T in) {
+    return type == FV_BC_FIXED_CELL ? T(fixed) : in;
+}
+
+// boundaryConditionValueCell for the velocity; the patch normal is sign * e_axis.
+// slip: (v - (v & n) n) * 2 - v, evaluated in the reference's component order.
+template <typename T>
+__device__ __forceinline__ void ghostVelocity(int type, const double* fixed, int axis, int sign, const T* in, T* out) {
+    if (type == FV_BC_FIXED_CELL) {
+        out[0] = T(fixed[0]); out[1] = T(fixed[1]); out[2] = T(fixed[2]);
+        return;
+    }
+    if (type == FV_BC_SLIP) {
+        // n = sign * e_axis ; v & n = ((0 + v0 n0) + v1 n1) + v2 n2
+        T n[3] = {T(0), T(0), T(0)};
+        n[axis] = T(sign);
+        T vn = 0;
+        vn += in[0] * n[0];
+        vn += in[1] * n[1];
+        vn += in[2] * n[2];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const T s = in[d] - n[d] * vn;
+            out[d] = s * T(2) - in[d];
+        }
+        return;
+    }
+    out[0] = in[0]; out[1] = in[1]; out[2] = in[2];
+}
+
+// Ghost neighbour state of a boundary face from the owner-side state (HancockStage.cpp:324-446).
+template <typename T, int NS, int EOS>
+__device__ __forceinline__ void ghostState(const MixParams& mp, const BCParams& bc, int patch, int axis, int sign,
+                                           const FaceState<T, NS>& own, FaceState<T, NS>& g) {
+    g.c[0] = 0;
+    g.rho[0] = 0;
+#pragma unroll
+    for (int k = 1; k <= NS; ++k) {
+        g.c[k] = ghostScalar<T>(bc.conc[patch][k - 1], bc.conc_value[patch][k - 1], own.c[k]);
+        g.rho[k] = g.c[k] * T(mp.M[k - 1]);
+        g.c[0] += g.c[k];
+        g.rho[0] += g.rho[k];
+    }
+    ghostVelocity<T>(bc.vel[patch], bc.vel_value[patch], axis, sign, own.v, g.v);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) g.m[d] = g.v[d] * g.rho[0];
+    g.p = ghostScalar<T>(bc.p[patch], bc.p_value[patch], own.p);
+    g.Uv = Mixture<T, NS, EOS>::UvFromp(mp, g.c, g.p);
+    T v2 = 0;
+    v2 += g.v[0] * g.v[0];
+    v2 += g.v[1] * g.v[1];
+    v2 += g.v[2] * g.v[2];
+    g.E = g.Uv + g.rho[0] * v2 * T(0.5) + T(0);
+    soundSpeed<T, NS, EOS>(mp, g);
+}
+
+// ------------------------------------------------------------------ fluxes
+// Scalar fluxes through a face with normal N = sign * e_axis, expressed along N: the
+// reference stores F (x) N and every consumer contracts it with +-N, which returns these
+// scalars exactly.  rho[0..NS], m[0..2], E.
+template <typename T, int NS>
+struct FaceFlux {
+    T rho[NS + 1];
+    T m[3];
+    T E;
+};
+
+// HLLC (HLLCSolver.cpp:52-403) or HLL (HLLSolver.cpp:52-300); returns false when no branch
+// applies (NaN wave speeds), which the reference reports as RiemannSolverError.
+template <typename T, int NS>
+__device__ __forceinline__ bool riemann(int flux, int axis, int sign, const FaceState<T, NS>& O,
+                                        const FaceState<T, NS>& B, FaceFlux<T, NS>& F) {
+    const T sg = T(sign);
+    const T uO = O.v[axis] * sg, uN = B.v[axis] * sg;
+    const T SO = smin(uO - O.cs, uN - B.cs);
+    const T SN = smax(uO + O.cs, uN + B.cs);
+    // (I & N)_d * p is sign * p on the normal axis and 0 * p elsewhere
+    if (flux == FV_FLUX_HLLC) {
+        const T Sc = ((B.p + T(0)) - (O.p + T(0)) + O.rho[0] * uO * (SO - uO) - B.rho[0] * uN * (SN - uN)) /
+                     (O.rho[0] * (SO - uO) - B.rho[0] * (SN - uN));
+        const T PON = T(0.5) * ((O.p + T(0)) + (B.p + T(0)) + O.rho[0] * (SO - uO) * (Sc - uO) +
+                                B.rho[0] * (SN - uN) * (Sc - uN));
+        if (SO >= T(0)) {
+#pragma unroll
+            for (int k = 0; k <= NS; ++k) F.rho[k] = (sg * uO) * O.rho[k] * sg;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) F.m[d] = O.m[d] * uO + (d == axis ? sg : T(0)) * (O.p + T(0));
+            F.E = uO * (O.E + O.p + T(0));
+        } else if (Sc >= T(0)) {
+            const T factor = SO - uO;
+            const T den = T(1) / (SO - Sc);
+#pragma unroll
+            for (int k = 0; k <= NS; ++k) {
+                const T rs = O.rho[k] * factor * den;
+                F.rho[k] = O.rho[k] * uO + SO * (rs - O.rho[k]);
+            }
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const T ms = (O.m[d] * factor - (d == axis ? sg : T(0)) * (O.p + T(0) - PON)) * den;
+                F.m[d] = O.m[d] * uO + (d == axis ? sg : T(0)) * (O.p + T(0)) + (ms - O.m[d]) * SO;
+            }
+            const T Es = (O.E * factor - (O.p + T(0)) * uO + PON * Sc) * den;
+            F.E = (O.E + O.p + T(0)) * uO + SO * (Es - O.E);
+        } else if (SN > T(0)) {
+            const T factor = SN - uN;
+            const T den = T(1) / (SN - Sc);
+#pragma unroll
+            for (int k = 0; k <= NS; ++k) {
+                const T rs = B.rho[k] * factor * den;
+                F.rho[k] = B.rho[k] * uN + SN * (rs - B.rho[k]);
+            }
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const T ms = (B.m[d] * factor - (d == axis ? sg : T(0)) * (B.p + T(0) - PON)) * den;
+                F.m[d] = B.m[d] * uN + (d == axis ? sg : T(0)) * (B.p + T(0)) + (ms - B.m[d]) * SN;
+            }
+            const T Es = (B.E * factor - (B.p + T(0)) * uN + PON * Sc) * den;
+            F.E = (B.E + B.p + T(0)) * uN + SN * (Es - B.E);
+        } else if (SN <= T(0)) {
+#pragma unroll
+            for (int k = 0; k <= NS; ++k) F.rho[k] = (sg * uN) * B.rho[k] * sg;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) F.m[d] = B.m[d] * uN + (d == axis ? sg : T(0)) * (B.p + T(0));
+            F.E = uN * (B.E + B.p + T(0));
+        } else {
+            return false;
+        }
+        return true;
+    }
+    // HLL
+    if (SO >= T(0)) {
+#pragma unroll
+        for (int k = 0; k <= NS; ++k) F.rho[k] = sg * (uO * O.rho[k]) * sg;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) F.m[d] = O.m[d] * uO + (d == axis ? sg : T(0)) * (O.p + T(0));
+        F.E = uO * (O.E + O.p + T(0));
+    } else if (SN > T(0)) {
+        const T den = T(1) / (SN - SO);
+#pragma unroll
+        for (int k = 0; k <= NS; ++k)
+            F.rho[k] = (SN * uO * O.rho[k] - SO * uN * B.rho[k] + SN * SO * (B.rho[k] - O.rho[k])) * den;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const T nd = (d == axis ? sg : T(0));
+            const T t1 = (O.m[d] * uO + nd * (O.p + T(0))) * SN;
+            const T t2 = (B.m[d] * uN + nd * (B.p + T(0))) * SO;
+            const T t3 = (B.m[d] - O.m[d]) * (SN * SO);
+            F.m[d] = ((t1 - t2) + t3) * den;
+        }
+        F.E = (SN * (uO * (O.E + O.p + T(0))) - SO * (uN * (B.E + B.p + T(0))) + SN * SO * (B.E - O.E)) * den;
+    } else if (SN <= T(0)) {
+#pragma unroll
+        for (int k = 0; k <= NS; ++k) F.rho[k] = sg * (uN * B.rho[k]) * sg;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) F.m[d] = B.m[d] * uN + (d == axis ? sg : T(0)) * (B.p + T(0));
+        F.E = uN * (B.E + B.p + T(0));
+    } else {
+        return false;
+    }
+    return true;
+}
+
+}  // namespace fv

@@ -1,0 +1,478 @@
+// fv_kernels.cuh -- CUDA kernels of the explicit finite-volume step (sm_100a).
+//
+// Storage: the conserved state is structure-of-arrays FP64, field f of cell i at
+// U[f * stride + i] with cells in the reference's order (x fastest, then y, then z).
+// Fields: rho_1..rho_N, rho (mixture density, evolved with its own flux as
+// Advection.cpp:433-435 does), m_x, m_y, m_z, E.  The reference carries all three momentum
+// components in every dimension (a transverse component is advected passively); a case whose
+// transverse velocities are all zero keeps them zero, and the kernels then touch only the first
+// `nmom` = dims momentum fields.
+//
+// Two step paths:
+//  * k_march  -- fused single-pass step for 2D/3D meshes whose limiter gives zero slopes on a
+//                multi-dimensional structured mesh (limiterZeroForNonPositiveR).  Then every face
+//                of a cell carries the same predicted state W (closure of Advection.cpp:237-303
+//                followed by the Hancock round trip of HancockStage.cpp:174-240, whose
+//                divergence cancels exactly face pair by face pair), so W is computed once per
+//                cell.  A CTA owns a tile of columns (x, or x-y in 3D) plus a one-cell halo ring
+//                and marches along the last axis; in-plane neighbours' W and fluxes are exchanged
+//                through shared memory, the marching-axis flux stays in registers.  The epilogue
+//                recovers the new primitives and reduces the CFL signal speed per CTA.
+//  * generic  -- k_prim / k_faces / k_fluxes / k_update: the full MUSCL-Hancock of the reference
+//                (Gauss gradient, r-ratio TVD limiter, reconstruction, Hancock predictor,
+//                Riemann flux, update) with face states in global scratch.  Used in 1D and for
+//                the limiters whose phi(r <= 0) is not zero.
+// Both end with k_finalize, which reduces the per-CTA maxima to the next time step exactly as
+// the CFL block of Schemi.cpp:807-833 and advances the device-resident clock.
+#pragma once
+
+#include "fv_device.cuh"
+
+namespace fv {
+
+struct Geometry {
+    const double* h[3];     // cell edge along axis a (n_a entries)
+    const double* cc[3];    // cell-centre coordinate along axis a
+    const double* fpos[3];  // own-axis coordinate of face i (n_a + 1 entries)
+    const double* aabb[3];  // transverse face-centre coordinate, corner pattern a,a,b,b
+    const double* abab[3];  // transverse face-centre coordinate, corner pattern a,b,a,b
+};
+
+struct StepParams {
+    int dims;
+    int n[3];
+    int periodic[3];
+    long long ncell;
+    long long stride;       // distance between fields of U
+    int nmom;               // momentum components carried (dims, or 3 when a transverse velocity is non-zero)
+    int limiter;
+    int flux;
+    int gravity;
+    int courant_only;
+    double courant;
+    double min_dt;
+    double ext[3];          // parallelepiped extents (the transverse sizes of 1D / 2D cells)
+    MixParams mix;
+    BCParams bc;
+    Geometry geo;
+};
+
+// Device-resident clock of one case (main's Time / mesh timestep / gravity vector).
+struct DevClock {
+    double time;
+    double dt;          // step to take next
+    double dt_used;     // step taken last
+    double t_end;       // clamp target (+inf for single steps)
+    double dt_free;     // CFL step before the end-time clamp
+    double g[3];
+    double g_delta[3];
+    long long steps;
+    int done;           // time >= t_end: further steps are no-ops
+    int err;            // fv_error_code raised by a kernel
+    int first;          // 1 until the first step: primitives come from the uploaded restart set
+    int pad;
+};
+
+__device__ __forceinline__ void raise(DevClock* ck, int code) { atomicCAS(&ck->err, 0, code); }
+
+// Index helpers
+__device__ __forceinline__ long long cellIndex(const StepParams& P, int i, int j, int k) {
+    return (long long)i + (long long)P.n[0] * ((long long)j + (long long)P.n[1] * k);
+}
+
+// Primitive recovery of a cell from its conserved state (Advection.cpp:455-479), or the
+// uploaded restart primitives before the first step (phaseInitialization keeps them as read).
+template <typename T, int NS, int EOS, int D>
+__device__ __forceinline__ void cellPrimitive(const StepParams& P, const double* __restrict__ U,
+                                              const double* __restrict__ prim, long long i, T* c, T* v, T& p,
+                                              T& rho0, T* rho, T* m, T& E) {
+    const long long s = P.stride;
+#pragma unroll
+    for (int k = 1; k <= NS; ++k) rho[k] = T(U[(k - 1) * s + i]);
+    rho0 = T(U[NS * s + i]);
+    rho[0] = rho0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) m[d] = d < P.nmom ? T(U[(NS + 1 + d) * s + i]) : T(0);
+    E = T(U[(NS + 4) * s + i]);
+    if (prim) {
+        c[0] = 0;
+#pragma unroll
+        for (int k = 1; k <= NS; ++k) {
+            c[k] = T(prim[(k - 1) * s + i]);
+            c[0] += c[k];
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) v[d] = T(prim[(NS + d) * s + i]);
+        p = T(prim[(NS + 3) * s + i]);
+        return;
+    }
+    c[0] = 0;
+#pragma unroll
+    for (int k = 1; k <= NS; ++k) {
+        c[k] = rho[k] / T(P.mix.M[k - 1]);
+        c[0] += c[k];
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) v[d] = m[d] / rho0;
+    T v2 = 0;
+    v2 += v[0] * v[0];
+    v2 += v[1] * v[1];
+    v2 += v[2] * v[2];
+    const T Uv = E - rho0 * v2 * T(0.5) - T(0);
+    p = Mixture<T, NS, EOS>::pFromUv(P.mix, c, Uv);
+}
+
+// Predicted face state of a cell whose slopes vanish: closure, zero Hancock divergence,
+// recalculation from conserved values, sound speed.
+template <typename T, int NS, int EOS>
+__device__ __forceinline__ void cellFaceState(const MixParams& mp, const T* c, const T* v, T p, FaceState<T, NS>& W) {
+#pragma unroll
+    for (int k = 1; k <= NS; ++k) W.c[k] = c[k];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) W.v[d] = v[d];
+    W.p = p;
+    closeFromPrimitive<T, NS, EOS>(mp, W);
+    closeFromConserved<T, NS, EOS>(mp, W);
+    soundSpeed<T, NS, EOS>(mp, W);
+}
+
+// Compact part of W shared with in-plane neighbours for a face normal to `axis`.
+template <typename T, int NS>
+struct SharedW {
+    T rho[NS + 1];
+    T m[3];
+    T E, p, cs;
+    T vn[2];  // velocity along the two in-plane axes
+};
+
+template <typename T, int NS>
+__device__ __forceinline__ void toShared(const FaceState<T, NS>& W, SharedW<T, NS>& s) {
+#pragma unroll
+    for (int k = 0; k <= NS; ++k) s.rho[k] = W.rho[k];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) s.m[d] = W.m[d];
+    s.E = W.E;
+    s.p = W.p;
+    s.cs = W.cs;
+    s.vn[0] = W.v[0];
+    s.vn[1] = W.v[1];
+}
+
+template <typename T, int NS>
+__device__ __forceinline__ void fromShared(const SharedW<T, NS>& s, FaceState<T, NS>& W) {
+#pragma unroll
+    for (int k = 0; k <= NS; ++k) W.rho[k] = s.rho[k];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) W.m[d] = s.m[d];
+    W.E = s.E;
+    W.p = s.p;
+    W.cs = s.cs;
+    W.v[0] = s.vn[0];
+    W.v[1] = s.vn[1];
+    W.v[2] = T(0);
+}
+
+template <typename T> __device__ __forceinline__ T blockMaxReduce(T v, T* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = smax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int lane = (threadIdx.x + threadIdx.y * blockDim.x) & 31;
+    const int warp = (threadIdx.x + threadIdx.y * blockDim.x) >> 5;
+    const int nw = (blockDim.x * blockDim.y + 31) >> 5;
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        v = lane < nw ? red[lane] : T(-1);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = smax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    }
+    return v;
+}
+
+// CFL signal of a cell: (|v| + c) / min edge (Schemi.cpp:807-828), from conserved values.
+template <typename T, int NS, int EOS, int D>
+__device__ __forceinline__ T cellSignal(const StepParams& P, const T* rho, T rho0, const T* m, T E, T minLS) {
+    T c[NS + 1];
+    c[0] = 0;
+#pragma unroll
+    for (int k = 1; k <= NS; ++k) {
+        c[k] = rho[k] / T(P.mix.M[k - 1]);
+        c[0] += c[k];
+    }
+    T v[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) v[d] = m[d] / rho0;
+    T v2 = 0;
+    v2 += v[0] * v[0];
+    v2 += v[1] * v[1];
+    v2 += v[2] * v[2];
+    const T Uv = E - rho0 * v2 * T(0.5) - T(0);
+    const T p = Mixture<T, NS, EOS>::pFromUv(P.mix, c, Uv);
+    const T sonic = Num<T>::sqrt_(Mixture<T, NS, EOS>::sqSonic(P.mix, c, rho0, Uv, p));
+    T s = mag3<T>(v[0], v[1], v[2]) + sonic;
+    s *= minLS;
+    return s;
+}
+
+// ============================================================================ fused march
+// Block: BX x BY threads (BY = 1 in 2D).  Thread (tx, ty) owns in-plane column
+// (x0 - 1 + tx, y0 - 1 + ty); the outer ring of the block is halo.  D = 2 marches along y,
+// D = 3 along z.  Rows per block along the marching axis: `rows`.
+template <typename T, int NS, int EOS, int D, int BX, int BY>
+__global__ void __launch_bounds__(BX* BY) k_march(const StepParams P, const double* __restrict__ U,
+                                                  double* __restrict__ Un, const double* __restrict__ prim0,
+                                                  DevClock* __restrict__ ck, double* __restrict__ blockMax, int rows) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    auto sW = reinterpret_cast<SharedW<T, NS>(*)[BX]>(smem_raw);
+    auto sFx = reinterpret_cast<FaceFlux<T, NS>(*)[BX]>(smem_raw + sizeof(SharedW<T, NS>) * BX * BY);
+    auto sFy = reinterpret_cast<FaceFlux<T, NS>(*)[BX]>(smem_raw + (sizeof(SharedW<T, NS>) + sizeof(FaceFlux<T, NS>)) * BX * BY);
+    __shared__ T red[32];
+
+    if (ck->done) return;
+    const double dt = ck->dt;
+    const double* __restrict__ prim = ck->first ? prim0 : nullptr;
+    const double gx_ = ck->g[0], gy_ = ck->g[1], gz_ = ck->g[2];
+
+    constexpr int MA = D - 1;  // marching axis
+    const int nx = P.n[0], ny = P.n[1];
+    const int nm = P.n[MA];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int X = blockIdx.x * (BX - 2) - 1 + tx;
+    const int Y = (D == 3) ? (int)(blockIdx.y * (BY - 2)) - 1 + ty : 0;
+    const int z0 = (D == 3 ? blockIdx.z : blockIdx.y) * rows;
+    const int z1 = min(z0 + rows, nm);
+    const bool perX = P.periodic[0], perY = (D == 3) && P.periodic[1], perM = P.periodic[MA];
+
+    // in-plane cell of this thread (wrapped for periodic axes)
+    int cx = X, cy = Y;
+    bool has = true;
+    if (X < 0 || X >= nx) {
+        if (perX && X >= -1 && X <= nx) cx = X < 0 ? X + nx : X - nx;
+        else has = false;
+    }
+    if (D == 3 && (Y < 0 || Y >= ny)) {
+        if (perY && Y >= -1 && Y <= ny) cy = Y < 0 ? Y + ny : Y - ny;
+        else has = false;
+    }
+    const bool interior = tx >= 1 && tx <= BX - 2 && X < nx && (D == 2 || (ty >= 1 && ty <= BY - 2 && Y < ny));
+
+    // geometry of the column
+    const double hxv = has ? P.geo.h[0][cx] : 1.0;
+    const double hyv = D == 3 ? (has ? P.geo.h[1][cy] : 1.0) : 0.0;
+    const double Lz = P.ext[2];
+
+    auto cellAt = [&](int zm) -> long long {
+        return D == 2 ? cellIndex(P, cx, zm, 0) : cellIndex(P, cx, cy, zm);
+    };
+    auto wrapM = [&](int zm, bool& ok) -> int {
+        ok = true;
+        if (zm < 0) { if (perM) return zm + nm; ok = false; return 0; }
+        if (zm >= nm) { if (perM) return zm - nm; ok = false; return 0; }
+        return zm;
+    };
+
+    FaceState<T, NS> Wc, Wn;
+    T cOld[NS + 1], vOld[3], pOld, rho0Old;
+    T rhoU[NS + 1], mU[3], EU;
+    (void)pOld; (void)EU; (void)cOld;
+    FaceFlux<T, NS> Gprev;
+    T GprevSign = T(-1);
+    T localMax = T(-1);
+    bool ok;
+
+    // ---- prologue: W(z0) and the flux of the face below z0
+    if (has && z0 < z1) {
+        T c[NS + 1], v[3], p, r0, rr[NS + 1], mm[3], EE;
+        cellPrimitive<T, NS, EOS, D>(P, U, prim, cellAt(z0), c, v, p, r0, rr, mm, EE);
+        cellFaceState<T, NS, EOS>(P.mix, c, v, p, Wc);
+        const int zb = wrapM(z0 - 1, ok);
+        if (ok) {
+            T c2[NS + 1], v2[3], p2, r02, rr2[NS + 1], mm2[3], EE2;
+            cellPrimitive<T, NS, EOS, D>(P, U, prim, cellAt(zb), c2, v2, p2, r02, rr2, mm2, EE2);
+            FaceState<T, NS> Wb;
+            cellFaceState<T, NS, EOS>(P.mix, c2, v2, p2, Wb);
+            if (!riemann<T, NS>(P.flux, MA, 1, Wb, Wc, Gprev)) raise(ck, FV_ERR_RIEMANN);
+            GprevSign = T(-1);
+        } else {
+            // boundary patch below: right (y-min) in 2D, bottom (z-min) in 3D; outward normal -e
+            const int patch = D == 2 ? FV_PATCH_RIGHT : FV_PATCH_BOTTOM;
+            FaceState<T, NS> Gs;
+            ghostState<T, NS, EOS>(P.mix, P.bc, patch, MA, -1, Wc, Gs);
+            if (!riemann<T, NS>(P.flux, MA, -1, Wc, Gs, Gprev)) raise(ck, FV_ERR_RIEMANN);
+            GprevSign = T(1);
+        }
+    }
+
+    for (int z = z0; z < z1; ++z) {
+        // own conserved state and primitives of row z (needed for the update and gravity)
+        if (has) {
+            T r0;
+            cellPrimitive<T, NS, EOS, D>(P, U, prim, cellAt(z), cOld, vOld, pOld, r0, rhoU, mU, EU);
+            rho0Old = r0;
+        }
+        // W of the next row
+        const int zn = wrapM(z + 1, ok);
+        const bool hasNext = has && ok;
+        if (hasNext) {
+            T c[NS + 1], v[3], p, r0, rr[NS + 1], mm[3], EE;
+            cellPrimitive<T, NS, EOS, D>(P, U, prim, cellAt(zn), c, v, p, r0, rr, mm, EE);
+            cellFaceState<T, NS, EOS>(P.mix, c, v, p, Wn);
+        }
+        if (has) toShared<T, NS>(Wc, sW[ty][tx]);
+        __syncthreads();
+        // in-plane fluxes through the low faces of this column
+        if (has && tx >= 1) {
+            FaceState<T, NS> Wl;
+            if (X == 0 && !perX) {
+                FaceState<T, NS> Gs;
+                ghostState<T, NS, EOS>(P.mix, P.bc, FV_PATCH_TAIL, 0, -1, Wc, Gs);
+                if (!riemann<T, NS>(P.flux, 0, -1, Wc, Gs, sFx[ty][tx])) raise(ck, FV_ERR_RIEMANN);
+            } else {
+                fromShared<T, NS>(sW[ty][tx - 1], Wl);
+                if (!riemann<T, NS>(P.flux, 0, 1, Wl, Wc, sFx[ty][tx])) raise(ck, FV_ERR_RIEMANN);
+            }
+        }
+        if (D == 3 && has && ty >= 1) {
+            FaceState<T, NS> Wl;
+            if (Y == 0 && !perY) {
+                FaceState<T, NS> Gs;
+                ghostState<T, NS, EOS>(P.mix, P.bc, FV_PATCH_RIGHT, 1, -1, Wc, Gs);
+                if (!riemann<T, NS>(P.flux, 1, -1, Wc, Gs, sFy[ty][tx])) raise(ck, FV_ERR_RIEMANN);
+            } else {
+                fromShared<T, NS>(sW[ty - 1][tx], Wl);
+                if (!riemann<T, NS>(P.flux, 1, 1, Wl, Wc, sFy[ty][tx])) raise(ck, FV_ERR_RIEMANN);
+            }
+        }
+        // marching-axis flux through the high face of this cell
+        FaceFlux<T, NS> Gnext;
+        if (has) {
+            if (hasNext) {
+                if (!riemann<T, NS>(P.flux, MA, 1, Wc, Wn, Gnext)) raise(ck, FV_ERR_RIEMANN);
+            } else {
+                const int patch = D == 2 ? FV_PATCH_LEFT : FV_PATCH_TOP;
+                FaceState<T, NS> Gs;
+                ghostState<T, NS, EOS>(P.mix, P.bc, patch, MA, 1, Wc, Gs);
+                if (!riemann<T, NS>(P.flux, MA, 1, Wc, Gs, Gnext)) raise(ck, FV_ERR_RIEMANN);
+            }
+        }
+        __syncthreads();
+        if (interior) {
+            // x-high face: inner (flux of the right neighbour's low face) or the point patch
+            FaceFlux<T, NS> Fxp;
+            if (X == nx - 1 && !perX) {
+                FaceState<T, NS> Gs;
+                ghostState<T, NS, EOS>(P.mix, P.bc, FV_PATCH_POINT, 0, 1, Wc, Gs);
+                if (!riemann<T, NS>(P.flux, 0, 1, Wc, Gs, Fxp)) raise(ck, FV_ERR_RIEMANN);
+            } else {
+                Fxp = sFx[ty][tx + 1];
+            }
+            const T sxm = (X == 0 && !perX) ? T(1) : T(-1);
+            FaceFlux<T, NS> Fyp;
+            T sym = T(-1);
+            if (D == 3) {
+                if (Y == ny - 1 && !perY) {
+                    FaceState<T, NS> Gs;
+                    ghostState<T, NS, EOS>(P.mix, P.bc, FV_PATCH_LEFT, 1, 1, Wc, Gs);
+                    if (!riemann<T, NS>(P.flux, 1, 1, Wc, Gs, Fyp)) raise(ck, FV_ERR_RIEMANN);
+                } else {
+                    Fyp = sFy[ty + 1][tx];
+                }
+                sym = (Y == 0 && !perY) ? T(1) : T(-1);
+            }
+            const FaceFlux<T, NS>& Fxm = sFx[ty][tx];
+            // face areas and volume (mesh.cpp: S = |rX0 - r00| * |r0Y - r00|, V = e1 * e2 * e3)
+            const T hx = T(hxv);
+            const T hm = T(P.geo.h[MA][z]);
+            T Sx, Sy, Sm, V, minLS;
+            if (D == 2) {
+                Sx = T(Lz) * hm;          // x faces: Lz * h_y
+                Sm = hx * T(Lz);          // y faces: h_x * Lz
+                Sy = T(0);
+                V = hx * hm * T(Lz);
+                minLS = T(1) / smin(smin(hx, hm), T(Lz));
+            } else {
+                const T hy = T(hyv);
+                Sx = hm * hy;             // x faces: h_z * h_y
+                Sy = hx * hm;             // y faces: h_x * h_z
+                Sm = hx * hy;             // z faces: h_x * h_y
+                V = hx * hy * hm;
+                minLS = T(1) / smin(smin(hx, hy), hm);
+            }
+            // divergence in the face order of mesh.cpp: 2D [x-, x+, y+, y-], 3D [x-, x+, y+, y-, z-, z+]
+            auto div = [&](auto get) -> T {
+                T s = get(Fxm) * sxm * Sx;
+                s += get(Fxp) * Sx;
+                if (D == 2) {
+                    s += get(Gnext) * Sm;
+                    s += get(Gprev) * GprevSign * Sm;
+                } else {
+                    s += get(Fyp) * Sy;
+                    s += get(sFy[ty][tx]) * sym * Sy;
+                    s += get(Gprev) * GprevSign * Sm;
+                    s += get(Gnext) * Sm;
+                }
+                return s / V;
+            };
+            const long long ic = cellAt(z);
+            const long long st = P.stride;
+            T rhoN[NS + 1], mN[3];
+            // FP64 accumulation of the conserved update: U_new = U - div * dt
+            double Enew = U[(NS + 4) * st + ic] -
+                          double(div([](const FaceFlux<T, NS>& f) { return f.E; })) * dt;
+            double mNew[3] = {0, 0, 0};
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+                if (d < P.nmom)
+                    mNew[d] = U[(NS + 1 + d) * st + ic] - double(div([d](const FaceFlux<T, NS>& f) { return f.m[d]; })) * dt;
+            if (P.gravity) {
+                // Advection.cpp:424-431 with the old density and velocity
+                T vg = 0;
+                vg += vOld[0] * T(gx_);
+                vg += vOld[1] * T(gy_);
+                vg += vOld[2] * T(gz_);
+                const T gvec[3] = {T(gx_), T(gy_), T(gz_)};
+                Enew += double(rho0Old * vg) * dt;
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+                    if (d < P.nmom) mNew[d] += double(gvec[d] * rho0Old) * dt;
+            }
+            double rNew[NS + 1];
+#pragma unroll
+            for (int k = 0; k <= NS; ++k)
+                rNew[k] = U[(k == 0 ? NS : k - 1) * st + ic] -
+                          double(div([k](const FaceFlux<T, NS>& f) { return f.rho[k]; })) * dt;
+            // store
+#pragma unroll
+            for (int k = 1; k <= NS; ++k) Un[(k - 1) * st + ic] = rNew[k];
+            Un[NS * st + ic] = rNew[0];
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+                if (d < P.nmom) Un[(NS + 1 + d) * st + ic] = mNew[d];
+            Un[(NS + 4) * st + ic] = Enew;
+            // CFL signal of the updated cell
+#pragma unroll
+            for (int k = 0; k <= NS; ++k) rhoN[k] = T(rNew[k]);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) mN[d] = T(mNew[d]);
+            const T s = cellSignal<T, NS, EOS, D>(P, rhoN, rhoN[0], mN, T(Enew), minLS);
+            localMax = smax(localMax, s);
+        }
+        // roll the marching window
+        if (has) {
+            Gprev = Gnext;
+            GprevSign = T(-1);
+            if (hasNext) Wc = Wn;
+        }
+    }
+    const T bm = blockMaxReduce<T>(localMax, red);
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        const long long b = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+        blockMax[b] = double(bm);
+    }
+}
+
+// ============================================================================ finalize
+// dt = Courant / max signal; dt = min(dt, dtSource) unless Courant-only; dt = max(dt, minTime);
+// time += dt_used; g += g_delta * dt_used; clamp to t_end (Schemi.cpp:802-835, 933-935).
+__global__ void k_finalize(const StepParams P, DevClock* ck, const double* __restrict__ blockMax, int nblocks);
+
+}  // namespace fv

@@ -1,0 +1,46 @@
+// fv_launch.cuh -- host-side launchers of the step kernels, instantiated once per arithmetic
+// (fv_f64.cu: FP64 without FMA contraction, fv_f32.cu: FP32 flux arithmetic).
+#pragma once
+
+#include "fv_generic.cuh"
+
+namespace fv {
+
+// Tile shape of the fused march (chosen by the autotuner in fv_tune.cpp).
+struct MarchShape {
+    int bx;      // threads along x (incl. the 2 halo columns)
+    int by;      // threads along y in 3D (incl. halo), 1 in 2D
+    int rows;    // cells per CTA along the marching axis
+};
+
+struct StepBuffers {
+    const double* U;
+    double* Un;
+    const double* prim0;
+    DevClock* ck;
+    double* blockMax;
+    long long blockMaxCap;
+    void* Pc;            // generic path: primitives (T)
+    void* FS;            // generic path: face states (T)
+    void* FL;            // generic path: face fluxes (T)
+    GenericLayout L;
+};
+
+enum StepPath { PATH_MARCH = 0, PATH_GENERIC = 1 };
+
+// Number of CTAs (= blockMax entries) one step writes.
+long long marchBlocks(const StepParams& P, const MarchShape& s);
+long long genericBlocks(const StepParams& P);
+
+// Enqueue one step (without the finalize kernel).  Returns cudaSuccess or the launch error.
+cudaError_t launchStepF64(const StepParams& P, const StepBuffers& B, int path, const MarchShape& s, cudaStream_t st);
+cudaError_t launchStepF32(const StepParams& P, const StepBuffers& B, int path, const MarchShape& s, cudaStream_t st);
+
+// Shared memory of the fused march for a shape (bytes), per precision.
+size_t marchSmemF64(int ns, int dims, const MarchShape& s);
+size_t marchSmemF32(int ns, int dims, const MarchShape& s);
+
+// Supported fused-march shapes.
+bool marchShapeSupported(int dims, const MarchShape& s);
+
+}  // namespace fv

@@ -1,0 +1,161 @@
+"""Parity of the CUDA path (through the C-ABI) against the reference's outputs and the oracle.
+
+FP64 mode is compiled without FMA contraction and follows the reference's operation order, so
+it is expected to reproduce the reference bit for bit; the bar written in the tests is the
+north-star tolerance, 1e-12 relative (L-inf over the field, relative to its max magnitude).
+"""
+
+import numpy as np
+import pytest
+
+from golden_cases import golden_steps, load_cases, rel_err
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+COMPARE = ["c1", "c2", "c3", "vx", "vy", "p", "rho", "E", "mx", "my"]
+CASES = load_cases()
+
+
+@pytest.fixture(scope="module")
+def fv():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from schemi_b200 import fv as fvmod
+
+    fvmod.load()
+    return fvmod
+
+
+def _advance(g, n, t_end):
+    for _ in range(n):
+        g.step()
+        t, dt = g.time()
+        if t + dt > t_end:
+            g.set_time(t, t_end - t)
+
+
+@pytest.mark.parametrize("name,case,prim,data", CASES, ids=[c[0] for c in CASES])
+def test_gpu_fp64_matches_reference(fv, name, case, prim, data):
+    g = fv.FVCase(case)
+    g.upload(prim)
+    t_end = float(data["t_end"])
+    done = 0
+    worst = 0.0
+    for target in golden_steps(data):
+        _advance(g, target - done, t_end)
+        done = target
+        t, _ = g.time()
+        assert abs(t - float(data[f"time_{target}"])) <= 1e-14 * max(1.0, abs(t))
+        out = g.download()
+        for f in COMPARE:
+            key = f"{f}_{target}"
+            if key in data and f in out:
+                linf, l1 = rel_err(out[f], data[key])
+                worst = max(worst, linf)
+                assert linf <= FP64_TOL, f"{name} step {target} {f}: rel Linf {linf:.3e} L1 {l1:.3e}"
+    print(f"{name}: max rel Linf vs reference = {worst:.3e}")
+
+
+def test_gpu_run_config1_full(fv):
+    """Config 1 through fv_run (device time loop in CUDA graphs): 955 steps to t = 0.2."""
+    name, case, prim, data = [c for c in CASES if c[0] == "shock_tube_1d_full"][0]
+    g = fv.FVCase(case)
+    g.upload(prim)
+    st = g.run(case.t_end)
+    n = int(data["n_steps"])
+    assert st.steps == n
+    assert st.time == pytest.approx(0.2, abs=1e-15)
+    out = g.download()
+    for f in COMPARE:
+        key = f"{f}_{n}"
+        if key in data:
+            linf, _ = rel_err(out[f], data[key])
+            assert linf <= FP64_TOL, f"{f}: {linf:.3e}"
+
+
+def _oracle_compare(fv, oracle_mod, case, prim, steps, tol, fields=COMPARE, l1=False):
+    g = fv.FVCase(case)
+    g.upload(prim)
+    oc = oracle_mod.OracleCase(case)
+    oc.upload(prim)
+    worst = 0.0
+    for _ in range(steps):
+        g.step()
+        oc.step()
+    a, b = g.download(), oc.download()
+    for f in fields:
+        if f in a and f in b:
+            linf, rl1 = rel_err(a[f], b[f])
+            e = rl1 if l1 else linf
+            worst = max(worst, e)
+            assert e <= tol, f"{case.name} {f}: rel {'L1' if l1 else 'Linf'} {e:.3e}"
+    return g, worst
+
+
+def test_gpu_periodic_kh_march_matches_oracle(fv, oracle_mod):
+    from schemi_b200 import cases
+
+    case, prim = cases.kelvin_helmholtz_2d(n=64)
+    g, worst = _oracle_compare(fv, oracle_mod, case, prim, 20, FP64_TOL)
+    assert g.path == fv.PATH_MARCH
+
+
+def test_gpu_march_equals_generic(fv):
+    """The fused march (zero slopes proven by the limiter) equals the full MUSCL-Hancock."""
+    from schemi_b200 import cases
+
+    case, prim = cases.kelvin_helmholtz_2d(n=48)
+    a = fv.FVCase(case)
+    b = fv.FVCase(case)
+    b.force_generic()
+    a.upload(prim)
+    b.upload(prim)
+    for _ in range(10):
+        a.step()
+        b.step()
+    oa, ob = a.download(), b.download()
+    for f in COMPARE:
+        if f in oa:
+            assert np.array_equal(oa[f], ob[f]), f
+
+
+def test_gpu_3d_vdw_periodic_matches_oracle(fv, oracle_mod):
+    from schemi_b200 import cases
+
+    case, prim = cases.reacting_shear_3d(n=16, precision="f64")
+    case.chemistry = "no"
+    _oracle_compare(fv, oracle_mod, case, prim, 5, FP64_TOL)
+
+
+def test_gpu_3d_generic_linear_matches_oracle(fv, oracle_mod):
+    from schemi_b200 import cases
+
+    case, prim = cases.reacting_shear_3d(n=10, precision="f64")
+    case.chemistry = "no"
+    case.limiter = "linear"
+    g, _ = _oracle_compare(fv, oracle_mod, case, prim, 3, FP64_TOL)
+    assert g.path == fv.PATH_GENERIC
+
+
+def test_gpu_fp32_flux_within_tolerance(fv, oracle_mod):
+    """FP32 flux arithmetic with FP64 accumulation: relative L1 error <= 1e-5 after 20 steps."""
+    from schemi_b200 import cases
+
+    case, prim = cases.kelvin_helmholtz_2d(n=64, precision="f32flux")
+    _oracle_compare(fv, oracle_mod, case, prim, 20, 1e-5, l1=True)
+
+
+def test_gpu_riemann_failure_status(fv):
+    from schemi_b200 import cases
+
+    c, p = cases.shock_tube_1d(n=200)
+    c.limiter = "UTCDFS"
+    g = fv.FVCase(c)
+    g.upload(p)
+    g.step()
+    with pytest.raises(fv.FVError) as ei:
+        g.step()
+    assert ei.value.status == 1
