@@ -185,6 +185,20 @@ fv_status fv_state_device(fv_handle* h, double** fields, int* n_fields, long lon
 /* Synchronises the handle's stream. */
 fv_status fv_sync(fv_handle* h);
 
+/* Asynchronous stepping for callers that keep the host off the step's critical path:
+ * fv_begin_steps puts the clock in single-step mode (no end-time clamp); fv_step_async enqueues
+ * one step + CFL on the handle's stream without synchronising or reading anything back;
+ * fv_check synchronises and reports a device-side error raised by any enqueued step. */
+fv_status fv_begin_steps(fv_handle* h);
+fv_status fv_step_async(fv_handle* h);
+fv_status fv_check(fv_handle* h);
+
+/* The handle's CUDA stream (cudaStream_t), for event timing and interop. */
+void* fv_stream(fv_handle* h);
+
+/* Kernel launches one step issues (fused march: 2, generic path: 5). */
+long long fv_kernels_per_step(const fv_handle* h);
+
 /* ---- Batched ensemble: many independent cases advanced by one persistent kernel ---- */
 typedef struct fv_batch fv_batch;
 

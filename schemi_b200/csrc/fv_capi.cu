@@ -797,6 +797,38 @@ fv_status fv_sync(fv_handle* h) {
     return FV_OK;
 }
 
+fv_status fv_begin_steps(fv_handle* h) {
+    if (!h) return FV_ERR_INIT;
+    fv_status st = readClock(h);
+    if (st != FV_OK) return st;
+    h->ckHost->t_end = std::numeric_limits<double>::infinity();
+    h->ckHost->done = 0;
+    FV_CUDA(h, cudaMemcpyAsync(h->ck, h->ckHost, sizeof(DevClock), cudaMemcpyHostToDevice, h->stream));
+    FV_CUDA(h, cudaStreamSynchronize(h->stream));
+    return FV_OK;
+}
+
+fv_status fv_step_async(fv_handle* h) {
+    if (!h) return FV_ERR_INIT;
+    FV_CUDA(h, enqueueStep(h, h->cur));
+    h->cur ^= 1;
+    return FV_OK;
+}
+
+void* fv_stream(fv_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+fv_status fv_check(fv_handle* h) {
+    if (!h) return FV_ERR_INIT;
+    fv_status st = readClock(h);
+    if (st != FV_OK) return st;
+    return clockError(h);
+}
+
+long long fv_kernels_per_step(const fv_handle* h) {
+    if (!h) return 0;
+    return h->path == PATH_MARCH ? 2 : 5;
+}
+
 // ---- introspection used by the tests and the bench (no reference counterpart)
 int fv_step_path(const fv_handle* h) { return h ? h->path : -1; }
 

@@ -75,6 +75,13 @@ def load():
     lib.fv_set_march_shape.argtypes = [P, I, I, I]
     lib.fv_force_generic.argtypes = [P]
     lib.fv_time_step_kernel.argtypes = [P, I, ctypes.POINTER(ctypes.c_float)]
+    lib.fv_begin_steps.argtypes = [P]
+    lib.fv_step_async.argtypes = [P]
+    lib.fv_check.argtypes = [P]
+    lib.fv_stream.restype = P
+    lib.fv_stream.argtypes = [P]
+    lib.fv_kernels_per_step.restype = LL
+    lib.fv_kernels_per_step.argtypes = [P]
     if hasattr(lib, "fv_batch_create"):
         lib.fv_batch_create.argtypes = [ctypes.POINTER(P), I, ctypes.POINTER(P)]
         lib.fv_batch_run.argtypes = [P, DP, LL, ctypes.POINTER(fv_batch_stats_t)]
@@ -176,7 +183,7 @@ class FVCase:
     def state_device(self):
         nf = self.case.n_conserved
         DP = ctypes.POINTER(ctypes.c_double)
-        arr = (DP * 8)()
+        arr = (DP * 16)()
         n_f, n_c = ctypes.c_int(), ctypes.c_longlong()
         self._check(self.lib.fv_state_device(self._h, arr, ctypes.byref(n_f), ctypes.byref(n_c)))
         return [ctypes.cast(arr[i], ctypes.c_void_p).value for i in range(n_f.value)], n_c.value
@@ -189,6 +196,23 @@ class FVCase:
 
     def force_generic(self) -> None:
         self._check(self.lib.fv_force_generic(self._h))
+
+    def begin_steps(self) -> None:
+        self._check(self.lib.fv_begin_steps(self._h))
+
+    def step_async(self) -> None:
+        self._check(self.lib.fv_step_async(self._h))
+
+    def check(self) -> None:
+        self._check(self.lib.fv_check(self._h))
+
+    @property
+    def stream_ptr(self) -> int:
+        return self.lib.fv_stream(self._h)
+
+    @property
+    def kernels_per_step(self) -> int:
+        return self.lib.fv_kernels_per_step(self._h)
 
     def time_step_kernel(self, iters: int) -> float:
         ms = ctypes.c_float()
