@@ -199,6 +199,28 @@ void* fv_stream(fv_handle* h);
 /* Kernel launches one step issues (fused march: 2, generic path: 5). */
 long long fv_kernels_per_step(const fv_handle* h);
 
+/* ---- One step that allocates no device memory (no counterpart in the reference) ----
+ * For hosts that cannot call cudaMalloc on the step's path: an application whose device memory
+ * belongs to a pooling allocator that forbids driver allocations, or a time loop that cannot
+ * afford the device-wide synchronisation cudaMalloc / cudaFree may cause.  The caller owns the
+ * state buffers; all intermediates live in one file-scope device array of
+ * FV_NOALLOC_SCRATCH_BYTES (2.5 MiB) that every GPU which loads the library keeps until exit.
+ *   state_in / state_out  device arrays, (n_species + 5) fields x n_cells, the layout of
+ *                          fv_state_device (rho_1..rho_N, rho, m_x, m_y, m_z, E; x fastest)
+ *   dt                     step to take; dt_next receives main's CFL step of the new state
+ *                          (unclamped); cfg->g is the gravity vector of this step
+ *   stream                 cudaStream_t or NULL
+ * Runs the full MUSCL-Hancock path (any limiter, 1D/2D/3D) on meshes of at most
+ * FV_NOALLOC_MAX_CELLS cells; larger meshes are rejected with FV_ERR_INIT.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) and should come before any
+ * stream capture.  Every call rewrites each part of the array it reads, so no state carries over
+ * between calls; calls that overlap on the GPU share the array and race.  Synchronises `stream`
+ * before returning. */
+#define FV_NOALLOC_MAX_CELLS 1024
+#define FV_NOALLOC_SCRATCH_BYTES 2621440
+fv_status fv_step_noalloc(const fv_config* cfg, const double* state_in, double* state_out, double dt,
+                          double* dt_next, void* stream);
+
 /* ---- Batched ensemble: many independent cases advanced by one persistent kernel ---- */
 typedef struct fv_batch fv_batch;
 

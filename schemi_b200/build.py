@@ -57,6 +57,8 @@ def build(verbose: bool = False, force: bool = False, extra_flags=None) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
     deps = _sources() + [os.path.join(HERE, "..", "include", "fvstep.h")]
     units = dict(UNITS)
+    if os.path.exists(os.path.join(CSRC, "fv_noalloc.cu")):
+        units["fv_noalloc.cu"] = ["--fmad=false"]
     if os.path.exists(os.path.join(CSRC, "fv_batch.cu")):
         units["fv_batch.cu"] = ["--fmad=false"]
     objs = []
