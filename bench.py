@@ -283,6 +283,13 @@ def run_ours(args):
         case, prim = cases.kelvin_helmholtz_2d(n=n, precision=prec)
         g = fv.FVCase(case)
         g.upload(prim)
+        if not args.no_autotune:
+            from schemi_b200 import autotune
+
+            shape = autotune.tune(g)   # cached per (mesh, species, EOS, precision, device)
+            g.upload(prim)             # tuning advanced the state: start again from the restart set
+        else:
+            shape = None
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
@@ -302,6 +309,7 @@ def run_ours(args):
         results[prec] = {
             "value": value, "ms_per_step": total_ms / args.steps, "clocks": clocks, "achieved_gbs": achieved,
             "bytes_per_cell_update": nbytes, "kernels_per_step": g.kernels_per_step, "path": g.path,
+            "march_shape": list(shape) if shape else None,
         }
         # e2e through the C-ABI with pinned host buffers
         pinned = []
@@ -336,7 +344,8 @@ def run_ours(args):
         "config": {"workload": f"kelvin_helmholtz_2d {n}x{n}", "cells_per_gpu": n * n, "species": 2,
                    "flux": "HLLC", "limiter": "vanLeer", "bc": "periodic x, slip y",
                    "l2": "flushed before every timed step (256 MiB write on the step stream)",
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": f"replicas x{world}", "march_shape_f64": head["march_shape"],
+                   "march_shape_f32flux": results["f32flux"]["march_shape"]},
         "gpu_launches": head["kernels_per_step"] * args.steps,
         "e2e": head["e2e"],
         "clocks": head["clocks"],
@@ -381,6 +390,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=1024, help="cells per axis of the KH workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

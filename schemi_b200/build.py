@@ -29,7 +29,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
           "-I", os.path.join(HERE, "..", "include")]
 UNITS = {
     "fv_f64.cu": ["--fmad=false"],
-    "fv_f32.cu": [],
+    "fv_f32.cu": ["-use_fast_math"],
     "fv_capi.cu": ["--fmad=false"],
 }
 

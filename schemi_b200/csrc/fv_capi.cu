@@ -473,6 +473,7 @@ fv_status fv_create(const fv_config* cfg, fv_handle** out) {
     mp.R = cfg->R;
     for (int k = 0; k < cfg->n_species; ++k) {
         mp.M[k] = cfg->M[k];
+        mp.invM[k] = 1.0 / cfg->M[k];
         mp.Cv[k] = cfg->Cv[k];
     }
     if (cfg->eos == FV_EOS_VAN_DER_WAALS) {

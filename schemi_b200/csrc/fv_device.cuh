@@ -54,12 +54,22 @@ template <typename T> __device__ __forceinline__ T mag3(T x, T y, T z) {
     return a * Num<T>::sqrt_(xa * xa + ya * ya + za * za);
 }
 
+// mag3(x, y, 0): the same value without the third quotient (0 / a = 0 exactly).
+template <typename T> __device__ __forceinline__ T mag2z(T x, T y) {
+    x = Num<T>::abs_(x); y = Num<T>::abs_(y);
+    const T a = x < y ? y : x;
+    if (a == T(0)) return T(0);
+    const T xa = x / a, ya = y / a;
+    return a * Num<T>::sqrt_(xa * xa + ya * ya + T(0));
+}
+
 // ------------------------------------------------------------------ mixture parameters
 struct MixParams {
     int ns;        // number of species
     int eos_kind;  // fv_eos
     double R;
     double M[MAXS];
+    double invM[MAXS];  // 1 / M (FP32-flux arithmetic only)
     double Cv[MAXS];
     double a[MAXS][MAXS];
     double b[MAXS][MAXS];
@@ -232,8 +242,10 @@ __device__ __forceinline__ void closeFromPrimitive(const MixParams& mp, FaceStat
 }
 
 // Recalculation from conserved face values (HancockStage.cpp:177-224, Advection.cpp:455-479).
+// `nmom` momentum components are carried; the others are exactly zero and so is their
+// velocity (0 / rho = +0 for a positive density).
 template <typename T, int NS, int EOS>
-__device__ __forceinline__ void closeFromConserved(const MixParams& mp, FaceState<T, NS>& s) {
+__device__ __forceinline__ void closeFromConserved(const MixParams& mp, FaceState<T, NS>& s, int nmom = 3) {
     s.c[0] = 0;
 #pragma unroll
     for (int k = 1; k <= NS; ++k) {
@@ -241,7 +253,7 @@ __device__ __forceinline__ void closeFromConserved(const MixParams& mp, FaceStat
         s.c[0] += s.c[k];
     }
 #pragma unroll
-    for (int d = 0; d < 3; ++d) s.v[d] = s.m[d] / s.rho[0];
+    for (int d = 0; d < 3; ++d) s.v[d] = d < nmom ? s.m[d] / s.rho[0] : T(0);
     T v2 = 0;
     v2 += s.v[0] * s.v[0];
     v2 += s.v[1] * s.v[1];

@@ -113,7 +113,7 @@ __device__ __forceinline__ void cellPrimitive(const StepParams& P, const double*
         c[0] += c[k];
     }
 #pragma unroll
-    for (int d = 0; d < 3; ++d) v[d] = m[d] / rho0;
+    for (int d = 0; d < 3; ++d) v[d] = d < P.nmom ? m[d] / rho0 : T(0);
     T v2 = 0;
     v2 += v[0] * v[0];
     v2 += v[1] * v[1];
@@ -125,15 +125,121 @@ __device__ __forceinline__ void cellPrimitive(const StepParams& P, const double*
 // Predicted face state of a cell whose slopes vanish: closure, zero Hancock divergence,
 // recalculation from conserved values, sound speed.
 template <typename T, int NS, int EOS>
-__device__ __forceinline__ void cellFaceState(const MixParams& mp, const T* c, const T* v, T p, FaceState<T, NS>& W) {
+__device__ __forceinline__ void cellFaceState(const MixParams& mp, const T* c, const T* v, T p, FaceState<T, NS>& W,
+                                              int nmom = 3) {
 #pragma unroll
     for (int k = 1; k <= NS; ++k) W.c[k] = c[k];
 #pragma unroll
     for (int d = 0; d < 3; ++d) W.v[d] = v[d];
     W.p = p;
     closeFromPrimitive<T, NS, EOS>(mp, W);
-    closeFromConserved<T, NS, EOS>(mp, W);
+    closeFromConserved<T, NS, EOS>(mp, W, nmom);
     soundSpeed<T, NS, EOS>(mp, W);
+}
+
+// FP32-flux predicted state: the closure / Hancock round trip is an identity up to rounding, so
+// the face state is the cell state itself (densities, momenta and energy as stored, primitives
+// recovered once with reciprocals).  Accuracy is bounded by the FP32 tolerance of this mode.
+template <int NS, int EOS>
+__device__ __forceinline__ void cellStateLean(const StepParams& P, const double* __restrict__ U, long long i,
+                                              FaceState<float, NS>& W) {
+    const long long s = P.stride;
+#pragma unroll
+    for (int k = 1; k <= NS; ++k) W.rho[k] = float(U[(k - 1) * s + i]);
+    W.rho[0] = float(U[NS * s + i]);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) W.m[d] = d < P.nmom ? float(U[(NS + 1 + d) * s + i]) : 0.f;
+    W.E = float(U[(NS + 4) * s + i]);
+    const float inv = 1.f / W.rho[0];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) W.v[d] = W.m[d] * inv;
+    const float v2 = W.v[0] * W.v[0] + W.v[1] * W.v[1] + W.v[2] * W.v[2];
+    W.Uv = W.E - 0.5f * W.rho[0] * v2;
+    W.c[0] = 0.f;
+#pragma unroll
+    for (int k = 1; k <= NS; ++k) {
+        W.c[k] = W.rho[k] * float(P.mix.invM[k - 1]);
+        W.c[0] += W.c[k];
+    }
+    const float ic0 = 1.f / W.c[0];
+    float Cvm = 0.f, Mm = 0.f, am = 0.f, bm = 0.f;
+    float X[NS];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        X[k] = W.c[k + 1] * ic0;
+        Cvm += X[k] * float(P.mix.Cv[k]);
+        Mm += X[k] * float(P.mix.M[k]);
+    }
+    const float g1 = float(P.mix.R) / Cvm;
+    if (EOS == FV_EOS_IDEAL) {
+        W.p = g1 * W.Uv;
+        W.cs = sqrtf(g1 * (W.Uv + W.p) * inv);
+    } else {
+#pragma unroll
+        for (int k = 0; k < NS; ++k)
+#pragma unroll
+            for (int l = 0; l < NS; ++l) {
+                am += X[k] * X[l] * float(P.mix.a[k][l]);
+                bm += X[k] * X[l] * float(P.mix.b[k][l]);
+            }
+        const float c0 = W.c[0];
+        const float acc = am * c0 * c0;
+        const float m_cb = 1.f - c0 * bm;
+        const float im = 1.f / m_cb;
+        W.p = g1 * (W.Uv + acc) * im - acc;
+        const float ac = am * c0;
+        const float dpdrho = (g1 * (2.f * ac * im - bm * (W.Uv + ac * c0) * im * im) - 2.f * ac) / Mm;
+        W.cs = sqrtf(dpdrho + g1 * im * (W.Uv + W.p) * inv);
+    }
+}
+
+// FP32-flux CFL signal (|v| + c) / minEdge of an updated cell.
+template <int NS, int EOS>
+__device__ __forceinline__ float cellSignalLean(const StepParams& P, const float* rho, const float* m, float E,
+                                                float minLS) {
+    FaceState<float, NS> W;
+    (void)W;
+    const float inv = 1.f / rho[0];
+    const float v0 = m[0] * inv, v1 = m[1] * inv, v2c = m[2] * inv;
+    const float vv = v0 * v0 + v1 * v1 + v2c * v2c;
+    const float Uv = E - 0.5f * rho[0] * vv;
+    float c[NS + 1];
+    c[0] = 0.f;
+#pragma unroll
+    for (int k = 1; k <= NS; ++k) {
+        c[k] = rho[k] * float(P.mix.invM[k - 1]);
+        c[0] += c[k];
+    }
+    const float ic0 = 1.f / c[0];
+    float Cvm = 0.f, Mm = 0.f, am = 0.f, bm = 0.f, X[NS];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        X[k] = c[k + 1] * ic0;
+        Cvm += X[k] * float(P.mix.Cv[k]);
+        Mm += X[k] * float(P.mix.M[k]);
+    }
+    const float g1 = float(P.mix.R) / Cvm;
+    float cs2;
+    if (EOS == FV_EOS_IDEAL) {
+        const float p = g1 * Uv;
+        cs2 = g1 * (Uv + p) * inv;
+    } else {
+#pragma unroll
+        for (int k = 0; k < NS; ++k)
+#pragma unroll
+            for (int l = 0; l < NS; ++l) {
+                am += X[k] * X[l] * float(P.mix.a[k][l]);
+                bm += X[k] * X[l] * float(P.mix.b[k][l]);
+            }
+        const float c0 = c[0];
+        const float acc = am * c0 * c0;
+        const float im = 1.f / (1.f - c0 * bm);
+        const float p = g1 * (Uv + acc) * im - acc;
+        const float ac = am * c0;
+        const float dpdrho = (g1 * (2.f * ac * im - bm * (Uv + ac * c0) * im * im) - 2.f * ac) / Mm;
+        cs2 = dpdrho + g1 * im * (Uv + p) * inv;
+    }
+    return (sqrtf(vv) + sqrtf(cs2)) * minLS;
 }
 
 // Compact part of W shared with in-plane neighbours for a face normal to `axis`.
@@ -200,7 +306,7 @@ __device__ __forceinline__ T cellSignal(const StepParams& P, const T* rho, T rho
     }
     T v[3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) v[d] = m[d] / rho0;
+    for (int d = 0; d < 3; ++d) v[d] = d < P.nmom ? m[d] / rho0 : T(0);
     T v2 = 0;
     v2 += v[0] * v[0];
     v2 += v[1] * v[1];
@@ -208,7 +314,7 @@ __device__ __forceinline__ T cellSignal(const StepParams& P, const T* rho, T rho
     const T Uv = E - rho0 * v2 * T(0.5) - T(0);
     const T p = Mixture<T, NS, EOS>::pFromUv(P.mix, c, Uv);
     const T sonic = Num<T>::sqrt_(Mixture<T, NS, EOS>::sqSonic(P.mix, c, rho0, Uv, p));
-    T s = mag3<T>(v[0], v[1], v[2]) + sonic;
+    T s = (P.nmom == 3 ? mag3<T>(v[0], v[1], v[2]) : mag2z<T>(v[0], v[1])) + sonic;
     s *= minLS;
     return s;
 }
@@ -216,25 +322,29 @@ __device__ __forceinline__ T cellSignal(const StepParams& P, const T* rho, T rho
 // ============================================================================ fused march
 // Block: BX x BY threads (BY = 1 in 2D).  Thread (tx, ty) owns in-plane column
 // (x0 - 1 + tx, y0 - 1 + ty); the outer ring of the block is halo.  D = 2 marches along y,
-// D = 3 along z.  Rows per block along the marching axis: `rows`.
-template <typename T, int NS, int EOS, int D, int BX, int BY>
-__global__ void __launch_bounds__(BX* BY) k_march(const StepParams P, const double* __restrict__ U,
-                                                  double* __restrict__ Un, const double* __restrict__ prim0,
-                                                  DevClock* __restrict__ ck, double* __restrict__ blockMax, int rows) {
+// D = 3 along z.  Rows per block along the marching axis: `rows`.  MINB: CTAs per SM the
+// register budget is sized for.
+template <typename T, int NS, int EOS, int D, int BX, int BY, int MINB>
+__global__ void __launch_bounds__(BX* BY, MINB) k_march(const StepParams P, const double* __restrict__ U,
+                                                        double* __restrict__ Un, const double* __restrict__ prim0,
+                                                        DevClock* __restrict__ ck, double* __restrict__ blockMax,
+                                                        int rows) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     auto sW = reinterpret_cast<SharedW<T, NS>(*)[BX]>(smem_raw);
     auto sFx = reinterpret_cast<FaceFlux<T, NS>(*)[BX]>(smem_raw + sizeof(SharedW<T, NS>) * BX * BY);
     auto sFy = reinterpret_cast<FaceFlux<T, NS>(*)[BX]>(smem_raw + (sizeof(SharedW<T, NS>) + sizeof(FaceFlux<T, NS>)) * BX * BY);
     __shared__ T red[32];
+    constexpr bool LEAN = sizeof(T) == 4;  // FP32-flux arithmetic
 
     if (ck->done) return;
     const double dt = ck->dt;
-    const double* __restrict__ prim = ck->first ? prim0 : nullptr;
+    const double* __restrict__ prim = (!LEAN && ck->first) ? prim0 : nullptr;
     const double gx_ = ck->g[0], gy_ = ck->g[1], gz_ = ck->g[2];
 
     constexpr int MA = D - 1;  // marching axis
     const int nx = P.n[0], ny = P.n[1];
     const int nm = P.n[MA];
+    const int nmom = P.nmom;
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int X = blockIdx.x * (BX - 2) - 1 + tx;
     const int Y = (D == 3) ? (int)(blockIdx.y * (BY - 2)) - 1 + ty : 0;
@@ -269,11 +379,23 @@ __global__ void __launch_bounds__(BX* BY) k_march(const StepParams P, const doub
         if (zm >= nm) { if (perM) return zm - nm; ok = false; return 0; }
         return zm;
     };
+    // predicted face state of a cell and its step-start velocity (for the gravity source)
+    auto stateOf = [&](long long cell, FaceState<T, NS>& W, T* vp) {
+        if constexpr (LEAN) {
+            cellStateLean<NS, EOS>(P, U, cell, W);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) vp[d] = W.v[d];
+        } else {
+            T c[NS + 1], v[3], p, r0, rr[NS + 1], mm[3], EE;
+            cellPrimitive<T, NS, EOS, D>(P, U, prim, cell, c, v, p, r0, rr, mm, EE);
+            cellFaceState<T, NS, EOS>(P.mix, c, v, p, W, nmom);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) vp[d] = v[d];
+        }
+    };
 
     FaceState<T, NS> Wc, Wn;
-    T cOld[NS + 1], vOld[3], pOld, rho0Old;
-    T rhoU[NS + 1], mU[3], EU;
-    (void)pOld; (void)EU; (void)cOld;
+    T vCur[3] = {T(0), T(0), T(0)}, vNext[3] = {T(0), T(0), T(0)};
     FaceFlux<T, NS> Gprev;
     T GprevSign = T(-1);
     T localMax = T(-1);
@@ -281,15 +403,12 @@ __global__ void __launch_bounds__(BX* BY) k_march(const StepParams P, const doub
 
     // ---- prologue: W(z0) and the flux of the face below z0
     if (has && z0 < z1) {
-        T c[NS + 1], v[3], p, r0, rr[NS + 1], mm[3], EE;
-        cellPrimitive<T, NS, EOS, D>(P, U, prim, cellAt(z0), c, v, p, r0, rr, mm, EE);
-        cellFaceState<T, NS, EOS>(P.mix, c, v, p, Wc);
+        stateOf(cellAt(z0), Wc, vCur);
         const int zb = wrapM(z0 - 1, ok);
         if (ok) {
-            T c2[NS + 1], v2[3], p2, r02, rr2[NS + 1], mm2[3], EE2;
-            cellPrimitive<T, NS, EOS, D>(P, U, prim, cellAt(zb), c2, v2, p2, r02, rr2, mm2, EE2);
             FaceState<T, NS> Wb;
-            cellFaceState<T, NS, EOS>(P.mix, c2, v2, p2, Wb);
+            T vb[3];
+            stateOf(cellAt(zb), Wb, vb);
             if (!riemann<T, NS>(P.flux, MA, 1, Wb, Wc, Gprev)) raise(ck, FV_ERR_RIEMANN);
             GprevSign = T(-1);
         } else {
@@ -303,20 +422,10 @@ __global__ void __launch_bounds__(BX* BY) k_march(const StepParams P, const doub
     }
 
     for (int z = z0; z < z1; ++z) {
-        // own conserved state and primitives of row z (needed for the update and gravity)
-        if (has) {
-            T r0;
-            cellPrimitive<T, NS, EOS, D>(P, U, prim, cellAt(z), cOld, vOld, pOld, r0, rhoU, mU, EU);
-            rho0Old = r0;
-        }
         // W of the next row
         const int zn = wrapM(z + 1, ok);
         const bool hasNext = has && ok;
-        if (hasNext) {
-            T c[NS + 1], v[3], p, r0, rr[NS + 1], mm[3], EE;
-            cellPrimitive<T, NS, EOS, D>(P, U, prim, cellAt(zn), c, v, p, r0, rr, mm, EE);
-            cellFaceState<T, NS, EOS>(P.mix, c, v, p, Wn);
-        }
+        if (hasNext) stateOf(cellAt(zn), Wn, vNext);
         if (has) toShared<T, NS>(Wc, sW[ty][tx]);
         __syncthreads();
         // in-plane fluxes through the low faces of this column
@@ -397,6 +506,7 @@ __global__ void __launch_bounds__(BX* BY) k_march(const StepParams P, const doub
                 V = hx * hy * hm;
                 minLS = T(1) / smin(smin(hx, hy), hm);
             }
+            const T invV = LEAN ? T(1) / V : T(0);
             // divergence in the face order of mesh.cpp: 2D [x-, x+, y+, y-], 3D [x-, x+, y+, y-, z-, z+]
             auto div = [&](auto get) -> T {
                 T s = get(Fxm) * sxm * Sx;
@@ -410,57 +520,64 @@ __global__ void __launch_bounds__(BX* BY) k_march(const StepParams P, const doub
                     s += get(Gprev) * GprevSign * Sm;
                     s += get(Gnext) * Sm;
                 }
-                return s / V;
+                return LEAN ? s * invV : s / V;
             };
             const long long ic = cellAt(z);
             const long long st = P.stride;
-            T rhoN[NS + 1], mN[3];
             // FP64 accumulation of the conserved update: U_new = U - div * dt
-            double Enew = U[(NS + 4) * st + ic] -
-                          double(div([](const FaceFlux<T, NS>& f) { return f.E; })) * dt;
+            const double rho0Old = U[NS * st + ic];
+            double Enew = U[(NS + 4) * st + ic] - double(div([](const FaceFlux<T, NS>& f) { return f.E; })) * dt;
             double mNew[3] = {0, 0, 0};
 #pragma unroll
             for (int d = 0; d < 3; ++d)
-                if (d < P.nmom)
+                if (d < nmom)
                     mNew[d] = U[(NS + 1 + d) * st + ic] - double(div([d](const FaceFlux<T, NS>& f) { return f.m[d]; })) * dt;
             if (P.gravity) {
                 // Advection.cpp:424-431 with the old density and velocity
+                const T r0 = T(rho0Old);
                 T vg = 0;
-                vg += vOld[0] * T(gx_);
-                vg += vOld[1] * T(gy_);
-                vg += vOld[2] * T(gz_);
+                vg += vCur[0] * T(gx_);
+                vg += vCur[1] * T(gy_);
+                vg += vCur[2] * T(gz_);
                 const T gvec[3] = {T(gx_), T(gy_), T(gz_)};
-                Enew += double(rho0Old * vg) * dt;
+                Enew += double(r0 * vg) * dt;
 #pragma unroll
                 for (int d = 0; d < 3; ++d)
-                    if (d < P.nmom) mNew[d] += double(gvec[d] * rho0Old) * dt;
+                    if (d < nmom) mNew[d] += double(gvec[d] * r0) * dt;
             }
             double rNew[NS + 1];
+            rNew[0] = rho0Old - double(div([](const FaceFlux<T, NS>& f) { return f.rho[0]; })) * dt;
 #pragma unroll
-            for (int k = 0; k <= NS; ++k)
-                rNew[k] = U[(k == 0 ? NS : k - 1) * st + ic] -
-                          double(div([k](const FaceFlux<T, NS>& f) { return f.rho[k]; })) * dt;
+            for (int k = 1; k <= NS; ++k)
+                rNew[k] = U[(k - 1) * st + ic] - double(div([k](const FaceFlux<T, NS>& f) { return f.rho[k]; })) * dt;
             // store
 #pragma unroll
             for (int k = 1; k <= NS; ++k) Un[(k - 1) * st + ic] = rNew[k];
             Un[NS * st + ic] = rNew[0];
 #pragma unroll
             for (int d = 0; d < 3; ++d)
-                if (d < P.nmom) Un[(NS + 1 + d) * st + ic] = mNew[d];
+                if (d < nmom) Un[(NS + 1 + d) * st + ic] = mNew[d];
             Un[(NS + 4) * st + ic] = Enew;
             // CFL signal of the updated cell
+            T rhoN[NS + 1], mN[3];
 #pragma unroll
             for (int k = 0; k <= NS; ++k) rhoN[k] = T(rNew[k]);
 #pragma unroll
             for (int d = 0; d < 3; ++d) mN[d] = T(mNew[d]);
-            const T s = cellSignal<T, NS, EOS, D>(P, rhoN, rhoN[0], mN, T(Enew), minLS);
+            T s;
+            if constexpr (LEAN) s = cellSignalLean<NS, EOS>(P, rhoN, mN, T(Enew), minLS);
+            else s = cellSignal<T, NS, EOS, D>(P, rhoN, rhoN[0], mN, T(Enew), minLS);
             localMax = smax(localMax, s);
         }
         // roll the marching window
         if (has) {
             Gprev = Gnext;
             GprevSign = T(-1);
-            if (hasNext) Wc = Wn;
+            if (hasNext) {
+                Wc = Wn;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) vCur[d] = vNext[d];
+            }
         }
     }
     const T bm = blockMaxReduce<T>(localMax, red);
@@ -468,6 +585,11 @@ __global__ void __launch_bounds__(BX* BY) k_march(const StepParams P, const doub
         const long long b = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
         blockMax[b] = double(bm);
     }
+}
+
+// CTAs per SM the register budget of k_march is sized for.
+template <typename T, int BX, int BY> constexpr int marchMinBlocks() {
+    return sizeof(T) == 8 ? (384 / (BX * BY) > 0 ? 384 / (BX * BY) : 1) : (512 / (BX * BY) > 0 ? 512 / (BX * BY) : 1);
 }
 
 // ============================================================================ finalize

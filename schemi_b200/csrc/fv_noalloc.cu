@@ -159,6 +159,7 @@ bool buildParams(const fv_config& c, StepParams& P) {
     mp.R = c.R;
     for (int k = 0; k < c.n_species; ++k) {
         mp.M[k] = c.M[k];
+        mp.invM[k] = 1.0 / c.M[k];
         mp.Cv[k] = c.Cv[k];
     }
     if (c.eos == FV_EOS_VAN_DER_WAALS) {
