@@ -258,6 +258,47 @@ def e2e_run(g, prim_pinned, steps):
     return wall, st, h2d, d2h
 
 
+def batched_vs_plain(n_cases: int, steps: int, torch):
+    """Config-4 shape: `n_cases` Richtmyer-Meshkov cases of seeded sizes 128^2..512^2 (FP32 flux,
+    HLLC + superbee, own end times), advanced `steps` ensemble steps by the batched persistent
+    kernel, against the same cases advanced one after the other by the single-case path."""
+    from schemi_b200 import cases, fv
+
+    handles, t_end, cells = [], [], 0
+    for i in range(n_cases):
+        case, prim, te = cases.richtmyer_meshkov(i, precision="f32flux")
+        g = fv.FVCase(case)
+        g.set_march_shape(128, 1, 16)
+        g.upload(prim)
+        handles.append(g)
+        t_end.append(te)
+        cells += case.n_cells
+    torch.cuda.synchronize()
+    # plain: each case on its own, `steps` steps through fv_run (device time per case)
+    plain_ms = 0.0
+    plain_updates = 0
+    for g, te in zip(handles, t_end):
+        st = g.run(te, max_steps=steps)
+        plain_ms += st.device_ms
+        plain_updates += st.steps * g.n_cells
+    batch = fv.FVBatch(handles)
+    batch.run(t_end, max_steps=16)  # warm-up (graph capture, kernel configuration)
+    st = batch.run(t_end, max_steps=steps)
+    out = {
+        "cases": n_cases, "cells": cells, "steps": steps, "arith": "f32flux",
+        "value": st.cell_updates / (st.device_ms / 1e3), "unit": "cell-updates/s",
+        "ms_per_ensemble_step": st.device_ms / steps,
+        "plain_value": plain_updates / (plain_ms / 1e3),
+        "launches_per_ensemble_step": st.launches / max(st.steps_max, 1),
+        "bytes_per_cell_update": 2 * 8 * (2 + 1 + 2 + 1),
+    }
+    out["batched_over_plain"] = out["value"] / out["plain_value"]
+    batch.close()
+    for g in handles:
+        g.close()
+    return out
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -363,6 +404,10 @@ def run_ours(args):
             "clocks": results["f32flux"]["clocks"],
         },
     }
+    if args.batch_cases > 0:
+        b = batched_vs_plain(args.batch_cases, args.steps, torch)
+        b["roofline_frac"] = b["value"] * b["bytes_per_cell_update"] / 1e9 / peak
+        line["batched"] = b
     if rank == 0 and not args.no_cpu_baseline:
         try:
             v, info = reference_throughput(n=128, steps=12, steps0=2, processes=1)
@@ -391,6 +436,7 @@ def main():
     ap.add_argument("--n", type=int, default=1024, help="cells per axis of the KH workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--batch-cases", type=int, default=512, help="cases of the batched ensemble (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

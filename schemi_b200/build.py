@@ -2,11 +2,13 @@
 
     python -m schemi_b200.build            # or build() from Python
 
-Translation units:
-  csrc/fv_f64.cu   FP64 step kernels, --fmad=false (bit-exact with the reference build)
-  csrc/fv_f32.cu   FP32-flux step kernels
-  csrc/fv_capi.cu  C-ABI, upload/download/finalize kernels, device time loop (--fmad=false)
-  csrc/fv_batch.cu batched persistent ensemble kernel
+Translation units (compiled in parallel):
+  csrc/fv_f64_ns<N>.cu  FP64 step kernels for N species, --fmad=false (bit-exact with the reference)
+  csrc/fv_f32_ns<N>.cu  FP32-flux step kernels for N species, fast math
+  csrc/fv_dispatch.cu   selects the unit of a species count
+  csrc/fv_capi.cu       C-ABI, upload/download/finalize kernels, device time loop (--fmad=false)
+  csrc/fv_batch.cu      batched ensemble (--fmad=false)
+  csrc/fv_noalloc.cu    the step without device allocation (--fmad=false)
 nvcc cross-compiles for sm_100a without a GPU.
 """
 
@@ -28,10 +30,12 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "--expt-relaxed-constexpr",
           "-I", os.path.join(HERE, "..", "include")]
 UNITS = {
-    "fv_f64.cu": ["--fmad=false"],
-    "fv_f32.cu": ["-use_fast_math"],
     "fv_capi.cu": ["--fmad=false"],
+    "fv_dispatch.cu": [],
 }
+for _ns in (1, 2, 3, 4):
+    UNITS[f"fv_f64_ns{_ns}.cu"] = ["--fmad=false"]
+    UNITS[f"fv_f32_ns{_ns}.cu"] = ["-use_fast_math"]
 
 
 def nvcc() -> str:
@@ -69,7 +73,7 @@ def build(verbose: bool = False, force: bool = False, extra_flags=None) -> str:
         if force or _stale(obj, deps):
             cmd = [nvcc(), *ARCH, *COMMON, *flags, *(extra_flags or []), "-c", os.path.join(CSRC, unit), "-o", obj]
             jobs.append(cmd)
-    with cf.ThreadPoolExecutor(max_workers=max(1, len(jobs))) as ex:
+    with cf.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 4))) as ex:
         futs = [ex.submit(subprocess.run, cmd, capture_output=True, text=True) for cmd in jobs]
         for cmd, fut in zip(jobs, futs):
             res = fut.result()

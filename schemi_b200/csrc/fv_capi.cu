@@ -109,58 +109,16 @@ __global__ void k_transverse(const StepParams P, const double* __restrict__ prim
 namespace fv {
 // CFL block of Schemi.cpp:802-835 and the last-step clamp of :933-935.
 __global__ void k_finalize(const StepParams P, DevClock* ck, const double* __restrict__ blockMax, int nblocks) {
-    __shared__ double red[32];
-    if (ck->done) return;
-    double m = -1;
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) m = smax(m, blockMax[b]);
-    m = blockMaxReduce<double>(m, red);
-    if (threadIdx.x != 0) return;
-    const double dtUsed = ck->dt;
-    double dtn = P.courant / m;
-    if (!P.courant_only) dtn = smin(dtn, kVeryBigD());
-    dtn = smax(dtn, P.min_dt);
-    if (P.gravity) {
-        for (int d = 0; d < 3; ++d) ck->g[d] += ck->g_delta[d] * dtUsed;
-    }
-    ck->time += dtUsed;
-    ck->steps += 1;
-    ck->first = 0;
-    ck->dt_used = dtUsed;
-    ck->dt_free = dtn;
-    if ((ck->time + dtn) > ck->t_end) dtn = ck->t_end - ck->time;
-    ck->dt = dtn;
-    if (!(ck->time < ck->t_end) || ck->err) ck->done = 1;
+    finalizeCase(P, ck, blockMax, nblocks);
+}
+__global__ void k_finalize_batch(const BatchCase* __restrict__ cases, int nCases) {
+    const BatchCase& C = cases[blockIdx.x];
+    finalizeCase(C.P, C.ck, C.blockMax, C.nTiles);
 }
 }  // namespace fv
 
 // ============================================================================ host side
-struct fv_handle {
-    fv_config cfg;
-    StepParams P;
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    double* U[2] = {nullptr, nullptr};
-    int cur = 0;
-    double* prim0 = nullptr;
-    DevClock* ck = nullptr;        // device clock
-    DevClock* ckHost = nullptr;    // pinned mirror
-    double* blockMax = nullptr;
-    long long blockMaxCap = 0;
-    double* geo = nullptr;         // all geometry tables
-    void* Pc = nullptr;            // generic scratch
-    void* FS = nullptr;
-    void* FL = nullptr;
-    GenericLayout L{};
-    double* outBuf = nullptr;      // download staging
-    int path = PATH_GENERIC;
-    MarchShape shape{128, 1, 32};
-    int nConserved = 0;
-    // graphs of step chunks, one per start buffer
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    int graphSteps = 0;
-    std::string err;
-};
+#include "fv_handle.h"
 
 namespace {
 

@@ -1,0 +1,41 @@
+// fv_handle.h -- private layout of the C-ABI handle (shared by fv_capi.cu and fv_batch.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "../../include/fvstep.h"
+#include "fv_launch.cuh"
+
+using namespace fv;
+
+extern "C" fv_status fv_set_march_shape(fv_handle* h, int bx, int by, int rows);
+
+struct fv_handle {
+    fv_config cfg;
+    StepParams P;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double* U[2] = {nullptr, nullptr};
+    int cur = 0;
+    double* prim0 = nullptr;
+    DevClock* ck = nullptr;        // device clock
+    DevClock* ckHost = nullptr;    // pinned mirror
+    double* blockMax = nullptr;
+    long long blockMaxCap = 0;
+    double* geo = nullptr;         // all geometry tables
+    void* Pc = nullptr;            // generic scratch
+    void* FS = nullptr;
+    void* FL = nullptr;
+    GenericLayout L{};
+    double* outBuf = nullptr;      // download staging
+    int path = PATH_GENERIC;
+    MarchShape shape{128, 1, 32};
+    int nConserved = 0;
+    // graphs of step chunks, one per start buffer
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int graphSteps = 0;
+    std::string err;
+};

@@ -324,11 +324,11 @@ __device__ __forceinline__ T cellSignal(const StepParams& P, const T* rho, T rho
 // (x0 - 1 + tx, y0 - 1 + ty); the outer ring of the block is halo.  D = 2 marches along y,
 // D = 3 along z.  Rows per block along the marching axis: `rows`.  MINB: CTAs per SM the
 // register budget is sized for.
-template <typename T, int NS, int EOS, int D, int BX, int BY, int MINB>
-__global__ void __launch_bounds__(BX* BY, MINB) k_march(const StepParams P, const double* __restrict__ U,
-                                                        double* __restrict__ Un, const double* __restrict__ prim0,
-                                                        DevClock* __restrict__ ck, double* __restrict__ blockMax,
-                                                        int rows) {
+template <typename T, int NS, int EOS, int D, int BX, int BY>
+__device__ __forceinline__ void marchTile(const StepParams& P, const double* __restrict__ U, double* __restrict__ Un,
+                                          const double* __restrict__ prim0, DevClock* __restrict__ ck,
+                                          double* __restrict__ blockMaxOut, int rows, int tileX, int tileY,
+                                          int tileZ) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     auto sW = reinterpret_cast<SharedW<T, NS>(*)[BX]>(smem_raw);
     auto sFx = reinterpret_cast<FaceFlux<T, NS>(*)[BX]>(smem_raw + sizeof(SharedW<T, NS>) * BX * BY);
@@ -336,7 +336,7 @@ __global__ void __launch_bounds__(BX* BY, MINB) k_march(const StepParams P, cons
     __shared__ T red[32];
     constexpr bool LEAN = sizeof(T) == 4;  // FP32-flux arithmetic
 
-    if (ck->done) return;
+    if (ck->done) return;  // uniform over the CTA
     const double dt = ck->dt;
     const double* __restrict__ prim = (!LEAN && ck->first) ? prim0 : nullptr;
     const double gx_ = ck->g[0], gy_ = ck->g[1], gz_ = ck->g[2];
@@ -346,9 +346,9 @@ __global__ void __launch_bounds__(BX* BY, MINB) k_march(const StepParams P, cons
     const int nm = P.n[MA];
     const int nmom = P.nmom;
     const int tx = threadIdx.x, ty = threadIdx.y;
-    const int X = blockIdx.x * (BX - 2) - 1 + tx;
-    const int Y = (D == 3) ? (int)(blockIdx.y * (BY - 2)) - 1 + ty : 0;
-    const int z0 = (D == 3 ? blockIdx.z : blockIdx.y) * rows;
+    const int X = tileX * (BX - 2) - 1 + tx;
+    const int Y = (D == 3) ? tileY * (BY - 2) - 1 + ty : 0;
+    const int z0 = tileZ * rows;
     const int z1 = min(z0 + rows, nm);
     const bool perX = P.periodic[0], perY = (D == 3) && P.periodic[1], perM = P.periodic[MA];
 
@@ -581,9 +581,62 @@ __global__ void __launch_bounds__(BX* BY, MINB) k_march(const StepParams P, cons
         }
     }
     const T bm = blockMaxReduce<T>(localMax, red);
-    if (threadIdx.x == 0 && threadIdx.y == 0) {
-        const long long b = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
-        blockMax[b] = double(bm);
+    if (threadIdx.x == 0 && threadIdx.y == 0) *blockMaxOut = double(bm);
+}
+
+// Single-case step: one CTA per tile.
+template <typename T, int NS, int EOS, int D, int BX, int BY, int MINB>
+__global__ void __launch_bounds__(BX* BY, MINB) k_march(const StepParams P, const double* __restrict__ U,
+                                                        double* __restrict__ Un, const double* __restrict__ prim0,
+                                                        DevClock* __restrict__ ck, double* __restrict__ blockMax,
+                                                        int rows) {
+    const long long b = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+    if (D == 2)
+        marchTile<T, NS, EOS, D, BX, BY>(P, U, Un, prim0, ck, blockMax + b, rows, blockIdx.x, 0, blockIdx.y);
+    else
+        marchTile<T, NS, EOS, D, BX, BY>(P, U, Un, prim0, ck, blockMax + b, rows, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// One case of a batched ensemble (device-side case table).
+struct BatchCase {
+    StepParams P;
+    const double* U0;      // state buffer read at even step counts (relative to stepsBase)
+    double* U1;            // the other buffer
+    const double* prim0;
+    DevClock* ck;
+    double* blockMax;      // this case's CTA partials
+    long long stepsBase;   // clock step count when the run started
+    int tiles[3];          // tiles along x, y (3D), marching axis
+    int nTiles;
+    long long tileBase;    // first tile of this case in the ensemble's tile list
+};
+
+// Ensemble step: a persistent grid strides over the tiles of all cases; each case picks its
+// read/write buffers from the parity of its own step count, so cases advance independently.
+template <typename T, int NS, int EOS, int D, int BX, int BY, int MINB>
+__global__ void __launch_bounds__(BX* BY, MINB) k_march_batch(const BatchCase* __restrict__ cases, int nCases,
+                                                              long long totalTiles, int rows) {
+    for (long long t = blockIdx.x; t < totalTiles; t += gridDim.x) {
+        // case of tile t: binary search over tileBase
+        int lo = 0, hi = nCases - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (cases[mid].tileBase <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        const BatchCase& C = cases[lo];
+        const DevClock* ck = C.ck;
+        if (ck->done) continue;
+        const long long local = t - C.tileBase;
+        const int tx = (int)(local % C.tiles[0]);
+        const long long rest = local / C.tiles[0];
+        const int tyy = D == 3 ? (int)(rest % C.tiles[1]) : 0;
+        const int tz = D == 3 ? (int)(rest / C.tiles[1]) : (int)rest;
+        const bool odd = ((ck->steps - C.stepsBase) & 1) != 0;
+        const double* Uin = odd ? C.U1 : C.U0;
+        double* Uout = odd ? const_cast<double*>(C.U0) : C.U1;
+        marchTile<T, NS, EOS, D, BX, BY>(C.P, Uin, Uout, C.prim0, C.ck, C.blockMax + local, rows, tx, tyy, tz);
+        __syncthreads();  // shared memory is reused by the next tile
     }
 }
 
@@ -595,6 +648,35 @@ template <typename T, int BX, int BY> constexpr int marchMinBlocks() {
 // ============================================================================ finalize
 // dt = Courant / max signal; dt = min(dt, dtSource) unless Courant-only; dt = max(dt, minTime);
 // time += dt_used; g += g_delta * dt_used; clamp to t_end (Schemi.cpp:802-835, 933-935).
+// Executed by one CTA.
+__device__ __forceinline__ void finalizeCase(const StepParams& P, DevClock* ck, const double* __restrict__ blockMax,
+                                             int nblocks) {
+    __shared__ double red[32];
+    if (ck->done) return;
+    double m = -1;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) m = smax(m, blockMax[b]);
+    m = blockMaxReduce<double>(m, red);
+    if (threadIdx.x != 0) return;
+    const double dtUsed = ck->dt;
+    double dtn = P.courant / m;
+    if (!P.courant_only) dtn = smin(dtn, kVeryBigD());
+    dtn = smax(dtn, P.min_dt);
+    if (P.gravity) {
+        for (int d = 0; d < 3; ++d) ck->g[d] += ck->g_delta[d] * dtUsed;
+    }
+    ck->time += dtUsed;
+    ck->steps += 1;
+    ck->first = 0;
+    ck->dt_used = dtUsed;
+    ck->dt_free = dtn;
+    if ((ck->time + dtn) > ck->t_end) dtn = ck->t_end - ck->time;
+    ck->dt = dtn;
+    if (!(ck->time < ck->t_end) || ck->err) ck->done = 1;
+}
+
 __global__ void k_finalize(const StepParams P, DevClock* ck, const double* __restrict__ blockMax, int nblocks);
+
+// One CTA per case of an ensemble.
+__global__ void k_finalize_batch(const BatchCase* __restrict__ cases, int nCases);
 
 }  // namespace fv

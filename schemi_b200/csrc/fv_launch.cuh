@@ -36,6 +36,14 @@ long long genericBlocks(const StepParams& P);
 cudaError_t launchStepF64(const StepParams& P, const StepBuffers& B, int path, const MarchShape& s, cudaStream_t st);
 cudaError_t launchStepF32(const StepParams& P, const StepBuffers& B, int path, const MarchShape& s, cudaStream_t st);
 
+// Enqueue one ensemble step kernel over the case table (without the per-case finalize).
+// With casesDev == nullptr and st == nullptr it only configures the kernel and returns, in
+// *gridBlocks, the persistent grid size (SMs x resident CTAs).
+cudaError_t launchBatchF64(int ns, int eos, int dims, const BatchCase* casesDev, int nCases, long long totalTiles,
+                           const MarchShape& s, int* gridBlocks, cudaStream_t st);
+cudaError_t launchBatchF32(int ns, int eos, int dims, const BatchCase* casesDev, int nCases, long long totalTiles,
+                           const MarchShape& s, int* gridBlocks, cudaStream_t st);
+
 // Shared memory of the fused march for a shape (bytes), per precision.
 size_t marchSmemF64(int ns, int dims, const MarchShape& s);
 size_t marchSmemF32(int ns, int dims, const MarchShape& s);

@@ -218,3 +218,40 @@ class FVCase:
         ms = ctypes.c_float()
         self._check(self.lib.fv_time_step_kernel(self._h, iters, ctypes.byref(ms)))
         return ms.value
+
+
+class FVBatch:
+    """Ensemble of FVCase handles advanced together by the batched persistent kernel."""
+
+    def __init__(self, handles: Sequence[FVCase]):
+        self.lib = load()
+        self.handles = list(handles)
+        arr = (ctypes.c_void_p * len(self.handles))(*[h.handle for h in self.handles])
+        b = ctypes.c_void_p()
+        st = self.lib.fv_batch_create(arr, len(self.handles), ctypes.byref(b))
+        if st != 0:
+            raise FVError(st, "fv_batch_create failed (see stderr)")
+        self._b = b
+
+    def run(self, t_end: Sequence[float], max_steps: int = 1 << 60) -> fv_batch_stats_t:
+        te = np.ascontiguousarray(np.asarray(t_end, dtype=np.float64))
+        if te.size != len(self.handles):
+            raise ValueError("one end time per case")
+        s = fv_batch_stats_t()
+        st = self.lib.fv_batch_run(self._b, te.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), max_steps,
+                                   ctypes.byref(s))
+        if st != 0:
+            raise FVError(st, "fv_batch_run")
+        return s
+
+    def close(self):
+        if getattr(self, "_b", None):
+            self.lib.fv_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
