@@ -459,6 +459,8 @@ fv_status fv_create(const fv_config* cfg, fv_handle** out) {
     }
     h->nConserved = cfg->n_species + 5;
     P.nmom = cfg->dims;
+    // rows are staged with 16-byte aligned bulk copies: field and row pitches must be even
+    P.tma = (P.n[0] % 2 == 0) ? 1 : 0;
     h->path = choosePath(*cfg);
     h->shape = defaultShape(*cfg);
 
@@ -799,6 +801,20 @@ fv_status fv_set_march_shape(fv_handle* h, int bx, int by, int rows) {
     destroyGraphs(h);
     return ensureScratch(h);
 }
+
+// Row staging through shared memory with bulk async copies (1) or direct global loads (0);
+// staging needs an even number of cells along x.
+fv_status fv_set_staging(fv_handle* h, int on) {
+    if (!h) return FV_ERR_INIT;
+    const int want = (on && h->P.n[0] % 2 == 0) ? 1 : 0;
+    if (want != h->P.tma) {
+        h->P.tma = want;
+        destroyGraphs(h);
+    }
+    return FV_OK;
+}
+
+int fv_get_staging(const fv_handle* h) { return h ? h->P.tma : -1; }
 
 fv_status fv_force_generic(fv_handle* h) {
     if (!h) return FV_ERR_INIT;

@@ -45,6 +45,7 @@ struct StepParams {
     long long ncell;
     long long stride;       // distance between fields of U
     int nmom;               // momentum components carried (dims, or 3 when a transverse velocity is non-zero)
+    int tma;                // 1: stage state rows into shared memory with bulk async copies (nx even)
     int limiter;
     int flux;
     int gravity;
@@ -80,20 +81,32 @@ __device__ __forceinline__ long long cellIndex(const StepParams& P, int i, int j
     return (long long)i + (long long)P.n[0] * ((long long)j + (long long)P.n[1] * k);
 }
 
+// Where a cell's conserved values are read from: its element of field slot 0 and the distance
+// between slots.  Slots 0..N are the densities, N+1.. the carried momenta, `eSlot` the energy
+// (global memory: N+4; a staged row in shared memory: N+1+nmom).
+struct Src {
+    const double* p;
+    long long fs;
+    int eSlot;
+};
+
+__device__ __forceinline__ Src globalSrc(const StepParams& P, const double* __restrict__ U, long long i) {
+    return Src{U + i, P.stride, P.mix.ns + 4};
+}
+
 // Primitive recovery of a cell from its conserved state (Advection.cpp:455-479), or the
 // uploaded restart primitives before the first step (phaseInitialization keeps them as read).
 template <typename T, int NS, int EOS, int D>
-__device__ __forceinline__ void cellPrimitive(const StepParams& P, const double* __restrict__ U,
-                                              const double* __restrict__ prim, long long i, T* c, T* v, T& p,
-                                              T& rho0, T* rho, T* m, T& E) {
+__device__ __forceinline__ void cellPrimitive(const StepParams& P, const Src& sc, const double* __restrict__ prim,
+                                              long long i, T* c, T* v, T& p, T& rho0, T* rho, T* m, T& E) {
     const long long s = P.stride;
 #pragma unroll
-    for (int k = 1; k <= NS; ++k) rho[k] = T(U[(k - 1) * s + i]);
-    rho0 = T(U[NS * s + i]);
+    for (int k = 1; k <= NS; ++k) rho[k] = T(sc.p[(k - 1) * sc.fs]);
+    rho0 = T(sc.p[NS * sc.fs]);
     rho[0] = rho0;
 #pragma unroll
-    for (int d = 0; d < 3; ++d) m[d] = d < P.nmom ? T(U[(NS + 1 + d) * s + i]) : T(0);
-    E = T(U[(NS + 4) * s + i]);
+    for (int d = 0; d < 3; ++d) m[d] = d < P.nmom ? T(sc.p[(NS + 1 + d) * sc.fs]) : T(0);
+    E = T(sc.p[sc.eSlot * sc.fs]);
     if (prim) {
         c[0] = 0;
 #pragma unroll
@@ -122,6 +135,13 @@ __device__ __forceinline__ void cellPrimitive(const StepParams& P, const double*
     p = Mixture<T, NS, EOS>::pFromUv(P.mix, c, Uv);
 }
 
+template <typename T, int NS, int EOS, int D>
+__device__ __forceinline__ void cellPrimitive(const StepParams& P, const double* __restrict__ U,
+                                              const double* __restrict__ prim, long long i, T* c, T* v, T& p,
+                                              T& rho0, T* rho, T* m, T& E) {
+    cellPrimitive<T, NS, EOS, D>(P, globalSrc(P, U, i), prim, i, c, v, p, rho0, rho, m, E);
+}
+
 // Predicted face state of a cell whose slopes vanish: closure, zero Hancock divergence,
 // recalculation from conserved values, sound speed.
 template <typename T, int NS, int EOS>
@@ -141,15 +161,13 @@ __device__ __forceinline__ void cellFaceState(const MixParams& mp, const T* c, c
 // the face state is the cell state itself (densities, momenta and energy as stored, primitives
 // recovered once with reciprocals).  Accuracy is bounded by the FP32 tolerance of this mode.
 template <int NS, int EOS>
-__device__ __forceinline__ void cellStateLean(const StepParams& P, const double* __restrict__ U, long long i,
-                                              FaceState<float, NS>& W) {
-    const long long s = P.stride;
+__device__ __forceinline__ void cellStateLean(const StepParams& P, const Src& sc, FaceState<float, NS>& W) {
 #pragma unroll
-    for (int k = 1; k <= NS; ++k) W.rho[k] = float(U[(k - 1) * s + i]);
-    W.rho[0] = float(U[NS * s + i]);
+    for (int k = 1; k <= NS; ++k) W.rho[k] = float(sc.p[(k - 1) * sc.fs]);
+    W.rho[0] = float(sc.p[NS * sc.fs]);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) W.m[d] = d < P.nmom ? float(U[(NS + 1 + d) * s + i]) : 0.f;
-    W.E = float(U[(NS + 4) * s + i]);
+    for (int d = 0; d < 3; ++d) W.m[d] = d < P.nmom ? float(sc.p[(NS + 1 + d) * sc.fs]) : 0.f;
+    W.E = float(sc.p[sc.eSlot * sc.fs]);
     const float inv = 1.f / W.rho[0];
 #pragma unroll
     for (int d = 0; d < 3; ++d) W.v[d] = W.m[d] * inv;
@@ -319,6 +337,63 @@ __device__ __forceinline__ T cellSignal(const StepParams& P, const T* rho, T rho
     return s;
 }
 
+// ============================================================================ bulk async copies
+// Rows of the state are staged into shared memory by the TMA unit's untiled bulk copies
+// (cp.async.bulk, 16-byte aligned source, destination and size), completing on an mbarrier
+// that carries the expected byte count.
+__device__ __forceinline__ uint32_t smemAddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbarInit(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smemAddr(bar)) : "memory");
+}
+__device__ __forceinline__ void mbarInval(uint64_t* bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smemAddr(bar)) : "memory");
+}
+__device__ __forceinline__ void fenceBarrierInit() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fenceProxyAsync() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbarArriveExpect(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smemAddr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbarArrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smemAddr(bar)) : "memory");
+}
+__device__ __forceinline__ void bulkCopyG2S(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smemAddr(dst)), "l"(src), "r"(bytes), "r"(smemAddr(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbarTryWait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smemAddr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Wait for a phase with a time limit of about a second; false on timeout.
+__device__ __forceinline__ bool mbarWaitBounded(uint64_t* bar, uint32_t parity) {
+    const long long t0 = clock64();
+    while (!mbarTryWait(bar, parity))
+        if (clock64() - t0 > 2000000000LL) return false;
+    return true;
+}
+
+// Ring of staged rows: stages along the marching axis, each holding NS+5 field slots of BY
+// in-plane rows of BX+2 doubles (a segment starting two columns left of the tile).
+template <int D> __host__ __device__ constexpr int ringStages() { return D == 3 ? 3 : 4; }
+template <int NS, int D, int BX, int BY> __host__ __device__ constexpr size_t ringBytes() {
+    return (size_t)ringStages<D>() * (NS + 5) * (D == 3 ? BY : 1) * (BX + 2) * sizeof(double);
+}
+template <typename T, int NS, int BX, int BY> __host__ __device__ constexpr size_t marchArraysBytes() {
+    return ((sizeof(SharedW<T, NS>) + 2 * sizeof(FaceFlux<T, NS>)) * BX * BY + 127) / 128 * 128;
+}
+template <typename T, int NS, int D, int BX, int BY> __host__ __device__ constexpr size_t marchSmemBytes() {
+    return marchArraysBytes<T, NS, BX, BY>() + ringBytes<NS, D, BX, BY>();
+}
+
 // ============================================================================ fused march
 // Block: BX x BY threads (BY = 1 in 2D).  Thread (tx, ty) owns in-plane column
 // (x0 - 1 + tx, y0 - 1 + ty); the outer ring of the block is halo.  D = 2 marches along y,
@@ -329,10 +404,15 @@ __device__ __forceinline__ void marchTile(const StepParams& P, const double* __r
                                           const double* __restrict__ prim0, DevClock* __restrict__ ck,
                                           double* __restrict__ blockMaxOut, int rows, int tileX, int tileY,
                                           int tileZ) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     auto sW = reinterpret_cast<SharedW<T, NS>(*)[BX]>(smem_raw);
     auto sFx = reinterpret_cast<FaceFlux<T, NS>(*)[BX]>(smem_raw + sizeof(SharedW<T, NS>) * BX * BY);
     auto sFy = reinterpret_cast<FaceFlux<T, NS>(*)[BX]>(smem_raw + (sizeof(SharedW<T, NS>) + sizeof(FaceFlux<T, NS>)) * BX * BY);
+    double* ring = reinterpret_cast<double*>(smem_raw + marchArraysBytes<T, NS, BX, BY>());
+    constexpr int S = ringStages<D>();
+    constexpr int BXL = BX + 2;
+    constexpr int BYR = D == 3 ? BY : 1;
+    __shared__ __align__(8) uint64_t mbar[S];
     __shared__ T red[32];
     constexpr bool LEAN = sizeof(T) == 4;  // FP32-flux arithmetic
 
@@ -379,20 +459,99 @@ __device__ __forceinline__ void marchTile(const StepParams& P, const double* __r
         if (zm >= nm) { if (perM) return zm - nm; ok = false; return 0; }
         return zm;
     };
+
+    // ---- staged rows.  Ring position q = 0 .. nq-1 holds row z0 - 1 + q of the marching axis
+    // in stage q % S; its k-th use completes phase k of mbar[q % S].
+    const bool tma = P.tma != 0;
+    const int nfl = NS + 2 + nmom;                 // field slots staged: densities, momenta, energy
+    const int x0m2 = tileX * (BX - 2) - 2;         // even: start of the staged segment
+    const int segStart = max(x0m2, 0), segEnd = min(x0m2 + BXL, nx);
+    const int nq = (z1 - z0) + 2;
+    const int lane = (tx + ty * BX) & 31, warpId = (tx + ty * BX) >> 5;
+    auto slotField = [&](int f) { return f <= NS + nmom ? f : NS + 4; };  // slot -> global field
+    auto rowOf = [&](int q, int& rr) -> bool {
+        bool ok2;
+        rr = wrapM(z0 - 1 + q, ok2);
+        return ok2;
+    };
+    // in-plane rows staged per plane (3D): y = y0 - 1 + j, wrapped when periodic
+    auto planeRow = [&](int j, int& yy) -> bool {
+        if (D == 2) { yy = 0; return true; }
+        const int y = tileY * (BY - 2) - 1 + j;
+        if (y >= 0 && y < ny) { yy = y; return true; }
+        if (perY && y >= -1 && y <= ny) { yy = y < 0 ? y + ny : y - ny; return true; }
+        return false;
+    };
+    auto issue = [&](int q) {  // warp 0
+        const int stg = q % S;
+        int rr;
+        const bool rowOk = rowOf(q, rr);
+        int validRows = 0;
+        for (int j = 0; j < BYR; ++j) {
+            int yy;
+            validRows += planeRow(j, yy) ? 1 : 0;
+        }
+        const uint32_t bytes = rowOk ? (uint32_t)(nfl * validRows * (segEnd - segStart) * (int)sizeof(double)) : 0u;
+        if (lane == 0) {
+            if (bytes) mbarArriveExpect(&mbar[stg], bytes);
+            else mbarArrive(&mbar[stg]);
+        }
+        __syncwarp();
+        if (!rowOk) return;
+        for (int job = lane; job < nfl * BYR; job += 32) {
+            const int f = job / BYR, j = job % BYR;
+            int yy;
+            if (!planeRow(j, yy)) continue;
+            const long long rowBase = D == 2 ? (long long)rr * nx : ((long long)rr * ny + yy) * nx;
+            const double* src = U + (long long)slotField(f) * P.stride + rowBase + segStart;
+            double* dst = ring + (((long long)stg * nfl + f) * BYR + j) * BXL + (segStart - x0m2);
+            bulkCopyG2S(dst, src, (uint32_t)((segEnd - segStart) * sizeof(double)), &mbar[stg]);
+        }
+    };
+    bool abortTile = false;
+    int qIssued = 0;   // ring positions [0, qIssued) have been armed (same value in every thread)
+    int qWaited = -1;  // highest position waited for successfully
+    auto waitRow = [&](int q) {  // all threads; uniform
+        int rr;
+        if (!rowOf(q, rr)) return;
+        const bool ok2 = mbarWaitBounded(&mbar[q % S], (uint32_t)((q / S) & 1));
+        if (__syncthreads_or(!ok2)) abortTile = true;
+        else qWaited = q;
+    };
+    // source of this thread's cell in row q: staged shared memory, or global memory for a column
+    // outside the staged segment (a periodic wrap column)
+    const bool fromRing = tma && has && cx == X && X >= segStart && X < segEnd;
+    auto srcOf = [&](int q, long long cell) -> Src {
+        if (fromRing)
+            return Src{ring + ((long long)(q % S) * nfl * BYR + (D == 3 ? ty : 0)) * BXL + (X - x0m2),
+                       (long long)BYR * BXL, NS + 1 + nmom};
+        return globalSrc(P, U, cell);
+    };
     // predicted face state of a cell and its step-start velocity (for the gravity source)
-    auto stateOf = [&](long long cell, FaceState<T, NS>& W, T* vp) {
+    auto stateOf = [&](const Src& sc, long long cell, FaceState<T, NS>& W, T* vp) {
         if constexpr (LEAN) {
-            cellStateLean<NS, EOS>(P, U, cell, W);
+            (void)cell;
+            cellStateLean<NS, EOS>(P, sc, W);
 #pragma unroll
             for (int d = 0; d < 3; ++d) vp[d] = W.v[d];
         } else {
-            T c[NS + 1], v[3], p, r0, rr[NS + 1], mm[3], EE;
-            cellPrimitive<T, NS, EOS, D>(P, U, prim, cell, c, v, p, r0, rr, mm, EE);
+            T c[NS + 1], v[3], p, r0, rr2[NS + 1], mm[3], EE;
+            cellPrimitive<T, NS, EOS, D>(P, sc, prim, cell, c, v, p, r0, rr2, mm, EE);
             cellFaceState<T, NS, EOS>(P.mix, c, v, p, W, nmom);
 #pragma unroll
             for (int d = 0; d < 3; ++d) vp[d] = v[d];
         }
     };
+    if (tma) {
+        if (tx == 0 && ty == 0) {
+            for (int s2 = 0; s2 < S; ++s2) mbarInit(&mbar[s2]);
+            fenceBarrierInit();
+        }
+        __syncthreads();
+        if (warpId == 0)
+            for (int q = 0; q < S && q < nq; ++q) issue(q);
+        qIssued = min(S, nq);
+    }
 
     FaceState<T, NS> Wc, Wn;
     T vCur[3] = {T(0), T(0), T(0)}, vNext[3] = {T(0), T(0), T(0)};
@@ -402,13 +561,17 @@ __device__ __forceinline__ void marchTile(const StepParams& P, const double* __r
     bool ok;
 
     // ---- prologue: W(z0) and the flux of the face below z0
-    if (has && z0 < z1) {
-        stateOf(cellAt(z0), Wc, vCur);
+    if (tma) {
+        waitRow(0);
+        waitRow(1);
+    }
+    if (has && z0 < z1 && !abortTile) {
+        stateOf(srcOf(1, cellAt(z0)), cellAt(z0), Wc, vCur);
         const int zb = wrapM(z0 - 1, ok);
         if (ok) {
             FaceState<T, NS> Wb;
             T vb[3];
-            stateOf(cellAt(zb), Wb, vb);
+            stateOf(srcOf(0, cellAt(zb)), cellAt(zb), Wb, vb);
             if (!riemann<T, NS>(P.flux, MA, 1, Wb, Wc, Gprev)) raise(ck, FV_ERR_RIEMANN);
             GprevSign = T(-1);
         } else {
@@ -421,13 +584,26 @@ __device__ __forceinline__ void marchTile(const StepParams& P, const double* __r
         }
     }
 
-    for (int z = z0; z < z1; ++z) {
+    for (int z = z0; z < z1 && !abortTile; ++z) {
+        const int qc = z - z0 + 1;  // ring position of row z
         // W of the next row
+        if (tma) {
+            waitRow(qc + 1);
+            if (abortTile) break;
+        }
         const int zn = wrapM(z + 1, ok);
         const bool hasNext = has && ok;
-        if (hasNext) stateOf(cellAt(zn), Wn, vNext);
+        if (hasNext) stateOf(srcOf(qc + 1, cellAt(zn)), cellAt(zn), Wn, vNext);
         if (has) toShared<T, NS>(Wc, sW[ty][tx]);
         __syncthreads();
+        // the stage of row z - 1 is free: refill it two rows ahead of its next reader
+        if (tma && qc - 1 + S < nq) {
+            if (warpId == 0) {
+                fenceProxyAsync();  // generic reads of the stage before its asynchronous refill
+                issue(qc - 1 + S);
+            }
+            qIssued = qc + S;
+        }
         // in-plane fluxes through the low faces of this column
         if (has && tx >= 1) {
             FaceState<T, NS> Wl;
@@ -524,14 +700,15 @@ __device__ __forceinline__ void marchTile(const StepParams& P, const double* __r
             };
             const long long ic = cellAt(z);
             const long long st = P.stride;
+            const Src so = srcOf(qc, ic);
             // FP64 accumulation of the conserved update: U_new = U - div * dt
-            const double rho0Old = U[NS * st + ic];
-            double Enew = U[(NS + 4) * st + ic] - double(div([](const FaceFlux<T, NS>& f) { return f.E; })) * dt;
+            const double rho0Old = so.p[NS * so.fs];
+            double Enew = so.p[so.eSlot * so.fs] - double(div([](const FaceFlux<T, NS>& f) { return f.E; })) * dt;
             double mNew[3] = {0, 0, 0};
 #pragma unroll
             for (int d = 0; d < 3; ++d)
                 if (d < nmom)
-                    mNew[d] = U[(NS + 1 + d) * st + ic] - double(div([d](const FaceFlux<T, NS>& f) { return f.m[d]; })) * dt;
+                    mNew[d] = so.p[(NS + 1 + d) * so.fs] - double(div([d](const FaceFlux<T, NS>& f) { return f.m[d]; })) * dt;
             if (P.gravity) {
                 // Advection.cpp:424-431 with the old density and velocity
                 const T r0 = T(rho0Old);
@@ -549,7 +726,7 @@ __device__ __forceinline__ void marchTile(const StepParams& P, const double* __r
             rNew[0] = rho0Old - double(div([](const FaceFlux<T, NS>& f) { return f.rho[0]; })) * dt;
 #pragma unroll
             for (int k = 1; k <= NS; ++k)
-                rNew[k] = U[(k - 1) * st + ic] - double(div([k](const FaceFlux<T, NS>& f) { return f.rho[k]; })) * dt;
+                rNew[k] = so.p[(k - 1) * so.fs] - double(div([k](const FaceFlux<T, NS>& f) { return f.rho[k]; })) * dt;
             // store
 #pragma unroll
             for (int k = 1; k <= NS; ++k) Un[(k - 1) * st + ic] = rNew[k];
@@ -579,6 +756,20 @@ __device__ __forceinline__ void marchTile(const StepParams& P, const double* __r
                 for (int d = 0; d < 3; ++d) vCur[d] = vNext[d];
             }
         }
+    }
+    if (tma) {
+        // every issued stage was waited for (or completed without copies); a timed-out wait
+        // drains the remaining phases with the same time limit before the barriers are dropped
+        if (abortTile) {
+            if (tx == 0 && ty == 0) raise(ck, FV_ERR_SYSTEM);
+            for (int q = qWaited + 1; q < qIssued; ++q) {
+                int rr;
+                if (rowOf(q, rr)) mbarWaitBounded(&mbar[q % S], (uint32_t)((q / S) & 1));
+            }
+        }
+        __syncthreads();
+        if (tx == 0 && ty == 0)
+            for (int s2 = 0; s2 < S; ++s2) mbarInval(&mbar[s2]);
     }
     const T bm = blockMaxReduce<T>(localMax, red);
     if (threadIdx.x == 0 && threadIdx.y == 0) *blockMaxOut = double(bm);

@@ -75,6 +75,8 @@ def load():
     lib.fv_set_march_shape.argtypes = [P, I, I, I]
     lib.fv_force_generic.argtypes = [P]
     lib.fv_time_step_kernel.argtypes = [P, I, ctypes.POINTER(ctypes.c_float)]
+    lib.fv_set_staging.argtypes = [P, I]
+    lib.fv_get_staging.argtypes = [P]
     lib.fv_begin_steps.argtypes = [P]
     lib.fv_step_async.argtypes = [P]
     lib.fv_check.argtypes = [P]
@@ -196,6 +198,13 @@ class FVCase:
 
     def force_generic(self) -> None:
         self._check(self.lib.fv_force_generic(self._h))
+
+    def set_staging(self, on: bool) -> None:
+        self._check(self.lib.fv_set_staging(self._h, int(bool(on))))
+
+    @property
+    def staging(self) -> bool:
+        return self.lib.fv_get_staging(self._h) == 1
 
     def begin_steps(self) -> None:
         self._check(self.lib.fv_begin_steps(self._h))
