@@ -236,6 +236,55 @@ fv_status fv_batch_create(fv_handle* const* cases, int n_cases, fv_batch** out);
 fv_status fv_batch_run(fv_batch* b, const double* t_end, long long max_steps, fv_batch_stats* stats);
 void fv_batch_destroy(fv_batch* b);
 
+/* ---- Adjoint of the step (no counterpart in the reference: it has no adjoint) ----
+ * Differentiates the zero-slope multi-dimensional step -- the fused march, i.e. 2D/3D with a
+ * limiter whose multi-dimensional slopes are zero, ideal-gas mixtures -- with every step's dt
+ * and gravity vector frozen at the recorded values.
+ *
+ * fv_record runs the time loop of fv_run from the handle's current state to t_end, stores the
+ * state every `checkpoint_every` steps on the device, records each step's dt and gravity, and
+ * accumulates the objective J = sum_{n=1..N} dt_{n-1} W(U^n) with the mixing width
+ * W = 4 / (L_x [L_z in 3D]) * sum_cells X_h (1 - X_h) * (cell area in 2D, cell volume in 3D),
+ * X_h the mole fraction of species `heavy_species`.
+ * fv_replay runs the recorded number of steps again from the handle's current state with the
+ * recorded dt and gravity of each step (e.g. after uploading a perturbed initial state).
+ * fv_adjoint sweeps the recorded trajectory backwards, recomputing the states between
+ * checkpoints, and returns dJtot/dU^0 for Jtot = dJ_dJ * J + <dJ_dU_T, U^N>.
+ * All state arrays are device pointers in the fv_state_device layout
+ * ((n_species + 5) fields x n_cells, rho_1..rho_N, rho, m_x, m_y, m_z, E; x fastest).
+ * dJ_dU_T may be NULL (zero). */
+enum fv_objective { FV_OBJ_NONE = 0, FV_OBJ_MIXING_WIDTH = 1 };
+
+typedef struct fv_record_config {
+    int checkpoint_every;     /* steps between stored states (>= 1) */
+    int objective;            /* fv_objective */
+    int heavy_species;        /* 0-based species index of X_h */
+    int pad;
+} fv_record_config;
+
+typedef struct fv_record_stats {
+    double objective;         /* J */
+    double time;              /* time reached */
+    long long steps;          /* N */
+    long long checkpoints;    /* stored states */
+    float device_ms;
+} fv_record_stats;
+
+typedef struct fv_adjoint_stats {
+    long long steps;          /* adjoint steps (= N) */
+    long long recomputed;     /* forward steps recomputed from checkpoints */
+    float device_ms;          /* whole sweep incl. recomputation */
+    float recompute_ms;       /* recomputation share */
+} fv_adjoint_stats;
+
+fv_status fv_record(fv_handle* h, const fv_record_config* rc, double t_end, long long max_steps,
+                    fv_record_stats* stats);
+fv_status fv_replay(fv_handle* h, fv_record_stats* stats);
+fv_status fv_adjoint(fv_handle* h, const double* dJ_dU_T, double dJ_dJ, double* dJ_dU_0, fv_adjoint_stats* stats);
+
+/* Copies the handle's conserved state (fv_state_device layout) to the device array dst. */
+fv_status fv_state_copy(fv_handle* h, double* dst);
+
 #ifdef __cplusplus
 }
 #endif

@@ -9,6 +9,8 @@ Translation units (compiled in parallel):
   csrc/fv_capi.cu       C-ABI, upload/download/finalize kernels, device time loop (--fmad=false)
   csrc/fv_batch.cu      batched ensemble (--fmad=false)
   csrc/fv_noalloc.cu    the step without device allocation (--fmad=false)
+  csrc/fv_adjoint.cu    recorded trajectories, checkpoints and the adjoint sweep
+  csrc/fv_adjoint_f64.cu / fv_adjoint_f32.cu  adjoint step kernels per arithmetic
 nvcc cross-compiles for sm_100a without a GPU.
 """
 
@@ -32,6 +34,9 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 UNITS = {
     "fv_capi.cu": ["--fmad=false"],
     "fv_dispatch.cu": [],
+    "fv_adjoint.cu": [],
+    "fv_adjoint_f64.cu": [],
+    "fv_adjoint_f32.cu": ["-use_fast_math"],
 }
 for _ns in (1, 2, 3, 4):
     UNITS[f"fv_f64_ns{_ns}.cu"] = ["--fmad=false"]

@@ -531,6 +531,7 @@ void fv_destroy(fv_handle* h) {
     if (!h) return;
     destroyGraphs(h);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    releaseTrajectory(h);
     for (auto& u : h->U)
         if (u) cudaFree(u);
     if (h->prim0) cudaFree(h->prim0);

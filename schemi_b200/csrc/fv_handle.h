@@ -12,6 +12,9 @@ using namespace fv;
 
 extern "C" fv_status fv_set_march_shape(fv_handle* h, int bx, int by, int rows);
 
+// Frees the recorded trajectory of a handle (fv_adjoint.cu); called by fv_destroy.
+void releaseTrajectory(fv_handle* h);
+
 struct fv_handle {
     fv_config cfg;
     StepParams P;
@@ -37,5 +40,7 @@ struct fv_handle {
     // graphs of step chunks, one per start buffer
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int graphSteps = 0;
+    // recorded trajectory of fv_record (checkpoints, per-step records, adjoint buffers)
+    struct Trajectory* traj = nullptr;
     std::string err;
 };

@@ -43,6 +43,24 @@ class fv_batch_stats_t(ctypes.Structure):
                 ("launches", ctypes.c_longlong), ("device_ms", ctypes.c_float)]
 
 
+class fv_record_config_t(ctypes.Structure):
+    _fields_ = [("checkpoint_every", ctypes.c_int), ("objective", ctypes.c_int), ("heavy_species", ctypes.c_int),
+                ("pad", ctypes.c_int)]
+
+
+class fv_record_stats_t(ctypes.Structure):
+    _fields_ = [("objective", ctypes.c_double), ("time", ctypes.c_double), ("steps", ctypes.c_longlong),
+                ("checkpoints", ctypes.c_longlong), ("device_ms", ctypes.c_float)]
+
+
+class fv_adjoint_stats_t(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_longlong), ("recomputed", ctypes.c_longlong), ("device_ms", ctypes.c_float),
+                ("recompute_ms", ctypes.c_float)]
+
+
+OBJ_NONE, OBJ_MIXING_WIDTH = 0, 1
+
+
 def library_path() -> str:
     return LIB_PATH
 
@@ -84,6 +102,10 @@ def load():
     lib.fv_stream.argtypes = [P]
     lib.fv_kernels_per_step.restype = LL
     lib.fv_kernels_per_step.argtypes = [P]
+    lib.fv_record.argtypes = [P, ctypes.POINTER(fv_record_config_t), D, LL, ctypes.POINTER(fv_record_stats_t)]
+    lib.fv_replay.argtypes = [P, ctypes.POINTER(fv_record_stats_t)]
+    lib.fv_adjoint.argtypes = [P, P, D, P, ctypes.POINTER(fv_adjoint_stats_t)]
+    lib.fv_state_copy.argtypes = [P, P]
     if hasattr(lib, "fv_batch_create"):
         lib.fv_batch_create.argtypes = [ctypes.POINTER(P), I, ctypes.POINTER(P)]
         lib.fv_batch_run.argtypes = [P, DP, LL, ctypes.POINTER(fv_batch_stats_t)]
@@ -227,6 +249,37 @@ class FVCase:
         ms = ctypes.c_float()
         self._check(self.lib.fv_time_step_kernel(self._h, iters, ctypes.byref(ms)))
         return ms.value
+
+    # ---- adjoint (fv_record / fv_replay / fv_adjoint)
+    @property
+    def n_conserved(self) -> int:
+        return self.case.n_conserved
+
+    def record(self, t_end: float, checkpoint_every: int = 50, objective: int = OBJ_MIXING_WIDTH,
+               heavy_species: int = 0, max_steps: int = 1 << 60) -> fv_record_stats_t:
+        """Forward to t_end storing checkpoints and each step's dt and gravity; returns the
+        mixing-width objective J = sum_n dt_{n-1} W(U^n) in ``.objective``."""
+        rc = fv_record_config_t(checkpoint_every, objective, heavy_species, 0)
+        s = fv_record_stats_t()
+        self._check(self.lib.fv_record(self._h, ctypes.byref(rc), t_end, max_steps, ctypes.byref(s)))
+        return s
+
+    def replay(self) -> fv_record_stats_t:
+        """The recorded number of steps again from the current state with the recorded dt."""
+        s = fv_record_stats_t()
+        self._check(self.lib.fv_replay(self._h, ctypes.byref(s)))
+        return s
+
+    def adjoint(self, dJ_dU_T_ptr: Optional[int], dJ_dJ: float, dJ_dU_0_ptr: int) -> fv_adjoint_stats_t:
+        """Backward sweep: writes dJtot/dU^0 to the device array at dJ_dU_0_ptr (fv_state_device
+        layout); dJ_dU_T_ptr may be None."""
+        s = fv_adjoint_stats_t()
+        self._check(self.lib.fv_adjoint(self._h, dJ_dU_T_ptr, float(dJ_dJ), dJ_dU_0_ptr, ctypes.byref(s)))
+        return s
+
+    def state_copy(self, dst_ptr: int) -> None:
+        """Copies the conserved state to the device array at dst_ptr."""
+        self._check(self.lib.fv_state_copy(self._h, dst_ptr))
 
 
 class FVBatch:
