@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define FV_ABI_VERSION 1
+#define FV_ABI_VERSION 2
 #define FV_MAX_SPECIES 4
 
 typedef int fv_status;
@@ -87,8 +87,26 @@ enum fv_patch {
  * closures and face fluxes in FP32; conserved variables stored and accumulated in FP64. */
 enum fv_precision { FV_PREC_F64 = 0, FV_PREC_F32_FLUX = 1 };
 
-/* Chemistry source (per-cell, after the advection step). */
-enum fv_chemistry { FV_CHEM_NONE = 0, FV_CHEM_A_B_2C = 1 };
+/* Chemistry source (per cell, after the advection step; abstractChemicalKinetics::
+ * solveChemicalKinetics, headers/abstractChemicalKinetics.hpp:618, called from
+ * secondOrderStepSolver.cpp:86-91).
+ *   CL2     Cl2 + M <-> 2Cl + M, species 0 = Cl2, 1 = Cl, third body M = total concentration
+ *           (chemicalKineticsChlorumDissociation.cpp; set/chemicalKinetics.txt "Cl2").
+ *   A_B_2C  A + B -> 2C, species 0 = A, 1 = B, 2 = C (no counterpart in the reference; the same
+ *           integrator, heat release q per mol of reaction as in chemicalKineticsH2Cl2Combustion.cpp). */
+enum fv_chemistry { FV_CHEM_NONE = 0, FV_CHEM_A_B_2C = 1, FV_CHEM_CL2 = 2 };
+
+/* Per-cell linear solver of the backward-Euler step (set/chemicalKinetics.txt #Iterative_solver:
+ * "Gauss-Seidel", "Jacobi", "GaussElimination", "conjugateGradient", "JacobiConjugateGradient"). */
+enum fv_chem_solver {
+    FV_CHEM_GAUSS_SEIDEL = 0, FV_CHEM_JACOBI = 1, FV_CHEM_GAUSS_ELIMINATION = 2,
+    FV_CHEM_CONJUGATE_GRADIENT = 3, FV_CHEM_JACOBI_CONJUGATE_GRADIENT = 4
+};
+
+/* Arrhenius rate constant k = A * T^n * exp(-E / (R T)), E in J/mol (R units of the case). */
+typedef struct fv_arrhenius {
+    double A, n, E;
+} fv_arrhenius;
 
 typedef struct fv_config {
     int dims;                 /* 1, 2 or 3 (#Dimensions_of_the_task) */
@@ -117,13 +135,13 @@ typedef struct fv_config {
     double bc_vel_value[6][3];
     int bc_p[6];
     double bc_p_value[6];
-    /* Chemistry: one-step A + B -> 2C, rate = A * c_A * c_B * exp(-Ea_R / T),
-     * heat release q per mol of reaction (species 0, 1 -> 2). */
+    /* Chemistry (set/chemicalKinetics.txt). */
     int chemistry;            /* fv_chemistry */
-    double chem_A;
-    double chem_Ea_R;
-    double chem_q;
-    int chem_substeps;        /* backward-Euler sub-steps per dt (>=1) */
+    fv_arrhenius chem_forward;  /* A_B_2C: the reaction; CL2: dissociation (#A_forw #n_forw #E_forw) */
+    fv_arrhenius chem_backward; /* CL2: recombination (#A_backw #n_backw #E_backw) */
+    double chem_q;            /* A_B_2C: heat release per mol of reaction (J/mol, > 0 exothermic) */
+    int chem_solver;          /* fv_chem_solver */
+    int chem_max_iter;        /* #Number_of_chemical_solver_iterations */
 } fv_config;
 
 /* Field indices of fv_download / fv_upload arrays (n_cells doubles each, x fastest).
@@ -211,7 +229,7 @@ long long fv_kernels_per_step(const fv_handle* h);
  *                          (unclamped); cfg->g is the gravity vector of this step
  *   stream                 cudaStream_t or NULL
  * Runs the full MUSCL-Hancock path (any limiter, 1D/2D/3D) on meshes of at most
- * FV_NOALLOC_MAX_CELLS cells; larger meshes are rejected with FV_ERR_INIT.  The first call on a
+ * FV_NOALLOC_MAX_CELLS cells; larger meshes and cases with chemistry are rejected with FV_ERR_INIT.  The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress) and should come before any
  * stream capture.  Every call rewrites each part of the array it reads, so no state carries over
  * between calls; calls that overlap on the GPU share the array and race.  Synchronises `stream`

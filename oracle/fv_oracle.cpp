@@ -19,6 +19,9 @@
  *   EOS                    src/thermodynamics/mixtureIdeal.cpp, idealFluid.cpp:13-60,
  *                          mixtureVanDerWaals.cpp:19-58,88-146,309-397, vanDerWaalsFluid.cpp:14-75
  *   boundary values        headers/boundaryConditionValue.hpp:34-515, src/boundary/slipFunction.cpp
+ *   chemistry              headers/abstractChemicalKinetics.hpp:25-620,
+ *                          src/chemicalReactions/chemicalKineticsChlorumDissociation.cpp:47-353,
+ *                          chemicalKineticsH2Cl2Combustion.cpp:362-389, templates/bunchOfFields.hpp:166-204
  * The operation order of every floating-point expression follows the reference so that the
  * restatement reproduces the reference binary to round-off.  Periodic patches and the
  * A+B->2C chemistry have no reference counterpart; they follow the same conventions.
@@ -267,6 +270,9 @@ struct fvo_case {
     std::vector<double> E, Uv, p;
     double time = 0, dt = 0;
     V3 g{};
+    // chemistry sub-cycling: carried from cell to cell in cell order like the reference's serial
+    // loop (1), or per cell (0)
+    int chemCarry = 1;
     std::string err;
 };
 
@@ -979,6 +985,353 @@ int doStep(fvo_case& cs, double dt) {
     return FV_OK;
 }
 
+// ---------------------------------------------------------------- chemistry
+// Per-cell backward-Euler kinetics in mass fractions: headers/abstractChemicalKinetics.hpp
+// (solvers :110-606, tolerances :30-32), the Cl2 mechanism
+// src/chemicalReactions/chemicalKineticsChlorumDissociation.cpp:47-70 (matrix), :128-150 (rates),
+// :152-273 (integration), :327-353 (two integrations + average), the heat release of
+// chemicalKineticsH2Cl2Combustion.cpp:362-389, and bunchOfFields::average
+// (templates/bunchOfFields.hpp:166-204).  A+B->2C is new (no reference counterpart) and uses
+// the same integrator.
+
+constexpr double kChemTol = 100 * 1E-12;  // convergenceTolerance = 100 * convergenceToleranceGlobal
+constexpr double kMassFracTol = 1E-2;     // massFracTolerance
+
+// Sparse per-cell system in the reference's layout: diagonal, per row the left (j < i) and right
+// (j > i) entries in list order, free term.
+struct ChemSystem {
+    int N = 0;
+    double D[FV_MAX_SPECIES] = {};
+    double A[FV_MAX_SPECIES][FV_MAX_SPECIES] = {};
+    int nl[FV_MAX_SPECIES] = {}, l[FV_MAX_SPECIES][FV_MAX_SPECIES] = {};
+    int nr[FV_MAX_SPECIES] = {}, r[FV_MAX_SPECIES][FV_MAX_SPECIES] = {};
+    double B[FV_MAX_SPECIES] = {};
+};
+
+// abstractChemicalKinetics::normalize: |x| < epsilon -> 0
+void chemNormalize(double* x, int N) {
+    for (int i = 0; i < N; ++i)
+        if (std::abs(x[i]) < std::numeric_limits<double>::epsilon()) x[i] = 0;
+}
+
+// matrixDotProduct (:73-104)
+void chemDot(const ChemSystem& m, const double* v, double* out) {
+    for (int i = 0; i < m.N; ++i) {
+        double s = m.D[i] * v[i];
+        for (int q = 0; q < m.nl[i]; ++q) s += m.A[i][m.l[i][q]] * v[m.l[i][q]];
+        for (int q = 0; q < m.nr[i]; ++q) s += m.A[i][m.r[i][q]] * v[m.r[i][q]];
+        out[i] = s;
+    }
+}
+
+double chemRelDiff(const double* nw, const double* old, int N) {
+    double mx = 0;
+    for (int i = 0; i < N; ++i) {
+        const double d = std::abs((nw[i] - old[i]) / (std::abs(nw[i]) + kStab));
+        if (i == 0 || d > mx) mx = d;
+    }
+    return 100. * mx;
+}
+
+double chemSum(const double* a, int N) {
+    double s = 0;
+    for (int i = 0; i < N; ++i) s += a[i];
+    return s;
+}
+
+// solveGS (:201-306): symmetric sweeps; false when it does not converge in maxIter iterations
+bool chemSolveGS(const ChemSystem& m, const double* init, int maxIter, double* out) {
+    const int N = m.N;
+    double old[FV_MAX_SPECIES] = {}, nw[FV_MAX_SPECIES] = {};
+    for (int i = 0; i < N; ++i) old[i] = nw[i] = init[i];
+    int it = 0;
+    while (true) {
+        ++it;
+        for (int i = 0; i < N; ++i) {
+            const double aii = 1. / m.D[i];
+            nw[i] = m.B[i] * aii;
+            for (int q = 0; q < m.nl[i]; ++q) nw[i] -= m.A[i][m.l[i][q]] * nw[m.l[i][q]] * aii;
+            for (int q = 0; q < m.nr[i]; ++q) nw[i] -= m.A[i][m.r[i][q]] * old[m.r[i][q]] * aii;
+        }
+        for (int i = N - 1; i >= 0; --i) {
+            const double aii = 1. / m.D[i];
+            nw[i] = m.B[i] * aii;
+            for (int q = m.nl[i] - 1; q >= 0; --q) nw[i] -= m.A[i][m.l[i][q]] * old[m.l[i][q]] * aii;
+            for (int q = m.nr[i] - 1; q >= 0; --q) nw[i] -= m.A[i][m.r[i][q]] * nw[m.r[i][q]] * aii;
+        }
+        if (chemRelDiff(nw, old, N) < kChemTol) {
+            chemNormalize(nw, N);
+            for (int i = 0; i < N; ++i) out[i] = nw[i];
+            return true;
+        }
+        if (it >= maxIter) return false;
+        for (int i = 0; i < N; ++i) old[i] = nw[i];
+    }
+}
+
+// solveJ (:110-199)
+bool chemSolveJ(const ChemSystem& m, const double* init, int maxIter, double* out) {
+    const int N = m.N;
+    double old[FV_MAX_SPECIES] = {}, nw[FV_MAX_SPECIES] = {};
+    for (int i = 0; i < N; ++i) old[i] = nw[i] = init[i];
+    int it = 0;
+    while (true) {
+        ++it;
+        for (int i = 0; i < N; ++i) {
+            const double aii = 1. / m.D[i];
+            double rs = 0;
+            for (int q = 0; q < m.nl[i]; ++q) rs -= m.A[i][m.l[i][q]] * old[m.l[i][q]];
+            for (int q = 0; q < m.nr[i]; ++q) rs -= m.A[i][m.r[i][q]] * old[m.r[i][q]];
+            nw[i] = (m.B[i] + rs) * aii;
+        }
+        for (int i = N - 1; i >= 0; --i) {
+            const double aii = 1. / m.D[i];
+            double rs = 0;
+            for (int q = m.nl[i] - 1; q >= 0; --q) rs -= m.A[i][m.l[i][q]] * old[m.l[i][q]];
+            for (int q = m.nr[i] - 1; q >= 0; --q) rs -= m.A[i][m.r[i][q]] * old[m.r[i][q]];
+            nw[i] = (m.B[i] + rs) * aii;
+        }
+        if (chemRelDiff(nw, old, N) < kChemTol) {
+            chemNormalize(nw, N);
+            for (int i = 0; i < N; ++i) out[i] = nw[i];
+            return true;
+        }
+        if (it >= maxIter) return false;
+        for (int i = 0; i < N; ++i) old[i] = nw[i];
+    }
+}
+
+// solveCG (:308-389) and solveJCG (:391-495); jacobi selects the preconditioned form
+bool chemSolveCG(const ChemSystem& m, const double* init, int maxIter, bool jacobi, double* out) {
+    const int N = m.N;
+    double x[FV_MAX_SPECIES] = {}, r[FV_MAX_SPECIES] = {}, d[FV_MAX_SPECIES] = {}, Ad[FV_MAX_SPECIES] = {},
+           P[FV_MAX_SPECIES] = {};
+    for (int i = 0; i < N; ++i) {
+        x[i] = init[i];
+        P[i] = 1. / m.D[i];
+    }
+    chemDot(m, x, Ad);
+    for (int i = 0; i < N; ++i) r[i] = m.B[i] - Ad[i];
+    for (int i = 0; i < N; ++i) d[i] = jacobi ? P[i] * r[i] : r[i];
+    int it = 0;
+    while (true) {
+        ++it;
+        double diff = 0;
+        for (int i = 0; i < N; ++i)
+            if (i == 0 || std::abs(r[i]) > diff) diff = std::abs(r[i]);
+        if (diff < kChemTol && it > 1) {
+            chemNormalize(x, N);
+            for (int i = 0; i < N; ++i) out[i] = x[i];
+            return true;
+        }
+        if (it >= maxIter) return false;
+        double t[FV_MAX_SPECIES] = {};
+        chemDot(m, d, Ad);
+        for (int i = 0; i < N; ++i) t[i] = jacobi ? r[i] * (P[i] * r[i]) : r[i] * r[i];
+        const double rr = chemSum(t, N);
+        for (int i = 0; i < N; ++i) t[i] = d[i] * Ad[i];
+        const double alpha = rr / (chemSum(t, N) + kStab);
+        for (int i = 0; i < N; ++i) x[i] += alpha * d[i];
+        double r1[FV_MAX_SPECIES] = {};
+        for (int i = 0; i < N; ++i) r1[i] = r[i] - alpha * Ad[i];
+        for (int i = 0; i < N; ++i) t[i] = jacobi ? r1[i] * (P[i] * r1[i]) : r1[i] * r1[i];
+        const double rr1 = chemSum(t, N);
+        const double beta = rr1 / (rr + kStab);
+        for (int i = 0; i < N; ++i) d[i] = (jacobi ? P[i] * r1[i] : r1[i]) + beta * d[i];
+        for (int i = 0; i < N; ++i) r[i] = r1[i];
+    }
+}
+
+// solveGE (:497-604): row pivoting on the raw value, then elimination and back substitution
+bool chemSolveGE(const ChemSystem& m, double* out) {
+    const int N = m.N;
+    double A[FV_MAX_SPECIES][FV_MAX_SPECIES] = {}, b[FV_MAX_SPECIES] = {};
+    for (int i = 0; i < N; ++i) {
+        A[i][i] = m.D[i];
+        for (int q = 0; q < m.nl[i]; ++q) A[i][m.l[i][q]] = m.A[i][m.l[i][q]];
+        for (int q = 0; q < m.nr[i]; ++q) A[i][m.r[i][q]] = m.A[i][m.r[i][q]];
+        b[i] = m.B[i];
+    }
+    for (int k = 0; k < N - 1; ++k) {
+        double mv = A[k][k];
+        int c = k;
+        for (int q = k + 1; q < N; ++q)
+            if (A[q][k] > mv) { mv = A[q][k]; c = q; }
+        if (c != k) {
+            for (int j = 0; j < N; ++j) std::swap(A[c][j], A[k][j]);
+            std::swap(b[c], b[k]);
+        }
+    }
+    for (int k = 0; k < N - 1; ++k)
+        for (int i = k + 1; i < N; ++i) {
+            const double ratio = A[i][k] / (A[k][k] + kStab);
+            for (int j = k + 1; j < N; ++j) A[i][j] = A[i][j] - ratio * A[k][j];
+            b[i] = b[i] - ratio * b[k];
+        }
+    double phi[FV_MAX_SPECIES] = {};
+    phi[N - 1] = b[N - 1] / (A[N - 1][N - 1] + kStab);
+    for (int i = N - 2; i >= 0; --i) {
+        double term = 0.0;
+        for (int j = i + 1; j < N; ++j) term += A[i][j] * phi[j];
+        phi[i] = (b[i] - term) / (A[i][i] + kStab);
+    }
+    chemNormalize(phi, N);
+    for (int i = 0; i < N; ++i) out[i] = phi[i];
+    return true;
+}
+
+bool chemSolve(const fv_config& cf, const ChemSystem& m, const double* init, double* out) {
+    switch (cf.chem_solver) {
+    case FV_CHEM_JACOBI: return chemSolveJ(m, init, cf.chem_max_iter, out);
+    case FV_CHEM_GAUSS_ELIMINATION: return chemSolveGE(m, out);
+    case FV_CHEM_CONJUGATE_GRADIENT: return chemSolveCG(m, init, cf.chem_max_iter, false, out);
+    case FV_CHEM_JACOBI_CONJUGATE_GRADIENT: return chemSolveCG(m, init, cf.chem_max_iter, true, out);
+    default: return chemSolveGS(m, init, cf.chem_max_iter, out);
+    }
+}
+
+// k = A T^n exp(-E / (R T)) (chemicalKineticsChlorumDissociation.cpp:133-137)
+double arrhenius(const fv_arrhenius& k, double T, double R) { return k.A * std::pow(T, k.n) * std::exp(-k.E / (R * T)); }
+
+// Mechanism matrix of one sub-step in mass fractions, with the concentrations c[0..N] of the
+// sub-step's start, the cell's temperature of the integration T and mixture density rho.
+void chemSystem(const fv_config& cf, const Mix& mx, double dt, double T, const double* c, double rho,
+                ChemSystem& m) {
+    m = ChemSystem();
+    m.N = mx.N;
+    if (cf.chemistry == FV_CHEM_CL2) {
+        // setMatrix (chemicalKineticsChlorumDissociation.cpp:47-70)
+        const double kd = arrhenius(cf.chem_forward, T, mx.R), kr = arrhenius(cf.chem_backward, T, mx.R);
+        const double Cl2 = c[1], Cl = c[2], M0 = c[0];
+        m.D[0] = (1 / dt + kd * M0) / mx.M[0];
+        m.A[0][1] = (-kr * Cl * M0) / mx.M[1];
+        m.B[0] = Cl2 / (rho * dt);
+        m.A[1][0] = (-2 * kd * M0) / mx.M[0];
+        m.D[1] = (1 / dt + 2 * kr * Cl * M0) / mx.M[1];
+        m.B[1] = Cl / (rho * dt);
+        m.nr[0] = 1; m.r[0][0] = 1;
+        m.nl[1] = 1; m.l[1][0] = 0;
+    } else {
+        // A + B -> 2C: rate k c_A c_B linearised as k c_B^old c_A^new (A) and k c_A^old c_B^new (B);
+        // C is produced by the mass of both, so the system conserves mass for any molar masses
+        const double k = arrhenius(cf.chem_forward, T, mx.R);
+        const double cA = c[1], cB = c[2], cC = c[3];
+        m.D[0] = (1 / dt + k * cB) / mx.M[0];
+        m.B[0] = cA / (rho * dt);
+        m.D[1] = (1 / dt + k * cA) / mx.M[1];
+        m.B[1] = cB / (rho * dt);
+        m.A[2][0] = (-k * cB) / mx.M[2];
+        m.A[2][1] = (-k * cA) / mx.M[2];
+        m.D[2] = (1 / dt) / mx.M[2];
+        m.B[2] = cC / (rho * dt);
+        m.nl[2] = 2; m.l[2][0] = 0; m.l[2][1] = 1;
+    }
+}
+
+struct ChemCell {
+    double Uv, T;
+    double c[FV_MAX_SPECIES + 1];
+    double dens[FV_MAX_SPECIES];
+};
+
+// timeStepIntegration for one cell (chemicalKineticsChlorumDissociation.cpp:152-273).  subIt is the
+// sub-step count, carried from cell to cell like the reference's serial loop.  Returns FV_OK or
+// the error of an exhausted sub-cycling.
+int chemIntegrate(const fv_config& cf, const Mix& mx, double dt, double rho, ChemCell& cell, long long& subIt) {
+    const int N = mx.N;
+    const ChemCell oldV = cell;
+    const double Tcell = oldV.T;
+    double subDt = dt / subIt;
+    ChemCell nv = oldV;
+    while (true) {
+        bool ok = true;
+        nv = oldV;
+        for (long long st = 0; st < subIt && ok; ++st) {
+            double wOld[FV_MAX_SPECIES] = {};
+            for (int k = 0; k < N; ++k) wOld[k] = nv.dens[k] / rho;
+            double sumOld = 0.;
+            for (int k = 0; k < N; ++k) sumOld = sumOld + wOld[k];
+            if (sumOld == 0.0) continue;
+            ChemSystem m;
+            chemSystem(cf, mx, subDt, Tcell, nv.c, rho, m);
+            double w[FV_MAX_SPECIES] = {};
+            if (!chemSolve(cf, m, wOld, w)) { ok = false; break; }
+            for (int k = 0; k < N; ++k) w[k] = std::max(0., w[k]);
+            double sumNew = 0.;
+            for (int k = 0; k < N; ++k) sumNew = sumNew + w[k];
+            if (std::abs(sumNew - sumOld) > kMassFracTol) { ok = false; break; }
+            for (int k = 0; k < N; ++k) {
+                w[k] /= sumNew;
+                w[k] *= sumOld;
+            }
+            double deltaU = 0;
+            if (cf.chemistry == FV_CHEM_A_B_2C) {
+                // heat release per mol of C formed: (q - dCv (T - 298.15)) / 2 (the form of
+                // chemicalKineticsH2Cl2Combustion.cpp:362-389 for a reaction forming 2 C)
+                const double deltaC = w[2] * rho / mx.M[2] - nv.c[3];
+                const double deltaCv = 2 * mx.Cv[2] - mx.Cv[0] - mx.Cv[1];
+                deltaU = (cf.chem_q - deltaCv * (Tcell - 298.15)) * 0.5 * deltaC;
+            }
+            for (int k = 0; k < N; ++k) nv.c[k + 1] = w[k] * rho / mx.M[k];
+            nv.c[0] = 0;
+            for (int k = 1; k <= N; ++k) nv.c[0] += nv.c[k];
+            nv.Uv += deltaU;
+            nv.T = mx.TFromUv(nv.c, nv.Uv);
+            if (nv.T < 0) { ok = false; break; }
+            for (int k = 0; k < N; ++k) nv.dens[k] = nv.c[k + 1] * mx.M[k];
+        }
+        if (ok) break;
+        subIt *= 10;
+        subDt = dt / subIt;
+        if (subDt < cf.min_timestep) return FV_ERR_SYSTEM;
+    }
+    cell = nv;
+    return FV_OK;
+}
+
+// solveChemicalKinetics (chemicalKineticsChlorumDissociation.cpp:327-353) over all cells.
+int chemistryStep(fvo_case& cs, double dt) {
+    const Mix& mx = cs.mix;
+    const int N = mx.N;
+    const long long nc = cs.nCells;
+    std::vector<ChemCell> cells(nc);
+    for (long long i = 0; i < nc; ++i) {
+        ChemCell& q = cells[i];
+        for (int k = 0; k <= N; ++k) q.c[k] = cs.c[k][i];
+        for (int k = 0; k < N; ++k) q.dens[k] = cs.rho[k + 1][i];
+        q.Uv = cs.Uv[i];
+        q.T = mx.TFromUv(q.c, q.Uv);
+    }
+    for (int pass = 0; pass < 2; ++pass) {
+        long long subIt = 1;
+        for (long long i = 0; i < nc; ++i) {
+            if (!cs.chemCarry) subIt = 1;  // per-cell sub-cycling (the CUDA path's behaviour)
+            const int st = chemIntegrate(cs.cfg, mx, dt, cs.rho[0][i], cells[i], subIt);
+            if (st != FV_OK) {
+                cs.err = "Timestep become too small.";
+                return st;
+            }
+        }
+    }
+    for (long long i = 0; i < nc; ++i) {
+        const ChemCell& q = cells[i];
+        const double v2 = vdot(cs.v[i], cs.v[i]);
+        const double E1 = q.Uv + cs.rho[0][i] * v2 * 0.5 + 0.0;
+        // bunchOfFields::average(phaseN1, 0.5)
+        for (int k = 0; k <= N; ++k) cs.c[k][i] = 0.5 * cs.c[k][i] + 0.5 * q.c[k];
+        for (int k = 1; k <= N; ++k) cs.rho[k][i] = 0.5 * cs.rho[k][i] + 0.5 * q.dens[k - 1];
+        cs.rho[0][i] = 0.5 * cs.rho[0][i] + 0.5 * cs.rho[0][i];
+        cs.m[i] = vadd(vmul(cs.m[i], 0.5), vmul(cs.m[i], 0.5));
+        cs.E[i] = 0.5 * cs.E[i] + 0.5 * E1;
+        cs.v[i] = vdiv(cs.m[i], cs.rho[0][i]);
+        cs.Uv[i] = cs.E[i] - 0.0 - 0.5 * cs.rho[0][i] * vdot(cs.v[i], cs.v[i]);
+        double cc[FV_MAX_SPECIES + 1];
+        for (int k = 0; k <= N; ++k) cc[k] = cs.c[k][i];
+        cs.p[i] = mx.pFromUv(cc, cs.Uv[i]);
+    }
+    return FV_OK;
+}
+
 // main's CFL block (Schemi.cpp:807-833)
 double cflTimestep(const fvo_case& cs) {
     double maxS = -std::numeric_limits<double>::infinity();
@@ -1004,6 +1357,9 @@ bool validate(const fv_config& cf, std::string& err) {
     if (cf.eos != FV_EOS_IDEAL && cf.eos != FV_EOS_VAN_DER_WAALS) { err = "unknown equation of state"; return false; }
     if (cf.flux != FV_FLUX_HLLC && cf.flux != FV_FLUX_HLL) { err = "unknown flux solver"; return false; }
     if (cf.limiter < 0 || cf.limiter > FV_LIM_SCHMIDTMANN) { err = "unknown limiter"; return false; }
+    if (cf.chemistry == FV_CHEM_CL2 && cf.n_species != 2) { err = "Cl2 dissociation needs 2 species"; return false; }
+    if (cf.chemistry == FV_CHEM_A_B_2C && cf.n_species != 3) { err = "A+B->2C needs 3 species"; return false; }
+    if (cf.chemistry < FV_CHEM_NONE || cf.chemistry > FV_CHEM_CL2) { err = "unknown chemistry"; return false; }
     return true;
 }
 
@@ -1061,6 +1417,12 @@ void fvo_destroy(fvo_case* c) { delete c; }
 
 long long fvo_n_cells(const fvo_case* c) { return c ? c->nCells : 0; }
 
+int fvo_set_chem_carry(fvo_case* c, int carry) {
+    if (!c) return FV_ERR_INIT;
+    c->chemCarry = carry ? 1 : 0;
+    return FV_OK;
+}
+
 int fvo_upload(fvo_case* cs, const double* const* prim) {
     const int NS = cs->N;
     const Mix& mx = cs->mix;
@@ -1091,8 +1453,13 @@ int fvo_upload(fvo_case* cs, const double* const* prim) {
 
 int fvo_step(fvo_case* cs, double* dt_used, double* dt_next) {
     const double dt = cs->dt;
-    const int st = doStep(*cs, dt);
+    int st = doStep(*cs, dt);
     if (st != FV_OK) return st;
+    if (cs->cfg.chemistry != FV_CHEM_NONE) {
+        // secondOrderStepSolver::calculateStep: chemistry after the advection, same dt
+        st = chemistryStep(*cs, dt);
+        if (st != FV_OK) return st;
+    }
     if (cs->cfg.gravity) {
         cs->g = vadd(cs->g, vmul(v3(cs->cfg.g_delta[0], cs->cfg.g_delta[1], cs->cfg.g_delta[2]), dt));
     }

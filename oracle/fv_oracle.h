@@ -40,6 +40,11 @@ int fvo_set_conserved(fvo_case* c, const double* const* in);
 
 long long fvo_n_cells(const fvo_case* c);
 
+/* Chemistry sub-cycling after a failed cell: carry = 1 (default) keeps the finer sub-step for the
+ * cells that follow in cell order, as the reference's serial loop does; carry = 0 sub-cycles each
+ * cell on its own, as the CUDA path does. */
+int fvo_set_chem_carry(fvo_case* c, int carry);
+
 #ifdef __cplusplus
 }
 #endif

@@ -58,6 +58,7 @@ def load():
         lib.fvo_get_conserved.argtypes = [P, ctypes.POINTER(DP)]
         lib.fvo_set_conserved.argtypes = [P, ctypes.POINTER(DP)]
         lib.fvo_n_cells.restype = ctypes.c_longlong
+        lib.fvo_set_chem_carry.argtypes = [P, ctypes.c_int]
         lib.fvo_n_cells.argtypes = [P]
         _lib = lib
     return _lib
@@ -136,6 +137,10 @@ class OracleCase:
     def set_conserved(self, fields: Sequence[np.ndarray]) -> None:
         arrs = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in fields]
         _check(load().fvo_set_conserved(self._h, _ptrs(arrs)))
+
+    def set_chem_carry(self, carry: bool) -> None:
+        """Chemistry sub-cycling carried on to the following cells (the reference) or per cell."""
+        _check(load().fvo_set_chem_carry(self._h, int(bool(carry))))
 
 
 def _check(st: int) -> None:

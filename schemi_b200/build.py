@@ -9,6 +9,7 @@ Translation units (compiled in parallel):
   csrc/fv_capi.cu       C-ABI, upload/download/finalize kernels, device time loop (--fmad=false)
   csrc/fv_batch.cu      batched ensemble (--fmad=false)
   csrc/fv_noalloc.cu    the step without device allocation (--fmad=false)
+  csrc/fv_chem.cu       chemistry pass (Cl2, A+B->2C), FP64 (--fmad=false)
   csrc/fv_adjoint.cu    recorded trajectories, checkpoints and the adjoint sweep
   csrc/fv_adjoint_f64.cu / fv_adjoint_f32.cu  adjoint step kernels per arithmetic
 nvcc cross-compiles for sm_100a without a GPU.
@@ -34,6 +35,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 UNITS = {
     "fv_capi.cu": ["--fmad=false"],
     "fv_dispatch.cu": [],
+    "fv_chem.cu": ["--fmad=false"],
     "fv_adjoint.cu": [],
     "fv_adjoint_f64.cu": [],
     "fv_adjoint_f32.cu": ["-use_fast_math"],

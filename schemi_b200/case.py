@@ -31,13 +31,22 @@ LIMITERS = ["zero", "minmod", "vanLeer", "linear", "vanAlbada", "HQUICK", "vanLe
 LIMITER = {name: i for i, name in enumerate(LIMITERS)}
 BC_TYPES = {"freeBoundary": 1, "slip": 2, "fixedValueCell": 3, "fixedValueSurface": 4, "periodic": 100}
 PRECISION = {"f64": 0, "f32flux": 1}
-CHEMISTRY = {"no": 0, "A+B->2C": 1}
+CHEMISTRY = {"no": 0, "A+B->2C": 1, "Cl2": 2}
+# set/chemicalKinetics.txt #Iterative_solver names (abstractChemicalKinetics.cpp:21-29)
+CHEM_SOLVERS = {"Gauss-Seidel": 0, "Jacobi": 1, "GaussElimination": 2, "conjugateGradient": 3,
+                "JacobiConjugateGradient": 4}
 
 # patch order of the task files: #Tail, #Point, #Bottom, #Right, #Left, #Top
 PATCHES = ["tail", "point", "bottom", "right", "left", "top"]
 # which patches a task of dimension D uses (the others are "blank" in the task files)
 PATCHES_USED = {1: ["tail", "point"], 2: ["tail", "point", "right", "left"],
                 3: ["tail", "point", "bottom", "right", "left", "top"]}
+
+
+class fv_arrhenius_t(ctypes.Structure):
+    """Mirror of ``fv_arrhenius``: k = A T^n exp(-E / (R T))."""
+
+    _fields_ = [("A", ctypes.c_double), ("n", ctypes.c_double), ("E", ctypes.c_double)]
 
 
 class fv_config_t(ctypes.Structure):
@@ -70,10 +79,11 @@ class fv_config_t(ctypes.Structure):
         ("bc_p", ctypes.c_int * 6),
         ("bc_p_value", ctypes.c_double * 6),
         ("chemistry", ctypes.c_int),
-        ("chem_A", ctypes.c_double),
-        ("chem_Ea_R", ctypes.c_double),
+        ("chem_forward", fv_arrhenius_t),
+        ("chem_backward", fv_arrhenius_t),
         ("chem_q", ctypes.c_double),
-        ("chem_substeps", ctypes.c_int),
+        ("chem_solver", ctypes.c_int),
+        ("chem_max_iter", ctypes.c_int),
     ]
 
 
@@ -134,10 +144,11 @@ class Case:
     bc: Dict[str, PatchBC] = field(default_factory=dict)
     precision: str = "f64"
     chemistry: str = "no"
-    chem_A: float = 0.0
-    chem_Ea_R: float = 0.0
+    chem_forward: Tuple[float, float, float] = (0.0, 0.0, 0.0)   # Arrhenius A, n, E (J/mol)
+    chem_backward: Tuple[float, float, float] = (0.0, 0.0, 0.0)
     chem_q: float = 0.0
-    chem_substeps: int = 1
+    chem_solver: str = "Gauss-Seidel"
+    chem_max_iter: int = 200
     name: str = "case"
 
     def __post_init__(self):
@@ -177,7 +188,7 @@ class Case:
 
     def expressible_in_reference(self) -> bool:
         """The reference has no periodic patch and no A+B->2C mechanism."""
-        return not self.periodic_axes() and self.chemistry == "no"
+        return not self.periodic_axes() and self.chemistry in ("no", "Cl2")
 
     def fv_config(self) -> fv_config_t:
         c = fv_config_t()
@@ -217,8 +228,11 @@ class Case:
             c.bc_p[pi] = BC_TYPES[pb.p.kind]
             c.bc_p_value[pi] = float(pb.p.value) if pb.p.kind.startswith("fixed") else 0.0
         c.chemistry = CHEMISTRY[self.chemistry]
-        c.chem_A, c.chem_Ea_R, c.chem_q = self.chem_A, self.chem_Ea_R, self.chem_q
-        c.chem_substeps = self.chem_substeps
+        c.chem_forward.A, c.chem_forward.n, c.chem_forward.E = self.chem_forward
+        c.chem_backward.A, c.chem_backward.n, c.chem_backward.E = self.chem_backward
+        c.chem_q = self.chem_q
+        c.chem_solver = CHEM_SOLVERS[self.chem_solver]
+        c.chem_max_iter = self.chem_max_iter
         return c
 
 

@@ -8,6 +8,7 @@ for tests (cells per axis divided by ``scale``) while keeping the physics of the
   shock_tube_1d        1D two-species shock tube, 1000 cells, HLLC + minmod, CFL 0.5, t = 0.2
   kelvin_helmholtz_2d  2D mixing layer 1024^2, periodic x / slip y, HLLC + vanLeer, t = 1
   reacting_shear_3d    3D reacting shear layer 256^3, vdW EOS, A+B->2C, periodic x and z
+  chlorine_dissociation_2d  hot Cl2/Cl mixture with the reference's Cl2 mechanism (chemistry pin)
   richtmyer_meshkov    one 2D shock-tube case of the 512-case ensemble (sizes 128^2..512^2)
   rayleigh_taylor_2d   2D RT 512x1536 with gravity and a 64-mode interface perturbation
 """
@@ -147,6 +148,43 @@ def rt_fields(nx: int, ny: int, a: np.ndarray) -> list:
     return [cA.ravel(), cB.ravel(), z.ravel(), z.ravel(), z.ravel(), p.ravel()]
 
 
+def chlorine_dissociation_2d(n: int = 4, T0: float = 1500.0, p0: float = 1e5, seed: int = 2030,
+                             eos: str = "vanDerWaals", precision: str = "f64",
+                             solver: str = "Gauss-Seidel") -> Tuple[Case, list]:
+    """Hot Cl2 / Cl mixture on [0,1]^2 m (SI) with the species, Arrhenius parameters and solver of
+    the reference's ClorumTest deck (tests/Chemical Reactions/ClorumTest/Chlorum/set: Cl2 M=0.0709,
+    Cv=25.635, Tc=416.9 K, Pc=7.9773e6 Pa; Cl M=0.03545, Cv=12.471; dissociation A=5.74e9, n=0,
+    E=232613.66 J/mol; recombination A=2.3e7, n=-1.5, E=0; Gauss-Seidel, 200 iterations), slip
+    walls, at rest, with seeded cell-to-cell variations of temperature (T0 +- 10%) and of the
+    Cl fraction (0..20%) so that every cell reacts at its own rate."""
+    from .case import R_SI
+
+    R = R_SI
+    sp = [Species(M=0.0709, Cv=25.635, Tc=416.9, Pc=7.9773e6), Species(M=0.03545, Cv=12.471, Tc=0.0, Pc=1.0)]
+    bc = {p: PatchBC.uniform("slip", 2) for p in ("tail", "point", "right", "left")}
+    case = Case(dims=2, n=(n, n, 1), L=(1.0, 1.0, 1.0), species=sp, t_end=1.0, R_units="SI", eos=eos,
+                limiter="vanAlbada", flux="HLLC", courant=0.47, bc=bc, precision=precision, chemistry="Cl2",
+                chem_forward=(5.74e9, 0.0, 232613.66), chem_backward=(2.3e7, -1.5, 0.0), chem_solver=solver,
+                chem_max_iter=200, name="chlorine_dissociation_2d")
+    rng = np.random.default_rng(seed)
+    T = T0 * (1 + 0.1 * rng.uniform(-1, 1, size=n * n))
+    xCl = 0.2 * rng.uniform(0, 1, size=n * n)
+    # total concentration from p0 at T (vdW with mole-fraction mixing of a and b)
+    a = np.array([27 * R * R * s.Tc ** 2 / (64 * s.Pc) for s in sp])
+    b = np.array([R * s.Tc / (8 * s.Pc) for s in sp])
+    X = np.stack([1 - xCl, xCl])
+    am = sum(X[k] * X[l] * np.sqrt(a[k] * a[l]) for k in range(2) for l in range(2))
+    bm = sum(X[k] * X[l] * 0.5 * (b[k] + b[l]) for k in range(2) for l in range(2))
+    c = p0 / (R * T)
+    if eos == "vanDerWaals":
+        for _ in range(50):
+            f = R * T * c / (1 - c * bm) - am * c * c - p0
+            df = R * T / (1 - c * bm) ** 2 - 2 * am * c
+            c = c - f / df
+    z = np.zeros(n * n)
+    return case, [c * X[0], c * X[1], z, z, z, np.full(n * n, p0)]
+
+
 def reacting_shear_3d(n: int = 256, seed: int = 2027, precision: str = "f32flux", t_end: float = 1e-3,
                       periodic: bool = True) -> Tuple[Case, list]:
     """3D reacting shear layer on [0,1]^3 m (SI units): species A, B, C with M = 0.029 kg/mol,
@@ -169,7 +207,7 @@ def reacting_shear_3d(n: int = 256, seed: int = 2027, precision: str = "f32flux"
           "right": PatchBC.uniform("slip", 3), "left": PatchBC.uniform("slip", 3)}
     case = Case(dims=3, n=(n, n, n), L=(1.0, 1.0, 1.0), species=sp, t_end=t_end, R_units="SI",
                 eos="vanDerWaals", limiter="vanLeer", flux="HLLC", courant=0.5, bc=bc, precision=precision,
-                chemistry="A+B->2C", chem_A=1e9, chem_Ea_R=8000.0, chem_q=2e6 * 0.058, chem_substeps=1,
+                chemistry="A+B->2C", chem_forward=(1e9, 0.0, 8000.0 * R), chem_q=2e6 * 0.058,
                 name="reacting_shear_3d")
     rng = np.random.default_rng(seed)
     yc = _centres(n, 1.0)[None, :, None] * np.ones((n, n, n))

@@ -181,8 +181,19 @@ bool validate(const fv_config& c, std::string& e) {
         }
         if (per && c.n[a] < 2) { e = "a periodic axis needs at least 2 cells"; return false; }
     }
-    if (c.chemistry != FV_CHEM_NONE && c.chemistry != FV_CHEM_A_B_2C) { e = "unknown chemistry"; return false; }
-    if (c.chemistry == FV_CHEM_A_B_2C && c.n_species < 3) { e = "A+B->2C needs 3 species"; return false; }
+    if (c.chemistry < FV_CHEM_NONE || c.chemistry > FV_CHEM_CL2) { e = "unknown chemistry"; return false; }
+    if (c.chemistry == FV_CHEM_A_B_2C && c.n_species != 3) { e = "A+B->2C needs 3 species (A, B, C)"; return false; }
+    if (c.chemistry == FV_CHEM_CL2 && c.n_species != 2) { e = "Cl2 dissociation needs 2 species (Cl2, Cl)"; return false; }
+    if (c.chemistry != FV_CHEM_NONE) {
+        if (c.chem_solver < FV_CHEM_GAUSS_SEIDEL || c.chem_solver > FV_CHEM_JACOBI_CONJUGATE_GRADIENT) {
+            e = "unknown chemical iterative solver";
+            return false;
+        }
+        if (c.chem_max_iter < 1 || c.chem_max_iter > 1000000) {
+            e = "chem_max_iter must be 1..1000000";
+            return false;
+        }
+    }
     return true;
 }
 
@@ -312,13 +323,22 @@ long long stepBlocks(fv_handle* h) {
     return h->path == PATH_MARCH ? marchBlocks(h->P, h->shape) : genericBlocks(h->P);
 }
 
-// enqueue step + finalize reading U[from]
+// enqueue step [+ chemistry] + finalize reading U[from]
 cudaError_t enqueueStep(fv_handle* h, int from) {
     const StepBuffers B = buffersFor(h, from);
     cudaError_t e = h->cfg.precision == FV_PREC_F64 ? launchStepF64(h->P, B, h->path, h->shape, h->stream)
                                                      : launchStepF32(h->P, B, h->path, h->shape, h->stream);
     if (e != cudaSuccess) return e;
-    k_finalize<<<1, 1024, 0, h->stream>>>(h->P, h->ck, h->blockMax, (int)stepBlocks(h));
+    int blocks = (int)stepBlocks(h);
+    if (h->cfg.chemistry != FV_CHEM_NONE) {
+        // secondOrderStepSolver::calculateStep: the chemistry of the advected state with the same
+        // dt; main's CFL block then reads the state after the chemistry
+        e = launchChemistry(h->cfg.n_species, h->cfg.eos, h->cfg.dims, h->P, h->chem, h->U[from ^ 1], h->ck,
+                            h->blockMax, h->stream);
+        if (e != cudaSuccess) return e;
+        blocks = chemistryBlocks(h->P);
+    }
+    k_finalize<<<1, 1024, 0, h->stream>>>(h->P, h->ck, h->blockMax, blocks);
     return cudaGetLastError();
 }
 
@@ -334,7 +354,8 @@ fv_status configureKernels(fv_handle* h) {
 }
 
 fv_status ensureScratch(fv_handle* h) {
-    const long long nb = std::max(marchBlocks(h->P, h->shape), genericBlocks(h->P));
+    long long nb = std::max(marchBlocks(h->P, h->shape), genericBlocks(h->P));
+    if (h->cfg.chemistry != FV_CHEM_NONE) nb = std::max<long long>(nb, chemistryBlocks(h->P));
     if (nb > h->blockMaxCap) {
         if (h->blockMax) cudaFree(h->blockMax);
         FV_CUDA(h, cudaMalloc(&h->blockMax, sizeof(double) * nb));
@@ -462,6 +483,16 @@ fv_status fv_create(const fv_config* cfg, fv_handle** out) {
     // rows are staged with 16-byte aligned bulk copies: field and row pitches must be even
     P.tma = (P.n[0] % 2 == 0) ? 1 : 0;
     h->path = choosePath(*cfg);
+    h->chem.mech = cfg->chemistry;
+    h->chem.solver = cfg->chem_solver;
+    h->chem.maxIter = cfg->chem_max_iter;
+    h->chem.Af = cfg->chem_forward.A;
+    h->chem.nf = cfg->chem_forward.n;
+    h->chem.Ef = cfg->chem_forward.E;
+    h->chem.Ab = cfg->chem_backward.A;
+    h->chem.nb = cfg->chem_backward.n;
+    h->chem.Eb = cfg->chem_backward.E;
+    h->chem.q = cfg->chem_q;
     h->shape = defaultShape(*cfg);
 
     // generic face layout
@@ -788,7 +819,7 @@ fv_status fv_check(fv_handle* h) {
 
 long long fv_kernels_per_step(const fv_handle* h) {
     if (!h) return 0;
-    return h->path == PATH_MARCH ? 2 : 5;
+    return (h->path == PATH_MARCH ? 2 : 5) + (h->cfg.chemistry != FV_CHEM_NONE ? 1 : 0);
 }
 
 // ---- introspection used by the tests and the bench (no reference counterpart)

@@ -6,6 +6,7 @@
 #include <string>
 
 #include "../../include/fvstep.h"
+#include "fv_chem_launch.h"
 #include "fv_launch.cuh"
 
 using namespace fv;
@@ -35,6 +36,7 @@ struct fv_handle {
     GenericLayout L{};
     double* outBuf = nullptr;      // download staging
     int path = PATH_GENERIC;
+    chem::ChemParams chem{};       // chemistry pass (cfg.chemistry != FV_CHEM_NONE)
     MarchShape shape{128, 1, 32};
     int nConserved = 0;
     // graphs of step chunks, one per start buffer

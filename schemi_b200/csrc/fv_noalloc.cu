@@ -193,6 +193,10 @@ bool buildParams(const fv_config& c, StepParams& P) {
 extern "C" fv_status fv_step_noalloc(const fv_config* cfg, const double* state_in, double* state_out, double dt,
                                      double* dt_next, void* stream) {
     if (!cfg || !state_in || !state_out) return FV_ERR_INIT;
+    if (cfg->chemistry != FV_CHEM_NONE) {
+        fprintf(stderr, "fv_step_noalloc: the step without device allocation has no chemistry pass\n");
+        return FV_ERR_INIT;
+    }
     StepParams P;
     if (!buildParams(*cfg, P)) {
         fprintf(stderr, "fv_step_noalloc: invalid configuration\n");

@@ -130,6 +130,23 @@ def _bc_block(case: Case, getter, vector: bool) -> str:
     return "\n".join(lines)
 
 
+def _chemistry_block(case: Case) -> str:
+    """set/chemicalKinetics.txt: the mechanism name, then the Arrhenius parameters, solver and
+    iteration count in the order ChlorumDissociation's constructor reads them
+    (chemicalKineticsChlorumDissociation.cpp:275-308)."""
+    if case.chemistry == "no":
+        return "#Type_of_chemical_reaction\nno"
+    if case.chemistry != "Cl2":
+        raise ValueError(f"the reference has no {case.chemistry} mechanism")
+    (af, nf, ef), (ab, nb, eb) = case.chem_forward, case.chem_backward
+    lines = ["#Type_of_chemical_reaction", "Cl2",
+             "#A_forw", _f(af), "#n_forw", _f(nf), "#E_forw", _f(ef),
+             "#A_backw", _f(ab), "#n_backw", _f(nb), "#E_backw", _f(eb),
+             "#Iterative_solver", case.chem_solver,
+             "#Number_of_chemical_solver_iterations", str(case.chem_max_iter)]
+    return "\n".join(lines)
+
+
 def write_deck(case: Case, directory: str, prim: Sequence[np.ndarray], frequency_of_output: int = 1,
                restart: bool = True) -> None:
     """Write ``directory/set`` and the restart point for the reference solver.
@@ -201,7 +218,7 @@ def write_deck(case: Case, directory: str, prim: Sequence[np.ndarray], frequency
     _write(sdir, "epsilon.txt", free + "\n#Values_in_zones\n0.0")
     _write(sdir, "a.txt", free + "\n#Values_in_zones\n0.0 0.0 0.0")
     _write(sdir, "b.txt", free + "\n#Values_in_zones\n0")
-    _write(sdir, "chemicalKinetics.txt", "#Type_of_chemical_reaction\nno")
+    _write(sdir, "chemicalKinetics.txt", _chemistry_block(case))
     _write(sdir, "transportCoefficients.txt", _TRANSPORT)
     _write(sdir, "turbulentParameters.txt", _TURB_PARAMS)
     _write(sdir, "turbPeak.txt", _TURB_PEAK)

@@ -23,7 +23,7 @@ from schemi_b200 import cases  # noqa: E402
 from schemi_b200.case import BC, Case, PatchBC  # noqa: E402
 import oracle as O  # noqa: E402
 
-FIELDS = {"c1": "concentration_1", "c2": "concentration_2", "c3": "concentration_3", "vx": "velocity_x",
+FIELDS = {"T": "temperature", "c1": "concentration_1", "c2": "concentration_2", "c3": "concentration_3", "vx": "velocity_x",
           "vy": "velocity_y", "vz": "velocity_z", "p": "pressure", "rho": "density", "E": "total_energy",
           "mx": "momentum_x", "my": "momentum_y"}
 
@@ -62,6 +62,14 @@ def golden_cases():
     c, p = cases.shock_tube_1d(n=200)
     c.flux, c.limiter = "HLL", "superbee"
     out.append(("tube_hll_superbee_200", c, p, 30, [30]))
+    # Cl2 <-> 2Cl chemistry (the ClorumTest mechanism and solver, hot mixture)
+    c, p = cases.chlorine_dissociation_2d(4)
+    out.append(("cl2_4x4_vdw_gs", c, p, 10, [1, 2, 10]))
+    c, p = cases.chlorine_dissociation_2d(4, eos="ideal")
+    out.append(("cl2_4x4_ideal_gs", c, p, 10, [1, 10]))
+    for solver, tag in (("Jacobi", "jacobi"), ("GaussElimination", "ge"), ("conjugateGradient", "cg")):
+        c, p = cases.chlorine_dissociation_2d(4, solver=solver)
+        out.append((f"cl2_4x4_vdw_{tag}", c, p, 6, [1, 6]))
     return out
 
 

@@ -14,7 +14,9 @@ pytestmark = pytest.mark.gpu
 
 FP64_TOL = 1e-12
 COMPARE = ["c1", "c2", "c3", "vx", "vy", "p", "rho", "E", "mx", "my"]
-CASES = load_cases()
+# the fixtures with chemistry are checked by test_gpu_chemistry.py (exp/pow round differently on
+# the GPU, and velocities that start from rest are compared on the flow's speed scale there)
+CASES = [c for c in load_cases() if c[1].chemistry == "no"]
 
 
 @pytest.fixture(scope="module")

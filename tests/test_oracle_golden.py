@@ -10,7 +10,7 @@ import pytest
 from golden_cases import golden_steps, load_cases, rel_err
 
 CASES = load_cases()
-COMPARE = ["c1", "c2", "c3", "vx", "vy", "p", "rho", "E", "mx", "my"]
+COMPARE = ["c1", "c2", "c3", "vx", "vy", "p", "rho", "E", "mx", "my", "T"]
 
 
 @pytest.mark.parametrize("name,case,prim,data", CASES, ids=[c[0] for c in CASES])
@@ -49,4 +49,17 @@ def test_oracle_riemann_failure_matches_reference(oracle_mod):
     oc.upload(p)
     oc.step()
     with pytest.raises(RuntimeError, match="status 1"):
+        oc.step()
+
+
+def test_oracle_chemistry_jcg_failure_matches_reference(oracle_mod):
+    """With the Jacobi-preconditioned CG solver the hot Cl2 case does not converge; the reference
+    divides the first step (1e-15) by ten, finds it below the minimal time step, prints "Timestep
+    become too small." and stops with systemError.  The oracle reports the same status."""
+    from schemi_b200 import cases
+
+    c, p = cases.chlorine_dissociation_2d(4, solver="JacobiConjugateGradient")
+    oc = oracle_mod.OracleCase(c)
+    oc.upload(p)
+    with pytest.raises(RuntimeError, match="status 4"):
         oc.step()

@@ -71,3 +71,31 @@ def test_rt_primitive_matches_numpy():
         pt = adjoint.rayleigh_taylor_primitive(a, nx, ny)
         for i in range(6):
             assert np.array_equal(pt[i].numpy(), np.asarray(prim[i]))
+
+
+def test_a_b_2c_oracle_conserves_mass_and_releases_heat(oracle_mod):
+    """A uniform mixture at rest: the advection leaves it alone, so one step is the chemistry
+    alone.  The mixture density is unchanged, the species densities still sum to it, C grows at
+    the expense of A and B, and the energy rises by q/2 per mole of C formed (equal heat
+    capacities: no dCv term)."""
+    from schemi_b200 import cases
+
+    case, prim = cases.reacting_shear_3d(n=4, precision="f64", periodic=True)
+    case.chem_forward = (1e14, 0.0, case.chem_forward[2])
+    n = case.n_cells
+    c = float(prim[0].max())
+    prim = [np.full(n, 0.4 * c), np.full(n, 0.4 * c), np.full(n, 0.2 * c), np.zeros(n), np.zeros(n), np.zeros(n),
+            np.full(n, 101325.0)]
+    oc = oracle_mod.OracleCase(case)
+    oc.upload(prim)
+    oc.set_time(0.0, 1e-5)  # a step long enough for the heat release to stand far above rounding
+    before = oc.download()
+    oc.step()
+    after = oc.download()
+    assert np.allclose(after["rho"], before["rho"], rtol=0, atol=1e-15 * before["rho"].max())
+    s = after["rho1"] + after["rho2"] + after["rho3"]
+    assert np.allclose(s, after["rho"], rtol=1e-14)
+    dC = after["c3"] - before["c3"]
+    assert (dC > 0).all() and (after["c1"] < before["c1"]).all()
+    dE = after["E"] - before["E"]
+    assert np.allclose(dE / dC, 0.5 * case.chem_q, rtol=1e-9)
