@@ -22,6 +22,8 @@ cpu_baseline / --impl reference: the reference solver compiled from its own sour
 
 batched   512 Richtmyer-Meshkov cases of seeded sizes 128^2..512^2 (FP32 flux) advanced by the
           persistent ensemble kernel, against the same cases one after the other.
+reacting_3d  3D reacting shear layer 256^3 (A+B->2C, van der Waals, FP32 flux + FP64 chemistry):
+          cell-updates/s of the whole step and the chemistry pass's share.
 adjoint   Rayleigh-Taylor 512 x 1536 to t = 5 (64 seeded interface modes): gradient of the
           time-integrated mixing width through the hand-written adjoint (checkpoint every 50
           steps); backward (incl. recomputation) over forward device time, FP64 and FP32 flux,
@@ -306,6 +308,55 @@ def batched_vs_plain(n_cases: int, steps: int, torch):
     return out
 
 
+def reacting_3d(torch, peak, n: int, steps: int, warmup: int, flush, autotune_shapes: bool):
+    """Config-3 shape: 3D reacting shear layer n^3 (van der Waals mixture of A, B, C; A+B->2C with
+    the FP64 chemistry pass; FP32 flux), periodic x and z, slip y.  Device time per step of the
+    whole step (fused march + chemistry + CFL), and of the same case without chemistry, so that the
+    chemistry pass's share is the difference."""
+    import copy
+
+    from schemi_b200 import cases, fv
+
+    case, prim = cases.reacting_shear_3d(n=n, precision="f32flux")
+    out = {"workload": f"reacting_shear_3d {n}^3, A+B->2C, vdW, f32flux step + FP64 chemistry",
+           "cells": case.n_cells}
+    results = {}
+    for label, c in (("with_chemistry", case), ("flow_only", None)):
+        if c is None:
+            c = copy.deepcopy(case)
+            c.chemistry = "no"
+        g = fv.FVCase(c)
+        g.upload(prim)
+        shape = None
+        if autotune_shapes:
+            from schemi_b200 import autotune
+
+            shape = autotune.tune(g)
+            g.upload(prim)
+        torch.cuda.synchronize()
+        with ClockSampler(torch.cuda.current_device()) as cs:
+            ms = time_steps(g, torch, steps, warmup, flush)
+        results[label] = {"ms_per_step": sum(ms) / steps, "kernels_per_step": g.kernels_per_step,
+                          "march_shape": list(shape) if shape else None, "clocks": cs.summary()}
+        g.close()
+    w, f = results["with_chemistry"], results["flow_only"]
+    ncell = case.n_cells
+    step_bytes = 2 * 8 * (case.n_species + 1 + case.dims + 1)   # conserved state read + written
+    chem_bytes = 8 * (case.n_species + 1 + 3 + 1) + 8 * (case.n_species + 1)  # read state, write rho_k, E
+    out.update({
+        "value": ncell / (w["ms_per_step"] / 1e3), "unit": "cell-updates/s", "ms_per_step": w["ms_per_step"],
+        "flow_only_value": ncell / (f["ms_per_step"] / 1e3), "flow_only_ms_per_step": f["ms_per_step"],
+        "chemistry_ms_per_step": w["ms_per_step"] - f["ms_per_step"],
+        "chemistry_share": (w["ms_per_step"] - f["ms_per_step"]) / w["ms_per_step"],
+        "kernels_per_step": w["kernels_per_step"], "march_shape": w["march_shape"], "clocks": w["clocks"],
+        "roofline": {"bound": "hbm", "bytes_per_cell_update": step_bytes + chem_bytes,
+                     "achieved": ncell * (step_bytes + chem_bytes) / (w["ms_per_step"] / 1e3) / 1e9, "peak": peak,
+                     "unit": "GB/s"},
+    })
+    out["roofline"]["frac"] = out["roofline"]["achieved"] / peak
+    return out
+
+
 def adjoint_rt(torch, peak, t_end: float, autotune_shapes: bool):
     """Config-5 shape: Rayleigh-Taylor 512x1536 (64 seeded interface modes) to t_end; gradient of
     the time-integrated mixing width with respect to the mode amplitudes through the hand-written
@@ -488,6 +539,9 @@ def run_ours(args):
         b = batched_vs_plain(args.batch_cases, args.steps, torch)
         b["roofline_frac"] = b["value"] * b["bytes_per_cell_update"] / 1e9 / peak
         line["batched"] = b
+    if args.reacting_n > 0:
+        line["reacting_3d"] = reacting_3d(torch, peak, args.reacting_n, args.steps, args.warmup, flush,
+                                          not args.no_autotune)
     if args.adjoint_t_end > 0 and rank == 0:
         line["adjoint"] = adjoint_rt(torch, peak, args.adjoint_t_end, not args.no_autotune)
     if rank == 0 and not args.no_cpu_baseline:
@@ -519,6 +573,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--batch-cases", type=int, default=512, help="cases of the batched ensemble (0: skip)")
+    ap.add_argument("--reacting-n", type=int, default=256,
+                    help="cells per axis of the 3D reacting shear layer workload (0: skip)")
     ap.add_argument("--adjoint-t-end", type=float, default=5.0,
                     help="end time of the Rayleigh-Taylor adjoint workload (0: skip)")
     args = ap.parse_args()

@@ -79,30 +79,31 @@ __device__ __forceinline__ void dot(const System<N>& m, const double* v, double*
     }
 }
 
-// solveGS (abstractChemicalKinetics.hpp:201-306)
+// solveGS (abstractChemicalKinetics.hpp:201-306); 1 / D[i] is the same value in every iteration
 template <int N>
 __device__ bool solveGS(const System<N>& m, const double* init, int maxIter, double* out) {
-    double old[N], nw[N];
+    double old[N], nw[N], aii[N];
 #pragma unroll
-    for (int i = 0; i < N; ++i) old[i] = nw[i] = init[i];
+    for (int i = 0; i < N; ++i) {
+        old[i] = nw[i] = init[i];
+        aii[i] = 1. / m.D[i];
+    }
     for (int it = 1;; ++it) {
 #pragma unroll
         for (int i = 0; i < N; ++i) {
-            const double aii = 1. / m.D[i];
-            nw[i] = m.B[i] * aii;
+            nw[i] = m.B[i] * aii[i];
 #pragma unroll
-            for (int q = 0; q < nLeft<N>(i); ++q) nw[i] -= m.A[i][left<N>(i, q)] * nw[left<N>(i, q)] * aii;
+            for (int q = 0; q < nLeft<N>(i); ++q) nw[i] -= m.A[i][left<N>(i, q)] * nw[left<N>(i, q)] * aii[i];
 #pragma unroll
-            for (int q = 0; q < nRight<N>(i); ++q) nw[i] -= m.A[i][right<N>(i, q)] * old[right<N>(i, q)] * aii;
+            for (int q = 0; q < nRight<N>(i); ++q) nw[i] -= m.A[i][right<N>(i, q)] * old[right<N>(i, q)] * aii[i];
         }
 #pragma unroll
         for (int i = N - 1; i >= 0; --i) {
-            const double aii = 1. / m.D[i];
-            nw[i] = m.B[i] * aii;
+            nw[i] = m.B[i] * aii[i];
 #pragma unroll
-            for (int q = nLeft<N>(i) - 1; q >= 0; --q) nw[i] -= m.A[i][left<N>(i, q)] * old[left<N>(i, q)] * aii;
+            for (int q = nLeft<N>(i) - 1; q >= 0; --q) nw[i] -= m.A[i][left<N>(i, q)] * old[left<N>(i, q)] * aii[i];
 #pragma unroll
-            for (int q = nRight<N>(i) - 1; q >= 0; --q) nw[i] -= m.A[i][right<N>(i, q)] * nw[right<N>(i, q)] * aii;
+            for (int q = nRight<N>(i) - 1; q >= 0; --q) nw[i] -= m.A[i][right<N>(i, q)] * nw[right<N>(i, q)] * aii[i];
         }
         if (relDiff<N>(nw, old) < kTol) {
             normalize<N>(nw);
@@ -119,29 +120,30 @@ __device__ bool solveGS(const System<N>& m, const double* init, int maxIter, dou
 // solveJ (:110-199)
 template <int N>
 __device__ bool solveJ(const System<N>& m, const double* init, int maxIter, double* out) {
-    double old[N], nw[N];
+    double old[N], nw[N], aii[N];
 #pragma unroll
-    for (int i = 0; i < N; ++i) old[i] = nw[i] = init[i];
+    for (int i = 0; i < N; ++i) {
+        old[i] = nw[i] = init[i];
+        aii[i] = 1. / m.D[i];
+    }
     for (int it = 1;; ++it) {
 #pragma unroll
         for (int i = 0; i < N; ++i) {
-            const double aii = 1. / m.D[i];
             double rs = 0;
 #pragma unroll
             for (int q = 0; q < nLeft<N>(i); ++q) rs -= m.A[i][left<N>(i, q)] * old[left<N>(i, q)];
 #pragma unroll
             for (int q = 0; q < nRight<N>(i); ++q) rs -= m.A[i][right<N>(i, q)] * old[right<N>(i, q)];
-            nw[i] = (m.B[i] + rs) * aii;
+            nw[i] = (m.B[i] + rs) * aii[i];
         }
 #pragma unroll
         for (int i = N - 1; i >= 0; --i) {
-            const double aii = 1. / m.D[i];
             double rs = 0;
 #pragma unroll
             for (int q = nLeft<N>(i) - 1; q >= 0; --q) rs -= m.A[i][left<N>(i, q)] * old[left<N>(i, q)];
 #pragma unroll
             for (int q = nRight<N>(i) - 1; q >= 0; --q) rs -= m.A[i][right<N>(i, q)] * old[right<N>(i, q)];
-            nw[i] = (m.B[i] + rs) * aii;
+            nw[i] = (m.B[i] + rs) * aii[i];
         }
         if (relDiff<N>(nw, old) < kTol) {
             normalize<N>(nw);
@@ -286,7 +288,8 @@ __device__ __forceinline__ bool solve(const ChemParams& C, const System<N>& m, c
 
 // k = A T^n exp(-E / (R T))
 __device__ __forceinline__ double arrhenius(double A, double n, double E, double T, double R) {
-    return A * pow(T, n) * exp(-E / (R * T));
+    const double Tn = n == 0.0 ? 1.0 : pow(T, n);  // pow(T, 0) is exactly 1
+    return A * Tn * exp(-E / (R * T));
 }
 
 // Mechanism matrix of one sub-step (species order of fvstep.h).
@@ -411,8 +414,10 @@ __device__ int integrate(const ChemParams& C, const MixParams& mx, double dt, do
 }
 
 // Chemistry of every cell of U (in place) with the step's dt, then the CFL signal of the result.
+// The register budget is sized for two CTAs of 256 threads per SM (the FP64 arithmetic is
+// latency-bound; the spills this costs stay in L1).
 template <int N, int EOS, int D>
-__global__ void __launch_bounds__(256) k_chemistry(const StepParams P, const ChemParams C, double* __restrict__ U,
+__global__ void __launch_bounds__(256, 2) k_chemistry(const StepParams P, const ChemParams C, double* __restrict__ U,
                                                    DevClock* __restrict__ ck, double* __restrict__ blockMax) {
     __shared__ double red[32];
     if (ck->done) return;  // uniform over the grid
