@@ -367,36 +367,40 @@ __device__ __forceinline__ bool riemann(int flux, int axis, int sign, const Face
 #pragma unroll
             for (int d = 0; d < 3; ++d) F.m[d] = O.m[d] * uO + (d == axis ? sg : T(0)) * (O.p + T(0));
             F.E = uO * (O.E + O.p + T(0));
-        } else if (Sc >= T(0)) {
-            const T factor = SO - uO;
-            const T den = T(1) / (SO - Sc);
+        } else if (Sc >= T(0) || SN > T(0)) {
+            // star flux of the side the contact leaves (owner when Sc >= 0): the reference's two
+            // branches are the same expression on (O, uO, SO) or (B, uN, SN)
+            auto star = [&](const T* rw, const T* mw, T Ew, T pw, T u, T S) {
+                const T factor = S - u;
+                const T den = T(1) / (S - Sc);
 #pragma unroll
-            for (int k = 0; k <= NS; ++k) {
-                const T rs = O.rho[k] * factor * den;
-                F.rho[k] = O.rho[k] * uO + SO * (rs - O.rho[k]);
-            }
+                for (int k = 0; k <= NS; ++k) {
+                    const T rs = rw[k] * factor * den;
+                    F.rho[k] = rw[k] * u + S * (rs - rw[k]);
+                }
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                const T ms = (O.m[d] * factor - (d == axis ? sg : T(0)) * (O.p + T(0) - PON)) * den;
-                F.m[d] = O.m[d] * uO + (d == axis ? sg : T(0)) * (O.p + T(0)) + (ms - O.m[d]) * SO;
-            }
-            const T Es = (O.E * factor - (O.p + T(0)) * uO + PON * Sc) * den;
-            F.E = (O.E + O.p + T(0)) * uO + SO * (Es - O.E);
-        } else if (SN > T(0)) {
-            const T factor = SN - uN;
-            const T den = T(1) / (SN - Sc);
+                for (int d = 0; d < 3; ++d) {
+                    const T ms = (mw[d] * factor - (d == axis ? sg : T(0)) * (pw + T(0) - PON)) * den;
+                    F.m[d] = mw[d] * u + (d == axis ? sg : T(0)) * (pw + T(0)) + (ms - mw[d]) * S;
+                }
+                const T Es = (Ew * factor - (pw + T(0)) * u + PON * Sc) * den;
+                F.E = (Ew + pw + T(0)) * u + S * (Es - Ew);
+            };
+            const bool own = Sc >= T(0);
+            if constexpr (sizeof(T) == 8) {
+                // FP64 (latency-bound): select the side by value and evaluate once, so that a warp
+                // whose faces see contacts moving both ways does not run both branches
+                T rw[NS + 1], mw[3];
 #pragma unroll
-            for (int k = 0; k <= NS; ++k) {
-                const T rs = B.rho[k] * factor * den;
-                F.rho[k] = B.rho[k] * uN + SN * (rs - B.rho[k]);
-            }
+                for (int k = 0; k <= NS; ++k) rw[k] = own ? O.rho[k] : B.rho[k];
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                const T ms = (B.m[d] * factor - (d == axis ? sg : T(0)) * (B.p + T(0) - PON)) * den;
-                F.m[d] = B.m[d] * uN + (d == axis ? sg : T(0)) * (B.p + T(0)) + (ms - B.m[d]) * SN;
+                for (int d = 0; d < 3; ++d) mw[d] = own ? O.m[d] : B.m[d];
+                star(rw, mw, own ? O.E : B.E, own ? O.p : B.p, own ? uO : uN, own ? SO : SN);
+            } else {
+                // FP32 (issue-bound): the selects cost more than the divergence they save
+                if (own) star(O.rho, O.m, O.E, O.p, uO, SO);
+                else star(B.rho, B.m, B.E, B.p, uN, SN);
             }
-            const T Es = (B.E * factor - (B.p + T(0)) * uN + PON * Sc) * den;
-            F.E = (B.E + B.p + T(0)) * uN + SN * (Es - B.E);
         } else if (SN <= T(0)) {
 #pragma unroll
             for (int k = 0; k <= NS; ++k) F.rho[k] = (sg * uN) * B.rho[k] * sg;
