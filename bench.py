@@ -29,8 +29,9 @@ adjoint   Rayleigh-Taylor 512 x 1536 to t = 5 (64 seeded interface modes): gradi
           steps); backward (incl. recomputation) over forward device time, FP64 and FP32 flux,
           and a central finite difference (h = 1e-6) along a seeded direction.
 
-Multi-GPU (torchrun): every rank advances its own replica of the case (the single-case step does
-not shard; "scaling": "weak").
+Multi-GPU (torchrun): every rank advances its own replica of the single case (the single-case
+step does not shard; "scaling": "weak"); the batched ensemble is sharded, its cases split over
+the ranks by estimated work with no per-step exchange.
 """
 
 from __future__ import annotations
@@ -267,14 +268,22 @@ def e2e_run(g, prim_pinned, steps):
     return wall, st, h2d, d2h
 
 
-def batched_vs_plain(n_cases: int, steps: int, torch):
+def batched_vs_plain(n_cases: int, steps: int, torch, rank: int = 0, world: int = 1, dist=None):
     """Config-4 shape: `n_cases` Richtmyer-Meshkov cases of seeded sizes 128^2..512^2 (FP32 flux,
     HLLC + superbee, own end times), advanced `steps` ensemble steps by the batched persistent
-    kernel, against the same cases advanced one after the other by the single-case path."""
-    from schemi_b200 import cases, fv
+    kernel, against the same cases advanced one after the other by the single-case path.  With
+    several ranks the cases are sharded by estimated work (schemi_b200.ensemble, no per-step
+    exchange); totals are summed and device times maxed over the ranks."""
+    from schemi_b200 import cases, ensemble, fv
 
+    draws = [cases.richtmyer_meshkov_draws(i) for i in range(n_cases)]
+    # work ~ cells x steps; steps ~ t_end / dt with dt ~ 0.5 / (n * 2.5) (post-shock signal speed)
+    ws = 1.2 * math.sqrt(1.4)
+    work = [ensemble.case_work(n * n, tr / ws, 0.5 / (n * 2.5)) for n, _, _, tr in draws]
+    shares = ensemble.partition(work, world)
+    mine = shares[rank]
     handles, t_end, cells = [], [], 0
-    for i in range(n_cases):
+    for i in mine:
         case, prim, te = cases.richtmyer_meshkov(i, precision="f32flux")
         g = fv.FVCase(case)
         g.set_march_shape(128, 1, 16)
@@ -292,14 +301,26 @@ def batched_vs_plain(n_cases: int, steps: int, torch):
         plain_updates += st.steps * g.n_cells
     batch = fv.FVBatch(handles)
     batch.run(t_end, max_steps=16)  # warm-up (graph capture, kernel configuration)
+    if dist is not None and world > 1:
+        dist.barrier()
     st = batch.run(t_end, max_steps=steps)
+    updates, ms = float(st.cell_updates), float(st.device_ms)
+    if dist is not None and world > 1:
+        t = torch.tensor([updates, float(plain_updates), float(cells)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        updates, plain_updates, cells = float(t[0]), float(t[1]), int(t[2])
+        t = torch.tensor([ms, plain_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, plain_ms = float(t[0]), float(t[1])
     out = {
         "cases": n_cases, "cells": cells, "steps": steps, "arith": "f32flux",
-        "value": st.cell_updates / (st.device_ms / 1e3), "unit": "cell-updates/s",
-        "ms_per_ensemble_step": st.device_ms / steps,
+        "value": updates / (ms / 1e3), "unit": "cell-updates/s",
+        "ms_per_ensemble_step": ms / steps,
         "plain_value": plain_updates / (plain_ms / 1e3),
         "launches_per_ensemble_step": st.launches / max(st.steps_max, 1),
         "bytes_per_cell_update": 2 * 8 * (2 + 1 + 2 + 1),
+        "sharding": {"ranks": world, "cases_per_rank": [len(x) for x in shares],
+                     "estimated_imbalance": ensemble.imbalance(work, shares)},
     }
     out["batched_over_plain"] = out["value"] / out["plain_value"]
     batch.close()
@@ -536,7 +557,7 @@ def run_ours(args):
         },
     }
     if args.batch_cases > 0:
-        b = batched_vs_plain(args.batch_cases, args.steps, torch)
+        b = batched_vs_plain(args.batch_cases, args.steps, torch, rank, world, dist)
         b["roofline_frac"] = b["value"] * b["bytes_per_cell_update"] / 1e9 / peak
         line["batched"] = b
     if args.reacting_n > 0:

@@ -68,6 +68,17 @@ def kelvin_helmholtz_2d(n: int = 1024, precision: str = "f64", seed: int = 2026,
     return case, [cA.ravel(), cB.ravel(), u.ravel(), v.ravel(), z.ravel(), p.ravel()]
 
 
+def richtmyer_meshkov_draws(index: int, base_seed: int = 2028) -> Tuple[int, float, float, float]:
+    """Seeded draws of ensemble case ``index``: cells per axis n ~ U{128..512}, interface
+    amplitude a ~ U(0.01, 0.05), wavelength lam ~ U(0.25, 1), end time in shock transits ~ U(2, 4)."""
+    rng = np.random.default_rng(base_seed + index)
+    n = int(rng.integers(128, 513))
+    a = float(rng.uniform(0.01, 0.05))
+    lam = float(rng.uniform(0.25, 1.0))
+    transits = float(rng.uniform(2.0, 4.0))
+    return n, a, lam, transits
+
+
 def richtmyer_meshkov(index: int, n: int = 0, precision: str = "f32flux", limiter: str = "superbee",
                       base_seed: int = 2028) -> Tuple[Case, list, float]:
     """Case ``index`` of the RM ensemble: light gas (gamma 1.4, rho 1) left of the interface
@@ -75,11 +86,7 @@ def richtmyer_meshkov(index: int, n: int = 0, precision: str = "f32flux", limite
     shock in the light gas starts at x = 0.3 (post-shock state from Rankine-Hugoniot).
     n ~ U{128..512} (seed base_seed + index) unless given; free at x=0, slip elsewhere.
     Returns (case, prim, t_end) with t_end ~ U(2, 4) shock transit times of the unit box."""
-    rng = np.random.default_rng(base_seed + index)
-    n_draw = int(rng.integers(128, 513))
-    a = float(rng.uniform(0.01, 0.05))
-    lam = float(rng.uniform(0.25, 1.0))
-    transits = float(rng.uniform(2.0, 4.0))
+    n_draw, a, lam, transits = richtmyer_meshkov_draws(index, base_seed)
     n = n or n_draw
     g1, g2 = 1.4, 1.09
     sp = [Species(M=1.0, Cv=1.0 / (g1 - 1.0)), Species(M=5.0, Cv=1.0 / (g2 - 1.0))]
