@@ -142,6 +142,9 @@ typedef struct fv_config {
     double chem_q;            /* A_B_2C: heat release per mol of reaction (J/mol, > 0 exothermic) */
     int chem_solver;          /* fv_chem_solver */
     int chem_max_iter;        /* #Number_of_chemical_solver_iterations */
+    /* #Constant_timestep: > 0 fixes every step to this dt (main then skips its CFL block,
+     * Schemi.cpp:178-181,664-668,807); <= 0 keeps the CFL step. */
+    double const_timestep;
 } fv_config;
 
 /* Field indices of fv_download / fv_upload arrays (n_cells doubles each, x fastest).

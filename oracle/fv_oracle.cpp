@@ -1346,6 +1346,7 @@ double cflTimestep(const fvo_case& cs) {
     double dt = cs.cfg.courant / maxS;
     if (!cs.cfg.courant_only) dt = std::min(dt, kVeryBig);
     dt = std::max(dt, cs.cfg.min_timestep);
+    if (cs.cfg.const_timestep > 0) dt = cs.cfg.const_timestep;  // no CFL block (Schemi.cpp:807)
     return dt;
 }
 
@@ -1409,7 +1410,7 @@ fvo_case* fvo_create(const fv_config* cfg, char* err, int err_len) {
     cs->Uv.assign(cs->nCells, 0.0);
     cs->p.assign(cs->nCells, 0.0);
     cs->g = v3(cfg->g[0], cfg->g[1], cfg->g[2]);
-    cs->dt = cfg->min_timestep;
+    cs->dt = cfg->const_timestep > 0 ? cfg->const_timestep : cfg->min_timestep;
     return cs;
 }
 
@@ -1446,7 +1447,7 @@ int fvo_upload(fvo_case* cs, const double* const* prim) {
         cs->E[i] = cs->Uv[i] + cs->rho[0][i] * v2 * 0.5 + 0.0;
     }
     cs->time = 0;
-    cs->dt = cs->cfg.min_timestep;
+    cs->dt = cs->cfg.const_timestep > 0 ? cs->cfg.const_timestep : cs->cfg.min_timestep;
     cs->g = v3(cs->cfg.g[0], cs->cfg.g[1], cs->cfg.g[2]);
     return FV_OK;
 }

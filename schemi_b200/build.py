@@ -13,6 +13,9 @@ Translation units (compiled in parallel):
   csrc/fv_adjoint.cu    recorded trajectories, checkpoints and the adjoint sweep
   csrc/fv_adjoint_f64.cu / fv_adjoint_f32.cu  adjoint step kernels per arithmetic
 nvcc cross-compiles for sm_100a without a GPU.
+
+The task-deck driver ``schemi_b200/lib/fvrun`` (host/fvrun.cpp, C++17, g++) links the library
+through its C-ABI with an $ORIGIN rpath, so the pair can be moved together.
 """
 
 from __future__ import annotations
@@ -27,6 +30,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libschemi_fv.so")
+DRIVER = os.path.join(LIBDIR, "fvrun")
+DRIVER_SRC = os.path.join(HERE, "host", "fvrun.cpp")
 BUILD = os.path.join(HERE, "_build")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -93,7 +98,20 @@ def build(verbose: bool = False, force: bool = False, extra_flags=None) -> str:
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError("link failed:\n" + res.stdout + res.stderr)
+    build_driver(force=force)
     return LIB
+
+
+def build_driver(force: bool = False) -> str:
+    """Compile the task-deck driver against the built library."""
+    deps = [DRIVER_SRC, LIB, os.path.join(HERE, "..", "include", "fvstep.h")]
+    if force or _stale(DRIVER, deps):
+        cmd = [os.environ.get("CXX", "g++"), "-std=c++17", "-O2", "-Wall", "-I", os.path.join(HERE, "..", "include"),
+               DRIVER_SRC, "-o", DRIVER, "-L", LIBDIR, "-lschemi_fv", "-Wl,-rpath,$ORIGIN"]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError("driver build failed:\n" + " ".join(cmd) + "\n" + res.stdout + res.stderr)
+    return DRIVER
 
 
 if __name__ == "__main__":

@@ -84,6 +84,7 @@ class fv_config_t(ctypes.Structure):
         ("chem_q", ctypes.c_double),
         ("chem_solver", ctypes.c_int),
         ("chem_max_iter", ctypes.c_int),
+        ("const_timestep", ctypes.c_double),
     ]
 
 
@@ -149,6 +150,7 @@ class Case:
     chem_q: float = 0.0
     chem_solver: str = "Gauss-Seidel"
     chem_max_iter: int = 200
+    const_timestep: float = 0.0   # > 0: every step takes this dt (#Constant_timestep)
     name: str = "case"
 
     def __post_init__(self):
@@ -233,6 +235,7 @@ class Case:
         c.chem_q = self.chem_q
         c.chem_solver = CHEM_SOLVERS[self.chem_solver]
         c.chem_max_iter = self.chem_max_iter
+        c.const_timestep = self.const_timestep
         return c
 
 

@@ -446,6 +446,7 @@ fv_status fv_create(const fv_config* cfg, fv_handle** out) {
     P.courant_only = cfg->courant_only;
     P.courant = cfg->courant;
     P.min_dt = cfg->min_timestep;
+    P.const_dt = cfg->const_timestep;
     MixParams& mp = P.mix;
     mp.ns = cfg->n_species;
     mp.eos_kind = cfg->eos;
@@ -603,8 +604,9 @@ static fv_status setMomentumComponents(fv_handle* h) {
 static fv_status resetClock(fv_handle* h) {
     DevClock& c = *h->ckHost;
     memset(&c, 0, sizeof(DevClock));
-    c.dt = h->cfg.min_timestep;
-    c.dt_free = h->cfg.min_timestep;
+    // Schemi.cpp:664-668: the first step is the minimal time step, or the constant step
+    c.dt = h->cfg.const_timestep > 0 ? h->cfg.const_timestep : h->cfg.min_timestep;
+    c.dt_free = c.dt;
     c.t_end = std::numeric_limits<double>::infinity();
     c.first = 1;
     for (int d = 0; d < 3; ++d) {
@@ -670,11 +672,13 @@ fv_status fv_run(fv_handle* h, double t_end, long long max_steps, fv_run_stats* 
     fv_status st = readClock(h);
     if (st != FV_OK) return st;
     const long long steps0 = h->ckHost->steps;
-    // main: mesh_.setTimestep(std::min(mesh_.timestep(), timeOfCalculation)) before the loop
+    // main: mesh_.setTimestep(std::min(mesh_.timestep(), timeOfCalculation)) before the loop; in
+    // the loop's own form (Schemi.cpp:933-935) so that a run resumed with the same end time takes
+    // the step the device clamp already chose
     DevClock& c = *h->ckHost;
     c.t_end = t_end;
     c.done = !(c.time < t_end);
-    c.dt = std::min(c.dt_free, t_end - c.time);
+    c.dt = (c.time + c.dt_free) > t_end ? t_end - c.time : c.dt_free;
     FV_CUDA(h, cudaMemcpyAsync(h->ck, h->ckHost, sizeof(DevClock), cudaMemcpyHostToDevice, h->stream));
     const int chunk = 32;  // steps per graph
     if (h->graphSteps != chunk) {

@@ -116,11 +116,20 @@ struct Mixture {
         const T acc = am * (c[0] * c[0]);
         return (p + acc) * (T(1) - c[0] * bm) / g1 - acc;
     }
+    // idealFluid.cpp:37-41, vanDerWaalsFluid.cpp:44-48 with Cv_mix = sum X_k Cv_k
     __device__ __forceinline__ static T TFromUv(const MixParams& mp, const T* c, T Uv) {
-        T g1, am, bm, Mm;
-        params(mp, c, g1, am, bm, Mm);
-        const T Cvm = T(mp.R) / g1;  // only used for output; not bit-matched
+        T X[NS];
+#pragma unroll
+        for (int k = 0; k < NS; ++k) X[k] = c[k + 1] / c[0];
+        T Cvm = 0;
+#pragma unroll
+        for (int k = 0; k < NS; ++k) Cvm += X[k] * T(mp.Cv[k]);
         if (EOS == FV_EOS_IDEAL) return Uv / ((c[0] + Num<T>::stab()) * Cvm);
+        T am = 0;
+#pragma unroll
+        for (int k = 0; k < NS; ++k)
+#pragma unroll
+            for (int l = 0; l < NS; ++l) am += X[k] * X[l] * T(mp.a[k][l]);
         return (Uv + am * (c[0] * c[0])) / ((c[0] + Num<T>::stab()) * Cvm);
     }
     // sqSonicSpeed = dpdrho + dpdUv * (Uv + p) / rho

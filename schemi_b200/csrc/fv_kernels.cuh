@@ -52,6 +52,7 @@ struct StepParams {
     int courant_only;
     double courant;
     double min_dt;
+    double const_dt;     // > 0: constant time step (main skips its CFL block)
     double ext[3];          // parallelepiped extents (the transverse sizes of 1D / 2D cells)
     MixParams mix;
     BCParams bc;
@@ -852,6 +853,7 @@ __device__ __forceinline__ void finalizeCase(const StepParams& P, DevClock* ck, 
     double dtn = P.courant / m;
     if (!P.courant_only) dtn = smin(dtn, kVeryBigD());
     dtn = smax(dtn, P.min_dt);
+    if (P.const_dt > 0) dtn = P.const_dt;  // Schemi.cpp:807: no CFL block with a constant step
     if (P.gravity) {
         for (int d = 0; d < 3; ++d) ck->g[d] += ck->g_delta[d] * dtUsed;
     }

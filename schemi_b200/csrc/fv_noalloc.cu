@@ -153,6 +153,7 @@ bool buildParams(const fv_config& c, StepParams& P) {
     P.courant_only = c.courant_only;
     P.courant = c.courant;
     P.min_dt = c.min_timestep;
+    P.const_dt = c.const_timestep;
     MixParams& mp = P.mix;
     mp.ns = c.n_species;
     mp.eos_kind = c.eos;

@@ -161,7 +161,8 @@ def write_deck(case: Case, directory: str, prim: Sequence[np.ndarray], frequency
     nx, ny, nz = case.n
     dims_name = {1: "1D", 2: "2D", 3: "3D"}[case.dims]
     ncell = [nx, ny if case.dims >= 2 else 1, nz if case.dims >= 3 else 1]
-    src_ts = "Courant" if case.courant_only else "Courant-Source=0.25,0.5"
+    # "<type>=<source coefficient>,<diffusion coefficient>" (Schemi.cpp:180-243)
+    src_ts = ("Courant" if case.courant_only else "Courant-Source") + "=0.25,0.5"
     main = [
         ("#Radius-vector_of_system's_parallelepiped", " ".join(_f(x) for x in case.L)),
         ("#Number_of_cells_in_direction", " ".join(str(x) for x in ncell)),
@@ -180,7 +181,7 @@ def write_deck(case: Case, directory: str, prim: Sequence[np.ndarray], frequency
         ("#Type_of_source_flag", "BHR"),
         ("#Type_of_flow_solver", case.flux),
         ("#Dimensions_of_the_task", dims_name),
-        ("#Constant_timestep", "-1E-8"),
+        ("#Constant_timestep", _f(case.const_timestep) if case.const_timestep > 0 else "-1E-8"),
         ("#Source_timestep_correction", src_ts),
         ("#Reconstruction", "star"),
         ("#Approximation_order", "SecondOrder"),

@@ -1,0 +1,666 @@
+// fvrun -- runs a Schemi task deck on the GPU through the C-ABI of include/fvstep.h and writes the
+// reference's result files.
+//
+//     fvrun [deck_directory]            (default: the current directory)
+//     fvrun --print-config [deck_dir]   parse the deck and print the fv_config it maps to (no GPU)
+//
+// The deck is what the reference reads (paths inside the Schemi project): set/main.txt (the 24
+// positional keys of main/Schemi.cpp:101-163), set/g.txt (:83-99), set/sub_<k>.txt,
+// set/velocity.txt, set/pressure.txt (phaseInitialization.cpp), set/chemicalKinetics.txt
+// (Schemi.cpp:672-716, chemicalKineticsChlorumDissociation.cpp:275-308) and
+// set/zonesDescription.txt (zone.cpp).  The time loop, its output schedule, the restart from
+// fieldsOutput/output_<N> + result/Time.tsv and the last-step clamp follow Schemi.cpp:312-573,
+// 664-670, 716-940; the files written follow output::dataOutput (src/service/output.cpp:14-308):
+// result/output_<NNNNNN>.tsv, result/Time.tsv, fieldsOutput/output_<NNNNNN>/*.dat and
+// timeOfCalculation.tsv, with the reference's 20 significant digits.
+//
+// Not supported (the run stops with a message): zones other than the outer zone, diffusion,
+// turbulence, approximation orders other than SecondOrder, the 1D mixing-zone width output, and
+// chemical mechanisms other than "no" and "Cl2".
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <filesystem>
+#include <fstream>
+#include <iostream>
+#include <map>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "fvstep.h"
+
+namespace {
+
+constexpr double kNA = 6.02214076E23;          // globalConstants.hpp NAvogardro
+constexpr double kRSI = 8.31446261815324;      // R_SI
+constexpr double kPlanckSI = 6.626E-34;        // PlanckConstant_SI
+const double kPi = std::acos(-1.0);            // Pi_number (g++ build)
+constexpr double kStab = 5 * 2.220446049250313080847e-16;  // stabilizator
+constexpr int kPrecision = 20;                 // ioPrecision
+constexpr int kNumberLength = 6;               // lengthOfNumber
+
+struct Fail : std::runtime_error {
+    int code;
+    Fail(const std::string& m, int c = FV_ERR_INIT) : std::runtime_error(m), code(c) {}
+};
+
+// whitespace tokens of a file, read like the reference's operator>> chains
+struct Tokens {
+    std::vector<std::string> t;
+    size_t i = 0;
+    Tokens(const std::string& path) {
+        std::ifstream f(path);
+        if (!f.is_open()) throw Fail(path + " not found.", FV_ERR_SYSTEM);
+        std::string w;
+        while (f >> w) t.push_back(w);
+    }
+    const std::string& next(const std::string& what) {
+        if (i >= t.size()) throw Fail("unexpected end of file while reading " + what);
+        return t[i++];
+    }
+    void skip() { next("a label"); }
+    double num(const std::string& what) {
+        const std::string& s = next(what);
+        try {
+            return std::stod(s);
+        } catch (...) {
+            throw Fail("not a number for " + what + ": " + s);
+        }
+    }
+};
+
+// onOffMap of globalConstants.hpp
+bool onOff(const std::string& s, const std::string& what) {
+    if (s == "on" || s == "yes") return true;
+    if (s == "off" || s == "no") return false;
+    throw Fail("Unknown " + what + " flag.");
+}
+
+int bcType(const std::string& s) {
+    if (s == "blank") return 0;  // patches of unused axes
+    if (s == "freeBoundary") return FV_BC_FREE;
+    if (s == "slip") return FV_BC_SLIP;
+    if (s == "fixedValueCell") return FV_BC_FIXED_CELL;
+    if (s == "fixedValueSurface") return FV_BC_FIXED_SURFACE;
+    throw Fail("unknown boundary condition type " + s);
+}
+
+int limiterIndex(const std::string& s) {
+    static const char* names[] = {"zero",       "minmod",  "vanLeer", "linear", "vanAlbada",
+                                  "HQUICK",     "vanLeer2", "superbee", "vanAlbada2", "minmod2",
+                                  "Sweby",      "Koren",   "Koren2",  "UTCDFS", "Schmidtmann"};
+    for (int i = 0; i < 15; ++i)
+        if (s == names[i]) return i;
+    throw Fail("unknown TVD limiter " + s);
+}
+
+struct Deck {
+    std::string dir;
+    fv_config cfg{};
+    double tEnd = 0;
+    long long freq = 1;
+    double minTime = 0;
+    std::string units, eos, readFrom;
+    std::vector<double> zoneC, zoneV, zoneP;  // outer-zone values: c_k, v, p
+    double hPlanck = 0;
+
+    std::string path(const std::string& rel) const { return dir + "/" + rel; }
+};
+
+// sub_k / velocity / pressure: six patch conditions, then the outer-zone values.
+void readPatches(Tokens& t, int nval, int field, int k, fv_config& c) {
+    for (int patch = 0; patch < 6; ++patch) {
+        t.skip();  // #<Patch>_boundary_condition
+        const std::string type = t.next("boundary condition");
+        const int bt = bcType(type);
+        double v[3] = {0, 0, 0};
+        if (bt == FV_BC_FIXED_CELL || bt == FV_BC_FIXED_SURFACE)
+            for (int q = 0; q < nval; ++q) v[q] = t.num("boundary value");
+        if (field == 0) {
+            c.bc_conc[patch][k] = bt;
+            c.bc_conc_value[patch][k] = v[0];
+        } else if (field == 1) {
+            c.bc_vel[patch] = bt;
+            for (int q = 0; q < 3; ++q) c.bc_vel_value[patch][q] = v[q];
+        } else {
+            c.bc_p[patch] = bt;
+            c.bc_p_value[patch] = v[0];
+        }
+    }
+}
+
+Deck readDeck(const std::string& dir) {
+    Deck d;
+    d.dir = dir;
+    fv_config& c = d.cfg;
+    // g.txt
+    {
+        Tokens t(d.path("set/g.txt"));
+        t.skip();
+        const std::string on = t.next("gravity flag");
+        t.skip();
+        for (int q = 0; q < 3; ++q) c.g[q] = t.num("g");
+        t.skip();
+        for (int q = 0; q < 3; ++q) c.g_delta[q] = t.num("g growth");
+        c.gravity = onOff(on, "gravitation");
+    }
+    // main.txt
+    std::string limiter, diffusion, turbulence, flux, dims, sourceTime, reconstruction, order, width;
+    {
+        Tokens t(d.path("set/main.txt"));
+        t.skip();
+        for (int q = 0; q < 3; ++q) c.L[q] = t.num("system size");
+        t.skip();
+        for (int q = 0; q < 3; ++q) c.n[q] = (int)t.num("number of cells");
+        t.skip(); d.tEnd = t.num("time of calculation");
+        t.skip(); c.courant = t.num("Courant number");
+        t.skip(); d.freq = (long long)t.num("frequency of output");
+        t.skip(); d.minTime = t.num("minimal time step");
+        t.skip(); c.n_species = (int)t.num("number of components");
+        t.skip(); d.units = t.next("gas constant");
+        t.skip(); d.eos = t.next("equation of state");
+        t.skip(); limiter = t.next("limiter");
+        t.skip(); t.next("iterations");
+        t.skip(); diffusion = t.next("diffusion flag");
+        t.skip(); turbulence = t.next("turbulence flag");
+        t.skip(); t.next("matrix solver");
+        t.skip(); t.next("source type");
+        t.skip(); flux = t.next("flow solver");
+        t.skip(); dims = t.next("dimensions");
+        t.skip(); c.const_timestep = t.num("constant time step");
+        t.skip(); sourceTime = t.next("source time step flag");
+        t.skip(); reconstruction = t.next("reconstruction");
+        t.skip(); order = t.next("approximation order");
+        t.skip(); d.readFrom = t.next("start point");
+        t.skip(); width = t.next("mixing zone width flag");
+        t.skip(); t.next("nonlinearity iterations");
+    }
+    if (onOff(diffusion, "diffusion")) throw Fail("#Diffusion_flag on: implicit diffusion is not part of this step");
+    if (onOff(turbulence, "turbulence"))
+        throw Fail("#Turbulence_flag on: turbulence models are not part of this step");
+    if (reconstruction != "linear" && reconstruction != "star") throw Fail("Unknown reconstruction flag.");
+    if (order != "SecondOrder") throw Fail("#Approximation_order " + order + ": only SecondOrder is implemented");
+    if (onOff(width, "mixed zone width calculation") && dims == "1D") throw Fail("#Calculation_of_mixing_zone_width on is not implemented");
+    c.dims = dims == "1D" ? 1 : dims == "2D" ? 2 : dims == "3D" ? 3 : 0;
+    if (!c.dims) throw Fail("unknown #Dimensions_of_the_task " + dims);
+    for (int q = c.dims; q < 3; ++q) c.n[q] = 1;
+    c.limiter = limiterIndex(limiter);
+    if (flux == "HLLC") c.flux = FV_FLUX_HLLC;
+    else if (flux == "HLL") c.flux = FV_FLUX_HLL;
+    else throw Fail("#Type_of_flow_solver " + flux + ": HLLC and HLL are implemented");
+    if (d.eos == "ideal") c.eos = FV_EOS_IDEAL;
+    else if (d.eos == "vanDerWaals") c.eos = FV_EOS_VAN_DER_WAALS;
+    else throw Fail("#Equation_of_state " + d.eos + ": ideal and vanDerWaals are implemented");
+    // phaseInitialization.cpp:418-435
+    if (d.units == "SI") { c.R = kRSI; d.hPlanck = kPlanckSI; }
+    else if (d.units == "1") { c.R = 1; d.hPlanck = kPlanckSI / kRSI; }
+    else if (d.units == "CGS") { c.R = kRSI * 1E7; d.hPlanck = kPlanckSI * 1E7; }
+    else if (d.units == "CGmS") { c.R = kRSI * 1E1; d.hPlanck = kPlanckSI * 1E4; }
+    else throw Fail("Unknown type of universal gas constant.");
+    c.min_timestep = d.minTime;
+    // "<type>=<source coefficient>,<diffusion coefficient>" (Schemi.cpp:180-243)
+    {
+        const size_t eq = sourceTime.find('='), com = sourceTime.find(',');
+        const auto count = [&](char ch) { return std::count(sourceTime.begin(), sourceTime.end(), ch); };
+        if ((count('=') != 1 && count(',') != 1) || eq > com)
+            throw Fail("Wrong format of time-step parameters settings");
+        const std::string type = sourceTime.substr(0, eq == std::string::npos ? 0 : eq);
+        if (type != "Courant" && type != "Courant-Source" && type != "Courant-Source-Diffusion")
+            throw Fail("Unknown source time-step flag.");
+        c.courant_only = type == "Courant";
+    }
+    c.precision = FV_PREC_F64;
+    if (c.n_species < 1 || c.n_species > FV_MAX_SPECIES) throw Fail("number of components must be 1..4");
+    // zones: the outer zone only
+    {
+        Tokens t(d.path("set/zonesDescription.txt"));
+        t.skip();
+        const int nz = (int)t.num("number of zones");
+        if (nz != 0) throw Fail("zones other than the outer zone are not implemented by this driver");
+    }
+    for (int k = 0; k < c.n_species; ++k) {
+        Tokens t(d.path("set/sub_" + std::to_string(k + 1) + ".txt"));
+        t.skip(); c.M[k] = t.num("molar mass");
+        t.skip(); c.Cv[k] = t.num("Cv");
+        t.skip(); c.Tc[k] = t.num("Tc");
+        t.skip(); c.Pc[k] = t.num("Pc");
+        for (int q = 0; q < 3; ++q) { t.skip(); t.next("transport parameter"); }
+        readPatches(t, 1, 0, k, c);
+        t.skip();
+        d.zoneC.push_back(t.num("zone concentration"));
+    }
+    {
+        Tokens t(d.path("set/velocity.txt"));
+        readPatches(t, 3, 1, 0, c);
+        t.skip();
+        for (int q = 0; q < 3; ++q) d.zoneV.push_back(t.num("zone velocity"));
+    }
+    {
+        Tokens t(d.path("set/pressure.txt"));
+        readPatches(t, 1, 2, 0, c);
+        t.skip();
+        d.zoneP.push_back(t.num("zone pressure"));
+    }
+    // chemistry
+    {
+        Tokens t(d.path("set/chemicalKinetics.txt"));
+        t.skip();
+        const std::string name = t.next("reaction name");
+        if (name == "no") {
+            c.chemistry = FV_CHEM_NONE;
+        } else if (name == "Cl2") {
+            c.chemistry = FV_CHEM_CL2;
+            double v[6];
+            for (double& x : v) { t.skip(); x = t.num("Arrhenius parameter"); }
+            c.chem_forward = fv_arrhenius{v[0], v[1], v[2]};
+            c.chem_backward = fv_arrhenius{v[3], v[4], v[5]};
+            t.skip();
+            const std::string solver = t.next("chemical solver");
+            static const std::map<std::string, int> solvers = {
+                {"Gauss-Seidel", FV_CHEM_GAUSS_SEIDEL}, {"Jacobi", FV_CHEM_JACOBI},
+                {"GaussElimination", FV_CHEM_GAUSS_ELIMINATION}, {"conjugateGradient", FV_CHEM_CONJUGATE_GRADIENT},
+                {"JacobiConjugateGradient", FV_CHEM_JACOBI_CONJUGATE_GRADIENT}};
+            auto it = solvers.find(solver);
+            if (it == solvers.end()) throw Fail("Unknown type of chemical iterative solver.");
+            c.chem_solver = it->second;
+            t.skip();
+            c.chem_max_iter = (int)t.num("chemical solver iterations");
+        } else {
+            throw Fail("chemical mechanism " + name + " is not implemented (no, Cl2)");
+        }
+    }
+    return d;
+}
+
+// ---------------------------------------------------------------- geometry (cell centres)
+// node coordinates 0 + d*i and the 8-corner average of the mesh generator (mesh.cpp:296-1900)
+std::vector<double> centres(const fv_config& c, int a) {
+    const bool used = a < c.dims;
+    const int n = used ? c.n[a] : 1;
+    const double L = c.L[a], d = L / n;
+    auto node = [&](int i) -> double {
+        if (used) return 0.0 + d * (double)(size_t)i;
+        return i == 0 ? 0.0 : L;
+    };
+    std::vector<double> out(n);
+    for (int i = 0; i < n; ++i) {
+        const double A = node(i), B = node(i + 1);
+        double seq[8];
+        for (int q = 0; q < 8; ++q) {
+            const int bit = a == 0 ? (q & 1) : (a == 1 ? ((q >> 1) & 1) : ((q >> 2) & 1));
+            seq[q] = bit ? B : A;
+        }
+        double s = seq[0] + seq[1];
+        for (int q = 2; q < 8; ++q) s = s + seq[q];
+        out[i] = s / 8.;
+    }
+    return out;
+}
+
+// ---------------------------------------------------------------- Helmholtz energy and entropy
+// mixtureIdeal::Fv/Sv (mixtureIdeal.cpp:300-354), mixtureVanDerWaals::Fv/Sv (:461-537) with
+// idealFluid::Fmx/Smx (idealFluid.cpp:90-116) and vanDerWaalsFluid::Fmx/Smx (:122-151).
+struct Thermo {
+    int N, eos;
+    double R, kB, h;
+    double molecMass[FV_MAX_SPECIES];
+    double aMolec[FV_MAX_SPECIES][FV_MAX_SPECIES], bMolec[FV_MAX_SPECIES][FV_MAX_SPECIES];
+
+    Thermo(const fv_config& c, double hPlanck) : N(c.n_species), eos(c.eos), R(c.R), kB(c.R / kNA), h(hPlanck) {
+        double a[FV_MAX_SPECIES][FV_MAX_SPECIES] = {}, b[FV_MAX_SPECIES][FV_MAX_SPECIES] = {};
+        for (int k = 0; k < N; ++k) {
+            molecMass[k] = c.M[k] / kNA;
+            b[k][k] = c.Tc[k] * R / (8 * c.Pc[k]);
+            a[k][k] = c.Pc[k] * b[k][k] * b[k][k] * 27;
+        }
+        for (int k = 0; k < N; ++k)
+            for (int l = 0; l < N; ++l)
+                if (k != l) {
+                    b[k][l] = std::pow(0.5 * (std::cbrt(b[k][k]) + std::cbrt(b[l][l])), 3);
+                    a[k][l] = std::sqrt(a[k][k] * a[l][l]);
+                }
+        for (int k = 0; k < N; ++k)
+            for (int l = 0; l < N; ++l) {
+                bMolec[k][l] = b[k][l] / kNA;
+                aMolec[k][l] = a[k][l] / (kNA * kNA);
+            }
+    }
+
+    // Sum over the species of a valarray expression, in the order libstdc++'s _Expr::sum() takes:
+    // from the last element down to the first.
+    template <class Term>
+    double speciesSum(Term term) const {
+        double s = term(N - 1);
+        for (int k = N - 2; k >= 0; --k) s += term(k);
+        return s;
+    }
+
+    // F (first) and S (second) per volume of a cell
+    void FS(const double* c, double T, double& F, double& S) const {
+        double x[FV_MAX_SPECIES] = {}, lam3[FV_MAX_SPECIES] = {};
+        for (int k = 0; k < N; ++k) x[k] = c[k + 1] / c[0];
+        const double molecConc = c[0] * kNA;
+        const double Vm = 1 / molecConc;
+        for (int k = 0; k < N; ++k) {
+            const double lam = std::sqrt((h * h) / (2 * kPi * molecMass[k] * kB * T));
+            lam3[k] = lam * lam * lam;
+        }
+        const double A = speciesSum([&](int k) { return x[k] * std::log(x[k] + kStab); });
+        const double C = speciesSum([&](int k) { return -x[k] * std::log(x[k] + kStab); });
+        if (eos == FV_EOS_IDEAL) {
+            const double B = speciesSum([&](int k) { return x[k] * std::log(Vm / lam3[k]); });
+            F = kB * T * (A - 1 - B) * molecConc;
+            S = kB * (C + B + 5. / 2.) * molecConc;
+            return;
+        }
+        // mixture a and b accumulate cell by cell from zero, k outer, l inner
+        double am = 0, bm = 0;
+        for (int k = 0; k < N; ++k)
+            for (int l = 0; l < N; ++l) {
+                am += x[k] * x[l] * aMolec[k][l];
+                bm += x[k] * x[l] * bMolec[k][l];
+            }
+        const double B = speciesSum([&](int k) { return x[k] * std::log((Vm - bm) / lam3[k]); });
+        F = (kB * T * (A - 1 - B) - am / Vm) * molecConc;
+        // mixtureVanDerWaals::Sv divides the molecular b by Avogadro's number once more
+        const double bs = bm / kNA;
+        const double B2 = speciesSum([&](int k) { return x[k] * std::log((Vm - bs) / lam3[k]); });
+        S = kB * (C + 5. / 2. + B2) * molecConc;
+    }
+};
+
+// ---------------------------------------------------------------- output (output.cpp:14-308)
+std::string number(long long n) {
+    const std::string s = std::to_string(n);
+    if ((int)s.size() > kNumberLength) throw Fail("Output number length larger than specified number of digits.", 3);
+    return std::string(kNumberLength - s.size(), '0') + s;
+}
+
+// `sonic`, when not empty, replaces the downloaded sonic speeds: with #Constant_timestep main never
+// recomputes its sonic-speed field after initialisation (Schemi.cpp:641-646, 807-812), and every
+// output carries the initial values.
+void writeOutput(const Deck& d, fv_handle* h, long long nOutput, double time, const Thermo& th,
+                 const std::vector<double>& sonic) {
+    const fv_config& c = d.cfg;
+    const int N = c.n_species;
+    const long long nc = (long long)c.n[0] * c.n[1] * c.n[2];
+    std::vector<std::vector<double>> f(FV_F_COUNT, std::vector<double>(nc));
+    std::vector<double*> ptr(FV_F_COUNT);
+    for (int i = 0; i < FV_F_COUNT; ++i) ptr[i] = f[i].data();
+    const fv_status st = fv_download(h, ptr.data());
+    if (st != FV_OK) throw Fail(std::string("fv_download: ") + fv_last_error(h), st);
+    const std::vector<double> cx = centres(c, 0), cy = centres(c, 1), cz = centres(c, 2);
+
+    const std::string num = number(nOutput);
+    std::filesystem::create_directories(d.path("result"));
+    std::ofstream out(d.path("result/output_" + num + ".tsv"));
+    if (!out.is_open()) throw Fail("Couldn't create outputFile.", FV_ERR_SYSTEM);
+    out.precision(kPrecision);
+    out << "coordinate_x" << '\t' << "coordinate_y" << '\t' << "coordinate_z" << '\t';
+    for (int k = 1; k <= N; ++k) out << "concentration_" << k << '\t';
+    out << "concentration" << '\t';
+    for (int k = 1; k <= N; ++k) out << "x_" << k << '\t';
+    for (int k = 1; k <= N; ++k) out << "density_" << k << '\t';
+    out << "density" << '\t';
+    for (int k = 1; k <= N; ++k) out << "w_" << k << '\t';
+    out << "velocity_x\tvelocity_y\tvelocity_z\tpressure\ttemperature\tk\tepsilon\ta_x\ta_y\ta_z\tb\t"
+           "turbulent_viscosity\tmomentum_x\tmomentum_y\tmomentum_z\ttotal_energy\tinternal_energy\t"
+           "Helmholtz_energy\tentropy\tsonic_speed\n";
+    for (long long i = 0; i < nc; ++i) {
+        const long long ix = i % c.n[0], iy = (i / c.n[0]) % c.n[1], iz = i / ((long long)c.n[0] * c.n[1]);
+        double cc[FV_MAX_SPECIES + 1];
+        cc[0] = 0;
+        for (int k = 1; k <= N; ++k) {
+            cc[k] = f[FV_F_CONC + k - 1][i];
+            cc[0] += cc[k];
+        }
+        const double T = f[FV_F_T][i];
+        double F, S;
+        th.FS(cc, T, F, S);
+        out << cx[ix] << '\t' << cy[iy] << '\t' << cz[iz] << '\t';
+        for (int k = 1; k <= N; ++k) out << cc[k] << '\t';
+        out << cc[0] << '\t';
+        for (int k = 1; k <= N; ++k) out << cc[k] / cc[0] << '\t';
+        for (int k = 0; k < N; ++k) out << f[FV_F_RHO_K + k][i] << '\t';
+        const double rho = f[FV_F_RHO][i];
+        out << rho << '\t';
+        for (int k = 0; k < N; ++k) out << f[FV_F_RHO_K + k][i] / rho << '\t';
+        out << f[FV_F_VX][i] << '\t' << f[FV_F_VY][i] << '\t' << f[FV_F_VZ][i] << '\t';
+        out << f[FV_F_P][i] << '\t' << T << '\t';
+        out << 0. << '\t' << 0. << '\t' << 0. << '\t' << 0. << '\t' << 0. << '\t' << 0. << '\t' << 0. << '\t';
+        out << f[FV_F_MX][i] << '\t' << f[FV_F_MY][i] << '\t' << f[FV_F_MZ][i] << '\t';
+        out << f[FV_F_E][i] << '\t' << f[FV_F_UV][i] << '\t' << F << '\t' << S << '\t'
+            << (sonic.empty() ? f[FV_F_SONIC][i] : sonic[i]) << '\n';
+    }
+    out.close();
+    {
+        std::ofstream tf(d.path("result/Time.tsv"), std::ios::app);
+        if (!tf.is_open()) throw Fail("Couldn't open ./result/Time.tsv.", FV_ERR_SYSTEM);
+        tf.precision(kPrecision);
+        tf << nOutput << '\t' << time << '\n';
+    }
+    // restart data (fieldsOutput/output_N): turbulence fields are zero without a turbulence model
+    const std::string dir = d.path("fieldsOutput/output_" + num + "/");
+    std::filesystem::create_directories(dir);
+    auto file = [&](const std::string& name) {
+        std::ofstream o(dir + name);
+        if (!o.is_open()) throw Fail("Couldn't create output file for field data " + dir + name, FV_ERR_SYSTEM);
+        o.precision(kPrecision);
+        return o;
+    };
+    {
+        auto o = file("a.dat");
+        for (long long i = 0; i < nc; ++i) o << 0. << '\t' << 0. << '\t' << 0. << '\n';
+    }
+    for (const char* name : {"b.dat", "epsilon.dat", "k.dat"}) {
+        auto o = file(name);
+        for (long long i = 0; i < nc; ++i) o << 0. << '\n';
+    }
+    {
+        auto o = file("pressure.dat");
+        for (long long i = 0; i < nc; ++i) o << f[FV_F_P][i] << '\n';
+    }
+    {
+        auto o = file("velocity.dat");
+        for (long long i = 0; i < nc; ++i) o << f[FV_F_VX][i] << '\t' << f[FV_F_VY][i] << '\t' << f[FV_F_VZ][i] << '\n';
+    }
+    for (int k = 0; k < N; ++k) {
+        auto o = file("sub_" + std::to_string(k + 1) + ".dat");
+        for (long long i = 0; i < nc; ++i) o << f[FV_F_CONC + k][i] << '\n';
+    }
+    std::cout << "./result/output_" << num << ".tsv output file is opened. Number of output: " << nOutput << '.'
+              << std::endl;
+}
+
+// restart fields of fieldsOutput/output_N (phaseInitialization.cpp:1382-1746)
+std::vector<double> column(const std::string& path, long long n, int cols, int col) {
+    std::ifstream f(path);
+    if (!f.is_open()) throw Fail("Couldn't open " + path, FV_ERR_SYSTEM);
+    std::vector<double> out(n);
+    for (long long i = 0; i < n; ++i)
+        for (int q = 0; q < cols; ++q) {
+            double v;
+            if (!(f >> v)) throw Fail("too few values in " + path);
+            if (q == col) out[i] = v;
+        }
+    return out;
+}
+
+void printConfig(const fv_config& c, const Deck& d) {
+    std::cout.precision(17);
+    std::cout << "{\"dims\": " << c.dims << ", \"n\": [" << c.n[0] << ", " << c.n[1] << ", " << c.n[2] << "]"
+              << ", \"L\": [" << c.L[0] << ", " << c.L[1] << ", " << c.L[2] << "]"
+              << ", \"n_species\": " << c.n_species << ", \"R\": " << c.R << ", \"M\": [";
+    for (int k = 0; k < c.n_species; ++k) std::cout << (k ? ", " : "") << c.M[k];
+    std::cout << "], \"Cv\": [";
+    for (int k = 0; k < c.n_species; ++k) std::cout << (k ? ", " : "") << c.Cv[k];
+    std::cout << "], \"eos\": " << c.eos << ", \"flux\": " << c.flux << ", \"limiter\": " << c.limiter
+              << ", \"courant\": " << c.courant << ", \"min_timestep\": " << c.min_timestep
+              << ", \"courant_only\": " << c.courant_only << ", \"gravity\": " << c.gravity << ", \"g\": ["
+              << c.g[0] << ", " << c.g[1] << ", " << c.g[2] << "], \"bc_vel\": [";
+    for (int p = 0; p < 6; ++p) std::cout << (p ? ", " : "") << c.bc_vel[p];
+    std::cout << "], \"bc_p\": [";
+    for (int p = 0; p < 6; ++p) std::cout << (p ? ", " : "") << c.bc_p[p];
+    std::cout << "], \"chemistry\": " << c.chemistry << ", \"const_timestep\": " << c.const_timestep
+              << ", \"t_end\": " << d.tEnd << ", \"frequency\": " << d.freq << ", \"start\": \"" << d.readFrom
+              << "\"}" << std::endl;
+}
+
+int run(const Deck& d) {
+    const fv_config& c = d.cfg;
+    const int N = c.n_species;
+    const long long nc = (long long)c.n[0] * c.n[1] * c.n[2];
+    const Thermo th(c, d.hPlanck);
+    const auto start = std::chrono::high_resolution_clock::now();
+    fv_handle* h = nullptr;
+    fv_status st = fv_create(&c, &h);
+    if (st != FV_OK) throw Fail("fv_create failed (see the messages above)", st);
+    struct Guard {
+        fv_handle* h;
+        ~Guard() { fv_destroy(h); }
+    } guard{h};
+
+    // restart set
+    std::vector<std::vector<double>> prim(N + 4, std::vector<double>(nc));
+    long long nouts = 0, nsteps = 0;
+    double time = 0;
+    const bool fresh = d.readFrom == "no" || d.readFrom == "initialisation";
+    if (fresh) {
+        for (int k = 0; k < N; ++k) std::fill(prim[k].begin(), prim[k].end(), d.zoneC[k]);
+        for (int q = 0; q < 3; ++q) std::fill(prim[N + q].begin(), prim[N + q].end(), d.zoneV[q]);
+        std::fill(prim[N + 3].begin(), prim[N + 3].end(), d.zoneP[0]);
+        std::filesystem::create_directories(d.path("result"));
+        std::ofstream(d.path("result/Time.tsv")).close();  // recreated
+    } else {
+        const long long point = std::stoll(d.readFrom);
+        std::ifstream tf(d.path("result/Time.tsv"));
+        if (!tf.is_open()) throw Fail("Couldn't open Time.tsv", FV_ERR_SYSTEM);
+        std::vector<std::string> lines;
+        std::string line;
+        while (std::getline(tf, line)) lines.push_back(line);
+        if ((long long)lines.size() <= point) throw Fail("Appropriate line wasn't found in Time.tsv", FV_ERR_SYSTEM);
+        if (point == 0) throw Fail("Time.tsv contains only one line.", FV_ERR_SYSTEM);
+        const std::string& ts = lines[point];
+        const size_t tab = ts.find('\t');
+        if (tab == std::string::npos) throw Fail("Could not find tab delimiter.");
+        nouts = std::stoll(ts.substr(0, tab));
+        time = std::stod(ts.substr(tab + 1));
+        if (d.tEnd - time <= 0)
+            throw Fail("Time of calculation lesser or equal than time of executed calculation.");
+        if (nouts != point) throw Fail("Number of output does not concur with <<readDataPoint>>.", FV_ERR_SYSTEM);
+        const bool last = (long long)lines.size() == point + 1;
+        {
+            std::ofstream nf(d.path("result/Time.tsv"));
+            for (long long q = 0; q <= point; ++q) nf << lines[q] << '\n';
+        }
+        nsteps = nouts * d.freq;
+        if (last) {
+            // the step count of timeOfCalculation.tsv; 0 when the file has no "steps" word,
+            // nouts * frequency when the file is missing or the count unreadable
+            std::ifstream sf(d.path("timeOfCalculation.tsv"));
+            if (sf.is_open()) {
+                nsteps = 0;
+                std::string w;
+                while (sf >> w)
+                    if (w == "steps") {
+                        try {
+                            if (!(sf >> w)) throw std::invalid_argument("no count");
+                            nsteps = std::stoll(w);
+                        } catch (...) {
+                            nsteps = nouts * d.freq;
+                        }
+                        break;
+                    }
+            }
+        }
+        const std::string dir = d.path("fieldsOutput/output_" + number(point) + "/");
+        for (int k = 0; k < N; ++k) prim[k] = column(dir + "sub_" + std::to_string(k + 1) + ".dat", nc, 1, 0);
+        for (int q = 0; q < 3; ++q) prim[N + q] = column(dir + "velocity.dat", nc, 3, q);
+        prim[N + 3] = column(dir + "pressure.dat", nc, 1, 0);
+    }
+    std::vector<const double*> pp(N + 4);
+    for (int q = 0; q < N + 4; ++q) pp[q] = prim[q].data();
+    if ((st = fv_upload(h, pp.data())) != FV_OK) throw Fail(std::string("fv_upload: ") + fv_last_error(h), st);
+    // first step: the minimal (or constant) step, not beyond the time of calculation
+    const double dt0 = std::min(c.const_timestep > 0 ? c.const_timestep : d.minTime, d.tEnd);
+    if ((st = fv_set_time(h, time, dt0)) != FV_OK) throw Fail("fv_set_time", st);
+    std::vector<double> sonic;
+    if (c.const_timestep > 0) {
+        sonic.resize(nc);
+        std::vector<double*> only(FV_F_COUNT, nullptr);
+        only[FV_F_SONIC] = sonic.data();
+        if ((st = fv_download(h, only.data())) != FV_OK) throw Fail(std::string("fv_download: ") + fv_last_error(h), st);
+    }
+
+    if (fresh) writeOutput(d, h, nouts, time, th, sonic);
+    nouts++;
+    if (d.readFrom == "initialisation") return 0;
+
+    while (time < d.tEnd) {
+        const long long toGo = std::max(1LL, nouts * d.freq - nsteps);
+        fv_run_stats rs{};
+        st = fv_run(h, d.tEnd, toGo, &rs);
+        nsteps += rs.steps;
+        time = rs.time;
+        if (st != FV_OK) {
+            std::clog << fv_last_error(h) << std::endl << "Step number " << nsteps << '.' << std::endl;
+            std::clog << "Emergency output." << std::endl;
+            writeOutput(d, h, nouts, time, th, sonic);
+            return st;
+        }
+        if (rs.steps == 0) break;
+        if (nsteps == nouts * d.freq || time == d.tEnd) {
+            std::cout << "Time = " << time << std::endl << "Step number = " << nsteps << std::endl;
+            writeOutput(d, h, nouts, time, th, sonic);
+            nouts++;
+        }
+    }
+    std::cout << "End" << std::endl;
+    std::ofstream tc(d.path("timeOfCalculation.tsv"));
+    tc.precision(kPrecision);
+    tc << "Time of execution" << std::endl
+       << std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::high_resolution_clock::now() - start)
+              .count()
+       << std::endl
+       << "Number of steps" << std::endl
+       << nsteps << std::endl;
+    // the reference's per-stage timers; the fused kernels have no separate stages
+    for (const char* stage : {"Time of TVD stage work:", "Time of Hancock stage work:", "Time of Riemann solver work:",
+                              "Time of time integration work:", "Time of Diffusion solver work:"})
+        tc << stage << std::endl << 0 << std::endl;
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    bool printOnly = false;
+    std::string dir = ".";
+    for (int i = 1; i < argc; ++i) {
+        const std::string a = argv[i];
+        if (a == "--print-config") printOnly = true;
+        else if (a == "-h" || a == "--help") {
+            std::cout << "usage: fvrun [--print-config] [deck_directory]" << std::endl;
+            return 0;
+        } else dir = a;
+    }
+    try {
+        const Deck d = readDeck(dir);
+        if (printOnly) {
+            printConfig(d.cfg, d);
+            return 0;
+        }
+        return run(d);
+    } catch (const Fail& e) {
+        std::clog << e.what() << std::endl;
+        return e.code ? e.code : 1;
+    } catch (const std::exception& e) {
+        std::clog << e.what() << std::endl;
+        return FV_ERR_SYSTEM;
+    }
+}

@@ -1,0 +1,113 @@
+"""Replays a task-deck fixture (``golden/deck_<name>.npz``) with a driver binary and compares the
+files it writes with the reference solver's.
+
+A fixture holds the task directory as the reference read it, the ``set/main.txt`` of every run
+made in that directory and every file the reference left behind (``golden/make_deck_golden.py``).
+``timeOfCalculation.tsv`` is compared without its measured milliseconds.  Fixtures with a
+non-zero ``tolerance`` (the chemistry deck) are compared value by value to that relative
+tolerance; all others byte for byte.
+"""
+
+import os
+import subprocess
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def fixtures():
+    return sorted(f[5:-4] for f in os.listdir(GOLDEN) if f.startswith("deck_") and f.endswith(".npz"))
+
+
+def load(name):
+    return np.load(os.path.join(GOLDEN, f"deck_{name}.npz"))
+
+
+def _write(d, rel, data):
+    path = os.path.join(d, rel)
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    with open(path, "wb") as f:
+        f.write(data)
+
+
+def unpack_inputs(z, d):
+    for k in z.files:
+        if k.startswith("in:"):
+            _write(d, k[3:].replace("|", os.sep), z[k].tobytes())
+
+
+def _tree(d):
+    found = {}
+    for root, _, names in os.walk(d):
+        for n in names:
+            full = os.path.join(root, n)
+            rel = os.path.relpath(full, d)
+            if not rel.startswith("set" + os.sep):
+                with open(full, "rb") as f:
+                    found[rel] = f.read()
+    return found
+
+
+def _numbers_close(a: bytes, b: bytes, tol: float, rel: str):
+    la, lb = a.decode().split("\n"), b.decode().split("\n")
+    if len(la) != len(lb):
+        return f"{rel}: {len(la)} lines, reference {len(lb)}"
+    for i, (x, y) in enumerate(zip(la, lb)):
+        tx, ty = x.split("\t"), y.split("\t")
+        if len(tx) != len(ty):
+            return f"{rel} line {i}: {len(tx)} columns, reference {len(ty)}"
+        for j, (u, v) in enumerate(zip(tx, ty)):
+            try:
+                fu, fv = float(u), float(v)
+            except ValueError:
+                if u != v:
+                    return f"{rel} line {i} column {j}: {u!r}, reference {v!r}"
+                continue
+            if abs(fu - fv) > tol * max(abs(fu), abs(fv), 1e-300):
+                return f"{rel} line {i} column {j}: {u}, reference {v}"
+    return None
+
+
+def _first_difference(a: bytes, b: bytes, rel: str):
+    la, lb = a.decode().split("\n"), b.decode().split("\n")
+    for i in range(min(len(la), len(lb))):
+        if la[i] != lb[i]:
+            return f"{rel} line {i}:\n  got       {la[i][:300]}\n  reference {lb[i][:300]}"
+    return f"{rel}: {len(la)} lines, reference {len(lb)}"
+
+
+def replay(driver, name, d, timeout=600):
+    """Runs every run of fixture ``name`` in directory ``d`` with ``driver``; returns a list of
+    differences from the reference's files (empty when they agree)."""
+    z = load(name)
+    unpack_inputs(z, d)
+    problems = []
+    for r in range(int(z["runs"])):
+        _write(d, os.path.join("set", "main.txt"), z[f"run{r}:main.txt"].tobytes())
+        res = subprocess.run([driver, d], capture_output=True, text=True, timeout=timeout)
+        if res.returncode != int(z["rc"][r]):
+            problems.append(f"run {r}: exit {res.returncode}, reference {int(z['rc'][r])}\n"
+                            + res.stdout[-1500:] + res.stderr[-1500:])
+            return problems
+    want = {k[4:].replace("|", os.sep): z[k].tobytes() for k in z.files if k.startswith("out:")}
+    got = _tree(d)
+    if sorted(got) != sorted(want):
+        problems.append(f"files: extra {sorted(set(got) - set(want))}, missing {sorted(set(want) - set(got))}")
+    tol = float(z["tolerance"])
+    for rel, data in sorted(want.items()):
+        if rel not in got:
+            continue
+        if rel == "timeOfCalculation.tsv":
+            g, w = got[rel].decode().split("\n"), data.decode().split("\n")
+            del g[1], w[1]  # measured milliseconds
+            if g != w:
+                problems.append(f"{rel}: {g}, reference {w}")
+        elif tol == 0:
+            if got[rel] != data:
+                problems.append(_first_difference(got[rel], data, rel))
+        else:
+            p = _numbers_close(got[rel], data, tol, rel)
+            if p:
+                problems.append(p)
+    return problems

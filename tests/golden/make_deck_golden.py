@@ -1,0 +1,154 @@
+"""Regenerates the task-deck fixtures ``deck_<name>.npz`` by running the reference solver.
+
+Each fixture holds a complete task directory as the reference reads it (``set/*.txt`` and, for
+restart decks, ``fieldsOutput/output_000001`` + ``result/Time.tsv``), the ``set/main.txt`` of
+every run made in that directory (a second run restarts from an output of the first), and every
+file the reference left behind: ``result/output_<NNNNNN>.tsv``, ``result/Time.tsv``,
+``fieldsOutput/output_<NNNNNN>/*.dat`` and ``timeOfCalculation.tsv``.  The GPU driver test
+replays the same runs with ``schemi_b200/lib/fvrun`` and compares the files byte for byte
+(numerically for the chemistry deck).
+
+The reference is compiled from its own sources by ``oracle/Makefile`` (``make -C oracle ref``);
+the decks are written by ``schemi_b200.deck``.
+
+    python tests/golden/make_deck_golden.py
+"""
+
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from schemi_b200 import cases  # noqa: E402
+from schemi_b200.case import BC, Case, PatchBC  # noqa: E402
+from schemi_b200.deck import write_deck  # noqa: E402
+import oracle as O  # noqa: E402
+
+START_KEY = "#Start_From_Time-Step"
+END_KEY = "#Time_of_calculation"
+
+
+def _t_after(case, prim, steps, frac):
+    """End time that the oracle reaches after ``steps`` steps plus ``frac`` of the next step."""
+    oc = O.OracleCase(case)
+    oc.upload(prim)
+    for _ in range(steps):
+        oc.step()
+    t, dt = oc.time()
+    return t + frac * dt
+
+
+def _set_main(text, **values):
+    lines = text.split("\n")
+    keys = {"start": START_KEY, "t_end": END_KEY}
+    for name, v in values.items():
+        i = lines.index(keys[name])
+        lines[i + 1] = v
+    return "\n".join(lines)
+
+
+def deck_cases():
+    """(name, case, prim, frequency, restart, [main.txt edits per run], tolerance)."""
+    out = []
+    # Kelvin-Helmholtz 8x8, slip walls: restart deck, then a second run from output 2
+    c, p = cases.kelvin_helmholtz_2d(n=8, periodic=False)
+    c.t_end = _t_after(c, p, 10, 0.37)
+    out.append(("kh8_restart", c, p, 4, True, [{}, {"start": "2", "t_end": repr(c.t_end * 1.6)}], 0.0))
+    # two-species tube from the uniform outer zone, driven through a fixed-value inflow
+    c, p = cases.shock_tube_1d(n=40)
+    p = [np.full_like(a, float(np.mean(a))) for a in p]
+    c.bc["tail"] = PatchBC([BC("fixedValueCell", 0.7), BC("fixedValueCell", 0.3)],
+                           BC("fixedValueCell", (0.3, 0.0, 0.0)), BC("fixedValueCell", 0.9))
+    c.bc["point"] = PatchBC([BC("freeBoundary"), BC("freeBoundary")], BC("freeBoundary"), BC("freeBoundary"))
+    c.t_end = _t_after(c, p, 14, 0.61)
+    out.append(("tube40_fresh", c, p, 5, False, [{}], 0.0))
+    out.append(("tube40_initialisation", c, p, 5, False, [{"start": "initialisation"}], 0.0))
+    # Rayleigh-Taylor 8x16 with growing gravity
+    c, p = cases.rayleigh_taylor_2d(nx=8, ny=16, modes=2)
+    c.g_delta = (0.0, -0.05, 0.0)
+    c.t_end = _t_after(c, p, 12, 0.5)
+    out.append(("rt8x16_gravity", c, p, 5, True, [{}], 0.0))
+    # three-species van der Waals mixture, 6x6 slip box
+    c3, p3 = cases.reacting_shear_3d(n=6, periodic=False)
+    c = Case(dims=2, n=(6, 6, 1), L=(1.0, 1.0, 1.0), species=c3.species, t_end=1.0, R_units="SI",
+             eos="vanDerWaals", limiter="vanLeer", name="vdw2d")
+    for k in ("tail", "point", "right", "left"):
+        c.bc[k] = PatchBC.uniform("slip", 3)
+    p = [a.reshape(6, 6, 6)[0].ravel() for a in p3]
+    c.t_end = _t_after(c, p, 7, 0.8)
+    out.append(("vdw3_6x6", c, p, 3, True, [{}], 0.0))
+    # constant time step: no CFL block, sonic speeds stay those of the initial state
+    c, p = cases.kelvin_helmholtz_2d(n=8, periodic=False, limiter="superbee")
+    oc = O.OracleCase(c)
+    oc.upload(p)
+    oc.step()
+    c.const_timestep = 0.5 * oc.time()[1]
+    c.t_end = 4.5 * c.const_timestep
+    out.append(("kh8_const_dt", c, p, 2, True, [{}], 0.0))
+    # Cl2 dissociation (chemistry pass): compared to a relative tolerance
+    c, p = cases.chlorine_dissociation_2d(4)
+    c.t_end = _t_after(c, p, 6, 0.5)
+    out.append(("cl2_4x4", c, p, 2, True, [{}], 1e-10))
+    return out
+
+
+def _files(d):
+    found = {}
+    for root, _, names in os.walk(d):
+        for n in names:
+            full = os.path.join(root, n)
+            found[os.path.relpath(full, d)] = open(full, "rb").read()
+    return found
+
+
+def _key(prefix, rel):
+    return prefix + ":" + rel.replace(os.sep, "|")
+
+
+def main():
+    binary = O.REF_BIN_PATCHED
+    if not os.path.exists(binary):
+        raise SystemExit(f"{binary} missing: run make -C oracle ref")
+    for name, case, prim, freq, restart, runs, tol in deck_cases():
+        d = tempfile.mkdtemp(prefix="schemi_deck_")
+        try:
+            write_deck(case, d, prim, frequency_of_output=freq, restart=restart)
+            inputs = _files(d)
+            base = inputs[os.path.join("set", "main.txt")].decode()
+            data = {_key("in", rel): np.frombuffer(b, dtype=np.uint8) for rel, b in inputs.items()}
+            rcs = []
+            for r, edits in enumerate(runs):
+                main_txt = _set_main(base, **edits)
+                with open(os.path.join(d, "set", "main.txt"), "w") as f:
+                    f.write(main_txt)
+                data[f"run{r}:main.txt"] = np.frombuffer(main_txt.encode(), dtype=np.uint8)
+                res = subprocess.run([binary], cwd=d, stdin=subprocess.DEVNULL, stdout=subprocess.PIPE,
+                                     stderr=subprocess.STDOUT, timeout=600)
+                rcs.append(res.returncode)
+                if res.returncode != 0:
+                    raise RuntimeError(f"{name} run {r}: reference failed\n" +
+                                       res.stdout.decode(errors="replace")[-2000:])
+            for rel, b in _files(d).items():
+                if rel.startswith("set" + os.sep):
+                    continue
+                data[_key("out", rel)] = np.frombuffer(b, dtype=np.uint8)
+            data["runs"] = np.int64(len(runs))
+            data["rc"] = np.asarray(rcs, dtype=np.int64)
+            data["tolerance"] = np.float64(tol)
+            np.savez_compressed(os.path.join(HERE, f"deck_{name}.npz"), **data)
+            outs = sorted(k for k in data if k.startswith("out:result|output_"))
+            print(f"deck_{name}: {len(runs)} run(s), outputs {[k.split('_')[-1] for k in outs]}")
+        finally:
+            shutil.rmtree(d, ignore_errors=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -67,6 +67,9 @@ def golden_cases():
     out.append(("cl2_4x4_vdw_gs", c, p, 10, [1, 2, 10]))
     c, p = cases.chlorine_dissociation_2d(4, eos="ideal")
     out.append(("cl2_4x4_ideal_gs", c, p, 10, [1, 10]))
+    c, p = cases.chlorine_dissociation_2d(4)
+    c.const_timestep = 2e-5  # #Constant_timestep: main skips its CFL block
+    out.append(("cl2_4x4_vdw_const_dt", c, p, 8, [1, 8]))
     for solver, tag in (("Jacobi", "jacobi"), ("GaussElimination", "ge"), ("conjugateGradient", "cg")):
         c, p = cases.chlorine_dissociation_2d(4, solver=solver)
         out.append((f"cl2_4x4_vdw_{tag}", c, p, 6, [1, 6]))

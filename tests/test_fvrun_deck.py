@@ -1,0 +1,145 @@
+"""Task-deck driver (schemi_b200/lib/fvrun): deck parsing on the CPU.
+
+``fvrun --print-config`` reads a deck the way the reference's main and phaseInitialization do
+(Schemi/main/Schemi.cpp:83-310, Schemi/src/thermodynamics/phaseInitialization.cpp:256-446) and
+prints the fv_config it maps to; these tests write decks with ``schemi_b200.deck`` and check that
+the driver recovers the case, and that decks outside the step (diffusion, zones, unknown names)
+are refused with the reference's messages or the driver's own.  The same driver source linked
+against the CPU oracle (oracle/lib/fvrun_oracle) replays the reference's deck fixtures, so the
+host side -- time loop, output schedule, restart, file writer -- is checked without a GPU.
+"""
+
+import json
+import os
+import subprocess
+
+import pytest
+
+from deck_replay import fixtures, load, replay, unpack_inputs
+from schemi_b200 import cases
+from schemi_b200.build import DRIVER
+from schemi_b200.case import BC, PatchBC
+from schemi_b200.deck import write_deck
+
+
+def _driver():
+    if not os.path.exists(DRIVER):
+        pytest.fail(f"{DRIVER} is not built (python -m schemi_b200.build)")
+    return DRIVER
+
+
+def _print_config(d):
+    res = subprocess.run([_driver(), "--print-config", d], capture_output=True, text=True, timeout=60)
+    return res
+
+
+def _deck_cases():
+    out = []
+    c, p = cases.kelvin_helmholtz_2d(n=8, periodic=False)
+    out.append(("kh", c, p))
+    c, p = cases.rayleigh_taylor_2d(nx=8, ny=16, modes=2)
+    c.g_delta = (0.0, -0.05, 0.0)
+    out.append(("rt", c, p))
+    c, p = cases.chlorine_dissociation_2d(4)
+    out.append(("cl2", c, p))
+    c, p = cases.shock_tube_1d(n=40)
+    c.bc["tail"] = PatchBC([BC("fixedValueCell", 0.7), BC("fixedValueCell", 0.3)],
+                           BC("fixedValueCell", (0.3, 0.0, 0.0)), BC("fixedValueCell", 0.9))
+    c.flux, c.limiter, c.courant_only, c.const_timestep = "HLL", "Schmidtmann", True, 1e-4
+    out.append(("tube", c, p))
+    return out
+
+
+@pytest.mark.parametrize("name,case,prim", _deck_cases(), ids=[c[0] for c in _deck_cases()])
+def test_print_config_matches_case(tmp_path, name, case, prim):
+    write_deck(case, str(tmp_path), prim, frequency_of_output=3, restart=True)
+    res = _print_config(str(tmp_path))
+    assert res.returncode == 0, res.stderr
+    got = json.loads(res.stdout.strip().splitlines()[-1])
+    want = case.fv_config()
+    N = case.n_species
+    assert got["dims"] == want.dims
+    assert got["n"] == list(want.n)
+    assert got["L"] == list(want.L)
+    assert got["n_species"] == N
+    assert got["R"] == want.R
+    assert got["M"] == list(want.M)[:N]
+    assert got["Cv"] == list(want.Cv)[:N]
+    for key in ("eos", "flux", "limiter", "courant_only", "gravity", "chemistry"):
+        assert got[key] == getattr(want, key), key
+    assert got["courant"] == want.courant
+    assert got["min_timestep"] == want.min_timestep
+    # a case without a constant step is written with a negative #Constant_timestep
+    if want.const_timestep > 0:
+        assert got["const_timestep"] == want.const_timestep
+    else:
+        assert got["const_timestep"] <= 0
+    assert got["g"] == list(want.g)
+    assert got["bc_vel"] == list(want.bc_vel)
+    assert got["bc_p"] == list(want.bc_p)
+    assert got["t_end"] == case.t_end
+    assert got["frequency"] == 3
+    assert got["start"] == "1"
+
+
+def _edit(path, key, value):
+    lines = open(path).read().split("\n")
+    lines[lines.index(key) + 1] = value
+    open(path, "w").write("\n".join(lines))
+
+
+@pytest.mark.parametrize("file,key,value,message", [
+    ("main.txt", "#Diffusion_flag", "on", "Diffusion"),
+    ("main.txt", "#Turbulence_flag", "yes", "Turbulence"),
+    ("main.txt", "#Approximation_order", "ThirdOrder", "SecondOrder"),
+    ("main.txt", "#TVD_limiter_type", "vanLeer3", "limiter"),
+    ("main.txt", "#Type_of_flow_solver", "KT", "HLLC"),
+    ("main.txt", "#Source_timestep_correction", "Courant", "Wrong format of time-step parameters settings"),
+    ("main.txt", "#Source_timestep_correction", "Implicit=0.25,0.5", "Unknown source time-step flag."),
+    ("main.txt", "#Defines_universal_gas_constant", "Planck", "Unknown type of universal gas constant."),
+    ("main.txt", "#Reconstruction", "cubic", "Unknown reconstruction flag."),
+    ("zonesDescription.txt", "#Number_of_zones", "1", "outer zone"),
+    ("g.txt", "#Free_fall_acceleration_flag", "maybe", "Unknown gravitation flag."),
+    ("chemicalKinetics.txt", "#Type_of_chemical_reaction", "H2Cl2Combustion", "not implemented"),
+])
+def test_unsupported_deck_refused(tmp_path, file, key, value, message):
+    c, p = cases.kelvin_helmholtz_2d(n=8, periodic=False)
+    write_deck(c, str(tmp_path), p, restart=True)
+    _edit(os.path.join(tmp_path, "set", file), key, value)
+    res = _print_config(str(tmp_path))
+    assert res.returncode != 0
+    assert message in res.stderr
+
+
+def test_missing_deck_file(tmp_path):
+    res = _print_config(str(tmp_path))
+    assert res.returncode != 0
+    assert "g.txt not found." in res.stderr
+
+
+def test_deck_fixtures_parse(tmp_path):
+    """Every committed deck fixture parses (its inputs written out, then --print-config)."""
+    names = fixtures()
+    assert len(names) >= 6
+    for name in names:
+        z = load(name)
+        d = tmp_path / name
+        unpack_inputs(z, str(d))
+        for r in range(int(z["runs"])):
+            (d / "set" / "main.txt").write_bytes(z[f"run{r}:main.txt"].tobytes())
+            res = _print_config(str(d))
+            assert res.returncode == 0, (name, res.stderr)
+
+
+ORACLE_DRIVER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "lib",
+                             "fvrun_oracle")
+
+
+@pytest.mark.parametrize("name", fixtures())
+def test_host_io_on_oracle_matches_reference_files(tmp_path, name):
+    """The driver's deck reader, time loop, output schedule, restart and file writer, linked
+    against the CPU oracle through the same C-ABI calls, reproduce the reference's files."""
+    if not os.path.exists(ORACLE_DRIVER):
+        subprocess.run(["make", "-s", "-C", os.path.dirname(os.path.dirname(ORACLE_DRIVER))], check=True)
+    problems = replay(ORACLE_DRIVER, name, str(tmp_path))
+    assert not problems, "\n".join(problems)

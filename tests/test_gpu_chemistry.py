@@ -39,7 +39,8 @@ def _compare(out, ref, fields, tol, what):
             assert linf <= tol, f"{what} field {f}: rel Linf {linf:.3e}"
 
 
-@pytest.mark.parametrize("name", ["cl2_4x4_vdw_gs", "cl2_4x4_ideal_gs", "cl2_4x4_vdw_jacobi", "cl2_4x4_vdw_ge"])
+@pytest.mark.parametrize("name", ["cl2_4x4_vdw_gs", "cl2_4x4_ideal_gs", "cl2_4x4_vdw_jacobi", "cl2_4x4_vdw_ge",
+                                  "cl2_4x4_vdw_const_dt"])
 def test_cl2_matches_reference_fixture(fv, name):
     cases = {c[0]: c for c in load_cases()}
     _, case, prim, data = cases[name]
