@@ -5,7 +5,8 @@ A fixture holds the task directory as the reference read it, the ``set/main.txt`
 made in that directory and every file the reference left behind (``golden/make_deck_golden.py``).
 ``timeOfCalculation.tsv`` is compared without its measured milliseconds.  Fixtures with a
 non-zero ``tolerance`` (the chemistry deck) are compared value by value to that relative
-tolerance; all others byte for byte.
+tolerance, velocities and momenta on the scale of the largest sonic speed (and density); all
+others byte for byte.
 """
 
 import os
@@ -49,10 +50,34 @@ def _tree(d):
     return found
 
 
-def _numbers_close(a: bytes, b: bytes, tol: float, rel: str):
+def _velocity_scale(want):
+    """Largest sonic speed and density of the reference's outputs: velocities and momenta are
+    compared on these scales, since a flow at rest carries only rounding-level velocities."""
+    c_max, rho_max = 0.0, 0.0
+    for rel, data in want.items():
+        if os.path.basename(rel).startswith("output_") and rel.endswith(".tsv"):
+            lines = data.decode().strip("\n").split("\n")
+            head = lines[0].split("\t")
+            rows = np.array([[float(x) for x in ln.split("\t")] for ln in lines[1:]])
+            c_max = max(c_max, float(np.abs(rows[:, head.index("sonic_speed")]).max()))
+            rho_max = max(rho_max, float(np.abs(rows[:, head.index("density")]).max()))
+    return c_max, rho_max
+
+
+def _numbers_close(a: bytes, b: bytes, tol: float, rel: str, scale):
     la, lb = a.decode().split("\n"), b.decode().split("\n")
     if len(la) != len(lb):
         return f"{rel}: {len(la)} lines, reference {len(lb)}"
+    c_max, rho_max = scale
+    floors = {}
+    if os.path.basename(rel) == "velocity.dat":
+        floors = {0: c_max, 1: c_max, 2: c_max}
+    elif rel.endswith(".tsv") and la:
+        for j, name in enumerate(lb[0].split("\t")):
+            if name.startswith("velocity_"):
+                floors[j] = c_max
+            elif name.startswith("momentum_"):
+                floors[j] = c_max * rho_max
     for i, (x, y) in enumerate(zip(la, lb)):
         tx, ty = x.split("\t"), y.split("\t")
         if len(tx) != len(ty):
@@ -64,7 +89,7 @@ def _numbers_close(a: bytes, b: bytes, tol: float, rel: str):
                 if u != v:
                     return f"{rel} line {i} column {j}: {u!r}, reference {v!r}"
                 continue
-            if abs(fu - fv) > tol * max(abs(fu), abs(fv), 1e-300):
+            if abs(fu - fv) > tol * max(abs(fu), abs(fv), floors.get(j, 0.0), 1e-300):
                 return f"{rel} line {i} column {j}: {u}, reference {v}"
     return None
 
@@ -95,6 +120,7 @@ def replay(driver, name, d, timeout=600):
     if sorted(got) != sorted(want):
         problems.append(f"files: extra {sorted(set(got) - set(want))}, missing {sorted(set(want) - set(got))}")
     tol = float(z["tolerance"])
+    scale = _velocity_scale(want) if tol > 0 else None
     for rel, data in sorted(want.items()):
         if rel not in got:
             continue
@@ -107,7 +133,7 @@ def replay(driver, name, d, timeout=600):
             if got[rel] != data:
                 problems.append(_first_difference(got[rel], data, rel))
         else:
-            p = _numbers_close(got[rel], data, tol, rel)
+            p = _numbers_close(got[rel], data, tol, rel, scale)
             if p:
                 problems.append(p)
     return problems
