@@ -31,7 +31,9 @@ def _cache_path() -> str:
 
 def _key(case, device: str) -> str:
     n = "x".join(str(v) for v in case.n[: case.dims])
-    return f"{case.dims}d|{n}|ns{case.n_species}|{case.eos}|{case.precision}|{device}"
+    # FP32-flux 2D cases run the warp-strip march, whose shapes are timed separately
+    kind = "|warp-strip" if case.dims == 2 and case.precision == "f32flux" else ""
+    return f"{case.dims}d|{n}|ns{case.n_species}|{case.eos}|{case.precision}|{device}{kind}"
 
 
 def load_cache() -> Dict[str, dict]:

@@ -55,6 +55,45 @@ struct fv_batch {
 
 namespace {
 
+// Tiles of every case for the ensemble kernel: the warp-strip march when every case runs it
+// (FP32-flux 2D cases without a transverse velocity), else the CTA march.  Each case's P is the
+// handle's with the kernel choice written into it, so tile counts and kernels agree.
+void layoutTiles(fv_batch* b) {
+    bool warp = true;
+    for (fv_handle* h : b->cases) warp = warp && warpStripMarch(h->P);
+    b->shape.warp = warp ? 1 : 0;
+    long long base = 0;
+    for (size_t i = 0; i < b->cases.size(); ++i) {
+        BatchCase& bc = b->host[i];
+        bc.P = b->cases[i]->P;
+        bc.P.warp2d = warp ? 1 : 0;
+        const StepParams& P = bc.P;
+        const int cols = marchTileColumns(P, b->shape.bx);
+        bc.tiles[0] = (P.n[0] + cols - 1) / cols;
+        if (P.dims == 2) {
+            bc.tiles[1] = 1;
+            bc.tiles[2] = (P.n[1] + b->shape.rows - 1) / b->shape.rows;
+        } else {
+            bc.tiles[1] = (P.n[1] + b->shape.by - 3) / (b->shape.by - 2);
+            bc.tiles[2] = (P.n[2] + b->shape.rows - 1) / b->shape.rows;
+        }
+        bc.nTiles = bc.tiles[0] * bc.tiles[1] * bc.tiles[2];
+        bc.tileBase = base;
+        base += bc.nTiles;
+    }
+    b->totalTiles = base;
+}
+
+cudaError_t configureGrid(fv_batch* b) {
+    int grid = 0;
+    const int n = (int)b->cases.size();
+    cudaError_t e = b->precision == FV_PREC_F64
+                        ? launchBatchF64(b->ns, b->eos, b->dims, nullptr, n, 0, b->shape, &grid, nullptr)
+                        : launchBatchF32(b->ns, b->eos, b->dims, nullptr, n, 0, b->shape, &grid, nullptr);
+    if (e == cudaSuccess) b->grid = grid;
+    return e;
+}
+
 cudaError_t enqueueEnsembleStep(fv_batch* b) {
     int grid = b->grid;
     cudaError_t e = b->precision == FV_PREC_F64
@@ -117,40 +156,22 @@ fv_status fv_batch_create(fv_handle* const* handles, int n_cases, fv_batch** out
             }
         }
     }
-    long long base = 0;
     for (fv_handle* h : b->cases) {
         BatchCase bc;
         memset(&bc, 0, sizeof(bc));
-        bc.P = h->P;
         bc.ck = h->ck;
         bc.prim0 = h->prim0;
         bc.blockMax = h->blockMax;
-        const StepParams& P = h->P;
-        bc.tiles[0] = (P.n[0] + b->shape.bx - 3) / (b->shape.bx - 2);
-        if (P.dims == 2) {
-            bc.tiles[1] = 1;
-            bc.tiles[2] = (P.n[1] + b->shape.rows - 1) / b->shape.rows;
-        } else {
-            bc.tiles[1] = (P.n[1] + b->shape.by - 3) / (b->shape.by - 2);
-            bc.tiles[2] = (P.n[2] + b->shape.rows - 1) / b->shape.rows;
-        }
-        bc.nTiles = bc.tiles[0] * bc.tiles[1] * bc.tiles[2];
-        bc.tileBase = base;
-        base += bc.nTiles;
         b->host.push_back(bc);
     }
-    b->totalTiles = base;
+    layoutTiles(b);
     cudaError_t e;
     if ((e = cudaMalloc(&b->dev, sizeof(BatchCase) * n_cases)) != cudaSuccess) return bail("case table", e);
     if ((e = cudaMalloc(&b->activeDev, sizeof(int))) != cudaSuccess) return bail("counter", e);
     if ((e = cudaMallocHost(&b->activeHost, sizeof(int))) != cudaSuccess) return bail("counter mirror", e);
     if ((e = cudaEventCreate(&b->ev0)) != cudaSuccess) return bail("event", e);
     if ((e = cudaEventCreate(&b->ev1)) != cudaSuccess) return bail("event", e);
-    int grid = 0;
-    e = b->precision == FV_PREC_F64 ? launchBatchF64(b->ns, b->eos, b->dims, nullptr, n_cases, 0, b->shape, &grid, nullptr)
-                                    : launchBatchF32(b->ns, b->eos, b->dims, nullptr, n_cases, 0, b->shape, &grid, nullptr);
-    if (e != cudaSuccess) return bail("kernel configuration", e);
-    b->grid = grid;
+    if ((e = configureGrid(b)) != cudaSuccess) return bail("kernel configuration", e);
     *out = b;
     return FV_OK;
 }
@@ -173,15 +194,25 @@ fv_status fv_batch_run(fv_batch* b, const double* t_end, long long max_steps, fv
     // per-case clocks: end time, first step clamp (Schemi.cpp:664-670), buffer pair and step base
     for (int i = 0; i < n; ++i)
         if (cudaStreamSynchronize(b->cases[i]->stream) != cudaSuccess) return FV_ERR_SYSTEM;
+    // an upload may have changed a case's carried momentum count, and with it the kernel choice
+    const int warpBefore = b->shape.warp;
+    const long long tilesBefore = b->totalTiles;
+    layoutTiles(b);
+    if (b->shape.warp != warpBefore || b->totalTiles != tilesBefore) {
+        if (b->graph) {
+            cudaGraphExecDestroy(b->graph);
+            b->graph = nullptr;
+        }
+        if (configureGrid(b) != cudaSuccess) return FV_ERR_SYSTEM;
+    }
     for (int i = 0; i < n; ++i) {
         fv_handle* h = b->cases[i];
-        b->host[i].P = h->P;  // refreshed: an upload may have changed the carried momentum count
         DevClock c;
         cudaError_t e = cudaMemcpy(&c, h->ck, sizeof(DevClock), cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) return FV_ERR_SYSTEM;
         c.t_end = t_end[i];
         c.done = !(c.time < t_end[i]) || c.err;
-        c.dt = std::min(c.dt_free, t_end[i] - c.time);
+        c.dt = (c.time + c.dt_free) > t_end[i] ? t_end[i] - c.time : c.dt_free;
         if ((e = cudaMemcpy(h->ck, &c, sizeof(DevClock), cudaMemcpyHostToDevice)) != cudaSuccess) return FV_ERR_SYSTEM;
         BatchCase& bc = b->host[i];
         bc.U0 = h->U[h->cur];

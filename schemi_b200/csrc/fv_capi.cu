@@ -483,6 +483,9 @@ fv_status fv_create(const fv_config* cfg, fv_handle** out) {
     P.nmom = cfg->dims;
     // rows are staged with 16-byte aligned bulk copies: field and row pitches must be even
     P.tma = (P.n[0] % 2 == 0) ? 1 : 0;
+    // the warp-strip march addresses fields with 32-bit offsets
+    P.warp2d = (cfg->precision == FV_PREC_F32_FLUX && cfg->dims == 2 &&
+                P.ncell * (cfg->n_species + 5) < (1LL << 31)) ? 1 : 0;
     h->path = choosePath(*cfg);
     h->chem.mech = cfg->chemistry;
     h->chem.solver = cfg->chem_solver;
@@ -593,6 +596,13 @@ static fv_status setMomentumComponents(fv_handle* h) {
         FV_CUDA(h, cudaMemcpyAsync(&flag, &h->ck->pad, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
         FV_CUDA(h, cudaStreamSynchronize(h->stream));
         if (flag) nmom = 3;
+        // a fixed-value patch velocity with a transverse component feeds the transverse momentum
+        for (int p = 0; p < 6; ++p) {
+            const int t = h->cfg.bc_vel[p];
+            if (t != FV_BC_FIXED_CELL && t != FV_BC_FIXED_SURFACE) continue;
+            for (int d = h->cfg.dims; d < 3; ++d)
+                if (h->cfg.bc_vel_value[p][d] != 0.0) nmom = 3;
+        }
     }
     if (nmom != h->P.nmom) {
         h->P.nmom = nmom;
@@ -884,7 +894,8 @@ fv_status fv_time_step_kernel(fv_handle* h, int iters, float* ms_per_step) {
 namespace fv {
 long long marchBlocks(const StepParams& P, const MarchShape& s) {
     if (P.dims < 2) return 0;
-    const long long gx = (P.n[0] + s.bx - 3) / (s.bx - 2);
+    const int cols = marchTileColumns(P, s.bx);
+    const long long gx = (P.n[0] + cols - 1) / cols;
     if (P.dims == 2) return gx * ((P.n[1] + s.rows - 1) / s.rows);
     const long long gy = (P.n[1] + s.by - 3) / (s.by - 2);
     return gx * gy * ((P.n[2] + s.rows - 1) / s.rows);

@@ -46,6 +46,7 @@ struct StepParams {
     long long stride;       // distance between fields of U
     int nmom;               // momentum components carried (dims, or 3 when a transverse velocity is non-zero)
     int tma;                // 1: stage state rows into shared memory with bulk async copies (nx even)
+    int warp2d;             // 1: FP32-flux 2D steps use the warp-strip march (k_warp2d) when nmom == 2
     int limiter;
     int flux;
     int gravity;
@@ -76,6 +77,16 @@ struct DevClock {
 };
 
 __device__ __forceinline__ void raise(DevClock* ck, int code) { atomicCAS(&ck->err, 0, code); }
+
+// Interior columns of a march tile of `bx` threads: the warp-strip march gives each warp 30 of
+// its 32 lanes (one halo lane per side), the CTA march shares one halo column per side.
+constexpr int kWarpStripCols = 30;
+__host__ __device__ inline bool warpStripMarch(const StepParams& P) {
+    return P.warp2d != 0 && P.dims == 2 && P.nmom == 2;
+}
+__host__ __device__ inline int marchTileColumns(const StepParams& P, int bx) {
+    return warpStripMarch(P) ? kWarpStripCols * (bx / 32) : bx - 2;
+}
 
 // Index helpers
 __device__ __forceinline__ long long cellIndex(const StepParams& P, int i, int j, int k) {

@@ -3,6 +3,7 @@
 #pragma once
 
 #include "fv_generic.cuh"
+#include "fv_warp2d.cuh"
 
 namespace fv {
 
@@ -11,6 +12,7 @@ struct MarchShape {
     int bx;      // threads along x (incl. the 2 halo columns)
     int by;      // threads along y in 3D (incl. halo), 1 in 2D
     int rows;    // cells per CTA along the marching axis
+    int warp;    // ensembles: 1 when every case runs the warp-strip march (FP32-flux 2D)
 };
 
 struct StepBuffers {
