@@ -59,9 +59,12 @@ namespace {
 // (FP32-flux 2D cases without a transverse velocity), else the CTA march.  Each case's P is the
 // handle's with the kernel choice written into it, so tile counts and kernels agree.
 void layoutTiles(fv_batch* b) {
-    bool warp = true;
-    for (fv_handle* h : b->cases) warp = warp && warpStripMarch(h->P);
-    b->shape.warp = warp ? 1 : 0;
+    bool warp = true, ring = true;
+    for (fv_handle* h : b->cases) {
+        warp = warp && warpStripMarch(h->P);
+        ring = ring && h->P.tma != 0;
+    }
+    b->shape.warp = warp ? (ring ? 2 : 1) : 0;
     long long base = 0;
     for (size_t i = 0; i < b->cases.size(); ++i) {
         BatchCase& bc = b->host[i];

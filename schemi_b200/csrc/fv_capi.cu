@@ -486,6 +486,7 @@ fv_status fv_create(const fv_config* cfg, fv_handle** out) {
     // the warp-strip march addresses fields with 32-bit offsets
     P.warp2d = (cfg->precision == FV_PREC_F32_FLUX && cfg->dims == 2 &&
                 P.ncell * (cfg->n_species + 5) < (1LL << 31)) ? 1 : 0;
+    if (P.warp2d) P.tma = 1;
     h->path = choosePath(*cfg);
     h->chem.mech = cfg->chemistry;
     h->chem.solver = cfg->chem_solver;
@@ -852,7 +853,9 @@ fv_status fv_set_march_shape(fv_handle* h, int bx, int by, int rows) {
 // staging needs an even number of cells along x.
 fv_status fv_set_staging(fv_handle* h, int on) {
     if (!h) return FV_ERR_INIT;
-    const int want = (on && h->P.n[0] % 2 == 0) ? 1 : 0;
+    // the CTA march stages rows by 16-byte bulk copies (nx even); the warp-strip march copies
+    // 8 bytes per lane
+    const int want = (on && (h->P.n[0] % 2 == 0 || h->P.warp2d)) ? 1 : 0;
     if (want != h->P.tma) {
         h->P.tma = want;
         destroyGraphs(h);

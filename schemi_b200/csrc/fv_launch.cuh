@@ -12,7 +12,8 @@ struct MarchShape {
     int bx;      // threads along x (incl. the 2 halo columns)
     int by;      // threads along y in 3D (incl. halo), 1 in 2D
     int rows;    // cells per CTA along the marching axis
-    int warp;    // ensembles: 1 when every case runs the warp-strip march (FP32-flux 2D)
+    int warp;    // ensembles: every case runs the warp-strip march (FP32-flux 2D): 1, rows through
+                 // registers; 2, rows through the shared-memory ring
 };
 
 struct StepBuffers {

@@ -323,13 +323,32 @@ template <int NS> __device__ __forceinline__ void restState(double* d) {
     d[NS + 3] = 1.0;
 }
 
+// Asynchronous 8-byte copies global -> shared (one per lane and field), in groups per row.
+__device__ __forceinline__ void cpAsync8(void* smem, const void* gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cpAsyncWait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Rows a warp keeps in its shared-memory ring (RING mode): the row being updated, the next one
+// and two in flight.
+constexpr int kWarpRingRows = 4;
+template <int NS> __host__ __device__ constexpr int warpRingDoubles() { return kWarpRingRows * (NS + 4) * 32; }
+
 // One strip: columns xs .. xs + 29 (lanes 1..30), rows z0 .. z0 + rows - 1.  Returns the lane's
 // CFL signal maximum (-1 when it updated nothing).  Field offsets are 32-bit (the host enables
-// this march only when (N + 5) * cells < 2^31).
-template <int NS, int EOS>
+// this march only when (N + 5) * cells < 2^31).  RING: rows arrive three ahead in the warp's
+// shared-memory ring `ring` by asynchronous copies (each lane copies and reads only its own
+// column, so no warp synchronisation is needed); otherwise they are loaded one row ahead into
+// registers.
+template <int NS, int EOS, bool RING>
 __device__ __forceinline__ float warpStrip(const StepParams& P, const double* __restrict__ U, double* __restrict__ Un,
                                            DevClock* __restrict__ ck, const LeanMix<NS>& L, double dt,
-                                           const double* g, int xs, int z0, int rows) {
+                                           const double* g, int xs, int z0, int rows, double* ring) {
     constexpr int NF = NS + 4;  // conserved fields carried: rho_1..rho_N, rho, m_x, m_y, E
     const int lane = threadIdx.x & 31;
     const int nx = P.n[0], ny = P.n[1];
@@ -375,13 +394,44 @@ __device__ __forceinline__ float warpStrip(const StepParams& P, const double* __
         }
     };
 
+    // ring slot of row r: rows z0 - 1, z0, z0 + 1, ... cycle through the slots
+    auto slotOf = [&](int r) -> double* { return ring + ((r - z0 + 1) & (kWarpRingRows - 1)) * (NF * 32) + lane; };
+    auto issue = [&](int r) {  // RING: copy row r into its slot (an empty group when outside)
+        bool ok;
+        const int zz = wrapY(r, ok);
+        if (has && ok && r < z0 + rows + 1) {
+            const double* q = U + ((long long)zz * nx + cx);
+            double* dst = slotOf(r);
+#pragma unroll
+            for (int f = 0; f < NF; ++f) cpAsync8(dst + f * 32, q + off[f]);
+        }
+        cpAsyncCommit();
+    };
+    auto fetch = [&](int r, double* d) {  // RING: row r from its slot
+        bool ok;
+        wrapY(r, ok);
+        if (has && ok) {
+            const double* src = slotOf(r);
+#pragma unroll
+            for (int f = 0; f < NF; ++f) d[f] = src[f * 32];
+        } else {
+            restState<NS>(d);
+        }
+    };
+
     bool bad = false;
     float localMax = -1.f;
     // Row z with the state of rows z (Wc, dCur) and z + 1 (Wn, dNext to be loaded) and the flux
     // through the face below row z (Gprev); leaves the flux above row z in Gnext.
     auto row = [&](int z, const LeanW<NS>& Wc, LeanW<NS>& Wn, const double* dCur, double* dNext,
                    const LeanF<NS>& Gprev, LeanF<NS>& Gnext) {
-        load(z + 1, dNext);
+        if constexpr (RING) {
+            issue(z + 3);         // into the slot of row z - 1, read for the last time a row ago
+            cpAsyncWait<2>();     // rows up to z + 1 have landed
+            fetch(z + 1, dNext);
+        } else {
+            load(z + 1, dNext);
+        }
         // x faces: low face of this lane from W of lane - 1
         LeanW<NS> Wl;
         shflUp<NS>(Wc, Wl);
@@ -423,11 +473,18 @@ __device__ __forceinline__ float warpStrip(const StepParams& P, const double* __
             // FP32 state after the step (for the CFL signal) takes the same increments
             float rhoN[NS + 1], mN[2], EN;
             double* q = Un + ((long long)z * nx + cx);
+            double dOld[NF];
+            if constexpr (RING) {
+                fetch(z, dOld);
+            } else {
+#pragma unroll
+                for (int f = 0; f < NF; ++f) dOld[f] = dCur[f];
+            }
 #pragma unroll
             for (int k = 0; k <= NS; ++k) {
                 const int f = k == 0 ? NS : k - 1;
                 const float inc = ((Fxp.rho[k] - Fx.rho[k]) * ax + (Gnext.rho[k] - Gprev.rho[k]) * ay) * dtf;
-                q[off[f]] = dCur[f] - double(inc);
+                q[off[f]] = dOld[f] - double(inc);
                 rhoN[k] = Wc.rho[k] - inc;
             }
             const float r0 = Wc.rho[0];
@@ -435,13 +492,13 @@ __device__ __forceinline__ float warpStrip(const StepParams& P, const double* __
             for (int d = 0; d < 2; ++d) {
                 float inc = ((Fxp.m[d] - Fx.m[d]) * ax + (Gnext.m[d] - Gprev.m[d]) * ay) * dtf;
                 if (grav) inc -= (d == 0 ? gx : gy) * r0 * dtf;
-                q[off[NS + 1 + d]] = dCur[NS + 1 + d] - double(inc);
+                q[off[NS + 1 + d]] = dOld[NS + 1 + d] - double(inc);
                 mN[d] = Wc.m[d] - inc;
             }
             {
                 float inc = ((Fxp.E - Fx.E) * ax + (Gnext.E - Gprev.E) * ay) * dtf;
                 if (grav) inc -= r0 * (Wc.v[0] * gx + Wc.v[1] * gy) * dtf;
-                q[off[NS + 3]] = dCur[NS + 3] - double(inc);
+                q[off[NS + 3]] = dOld[NS + 3] - double(inc);
                 EN = Wc.E - inc;
             }
             localMax = fmaxf(localMax, leanSignal<NS, EOS>(L, rhoN, mN, EN, minLS));
@@ -454,8 +511,15 @@ __device__ __forceinline__ float warpStrip(const StepParams& P, const double* __
     // prologue: the cell below the strip's first row and the flux through the face between
     {
         double dBelow[NF];
-        load(z0 - 1, dBelow);
-        load(z0, dA);
+        if constexpr (RING) {
+            for (int r = z0 - 1; r < z0 + 3; ++r) issue(r);
+            cpAsyncWait<2>();
+            fetch(z0 - 1, dBelow);
+            fetch(z0, dA);
+        } else {
+            load(z0 - 1, dBelow);
+            load(z0, dA);
+        }
         LeanW<NS> Wb;
         leanClose<NS, EOS>(L, dBelow, Wb);
         leanClose<NS, EOS>(L, dA, WA);
@@ -476,16 +540,18 @@ __device__ __forceinline__ float warpStrip(const StepParams& P, const double* __
         row(z + 1, WB, WA, dB, dA, GB, GA);
     }
     if (z < z1) row(z, WA, WB, dA, dB, GA, GB);
+    if constexpr (RING) cpAsyncWait<0>();  // no copy outlives the strip
     if (bad) raise(ck, FV_ERR_RIEMANN);
     return localMax;
 }
 
 // CTA = NW independent warps, each on one strip; grid x: strips / NW, grid y: row tiles.
-template <int NS, int EOS>
+template <int NS, int EOS, bool RING>
 __device__ __forceinline__ void warpTile(const StepParams& P, const double* __restrict__ U, double* __restrict__ Un,
                                          DevClock* __restrict__ ck, double* __restrict__ blockMaxOut, int rows,
                                          int tileX, int tileZ) {
     __shared__ float red[32];
+    extern __shared__ __align__(16) double warpRing[];
     const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     float m = -1.f;
     if (!ck->done) {
@@ -493,7 +559,9 @@ __device__ __forceinline__ void warpTile(const StepParams& P, const double* __re
         leanMix<NS, EOS>(P.mix, L);
         const int strip = tileX * nw + w;
         const int xs = strip * kWarpStripCols;
-        if (xs < P.n[0]) m = warpStrip<NS, EOS>(P, U, Un, ck, L, ck->dt, ck->g, xs, tileZ * rows, rows);
+        if (xs < P.n[0])
+            m = warpStrip<NS, EOS, RING>(P, U, Un, ck, L, ck->dt, ck->g, xs, tileZ * rows, rows,
+                                         RING ? warpRing + w * warpRingDoubles<NS>() : nullptr);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
@@ -506,17 +574,17 @@ __device__ __forceinline__ void warpTile(const StepParams& P, const double* __re
     }
 }
 
-template <int NS, int EOS, int NW, int MINB>
+template <int NS, int EOS, int NW, int MINB, bool RING>
 __global__ void __launch_bounds__(32 * NW, MINB) k_warp2d(const StepParams P, const double* __restrict__ U,
                                                           double* __restrict__ Un, DevClock* __restrict__ ck,
                                                           double* __restrict__ blockMax, int rows) {
     if (ck->done) return;  // uniform over the grid
-    warpTile<NS, EOS>(P, U, Un, ck, blockMax + blockIdx.x + (long long)gridDim.x * blockIdx.y, rows, blockIdx.x,
-                      blockIdx.y);
+    warpTile<NS, EOS, RING>(P, U, Un, ck, blockMax + blockIdx.x + (long long)gridDim.x * blockIdx.y, rows,
+                            blockIdx.x, blockIdx.y);
 }
 
 // Ensemble version: one CTA per tile of any case (the tile list of all cases in order).
-template <int NS, int EOS, int NW, int MINB>
+template <int NS, int EOS, int NW, int MINB, bool RING>
 __global__ void __launch_bounds__(32 * NW, MINB) k_warp2d_batch(const BatchCase* __restrict__ cases, int nCases,
                                                                 long long totalTiles, int rows) {
     static_assert(sizeof(StepParams) % 8 == 0, "StepParams is copied in 8-byte words");
@@ -544,7 +612,7 @@ __global__ void __launch_bounds__(32 * NW, MINB) k_warp2d_batch(const BatchCase*
         for (int i = threadIdx.x; i < (int)(sizeof(StepParams) / 8); i += blockDim.x) dst[i] = src[i];
     }
     __syncthreads();
-    warpTile<NS, EOS>(sP, Uin, Uout, C.ck, C.blockMax + local, rows, tx, tz);
+    warpTile<NS, EOS, RING>(sP, Uin, Uout, C.ck, C.blockMax + local, rows, tx, tz);
 }
 
 }  // namespace fv
