@@ -81,6 +81,7 @@ void layoutTiles(fv_batch* b) {
             bc.tiles[2] = (P.n[2] + b->shape.rows - 1) / b->shape.rows;
         }
         bc.nTiles = bc.tiles[0] * bc.tiles[1] * bc.tiles[2];
+        bc.nPartials = bc.nTiles * marchPartialsPerTile(P, b->shape.bx);
         bc.tileBase = base;
         base += bc.nTiles;
     }

@@ -113,7 +113,7 @@ __global__ void k_finalize(const StepParams P, DevClock* ck, const double* __res
 }
 __global__ void k_finalize_batch(const BatchCase* __restrict__ cases, int nCases) {
     const BatchCase& C = cases[blockIdx.x];
-    finalizeCase(C.P, C.ck, C.blockMax, C.nTiles);
+    finalizeCase(C.P, C.ck, C.blockMax, C.nPartials);
 }
 }  // namespace fv
 
@@ -899,7 +899,7 @@ long long marchBlocks(const StepParams& P, const MarchShape& s) {
     if (P.dims < 2) return 0;
     const int cols = marchTileColumns(P, s.bx);
     const long long gx = (P.n[0] + cols - 1) / cols;
-    if (P.dims == 2) return gx * ((P.n[1] + s.rows - 1) / s.rows);
+    if (P.dims == 2) return gx * ((P.n[1] + s.rows - 1) / s.rows) * marchPartialsPerTile(P, s.bx);
     const long long gy = (P.n[1] + s.by - 3) / (s.by - 2);
     return gx * gy * ((P.n[2] + s.rows - 1) / s.rows);
 }

@@ -87,6 +87,10 @@ __host__ __device__ inline bool warpStripMarch(const StepParams& P) {
 __host__ __device__ inline int marchTileColumns(const StepParams& P, int bx) {
     return warpStripMarch(P) ? kWarpStripCols * (bx / 32) : bx - 2;
 }
+// CFL partial maxima per tile: the warp-strip march writes one per warp (no CTA barrier).
+__host__ __device__ inline int marchPartialsPerTile(const StepParams& P, int bx) {
+    return warpStripMarch(P) ? bx / 32 : 1;
+}
 
 // Index helpers
 __device__ __forceinline__ long long cellIndex(const StepParams& P, int i, int j, int k) {
@@ -811,6 +815,7 @@ struct BatchCase {
     long long stepsBase;   // clock step count when the run started
     int tiles[3];          // tiles along x, y (3D), marching axis
     int nTiles;
+    int nPartials;         // CFL partial maxima the step writes (one per CTA, or per warp)
     long long tileBase;    // first tile of this case in the ensemble's tile list
 };
 

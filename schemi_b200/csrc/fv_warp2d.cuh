@@ -10,8 +10,8 @@
 //   * takes the high-x-face flux from lane + 1 by shuffle and updates its cell in FP64
 //     (U_new = U_old - dt * div F, with the gravity source of Advection.cpp:424-431);
 //   * derives the CFL signal (|v| + c) / min edge of the updated cell.
-// Warps never wait for one another: no shared-memory exchange and no CTA barrier inside the
-// march, one barrier at the end for the per-CTA CFL maximum.
+// Warps never wait for one another: no shared-memory exchange and no CTA barrier; each warp
+// writes its own CFL partial maximum.
 //
 // Arithmetic follows the FP32-flux contract of the CTA march (same HLLC / HLL, FP32 closure,
 // FP64 accumulation), with the area-to-volume ratios of the uniform-axis cells written as
@@ -226,6 +226,75 @@ __device__ __forceinline__ bool leanRiemann(int flux, const LeanW<NS>& O, const 
     return true;
 }
 
+// ---- paired FP32 arithmetic: one FFMA2 / FADD2 / FMUL2 computes two independent lanes of work
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 sel2(bool a, bool b, float2 x, float2 y) {
+    return make_float2(a ? x.x : y.x, b ? x.y : y.y);
+}
+
+// The two HLLC fluxes a lane computes per row, paired: component .x is the low x face (owner Ox,
+// neighbour Bx), component .y the face above the row (owner Oy, neighbour By); momenta as
+// normal / tangential pairs.  Without branches: each face takes the flux of the side K the
+// contact leaves (the owner when SO >= 0 or Sc >= 0, else the neighbour) plus S_K times the
+// star correction where the star region applies -- the cases and expressions of leanRiemann.
+// okx / oky are false for NaN speeds.
+template <int NS>
+__device__ __forceinline__ void hllcPair(const LeanW<NS>& Ox, const LeanW<NS>& Bx, const LeanW<NS>& Oy,
+                                         const LeanW<NS>& By, LeanF<NS>& Fx, LeanF<NS>& Fy, bool& okx, bool& oky) {
+    const float2 uO = make_float2(Ox.v[0], Oy.v[1]), uN = make_float2(Bx.v[0], By.v[1]);
+    const float2 cO = make_float2(Ox.cs, Oy.cs), cN = make_float2(Bx.cs, By.cs);
+    const float2 pO = make_float2(Ox.p, Oy.p), pN = make_float2(Bx.p, By.p);
+    const float2 a = sub2(uO, cO), b = sub2(uN, cN), c = add2(uO, cO), d = add2(uN, cN);
+    const float2 SO = make_float2(smin(a.x, b.x), smin(a.y, b.y));
+    const float2 SN = make_float2(smax(c.x, d.x), smax(c.y, d.y));
+    const float2 dO = mul2(make_float2(Ox.rho[0], Oy.rho[0]), sub2(SO, uO));
+    const float2 dN = mul2(make_float2(Bx.rho[0], By.rho[0]), sub2(SN, uN));
+    const float2 num = sub2(fma2(dO, uO, sub2(pN, pO)), mul2(dN, uN));
+    const float2 dd = sub2(dO, dN);
+    const float2 Sc = mul2(num, make_float2(rcpf(dd.x), rcpf(dd.y)));
+    const float2 PON =
+        mul2(fma2(dN, sub2(Sc, uN), fma2(dO, sub2(Sc, uO), add2(pO, pN))), make_float2(0.5f, 0.5f));
+    const bool supX = SO.x >= 0.f, supY = SO.y >= 0.f;
+    const bool ownX = supX || Sc.x >= 0.f, ownY = supY || Sc.y >= 0.f;
+    const bool stX = !supX && (Sc.x >= 0.f || SN.x > 0.f), stY = !supY && (Sc.y >= 0.f || SN.y > 0.f);
+    okx = supX || stX || SN.x <= 0.f;
+    oky = supY || stY || SN.y <= 0.f;
+    // side K the contact leaves
+    const float2 u = sel2(ownX, ownY, uO, uN), S = sel2(ownX, ownY, SO, SN), p = sel2(ownX, ownY, pO, pN);
+    const float2 E = sel2(ownX, ownY, make_float2(Ox.E, Oy.E), make_float2(Bx.E, By.E));
+    const float2 mn = sel2(ownX, ownY, make_float2(Ox.m[0], Oy.m[1]), make_float2(Bx.m[0], By.m[1]));
+    const float2 mt = sel2(ownX, ownY, make_float2(Ox.m[1], Oy.m[0]), make_float2(Bx.m[1], By.m[0]));
+    const float2 factor = sub2(S, u);
+    const float2 sd = sub2(S, Sc);
+    const float2 den = make_float2(stX ? rcpf(sd.x) : 0.f, stY ? rcpf(sd.y) : 0.f);
+    const float2 w = make_float2(stX ? S.x : 0.f, stY ? S.y : 0.f);
+    const float2 fd = mul2(factor, den);
+#pragma unroll
+    for (int k = 0; k <= NS; ++k) {
+        const float2 r = sel2(ownX, ownY, make_float2(Ox.rho[k], Oy.rho[k]), make_float2(Bx.rho[k], By.rho[k]));
+        const float2 f = fma2(w, sub2(mul2(r, fd), r), mul2(r, u));
+        Fx.rho[k] = f.x;
+        Fy.rho[k] = f.y;
+    }
+    // normal momentum: mn u + p + w ((mn factor - (p - PON)) den - mn)
+    const float2 ms = mul2(sub2(mul2(mn, factor), sub2(p, PON)), den);
+    const float2 Fmn = fma2(w, sub2(ms, mn), fma2(mn, u, p));
+    // tangential momentum: mt u + w (mt fd - mt)
+    const float2 Fmt = fma2(w, sub2(mul2(mt, fd), mt), mul2(mt, u));
+    // energy: (E + p) u + w ((E factor - p u + PON Sc) den - E)
+    const float2 Es = mul2(fma2(PON, Sc, sub2(mul2(E, factor), mul2(p, u))), den);
+    const float2 FE = fma2(w, sub2(Es, E), mul2(add2(E, p), u));
+    Fx.m[0] = Fmn.x;
+    Fx.m[1] = Fmt.x;
+    Fy.m[1] = Fmn.y;
+    Fy.m[0] = Fmt.y;
+    Fx.E = FE.x;
+    Fy.E = FE.y;
+}
+
 // Ghost state beyond a boundary patch of a 2D mesh (the ghostState of fv_device.cuh on a lean
 // state): fixed-value concentrations / velocity / pressure, slip mirrors the normal velocity.
 template <int NS, int EOS>
@@ -368,11 +437,11 @@ __device__ __forceinline__ float warpStrip(const StepParams& P, const double* __
     int off[NF];  // field offsets in the state (E follows m_z)
 #pragma unroll
     for (int f = 0; f < NF; ++f) off[f] = (f < NF - 1 ? f : NS + 4) * st;
-    const float ax = has ? 1.f / float(P.geo.h[0][cx]) : 0.f;
     const float hxf = has ? float(P.geo.h[0][cx]) : 1.f;
     const float Lz = float(P.ext[2]);
     const float gx = float(g[0]), gy = float(g[1]);
     const float dtf = float(dt);
+    const float axdt = dtf / hxf;  // dt * (x face area) / volume
     const bool grav = P.gravity != 0;
     const int flux = P.flux;
 
@@ -432,31 +501,25 @@ __device__ __forceinline__ float warpStrip(const StepParams& P, const double* __
         } else {
             load(z + 1, dNext);
         }
-        // x faces: low face of this lane from W of lane - 1
-        LeanW<NS> Wl;
-        shflUp<NS>(Wc, Wl);
-        LeanF<NS> Fx;
-        if (xLoPatch) {
-            LeanW<NS> Gs;
-            leanGhost<NS, EOS>(L, P.bc, FV_PATCH_TAIL, Wc, Gs);
-            bad |= !leanRiemann<NS, 0>(flux, Gs, Wc, Fx);
-        } else {
-            const bool ok = leanRiemann<NS, 0>(flux, Wl, Wc, Fx);
-            bad |= !ok && has && lane >= 1;
-        }
-        // y face above this row
+        // the low x face of this lane (owner: W of lane - 1, or the tail-patch ghost) and the
+        // face above this row (neighbour: W of the next row, or the left-patch ghost)
+        LeanW<NS> Ox;
+        shflUp<NS>(Wc, Ox);
+        if (xLoPatch) leanGhost<NS, EOS>(L, P.bc, FV_PATCH_TAIL, Wc, Ox);
         leanClose<NS, EOS>(L, dNext, Wn);
-        {
-            bool okN;
-            wrapY(z + 1, okN);
-            if (okN) {
-                bad |= !leanRiemann<NS, 1>(flux, Wc, Wn, Gnext) && has;
-            } else {
-                LeanW<NS> Gs;
-                leanGhost<NS, EOS>(L, P.bc, FV_PATCH_LEFT, Wc, Gs);
-                bad |= !leanRiemann<NS, 1>(flux, Wc, Gs, Gnext) && has;
-            }
+        bool okN;
+        wrapY(z + 1, okN);
+        LeanW<NS> By = Wn;
+        if (!okN) leanGhost<NS, EOS>(L, P.bc, FV_PATCH_LEFT, Wc, By);
+        LeanF<NS> Fx;
+        bool okx, oky;
+        if (flux == FV_FLUX_HLLC) {
+            hllcPair<NS>(Ox, Wc, Wc, By, Fx, Gnext, okx, oky);
+        } else {
+            okx = leanRiemann<NS, 0>(flux, Ox, Wc, Fx);
+            oky = leanRiemann<NS, 1>(flux, Wc, By, Gnext);
         }
+        bad |= (!okx && has && lane >= 1) || (!oky && has);
         // high x face: the low face of lane + 1, or the point patch
         LeanF<NS> Fxp;
         shflDown<NS>(Fx, Fxp);
@@ -467,11 +530,8 @@ __device__ __forceinline__ float warpStrip(const StepParams& P, const double* __
         }
         if (interior) {
             const float hy = float(P.geo.h[1][z]);
-            const float ay = 1.f / hy;
+            const float aydt = dtf / hy;
             const float minLS = 1.f / fminf(fminf(hxf, hy), Lz);
-            // FP32 increments dt * div F (+ gravity), accumulated into the FP64 state; the
-            // FP32 state after the step (for the CFL signal) takes the same increments
-            float rhoN[NS + 1], mN[2], EN;
             double* q = Un + ((long long)z * nx + cx);
             double dOld[NF];
             if constexpr (RING) {
@@ -480,27 +540,58 @@ __device__ __forceinline__ float warpStrip(const StepParams& P, const double* __
 #pragma unroll
                 for (int f = 0; f < NF; ++f) dOld[f] = dCur[f];
             }
+            // per field in state order (rho_1..rho_N, rho, m_x, m_y, E): FP32 increments
+            // dt * div F (+ gravity), two fields per paired instruction
+            float fxp[NF], fxm[NF], gn[NF], gp[NF], w0[NF], inc[NF];
+            auto flat = [&](const LeanF<NS>& F, float* o) {
 #pragma unroll
-            for (int k = 0; k <= NS; ++k) {
-                const int f = k == 0 ? NS : k - 1;
-                const float inc = ((Fxp.rho[k] - Fx.rho[k]) * ax + (Gnext.rho[k] - Gprev.rho[k]) * ay) * dtf;
-                q[off[f]] = dOld[f] - double(inc);
-                rhoN[k] = Wc.rho[k] - inc;
-            }
-            const float r0 = Wc.rho[0];
+                for (int k = 1; k <= NS; ++k) o[k - 1] = F.rho[k];
+                o[NS] = F.rho[0];
+                o[NS + 1] = F.m[0];
+                o[NS + 2] = F.m[1];
+                o[NS + 3] = F.E;
+            };
+            flat(Fxp, fxp);
+            flat(Fx, fxm);
+            flat(Gnext, gn);
+            flat(Gprev, gp);
 #pragma unroll
-            for (int d = 0; d < 2; ++d) {
-                float inc = ((Fxp.m[d] - Fx.m[d]) * ax + (Gnext.m[d] - Gprev.m[d]) * ay) * dtf;
-                if (grav) inc -= (d == 0 ? gx : gy) * r0 * dtf;
-                q[off[NS + 1 + d]] = dOld[NS + 1 + d] - double(inc);
-                mN[d] = Wc.m[d] - inc;
+            for (int k = 1; k <= NS; ++k) w0[k - 1] = Wc.rho[k];
+            w0[NS] = Wc.rho[0];
+            w0[NS + 1] = Wc.m[0];
+            w0[NS + 2] = Wc.m[1];
+            w0[NS + 3] = Wc.E;
+            const float2 ax2 = make_float2(axdt, axdt), ay2 = make_float2(aydt, aydt);
+#pragma unroll
+            for (int f = 0; f + 1 < NF; f += 2) {
+                const float2 dx = sub2(make_float2(fxp[f], fxp[f + 1]), make_float2(fxm[f], fxm[f + 1]));
+                const float2 dy = sub2(make_float2(gn[f], gn[f + 1]), make_float2(gp[f], gp[f + 1]));
+                const float2 i2 = fma2(dx, ax2, mul2(dy, ay2));
+                inc[f] = i2.x;
+                inc[f + 1] = i2.y;
             }
-            {
-                float inc = ((Fxp.E - Fx.E) * ax + (Gnext.E - Gprev.E) * ay) * dtf;
-                if (grav) inc -= r0 * (Wc.v[0] * gx + Wc.v[1] * gy) * dtf;
-                q[off[NS + 3]] = dOld[NS + 3] - double(inc);
-                EN = Wc.E - inc;
+            if (NF & 1) inc[NF - 1] = (fxp[NF - 1] - fxm[NF - 1]) * axdt + (gn[NF - 1] - gp[NF - 1]) * aydt;
+            if (grav) {
+                const float r0 = Wc.rho[0] * dtf;
+                inc[NS + 1] -= gx * r0;
+                inc[NS + 2] -= gy * r0;
+                inc[NS + 3] -= r0 * (Wc.v[0] * gx + Wc.v[1] * gy);
             }
+            // FP64 accumulation; the FP32 state after the step (for the CFL signal) takes the
+            // same increments
+            float wn[NF];
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                q[off[f]] = dOld[f] - double(inc[f]);
+                wn[f] = w0[f] - inc[f];
+            }
+            float rhoN[NS + 1], mN[2];
+#pragma unroll
+            for (int k = 1; k <= NS; ++k) rhoN[k] = wn[k - 1];
+            rhoN[0] = wn[NS];
+            mN[0] = wn[NS + 1];
+            mN[1] = wn[NS + 2];
+            const float EN = wn[NS + 3];
             localMax = fmaxf(localMax, leanSignal<NS, EOS>(L, rhoN, mN, EN, minLS));
         }
     };
@@ -546,11 +637,12 @@ __device__ __forceinline__ float warpStrip(const StepParams& P, const double* __
 }
 
 // CTA = NW independent warps, each on one strip; grid x: strips / NW, grid y: row tiles.
+// The warps of a tile are independent to the end: each writes its own CFL partial maximum to
+// partials[w] (no CTA barrier).
 template <int NS, int EOS, bool RING>
 __device__ __forceinline__ void warpTile(const StepParams& P, const double* __restrict__ U, double* __restrict__ Un,
-                                         DevClock* __restrict__ ck, double* __restrict__ blockMaxOut, int rows,
+                                         DevClock* __restrict__ ck, double* __restrict__ partials, int rows,
                                          int tileX, int tileZ) {
-    __shared__ float red[32];
     extern __shared__ __align__(16) double warpRing[];
     const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     float m = -1.f;
@@ -565,13 +657,7 @@ __device__ __forceinline__ void warpTile(const StepParams& P, const double* __re
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) red[w] = m;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        float b = red[0];
-        for (int i = 1; i < nw; ++i) b = fmaxf(b, red[i]);
-        *blockMaxOut = double(b);
-    }
+    if ((threadIdx.x & 31) == 0) partials[w] = double(m);
 }
 
 template <int NS, int EOS, int NW, int MINB, bool RING>
@@ -579,7 +665,7 @@ __global__ void __launch_bounds__(32 * NW, MINB) k_warp2d(const StepParams P, co
                                                           double* __restrict__ Un, DevClock* __restrict__ ck,
                                                           double* __restrict__ blockMax, int rows) {
     if (ck->done) return;  // uniform over the grid
-    warpTile<NS, EOS, RING>(P, U, Un, ck, blockMax + blockIdx.x + (long long)gridDim.x * blockIdx.y, rows,
+    warpTile<NS, EOS, RING>(P, U, Un, ck, blockMax + (blockIdx.x + (long long)gridDim.x * blockIdx.y) * NW, rows,
                             blockIdx.x, blockIdx.y);
 }
 
@@ -612,7 +698,7 @@ __global__ void __launch_bounds__(32 * NW, MINB) k_warp2d_batch(const BatchCase*
         for (int i = threadIdx.x; i < (int)(sizeof(StepParams) / 8); i += blockDim.x) dst[i] = src[i];
     }
     __syncthreads();
-    warpTile<NS, EOS, RING>(sP, Uin, Uout, C.ck, C.blockMax + local, rows, tx, tz);
+    warpTile<NS, EOS, RING>(sP, Uin, Uout, C.ck, C.blockMax + local * NW, rows, tx, tz);
 }
 
 }  // namespace fv
