@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define FV_ABI_VERSION 2
+#define FV_ABI_VERSION 3
 #define FV_MAX_SPECIES 4
 
 typedef int fv_status;
@@ -96,6 +96,16 @@ enum fv_precision { FV_PREC_F64 = 0, FV_PREC_F32_FLUX = 1 };
  *           integrator, heat release q per mol of reaction as in chemicalKineticsH2Cl2Combustion.cpp). */
 enum fv_chemistry { FV_CHEM_NONE = 0, FV_CHEM_A_B_2C = 1, FV_CHEM_CL2 = 2 };
 
+/* Step solver of #Approximation_order (abstractStepSolver::createStepSolver,
+ * src/interfaces/abstractStepSolver.cpp:56-146).
+ *   SECOND_ORDER     "SecondOrder": MUSCL-Hancock, one stage (secondOrderStepSolver.cpp).
+ *   SECOND_ORDER_RK  "SecondOrderRK": two stages of the TVD reconstruction without the Hancock
+ *                    predictor (Advection2dOrder.cpp), then the 0.5 average with the step's start
+ *                    state (secondOrderStepSolverRK.cpp:48-71, bunchOfFields::average); the
+ *                    averaged concentrations are part of the state.  Not with chemistry, the
+ *                    batched ensemble, the adjoint or fv_step_noalloc. */
+enum fv_step_solver { FV_ORDER_SECOND = 0, FV_ORDER_SECOND_RK = 1 };
+
 /* Per-cell linear solver of the backward-Euler step (set/chemicalKinetics.txt #Iterative_solver:
  * "Gauss-Seidel", "Jacobi", "GaussElimination", "conjugateGradient", "JacobiConjugateGradient"). */
 enum fv_chem_solver {
@@ -145,6 +155,8 @@ typedef struct fv_config {
     /* #Constant_timestep: > 0 fixes every step to this dt (main then skips its CFL block,
      * Schemi.cpp:178-181,664-668,807); <= 0 keeps the CFL step. */
     double const_timestep;
+    /* #Approximation_order: the step solver (fv_step_solver). */
+    int order;
 } fv_config;
 
 /* Field indices of fv_download / fv_upload arrays (n_cells doubles each, x fastest).

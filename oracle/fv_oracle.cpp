@@ -834,7 +834,10 @@ void cellPrimitivesFromConserved(fvo_case& cs, long long i) {
     cs.p[i] = mx.pFromUv(cc, cs.Uv[i]);
 }
 
-int doStep(fvo_case& cs, double dt) {
+// One advection of the state by dt: MUSCL-Hancock (Advection.cpp, hancock = true) or the same
+// TVD reconstruction without the predictor (Advection2dOrder.cpp:20-636, hancock = false), whose
+// boundary neighbour is the ghost of the reconstructed owner face (Advection2dOrder.cpp:394-522).
+int doStep(fvo_case& cs, double dt, bool hancock = true) {
     const Mix& mx = cs.mix;
     const int NS = mx.N;
     const long long nc = cs.nCells;
@@ -879,7 +882,7 @@ int doStep(fvo_case& cs, double dt) {
 
     // 3. Hancock half step (HancockStage.cpp:10-240)
     const double halfTimestep = 0.5 * dt;
-    for (long long i = 0; i < nc; ++i) {
+    for (long long i = 0; hancock && i < nc; ++i) {
         const Cell& c = cs.cells[i];
         double divR[FV_MAX_SPECIES + 1];
         for (int k = 0; k <= NS; ++k) {
@@ -914,10 +917,10 @@ int doStep(fvo_case& cs, double dt) {
         }
     }
     for (size_t f = 0; f < nf; ++f) {
-        closeFromConserved(mx, own[f]);
+        if (hancock) closeFromConserved(mx, own[f]);
         const Face& F = cs.faces[f];
         if (F.nei >= 0) {
-            closeFromConserved(mx, nei[f]);
+            if (hancock) closeFromConserved(mx, nei[f]);
         } else {
             // ghost neighbour state (HancockStage.cpp:324-446)
             FState& s = nei[f];
@@ -982,6 +985,42 @@ int doStep(fvo_case& cs, double dt) {
         for (int k = 0; k <= NS; ++k) cs.rho[k][i] -= dR[k] / c.V * dt;
     }
     for (long long i = 0; i < nc; ++i) cellPrimitivesFromConserved(cs, i);
+    return FV_OK;
+}
+
+// ---------------------------------------------------------------- SecondOrderRK
+// secondOrderStepSolverRK::calculateStep (secondOrderStepSolverRK.cpp:48-71): two advections
+// without the predictor, then Un2.average(Un, 0.5) and copyFrom (bunchOfFields.hpp:166-237):
+// concentrations, densities, momentum and energy averaged field by field, then v = m / rho,
+// Uv = E - k - 0.5 rho (v & v), p = pFromUv(c, Uv).  The averaged concentrations are kept as
+// the state (the next step reconstructs from them).
+int rk2Step(fvo_case& cs, double dt) {
+    const int NS = cs.mix.N;
+    const long long nc = cs.nCells;
+    std::vector<double> c0[FV_MAX_SPECIES + 1], r0[FV_MAX_SPECIES + 1], E0 = cs.E;
+    std::vector<V3> m0 = cs.m;
+    for (int k = 0; k <= NS; ++k) {
+        c0[k] = cs.c[k];
+        r0[k] = cs.rho[k];
+    }
+    int st = doStep(cs, dt, false);
+    if (st != FV_OK) return st;
+    st = doStep(cs, dt, false);
+    if (st != FV_OK) return st;
+    const double own = 0.5, in = 1 - own;
+    for (long long i = 0; i < nc; ++i) {
+        for (int k = 0; k <= NS; ++k) {
+            cs.c[k][i] = own * cs.c[k][i] + in * c0[k][i];
+            cs.rho[k][i] = own * cs.rho[k][i] + in * r0[k][i];
+        }
+        for (int d = 0; d < 3; ++d) cs.m[i].x[d] = cs.m[i].x[d] * own + m0[i].x[d] * in;
+        cs.E[i] = own * cs.E[i] + in * E0[i];
+        cs.v[i] = vdiv(cs.m[i], cs.rho[0][i]);
+        cs.Uv[i] = (cs.E[i] - 0.0) - 0.5 * cs.rho[0][i] * vdot(cs.v[i], cs.v[i]);
+        double cc[FV_MAX_SPECIES + 1];
+        for (int k = 0; k <= NS; ++k) cc[k] = cs.c[k][i];
+        cs.p[i] = cs.mix.pFromUv(cc, cs.Uv[i]);
+    }
     return FV_OK;
 }
 
@@ -1361,6 +1400,11 @@ bool validate(const fv_config& cf, std::string& err) {
     if (cf.chemistry == FV_CHEM_CL2 && cf.n_species != 2) { err = "Cl2 dissociation needs 2 species"; return false; }
     if (cf.chemistry == FV_CHEM_A_B_2C && cf.n_species != 3) { err = "A+B->2C needs 3 species"; return false; }
     if (cf.chemistry < FV_CHEM_NONE || cf.chemistry > FV_CHEM_CL2) { err = "unknown chemistry"; return false; }
+    if (cf.order != FV_ORDER_SECOND && cf.order != FV_ORDER_SECOND_RK) { err = "unknown step solver"; return false; }
+    if (cf.order == FV_ORDER_SECOND_RK && cf.chemistry != FV_CHEM_NONE) {
+        err = "SecondOrderRK with chemistry is not implemented";
+        return false;
+    }
     return true;
 }
 
@@ -1454,7 +1498,7 @@ int fvo_upload(fvo_case* cs, const double* const* prim) {
 
 int fvo_step(fvo_case* cs, double* dt_used, double* dt_next) {
     const double dt = cs->dt;
-    int st = doStep(*cs, dt);
+    int st = cs->cfg.order == FV_ORDER_SECOND_RK ? rk2Step(*cs, dt) : doStep(*cs, dt);
     if (st != FV_OK) return st;
     if (cs->cfg.chemistry != FV_CHEM_NONE) {
         // secondOrderStepSolver::calculateStep: chemistry after the advection, same dt

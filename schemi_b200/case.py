@@ -35,6 +35,8 @@ CHEMISTRY = {"no": 0, "A+B->2C": 1, "Cl2": 2}
 # set/chemicalKinetics.txt #Iterative_solver names (abstractChemicalKinetics.cpp:21-29)
 CHEM_SOLVERS = {"Gauss-Seidel": 0, "Jacobi": 1, "GaussElimination": 2, "conjugateGradient": 3,
                 "JacobiConjugateGradient": 4}
+# #Approximation_order values with a GPU step (abstractStepSolver.cpp:56-146)
+ORDERS = {"SecondOrder": 0, "SecondOrderRK": 1}
 
 # patch order of the task files: #Tail, #Point, #Bottom, #Right, #Left, #Top
 PATCHES = ["tail", "point", "bottom", "right", "left", "top"]
@@ -85,6 +87,7 @@ class fv_config_t(ctypes.Structure):
         ("chem_solver", ctypes.c_int),
         ("chem_max_iter", ctypes.c_int),
         ("const_timestep", ctypes.c_double),
+        ("order", ctypes.c_int),
     ]
 
 
@@ -151,6 +154,7 @@ class Case:
     chem_solver: str = "Gauss-Seidel"
     chem_max_iter: int = 200
     const_timestep: float = 0.0   # > 0: every step takes this dt (#Constant_timestep)
+    order: str = "SecondOrder"    # #Approximation_order: "SecondOrder" or "SecondOrderRK"
     name: str = "case"
 
     def __post_init__(self):
@@ -236,6 +240,7 @@ class Case:
         c.chem_solver = CHEM_SOLVERS[self.chem_solver]
         c.chem_max_iter = self.chem_max_iter
         c.const_timestep = self.const_timestep
+        c.order = ORDERS[self.order]
         return c
 
 

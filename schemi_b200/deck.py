@@ -184,7 +184,7 @@ def write_deck(case: Case, directory: str, prim: Sequence[np.ndarray], frequency
         ("#Constant_timestep", _f(case.const_timestep) if case.const_timestep > 0 else "-1E-8"),
         ("#Source_timestep_correction", src_ts),
         ("#Reconstruction", "star"),
-        ("#Approximation_order", "SecondOrder"),
+        ("#Approximation_order", case.order),
         ("#Start_From_Time-Step", "1" if restart else "no"),
         ("#Calculation_of_mixing_zone_width", "off"),
         ("#Nonlinearity_iterations", "off"),

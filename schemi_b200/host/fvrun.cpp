@@ -15,8 +15,8 @@
 // timeOfCalculation.tsv, with the reference's 20 significant digits.
 //
 // Not supported (the run stops with a message): zones other than the outer zone, diffusion,
-// turbulence, approximation orders other than SecondOrder, the 1D mixing-zone width output, and
-// chemical mechanisms other than "no" and "Cl2".
+// turbulence, approximation orders other than SecondOrder and SecondOrderRK, the 1D mixing-zone
+// width output, and chemical mechanisms other than "no" and "Cl2".
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -184,7 +184,9 @@ Deck readDeck(const std::string& dir) {
     if (onOff(turbulence, "turbulence"))
         throw Fail("#Turbulence_flag on: turbulence models are not part of this step");
     if (reconstruction != "linear" && reconstruction != "star") throw Fail("Unknown reconstruction flag.");
-    if (order != "SecondOrder") throw Fail("#Approximation_order " + order + ": only SecondOrder is implemented");
+    if (order == "SecondOrder") c.order = FV_ORDER_SECOND;
+    else if (order == "SecondOrderRK") c.order = FV_ORDER_SECOND_RK;
+    else throw Fail("#Approximation_order " + order + ": SecondOrder and SecondOrderRK are implemented");
     if (onOff(width, "mixed zone width calculation") && dims == "1D") throw Fail("#Calculation_of_mixing_zone_width on is not implemented");
     c.dims = dims == "1D" ? 1 : dims == "2D" ? 2 : dims == "3D" ? 3 : 0;
     if (!c.dims) throw Fail("unknown #Dimensions_of_the_task " + dims);
@@ -508,7 +510,7 @@ void printConfig(const fv_config& c, const Deck& d) {
     for (int p = 0; p < 6; ++p) std::cout << (p ? ", " : "") << c.bc_p[p];
     std::cout << "], \"chemistry\": " << c.chemistry << ", \"const_timestep\": " << c.const_timestep
               << ", \"t_end\": " << d.tEnd << ", \"frequency\": " << d.freq << ", \"start\": \"" << d.readFrom
-              << "\"}" << std::endl;
+              << "\", \"order\": " << c.order << "}" << std::endl;
 }
 
 int run(const Deck& d) {

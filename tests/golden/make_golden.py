@@ -6,7 +6,7 @@ task deck by ``schemi_b200.deck`` and fed to it through its restart reader.  The
 the reference's per-step outputs, so the parity tests need neither the reference sources nor
 the binary at run time.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [fixture names]
 """
 
 import os
@@ -73,11 +73,27 @@ def golden_cases():
     for solver, tag in (("Jacobi", "jacobi"), ("GaussElimination", "ge"), ("conjugateGradient", "cg")):
         c, p = cases.chlorine_dissociation_2d(4, solver=solver)
         out.append((f"cl2_4x4_vdw_{tag}", c, p, 6, [1, 6]))
+    # SecondOrderRK: two stages without the Hancock predictor, then the 0.5 average
+    c, p = cases.kelvin_helmholtz_2d(n=24, periodic=False)
+    c.order = "SecondOrderRK"
+    out.append(("kh_slip_24_rk2", c, p, 10, [1, 2, 10]))
+    c, p = cases.kelvin_helmholtz_2d(n=24, periodic=False, limiter="linear")
+    c.order = "SecondOrderRK"
+    out.append(("kh_slip_24_rk2_linear", c, p, 8, [1, 8]))
+    c, p = cases.shock_tube_1d(n=200)
+    c.order = "SecondOrderRK"
+    out.append(("tube_rk2_minmod_200", c, p, 30, [1, 2, 30]))
+    c, p = cases.rayleigh_taylor_2d(nx=16, ny=48, modes=4)
+    c.order = "SecondOrderRK"
+    c.g_delta = (0.0, -0.02, 0.0)
+    out.append(("rt_16x48_rk2_gravity", c, p, 10, [1, 10]))
     return out
 
 
-def main():
+def main(only=None):
     for name, case, prim, nsteps, keep in golden_cases():
+        if only and name not in only:
+            continue
         if nsteps is not None:
             oc = O.OracleCase(case)
             oc.upload(prim)
@@ -101,4 +117,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or None)
