@@ -244,7 +244,7 @@ long long fv_kernels_per_step(const fv_handle* h);
  *                          (unclamped); cfg->g is the gravity vector of this step
  *   stream                 cudaStream_t or NULL
  * Runs the full MUSCL-Hancock path (any limiter, 1D/2D/3D) on meshes of at most
- * FV_NOALLOC_MAX_CELLS cells; larger meshes and cases with chemistry are rejected with FV_ERR_INIT.  The first call on a
+ * FV_NOALLOC_MAX_CELLS cells; larger meshes, cases with chemistry and SecondOrderRK are rejected with FV_ERR_INIT.  The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress) and should come before any
  * stream capture.  Every call rewrites each part of the array it reads, so no state carries over
  * between calls; calls that overlap on the GPU share the array and race.  Synchronises `stream`

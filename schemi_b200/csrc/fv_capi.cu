@@ -104,6 +104,86 @@ __global__ void k_transverse(const StepParams P, const double* __restrict__ prim
     if (nz) atomicOr(flag, 1);
 }
 
+// SecondOrderRK: Un2.average(Un, 0.5) + copyFrom (secondOrderStepSolverRK.cpp:64-66,
+// bunchOfFields.hpp:166-237) of the state after the second stage U2 with the step's start state
+// U0, then main's CFL signal of the averaged state.  Concentrations are averaged as fields: c of
+// U2 is rho_k / M_k with c_0 their sum (Advection2dOrder.cpp:578-585), c of U0 the stored ones
+// (or the restart set before step 1).  Writes the averaged state to Un and conc.
+template <int NS, int EOS, int D>
+__global__ void k_rk_average(const StepParams P, const double* __restrict__ U2, const double* __restrict__ U0,
+                             const double* __restrict__ prim0, DevClock* __restrict__ ck, double* __restrict__ Un,
+                             double* __restrict__ conc, double* __restrict__ blockMax) {
+    __shared__ double red[32];
+    if (ck->done) return;
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    double localMax = -1;
+    if (i < P.ncell) {
+        const long long s = P.stride;
+        const double own = 0.5, in = 1 - own;
+        double c2[NS + 1], c0[NS + 1], c[NS + 1];
+        c2[0] = 0;
+#pragma unroll
+        for (int k = 1; k <= NS; ++k) {
+            c2[k] = U2[(k - 1) * s + i] / P.mix.M[k - 1];
+            c2[0] += c2[k];
+        }
+        if (ck->first) {
+            c0[0] = 0;
+#pragma unroll
+            for (int k = 1; k <= NS; ++k) {
+                c0[k] = prim0[(k - 1) * s + i];
+                c0[0] += c0[k];
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k <= NS; ++k) c0[k] = conc[k * s + i];
+        }
+#pragma unroll
+        for (int k = 0; k <= NS; ++k) {
+            c[k] = own * c2[k] + in * c0[k];
+            conc[k * s + i] = c[k];
+        }
+        double rho[NS + 1];
+#pragma unroll
+        for (int k = 0; k <= NS; ++k) {
+            const int f = k == 0 ? NS : k - 1;
+            rho[k] = own * U2[f * s + i] + in * U0[f * s + i];
+            Un[f * s + i] = rho[k];
+        }
+        double m[3] = {0, 0, 0};
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            if (d < P.nmom) {
+                m[d] = U2[(NS + 1 + d) * s + i] * own + U0[(NS + 1 + d) * s + i] * in;
+                Un[(NS + 1 + d) * s + i] = m[d];
+            }
+        const double E = own * U2[(NS + 4) * s + i] + in * U0[(NS + 4) * s + i];
+        Un[(NS + 4) * s + i] = E;
+        // copyFrom: v = m / rho, Uv = E - k - 0.5 rho (v & v), p = pFromUv(c, Uv); CFL signal
+        double v[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) v[d] = d < P.nmom ? m[d] / rho[0] : 0.0;
+        double vv = 0;
+        vv += v[0] * v[0];
+        vv += v[1] * v[1];
+        vv += v[2] * v[2];
+        const double Uv = (E - 0.0) - 0.5 * rho[0] * vv;
+        const double p = Mixture<double, NS, EOS>::pFromUv(P.mix, c, Uv);
+        const double sonic = sqrt(Mixture<double, NS, EOS>::sqSonic(P.mix, c, rho[0], Uv, p));
+        int ijk[3];
+        ijk[0] = (int)(i % P.n[0]);
+        ijk[1] = D >= 2 ? (int)((i / P.n[0]) % P.n[1]) : 0;
+        ijk[2] = D >= 3 ? (int)(i / ((long long)P.n[0] * P.n[1])) : 0;
+        const double ex = extent(P, 0, ijk[0]), ey = extent(P, 1, ijk[1]), ez = extent(P, 2, ijk[2]);
+        const double minLS = 1.0 / smin(smin(ex, ey), ez);
+        double sg = (P.nmom == 3 ? mag3<double>(v[0], v[1], v[2]) : mag2z<double>(v[0], v[1])) + sonic;
+        sg *= minLS;
+        localMax = sg;
+    }
+    const double bm = blockMaxReduce<double>(localMax, red);
+    if (threadIdx.x == 0) blockMax[blockIdx.x] = bm;
+}
+
 }  // namespace
 
 namespace fv {
@@ -184,6 +264,11 @@ bool validate(const fv_config& c, std::string& e) {
     if (c.chemistry < FV_CHEM_NONE || c.chemistry > FV_CHEM_CL2) { e = "unknown chemistry"; return false; }
     if (c.chemistry == FV_CHEM_A_B_2C && c.n_species != 3) { e = "A+B->2C needs 3 species (A, B, C)"; return false; }
     if (c.chemistry == FV_CHEM_CL2 && c.n_species != 2) { e = "Cl2 dissociation needs 2 species (Cl2, Cl)"; return false; }
+    if (c.order != FV_ORDER_SECOND && c.order != FV_ORDER_SECOND_RK) { e = "unknown step solver (order)"; return false; }
+    if (c.order == FV_ORDER_SECOND_RK && c.chemistry != FV_CHEM_NONE) {
+        e = "SecondOrderRK with chemistry is not implemented";
+        return false;
+    }
     if (c.chemistry != FV_CHEM_NONE) {
         if (c.chem_solver < FV_CHEM_GAUSS_SEIDEL || c.chem_solver > FV_CHEM_JACOBI_CONJUGATE_GRADIENT) {
             e = "unknown chemical iterative solver";
@@ -324,7 +409,49 @@ long long stepBlocks(fv_handle* h) {
 }
 
 // enqueue step [+ chemistry] + finalize reading U[from]
+template <int NS, int EOS>
+void launchAverage(fv_handle* h, int from) {
+    const int tpb = 128;
+    const unsigned g = (unsigned)genericBlocks(h->P);
+    switch (h->cfg.dims) {
+    case 1: k_rk_average<NS, EOS, 1><<<g, tpb, 0, h->stream>>>(h->P, h->Ustage, h->U[from], h->prim0, h->ck, h->U[from ^ 1], h->conc, h->blockMax); break;
+    case 2: k_rk_average<NS, EOS, 2><<<g, tpb, 0, h->stream>>>(h->P, h->Ustage, h->U[from], h->prim0, h->ck, h->U[from ^ 1], h->conc, h->blockMax); break;
+    default: k_rk_average<NS, EOS, 3><<<g, tpb, 0, h->stream>>>(h->P, h->Ustage, h->U[from], h->prim0, h->ck, h->U[from ^ 1], h->conc, h->blockMax); break;
+    }
+}
+
+// SecondOrderRK: stage 1 U[from] -> U[from ^ 1] (concentrations of the start state), stage 2
+// U[from ^ 1] -> Ustage, average (Ustage, U[from]) -> U[from ^ 1] with the CFL partials.
+cudaError_t enqueueRk2(fv_handle* h, int from) {
+    StepBuffers B1 = buffersFor(h, from);
+    StepParams P2 = h->P;
+    P2.conc = nullptr;  // stage 2 reads the first stage's own rho_k / M_k
+    StepBuffers B2 = B1;
+    B2.U = h->U[from ^ 1];
+    B2.Un = h->Ustage;
+    B2.prim0 = nullptr;
+    const bool f64 = h->cfg.precision == FV_PREC_F64;
+    cudaError_t e = f64 ? launchStepF64(h->P, B1, h->path, h->shape, h->stream)
+                        : launchStepF32(h->P, B1, h->path, h->shape, h->stream);
+    if (e != cudaSuccess) return e;
+    e = f64 ? launchStepF64(P2, B2, h->path, h->shape, h->stream) : launchStepF32(P2, B2, h->path, h->shape, h->stream);
+    if (e != cudaSuccess) return e;
+    const int ns = h->cfg.n_species;
+    const bool vdw = h->cfg.eos == FV_EOS_VAN_DER_WAALS;
+    switch (ns) {
+    case 1: vdw ? launchAverage<1, 1>(h, from) : launchAverage<1, 0>(h, from); break;
+    case 2: vdw ? launchAverage<2, 1>(h, from) : launchAverage<2, 0>(h, from); break;
+    case 3: vdw ? launchAverage<3, 1>(h, from) : launchAverage<3, 0>(h, from); break;
+    default: vdw ? launchAverage<4, 1>(h, from) : launchAverage<4, 0>(h, from); break;
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_finalize<<<1, 1024, 0, h->stream>>>(h->P, h->ck, h->blockMax, (int)genericBlocks(h->P));
+    return cudaGetLastError();
+}
+
 cudaError_t enqueueStep(fv_handle* h, int from) {
+    if (h->cfg.order == FV_ORDER_SECOND_RK) return enqueueRk2(h, from);
     const StepBuffers B = buffersFor(h, from);
     cudaError_t e = h->cfg.precision == FV_PREC_F64 ? launchStepF64(h->P, B, h->path, h->shape, h->stream)
                                                      : launchStepF32(h->P, B, h->path, h->shape, h->stream);
@@ -487,6 +614,7 @@ fv_status fv_create(const fv_config* cfg, fv_handle** out) {
     P.warp2d = (cfg->precision == FV_PREC_F32_FLUX && cfg->dims == 2 &&
                 P.ncell * (cfg->n_species + 5) < (1LL << 31)) ? 1 : 0;
     if (P.warp2d) P.tma = 1;
+    P.hancock = cfg->order == FV_ORDER_SECOND ? 1 : 0;
     h->path = choosePath(*cfg);
     h->chem.mech = cfg->chemistry;
     h->chem.solver = cfg->chem_solver;
@@ -529,6 +657,13 @@ fv_status fv_create(const fv_config* cfg, fv_handle** out) {
     const size_t stateBytes = sizeof(double) * h->nConserved * P.ncell;
     for (int b = 0; b < 2; ++b)
         if ((ce = cudaMalloc(&h->U[b], stateBytes)) != cudaSuccess) return bail(ce, "state");
+    if (cfg->order == FV_ORDER_SECOND_RK) {
+        // the second stage's state and the averaged concentrations c_0..c_N
+        if ((ce = cudaMalloc(&h->Ustage, stateBytes)) != cudaSuccess) return bail(ce, "stage state");
+        if ((ce = cudaMalloc(&h->conc, sizeof(double) * (cfg->n_species + 1) * P.ncell)) != cudaSuccess)
+            return bail(ce, "concentrations");
+        P.conc = h->conc;
+    }
     if ((ce = cudaMalloc(&h->prim0, sizeof(double) * (cfg->n_species + 4) * P.ncell)) != cudaSuccess)
         return bail(ce, "restart set");
     if ((ce = cudaMalloc(&h->ck, sizeof(DevClock))) != cudaSuccess) return bail(ce, "clock");
@@ -571,6 +706,8 @@ void fv_destroy(fv_handle* h) {
     for (auto& u : h->U)
         if (u) cudaFree(u);
     if (h->prim0) cudaFree(h->prim0);
+    if (h->Ustage) cudaFree(h->Ustage);
+    if (h->conc) cudaFree(h->conc);
     if (h->ck) cudaFree(h->ck);
     if (h->ckHost) cudaFreeHost(h->ckHost);
     if (h->blockMax) cudaFree(h->blockMax);
@@ -834,7 +971,9 @@ fv_status fv_check(fv_handle* h) {
 
 long long fv_kernels_per_step(const fv_handle* h) {
     if (!h) return 0;
-    return (h->path == PATH_MARCH ? 2 : 5) + (h->cfg.chemistry != FV_CHEM_NONE ? 1 : 0);
+    const int stage = h->path == PATH_MARCH ? 1 : 4;
+    if (h->cfg.order == FV_ORDER_SECOND_RK) return 2 * stage + 2;  // two stages, average, finalize
+    return stage + 1 + (h->cfg.chemistry != FV_CHEM_NONE ? 1 : 0);
 }
 
 // ---- introspection used by the tests and the bench (no reference counterpart)

@@ -5,7 +5,8 @@
 //             r-ratio TVD limiter (TVDLimiter.cpp:12-272, including its [direction][component]
 //             neighbour-gradient layout for the velocity tensor), reconstruction at every face
 //             of the cell (Advection.cpp:114-235), closure (:237-387), Hancock half step over the
-//             cell's own faces (HancockStage.cpp:17-240)
+//             cell's own faces (HancockStage.cpp:17-240); SecondOrderRK stages stop after the
+//             closure (Advection2dOrder.cpp, no predictor)
 //   k_fluxes  per face: ghost neighbour on boundary patches (HancockStage.cpp:324-446) and the
 //             Riemann flux
 //   k_update  per cell: divergence in the cell's face order, conservative update, gravity,
@@ -492,6 +493,12 @@ __global__ void k_faces(const StepParams P, const GenericLayout L, const T* __re
             st.p = dot + prim_i[NS + 3];
         }
         closeFromPrimitive<T, NS, EOS>(P.mix, st);
+        if (!P.hancock) {
+            // SecondOrderRK stage (Advection2dOrder.cpp): the closed reconstruction is the face state
+            soundSpeed<T, NS, EOS>(P.mix, st);
+            storeFace<T, NS>(FS, L.nfaces, g.own ? 0 : 1, g.f, st);
+            continue;
+        }
         const int a = fa[s];
         const T nsg = g.own ? T(g.sign) : T(-g.sign);
         const T S = T(g.S);
@@ -506,6 +513,7 @@ __global__ void k_faces(const StepParams P, const GenericLayout L, const T* __re
         divE += ((st.v[a] * st.E) * nsg + (st.v[a] * (st.p + T(0))) * nsg) * S;
         storeFace<T, NS>(FS, nf, g.own ? 0 : 1, g.f, st);
     }
+    if (!P.hancock) return;
 #pragma unroll
     for (int k = 0; k <= NS; ++k) divR[k] /= V;
 #pragma unroll

@@ -23,6 +23,8 @@ struct fv_handle {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double* U[2] = {nullptr, nullptr};
+    double* Ustage = nullptr;      // SecondOrderRK: state after the second stage
+    double* conc = nullptr;        // SecondOrderRK: averaged concentrations c_0..c_N
     int cur = 0;
     double* prim0 = nullptr;
     DevClock* ck = nullptr;        // device clock

@@ -47,6 +47,9 @@ struct StepParams {
     int nmom;               // momentum components carried (dims, or 3 when a transverse velocity is non-zero)
     int tma;                // 1: stage state rows into shared memory with bulk async copies (nx even)
     int warp2d;             // 1: FP32-flux 2D steps use the warp-strip march (k_warp2d) when nmom == 2
+    int hancock;            // 1: MUSCL-Hancock (SecondOrder); 0: no predictor (SecondOrderRK stages)
+    const double* conc;     // stored concentrations c_0..c_N (stride apart), read instead of rho_k / M_k
+                            // when not null and the restart set is not in use (SecondOrderRK)
     int limiter;
     int flux;
     int gravity;
@@ -135,11 +138,17 @@ __device__ __forceinline__ void cellPrimitive(const StepParams& P, const Src& sc
         p = T(prim[(NS + 3) * s + i]);
         return;
     }
-    c[0] = 0;
+    if (P.conc) {
+        // concentrations of the step's start state (averaged by the previous SecondOrderRK step)
 #pragma unroll
-    for (int k = 1; k <= NS; ++k) {
-        c[k] = rho[k] / T(P.mix.M[k - 1]);
-        c[0] += c[k];
+        for (int k = 0; k <= NS; ++k) c[k] = T(P.conc[k * s + i]);
+    } else {
+        c[0] = 0;
+#pragma unroll
+        for (int k = 1; k <= NS; ++k) {
+            c[k] = rho[k] / T(P.mix.M[k - 1]);
+            c[0] += c[k];
+        }
     }
 #pragma unroll
     for (int d = 0; d < 3; ++d) v[d] = d < P.nmom ? m[d] / rho0 : T(0);
@@ -158,18 +167,18 @@ __device__ __forceinline__ void cellPrimitive(const StepParams& P, const double*
     cellPrimitive<T, NS, EOS, D>(P, globalSrc(P, U, i), prim, i, c, v, p, rho0, rho, m, E);
 }
 
-// Predicted face state of a cell whose slopes vanish: closure, zero Hancock divergence,
-// recalculation from conserved values, sound speed.
+// Face state of a cell whose slopes vanish: closure, then (MUSCL-Hancock) the zero Hancock
+// divergence and the recalculation from conserved values, sound speed.
 template <typename T, int NS, int EOS>
 __device__ __forceinline__ void cellFaceState(const MixParams& mp, const T* c, const T* v, T p, FaceState<T, NS>& W,
-                                              int nmom = 3) {
+                                              int nmom = 3, bool hancock = true) {
 #pragma unroll
     for (int k = 1; k <= NS; ++k) W.c[k] = c[k];
 #pragma unroll
     for (int d = 0; d < 3; ++d) W.v[d] = v[d];
     W.p = p;
     closeFromPrimitive<T, NS, EOS>(mp, W);
-    closeFromConserved<T, NS, EOS>(mp, W, nmom);
+    if (hancock) closeFromConserved<T, NS, EOS>(mp, W, nmom);
     soundSpeed<T, NS, EOS>(mp, W);
 }
 
@@ -553,7 +562,7 @@ __device__ __forceinline__ void marchTile(const StepParams& P, const double* __r
         } else {
             T c[NS + 1], v[3], p, r0, rr2[NS + 1], mm[3], EE;
             cellPrimitive<T, NS, EOS, D>(P, sc, prim, cell, c, v, p, r0, rr2, mm, EE);
-            cellFaceState<T, NS, EOS>(P.mix, c, v, p, W, nmom);
+            cellFaceState<T, NS, EOS>(P.mix, c, v, p, W, nmom, P.hancock != 0);
 #pragma unroll
             for (int d = 0; d < 3; ++d) vp[d] = v[d];
         }

@@ -134,7 +134,9 @@ bool buildParams(const fv_config& c, StepParams& P) {
     if (c.flux != FV_FLUX_HLLC && c.flux != FV_FLUX_HLL) return false;
     if (c.limiter < 0 || c.limiter > FV_LIM_SCHMIDTMANN) return false;
     if (c.precision != FV_PREC_F64 && c.precision != FV_PREC_F32_FLUX) return false;
+    if (c.order != FV_ORDER_SECOND) return false;  // one MUSCL-Hancock stage only
     memset(&P, 0, sizeof(P));
+    P.hancock = 1;
     P.dims = c.dims;
     for (int a = 0; a < 3; ++a) {
         P.n[a] = a < c.dims ? c.n[a] : 1;

@@ -47,6 +47,9 @@ def _deck_cases():
                            BC("fixedValueCell", (0.3, 0.0, 0.0)), BC("fixedValueCell", 0.9))
     c.flux, c.limiter, c.courant_only, c.const_timestep = "HLL", "Schmidtmann", True, 1e-4
     out.append(("tube", c, p))
+    c, p = cases.kelvin_helmholtz_2d(n=8, periodic=False)
+    c.order = "SecondOrderRK"
+    out.append(("kh_rk2", c, p))
     return out
 
 
@@ -77,6 +80,7 @@ def test_print_config_matches_case(tmp_path, name, case, prim):
     assert got["g"] == list(want.g)
     assert got["bc_vel"] == list(want.bc_vel)
     assert got["bc_p"] == list(want.bc_p)
+    assert got["order"] == want.order
     assert got["t_end"] == case.t_end
     assert got["frequency"] == 3
     assert got["start"] == "1"

@@ -1,0 +1,102 @@
+"""SecondOrderRK on the GPU (two stages without the Hancock predictor, then the 0.5 average that
+keeps the averaged concentrations as state; secondOrderStepSolverRK.cpp, Advection2dOrder.cpp).
+
+The reference fixtures of this step solver (tests/golden/*_rk2*.npz) are checked step by step by
+test_gpu_parity.py; these tests cover the device time loop, the periodic mesh (which the reference
+cannot express) against the oracle, the FP32-flux arithmetic and the kernel count.
+"""
+
+import numpy as np
+import pytest
+
+from golden_cases import rel_err
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ["c1", "c2", "vx", "vy", "p", "rho", "E", "T"]
+
+
+@pytest.fixture(scope="module")
+def fv():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from schemi_b200 import fv as fvmod
+
+    fvmod.load()
+    return fvmod
+
+
+def _rk2(case):
+    case.order = "SecondOrderRK"
+    return case
+
+
+@pytest.mark.parametrize("limiter,path", [("vanLeer", "march"), ("linear", "generic")])
+def test_rk2_periodic_run_matches_oracle(fv, oracle_mod, limiter, path):
+    """Periodic KH through fv_run (CUDA graphs): FP64 within 1e-12 of the oracle."""
+    from schemi_b200 import cases
+
+    case, prim = cases.kelvin_helmholtz_2d(n=40, limiter=limiter)
+    _rk2(case)
+    case.t_end = 0.05
+    g = fv.FVCase(case)
+    g.upload(prim)
+    st = g.run(case.t_end)
+    oc = oracle_mod.OracleCase(case)
+    oc.upload(prim)
+    _, steps = oc.run(case.t_end)
+    assert st.steps == steps
+    assert g.time()[0] == oc.time()[0]
+    assert g.path == (fv.PATH_MARCH if path == "march" else fv.PATH_GENERIC)
+    a, b = g.download(), oc.download()
+    for f in FIELDS:
+        linf, _ = rel_err(a[f], b[f])
+        assert linf <= 1e-12, f"{f}: {linf:.3e}"
+
+
+def test_rk2_f32flux_within_tolerance(fv, oracle_mod):
+    """FP32-flux stages (warp-strip march) with the FP64 average: relative L1 <= 1e-5."""
+    from schemi_b200 import cases
+
+    case, prim = cases.kelvin_helmholtz_2d(n=64, precision="f32flux")
+    _rk2(case)
+    g = fv.FVCase(case)
+    g.upload(prim)
+    ref_case, _ = cases.kelvin_helmholtz_2d(n=64)
+    _rk2(ref_case)
+    oc = oracle_mod.OracleCase(ref_case)
+    oc.upload(prim)
+    for _ in range(15):
+        g.step()
+        oc.step()
+    a, b = g.download(), oc.download()
+    for f in ["c1", "c2", "vx", "p", "rho", "E"]:
+        _, l1 = rel_err(a[f], b[f])
+        assert l1 <= 1e-5, f"{f}: {l1:.3e}"
+
+
+def test_rk2_kernels_per_step(fv):
+    from schemi_b200 import cases
+
+    case, prim = cases.kelvin_helmholtz_2d(n=32)
+    g = fv.FVCase(_rk2(case))
+    assert g.kernels_per_step() == 4  # two march stages, the average, the CFL finalize
+    case, prim = cases.shock_tube_1d(n=50)
+    g = fv.FVCase(_rk2(case))
+    assert g.kernels_per_step() == 10  # two generic stages of four kernels, average, finalize
+
+
+def test_rk2_rejected_where_unsupported(fv):
+    from schemi_b200 import cases
+
+    case, prim = cases.chlorine_dissociation_2d(4)
+    _rk2(case)
+    with pytest.raises(fv.FVError):
+        fv.FVCase(case)
+    case, prim, _ = cases.richtmyer_meshkov(0, n=32, precision="f32flux")
+    g = fv.FVCase(_rk2(case))
+    g.upload(prim)
+    with pytest.raises(fv.FVError):
+        fv.FVBatch([g])
