@@ -102,9 +102,13 @@ enum fv_chemistry { FV_CHEM_NONE = 0, FV_CHEM_A_B_2C = 1, FV_CHEM_CL2 = 2 };
  *   SECOND_ORDER_RK  "SecondOrderRK": two stages of the TVD reconstruction without the Hancock
  *                    predictor (Advection2dOrder.cpp), then the 0.5 average with the step's start
  *                    state (secondOrderStepSolverRK.cpp:48-71, bunchOfFields::average); the
- *                    averaged concentrations are part of the state.  Not with chemistry, the
- *                    batched ensemble, the adjoint or fv_step_noalloc. */
-enum fv_step_solver { FV_ORDER_SECOND = 0, FV_ORDER_SECOND_RK = 1 };
+ *                    averaged concentrations are part of the state.
+ *   THIRD            "ThirdOrder": SSP-RK3 of three advections reconstructed with per-face limited
+ *                    surface gradients (Advection3dOrder.cpp, templates/thirdOrderLimiter.hpp),
+ *                    averages 0.25 and 2/3 with the start state (thirdOrderStepSolver.cpp:48-82).
+ * The multi-stage solvers run on the generic path (SecondOrderRK also on the fused march) and are
+ * not combined with chemistry, the batched ensemble, the adjoint or fv_step_noalloc. */
+enum fv_step_solver { FV_ORDER_SECOND = 0, FV_ORDER_SECOND_RK = 1, FV_ORDER_THIRD = 2 };
 
 /* Per-cell linear solver of the backward-Euler step (set/chemicalKinetics.txt #Iterative_solver:
  * "Gauss-Seidel", "Jacobi", "GaussElimination", "conjugateGradient", "JacobiConjugateGradient"). */

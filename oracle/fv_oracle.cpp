@@ -609,6 +609,140 @@ void gradVector(const fvo_case& cs, const std::vector<V3>& phi, std::vector<T9>&
     }
 }
 
+// ---------------------------------------------------------------- ThirdOrder reconstruction
+// Limiter functions without the xi bound, as calculateNoRSLimit applies them component by
+// component (the <Name>LimiterCalculation(r) overloads of src/limiters/*.cpp); linear returns
+// the gradient and zero returns zero (phiNoRSLinear / the caller).
+double limiterPhiNoRS(int lim, double r) {
+    switch (lim) {
+    case FV_LIM_ZERO: return 0;
+    case FV_LIM_MINMOD: return r <= 0. ? 0 : (r <= 1. ? r : 1.);
+    case FV_LIM_VANLEER: return r < 0. ? 0 : 2 * r / (1 + r);
+    case FV_LIM_LINEAR: return 1;
+    case FV_LIM_VANALBADA: return r <= 0. ? 0 : (r * r + r) / (1 + r * r);
+    case FV_LIM_HQUICK: return r <= 0. ? 0 : 4 * r / (3 + r);
+    case FV_LIM_VANLEER2: {
+        if (r <= 0.) return 0;
+        const double denom = 1 + r;
+        return 4 * r / (denom * denom);
+    }
+    case FV_LIM_SUPERBEE:
+        if (r <= 0.) return 0;
+        if (r <= 0.5) return 2 * r;
+        if (r <= 1.) return r;
+        return std::min(r, 2.0);
+    case FV_LIM_VANALBADA2: return r <= 0. ? 0 : 2 * r / (1 + r * r);
+    case FV_LIM_MINMOD2: return r <= 0. ? 0 : std::min(1.0, 4 * r / (1 + r));
+    case FV_LIM_SWEBY: {
+        const double b = 2.0;
+        return r <= 0. ? 0 : std::min(std::min(1.0, b * r), std::min(b, r));
+    }
+    case FV_LIM_KOREN: return r <= 0 ? 0 : std::min({2 * r, (1 + 2 * r) / 3, 2.0});
+    case FV_LIM_KOREN2:
+        if (r <= 0) return std::min(0.0, std::max(-kTwoThirds, (1 + 2 * r) / 3));
+        return std::min(2 * kTwoThirds * r, std::min((1 + 2 * r) / 3, 2.0));
+    case FV_LIM_UTCDFS:
+        if (r < -1) return r * (r + 1) / (r * r + 1);
+        if ((r >= -1) && (r < 0)) return 0;
+        if ((r >= 0) && (r < 0.5)) return r * r * r - 2 * (r * r) + 2 * r;
+        if ((r >= 0.5) && (r < 2)) return 0.75 * r + 0.25;
+        return (2 * (r * r) - 2 * r - 9.0 / 4.0) / (r * r - r - 1);
+    case FV_LIM_SCHMIDTMANN: {
+        const double alpha = 1, beta = 2, gamma = 1.5;
+        const double phiO3 = (2 + r) / 3;
+        return std::max(0.0, std::min(phiO3, std::max(-alpha * r, std::min({beta * r, phiO3, gamma}))));
+    }
+    }
+    return 0;
+}
+
+// centre of face f seen from cell i (the wrap face of a periodic axis sits one period further
+// on for its neighbour-side cell)
+V3 faceCentreFrom(long long i, const Face& F) {
+    return F.own == i ? F.rC : vsub(F.rC, F.neiShift);
+}
+
+// surfGrad of a scalar (gradient.hpp:96-168): inner faces (phi_N - phi_O) / |d|^2 * d, patches
+// (ghost - phi_O) / |dR| * dR / |dR| with dR = 2 (r_f - r_O)
+void surfGradScalar(const fvo_case& cs, const std::vector<double>& phi, int field, int k, std::vector<V3>& sg,
+                    bool& bad) {
+    const size_t nf = cs.faces.size();
+    sg.assign(nf, v3(0, 0, 0));
+    for (size_t f = 0; f < nf; ++f) {
+        const Face& F = cs.faces[f];
+        const V3& rO = cs.cells[F.own].rC;
+        if (F.nei >= 0) {
+            const V3 d = vsub(vadd(cs.cells[F.nei].rC, F.neiShift), rO);
+            const double m = mag3(d);
+            const double q = (phi[F.nei] - phi[F.own]) / (m * m);
+            sg[f] = v3(q * d.x[0], q * d.x[1], q * d.x[2]);
+        } else {
+            const double b = bcCellS(cs, phi[F.own], field, k, F.patch, bad);
+            const V3 dR = vmul(vsub(F.rC, rO), 2.);
+            const double dm = mag3(dR);
+            const V3 dn = vdiv(dR, dm);
+            const double q = (b - phi[F.own]) / dm;
+            sg[f] = v3(q * dn.x[0], q * dn.x[1], q * dn.x[2]);
+        }
+    }
+}
+
+void surfGradVector(const fvo_case& cs, const std::vector<V3>& phi, std::vector<T9>& sg, bool& bad) {
+    const size_t nf = cs.faces.size();
+    sg.assign(nf, T9{});
+    for (size_t f = 0; f < nf; ++f) {
+        const Face& F = cs.faces[f];
+        const V3& rO = cs.cells[F.own].rC;
+        if (F.nei >= 0) {
+            const V3 d = vsub(vadd(cs.cells[F.nei].rC, F.neiShift), rO);
+            const double m = mag3(d);
+            sg[f] = outer(vdiv(vsub(phi[F.nei], phi[F.own]), m * m), d);
+        } else {
+            const V3 b = bcCellV(cs, phi[F.own], F.patch, F.N, bad);
+            const V3 dR = vmul(vsub(F.rC, rO), 2.);
+            const double dm = mag3(dR);
+            const V3 dn = vdiv(dR, dm);
+            sg[f] = outer(vdiv(vsub(b, phi[F.own]), dm), dn);
+        }
+    }
+}
+
+// thirdOrderLimiter (templates/thirdOrderLimiter.hpp:19-72): for face s1 of a cell and its
+// farthest other face s2, r = g1 / (g2 + eps), retr = 1 / (r + eps), result
+// 0.5 ((1 - 1/3) phi(r) g2 + (1 + 1/3) phi(retr) g1), component by component.
+int farFace(const fvo_case& cs, long long i, int j) {
+    const Cell& c = cs.cells[i];
+    const V3 r1 = faceCentreFrom(i, cs.faces[c.faces[j]]);
+    int far = 0;
+    double best = 0;
+    for (int j2 = 0; j2 < c.nFaces; ++j2) {
+        if (j2 == j) continue;
+        const double dist = mag3(vsub(faceCentreFrom(i, cs.faces[c.faces[j2]]), r1));
+        if (best < dist) {
+            best = dist;
+            far = j2;
+        }
+    }
+    return far;
+}
+
+inline double thirdOrderComponent(int lim, double g1, double g2) {
+    const double r = g1 / (g2 + kStab);
+    const double retr = 1. / (r + kStab);
+    double limGrad, limOpp;
+    if (lim == FV_LIM_ZERO) {
+        limGrad = 0;
+        limOpp = 0;
+    } else if (lim == FV_LIM_LINEAR) {
+        limGrad = g1;
+        limOpp = g2;
+    } else {
+        limGrad = limiterPhiNoRS(lim, retr) * g1;
+        limOpp = limiterPhiNoRS(lim, r) * g2;
+    }
+    return 0.5 * ((1 - 1. / 3.) * limOpp + (1 + 1. / 3.) * limGrad);
+}
+
 // TVDLimiter for a scalar field (TVDLimiter.cpp:12-125)
 void tvdScalar(const fvo_case& cs, const std::vector<V3>& grad, const std::vector<double>& phi, int field, int k,
                std::vector<V3>& out, bool& bad) {
@@ -836,27 +970,38 @@ void cellPrimitivesFromConserved(fvo_case& cs, long long i) {
 
 // One advection of the state by dt: MUSCL-Hancock (Advection.cpp, hancock = true) or the same
 // TVD reconstruction without the predictor (Advection2dOrder.cpp:20-636, hancock = false), whose
-// boundary neighbour is the ghost of the reconstructed owner face (Advection2dOrder.cpp:394-522).
-int doStep(fvo_case& cs, double dt, bool hancock = true) {
+// boundary neighbour is the ghost of the reconstructed owner face (Advection2dOrder.cpp:394-522);
+// third = true reconstructs with the per-face limited surface gradients of Advection3dOrder.cpp
+// (no predictor either).
+int doStep(fvo_case& cs, double dt, bool hancock = true, bool third = false) {
     const Mix& mx = cs.mix;
     const int NS = mx.N;
     const long long nc = cs.nCells;
     const size_t nf = cs.faces.size();
     bool bad = false;
 
-    // 1. limited gradients (Advection.cpp:58-79)
+    // 1. limited gradients (Advection.cpp:58-79; Advection3dOrder.cpp:56-107 surface gradients)
     std::vector<V3> limC[FV_MAX_SPECIES + 1];
-    for (int k = 1; k <= NS; ++k) {
-        std::vector<V3> g;
-        gradScalar(cs, cs.c[k], 0, k - 1, g);
-        tvdScalar(cs, g, cs.c[k], 0, k - 1, limC[k], bad);
-    }
     std::vector<T9> gv, limV;
-    gradVector(cs, cs.v, gv);
-    tvdVector(cs, gv, cs.v, limV, bad);
     std::vector<V3> gp, limP;
-    gradScalar(cs, cs.p, 2, 0, gp);
-    tvdScalar(cs, gp, cs.p, 2, 0, limP, bad);
+    std::vector<V3> sgC[FV_MAX_SPECIES + 1], sgP;
+    std::vector<T9> sgV;
+    if (third) {
+        for (int k = 1; k <= NS; ++k) surfGradScalar(cs, cs.c[k], 0, k - 1, sgC[k], bad);
+        surfGradVector(cs, cs.v, sgV, bad);
+        surfGradScalar(cs, cs.p, 2, 0, sgP, bad);
+    } else {
+        for (int k = 1; k <= NS; ++k) {
+            std::vector<V3> g;
+            gradScalar(cs, cs.c[k], 0, k - 1, g);
+            tvdScalar(cs, g, cs.c[k], 0, k - 1, limC[k], bad);
+        }
+        gradVector(cs, cs.v, gv);
+        tvdVector(cs, gv, cs.v, limV, bad);
+        gradScalar(cs, cs.p, 2, 0, gp);
+        tvdScalar(cs, gp, cs.p, 2, 0, limP, bad);
+    }
+    const int lim = cs.cfg.limiter;
 
     // 2. reconstruction (Advection.cpp:114-235) and closure
     std::vector<FState> own(nf), nei(nf);
@@ -868,9 +1013,26 @@ int doStep(fvo_case& cs, double dt, bool hancock = true) {
             // across a periodic wrap face the neighbour-side cell sits one period further on
             const V3 delta = (F.own == i) ? vsub(F.rC, c.rC) : vsub(F.rC, vadd(c.rC, F.neiShift));
             FState s{};
-            for (int k = 1; k <= NS; ++k) s.c[k] = vdot(limC[k][i], delta) + cs.c[k][i];
-            s.v = vadd(tdot(limV[i], delta), cs.v[i]);
-            s.p = vdot(limP[i], delta) + cs.p[i];
+            if (third) {
+                // the cell's limited gradient for this face (thirdOrderLimiter) against its farthest face
+                const int far = farFace(cs, i, j);
+                const int f2 = c.faces[far];
+                for (int k = 1; k <= NS; ++k) {
+                    V3 lg;
+                    for (int q = 0; q < 3; ++q) lg.x[q] = thirdOrderComponent(lim, sgC[k][fi].x[q], sgC[k][f2].x[q]);
+                    s.c[k] = vdot(lg, delta) + cs.c[k][i];
+                }
+                T9 lv;
+                for (int q = 0; q < 9; ++q) lv.x[q] = thirdOrderComponent(lim, sgV[fi].x[q], sgV[f2].x[q]);
+                s.v = vadd(tdot(lv, delta), cs.v[i]);
+                V3 lp;
+                for (int q = 0; q < 3; ++q) lp.x[q] = thirdOrderComponent(lim, sgP[fi].x[q], sgP[f2].x[q]);
+                s.p = vdot(lp, delta) + cs.p[i];
+            } else {
+                for (int k = 1; k <= NS; ++k) s.c[k] = vdot(limC[k][i], delta) + cs.c[k][i];
+                s.v = vadd(tdot(limV[i], delta), cs.v[i]);
+                s.p = vdot(limP[i], delta) + cs.p[i];
+            }
             if (F.own == i) own[fi] = s;
             else nei[fi] = s;
         }
@@ -988,39 +1150,70 @@ int doStep(fvo_case& cs, double dt, bool hancock = true) {
     return FV_OK;
 }
 
-// ---------------------------------------------------------------- SecondOrderRK
-// secondOrderStepSolverRK::calculateStep (secondOrderStepSolverRK.cpp:48-71): two advections
-// without the predictor, then Un2.average(Un, 0.5) and copyFrom (bunchOfFields.hpp:166-237):
-// concentrations, densities, momentum and energy averaged field by field, then v = m / rho,
-// Uv = E - k - 0.5 rho (v & v), p = pFromUv(c, Uv).  The averaged concentrations are kept as
-// the state (the next step reconstructs from them).
-int rk2Step(fvo_case& cs, double dt) {
-    const int NS = cs.mix.N;
-    const long long nc = cs.nCells;
-    std::vector<double> c0[FV_MAX_SPECIES + 1], r0[FV_MAX_SPECIES + 1], E0 = cs.E;
-    std::vector<V3> m0 = cs.m;
-    for (int k = 0; k <= NS; ++k) {
-        c0[k] = cs.c[k];
-        r0[k] = cs.rho[k];
+// ---------------------------------------------------------------- SecondOrderRK / ThirdOrder
+// The state a multi-stage step keeps as its start state Un.
+struct StartState {
+    std::vector<double> c[FV_MAX_SPECIES + 1], rho[FV_MAX_SPECIES + 1], E;
+    std::vector<V3> m;
+};
+
+StartState saveState(const fvo_case& cs) {
+    StartState u;
+    for (int k = 0; k <= cs.mix.N; ++k) {
+        u.c[k] = cs.c[k];
+        u.rho[k] = cs.rho[k];
     }
-    int st = doStep(cs, dt, false);
-    if (st != FV_OK) return st;
-    st = doStep(cs, dt, false);
-    if (st != FV_OK) return st;
-    const double own = 0.5, in = 1 - own;
-    for (long long i = 0; i < nc; ++i) {
+    u.E = cs.E;
+    u.m = cs.m;
+    return u;
+}
+
+// gasPhase = (gasPhase).average(Un, ownWeight) followed by copyFrom (bunchOfFields.hpp:166-237):
+// concentrations, densities, momentum and energy averaged field by field, then v = m / rho,
+// Uv = E - k - 0.5 rho (v & v), p = pFromUv(c, Uv).  The averaged concentrations stay the state
+// (the next stage or step reconstructs from them).
+void averageWith(fvo_case& cs, const StartState& u, double ownWeight) {
+    const int NS = cs.mix.N;
+    const double own = ownWeight, in = 1 - ownWeight;
+    for (long long i = 0; i < cs.nCells; ++i) {
         for (int k = 0; k <= NS; ++k) {
-            cs.c[k][i] = own * cs.c[k][i] + in * c0[k][i];
-            cs.rho[k][i] = own * cs.rho[k][i] + in * r0[k][i];
+            cs.c[k][i] = own * cs.c[k][i] + in * u.c[k][i];
+            cs.rho[k][i] = own * cs.rho[k][i] + in * u.rho[k][i];
         }
-        for (int d = 0; d < 3; ++d) cs.m[i].x[d] = cs.m[i].x[d] * own + m0[i].x[d] * in;
-        cs.E[i] = own * cs.E[i] + in * E0[i];
+        for (int d = 0; d < 3; ++d) cs.m[i].x[d] = cs.m[i].x[d] * own + u.m[i].x[d] * in;
+        cs.E[i] = own * cs.E[i] + in * u.E[i];
         cs.v[i] = vdiv(cs.m[i], cs.rho[0][i]);
         cs.Uv[i] = (cs.E[i] - 0.0) - 0.5 * cs.rho[0][i] * vdot(cs.v[i], cs.v[i]);
         double cc[FV_MAX_SPECIES + 1];
         for (int k = 0; k <= NS; ++k) cc[k] = cs.c[k][i];
         cs.p[i] = cs.mix.pFromUv(cc, cs.Uv[i]);
     }
+}
+
+// secondOrderStepSolverRK::calculateStep (secondOrderStepSolverRK.cpp:48-71): two advections
+// without the predictor, then Un2.average(Un, 0.5).
+int rk2Step(fvo_case& cs, double dt) {
+    const StartState u = saveState(cs);
+    int st = doStep(cs, dt, false);
+    if (st != FV_OK) return st;
+    st = doStep(cs, dt, false);
+    if (st != FV_OK) return st;
+    averageWith(cs, u, 0.5);
+    return FV_OK;
+}
+
+// thirdOrderStepSolver::calculateStep (thirdOrderStepSolver.cpp:48-82): SSP-RK3 of
+// Advection3dOrder -- U1 = L(Un), U2 = 0.25 L(U1) + 0.75 Un, U3 = 2/3 L(U2) + 1/3 Un.
+int rk3Step(fvo_case& cs, double dt) {
+    const StartState u = saveState(cs);
+    int st = doStep(cs, dt, false, true);
+    if (st != FV_OK) return st;
+    st = doStep(cs, dt, false, true);
+    if (st != FV_OK) return st;
+    averageWith(cs, u, 0.25);
+    st = doStep(cs, dt, false, true);
+    if (st != FV_OK) return st;
+    averageWith(cs, u, kTwoThirds);
     return FV_OK;
 }
 
@@ -1400,9 +1593,12 @@ bool validate(const fv_config& cf, std::string& err) {
     if (cf.chemistry == FV_CHEM_CL2 && cf.n_species != 2) { err = "Cl2 dissociation needs 2 species"; return false; }
     if (cf.chemistry == FV_CHEM_A_B_2C && cf.n_species != 3) { err = "A+B->2C needs 3 species"; return false; }
     if (cf.chemistry < FV_CHEM_NONE || cf.chemistry > FV_CHEM_CL2) { err = "unknown chemistry"; return false; }
-    if (cf.order != FV_ORDER_SECOND && cf.order != FV_ORDER_SECOND_RK) { err = "unknown step solver"; return false; }
-    if (cf.order == FV_ORDER_SECOND_RK && cf.chemistry != FV_CHEM_NONE) {
-        err = "SecondOrderRK with chemistry is not implemented";
+    if (cf.order != FV_ORDER_SECOND && cf.order != FV_ORDER_SECOND_RK && cf.order != FV_ORDER_THIRD) {
+        err = "unknown step solver";
+        return false;
+    }
+    if (cf.order != FV_ORDER_SECOND && cf.chemistry != FV_CHEM_NONE) {
+        err = "multi-stage step solvers with chemistry are not implemented";
         return false;
     }
     return true;
@@ -1498,7 +1694,9 @@ int fvo_upload(fvo_case* cs, const double* const* prim) {
 
 int fvo_step(fvo_case* cs, double* dt_used, double* dt_next) {
     const double dt = cs->dt;
-    int st = cs->cfg.order == FV_ORDER_SECOND_RK ? rk2Step(*cs, dt) : doStep(*cs, dt);
+    int st = cs->cfg.order == FV_ORDER_SECOND_RK ? rk2Step(*cs, dt)
+             : cs->cfg.order == FV_ORDER_THIRD   ? rk3Step(*cs, dt)
+                                                 : doStep(*cs, dt);
     if (st != FV_OK) return st;
     if (cs->cfg.chemistry != FV_CHEM_NONE) {
         // secondOrderStepSolver::calculateStep: chemistry after the advection, same dt

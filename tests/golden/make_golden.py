@@ -87,6 +87,29 @@ def golden_cases():
     c.order = "SecondOrderRK"
     c.g_delta = (0.0, -0.02, 0.0)
     out.append(("rt_16x48_rk2_gravity", c, p, 10, [1, 10]))
+    # ThirdOrder: SSP-RK3 with the directional limiter of thirdOrderLimiter.hpp
+    c, p = cases.kelvin_helmholtz_2d(n=24, periodic=False)
+    c.order = "ThirdOrder"
+    out.append(("kh_slip_24_rk3", c, p, 8, [1, 2, 8]))
+    c, p = cases.kelvin_helmholtz_2d(n=20, periodic=False, limiter="Sweby")
+    c.order = "ThirdOrder"
+    out.append(("kh_slip_20_rk3_sweby", c, p, 6, [1, 6]))
+    c, p = cases.kelvin_helmholtz_2d(n=20, periodic=False, limiter="Schmidtmann")
+    c.order = "ThirdOrder"
+    out.append(("kh_slip_20_rk3_schmidtmann", c, p, 6, [1, 6]))
+    c, p = cases.shock_tube_1d(n=200)
+    c.order = "ThirdOrder"
+    out.append(("tube_rk3_minmod_200", c, p, 30, [1, 2, 30]))
+    c, p = cases.rayleigh_taylor_2d(nx=16, ny=48, modes=4)
+    c.order = "ThirdOrder"
+    out.append(("rt_16x48_rk3_gravity", c, p, 8, [1, 8]))
+    c, p = cases.shock_tube_1d(n=100)
+    c.bc["tail"] = PatchBC([BC("fixedValueCell", 1.0), BC("fixedValueCell", 0.0)],
+                           BC("fixedValueCell", (0.2, 0.0, 0.0)), BC("fixedValueCell", 1.0))
+    c.bc["point"] = PatchBC([BC("slip"), BC("slip")], BC("slip"), BC("slip"))
+    c.order = "ThirdOrder"
+    c.limiter = "vanAlbada"
+    out.append(("tube_rk3_fixedvalue_slip_100", c, p, 20, [1, 20]))
     return out
 
 

@@ -52,6 +52,23 @@ def test_oracle_riemann_failure_matches_reference(oracle_mod):
         oc.step()
 
 
+@pytest.mark.parametrize("limiter,fails_at", [("Koren", 1), ("vanAlbada", 1), ("HQUICK", 2)])
+def test_oracle_third_order_riemann_failure_matches_reference(oracle_mod, limiter, fails_at):
+    """ThirdOrder with these limiters on the slip-walled KH layer ends in the reference with
+    "Fatal error in Riemann solver." at the listed step (20 cells: Koren, vanAlbada at the first
+    step; 10 cells: HQUICK at the second); the oracle reports RiemannSolverError at the same step."""
+    from schemi_b200 import cases
+
+    c, p = cases.kelvin_helmholtz_2d(n=20 if fails_at == 1 else 10, periodic=False, limiter=limiter)
+    c.order = "ThirdOrder"
+    oc = oracle_mod.OracleCase(c)
+    oc.upload(p)
+    for _ in range(fails_at - 1):
+        oc.step()
+    with pytest.raises(RuntimeError, match="status 1"):
+        oc.step()
+
+
 def test_oracle_chemistry_jcg_failure_matches_reference(oracle_mod):
     """With the Jacobi-preconditioned CG solver the hot Cl2 case does not converge; the reference
     divides the first step (1e-15) by ten, finds it below the minimal time step, prints "Timestep
