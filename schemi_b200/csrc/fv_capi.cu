@@ -109,17 +109,19 @@ __global__ void k_transverse(const StepParams P, const double* __restrict__ prim
 // U0, then main's CFL signal of the averaged state.  Concentrations are averaged as fields: c of
 // U2 is rho_k / M_k with c_0 their sum (Advection2dOrder.cpp:578-585), c of U0 the stored ones
 // (or the restart set before step 1).  Writes the averaged state to Un and conc.
+// ThirdOrder uses the same kernel with the weights 0.25 and 2/3 (thirdOrderStepSolver.cpp:64-82),
+// reading the start state's concentrations from concIn and writing the averaged ones to concOut.
 template <int NS, int EOS, int D>
 __global__ void k_rk_average(const StepParams P, const double* __restrict__ U2, const double* __restrict__ U0,
                              const double* __restrict__ prim0, DevClock* __restrict__ ck, double* __restrict__ Un,
-                             double* __restrict__ conc, double* __restrict__ blockMax) {
+                             const double* concIn, double* concOut, double ownWeight, double* __restrict__ blockMax) {
     __shared__ double red[32];
     if (ck->done) return;
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     double localMax = -1;
     if (i < P.ncell) {
         const long long s = P.stride;
-        const double own = 0.5, in = 1 - own;
+        const double own = ownWeight, in = 1 - ownWeight;
         double c2[NS + 1], c0[NS + 1], c[NS + 1];
         c2[0] = 0;
 #pragma unroll
@@ -136,12 +138,12 @@ __global__ void k_rk_average(const StepParams P, const double* __restrict__ U2, 
             }
         } else {
 #pragma unroll
-            for (int k = 0; k <= NS; ++k) c0[k] = conc[k * s + i];
+            for (int k = 0; k <= NS; ++k) c0[k] = concIn[k * s + i];
         }
 #pragma unroll
         for (int k = 0; k <= NS; ++k) {
             c[k] = own * c2[k] + in * c0[k];
-            conc[k * s + i] = c[k];
+            concOut[k * s + i] = c[k];
         }
         double rho[NS + 1];
 #pragma unroll
@@ -264,9 +266,12 @@ bool validate(const fv_config& c, std::string& e) {
     if (c.chemistry < FV_CHEM_NONE || c.chemistry > FV_CHEM_CL2) { e = "unknown chemistry"; return false; }
     if (c.chemistry == FV_CHEM_A_B_2C && c.n_species != 3) { e = "A+B->2C needs 3 species (A, B, C)"; return false; }
     if (c.chemistry == FV_CHEM_CL2 && c.n_species != 2) { e = "Cl2 dissociation needs 2 species (Cl2, Cl)"; return false; }
-    if (c.order != FV_ORDER_SECOND && c.order != FV_ORDER_SECOND_RK) { e = "unknown step solver (order)"; return false; }
-    if (c.order == FV_ORDER_SECOND_RK && c.chemistry != FV_CHEM_NONE) {
-        e = "SecondOrderRK with chemistry is not implemented";
+    if (c.order != FV_ORDER_SECOND && c.order != FV_ORDER_SECOND_RK && c.order != FV_ORDER_THIRD) {
+        e = "unknown step solver (order)";
+        return false;
+    }
+    if (c.order != FV_ORDER_SECOND && c.chemistry != FV_CHEM_NONE) {
+        e = "multi-stage step solvers with chemistry are not implemented";
         return false;
     }
     if (c.chemistry != FV_CHEM_NONE) {
@@ -409,14 +414,26 @@ long long stepBlocks(fv_handle* h) {
 }
 
 // enqueue step [+ chemistry] + finalize reading U[from]
+// (Ustage, U[from]) averaged into U[from ^ 1]
 template <int NS, int EOS>
-void launchAverage(fv_handle* h, int from) {
+void launchAverage(fv_handle* h, int from, const double* concIn, double* concOut, double ownWeight) {
     const int tpb = 128;
     const unsigned g = (unsigned)genericBlocks(h->P);
     switch (h->cfg.dims) {
-    case 1: k_rk_average<NS, EOS, 1><<<g, tpb, 0, h->stream>>>(h->P, h->Ustage, h->U[from], h->prim0, h->ck, h->U[from ^ 1], h->conc, h->blockMax); break;
-    case 2: k_rk_average<NS, EOS, 2><<<g, tpb, 0, h->stream>>>(h->P, h->Ustage, h->U[from], h->prim0, h->ck, h->U[from ^ 1], h->conc, h->blockMax); break;
-    default: k_rk_average<NS, EOS, 3><<<g, tpb, 0, h->stream>>>(h->P, h->Ustage, h->U[from], h->prim0, h->ck, h->U[from ^ 1], h->conc, h->blockMax); break;
+    case 1: k_rk_average<NS, EOS, 1><<<g, tpb, 0, h->stream>>>(h->P, h->Ustage, h->U[from], h->prim0, h->ck, h->U[from ^ 1], concIn, concOut, ownWeight, h->blockMax); break;
+    case 2: k_rk_average<NS, EOS, 2><<<g, tpb, 0, h->stream>>>(h->P, h->Ustage, h->U[from], h->prim0, h->ck, h->U[from ^ 1], concIn, concOut, ownWeight, h->blockMax); break;
+    default: k_rk_average<NS, EOS, 3><<<g, tpb, 0, h->stream>>>(h->P, h->Ustage, h->U[from], h->prim0, h->ck, h->U[from ^ 1], concIn, concOut, ownWeight, h->blockMax); break;
+    }
+}
+
+void average(fv_handle* h, int from, const double* concIn, double* concOut, double ownWeight) {
+    const int ns = h->cfg.n_species;
+    const bool vdw = h->cfg.eos == FV_EOS_VAN_DER_WAALS;
+    switch (ns) {
+    case 1: vdw ? launchAverage<1, 1>(h, from, concIn, concOut, ownWeight) : launchAverage<1, 0>(h, from, concIn, concOut, ownWeight); break;
+    case 2: vdw ? launchAverage<2, 1>(h, from, concIn, concOut, ownWeight) : launchAverage<2, 0>(h, from, concIn, concOut, ownWeight); break;
+    case 3: vdw ? launchAverage<3, 1>(h, from, concIn, concOut, ownWeight) : launchAverage<3, 0>(h, from, concIn, concOut, ownWeight); break;
+    default: vdw ? launchAverage<4, 1>(h, from, concIn, concOut, ownWeight) : launchAverage<4, 0>(h, from, concIn, concOut, ownWeight); break;
     }
 }
 
@@ -436,22 +453,44 @@ cudaError_t enqueueRk2(fv_handle* h, int from) {
     if (e != cudaSuccess) return e;
     e = f64 ? launchStepF64(P2, B2, h->path, h->shape, h->stream) : launchStepF32(P2, B2, h->path, h->shape, h->stream);
     if (e != cudaSuccess) return e;
-    const int ns = h->cfg.n_species;
-    const bool vdw = h->cfg.eos == FV_EOS_VAN_DER_WAALS;
-    switch (ns) {
-    case 1: vdw ? launchAverage<1, 1>(h, from) : launchAverage<1, 0>(h, from); break;
-    case 2: vdw ? launchAverage<2, 1>(h, from) : launchAverage<2, 0>(h, from); break;
-    case 3: vdw ? launchAverage<3, 1>(h, from) : launchAverage<3, 0>(h, from); break;
-    default: vdw ? launchAverage<4, 1>(h, from) : launchAverage<4, 0>(h, from); break;
-    }
+    average(h, from, h->conc, h->conc, 0.5);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_finalize<<<1, 1024, 0, h->stream>>>(h->P, h->ck, h->blockMax, (int)genericBlocks(h->P));
     return cudaGetLastError();
 }
 
+// ThirdOrder (SSP-RK3): stage 1 U[from] -> U[from ^ 1]; stage 2 U[from ^ 1] -> Ustage;
+// average 0.25 (Ustage, U[from]) -> U[from ^ 1] with its concentrations in concStage; stage 3
+// U[from ^ 1] (concentrations concStage) -> Ustage; average 2/3 (Ustage, U[from]) -> U[from ^ 1]
+// with the CFL partials; finalize.
+cudaError_t enqueueRk3(fv_handle* h, int from) {
+    const bool f64 = h->cfg.precision == FV_PREC_F64;
+    auto stage = [&](const StepParams& Ps, const double* in, double* out, const double* prim) {
+        StepBuffers B = buffersFor(h, from);
+        B.U = in;
+        B.Un = out;
+        B.prim0 = prim;
+        return f64 ? launchStepF64(Ps, B, h->path, h->shape, h->stream) : launchStepF32(Ps, B, h->path, h->shape, h->stream);
+    };
+    StepParams P2 = h->P, P3 = h->P;
+    P2.conc = nullptr;         // the first stage's own rho_k / M_k
+    P3.conc = h->concStage;    // the 0.25 average's concentrations
+    cudaError_t e = stage(h->P, h->U[from], h->U[from ^ 1], h->prim0);
+    if (e != cudaSuccess) return e;
+    if ((e = stage(P2, h->U[from ^ 1], h->Ustage, nullptr)) != cudaSuccess) return e;
+    average(h, from, h->conc, h->concStage, 0.25);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = stage(P3, h->U[from ^ 1], h->Ustage, nullptr)) != cudaSuccess) return e;
+    average(h, from, h->conc, h->conc, 2. / 3.);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_finalize<<<1, 1024, 0, h->stream>>>(h->P, h->ck, h->blockMax, (int)genericBlocks(h->P));
+    return cudaGetLastError();
+}
+
 cudaError_t enqueueStep(fv_handle* h, int from) {
     if (h->cfg.order == FV_ORDER_SECOND_RK) return enqueueRk2(h, from);
+    if (h->cfg.order == FV_ORDER_THIRD) return enqueueRk3(h, from);
     const StepBuffers B = buffersFor(h, from);
     cudaError_t e = h->cfg.precision == FV_PREC_F64 ? launchStepF64(h->P, B, h->path, h->shape, h->stream)
                                                      : launchStepF32(h->P, B, h->path, h->shape, h->stream);
@@ -503,6 +542,7 @@ fv_status ensureScratch(fv_handle* h) {
 
 int choosePath(const fv_config& c) {
     if (c.dims < 2) return PATH_GENERIC;
+    if (c.order == FV_ORDER_THIRD) return PATH_GENERIC;  // directional slopes: k_faces3
     for (int a = 0; a < c.dims; ++a)
         if (c.n[a] < 2) return PATH_GENERIC;
     return limiterZeroForNonPositiveR(c.limiter) ? PATH_MARCH : PATH_GENERIC;
@@ -615,6 +655,7 @@ fv_status fv_create(const fv_config* cfg, fv_handle** out) {
                 P.ncell * (cfg->n_species + 5) < (1LL << 31)) ? 1 : 0;
     if (P.warp2d) P.tma = 1;
     P.hancock = cfg->order == FV_ORDER_SECOND ? 1 : 0;
+    P.third = cfg->order == FV_ORDER_THIRD ? 1 : 0;
     h->path = choosePath(*cfg);
     h->chem.mech = cfg->chemistry;
     h->chem.solver = cfg->chem_solver;
@@ -657,11 +698,14 @@ fv_status fv_create(const fv_config* cfg, fv_handle** out) {
     const size_t stateBytes = sizeof(double) * h->nConserved * P.ncell;
     for (int b = 0; b < 2; ++b)
         if ((ce = cudaMalloc(&h->U[b], stateBytes)) != cudaSuccess) return bail(ce, "state");
-    if (cfg->order == FV_ORDER_SECOND_RK) {
-        // the second stage's state and the averaged concentrations c_0..c_N
+    if (cfg->order != FV_ORDER_SECOND) {
+        // the last stage's state and the averaged concentrations c_0..c_N (ThirdOrder: also those
+        // of its intermediate average)
+        const size_t concBytes = sizeof(double) * (cfg->n_species + 1) * P.ncell;
         if ((ce = cudaMalloc(&h->Ustage, stateBytes)) != cudaSuccess) return bail(ce, "stage state");
-        if ((ce = cudaMalloc(&h->conc, sizeof(double) * (cfg->n_species + 1) * P.ncell)) != cudaSuccess)
-            return bail(ce, "concentrations");
+        if ((ce = cudaMalloc(&h->conc, concBytes)) != cudaSuccess) return bail(ce, "concentrations");
+        if (cfg->order == FV_ORDER_THIRD && (ce = cudaMalloc(&h->concStage, concBytes)) != cudaSuccess)
+            return bail(ce, "stage concentrations");
         P.conc = h->conc;
     }
     if ((ce = cudaMalloc(&h->prim0, sizeof(double) * (cfg->n_species + 4) * P.ncell)) != cudaSuccess)
@@ -708,6 +752,7 @@ void fv_destroy(fv_handle* h) {
     if (h->prim0) cudaFree(h->prim0);
     if (h->Ustage) cudaFree(h->Ustage);
     if (h->conc) cudaFree(h->conc);
+    if (h->concStage) cudaFree(h->concStage);
     if (h->ck) cudaFree(h->ck);
     if (h->ckHost) cudaFreeHost(h->ckHost);
     if (h->blockMax) cudaFree(h->blockMax);
@@ -973,6 +1018,7 @@ long long fv_kernels_per_step(const fv_handle* h) {
     if (!h) return 0;
     const int stage = h->path == PATH_MARCH ? 1 : 4;
     if (h->cfg.order == FV_ORDER_SECOND_RK) return 2 * stage + 2;  // two stages, average, finalize
+    if (h->cfg.order == FV_ORDER_THIRD) return 3 * stage + 3;      // three stages, two averages, finalize
     return stage + 1 + (h->cfg.chemistry != FV_CHEM_NONE ? 1 : 0);
 }
 

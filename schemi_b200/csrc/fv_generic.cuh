@@ -535,6 +535,252 @@ __global__ void k_faces(const StepParams P, const GenericLayout L, const T* __re
     }
 }
 
+// ---------------------------------------------------------------------------- k_faces3
+// ThirdOrder reconstruction (Advection3dOrder.cpp:56-235 with templates/thirdOrderLimiter.hpp):
+// surface gradients at every face of the cell (gradient.hpp:96-168: inner faces
+// (phi_N - phi_O) / |d|^2 * d, patches (ghost - phi_O) / |dR| * dR / |dR| with dR = 2 (r_f - r_O)),
+// for each face the limited gradient against the cell's farthest other face, component by
+// component 0.5 ((1 - 1/3) phi(r) g_far + (1 + 1/3) phi(1 / (r + eps)) g_face) with
+// r = g_face / (g_far + eps) and the limiter without its xi bound, then the face value
+// phi_i + g . delta, closure and sound speed (no predictor).
+
+// <Name>LimiterCalculation(r) of src/limiters/*.cpp (calculateNoRSLimit); linear: 1.
+template <typename T> __device__ __forceinline__ T limiterPhiNoRS(int lim, T r) {
+    const T one = 1, two = 2;
+    switch (lim) {
+    case FV_LIM_ZERO: return 0;
+    case FV_LIM_MINMOD: return r <= T(0) ? T(0) : (r <= one ? r : one);
+    case FV_LIM_VANLEER: return r < T(0) ? T(0) : two * r / (one + r);
+    case FV_LIM_LINEAR: return one;
+    case FV_LIM_VANALBADA: return r <= T(0) ? T(0) : (r * r + r) / (one + r * r);
+    case FV_LIM_HQUICK: return r <= T(0) ? T(0) : T(4) * r / (T(3) + r);
+    case FV_LIM_VANLEER2: {
+        if (r <= T(0)) return 0;
+        const T denom = one + r;
+        return T(4) * r / (denom * denom);
+    }
+    case FV_LIM_SUPERBEE:
+        if (r <= T(0)) return 0;
+        if (r <= T(0.5)) return two * r;
+        if (r <= one) return r;
+        return smin(r, two);
+    case FV_LIM_VANALBADA2: return r <= T(0) ? T(0) : two * r / (one + r * r);
+    case FV_LIM_MINMOD2: return r <= T(0) ? T(0) : smin(one, T(4) * r / (one + r));
+    case FV_LIM_SWEBY: {
+        const T b = 2;
+        return r <= T(0) ? T(0) : smin(smin(one, b * r), smin(b, r));
+    }
+    case FV_LIM_KOREN: return r <= T(0) ? T(0) : smin(smin(two * r, (one + two * r) / T(3)), two);
+    case FV_LIM_KOREN2: {
+        const T tt = T(2. / 3.);
+        if (r <= T(0)) return smin(T(0), smax(-tt, (one + two * r) / T(3)));
+        return smin(two * tt * r, smin((one + two * r) / T(3), two));
+    }
+    case FV_LIM_UTCDFS:
+        if (r < T(-1)) return r * (r + one) / (r * r + one);
+        if ((r >= T(-1)) && (r < T(0))) return 0;
+        if ((r >= T(0)) && (r < T(0.5))) return r * r * r - two * (r * r) + two * r;
+        if ((r >= T(0.5)) && (r < two)) return T(0.75) * r + T(0.25);
+        return (two * (r * r) - two * r - T(9.0 / 4.0)) / (r * r - r - one);
+    case FV_LIM_SCHMIDTMANN: {
+        const T alpha = 1, beta = 2, gamma = 1.5;
+        const T phiO3 = (two + r) / T(3);
+        return smax(T(0), smin(phiO3, smax(-alpha * r, smin(smin(beta * r, phiO3), gamma))));
+    }
+    }
+    return 0;
+}
+
+template <typename T> __device__ __forceinline__ T thirdOrderComponent(int lim, T g1, T g2) {
+    const T r = g1 / (g2 + Num<T>::stab());
+    const T retr = T(1) / (r + Num<T>::stab());
+    T limGrad, limOpp;
+    if (lim == FV_LIM_ZERO) {
+        limGrad = T(0);
+        limOpp = T(0);
+    } else if (lim == FV_LIM_LINEAR) {
+        limGrad = g1;
+        limOpp = g2;
+    } else {
+        limGrad = limiterPhiNoRS<T>(lim, retr) * g1;
+        limOpp = limiterPhiNoRS<T>(lim, r) * g2;
+    }
+    return T(0.5) * ((T(1) - T(1. / 3.)) * limOpp + (T(1) + T(1. / 3.)) * limGrad);
+}
+
+template <typename T, int NS, int EOS, int D>
+__global__ void k_faces3(const StepParams P, const GenericLayout L, const T* __restrict__ Pc, DevClock* __restrict__ ck,
+                         T* __restrict__ FS) {
+    if (ck->done) return;
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= P.ncell) return;
+    const long long n = P.ncell;
+    const int nx = P.n[0], ny = P.n[1];
+    int ijk[3];
+    ijk[0] = (int)(i % nx);
+    ijk[1] = D >= 2 ? (int)((i / nx) % ny) : 0;
+    ijk[2] = D >= 3 ? (int)(i / ((long long)nx * ny)) : 0;
+    const T rc[3] = {T(P.geo.cc[0][ijk[0]]), T(P.geo.cc[1][ijk[1]]), T(P.geo.cc[2][ijk[2]])};
+    bool bad = false;
+    const int lim = P.limiter;
+
+    // faces of the cell in mesh.cpp order: [x-, x+, y+, y-, z-, z+]
+    constexpr int NFC = 2 * D;
+    int fa[NFC], fh[NFC];
+    {
+        int q = 0;
+        fa[q] = 0; fh[q++] = 0;
+        fa[q] = 0; fh[q++] = 1;
+        if (D >= 2) { fa[q] = 1; fh[q++] = 1; fa[q] = 1; fh[q++] = 0; }
+        if (D >= 3) { fa[q] = 2; fh[q++] = 0; fa[q] = 2; fh[q++] = 1; }
+    }
+    FaceGeo fg[NFC];
+    long long nbIdx[NFC];
+    T nbSh[NFC];     // periodic shift of the neighbour across face s along its axis
+    T fc[NFC][3];    // face centre seen from this cell
+#pragma unroll
+    for (int s = 0; s < NFC; ++s) {
+        fg[s] = faceOf(P, L, ijk, fa[s], fh[s]);
+        int nb[3];
+        double sh = 0;
+        nbIdx[s] = -1;
+        nbSh[s] = T(0);
+        if (!fg[s].boundary && neighbourOf(P, ijk, fa[s], fh[s], nb, sh)) {
+            nbIdx[s] = cellIndex(P, nb[0], nb[1], nb[2]);
+            nbSh[s] = T(sh);
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            fc[s][d] = (!fg[s].own && !fg[s].boundary && d == fa[s]) ? T(fg[s].rc[d]) + nbSh[s] : T(fg[s].rc[d]);
+    }
+    T prim_i[NS + 4];
+#pragma unroll
+    for (int q = 0; q < NS + 4; ++q) prim_i[q] = primAt<T, NS>(Pc, n, q, i);
+
+    // surface gradients: scalars (c_1..c_N, p) sgS[s][j][3], velocity sgV[s][9] ([3*component + direction])
+    constexpr int NSC = NS + 1;
+    T sgS[NFC][NSC][3];
+    T sgV[NFC][9];
+#pragma unroll
+    for (int s = 0; s < NFC; ++s) {
+        const FaceGeo& g = fg[s];
+        const int a = fa[s];
+        if (g.boundary) {
+            T d3[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) d3[d] = (T(g.rc[d]) - rc[d]) * T(2);
+            const T dm = mag3<T>(d3[0], d3[1], d3[2]);
+            const T dn[3] = {d3[0] / dm, d3[1] / dm, d3[2] / dm};
+#pragma unroll
+            for (int j = 0; j < NSC; ++j) {
+                const int q = j < NS ? j : NS + 3;
+                const T b = cellGhostScalar<T, NS>(P, g.patch, q, prim_i[q], bad);
+                const T qv = (b - prim_i[q]) / dm;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) sgS[s][j][d] = qv * dn[d];
+            }
+            const T vi[3] = {prim_i[NS], prim_i[NS + 1], prim_i[NS + 2]};
+            T gv[3];
+            ghostVelocity<T>(P.bc.vel[g.patch], P.bc.vel_value[g.patch], a, g.sign, vi, gv);
+            if (P.bc.vel[g.patch] == FV_BC_FIXED_SURFACE) bad = true;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const T qv = (gv[c] - vi[c]) / dm;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) sgV[s][3 * c + d] = qv * dn[d];
+            }
+        } else {
+            // the face's owner and neighbour cells; the neighbour centre shifted by one period
+            // across a wrap face
+            const long long j = nbIdx[s];
+            const int nbAxis = fh[s] ? ijk[a] + 1 : ijk[a] - 1;
+            const int na = P.n[a];
+            const int nbA = nbAxis < 0 ? nbAxis + na : (nbAxis >= na ? nbAxis - na : nbAxis);
+            T dvec[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const T cNb = d == a ? T(P.geo.cc[a][nbA]) : rc[d];
+                const T cOwn = g.own ? rc[d] : cNb;
+                const T cNei = g.own ? cNb : rc[d];
+                const T shift = d == a ? (g.own ? nbSh[s] : -nbSh[s]) : T(0);
+                dvec[d] = (cNei + shift) - cOwn;
+            }
+            const T m = mag3<T>(dvec[0], dvec[1], dvec[2]);
+            const T m2 = m * m;
+            const long long iOwn = g.own ? i : j, iNei = g.own ? j : i;
+#pragma unroll
+            for (int jj = 0; jj < NSC; ++jj) {
+                const int q = jj < NS ? jj : NS + 3;
+                const T qv = (primAt<T, NS>(Pc, n, q, iNei) - primAt<T, NS>(Pc, n, q, iOwn)) / m2;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) sgS[s][jj][d] = qv * dvec[d];
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const T qv = (primAt<T, NS>(Pc, n, NS + c, iNei) - primAt<T, NS>(Pc, n, NS + c, iOwn)) / m2;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) sgV[s][3 * c + d] = qv * dvec[d];
+            }
+        }
+    }
+    if (bad) raise(ck, FV_ERR_BOUNDARY);
+
+#pragma unroll
+    for (int s = 0; s < NFC; ++s) {
+        // farthest other face of the cell (first of equals)
+        int far = 0;
+        T best = T(0);
+#pragma unroll
+        for (int s2 = 0; s2 < NFC; ++s2) {
+            if (s2 == s) continue;
+            const T dist = mag3<T>(fc[s2][0] - fc[s][0], fc[s2][1] - fc[s][1], fc[s2][2] - fc[s][2]);
+            if (best < dist) {
+                best = dist;
+                far = s2;
+            }
+        }
+        const FaceGeo& g = fg[s];
+        const int a = fa[s];
+        T delta[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const T self = (!g.own && !g.boundary && d == a) ? rc[d] - nbSh[s] : rc[d];
+            delta[d] = T(g.rc[d]) - self;
+        }
+        FaceState<T, NS> st;
+#pragma unroll
+        for (int k = 1; k <= NS; ++k) {
+            T lg[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) lg[d] = thirdOrderComponent<T>(lim, sgS[s][k - 1][d], sgS[far][k - 1][d]);
+            T dot = T(0);
+            dot += lg[0] * delta[0];
+            dot += lg[1] * delta[1];
+            dot += lg[2] * delta[2];
+            st.c[k] = dot + prim_i[k - 1];
+        }
+        T lv[9];
+#pragma unroll
+        for (int m = 0; m < 9; ++m) lv[m] = thirdOrderComponent<T>(lim, sgV[s][m], sgV[far][m]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            st.v[c] = prim_i[NS + c] + (lv[3 * c] * delta[0] + lv[3 * c + 1] * delta[1] + lv[3 * c + 2] * delta[2]);
+        {
+            T lp[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) lp[d] = thirdOrderComponent<T>(lim, sgS[s][NS][d], sgS[far][NS][d]);
+            T dot = T(0);
+            dot += lp[0] * delta[0];
+            dot += lp[1] * delta[1];
+            dot += lp[2] * delta[2];
+            st.p = dot + prim_i[NS + 3];
+        }
+        closeFromPrimitive<T, NS, EOS>(P.mix, st);
+        soundSpeed<T, NS, EOS>(P.mix, st);
+        storeFace<T, NS>(FS, L.nfaces, g.own ? 0 : 1, g.f, st);
+    }
+}
+
 // ---------------------------------------------------------------------------- k_fluxes
 template <typename T, int NS, int EOS, int D>
 __global__ void k_fluxes(const StepParams P, const GenericLayout L, const T* __restrict__ FS, DevClock* __restrict__ ck,

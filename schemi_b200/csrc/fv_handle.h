@@ -24,7 +24,8 @@ struct fv_handle {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double* U[2] = {nullptr, nullptr};
     double* Ustage = nullptr;      // SecondOrderRK: state after the second stage
-    double* conc = nullptr;        // SecondOrderRK: averaged concentrations c_0..c_N
+    double* conc = nullptr;        // SecondOrderRK / ThirdOrder: averaged concentrations c_0..c_N
+    double* concStage = nullptr;   // ThirdOrder: concentrations of the 0.25 average
     int cur = 0;
     double* prim0 = nullptr;
     DevClock* ck = nullptr;        // device clock

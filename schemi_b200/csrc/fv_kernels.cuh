@@ -47,7 +47,8 @@ struct StepParams {
     int nmom;               // momentum components carried (dims, or 3 when a transverse velocity is non-zero)
     int tma;                // 1: stage state rows into shared memory with bulk async copies (nx even)
     int warp2d;             // 1: FP32-flux 2D steps use the warp-strip march (k_warp2d) when nmom == 2
-    int hancock;            // 1: MUSCL-Hancock (SecondOrder); 0: no predictor (SecondOrderRK stages)
+    int hancock;            // 1: MUSCL-Hancock (SecondOrder); 0: no predictor (SecondOrderRK / ThirdOrder stages)
+    int third;              // 1: ThirdOrder reconstruction (per-face limited surface gradients, k_faces3)
     const double* conc;     // stored concentrations c_0..c_N (stride apart), read instead of rho_k / M_k
                             // when not null and the restart set is not in use (SecondOrderRK)
     int limiter;

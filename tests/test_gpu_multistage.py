@@ -1,9 +1,12 @@
-"""SecondOrderRK on the GPU (two stages without the Hancock predictor, then the 0.5 average that
-keeps the averaged concentrations as state; secondOrderStepSolverRK.cpp, Advection2dOrder.cpp).
+"""Multi-stage step solvers on the GPU: SecondOrderRK (two stages without the Hancock predictor,
+then the 0.5 average that keeps the averaged concentrations as state; secondOrderStepSolverRK.cpp,
+Advection2dOrder.cpp) and ThirdOrder (SSP-RK3 of the directional reconstruction;
+thirdOrderStepSolver.cpp, Advection3dOrder.cpp, thirdOrderLimiter.hpp).
 
-The reference fixtures of this step solver (tests/golden/*_rk2*.npz) are checked step by step by
-test_gpu_parity.py; these tests cover the device time loop, the periodic mesh (which the reference
-cannot express) against the oracle, the FP32-flux arithmetic and the kernel count.
+The reference fixtures of these step solvers (tests/golden/*_rk2*.npz, *_rk3*.npz) are checked
+step by step by test_gpu_parity.py; these tests cover the device time loop, periodic meshes
+(which the reference cannot express) against the oracle, the FP32-flux arithmetic and the
+kernel counts.
 """
 
 import numpy as np
@@ -30,6 +33,11 @@ def fv():
 
 def _rk2(case):
     case.order = "SecondOrderRK"
+    return case
+
+
+def _rk3(case):
+    case.order = "ThirdOrder"
     return case
 
 
@@ -100,3 +108,55 @@ def test_rk2_rejected_where_unsupported(fv):
     g.upload(prim)
     with pytest.raises(fv.FVError):
         fv.FVBatch([g])
+
+
+@pytest.mark.parametrize("limiter", ["vanLeer", "minmod2"])
+def test_rk3_periodic_run_matches_oracle(fv, oracle_mod, limiter):
+    """Periodic KH (wrap faces in the directional limiter) through fv_run: FP64 within 1e-12."""
+    from schemi_b200 import cases
+
+    case, prim = cases.kelvin_helmholtz_2d(n=32, limiter=limiter)
+    _rk3(case)
+    case.t_end = 0.04
+    g = fv.FVCase(case)
+    g.upload(prim)
+    st = g.run(case.t_end)
+    oc = oracle_mod.OracleCase(case)
+    oc.upload(prim)
+    _, steps = oc.run(case.t_end)
+    assert st.steps == steps
+    assert g.time()[0] == oc.time()[0]
+    assert g.path == fv.PATH_GENERIC
+    a, b = g.download(), oc.download()
+    for f in FIELDS:
+        linf, _ = rel_err(a[f], b[f])
+        assert linf <= 1e-12, f"{f}: {linf:.3e}"
+
+
+def test_rk3_f32flux_within_tolerance(fv, oracle_mod):
+    from schemi_b200 import cases
+
+    case, prim = cases.kelvin_helmholtz_2d(n=48, precision="f32flux")
+    _rk3(case)
+    g = fv.FVCase(case)
+    g.upload(prim)
+    ref_case, _ = cases.kelvin_helmholtz_2d(n=48)
+    _rk3(ref_case)
+    oc = oracle_mod.OracleCase(ref_case)
+    oc.upload(prim)
+    for _ in range(10):
+        g.step()
+        oc.step()
+    a, b = g.download(), oc.download()
+    for f in ["c1", "c2", "vx", "p", "rho", "E"]:
+        _, l1 = rel_err(a[f], b[f])
+        assert l1 <= 1e-5, f"{f}: {l1:.3e}"
+
+
+def test_rk3_kernels_per_step(fv):
+    from schemi_b200 import cases
+
+    case, prim = cases.kelvin_helmholtz_2d(n=32)
+    g = fv.FVCase(_rk3(case))
+    assert g.path == fv.PATH_GENERIC
+    assert g.kernels_per_step() == 15  # three generic stages of four kernels, two averages, finalize
