@@ -90,10 +90,10 @@ def test_rk2_kernels_per_step(fv):
 
     case, prim = cases.kelvin_helmholtz_2d(n=32)
     g = fv.FVCase(_rk2(case))
-    assert g.kernels_per_step() == 4  # two march stages, the average, the CFL finalize
+    assert g.kernels_per_step == 4  # two march stages, the average, the CFL finalize
     case, prim = cases.shock_tube_1d(n=50)
     g = fv.FVCase(_rk2(case))
-    assert g.kernels_per_step() == 10  # two generic stages of four kernels, average, finalize
+    assert g.kernels_per_step == 10  # two generic stages of four kernels, average, finalize
 
 
 def test_rk2_rejected_where_unsupported(fv):
@@ -159,4 +159,4 @@ def test_rk3_kernels_per_step(fv):
     case, prim = cases.kelvin_helmholtz_2d(n=32)
     g = fv.FVCase(_rk3(case))
     assert g.path == fv.PATH_GENERIC
-    assert g.kernels_per_step() == 15  # three generic stages of four kernels, two averages, finalize
+    assert g.kernels_per_step == 15  # three generic stages of four kernels, two averages, finalize
