@@ -15,8 +15,8 @@
 // timeOfCalculation.tsv, with the reference's 20 significant digits.
 //
 // Not supported (the run stops with a message): zones other than the outer zone, diffusion,
-// turbulence, approximation orders other than SecondOrder and SecondOrderRK, the 1D mixing-zone
-// width output, and chemical mechanisms other than "no" and "Cl2".
+// turbulence, the ThirdOrderCada approximation order, the 1D mixing-zone width output, and
+// chemical mechanisms other than "no" and "Cl2".
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -186,7 +186,8 @@ Deck readDeck(const std::string& dir) {
     if (reconstruction != "linear" && reconstruction != "star") throw Fail("Unknown reconstruction flag.");
     if (order == "SecondOrder") c.order = FV_ORDER_SECOND;
     else if (order == "SecondOrderRK") c.order = FV_ORDER_SECOND_RK;
-    else throw Fail("#Approximation_order " + order + ": SecondOrder and SecondOrderRK are implemented");
+    else if (order == "ThirdOrder") c.order = FV_ORDER_THIRD;
+    else throw Fail("#Approximation_order " + order + ": SecondOrder, SecondOrderRK and ThirdOrder are implemented");
     if (onOff(width, "mixed zone width calculation") && dims == "1D") throw Fail("#Calculation_of_mixing_zone_width on is not implemented");
     c.dims = dims == "1D" ? 1 : dims == "2D" ? 2 : dims == "3D" ? 3 : 0;
     if (!c.dims) throw Fail("unknown #Dimensions_of_the_task " + dims);

@@ -95,7 +95,7 @@ def _edit(path, key, value):
 @pytest.mark.parametrize("file,key,value,message", [
     ("main.txt", "#Diffusion_flag", "on", "Diffusion"),
     ("main.txt", "#Turbulence_flag", "yes", "Turbulence"),
-    ("main.txt", "#Approximation_order", "ThirdOrder", "SecondOrder"),
+    ("main.txt", "#Approximation_order", "ThirdOrderCada", "ThirdOrder are implemented"),
     ("main.txt", "#TVD_limiter_type", "vanLeer3", "limiter"),
     ("main.txt", "#Type_of_flow_solver", "KT", "HLLC"),
     ("main.txt", "#Source_timestep_correction", "Courant", "Wrong format of time-step parameters settings"),
