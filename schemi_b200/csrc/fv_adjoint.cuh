@@ -750,9 +750,16 @@ __global__ void __launch_bounds__(BX * BY, adjointMinBlocks<T, BX, BY>()) k_adjo
         if (hasNext) {
             loadW(cellAt(zn), Wn);
             loadPacked<NS, NMOM>(P, A.lamIn, cellAt(zn), ln);
-            ivn = invVol(zn);
+            if constexpr (sizeof(T) == 4) {
+                // FP32 face arithmetic: the volume scaling of the adjoint in FP32 as well
+                const T ivf = T(1) / (T(hx) * T(P.geo.h[MA][zn]) * T(D == 2 ? Lz : hy));
 #pragma unroll
-            for (int i = 0; i < NL; ++i) lvn[i] = T(ln[i] * ivn);
+                for (int i = 0; i < NL; ++i) lvn[i] = T(ln[i]) * ivf;
+            } else {
+                ivn = invVol(zn);
+#pragma unroll
+                for (int i = 0; i < NL; ++i) lvn[i] = T(ln[i] * ivn);
+            }
         }
         // publish this row
         if (has) {
@@ -874,15 +881,30 @@ __global__ void __launch_bounds__(BX * BY, adjointMinBlocks<T, BX, BY>()) k_adjo
                 out[NS] += r0bar;
             }
             if (A.objGain != 0.0 && A.n >= 1) {
-                const double c0 = double(Wc.c[0]);
-                double ch = 0;
+                if constexpr (sizeof(T) == 4) {
+                    // the objective's gradient term in the face arithmetic, added to the FP64 sum
+                    const T c0 = Wc.c[0];
+                    T ch = 0;
 #pragma unroll
-                for (int k = 0; k < NS; ++k) ch = k == A.heavy ? double(Wc.c[k + 1]) : ch;
-                const double Xh = ch / c0;
-                const double meas = D == 2 ? hx * P.geo.h[MA][z] : hx * hy * P.geo.h[MA][z];
-                const double dWdX = A.objGain * A.rec[A.n - 1].dt * A.objScale * meas * (1.0 - 2.0 * Xh);
+                    for (int k = 0; k < NS; ++k) ch = k == A.heavy ? Wc.c[k + 1] : ch;
+                    const T ic0 = T(1) / c0;
+                    const T Xh = ch * ic0;
+                    const T meas = D == 2 ? T(hx * P.geo.h[MA][z]) : T(hx * hy * P.geo.h[MA][z]);
+                    const T dWdX = T(A.objGain * A.rec[A.n - 1].dt * A.objScale) * meas * (T(1) - T(2) * Xh);
 #pragma unroll
-                for (int k = 0; k < NS; ++k) out[k] += dWdX * ((k == A.heavy ? 1.0 : 0.0) - Xh) / c0 * mp.invM[k];
+                    for (int k = 0; k < NS; ++k)
+                        out[k] += double(dWdX * ((k == A.heavy ? T(1) : T(0)) - Xh) * ic0 * T(mp.invM[k]));
+                } else {
+                    const double c0 = double(Wc.c[0]);
+                    double ch = 0;
+#pragma unroll
+                    for (int k = 0; k < NS; ++k) ch = k == A.heavy ? double(Wc.c[k + 1]) : ch;
+                    const double Xh = ch / c0;
+                    const double meas = D == 2 ? hx * P.geo.h[MA][z] : hx * hy * P.geo.h[MA][z];
+                    const double dWdX = A.objGain * A.rec[A.n - 1].dt * A.objScale * meas * (1.0 - 2.0 * Xh);
+#pragma unroll
+                    for (int k = 0; k < NS; ++k) out[k] += dWdX * ((k == A.heavy ? 1.0 : 0.0) - Xh) / c0 * mp.invM[k];
+                }
             }
             const long long ic = cellAt(z);
             const long long st = P.stride;
