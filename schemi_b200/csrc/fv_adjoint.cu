@@ -7,8 +7,9 @@
 // and added, weighted by the step's dt, into a device accumulator in a fixed order.  Every
 // `checkpoint_every` steps the state is copied into a checkpoint.  fv_adjoint walks the segments
 // between checkpoints from the last one back: it recomputes the segment's states with the
-// recorded dt and gravity on a clock of its own (the same step kernels, so the states are the
-// recorded ones), then applies the adjoint step kernel from the segment's last step to its first.
+// recorded dt and gravity on clocks of its own, one per step (the same step kernels, so the
+// states are the recorded ones), then applies the adjoint step kernel from the segment's last
+// step to its first.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -37,6 +38,31 @@ __global__ void k_record_step(const DevClock* __restrict__ ck, StepRecord* rec) 
     r.ran = ck->done ? 0 : 1;
     r.pad = 0;
     *rec = r;
+}
+
+// Clocks of the steps rec[0 .. count-1] of a recomputed segment, one per step (the recorded dt
+// and gravity, no end time), so that the segment's step kernels run back to back with no clock
+// or CFL kernel between them; first sets whether the segment's first step reads its primitives
+// from the restart set.
+__global__ void k_schedule_segment(DevClock* clocks, const StepRecord* __restrict__ rec, int count, int first) {
+    for (int j = threadIdx.x; j < count; j += blockDim.x) {
+        DevClock c = {};
+        c.dt = rec[j].dt;
+        for (int d = 0; d < 3; ++d) c.g[d] = rec[j].g[d];
+        c.t_end = INFINITY;
+        c.first = j == 0 ? first : 0;
+        clocks[j] = c;
+    }
+}
+
+// Raises on ck the error a step of the segment raised (the first in step order).
+__global__ void k_segment_errors(const DevClock* __restrict__ clocks, int count, DevClock* ck) {
+    if (threadIdx.x != 0) return;
+    for (int j = 0; j < count; ++j)
+        if (clocks[j].err) {
+            atomicCAS(&ck->err, 0, clocks[j].err);
+            return;
+        }
 }
 
 // Clock of a replayed or recomputed step: the recorded dt and gravity, no end time; first >= 0
@@ -133,6 +159,8 @@ struct Trajectory {
     double* J = nullptr;
     double* partial = nullptr;
     DevClock* clock = nullptr;  // clock of recomputed steps
+    DevClock* segClocks = nullptr;  // one clock per step of a recomputed segment
+    long long segClockCap = 0;
     double* prim0 = nullptr;    // restart set of the recorded start state
     int first0 = 0;             // the recorded first step read the restart set
     std::vector<double*> segment;
@@ -151,6 +179,7 @@ void releaseTrajectory(fv_handle* h) {
     if (t->J) cudaFree(t->J);
     if (t->partial) cudaFree(t->partial);
     if (t->clock) cudaFree(t->clock);
+    if (t->segClocks) cudaFree(t->segClocks);
     if (t->prim0) cudaFree(t->prim0);
     for (double* p : t->lam)
         if (p) cudaFree(p);
@@ -186,9 +215,10 @@ fv_status clockStatus(fv_handle* h, const DevClock& c) {
     return fail(h, c.err, "device error");
 }
 
-// One forward step U -> Un on clock ck (step kernel + CFL finalize); prim0 is the restart set a
-// first step reads.
-cudaError_t enqueueForward(fv_handle* h, const double* U, double* Un, DevClock* ck, const double* prim0) {
+// One forward step U -> Un on clock ck (step kernel, and the CFL finalize unless the clock is a
+// recomputed step's); prim0 is the restart set a first step reads.
+cudaError_t enqueueForward(fv_handle* h, const double* U, double* Un, DevClock* ck, const double* prim0,
+                           bool finalize = true) {
     StepBuffers B{};
     B.U = U;
     B.Un = Un;
@@ -199,7 +229,7 @@ cudaError_t enqueueForward(fv_handle* h, const double* U, double* Un, DevClock* 
     B.L = h->L;
     cudaError_t e = h->cfg.precision == FV_PREC_F64 ? launchStepF64(h->P, B, PATH_MARCH, h->shape, h->stream)
                                                      : launchStepF32(h->P, B, PATH_MARCH, h->shape, h->stream);
-    if (e != cudaSuccess) return e;
+    if (e != cudaSuccess || !finalize) return e;
     k_finalize<<<1, 1024, 0, h->stream>>>(h->P, ck, h->blockMax, (int)marchBlocks(h->P, h->shape));
     return cudaGetLastError();
 }
@@ -399,6 +429,13 @@ fv_status fv_adjoint(fv_handle* h, const double* dJ_dU_T, double dJ_dJ, double* 
     }
     for (double*& p : t->lam)
         if (!p) FV_ADJ_CUDA(h, cudaMalloc(&p, bytes));
+    if (t->segClockCap < segStates) {
+        if (t->segClocks) FV_ADJ_CUDA(h, cudaFree(t->segClocks));
+        t->segClocks = nullptr;
+        t->segClockCap = 0;
+        FV_ADJ_CUDA(h, cudaMalloc(&t->segClocks, sizeof(DevClock) * segStates));
+        t->segClockCap = segStates;
+    }
     fv_status st = ensureEvents(h, t, 2 * (size_t)K + 2);
     if (st != FV_OK) return st;
     FV_ADJ_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -413,7 +450,6 @@ fv_status fv_adjoint(fv_handle* h, const double* dJ_dU_T, double dJ_dJ, double* 
     }
     FV_ADJ_CUDA(h, cudaMemsetAsync(&t->clock->err, 0, sizeof(int), h->stream));
     long long recomputed = 0;
-    const int rows = 8;
     for (long long k = K - 1; k >= 0; --k) {
         const long long s0 = k * C;
         const long long len = std::min<long long>(C, N - s0);
@@ -421,9 +457,13 @@ fv_status fv_adjoint(fv_handle* h, const double* dJ_dU_T, double dJ_dJ, double* 
         const long long upto = (k == K - 1 && objective) ? len : len - 1;
         FV_ADJ_CUDA(h, cudaEventRecord(ev[1 + 2 * (K - 1 - k)], h->stream));
         FV_ADJ_CUDA(h, cudaMemcpyAsync(t->segment[0], t->checkpoints[k], bytes, cudaMemcpyDeviceToDevice, h->stream));
-        for (long long j = 0; j < upto; ++j) {
-            k_schedule_step<<<1, 1, 0, h->stream>>>(t->clock, t->rec + s0 + j, (s0 + j == 0) ? t->first0 : 0);
-            FV_ADJ_CUDA(h, enqueueForward(h, t->segment[j], t->segment[j + 1], t->clock, t->prim0));
+        if (upto > 0) {
+            k_schedule_segment<<<1, 64, 0, h->stream>>>(t->segClocks, t->rec + s0, (int)upto,
+                                                         s0 == 0 ? t->first0 : 0);
+            for (long long j = 0; j < upto; ++j)
+                FV_ADJ_CUDA(h, enqueueForward(h, t->segment[j], t->segment[j + 1], t->segClocks + j, t->prim0,
+                                              false));
+            k_segment_errors<<<1, 32, 0, h->stream>>>(t->segClocks, (int)upto, t->clock);
         }
         recomputed += upto;
         FV_ADJ_CUDA(h, cudaEventRecord(ev[2 + 2 * (K - 1 - k)], h->stream));
@@ -444,7 +484,7 @@ fv_status fv_adjoint(fv_handle* h, const double* dJ_dU_T, double dJ_dJ, double* 
             A.objGain = objective ? dJ_dJ : 0.0;
             A.objScale = t->scale;
             A.heavy = t->cfg.heavy_species;
-            A.rows = rows;
+            A.rows = 0;  // tile height chosen by the launcher (whole waves of resident CTAs)
             FV_ADJ_CUDA(h, h->cfg.precision == FV_PREC_F64
                                ? launchAdjointF64(h->cfg.n_species, h->cfg.dims, h->P, A, h->stream)
                                : launchAdjointF32(h->cfg.n_species, h->cfg.dims, h->P, A, h->stream));

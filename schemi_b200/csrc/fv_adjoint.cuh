@@ -572,7 +572,7 @@ struct AdjParams {
     double objGain;         // 0: no objective term
     double objScale;
     int heavy;
-    int rows;
+    int rows;               // rows per tile along the marching axis (<= 0: the launcher's choice)
 };
 
 // Storage field of packed index i.
@@ -593,9 +593,35 @@ __device__ __forceinline__ void loadPacked(const StepParams& P, const double* __
 // adjoint divided by the cell volume, and the face-state adjoints handed over by the low
 // neighbours (along x, and along y in 3D).  Layout [array][field][BY][BX].
 template <typename T, int NS, int D, int NMOM, int BX, int BY>
+constexpr size_t adjointExchangeBytes() {
+    return (sizeof(T) * size_t(BX) * BY *
+                (size_t(fsSize<NS, NMOM>()) + (NS + 2 + NMOM) + fsSize<NS, NMOM>() * (D == 3 ? 2 : 1)) +
+            15) / 16 * 16;
+}
+
+// 2D tiles fetch the next rows' conserved values and adjoint (2 NL doubles per column) into a
+// ring of kAdjRingSlots rows with cp.async, one row ahead of their use.  Layout
+// [slot][value][BX]; 3D tiles read them directly.
+constexpr int kAdjRingSlots = 2;
+template <int NS, int D, int NMOM, int BX, int BY>
+constexpr size_t adjointRingBytes() {
+    return D == 2 ? sizeof(double) * size_t(kAdjRingSlots) * 2 * (NS + 2 + NMOM) * BX * BY : 0;
+}
+
+template <typename T, int NS, int D, int NMOM, int BX, int BY>
 constexpr size_t adjointSmemBytes() {
-    return sizeof(T) * size_t(BX) * BY *
-           (size_t(fsSize<NS, NMOM>()) + (NS + 2 + NMOM) + fsSize<NS, NMOM>() * (D == 3 ? 2 : 1));
+    return adjointExchangeBytes<T, NS, D, NMOM, BX, BY>() + adjointRingBytes<NS, D, NMOM, BX, BY>();
+}
+
+__device__ __forceinline__ void ringCopy8(void* smem, const void* gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void ringCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void ringWait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 // CTAs per SM the register budget of k_adjoint is sized for: 384 threads per SM (170 registers)
@@ -625,6 +651,8 @@ __global__ void __launch_bounds__(BX * BY, adjointMinBlocks<T, BX, BY>()) k_adjo
     T* sL = sF + NFS * SL;
     T* sBx = sL + NL * SL;
     T* sBy = sBx + NFS * SL;  // 3D only
+    constexpr bool RING = D == 2;
+    double* sRing = reinterpret_cast<double*>(adj_smem + adjointExchangeBytes<T, NS, D, NMOM, BX, BY>());
 
     const int tx = threadIdx.x, ty = D == 3 ? threadIdx.y : 0;
     const int slot = ty * BX + tx;
@@ -698,6 +726,17 @@ __global__ void __launch_bounds__(BX * BY, adjointMinBlocks<T, BX, BY>()) k_adjo
         for (int i = 0; i < NL; ++i) Fb[i] = T(dtS) * (lvR[i] - lvL[i]);
     };
     const T zeros[NL] = {};
+    // ring slot of loop row z (2D): the next rows' values, fetched a row ahead
+    auto ringSlot = [&](int z) { return sRing + (size_t)(z & (kAdjRingSlots - 1)) * 2 * NL * SL + slot; };
+    auto ringIssue = [&](int z, long long cell) {
+        double* dst = ringSlot(z);
+        const long long st = P.stride;
+#pragma unroll
+        for (int i = 0; i < NL; ++i) {
+            ringCopy8(dst + i * SL, A.U + storageField<NS, NMOM>(i) * st + cell);
+            ringCopy8(dst + (NL + i) * SL, A.lamIn + storageField<NS, NMOM>(i) * st + cell);
+        }
+    };
 
     WS Wc, Wn;
     WB Bc;
@@ -743,13 +782,39 @@ __global__ void __launch_bounds__(BX * BY, adjointMinBlocks<T, BX, BY>()) k_adjo
         }
     }
 
+    if constexpr (RING) {
+        if (z0 < z1) {
+            const int zq = wrapM(z0 + 1, ok);
+            if (has && ok) ringIssue(z0 + 1, cellAt(zq));
+        }
+        ringCommit();
+    }
+
     for (int z = z0; z < z1; ++z) {
         const int zn = wrapM(z + 1, ok);
         const bool hasNext = has && ok;
         areas(z);
+        if constexpr (RING) {
+            bool okq;
+            const int zq = wrapM(z + 2, okq);
+            if (has && okq && z + 1 < z1) ringIssue(z + 2, cellAt(zq));
+            ringCommit();
+            ringWait<1>();  // the values of row z + 1 have landed
+        }
         if (hasNext) {
-            loadW(cellAt(zn), Wn);
-            loadPacked<NS, NMOM>(P, A.lamIn, cellAt(zn), ln);
+            if constexpr (RING) {
+                const double* src = ringSlot(z + 1);
+                T ut[NL];
+#pragma unroll
+                for (int i = 0; i < NL; ++i) {
+                    ut[i] = T(src[i * SL]);
+                    ln[i] = src[(NL + i) * SL];
+                }
+                wForward<T, NS, NMOM>(mp, ut, Wn);
+            } else {
+                loadW(cellAt(zn), Wn);
+                loadPacked<NS, NMOM>(P, A.lamIn, cellAt(zn), ln);
+            }
             if constexpr (sizeof(T) == 4) {
                 // FP32 face arithmetic: the volume scaling of the adjoint in FP32 as well
                 const T ivf = T(1) / (T(hx) * T(P.geo.h[MA][zn]) * T(D == 2 ? Lz : hy));
@@ -928,6 +993,7 @@ __global__ void __launch_bounds__(BX * BY, adjointMinBlocks<T, BX, BY>()) k_adjo
         zero<T, NS, NMOM>(Bn);
         __syncthreads();
     }
+    if constexpr (RING) ringWait<0>();  // no copy outlives the tile
 }
 
 }  // namespace adj
