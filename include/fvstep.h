@@ -106,9 +106,14 @@ enum fv_chemistry { FV_CHEM_NONE = 0, FV_CHEM_A_B_2C = 1, FV_CHEM_CL2 = 2 };
  *   THIRD            "ThirdOrder": SSP-RK3 of three advections reconstructed with per-face limited
  *                    surface gradients (Advection3dOrder.cpp, templates/thirdOrderLimiter.hpp),
  *                    averages 0.25 and 2/3 with the start state (thirdOrderStepSolver.cpp:48-82).
+ *   THIRD_CADA       "ThirdOrderCada": the ThirdOrder stages with the smoothness-switched limiter
+ *                    of templates/thirdOrderLimiterCada.hpp (per face and field: unlimited where
+ *                    the indicator eta of the face's and the farthest face's surface gradients is
+ *                    below 1 - 1e-6, limited above 1 + 1e-6, blended in between;
+ *                    thirdOrderStepSolverCada.cpp, Advection3dOrderCada.cpp).
  * The multi-stage solvers run on the generic path (SecondOrderRK also on the fused march) and are
  * not combined with chemistry, the batched ensemble, the adjoint or fv_step_noalloc. */
-enum fv_step_solver { FV_ORDER_SECOND = 0, FV_ORDER_SECOND_RK = 1, FV_ORDER_THIRD = 2 };
+enum fv_step_solver { FV_ORDER_SECOND = 0, FV_ORDER_SECOND_RK = 1, FV_ORDER_THIRD = 2, FV_ORDER_THIRD_CADA = 3 };
 
 /* Per-cell linear solver of the backward-Euler step (set/chemicalKinetics.txt #Iterative_solver:
  * "Gauss-Seidel", "Jacobi", "GaussElimination", "conjugateGradient", "JacobiConjugateGradient"). */

@@ -41,6 +41,7 @@ namespace {
 
 constexpr double kStab = 5 * std::numeric_limits<double>::epsilon(); // globalConstants.hpp:33
 constexpr double kTwoThirds = 2. / 3.;
+constexpr double kPi = 3.14159265358979323846;  // Pi_number (globalConstants.hpp:38-40): the double nearest pi
 constexpr double kVeryBig = 1E-3 * std::numeric_limits<double>::max(); // globalConstants.hpp:35
 
 struct V3 {
@@ -743,6 +744,38 @@ inline double thirdOrderComponent(int lim, double g1, double g2) {
     return 0.5 * ((1 - 1. / 3.) * limOpp + (1 + 1. / 3.) * limGrad);
 }
 
+// thirdOrderLimiterCada (templates/thirdOrderLimiterCada.hpp:19-133) for one face s1 of cell i
+// and its farthest face: with dx2 = (1 / minimalLengthScale_i)^2 (minimalLengthScale = 1 / min
+// edge, Schemi.cpp:648-662), delta2 = dx2 (g & g) for the face's gradient gN and the farthest
+// face's gO (dot product of the NC components in storage order), eta = (delta2N + delta2O) /
+// (sqrt(5/2) (8 pi)^2 dx2).  eta < 1 - 1e-6: the unlimited 0.5 ((1 - 1/3) gO + (1 + 1/3) gN);
+// eta > 1 + 1e-6: thirdOrderComponent; otherwise 0.5 ((1 - e) unlimited + (1 + e) limited) with
+// e = (eta - 1) / 1e-6.
+template <int NC>
+void cadaLimit(int lim, const double* gN, const double* gO, double minLS, double* out) {
+    const double pi8 = 8 * kPi;
+    const double alpha = pi8 * pi8, eps = 1E-6;
+    const double inv = 1 / minLS;
+    const double dx2 = inv * inv;
+    double sN = 0, sO = 0;
+    for (int q = 0; q < NC; ++q) sN += gN[q] * gN[q];
+    for (int q = 0; q < NC; ++q) sO += gO[q] * gO[q];
+    const double delta2Near = dx2 * sN, delta2Oppose = dx2 * sO;
+    const double eta = (delta2Near + delta2Oppose) / (std::sqrt(5.0 / 2.0) * alpha * dx2);
+    for (int q = 0; q < NC; ++q) {
+        const double unlimited = 0.5 * ((1 - 1. / 3.) * gO[q] + (1 + 1. / 3.) * gN[q]);
+        if (eta < (1 - eps)) {
+            out[q] = unlimited;
+        } else if (eta > (1 + eps)) {
+            out[q] = thirdOrderComponent(lim, gN[q], gO[q]);
+        } else {
+            const double limited = thirdOrderComponent(lim, gN[q], gO[q]);
+            const double eta1eps = (eta - 1) / eps;
+            out[q] = 0.5 * ((1 - eta1eps) * unlimited + (1 + eta1eps) * limited);
+        }
+    }
+}
+
 // TVDLimiter for a scalar field (TVDLimiter.cpp:12-125)
 void tvdScalar(const fvo_case& cs, const std::vector<V3>& grad, const std::vector<double>& phi, int field, int k,
                std::vector<V3>& out, bool& bad) {
@@ -972,8 +1005,8 @@ void cellPrimitivesFromConserved(fvo_case& cs, long long i) {
 // TVD reconstruction without the predictor (Advection2dOrder.cpp:20-636, hancock = false), whose
 // boundary neighbour is the ghost of the reconstructed owner face (Advection2dOrder.cpp:394-522);
 // third = true reconstructs with the per-face limited surface gradients of Advection3dOrder.cpp
-// (no predictor either).
-int doStep(fvo_case& cs, double dt, bool hancock = true, bool third = false) {
+// (no predictor either), cada = true with those of Advection3dOrderCada.cpp.
+int doStep(fvo_case& cs, double dt, bool hancock = true, bool third = false, bool cada = false) {
     const Mix& mx = cs.mix;
     const int NS = mx.N;
     const long long nc = cs.nCells;
@@ -1019,14 +1052,20 @@ int doStep(fvo_case& cs, double dt, bool hancock = true, bool third = false) {
                 const int f2 = c.faces[far];
                 for (int k = 1; k <= NS; ++k) {
                     V3 lg;
-                    for (int q = 0; q < 3; ++q) lg.x[q] = thirdOrderComponent(lim, sgC[k][fi].x[q], sgC[k][f2].x[q]);
+                    if (cada) cadaLimit<3>(lim, sgC[k][fi].x, sgC[k][f2].x, c.minLS, lg.x);
+                    else
+                        for (int q = 0; q < 3; ++q) lg.x[q] = thirdOrderComponent(lim, sgC[k][fi].x[q], sgC[k][f2].x[q]);
                     s.c[k] = vdot(lg, delta) + cs.c[k][i];
                 }
                 T9 lv;
-                for (int q = 0; q < 9; ++q) lv.x[q] = thirdOrderComponent(lim, sgV[fi].x[q], sgV[f2].x[q]);
+                if (cada) cadaLimit<9>(lim, sgV[fi].x, sgV[f2].x, c.minLS, lv.x);
+                else
+                    for (int q = 0; q < 9; ++q) lv.x[q] = thirdOrderComponent(lim, sgV[fi].x[q], sgV[f2].x[q]);
                 s.v = vadd(tdot(lv, delta), cs.v[i]);
                 V3 lp;
-                for (int q = 0; q < 3; ++q) lp.x[q] = thirdOrderComponent(lim, sgP[fi].x[q], sgP[f2].x[q]);
+                if (cada) cadaLimit<3>(lim, sgP[fi].x, sgP[f2].x, c.minLS, lp.x);
+                else
+                    for (int q = 0; q < 3; ++q) lp.x[q] = thirdOrderComponent(lim, sgP[fi].x[q], sgP[f2].x[q]);
                 s.p = vdot(lp, delta) + cs.p[i];
             } else {
                 for (int k = 1; k <= NS; ++k) s.c[k] = vdot(limC[k][i], delta) + cs.c[k][i];
@@ -1203,15 +1242,16 @@ int rk2Step(fvo_case& cs, double dt) {
 }
 
 // thirdOrderStepSolver::calculateStep (thirdOrderStepSolver.cpp:48-82): SSP-RK3 of
-// Advection3dOrder -- U1 = L(Un), U2 = 0.25 L(U1) + 0.75 Un, U3 = 2/3 L(U2) + 1/3 Un.
-int rk3Step(fvo_case& cs, double dt) {
+// Advection3dOrder -- U1 = L(Un), U2 = 0.25 L(U1) + 0.75 Un, U3 = 2/3 L(U2) + 1/3 Un; with
+// cada, of Advection3dOrderCada (thirdOrderStepSolverCada.cpp:48-84, the same stages).
+int rk3Step(fvo_case& cs, double dt, bool cada) {
     const StartState u = saveState(cs);
-    int st = doStep(cs, dt, false, true);
+    int st = doStep(cs, dt, false, true, cada);
     if (st != FV_OK) return st;
-    st = doStep(cs, dt, false, true);
+    st = doStep(cs, dt, false, true, cada);
     if (st != FV_OK) return st;
     averageWith(cs, u, 0.25);
-    st = doStep(cs, dt, false, true);
+    st = doStep(cs, dt, false, true, cada);
     if (st != FV_OK) return st;
     averageWith(cs, u, kTwoThirds);
     return FV_OK;
@@ -1593,7 +1633,7 @@ bool validate(const fv_config& cf, std::string& err) {
     if (cf.chemistry == FV_CHEM_CL2 && cf.n_species != 2) { err = "Cl2 dissociation needs 2 species"; return false; }
     if (cf.chemistry == FV_CHEM_A_B_2C && cf.n_species != 3) { err = "A+B->2C needs 3 species"; return false; }
     if (cf.chemistry < FV_CHEM_NONE || cf.chemistry > FV_CHEM_CL2) { err = "unknown chemistry"; return false; }
-    if (cf.order != FV_ORDER_SECOND && cf.order != FV_ORDER_SECOND_RK && cf.order != FV_ORDER_THIRD) {
+    if (cf.order < FV_ORDER_SECOND || cf.order > FV_ORDER_THIRD_CADA) {
         err = "unknown step solver";
         return false;
     }
@@ -1694,9 +1734,10 @@ int fvo_upload(fvo_case* cs, const double* const* prim) {
 
 int fvo_step(fvo_case* cs, double* dt_used, double* dt_next) {
     const double dt = cs->dt;
-    int st = cs->cfg.order == FV_ORDER_SECOND_RK ? rk2Step(*cs, dt)
-             : cs->cfg.order == FV_ORDER_THIRD   ? rk3Step(*cs, dt)
-                                                 : doStep(*cs, dt);
+    const int order = cs->cfg.order;
+    int st = order == FV_ORDER_SECOND_RK                                     ? rk2Step(*cs, dt)
+             : (order == FV_ORDER_THIRD || order == FV_ORDER_THIRD_CADA) ? rk3Step(*cs, dt, order == FV_ORDER_THIRD_CADA)
+                                                                         : doStep(*cs, dt);
     if (st != FV_OK) return st;
     if (cs->cfg.chemistry != FV_CHEM_NONE) {
         // secondOrderStepSolver::calculateStep: chemistry after the advection, same dt

@@ -36,7 +36,7 @@ CHEMISTRY = {"no": 0, "A+B->2C": 1, "Cl2": 2}
 CHEM_SOLVERS = {"Gauss-Seidel": 0, "Jacobi": 1, "GaussElimination": 2, "conjugateGradient": 3,
                 "JacobiConjugateGradient": 4}
 # #Approximation_order values with a GPU step (abstractStepSolver.cpp:56-146)
-ORDERS = {"SecondOrder": 0, "SecondOrderRK": 1, "ThirdOrder": 2}
+ORDERS = {"SecondOrder": 0, "SecondOrderRK": 1, "ThirdOrder": 2, "ThirdOrderCada": 3}
 
 # patch order of the task files: #Tail, #Point, #Bottom, #Right, #Left, #Top
 PATCHES = ["tail", "point", "bottom", "right", "left", "top"]
@@ -154,7 +154,7 @@ class Case:
     chem_solver: str = "Gauss-Seidel"
     chem_max_iter: int = 200
     const_timestep: float = 0.0   # > 0: every step takes this dt (#Constant_timestep)
-    order: str = "SecondOrder"    # #Approximation_order: "SecondOrder", "SecondOrderRK", "ThirdOrder"
+    order: str = "SecondOrder"    # #Approximation_order: a key of ORDERS
     name: str = "case"
 
     def __post_init__(self):

@@ -599,18 +599,21 @@ constexpr size_t adjointExchangeBytes() {
             15) / 16 * 16;
 }
 
-// 2D tiles fetch the next rows' conserved values and adjoint (2 NL doubles per column) into a
-// ring of kAdjRingSlots rows with cp.async, one row ahead of their use.  Layout
-// [slot][value][BX]; 3D tiles read them directly.
+// FP64 2D tiles fetch the next rows' conserved values and adjoint (2 NL doubles per column) into
+// a ring of kAdjRingSlots rows with cp.async, one row ahead of their use.  Layout
+// [slot][value][BX].  FP32 and 3D tiles read them directly (in FP32 the ring measured no
+// faster: the kernel's stalls there are arithmetic dependencies, not the row loads).
 constexpr int kAdjRingSlots = 2;
-template <int NS, int D, int NMOM, int BX, int BY>
+template <typename T, int D>
+constexpr bool adjointRing() { return D == 2 && sizeof(T) == 8; }
+template <typename T, int NS, int D, int NMOM, int BX, int BY>
 constexpr size_t adjointRingBytes() {
-    return D == 2 ? sizeof(double) * size_t(kAdjRingSlots) * 2 * (NS + 2 + NMOM) * BX * BY : 0;
+    return adjointRing<T, D>() ? sizeof(double) * size_t(kAdjRingSlots) * 2 * (NS + 2 + NMOM) * BX * BY : 0;
 }
 
 template <typename T, int NS, int D, int NMOM, int BX, int BY>
 constexpr size_t adjointSmemBytes() {
-    return adjointExchangeBytes<T, NS, D, NMOM, BX, BY>() + adjointRingBytes<NS, D, NMOM, BX, BY>();
+    return adjointExchangeBytes<T, NS, D, NMOM, BX, BY>() + adjointRingBytes<T, NS, D, NMOM, BX, BY>();
 }
 
 __device__ __forceinline__ void ringCopy8(void* smem, const void* gmem) {
@@ -651,7 +654,7 @@ __global__ void __launch_bounds__(BX * BY, adjointMinBlocks<T, BX, BY>()) k_adjo
     T* sL = sF + NFS * SL;
     T* sBx = sL + NL * SL;
     T* sBy = sBx + NFS * SL;  // 3D only
-    constexpr bool RING = D == 2;
+    constexpr bool RING = adjointRing<T, D>();
     double* sRing = reinterpret_cast<double*>(adj_smem + adjointExchangeBytes<T, NS, D, NMOM, BX, BY>());
 
     const int tx = threadIdx.x, ty = D == 3 ? threadIdx.y : 0;
@@ -684,17 +687,16 @@ __global__ void __launch_bounds__(BX * BY, adjointMinBlocks<T, BX, BY>()) k_adjo
 
     const StepRecord rec = A.rec[A.n];
     const double dt = rec.dt;
+    const bool objTerm = A.objGain != 0.0 && A.n >= 1;
+    const double objW = objTerm ? A.objGain * A.rec[A.n - 1].dt * A.objScale : 0.0;
     const double hx = has ? P.geo.h[0][cx] : 1.0;
     const double hy = D == 3 ? (has ? P.geo.h[1][cy] : 1.0) : 0.0;
     const double Lz = P.ext[2];
-    // face areas of this column's cell and the inverse cell volume of row zm (mesh.cpp)
+    // face areas of this column's cell and the inverse cell volume of a row of height hm
+    // (mesh.cpp)
     double Sx = 0, Sy = 0, Sm = 0;
-    auto invVol = [&](int zm) -> double {
-        const double hm = P.geo.h[MA][zm];
-        return D == 2 ? 1.0 / (hx * hm * Lz) : 1.0 / (hx * hy * hm);
-    };
-    auto areas = [&](int zm) {
-        const double hm = P.geo.h[MA][zm];
+    auto invVol = [&](double hm) -> double { return D == 2 ? 1.0 / (hx * hm * Lz) : 1.0 / (hx * hy * hm); };
+    auto areas = [&](double hm) {
         if (D == 2) {
             Sx = Lz * hm;
             Sm = hx * Lz;
@@ -744,6 +746,7 @@ __global__ void __launch_bounds__(BX * BY, adjointMinBlocks<T, BX, BY>()) k_adjo
     double lc[NL], ln[NL];
     T lvc[NL], lvn[NL];
     double ivc = 1, ivn = 1;
+    double hmC = P.geo.h[MA][z0 < z1 ? z0 : 0], hmN = hmC;  // heights of rows z and z + 1
     zero<T, NS, NMOM>(Bc);
     zero<T, NS, NMOM>(Bn);
     bool ok;
@@ -752,10 +755,10 @@ __global__ void __launch_bounds__(BX * BY, adjointMinBlocks<T, BX, BY>()) k_adjo
     if (has && z0 < z1) {
         loadW(cellAt(z0), Wc);
         loadPacked<NS, NMOM>(P, A.lamIn, cellAt(z0), lc);
-        ivc = invVol(z0);
+        ivc = invVol(hmC);
 #pragma unroll
         for (int i = 0; i < NL; ++i) lvc[i] = T(lc[i] * ivc);
-        areas(z0);
+        areas(hmC);
         if (interior) {
             const int zb = wrapM(z0 - 1, ok);
             T Fb[NL];
@@ -764,7 +767,7 @@ __global__ void __launch_bounds__(BX * BY, adjointMinBlocks<T, BX, BY>()) k_adjo
             if (ok) {
                 double lb[NL];
                 loadPacked<NS, NMOM>(P, A.lamIn, cellAt(zb), lb);
-                const double ivb = invVol(zb);
+                const double ivb = invVol(P.geo.h[MA][zb]);
                 T lvb[NL];
 #pragma unroll
                 for (int i = 0; i < NL; ++i) lvb[i] = T(lb[i] * ivb);
@@ -793,7 +796,8 @@ __global__ void __launch_bounds__(BX * BY, adjointMinBlocks<T, BX, BY>()) k_adjo
     for (int z = z0; z < z1; ++z) {
         const int zn = wrapM(z + 1, ok);
         const bool hasNext = has && ok;
-        areas(z);
+        if (ok) hmN = P.geo.h[MA][zn];
+        areas(hmC);
         if constexpr (RING) {
             bool okq;
             const int zq = wrapM(z + 2, okq);
@@ -817,11 +821,11 @@ __global__ void __launch_bounds__(BX * BY, adjointMinBlocks<T, BX, BY>()) k_adjo
             }
             if constexpr (sizeof(T) == 4) {
                 // FP32 face arithmetic: the volume scaling of the adjoint in FP32 as well
-                const T ivf = T(1) / (T(hx) * T(P.geo.h[MA][zn]) * T(D == 2 ? Lz : hy));
+                const T ivf = T(1) / (T(hx) * T(hmN) * T(D == 2 ? Lz : hy));
 #pragma unroll
                 for (int i = 0; i < NL; ++i) lvn[i] = T(ln[i]) * ivf;
             } else {
-                ivn = invVol(zn);
+                ivn = invVol(hmN);
 #pragma unroll
                 for (int i = 0; i < NL; ++i) lvn[i] = T(ln[i] * ivn);
             }
@@ -945,7 +949,7 @@ __global__ void __launch_bounds__(BX * BY, adjointMinBlocks<T, BX, BY>()) k_adjo
                 }
                 out[NS] += r0bar;
             }
-            if (A.objGain != 0.0 && A.n >= 1) {
+            if (objTerm) {
                 if constexpr (sizeof(T) == 4) {
                     // the objective's gradient term in the face arithmetic, added to the FP64 sum
                     const T c0 = Wc.c[0];
@@ -954,8 +958,8 @@ __global__ void __launch_bounds__(BX * BY, adjointMinBlocks<T, BX, BY>()) k_adjo
                     for (int k = 0; k < NS; ++k) ch = k == A.heavy ? Wc.c[k + 1] : ch;
                     const T ic0 = T(1) / c0;
                     const T Xh = ch * ic0;
-                    const T meas = D == 2 ? T(hx * P.geo.h[MA][z]) : T(hx * hy * P.geo.h[MA][z]);
-                    const T dWdX = T(A.objGain * A.rec[A.n - 1].dt * A.objScale) * meas * (T(1) - T(2) * Xh);
+                    const T meas = D == 2 ? T(hx * hmC) : T(hx * hy * hmC);
+                    const T dWdX = T(objW) * meas * (T(1) - T(2) * Xh);
 #pragma unroll
                     for (int k = 0; k < NS; ++k)
                         out[k] += double(dWdX * ((k == A.heavy ? T(1) : T(0)) - Xh) * ic0 * T(mp.invM[k]));
@@ -965,8 +969,8 @@ __global__ void __launch_bounds__(BX * BY, adjointMinBlocks<T, BX, BY>()) k_adjo
 #pragma unroll
                     for (int k = 0; k < NS; ++k) ch = k == A.heavy ? double(Wc.c[k + 1]) : ch;
                     const double Xh = ch / c0;
-                    const double meas = D == 2 ? hx * P.geo.h[MA][z] : hx * hy * P.geo.h[MA][z];
-                    const double dWdX = A.objGain * A.rec[A.n - 1].dt * A.objScale * meas * (1.0 - 2.0 * Xh);
+                    const double meas = D == 2 ? hx * hmC : hx * hy * hmC;
+                    const double dWdX = objW * meas * (1.0 - 2.0 * Xh);
 #pragma unroll
                     for (int k = 0; k < NS; ++k) out[k] += dWdX * ((k == A.heavy ? 1.0 : 0.0) - Xh) / c0 * mp.invM[k];
                 }
@@ -986,6 +990,7 @@ __global__ void __launch_bounds__(BX * BY, adjointMinBlocks<T, BX, BY>()) k_adjo
             }
             ivc = ivn;
         }
+        hmC = hmN;
         Bc.f = Bn;
 #pragma unroll
         for (int k = 0; k <= NS; ++k) Bc.c[k] = 0;

@@ -266,7 +266,7 @@ bool validate(const fv_config& c, std::string& e) {
     if (c.chemistry < FV_CHEM_NONE || c.chemistry > FV_CHEM_CL2) { e = "unknown chemistry"; return false; }
     if (c.chemistry == FV_CHEM_A_B_2C && c.n_species != 3) { e = "A+B->2C needs 3 species (A, B, C)"; return false; }
     if (c.chemistry == FV_CHEM_CL2 && c.n_species != 2) { e = "Cl2 dissociation needs 2 species (Cl2, Cl)"; return false; }
-    if (c.order != FV_ORDER_SECOND && c.order != FV_ORDER_SECOND_RK && c.order != FV_ORDER_THIRD) {
+    if (c.order < FV_ORDER_SECOND || c.order > FV_ORDER_THIRD_CADA) {
         e = "unknown step solver (order)";
         return false;
     }
@@ -490,7 +490,7 @@ cudaError_t enqueueRk3(fv_handle* h, int from) {
 
 cudaError_t enqueueStep(fv_handle* h, int from) {
     if (h->cfg.order == FV_ORDER_SECOND_RK) return enqueueRk2(h, from);
-    if (h->cfg.order == FV_ORDER_THIRD) return enqueueRk3(h, from);
+    if (h->cfg.order == FV_ORDER_THIRD || h->cfg.order == FV_ORDER_THIRD_CADA) return enqueueRk3(h, from);
     const StepBuffers B = buffersFor(h, from);
     cudaError_t e = h->cfg.precision == FV_PREC_F64 ? launchStepF64(h->P, B, h->path, h->shape, h->stream)
                                                      : launchStepF32(h->P, B, h->path, h->shape, h->stream);
@@ -542,7 +542,7 @@ fv_status ensureScratch(fv_handle* h) {
 
 int choosePath(const fv_config& c) {
     if (c.dims < 2) return PATH_GENERIC;
-    if (c.order == FV_ORDER_THIRD) return PATH_GENERIC;  // directional slopes: k_faces3
+    if (c.order == FV_ORDER_THIRD || c.order == FV_ORDER_THIRD_CADA) return PATH_GENERIC;  // directional slopes: k_faces3
     for (int a = 0; a < c.dims; ++a)
         if (c.n[a] < 2) return PATH_GENERIC;
     return limiterZeroForNonPositiveR(c.limiter) ? PATH_MARCH : PATH_GENERIC;
@@ -655,7 +655,8 @@ fv_status fv_create(const fv_config* cfg, fv_handle** out) {
                 P.ncell * (cfg->n_species + 5) < (1LL << 31)) ? 1 : 0;
     if (P.warp2d) P.tma = 1;
     P.hancock = cfg->order == FV_ORDER_SECOND ? 1 : 0;
-    P.third = cfg->order == FV_ORDER_THIRD ? 1 : 0;
+    P.third = (cfg->order == FV_ORDER_THIRD || cfg->order == FV_ORDER_THIRD_CADA) ? 1 : 0;
+    P.cada = cfg->order == FV_ORDER_THIRD_CADA ? 1 : 0;
     h->path = choosePath(*cfg);
     h->chem.mech = cfg->chemistry;
     h->chem.solver = cfg->chem_solver;
@@ -704,7 +705,8 @@ fv_status fv_create(const fv_config* cfg, fv_handle** out) {
         const size_t concBytes = sizeof(double) * (cfg->n_species + 1) * P.ncell;
         if ((ce = cudaMalloc(&h->Ustage, stateBytes)) != cudaSuccess) return bail(ce, "stage state");
         if ((ce = cudaMalloc(&h->conc, concBytes)) != cudaSuccess) return bail(ce, "concentrations");
-        if (cfg->order == FV_ORDER_THIRD && (ce = cudaMalloc(&h->concStage, concBytes)) != cudaSuccess)
+        if ((cfg->order == FV_ORDER_THIRD || cfg->order == FV_ORDER_THIRD_CADA) &&
+            (ce = cudaMalloc(&h->concStage, concBytes)) != cudaSuccess)
             return bail(ce, "stage concentrations");
         P.conc = h->conc;
     }
@@ -1018,7 +1020,8 @@ long long fv_kernels_per_step(const fv_handle* h) {
     if (!h) return 0;
     const int stage = h->path == PATH_MARCH ? 1 : 4;
     if (h->cfg.order == FV_ORDER_SECOND_RK) return 2 * stage + 2;  // two stages, average, finalize
-    if (h->cfg.order == FV_ORDER_THIRD) return 3 * stage + 3;      // three stages, two averages, finalize
+    if (h->cfg.order == FV_ORDER_THIRD || h->cfg.order == FV_ORDER_THIRD_CADA)
+        return 3 * stage + 3;  // three stages, two averages, finalize
     return stage + 1 + (h->cfg.chemistry != FV_CHEM_NONE ? 1 : 0);
 }
 

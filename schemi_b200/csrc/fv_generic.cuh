@@ -608,6 +608,42 @@ template <typename T> __device__ __forceinline__ T thirdOrderComponent(int lim, 
     return T(0.5) * ((T(1) - T(1. / 3.)) * limOpp + (T(1) + T(1. / 3.)) * limGrad);
 }
 
+// thirdOrderLimiterCada (templates/thirdOrderLimiterCada.hpp:19-133) for one face and the
+// cell's farthest face, NC gradient components in storage order: dx2 = (1 / minLS)^2 with minLS
+// the cell's 1 / min edge (Schemi.cpp:648-662), eta = (dx2 (gN & gN) + dx2 (gO & gO)) /
+// (sqrt(5/2) (8 pi)^2 dx2); below 1 - 1e-6 the unlimited 0.5 ((1 - 1/3) gO + (1 + 1/3) gN),
+// above 1 + 1e-6 thirdOrderComponent, in between 0.5 ((1 - e) unlimited + (1 + e) limited) with
+// e = (eta - 1) / 1e-6.
+template <typename T, int NC>
+__device__ __forceinline__ void cadaLimit(int lim, const T* gN, const T* gO, T minLS, T* out) {
+    const T pi8 = T(8) * T(3.14159265358979323846);
+    const T alpha = pi8 * pi8, eps = T(1E-6);
+    const T inv = T(1) / minLS;
+    const T dx2 = inv * inv;
+    T sN = T(0), sO = T(0);
+#pragma unroll
+    for (int q = 0; q < NC; ++q) sN += gN[q] * gN[q];
+#pragma unroll
+    for (int q = 0; q < NC; ++q) sO += gO[q] * gO[q];
+    const T delta2Near = dx2 * sN, delta2Oppose = dx2 * sO;
+    const T eta = (delta2Near + delta2Oppose) / (sqrt(T(5.0 / 2.0)) * alpha * dx2);
+#pragma unroll
+    for (int q = 0; q < NC; ++q) {
+        const T unlimited = T(0.5) * ((T(1) - T(1. / 3.)) * gO[q] + (T(1) + T(1. / 3.)) * gN[q]);
+        if (eta < (T(1) - eps)) {
+            out[q] = unlimited;
+        } else {
+            const T limited = thirdOrderComponent<T>(lim, gN[q], gO[q]);
+            if (eta > (T(1) + eps)) {
+                out[q] = limited;
+            } else {
+                const T eta1eps = (eta - T(1)) / eps;
+                out[q] = T(0.5) * ((T(1) - eta1eps) * unlimited + (T(1) + eta1eps) * limited);
+            }
+        }
+    }
+}
+
 template <typename T, int NS, int EOS, int D>
 __global__ void k_faces3(const StepParams P, const GenericLayout L, const T* __restrict__ Pc, DevClock* __restrict__ ck,
                          T* __restrict__ FS) {
@@ -623,6 +659,9 @@ __global__ void k_faces3(const StepParams P, const GenericLayout L, const T* __r
     const T rc[3] = {T(P.geo.cc[0][ijk[0]]), T(P.geo.cc[1][ijk[1]]), T(P.geo.cc[2][ijk[2]])};
     bool bad = false;
     const int lim = P.limiter;
+    const bool cada = P.cada != 0;
+    // the cell's minimal length scale (1 / min edge) of the Cada switch
+    const T minLS = T(1) / smin(smin(T(extent(P, 0, ijk[0])), T(extent(P, 1, ijk[1]))), T(extent(P, 2, ijk[2])));
 
     // faces of the cell in mesh.cpp order: [x-, x+, y+, y-, z-, z+]
     constexpr int NFC = 2 * D;
@@ -751,8 +790,12 @@ __global__ void k_faces3(const StepParams P, const GenericLayout L, const T* __r
 #pragma unroll
         for (int k = 1; k <= NS; ++k) {
             T lg[3];
+            if (cada) {
+                cadaLimit<T, 3>(lim, sgS[s][k - 1], sgS[far][k - 1], minLS, lg);
+            } else {
 #pragma unroll
-            for (int d = 0; d < 3; ++d) lg[d] = thirdOrderComponent<T>(lim, sgS[s][k - 1][d], sgS[far][k - 1][d]);
+                for (int d = 0; d < 3; ++d) lg[d] = thirdOrderComponent<T>(lim, sgS[s][k - 1][d], sgS[far][k - 1][d]);
+            }
             T dot = T(0);
             dot += lg[0] * delta[0];
             dot += lg[1] * delta[1];
@@ -760,15 +803,23 @@ __global__ void k_faces3(const StepParams P, const GenericLayout L, const T* __r
             st.c[k] = dot + prim_i[k - 1];
         }
         T lv[9];
+        if (cada) {
+            cadaLimit<T, 9>(lim, sgV[s], sgV[far], minLS, lv);
+        } else {
 #pragma unroll
-        for (int m = 0; m < 9; ++m) lv[m] = thirdOrderComponent<T>(lim, sgV[s][m], sgV[far][m]);
+            for (int m = 0; m < 9; ++m) lv[m] = thirdOrderComponent<T>(lim, sgV[s][m], sgV[far][m]);
+        }
 #pragma unroll
         for (int c = 0; c < 3; ++c)
             st.v[c] = prim_i[NS + c] + (lv[3 * c] * delta[0] + lv[3 * c + 1] * delta[1] + lv[3 * c + 2] * delta[2]);
         {
             T lp[3];
+            if (cada) {
+                cadaLimit<T, 3>(lim, sgS[s][NS], sgS[far][NS], minLS, lp);
+            } else {
 #pragma unroll
-            for (int d = 0; d < 3; ++d) lp[d] = thirdOrderComponent<T>(lim, sgS[s][NS][d], sgS[far][NS][d]);
+                for (int d = 0; d < 3; ++d) lp[d] = thirdOrderComponent<T>(lim, sgS[s][NS][d], sgS[far][NS][d]);
+            }
             T dot = T(0);
             dot += lp[0] * delta[0];
             dot += lp[1] * delta[1];

@@ -49,6 +49,7 @@ struct StepParams {
     int warp2d;             // 1: FP32-flux 2D steps use the warp-strip march (k_warp2d) when nmom == 2
     int hancock;            // 1: MUSCL-Hancock (SecondOrder); 0: no predictor (SecondOrderRK / ThirdOrder stages)
     int third;              // 1: ThirdOrder reconstruction (per-face limited surface gradients, k_faces3)
+    int cada;               // 1: with third, the smoothness-switched limiter of ThirdOrderCada
     const double* conc;     // stored concentrations c_0..c_N (stride apart), read instead of rho_k / M_k
                             // when not null and the restart set is not in use (SecondOrderRK)
     int limiter;

@@ -15,8 +15,8 @@
 // timeOfCalculation.tsv, with the reference's 20 significant digits.
 //
 // Not supported (the run stops with a message): zones other than the outer zone, diffusion,
-// turbulence, the ThirdOrderCada approximation order, the 1D mixing-zone width output, and
-// chemical mechanisms other than "no" and "Cl2".
+// turbulence, the 1D mixing-zone width output, and chemical mechanisms other than "no" and
+// "Cl2".
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -187,7 +187,8 @@ Deck readDeck(const std::string& dir) {
     if (order == "SecondOrder") c.order = FV_ORDER_SECOND;
     else if (order == "SecondOrderRK") c.order = FV_ORDER_SECOND_RK;
     else if (order == "ThirdOrder") c.order = FV_ORDER_THIRD;
-    else throw Fail("#Approximation_order " + order + ": SecondOrder, SecondOrderRK and ThirdOrder are implemented");
+    else if (order == "ThirdOrderCada") c.order = FV_ORDER_THIRD_CADA;
+    else throw Fail("Unknown gas dynamics approximation order.");  // abstractStepSolver.cpp:87-94
     if (onOff(width, "mixed zone width calculation") && dims == "1D") throw Fail("#Calculation_of_mixing_zone_width on is not implemented");
     c.dims = dims == "1D" ? 1 : dims == "2D" ? 2 : dims == "3D" ? 3 : 0;
     if (!c.dims) throw Fail("unknown #Dimensions_of_the_task " + dims);

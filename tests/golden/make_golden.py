@@ -110,7 +110,40 @@ def golden_cases():
     c.order = "ThirdOrder"
     c.limiter = "vanAlbada"
     out.append(("tube_rk3_fixedvalue_slip_100", c, p, 20, [1, 20]))
+    # ThirdOrderCada: the same stages with the smoothness switch of thirdOrderLimiterCada.hpp
+    # (the tube's jumps are limited, its rarefaction and the shear layers are not)
+    c, p = cases.shock_tube_1d(n=200)
+    c.order = "ThirdOrderCada"
+    out.append(("tube_cada_minmod_200", c, p, 30, [1, 2, 30]))
+    c, p = cases.kelvin_helmholtz_2d(n=24, periodic=False)
+    c.order = "ThirdOrderCada"
+    out.append(("kh_slip_24_cada", c, p, 8, [1, 2, 8]))
+    c, p = cases.rayleigh_taylor_2d(nx=16, ny=48, modes=4)
+    c.order = "ThirdOrderCada"
+    c.limiter = "superbee"
+    out.append(("rt_16x48_cada_superbee_gravity", c, p, 8, [1, 8]))
+    out.append(("tube_cada_blend_50", *cada_blend_tube(), 3, [1, 3]))
     return out
+
+
+def cada_blend_tube():
+    """A 1D tube whose cell 20 sits inside the blend window of thirdOrderLimiterCada.hpp at the
+    first stage: its face pressure gradients are 15 and sqrt(T - 15^2), T = sqrt(5/2) (8 pi)^2,
+    so eta = 1 up to rounding (1e-15, the window is 1e-6); a jump of 1 at cell 35 (gradient 50,
+    eta 2.5) is limited and the uniform regions are not."""
+    import math
+
+    c, _ = cases.shock_tube_1d(n=50)
+    c.order = "ThirdOrderCada"
+    n, h = 50, 1.0 / 50
+    T = math.sqrt(5.0 / 2.0) * (8 * math.pi) ** 2
+    g2 = math.sqrt(T - 15.0 ** 2)
+    pr = np.ones(n)
+    pr[20] = 1.0 + 15.0 * h
+    pr[21:] = pr[20] + g2 * h
+    pr[35:] += 1.0
+    prim = [np.full(n, 0.5), np.full(n, 0.3), np.zeros(n), np.zeros(n), np.zeros(n), pr]
+    return c, prim
 
 
 def main(only=None):

@@ -50,6 +50,9 @@ def _deck_cases():
     c, p = cases.kelvin_helmholtz_2d(n=8, periodic=False)
     c.order = "SecondOrderRK"
     out.append(("kh_rk2", c, p))
+    c, p = cases.shock_tube_1d(n=40)
+    c.order = "ThirdOrderCada"
+    out.append(("tube_cada", c, p))
     return out
 
 
@@ -95,7 +98,7 @@ def _edit(path, key, value):
 @pytest.mark.parametrize("file,key,value,message", [
     ("main.txt", "#Diffusion_flag", "on", "Diffusion"),
     ("main.txt", "#Turbulence_flag", "yes", "Turbulence"),
-    ("main.txt", "#Approximation_order", "ThirdOrderCada", "ThirdOrder are implemented"),
+    ("main.txt", "#Approximation_order", "FourthOrder", "Unknown gas dynamics approximation order."),
     ("main.txt", "#TVD_limiter_type", "vanLeer3", "limiter"),
     ("main.txt", "#Type_of_flow_solver", "KT", "HLLC"),
     ("main.txt", "#Source_timestep_correction", "Courant", "Wrong format of time-step parameters settings"),
