@@ -743,7 +743,8 @@ __global__ void __launch_bounds__(BX * BY, adjointMinBlocks<T, BX, BY>()) k_adjo
     WS Wc, Wn;
     WB Bc;
     FB Bn;
-    double lc[NL], ln[NL];
+    // lvc, lvn: the adjoint of rows z and z + 1 divided by the cell volume (face arithmetic); the
+    // FP64 adjoint of row z is read again for its output rather than kept through the row
     T lvc[NL], lvn[NL];
     double ivc = 1, ivn = 1;
     double hmC = P.geo.h[MA][z0 < z1 ? z0 : 0], hmN = hmC;  // heights of rows z and z + 1
@@ -754,10 +755,11 @@ __global__ void __launch_bounds__(BX * BY, adjointMinBlocks<T, BX, BY>()) k_adjo
     // ---- prologue: row z0 and the face below it
     if (has && z0 < z1) {
         loadW(cellAt(z0), Wc);
-        loadPacked<NS, NMOM>(P, A.lamIn, cellAt(z0), lc);
+        double l0[NL];
+        loadPacked<NS, NMOM>(P, A.lamIn, cellAt(z0), l0);
         ivc = invVol(hmC);
 #pragma unroll
-        for (int i = 0; i < NL; ++i) lvc[i] = T(lc[i] * ivc);
+        for (int i = 0; i < NL; ++i) lvc[i] = T(l0[i] * ivc);
         areas(hmC);
         if (interior) {
             const int zb = wrapM(z0 - 1, ok);
@@ -806,6 +808,7 @@ __global__ void __launch_bounds__(BX * BY, adjointMinBlocks<T, BX, BY>()) k_adjo
             ringWait<1>();  // the values of row z + 1 have landed
         }
         if (hasNext) {
+            double ln[NL];
             if constexpr (RING) {
                 const double* src = ringSlot(z + 1);
                 T ut[NL];
@@ -936,6 +939,9 @@ __global__ void __launch_bounds__(BX * BY, adjointMinBlocks<T, BX, BY>()) k_adjo
             if (D == 3) unpackAdd<T, NS, NMOM>(sBy + slot, SL, Bc.f);
             T ub[NL];
             wReverse<T, NS, NMOM>(mp, Wc, Bc, ub);
+            const long long ic = cellAt(z);
+            double lc[NL];
+            loadPacked<NS, NMOM>(P, A.lamIn, ic, lc);
             double out[NL];
 #pragma unroll
             for (int i = 0; i < NL; ++i) out[i] = lc[i] + double(ub[i]);
@@ -975,7 +981,6 @@ __global__ void __launch_bounds__(BX * BY, adjointMinBlocks<T, BX, BY>()) k_adjo
                     for (int k = 0; k < NS; ++k) out[k] += dWdX * ((k == A.heavy ? 1.0 : 0.0) - Xh) / c0 * mp.invM[k];
                 }
             }
-            const long long ic = cellAt(z);
             const long long st = P.stride;
 #pragma unroll
             for (int i = 0; i < NL; ++i) A.lamOut[storageField<NS, NMOM>(i) * st + ic] = out[i];
@@ -984,10 +989,7 @@ __global__ void __launch_bounds__(BX * BY, adjointMinBlocks<T, BX, BY>()) k_adjo
         if (hasNext) {
             Wc = Wn;
 #pragma unroll
-            for (int i = 0; i < NL; ++i) {
-                lc[i] = ln[i];
-                lvc[i] = lvn[i];
-            }
+            for (int i = 0; i < NL; ++i) lvc[i] = lvn[i];
             ivc = ivn;
         }
         hmC = hmN;
