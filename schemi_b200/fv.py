@@ -189,20 +189,30 @@ class FVCase:
     def set_time(self, t: float, dt: float) -> None:
         self._check(self.lib.fv_set_time(self._h, t, dt))
 
-    def download(self) -> Dict[str, np.ndarray]:
-        N = self.case.n_species
-        out = [None] * FV_F_COUNT
+    def download_fields(self) -> Dict[str, int]:
+        """Names of the fields fv_download writes for this case, with their fv_download index."""
         names = {}
-        for k in range(N):
-            out[k] = np.empty(self.n_cells)
+        for k in range(self.case.n_species):
             names[f"c{k + 1}"] = k
-            out[8 + k] = np.empty(self.n_cells)
             names[f"rho{k + 1}"] = 8 + k
-        for name, i in FIELD_INDEX.items():
-            out[i] = np.empty(self.n_cells)
-            names[name] = i
-        self._check(self.lib.fv_download(self._h, _ptrs(out)))
-        return {name: out[i] for name, i in names.items()}
+        names.update(FIELD_INDEX)
+        return names
+
+    def download(self, out: Optional[Dict[str, np.ndarray]] = None) -> Dict[str, np.ndarray]:
+        """fv_download into new arrays, or into ``out`` (name -> contiguous float64 array of
+        n_cells, e.g. views of pinned host memory, which the copies then reach by DMA)."""
+        names = self.download_fields()
+        arrs = [None] * FV_F_COUNT
+        for name, i in names.items():
+            if out is not None:
+                a = out[name]
+                if a.dtype != np.float64 or a.size != self.n_cells or not a.flags.c_contiguous:
+                    raise ValueError(f"download buffer {name}: contiguous float64 of {self.n_cells} values")
+                arrs[i] = a
+            else:
+                arrs[i] = np.empty(self.n_cells)
+        self._check(self.lib.fv_download(self._h, _ptrs(arrs)))
+        return {name: arrs[i] for name, i in names.items()}
 
     def state_device(self):
         nf = self.case.n_conserved

@@ -216,3 +216,28 @@ def test_gpu_riemann_failure_status(fv):
     with pytest.raises(fv.FVError) as ei:
         g.step()
     assert ei.value.status == 1
+
+
+def test_gpu_download_into_pinned_buffers(fv):
+    """fv_download into caller-owned page-locked arrays returns the same values as into new
+    arrays, and a buffer of the wrong size is refused before the call."""
+    import torch
+
+    from schemi_b200 import cases
+
+    case, prim = cases.kelvin_helmholtz_2d(n=48)
+    g = fv.FVCase(case)
+    g.upload(prim)
+    for _ in range(3):
+        g.step()
+    ref = g.download()
+    outs = {name: torch.zeros(g.n_cells, dtype=torch.float64, pin_memory=True).numpy()
+            for name in g.download_fields()}
+    got = g.download(outs)
+    assert set(got) == set(ref)
+    for name in ref:
+        assert got[name] is outs[name]
+        assert np.array_equal(got[name], ref[name]), name
+    outs["p"] = np.zeros(g.n_cells - 1)
+    with pytest.raises(ValueError):
+        g.download(outs)
