@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define FV_ABI_VERSION 3
+#define FV_ABI_VERSION 4
 #define FV_MAX_SPECIES 4
 
 typedef int fv_status;
@@ -176,6 +176,10 @@ enum fv_field {
     FV_F_RHO_K,               /* rho_1..rho_N occupy FV_F_RHO_K + k */
     FV_F_RHO = FV_F_RHO_K + FV_MAX_SPECIES,
     FV_F_MX, FV_F_MY, FV_F_MZ, FV_F_E, FV_F_UV, FV_F_T, FV_F_SONIC,
+    FV_F_CONC0,               /* total concentration c_0 as the state holds it: after a SecondOrderRK,
+                                 ThirdOrder or ThirdOrderCada step the averaged field
+                                 (bunchOfFields::average), which can differ from the sum of c_1..c_N in
+                                 the last bit; otherwise that sum (ABI version 4) */
     FV_F_COUNT
 };
 

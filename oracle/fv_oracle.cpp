@@ -1792,6 +1792,7 @@ int fvo_download(fvo_case* cs, double* const* out) {
         if (out[FV_F_UV]) out[FV_F_UV][i] = cs->Uv[i];
         if (out[FV_F_T]) out[FV_F_T][i] = mx.TFromUv(cc, cs->Uv[i]);
         if (out[FV_F_SONIC]) out[FV_F_SONIC][i] = std::sqrt(mx.sqSonicSpeed(cc, cs->rho[0][i], cs->Uv[i], cs->p[i]));
+        if (out[FV_F_CONC0]) out[FV_F_CONC0][i] = cs->c[0][i];
     }
     return FV_OK;
 }

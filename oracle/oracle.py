@@ -27,7 +27,7 @@ REF_BIN_PATCHED = os.path.join(HERE, "_ref", "schemi_patched")
 
 FV_F_COUNT = 22
 FIELD_NAMES = ["c1", "c2", "c3", "c4", "vx", "vy", "vz", "p", "rho1", "rho2", "rho3", "rho4", "rho",
-               "mx", "my", "mz", "E", "Uv", "T", "sonic"]
+               "mx", "my", "mz", "E", "Uv", "T", "sonic", "c0"]
 
 _lib = None
 
@@ -122,7 +122,7 @@ class OracleCase:
             want[k] = out[k]; idx[f"c{k + 1}"] = k
             want[8 + k] = out[8 + k]; idx[f"rho{k + 1}"] = 8 + k
         for name, i in (("vx", 4), ("vy", 5), ("vz", 6), ("p", 7), ("rho", 12), ("mx", 13), ("my", 14),
-                        ("mz", 15), ("E", 16), ("Uv", 17), ("T", 18), ("sonic", 19)):
+                        ("mz", 15), ("E", 16), ("Uv", 17), ("T", 18), ("sonic", 19), ("c0", 20)):
             want[i] = out[i]
             idx[name] = i
         _check(load().fvo_download(self._h, _ptrs(want)))

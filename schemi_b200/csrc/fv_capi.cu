@@ -93,6 +93,7 @@ __global__ void k_download(const StepParams P, const double* __restrict__ U, con
     out[FV_F_UV * n + i] = Uv;
     out[FV_F_T * n + i] = Mixture<double, NS, EOS>::TFromUv(P.mix, c, Uv);
     out[FV_F_SONIC * n + i] = sqrt(Mixture<double, NS, EOS>::sqSonic(P.mix, c, rho0, Uv, p));
+    out[FV_F_CONC0 * n + i] = c[0];
 }
 
 // flag |= (any transverse velocity component of the restart set is non-zero)

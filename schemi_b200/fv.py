@@ -19,7 +19,7 @@ LIB_PATH = os.path.join(HERE, "lib", "libschemi_fv.so")
 
 FV_F_COUNT = 22
 FIELD_INDEX = {"vx": 4, "vy": 5, "vz": 6, "p": 7, "rho": 12, "mx": 13, "my": 14, "mz": 15, "E": 16, "Uv": 17,
-               "T": 18, "sonic": 19}
+               "T": 18, "sonic": 19, "c0": 20}
 ERRORS = {0: "noErrors", 1: "RiemannSolverError", 2: "negativeTemperatureError", 4: "systemError",
           5: "boundaryConditionError", 11: "initialisationError", 12: "NaNError"}
 PATH_MARCH, PATH_GENERIC = 0, 1

@@ -418,11 +418,8 @@ void writeOutput(const Deck& d, fv_handle* h, long long nOutput, double time, co
     for (long long i = 0; i < nc; ++i) {
         const long long ix = i % c.n[0], iy = (i / c.n[0]) % c.n[1], iz = i / ((long long)c.n[0] * c.n[1]);
         double cc[FV_MAX_SPECIES + 1];
-        cc[0] = 0;
-        for (int k = 1; k <= N; ++k) {
-            cc[k] = f[FV_F_CONC + k - 1][i];
-            cc[0] += cc[k];
-        }
+        cc[0] = f[FV_F_CONC0][i];  // the state's total (an averaged field after a multi-stage step)
+        for (int k = 1; k <= N; ++k) cc[k] = f[FV_F_CONC + k - 1][i];
         const double T = f[FV_F_T][i];
         double F, S;
         th.FS(cc, T, F, S);

@@ -11,7 +11,7 @@ replays the same runs with ``schemi_b200/lib/fvrun`` and compares the files byte
 The reference is compiled from its own sources by ``oracle/Makefile`` (``make -C oracle ref``);
 the decks are written by ``schemi_b200.deck``.
 
-    python tests/golden/make_deck_golden.py
+    python tests/golden/make_deck_golden.py [fixture names without the deck_ prefix]
 """
 
 import os
@@ -97,6 +97,17 @@ def deck_cases():
     c, p = cases.chlorine_dissociation_2d(4)
     c.t_end = _t_after(c, p, 6, 0.5)
     out.append(("cl2_4x4", c, p, 2, True, [{}], 1e-10))
+    # multi-stage step solvers: ThirdOrderCada with a restart from output 2 (the averaged
+    # concentrations go through the output files), SecondOrderRK with growing gravity
+    c, p = cases.kelvin_helmholtz_2d(n=8, periodic=False)
+    c.order = "ThirdOrderCada"
+    c.t_end = _t_after(c, p, 6, 0.45)
+    out.append(("kh8_cada_restart", c, p, 3, True, [{}, {"start": "2", "t_end": repr(c.t_end * 1.5)}], 0.0))
+    c, p = cases.rayleigh_taylor_2d(nx=8, ny=16, modes=2)
+    c.order = "SecondOrderRK"
+    c.g_delta = (0.0, -0.05, 0.0)
+    c.t_end = _t_after(c, p, 9, 0.5)
+    out.append(("rt8x16_rk2_gravity", c, p, 4, True, [{}], 0.0))
     return out
 
 
@@ -113,11 +124,13 @@ def _key(prefix, rel):
     return prefix + ":" + rel.replace(os.sep, "|")
 
 
-def main():
+def main(only=None):
     binary = O.REF_BIN_PATCHED
     if not os.path.exists(binary):
         raise SystemExit(f"{binary} missing: run make -C oracle ref")
     for name, case, prim, freq, restart, runs, tol in deck_cases():
+        if only and name not in only:
+            continue
         d = tempfile.mkdtemp(prefix="schemi_deck_")
         try:
             write_deck(case, d, prim, frequency_of_output=freq, restart=restart)
@@ -151,4 +164,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or None)

@@ -17,7 +17,7 @@ from golden_cases import rel_err
 
 pytestmark = pytest.mark.gpu
 
-FIELDS = ["c1", "c2", "vx", "vy", "p", "rho", "E", "T"]
+FIELDS = ["c1", "c2", "c0", "vx", "vy", "p", "rho", "E", "T"]
 
 
 @pytest.fixture(scope="module")
