@@ -111,8 +111,10 @@ enum fv_chemistry { FV_CHEM_NONE = 0, FV_CHEM_A_B_2C = 1, FV_CHEM_CL2 = 2 };
  *                    the indicator eta of the face's and the farthest face's surface gradients is
  *                    below 1 - 1e-6, limited above 1 + 1e-6, blended in between;
  *                    thirdOrderStepSolverCada.cpp, Advection3dOrderCada.cpp).
- * The multi-stage solvers run on the generic path (SecondOrderRK also on the fused march) and are
- * not combined with chemistry, the batched ensemble, the adjoint or fv_step_noalloc. */
+ * The multi-stage solvers run on the generic path (SecondOrderRK also on the fused march); with a
+ * chemical mechanism the chemistry pass follows the last average (secondOrderStepSolverRK.cpp:
+ * 114-118, thirdOrderStepSolver.cpp:125-129).  They are not combined with the batched ensemble,
+ * the adjoint or fv_step_noalloc. */
 enum fv_step_solver { FV_ORDER_SECOND = 0, FV_ORDER_SECOND_RK = 1, FV_ORDER_THIRD = 2, FV_ORDER_THIRD_CADA = 3 };
 
 /* Per-cell linear solver of the backward-Euler step (set/chemicalKinetics.txt #Iterative_solver:

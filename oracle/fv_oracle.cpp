@@ -1637,10 +1637,6 @@ bool validate(const fv_config& cf, std::string& err) {
         err = "unknown step solver";
         return false;
     }
-    if (cf.order != FV_ORDER_SECOND && cf.chemistry != FV_CHEM_NONE) {
-        err = "multi-stage step solvers with chemistry are not implemented";
-        return false;
-    }
     return true;
 }
 
@@ -1740,7 +1736,9 @@ int fvo_step(fvo_case* cs, double* dt_used, double* dt_next) {
                                                                          : doStep(*cs, dt);
     if (st != FV_OK) return st;
     if (cs->cfg.chemistry != FV_CHEM_NONE) {
-        // secondOrderStepSolver::calculateStep: chemistry after the advection, same dt
+        // chemistry after the advection (and after the multi-stage average), same dt:
+        // secondOrderStepSolver.cpp:87-91, secondOrderStepSolverRK.cpp:114-118,
+        // thirdOrderStepSolver.cpp:125-129
         st = chemistryStep(*cs, dt);
         if (st != FV_OK) return st;
     }

@@ -271,10 +271,6 @@ bool validate(const fv_config& c, std::string& e) {
         e = "unknown step solver (order)";
         return false;
     }
-    if (c.order != FV_ORDER_SECOND && c.chemistry != FV_CHEM_NONE) {
-        e = "multi-stage step solvers with chemistry are not implemented";
-        return false;
-    }
     if (c.chemistry != FV_CHEM_NONE) {
         if (c.chem_solver < FV_CHEM_GAUSS_SEIDEL || c.chem_solver > FV_CHEM_JACOBI_CONJUGATE_GRADIENT) {
             e = "unknown chemical iterative solver";
@@ -438,6 +434,23 @@ void average(fv_handle* h, int from, const double* concIn, double* concOut, doub
     }
 }
 
+// The chemistry pass after a multi-stage average (secondOrderStepSolverRK.cpp:114-118,
+// thirdOrderStepSolver.cpp:125-129) on U[from ^ 1] and the stored concentrations, then the CFL
+// finalize over its partials; without chemistry the finalize over the average's partials.
+cudaError_t chemistryAndFinalize(fv_handle* h, int from) {
+    int blocks = (int)genericBlocks(h->P);
+    if (h->cfg.chemistry != FV_CHEM_NONE) {
+        chem::ChemParams C = h->chem;
+        C.conc = h->conc;
+        cudaError_t e = launchChemistry(h->cfg.n_species, h->cfg.eos, h->cfg.dims, h->P, C, h->U[from ^ 1], h->ck,
+                                        h->blockMax, h->stream);
+        if (e != cudaSuccess) return e;
+        blocks = chemistryBlocks(h->P);
+    }
+    k_finalize<<<1, 1024, 0, h->stream>>>(h->P, h->ck, h->blockMax, blocks);
+    return cudaGetLastError();
+}
+
 // SecondOrderRK: stage 1 U[from] -> U[from ^ 1] (concentrations of the start state), stage 2
 // U[from ^ 1] -> Ustage, average (Ustage, U[from]) -> U[from ^ 1] with the CFL partials.
 cudaError_t enqueueRk2(fv_handle* h, int from) {
@@ -457,8 +470,7 @@ cudaError_t enqueueRk2(fv_handle* h, int from) {
     average(h, from, h->conc, h->conc, 0.5);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_finalize<<<1, 1024, 0, h->stream>>>(h->P, h->ck, h->blockMax, (int)genericBlocks(h->P));
-    return cudaGetLastError();
+    return chemistryAndFinalize(h, from);
 }
 
 // ThirdOrder (SSP-RK3): stage 1 U[from] -> U[from ^ 1]; stage 2 U[from ^ 1] -> Ustage;
@@ -485,8 +497,7 @@ cudaError_t enqueueRk3(fv_handle* h, int from) {
     if ((e = stage(P3, h->U[from ^ 1], h->Ustage, nullptr)) != cudaSuccess) return e;
     average(h, from, h->conc, h->conc, 2. / 3.);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_finalize<<<1, 1024, 0, h->stream>>>(h->P, h->ck, h->blockMax, (int)genericBlocks(h->P));
-    return cudaGetLastError();
+    return chemistryAndFinalize(h, from);
 }
 
 cudaError_t enqueueStep(fv_handle* h, int from) {
@@ -669,6 +680,7 @@ fv_status fv_create(const fv_config* cfg, fv_handle** out) {
     h->chem.nb = cfg->chem_backward.n;
     h->chem.Eb = cfg->chem_backward.E;
     h->chem.q = cfg->chem_q;
+    h->chem.conc = nullptr;  // the multi-stage enqueues pass the stored concentrations
     h->shape = defaultShape(*cfg);
 
     // generic face layout
@@ -1020,10 +1032,11 @@ fv_status fv_check(fv_handle* h) {
 long long fv_kernels_per_step(const fv_handle* h) {
     if (!h) return 0;
     const int stage = h->path == PATH_MARCH ? 1 : 4;
-    if (h->cfg.order == FV_ORDER_SECOND_RK) return 2 * stage + 2;  // two stages, average, finalize
+    const int chem = h->cfg.chemistry != FV_CHEM_NONE ? 1 : 0;
+    if (h->cfg.order == FV_ORDER_SECOND_RK) return 2 * stage + 2 + chem;  // two stages, average, finalize
     if (h->cfg.order == FV_ORDER_THIRD || h->cfg.order == FV_ORDER_THIRD_CADA)
-        return 3 * stage + 3;  // three stages, two averages, finalize
-    return stage + 1 + (h->cfg.chemistry != FV_CHEM_NONE ? 1 : 0);
+        return 3 * stage + 3 + chem;  // three stages, two averages, finalize
+    return stage + 1 + chem;
 }
 
 // ---- introspection used by the tests and the bench (no reference counterpart)

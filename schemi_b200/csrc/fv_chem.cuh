@@ -434,14 +434,23 @@ __global__ void __launch_bounds__(256, 2) k_chemistry(const StepParams P, const 
 #pragma unroll
         for (int d = 0; d < 3; ++d) m[d] = d < P.nmom ? U[(N + 1 + d) * st + i] : 0.0;
         double E = U[(N + 4) * st + i];
-        // derived fields after the advection (Advection.cpp:455-479)
+        // derived fields after the advection (Advection.cpp:455-479), or the concentrations the
+        // multi-stage average left (bunchOfFields::average)
         Cell<N> q;
-        q.c[0] = 0;
+        double cIn[N + 1];
+        if (C.conc) {
 #pragma unroll
-        for (int k = 1; k <= N; ++k) {
-            q.c[k] = rhoS[k - 1] / mx.M[k - 1];
-            q.c[0] += q.c[k];
+            for (int k = 0; k <= N; ++k) q.c[k] = C.conc[k * st + i];
+        } else {
+            q.c[0] = 0;
+#pragma unroll
+            for (int k = 1; k <= N; ++k) {
+                q.c[k] = rhoS[k - 1] / mx.M[k - 1];
+                q.c[0] += q.c[k];
+            }
         }
+#pragma unroll
+        for (int k = 0; k <= N; ++k) cIn[k] = q.c[k];
         double v[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) v[d] = m[d] / rho;
@@ -467,6 +476,13 @@ __global__ void __launch_bounds__(256, 2) k_chemistry(const StepParams P, const 
             }
             E = 0.5 * E + 0.5 * E1;
             U[(N + 4) * st + i] = E;
+            if (C.conc) {
+#pragma unroll
+                for (int k = 0; k <= N; ++k) {
+                    cIn[k] = 0.5 * cIn[k] + 0.5 * q.c[k];
+                    C.conc[k * st + i] = cIn[k];
+                }
+            }
         }
         // CFL signal of the new state
         int ijk[3];
@@ -475,11 +491,16 @@ __global__ void __launch_bounds__(256, 2) k_chemistry(const StepParams P, const 
         ijk[2] = D >= 3 ? (int)(i / ((long long)P.n[0] * P.n[1])) : 0;
         const double ex = extent(P, 0, ijk[0]), ey = extent(P, 1, ijk[1]), ez = extent(P, 2, ijk[2]);
         const double minLS = 1.0 / smin(smin(ex, ey), ez);
-        double rr[N + 1];
-        rr[0] = rho;
+        if (C.conc) {
+            // the state's own (averaged) concentrations, as main's CFL block reads them
+            localMax = smax(localMax, cellSignalC<double, N, EOS, D>(P, cIn, rho, m, E, minLS));
+        } else {
+            double rr[N + 1];
+            rr[0] = rho;
 #pragma unroll
-        for (int k = 1; k <= N; ++k) rr[k] = rhoS[k - 1];
-        localMax = smax(localMax, cellSignal<double, N, EOS, D>(P, rr, rho, m, E, minLS));
+            for (int k = 1; k <= N; ++k) rr[k] = rhoS[k - 1];
+            localMax = smax(localMax, cellSignal<double, N, EOS, D>(P, rr, rho, m, E, minLS));
+        }
     }
     const double bm = blockMaxReduce<double>(localMax, red);
     if (threadIdx.x == 0) blockMax[blockIdx.x] = bm;

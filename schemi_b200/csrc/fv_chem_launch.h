@@ -15,6 +15,9 @@ struct ChemParams {
     int maxIter;
     double Af, nf, Ef, Ab, nb, Eb;
     double q;
+    double* conc;     // concentrations c_0..c_N kept as state (stride apart) after a multi-stage
+                      // average: read as the pass's input and replaced by their 0.5 average with
+                      // the integrated ones; null: c_k = rho_k / M_k
 };
 
 }  // namespace chem

@@ -339,16 +339,10 @@ template <typename T> __device__ __forceinline__ T blockMaxReduce(T v, T* red) {
     return v;
 }
 
-// CFL signal of a cell: (|v| + c) / min edge (Schemi.cpp:807-828), from conserved values.
+// CFL signal of a cell: (|v| + c) / min edge (Schemi.cpp:807-828), from its concentrations
+// c_0..c_N and conserved density, momentum and energy.
 template <typename T, int NS, int EOS, int D>
-__device__ __forceinline__ T cellSignal(const StepParams& P, const T* rho, T rho0, const T* m, T E, T minLS) {
-    T c[NS + 1];
-    c[0] = 0;
-#pragma unroll
-    for (int k = 1; k <= NS; ++k) {
-        c[k] = rho[k] / T(P.mix.M[k - 1]);
-        c[0] += c[k];
-    }
+__device__ __forceinline__ T cellSignalC(const StepParams& P, const T* c, T rho0, const T* m, T E, T minLS) {
     T v[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) v[d] = d < P.nmom ? m[d] / rho0 : T(0);
@@ -362,6 +356,19 @@ __device__ __forceinline__ T cellSignal(const StepParams& P, const T* rho, T rho
     T s = (P.nmom == 3 ? mag3<T>(v[0], v[1], v[2]) : mag2z<T>(v[0], v[1])) + sonic;
     s *= minLS;
     return s;
+}
+
+// The same from conserved values (c_k = rho_k / M_k).
+template <typename T, int NS, int EOS, int D>
+__device__ __forceinline__ T cellSignal(const StepParams& P, const T* rho, T rho0, const T* m, T E, T minLS) {
+    T c[NS + 1];
+    c[0] = 0;
+#pragma unroll
+    for (int k = 1; k <= NS; ++k) {
+        c[k] = rho[k] / T(P.mix.M[k - 1]);
+        c[0] += c[k];
+    }
+    return cellSignalC<T, NS, EOS, D>(P, c, rho0, m, E, minLS);
 }
 
 // ============================================================================ bulk async copies

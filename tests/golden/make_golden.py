@@ -123,6 +123,14 @@ def golden_cases():
     c.limiter = "superbee"
     out.append(("rt_16x48_cada_superbee_gravity", c, p, 8, [1, 8]))
     out.append(("tube_cada_blend_50", *cada_blend_tube(), 3, [1, 3]))
+    # chemistry after the multi-stage average (secondOrderStepSolverRK.cpp:114-118,
+    # thirdOrderStepSolver.cpp:125-129)
+    c, p = cases.chlorine_dissociation_2d(4)
+    c.order = "SecondOrderRK"
+    out.append(("cl2_4x4_vdw_gs_rk2", c, p, 8, [1, 2, 8]))
+    c, p = cases.chlorine_dissociation_2d(4, eos="ideal")
+    c.order = "ThirdOrder"
+    out.append(("cl2_4x4_ideal_gs_rk3", c, p, 6, [1, 6]))
     return out
 
 
