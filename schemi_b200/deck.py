@@ -148,11 +148,17 @@ def _chemistry_block(case: Case) -> str:
 
 
 def write_deck(case: Case, directory: str, prim: Sequence[np.ndarray], frequency_of_output: int = 1,
-               restart: bool = True) -> None:
+               restart: bool = True, zones=None, modifiers=None) -> None:
     """Write ``directory/set`` and the restart point for the reference solver.
 
-    ``prim`` is the restart set c_1..c_N, v_x, v_y, v_z, p (flattened in cell order, x fastest).
+    ``prim`` is the restart set c_1..c_N, v_x, v_y, v_z, p (flattened in cell order, x fastest);
+    the outer zone of the initial fields takes its means.  ``zones``: zones before the outer one,
+    each ``(description, [c_1..c_N], (v_x, v_y, v_z), p)`` with the description in the syntax of
+    zonesDescription.txt (zone.cpp:25-125), e.g. ``"sphere 0.5 0.5 0.5 0.2"`` or
+    ``"plane 0 1 0 point: 0 0.5 0"``.  ``modifiers``: ``{k: (A, B, x0, c)}`` written as
+    ``set/sub_<k>_modifFunction.txt`` (gaussian, phaseInitialization.cpp:1197-1228).
     """
+    zones = list(zones or [])
     if not case.expressible_in_reference():
         raise ValueError("the reference has no periodic patch or A+B->2C mechanism")
     N = case.n_species
@@ -194,9 +200,14 @@ def write_deck(case: Case, directory: str, prim: Sequence[np.ndarray], frequency
     _write(sdir, "g.txt", "#Free_fall_acceleration_flag\n" + ("on" if case.gravity is not None else "off") +
            "\n#Free_fall_acceleration_vector_components\n" + " ".join(_f(x) for x in g) +
            "\n#Acceleration_growth\n" + " ".join(_f(x) for x in case.g_delta))
-    # one outer zone; the fields themselves come from the restart point
-    _write(sdir, "zonesDescription.txt", "#Number_of_zones\n0\n#Outer_zone: yes\n#Zones_description")
+    # the zones, then the outer zone (a restart takes the fields from the restart point instead)
+    _write(sdir, "zonesDescription.txt", f"#Number_of_zones\n{len(zones)}\n#Outer_zone: yes\n#Zones_description" +
+           "".join("\n" + z[0] for z in zones))
     mean = [float(np.mean(a)) for a in prim]
+    zone_c = [[_f(z[1][k]) for z in zones] + [_f(mean[k])] for k in range(N)]
+    zone_v = " ".join(_f(x) for z in zones for x in z[2]) + (" " if zones else "") + " ".join(_f(x) for x in mean[N:N + 3])
+    zone_p = " ".join([_f(z[3]) for z in zones] + [_f(mean[N + 3])])
+    nzv = len(zones) + 1
     for k, sp in enumerate(case.species):
         body = [
             "#Molar_mass_(kg/mol)", _f(sp.M),
@@ -207,18 +218,20 @@ def write_deck(case: Case, directory: str, prim: Sequence[np.ndarray], frequency
             "#Lennard_Jones_eps/kB_(K)", "1",
             "#Lennard_Jones_sigma_(A)", "1",
             _bc_block(case, lambda pb, k=k: pb.conc[k], False),
-            "#Values_in_zones", _f(mean[k]),
+            "#Values_in_zones", " ".join(zone_c[k]),
         ]
         _write(sdir, f"sub_{k + 1}.txt", "\n".join(body))
-    _write(sdir, "velocity.txt", _bc_block(case, lambda pb: pb.vel, True) + "\n#Values_in_zones\n" +
-           " ".join(_f(x) for x in mean[N:N + 3]))
-    _write(sdir, "pressure.txt", _bc_block(case, lambda pb: pb.p, False) + "\n#Values_in_zones\n" + _f(mean[N + 3]))
+    for k, (A, B, x0, w) in (modifiers or {}).items():
+        _write(sdir, f"sub_{k}_modifFunction.txt",
+               f"#Function\ngaussian\n#A\n{_f(A)}\n#B\n{_f(B)}\n#x0\n{_f(x0)}\n#c\n{_f(w)}")
+    _write(sdir, "velocity.txt", _bc_block(case, lambda pb: pb.vel, True) + "\n#Values_in_zones\n" + zone_v)
+    _write(sdir, "pressure.txt", _bc_block(case, lambda pb: pb.p, False) + "\n#Values_in_zones\n" + zone_p)
     free = "\n".join(f"{lab}\n{'freeBoundary' if p in PATCHES_USED[case.dims] else 'blank'}"
                      for lab, p in zip(_PATCH_LABELS, PATCHES))
-    _write(sdir, "k.txt", free + "\n#Values_in_zones\n0.0")
-    _write(sdir, "epsilon.txt", free + "\n#Values_in_zones\n0.0")
-    _write(sdir, "a.txt", free + "\n#Values_in_zones\n0.0 0.0 0.0")
-    _write(sdir, "b.txt", free + "\n#Values_in_zones\n0")
+    _write(sdir, "k.txt", free + "\n#Values_in_zones\n" + " ".join(["0.0"] * nzv))
+    _write(sdir, "epsilon.txt", free + "\n#Values_in_zones\n" + " ".join(["0.0"] * nzv))
+    _write(sdir, "a.txt", free + "\n#Values_in_zones\n" + " ".join(["0.0 0.0 0.0"] * nzv))
+    _write(sdir, "b.txt", free + "\n#Values_in_zones\n" + " ".join(["0"] * nzv))
     _write(sdir, "chemicalKinetics.txt", _chemistry_block(case))
     _write(sdir, "transportCoefficients.txt", _TRANSPORT)
     _write(sdir, "turbulentParameters.txt", _TURB_PARAMS)

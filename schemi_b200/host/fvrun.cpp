@@ -8,15 +8,15 @@
 // positional keys of main/Schemi.cpp:101-163), set/g.txt (:83-99), set/sub_<k>.txt,
 // set/velocity.txt, set/pressure.txt (phaseInitialization.cpp), set/chemicalKinetics.txt
 // (Schemi.cpp:672-716, chemicalKineticsChlorumDissociation.cpp:275-308) and
-// set/zonesDescription.txt (zone.cpp).  The time loop, its output schedule, the restart from
+// set/zonesDescription.txt (zone.cpp: planes, spheres, cylinders, the outer zone) with the
+// optional set/sub_<k>_modifFunction.txt of a fresh run.  The time loop, its output schedule, the restart from
 // fieldsOutput/output_<N> + result/Time.tsv and the last-step clamp follow Schemi.cpp:312-573,
 // 664-670, 716-940; the files written follow output::dataOutput (src/service/output.cpp:14-308):
 // result/output_<NNNNNN>.tsv, result/Time.tsv, fieldsOutput/output_<NNNNNN>/*.dat and
 // timeOfCalculation.tsv, with the reference's 20 significant digits.
 //
-// Not supported (the run stops with a message): zones other than the outer zone, diffusion,
-// turbulence, the 1D mixing-zone width output, and chemical mechanisms other than "no" and
-// "Cl2".
+// Not supported (the run stops with a message): diffusion, turbulence, the 1D mixing-zone width
+// output, and chemical mechanisms other than "no" and "Cl2".
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -81,6 +81,120 @@ bool onOff(const std::string& s, const std::string& what) {
     throw Fail("Unknown " + what + " flag.");
 }
 
+// ---------------------------------------------------------------- zones of the initial fields
+// zone.cpp:25-125 and its shapes (src/service/zoneUnderPlane(s).cpp, zoneInsideSphere.cpp,
+// zoneInsideCylinder.cpp, outerZone.cpp) on the geometry of src/primitives/plane.cpp,
+// sphere.cpp, cylinder.cpp and line.cpp: a cell takes the values of the first zone that holds
+// its centre.  Vector arithmetic as the reference's (component-wise, dot products summed from
+// the first component, magnitudes by the 3-argument std::hypot).
+struct Vec3 {
+    double x[3];
+};
+Vec3 vsub(const Vec3& a, const Vec3& b) { return {{a.x[0] - b.x[0], a.x[1] - b.x[1], a.x[2] - b.x[2]}}; }
+Vec3 vscale(double s, const Vec3& a) { return {{s * a.x[0], s * a.x[1], s * a.x[2]}}; }
+Vec3 vdivs(const Vec3& a, double s) { return {{a.x[0] / s, a.x[1] / s, a.x[2] / s}}; }
+double vdot(const Vec3& a, const Vec3& b) {
+    double r = 0;
+    for (int i = 0; i < 3; ++i) r += a.x[i] * b.x[i];
+    return r;
+}
+double vmag(const Vec3& a) { return std::hypot(a.x[0], a.x[1], a.x[2]); }
+
+struct ZonePlane {  // plane(n, p): normale n / |n|
+    Vec3 n, p;
+    ZonePlane(const Vec3& nn, const Vec3& pp) : n(vdivs(nn, vmag(nn))), p(pp) {}
+    bool under(const Vec3& q) const { return vdot(vsub(p, q), n) >= 0; }
+};
+
+struct Zone {
+    enum Kind { PLANES, SPHERE, CYLINDER, OUTER } kind = OUTER;
+    std::vector<ZonePlane> planes;  // PLANES (one for "plane"), the two caps of CYLINDER
+    Vec3 c{};                       // SPHERE centre, CYLINDER axis point
+    Vec3 t{};                       // CYLINDER axis tangent
+    double r = 0;
+    bool contains(const Vec3& q) const {
+        switch (kind) {
+        case PLANES: {
+            bool in = true;
+            for (const ZonePlane& pl : planes) in = in && pl.under(q);
+            return in;
+        }
+        case SPHERE: return vmag(vsub(q, c)) <= r;
+        case CYLINDER: {
+            bool in = true;
+            for (const ZonePlane& pl : planes) in = in && pl.under(q);
+            const Vec3 w = vsub(c, q);
+            return in && vmag(vsub(w, vscale(vdot(w, t), t))) <= r;
+        }
+        default: return true;
+        }
+    }
+};
+
+std::vector<Zone> readZones(const std::string& path) {
+    Tokens t(path);
+    t.skip();
+    const long long nz = (long long)t.num("number of zones");
+    t.skip();
+    bool outer;
+    try {
+        outer = onOff(t.next("outer zone flag"), "outer zone");
+    } catch (const Fail&) {
+        throw Fail("Unknown flag for outer zone description.");
+    }
+    t.skip();
+    auto vec = [&](const char* what) {
+        Vec3 v;
+        for (double& x : v.x) x = t.num(what);
+        return v;
+    };
+    auto radius = [&]() {
+        const double r = t.num("zone radius");
+        if (r <= 0) throw Fail("Radius cannot be less or equal zero.");
+        return r;
+    };
+    std::vector<Zone> zones;
+    for (long long z = 0; z < nz; ++z) {
+        const std::string type = t.next("zone type");
+        Zone zn;
+        if (type == "plane" || type == "planes") {
+            zn.kind = Zone::PLANES;
+            const long long np = type == "plane" ? 1 : (long long)t.num("number of planes");
+            for (long long q = 0; q < np; ++q) {
+                const Vec3 n = vec("plane normal");
+                t.skip();
+                zn.planes.emplace_back(n, vec("plane point"));
+            }
+        } else if (type == "sphere") {
+            zn.kind = Zone::SPHERE;
+            zn.c = vec("sphere centre");
+            zn.r = radius();
+        } else if (type == "cylinder") {
+            zn.kind = Zone::CYLINDER;
+            const Vec3 n1 = vec("cylinder axis");
+            t.skip();
+            const Vec3 c1 = vec("cylinder base point");
+            t.skip();
+            const Vec3 c2 = vec("cylinder top point");
+            const double r = radius();
+            // cylinder.cpp: caps plane(n1 / |n1|, c1), plane(-n1 / |-n1|, c2) (each plane divides by
+            // the length again), axis line(n1 / |n1|, c2)
+            const Vec3 u = vdivs(n1, vmag(n1));
+            const Vec3 n2 = vscale(-1, n1);
+            zn.planes.emplace_back(u, c1);
+            zn.planes.emplace_back(vdivs(n2, vmag(n2)), c2);
+            zn.t = vdivs(u, vmag(u));
+            zn.c = c2;
+            zn.r = r;
+        } else {
+            throw Fail("Unknown zone type.");
+        }
+        zones.push_back(zn);
+    }
+    if (outer) zones.push_back(Zone{});
+    return zones;
+}
+
 int bcType(const std::string& s) {
     if (s == "blank") return 0;  // patches of unused axes
     if (s == "freeBoundary") return FV_BC_FREE;
@@ -106,13 +220,15 @@ struct Deck {
     long long freq = 1;
     double minTime = 0;
     std::string units, eos, readFrom;
-    std::vector<double> zoneC, zoneV, zoneP;  // outer-zone values: c_k, v, p
+    std::vector<Zone> zones;                  // zones of the initial fields, the outer one last
+    std::vector<std::vector<double>> zoneC;   // [k][zone] concentration c_k
+    std::vector<double> zoneV, zoneP;         // [3 * zone + q] velocity, [zone] pressure
     double hPlanck = 0;
 
     std::string path(const std::string& rel) const { return dir + "/" + rel; }
 };
 
-// sub_k / velocity / pressure: six patch conditions, then the outer-zone values.
+// sub_k / velocity / pressure: six patch conditions, then the values of every zone.
 void readPatches(Tokens& t, int nval, int field, int k, fv_config& c) {
     for (int patch = 0; patch < 6; ++patch) {
         t.skip();  // #<Patch>_boundary_condition
@@ -220,13 +336,8 @@ Deck readDeck(const std::string& dir) {
     }
     c.precision = FV_PREC_F64;
     if (c.n_species < 1 || c.n_species > FV_MAX_SPECIES) throw Fail("number of components must be 1..4");
-    // zones: the outer zone only
-    {
-        Tokens t(d.path("set/zonesDescription.txt"));
-        t.skip();
-        const int nz = (int)t.num("number of zones");
-        if (nz != 0) throw Fail("zones other than the outer zone are not implemented by this driver");
-    }
+    d.zones = readZones(d.path("set/zonesDescription.txt"));
+    const size_t nzv = d.zones.size();
     for (int k = 0; k < c.n_species; ++k) {
         Tokens t(d.path("set/sub_" + std::to_string(k + 1) + ".txt"));
         t.skip(); c.M[k] = t.num("molar mass");
@@ -235,20 +346,21 @@ Deck readDeck(const std::string& dir) {
         t.skip(); c.Pc[k] = t.num("Pc");
         for (int q = 0; q < 3; ++q) { t.skip(); t.next("transport parameter"); }
         readPatches(t, 1, 0, k, c);
-        t.skip();
-        d.zoneC.push_back(t.num("zone concentration"));
+        if (t.next("values label") != "#Values_in_zones") throw Fail("Wrong position in file.");
+        d.zoneC.emplace_back();
+        for (size_t z = 0; z < nzv; ++z) d.zoneC[k].push_back(t.num("zone concentration"));
     }
     {
         Tokens t(d.path("set/velocity.txt"));
         readPatches(t, 3, 1, 0, c);
-        t.skip();
-        for (int q = 0; q < 3; ++q) d.zoneV.push_back(t.num("zone velocity"));
+        if (t.next("values label") != "#Values_in_zones") throw Fail("Wrong position in file.");
+        for (size_t z = 0; z < 3 * nzv; ++z) d.zoneV.push_back(t.num("zone velocity"));
     }
     {
         Tokens t(d.path("set/pressure.txt"));
         readPatches(t, 1, 2, 0, c);
-        t.skip();
-        d.zoneP.push_back(t.num("zone pressure"));
+        if (t.next("values label") != "#Values_in_zones") throw Fail("Wrong position in file.");
+        for (size_t z = 0; z < nzv; ++z) d.zoneP.push_back(t.num("zone pressure"));
     }
     // chemistry
     {
@@ -304,6 +416,42 @@ std::vector<double> centres(const fv_config& c, int a) {
         out[i] = s / 8.;
     }
     return out;
+}
+
+// Initial fields of a fresh run (phaseInitialization.cpp:1160-1310): every cell takes the values
+// of the first zone holding its centre, then a species' concentration is scaled by the optional
+// set/sub_<k>_modifFunction.txt ("gaussian": A + B exp(-((x - x0) / c)^2) of the centre's x).
+void initialFields(const Deck& d, const fv_config& c, std::vector<std::vector<double>>& prim) {
+    const int N = c.n_species;
+    const std::vector<double> cx = centres(c, 0), cy = centres(c, 1), cz = centres(c, 2);
+    const long long nc = (long long)c.n[0] * c.n[1] * c.n[2];
+    auto zoneOf = [&](long long i, const std::string& what) -> size_t {
+        const long long ix = i % c.n[0], iy = (i / c.n[0]) % c.n[1], iz = i / ((long long)c.n[0] * c.n[1]);
+        const Vec3 rc{{cx[ix], cy[iy], cz[iz]}};
+        for (size_t z = 0; z < d.zones.size(); ++z)
+            if (d.zones[z].contains(rc)) return z;
+        throw Fail("Cell " + std::to_string(i) + " of " + what + " dropped out of all zones.");
+    };
+    for (int k = 0; k < N; ++k) {
+        for (long long i = 0; i < nc; ++i)
+            prim[k][i] = d.zoneC[k][zoneOf(i, std::to_string(k + 1) + " component concentration")];
+        std::ifstream mf(d.path("set/sub_" + std::to_string(k + 1) + "_modifFunction.txt"));
+        if (!mf.is_open()) continue;
+        std::string skip, name;
+        mf >> skip >> name;
+        if (name != "gaussian") continue;  // other names leave the field as it is
+        double A, B, x0, w;
+        mf >> skip >> A >> skip >> B >> skip >> x0 >> skip >> w;
+        for (long long i = 0; i < nc; ++i) {
+            const double u = (cx[i % c.n[0]] - x0) / w;
+            prim[k][i] *= A + B * std::exp(-(u * u));
+        }
+    }
+    for (long long i = 0; i < nc; ++i) {
+        const size_t z = zoneOf(i, "velocity");
+        for (int q = 0; q < 3; ++q) prim[N + q][i] = d.zoneV[3 * z + q];
+    }
+    for (long long i = 0; i < nc; ++i) prim[N + 3][i] = d.zoneP[zoneOf(i, "pressure")];
 }
 
 // ---------------------------------------------------------------- Helmholtz energy and entropy
@@ -532,9 +680,7 @@ int run(const Deck& d) {
     double time = 0;
     const bool fresh = d.readFrom == "no" || d.readFrom == "initialisation";
     if (fresh) {
-        for (int k = 0; k < N; ++k) std::fill(prim[k].begin(), prim[k].end(), d.zoneC[k]);
-        for (int q = 0; q < 3; ++q) std::fill(prim[N + q].begin(), prim[N + q].end(), d.zoneV[q]);
-        std::fill(prim[N + 3].begin(), prim[N + 3].end(), d.zoneP[0]);
+        initialFields(d, c, prim);
         std::filesystem::create_directories(d.path("result"));
         std::ofstream(d.path("result/Time.tsv")).close();  // recreated
     } else {

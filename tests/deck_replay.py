@@ -3,7 +3,8 @@ files it writes with the reference solver's.
 
 A fixture holds the task directory as the reference read it, the ``set/main.txt`` of every run
 made in that directory and every file the reference left behind (``golden/make_deck_golden.py``).
-``timeOfCalculation.tsv`` is compared without its measured milliseconds.  Fixtures with a
+``timeOfCalculation.tsv`` is compared without its measured milliseconds (the value after every
+"Time of ..." label: the run's and each stage's wall time).  Fixtures with a
 non-zero ``tolerance`` (the chemistry deck) are compared value by value to that relative
 tolerance, velocities and momenta on the scale of the largest sonic speed (and density); all
 others byte for byte.
@@ -125,8 +126,11 @@ def replay(driver, name, d, timeout=600):
         if rel not in got:
             continue
         if rel == "timeOfCalculation.tsv":
-            g, w = got[rel].decode().split("\n"), data.decode().split("\n")
-            del g[1], w[1]  # measured milliseconds
+            def untimed(text):
+                lines = text.split("\n")
+                return [x for i, x in enumerate(lines) if not (i > 0 and lines[i - 1].startswith("Time of"))]
+
+            g, w = untimed(got[rel].decode()), untimed(data.decode())
             if g != w:
                 problems.append(f"{rel}: {g}, reference {w}")
         elif tol == 0:

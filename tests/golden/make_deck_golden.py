@@ -56,7 +56,8 @@ def _set_main(text, **values):
 
 
 def deck_cases():
-    """(name, case, prim, frequency, restart, [main.txt edits per run], tolerance)."""
+    """(name, case, prim, frequency, restart, [main.txt edits per run], tolerance[, write_deck
+    keyword arguments])."""
     out = []
     # Kelvin-Helmholtz 8x8, slip walls: restart deck, then a second run from output 2
     c, p = cases.kelvin_helmholtz_2d(n=8, periodic=False)
@@ -108,6 +109,18 @@ def deck_cases():
     c.g_delta = (0.0, -0.05, 0.0)
     c.t_end = _t_after(c, p, 9, 0.5)
     out.append(("rt8x16_rk2_gravity", c, p, 4, True, [{}], 0.0))
+    # initial fields from zones (a fresh run): a plane, a sphere, a slab of two planes and a
+    # cylinder before the outer zone (first match wins), and a gaussian modifier of species 1
+    c, p = cases.kelvin_helmholtz_2d(n=16, periodic=False)
+    zones = [
+        ("plane 0 1 0 point: 0 0.25 0", [0.05, 0.02], (0.3, 0.0, 0.0), 2.6),
+        ("sphere 0.5 0.6 0.5 0.15", [0.01, 0.2], (-0.2, 0.05, 0.0), 2.4),
+        ("planes 2 1 0 0 point: 0.8 0 0 -1 0 0 point: 0.7 0 0", [0.03, 0.1], (0.0, -0.1, 0.0), 2.55),
+        ("cylinder 0 0 1 top: 0.2 0.8 1 bottom: 0.2 0.8 0 0.12", [0.06, 0.05], (0.1, 0.1, 0.0), 2.7),
+    ]
+    c.t_end = _t_after(c, p, 6, 0.3)
+    out.append(("kh16_zones_fresh", c, p, 3, False, [{}], 0.0,
+                {"zones": zones, "modifiers": {1: (1.0, 0.5, 0.5, 0.2)}}))
     return out
 
 
@@ -128,12 +141,12 @@ def main(only=None):
     binary = O.REF_BIN_PATCHED
     if not os.path.exists(binary):
         raise SystemExit(f"{binary} missing: run make -C oracle ref")
-    for name, case, prim, freq, restart, runs, tol in deck_cases():
+    for name, case, prim, freq, restart, runs, tol, *extra in deck_cases():
         if only and name not in only:
             continue
         d = tempfile.mkdtemp(prefix="schemi_deck_")
         try:
-            write_deck(case, d, prim, frequency_of_output=freq, restart=restart)
+            write_deck(case, d, prim, frequency_of_output=freq, restart=restart, **(extra[0] if extra else {}))
             inputs = _files(d)
             base = inputs[os.path.join("set", "main.txt")].decode()
             data = {_key("in", rel): np.frombuffer(b, dtype=np.uint8) for rel, b in inputs.items()}

@@ -105,7 +105,7 @@ def _edit(path, key, value):
     ("main.txt", "#Source_timestep_correction", "Implicit=0.25,0.5", "Unknown source time-step flag."),
     ("main.txt", "#Defines_universal_gas_constant", "Planck", "Unknown type of universal gas constant."),
     ("main.txt", "#Reconstruction", "cubic", "Unknown reconstruction flag."),
-    ("zonesDescription.txt", "#Number_of_zones", "1", "outer zone"),
+    ("zonesDescription.txt", "#Number_of_zones", "1", "end of file"),
     ("g.txt", "#Free_fall_acceleration_flag", "maybe", "Unknown gravitation flag."),
     ("chemicalKinetics.txt", "#Type_of_chemical_reaction", "H2Cl2Combustion", "not implemented"),
 ])
@@ -150,3 +150,43 @@ def test_host_io_on_oracle_matches_reference_files(tmp_path, name):
         subprocess.run(["make", "-s", "-C", os.path.dirname(os.path.dirname(ORACLE_DRIVER))], check=True)
     problems = replay(ORACLE_DRIVER, name, str(tmp_path))
     assert not problems, "\n".join(problems)
+
+
+def _replace(path, old, new):
+    text = open(path).read()
+    assert old in text
+    open(path, "w").write(text.replace(old, new))
+
+
+def test_unknown_outer_zone_flag_refused(tmp_path):
+    c, p = cases.kelvin_helmholtz_2d(n=8, periodic=False)
+    write_deck(c, str(tmp_path), p, restart=False)
+    _replace(os.path.join(tmp_path, "set", "zonesDescription.txt"), "#Outer_zone: yes", "#Outer_zone: maybe")
+    res = _print_config(str(tmp_path))
+    assert res.returncode != 0
+    assert "Unknown flag for outer zone description." in res.stderr
+
+
+@pytest.mark.parametrize("description,message", [
+    ("cube 0 0 0 1", "Unknown zone type."),
+    ("sphere 0.5 0.5 0.5 0", "Radius cannot be less or equal zero."),
+])
+def test_bad_zone_refused(tmp_path, description, message):
+    c, p = cases.kelvin_helmholtz_2d(n=8, periodic=False)
+    write_deck(c, str(tmp_path), p, restart=False,
+               zones=[(description, [0.05, 0.02], (0.0, 0.0, 0.0), 2.5)])
+    res = _print_config(str(tmp_path))
+    assert res.returncode != 0
+    assert message in res.stderr
+
+
+def test_cells_outside_every_zone_refused(tmp_path):
+    """Without the outer zone a cell outside every zone stops the fresh run with the reference's
+    message (phaseInitialization.cpp:1188-1193)."""
+    c, p = cases.kelvin_helmholtz_2d(n=8, periodic=False)
+    write_deck(c, str(tmp_path), p, restart=False,
+               zones=[("sphere 0.5 0.5 0.5 0.1", [0.05, 0.02], (0.0, 0.0, 0.0), 2.5)])
+    _replace(os.path.join(tmp_path, "set", "zonesDescription.txt"), "#Outer_zone: yes", "#Outer_zone: no")
+    res = subprocess.run([ORACLE_DRIVER, str(tmp_path)], capture_output=True, text=True, timeout=60)
+    assert res.returncode != 0
+    assert "Cell 0 of 1 component concentration dropped out of all zones." in res.stderr
