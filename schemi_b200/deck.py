@@ -148,7 +148,7 @@ def _chemistry_block(case: Case) -> str:
 
 
 def write_deck(case: Case, directory: str, prim: Sequence[np.ndarray], frequency_of_output: int = 1,
-               restart: bool = True, zones=None, modifiers=None) -> None:
+               restart: bool = True, zones=None, modifiers=None, mixing_width: bool = False) -> None:
     """Write ``directory/set`` and the restart point for the reference solver.
 
     ``prim`` is the restart set c_1..c_N, v_x, v_y, v_z, p (flattened in cell order, x fastest);
@@ -157,6 +157,8 @@ def write_deck(case: Case, directory: str, prim: Sequence[np.ndarray], frequency
     zonesDescription.txt (zone.cpp:25-125), e.g. ``"sphere 0.5 0.5 0.5 0.2"`` or
     ``"plane 0 1 0 point: 0 0.5 0"``.  ``modifiers``: ``{k: (A, B, x0, c)}`` written as
     ``set/sub_<k>_modifFunction.txt`` (gaussian, phaseInitialization.cpp:1197-1228).
+    ``mixing_width``: ``#Calculation_of_mixing_zone_width on`` (a 1D task then writes
+    ``result/timeWidth.tsv``).
     """
     zones = list(zones or [])
     if not case.expressible_in_reference():
@@ -192,7 +194,7 @@ def write_deck(case: Case, directory: str, prim: Sequence[np.ndarray], frequency
         ("#Reconstruction", "star"),
         ("#Approximation_order", case.order),
         ("#Start_From_Time-Step", "1" if restart else "no"),
-        ("#Calculation_of_mixing_zone_width", "off"),
+        ("#Calculation_of_mixing_zone_width", "on" if mixing_width else "off"),
         ("#Nonlinearity_iterations", "off"),
     ]
     _write(sdir, "main.txt", "\n".join(f"{k}\n{v}" for k, v in main))

@@ -15,8 +15,9 @@
 // result/output_<NNNNNN>.tsv, result/Time.tsv, fieldsOutput/output_<NNNNNN>/*.dat and
 // timeOfCalculation.tsv, with the reference's 20 significant digits.
 //
-// Not supported (the run stops with a message): diffusion, turbulence, the 1D mixing-zone width
-// output, and chemical mechanisms other than "no" and "Cl2".
+// A 1D task with #Calculation_of_mixing_zone_width on also writes result/timeWidth.tsv
+// (output::mixedZoneWidth1D).  Not supported (the run stops with a message): diffusion,
+// turbulence, and chemical mechanisms other than "no" and "Cl2".
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -223,6 +224,7 @@ struct Deck {
     std::vector<Zone> zones;                  // zones of the initial fields, the outer one last
     std::vector<std::vector<double>> zoneC;   // [k][zone] concentration c_k
     std::vector<double> zoneV, zoneP;         // [3 * zone + q] velocity, [zone] pressure
+    bool width1D = false;                     // 1D task with #Calculation_of_mixing_zone_width on
     double hPlanck = 0;
 
     std::string path(const std::string& rel) const { return dir + "/" + rel; }
@@ -305,7 +307,7 @@ Deck readDeck(const std::string& dir) {
     else if (order == "ThirdOrder") c.order = FV_ORDER_THIRD;
     else if (order == "ThirdOrderCada") c.order = FV_ORDER_THIRD_CADA;
     else throw Fail("Unknown gas dynamics approximation order.");  // abstractStepSolver.cpp:87-94
-    if (onOff(width, "mixed zone width calculation") && dims == "1D") throw Fail("#Calculation_of_mixing_zone_width on is not implemented");
+    d.width1D = onOff(width, "mixed zone width calculation") && dims == "1D";
     c.dims = dims == "1D" ? 1 : dims == "2D" ? 2 : dims == "3D" ? 3 : 0;
     if (!c.dims) throw Fail("unknown #Dimensions_of_the_task " + dims);
     for (int q = c.dims; q < 3; ++q) c.n[q] = 1;
@@ -660,6 +662,50 @@ void printConfig(const fv_config& c, const Deck& d) {
               << "\", \"order\": " << c.order << "}" << std::endl;
 }
 
+// output::mixedZoneWidth1D (src/service/output.cpp:310-391): the distance between the first
+// crossings (in cell order) of the mole fraction c_1 / c_0 through 0.01 and through 0.99, each at
+// the mid-point of the two cells, or at an end of the tube when there is none; appended to
+// result/timeWidth.tsv as "time<TAB>width".
+void writeWidth(const Deck& d, fv_handle* h, double time) {
+    const fv_config& c = d.cfg;
+    const long long n = c.n[0];
+    std::vector<double> c0(n), c1(n);
+    std::vector<double*> ptr(FV_F_COUNT, nullptr);
+    ptr[FV_F_CONC0] = c0.data();
+    ptr[FV_F_CONC] = c1.data();
+    const fv_status st = fv_download(h, ptr.data());
+    if (st != FV_OK) throw Fail(std::string("fv_download: ") + fv_last_error(h), st);
+    const std::vector<double> x = centres(c, 0);
+    const double zeroMix = 0.01;
+    auto X = [&](long long i) { return c1[i] / c0[i]; };
+    double rL = 0, rR = 0;
+    bool found = false;
+    for (long long i = 0; i + 1 < n; ++i) {
+        const bool b1 = X(i) >= zeroMix && X(i + 1) < zeroMix, b2 = X(i) < zeroMix && X(i + 1) >= zeroMix;
+        if (b1 || b2) {
+            rL = 0.5 * (x[i] + x[i + 1]);
+            found = true;
+            break;
+        }
+    }
+    if (!found) rL = X(0) < X(n - 1) ? x[0] : x[n - 1];
+    found = false;
+    for (long long i = 0; i + 1 < n; ++i) {
+        const bool b1 = X(i) > (1 - zeroMix) && X(i + 1) <= (1 - zeroMix);
+        const bool b2 = X(i) <= (1 - zeroMix) && X(i + 1) > (1 - zeroMix);
+        if (b1 || b2) {
+            rR = 0.5 * (x[i] + x[i + 1]);
+            found = true;
+            break;
+        }
+    }
+    if (!found) rR = X(0) > X(n - 1) ? x[0] : x[n - 1];
+    std::ofstream f(d.path("result/timeWidth.tsv"), std::ios::app);
+    if (!f.is_open()) throw Fail("Couldn't create ./result/timeWidth.tsv.", FV_ERR_SYSTEM);
+    f.precision(kPrecision);
+    f << time << '\t' << std::abs(rR - rL) << '\n';
+}
+
 int run(const Deck& d) {
     const fv_config& c = d.cfg;
     const int N = c.n_species;
@@ -676,13 +722,15 @@ int run(const Deck& d) {
 
     // restart set
     std::vector<std::vector<double>> prim(N + 4, std::vector<double>(nc));
-    long long nouts = 0, nsteps = 0;
+    long long nouts = 0, nsteps = 0, noutsW = 0;
+    const long long freqW = std::min(d.freq, 1000LL);  // Schemi.cpp:178
     double time = 0;
     const bool fresh = d.readFrom == "no" || d.readFrom == "initialisation";
     if (fresh) {
         initialFields(d, c, prim);
         std::filesystem::create_directories(d.path("result"));
         std::ofstream(d.path("result/Time.tsv")).close();  // recreated
+        if (d.width1D) std::ofstream(d.path("result/timeWidth.tsv")) << "Time" << '\t' << "Width" << std::endl;
     } else {
         const long long point = std::stoll(d.readFrom);
         std::ifstream tf(d.path("result/Time.tsv"));
@@ -725,6 +773,34 @@ int run(const Deck& d) {
                     }
             }
         }
+        if (d.width1D) {
+            // Schemi.cpp:478-541: the width outputs up to the restart time; the file is rewritten
+            // with those lines (the header and the outputs at times not after it)
+            std::vector<std::string> wlines;
+            {
+                std::ifstream wf(d.path("result/timeWidth.tsv"));
+                if (!wf.is_open()) throw Fail("Couldn't open timeWidth.tsv", FV_ERR_SYSTEM);
+                std::string wl;
+                while (std::getline(wf, wl)) wlines.push_back(wl);
+            }
+            long long lineNumber = 0;
+            for (const std::string& wl : wlines) {
+                lineNumber++;
+                if (lineNumber == 1) continue;
+                const size_t wt = wl.find('\t');
+                if (wt == std::string::npos) throw Fail("Could not find tab delimiter.");
+                const double tw = std::stod(wl.substr(0, wt));
+                if (tw == time) break;
+                if (tw > time) {
+                    lineNumber--;
+                    break;
+                }
+            }
+            noutsW = lineNumber - 1;
+            std::ofstream wn(d.path("result/timeWidth.tsv"));
+            if (!wn.is_open()) throw Fail("Couldn't open timeWidth.tsv", FV_ERR_SYSTEM);
+            for (long long q = 0; q < lineNumber; ++q) wn << wlines[q] << '\n';
+        }
         const std::string dir = d.path("fieldsOutput/output_" + number(point) + "/");
         for (int k = 0; k < N; ++k) prim[k] = column(dir + "sub_" + std::to_string(k + 1) + ".dat", nc, 1, 0);
         for (int q = 0; q < 3; ++q) prim[N + q] = column(dir + "velocity.dat", nc, 3, q);
@@ -744,12 +820,17 @@ int run(const Deck& d) {
         if ((st = fv_download(h, only.data())) != FV_OK) throw Fail(std::string("fv_download: ") + fv_last_error(h), st);
     }
 
-    if (fresh) writeOutput(d, h, nouts, time, th, sonic);
-    nouts++;
+    if (fresh) {
+        writeOutput(d, h, nouts, time, th, sonic);
+        if (d.width1D) writeWidth(d, h, time);
+    }
+    nouts++, noutsW++;
     if (d.readFrom == "initialisation") return 0;
 
     while (time < d.tEnd) {
-        const long long toGo = std::max(1LL, nouts * d.freq - nsteps);
+        long long next = nouts * d.freq;
+        if (d.width1D) next = std::min(next, noutsW * freqW);
+        const long long toGo = std::max(1LL, next - nsteps);
         fv_run_stats rs{};
         st = fv_run(h, d.tEnd, toGo, &rs);
         nsteps += rs.steps;
@@ -765,6 +846,10 @@ int run(const Deck& d) {
             std::cout << "Time = " << time << std::endl << "Step number = " << nsteps << std::endl;
             writeOutput(d, h, nouts, time, th, sonic);
             nouts++;
+        }
+        if (d.width1D && (nsteps == noutsW * freqW || time == d.tEnd)) {
+            writeWidth(d, h, time);
+            noutsW++;
         }
     }
     std::cout << "End" << std::endl;

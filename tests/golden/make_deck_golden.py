@@ -121,6 +121,21 @@ def deck_cases():
     c.t_end = _t_after(c, p, 6, 0.3)
     out.append(("kh16_zones_fresh", c, p, 3, False, [{}], 0.0,
                 {"zones": zones, "modifiers": {1: (1.0, 0.5, 0.5, 0.2)}}))
+    # 1D mixing-zone width (output::mixedZoneWidth1D): a fresh run, then a restart from output 2
+    # that appends to result/timeWidth.tsv
+    c, p = cases.shock_tube_1d(n=60)
+    c.t_end = _t_after(c, p, 9, 0.4)
+    out.append(("tube60_width", c, p, 3, False, [{}, {"start": "2", "t_end": repr(c.t_end * 1.5)}], 0.0,
+                {"mixing_width": True}))
+    # the same with a finite mixing zone: mole fraction 1 for x <= 0.4, 0.83 up to 0.6, 0 beyond
+    # (zones; the outer zone takes the means of the restart set below)
+    c, _ = cases.shock_tube_1d(n=60)
+    p = [np.zeros(60), np.full(60, 0.125), np.zeros(60), np.zeros(60), np.zeros(60), np.full(60, 0.1)]
+    zones = [("plane 1 0 0 point: 0.4 0 0", [1.0, 0.0], (0.0, 0.0, 0.0), 1.0),
+             ("plane 1 0 0 point: 0.6 0 0", [0.3, 0.06], (0.0, 0.0, 0.0), 0.5)]
+    c.t_end = 0.03
+    out.append(("tube60_zones_width", c, p, 4, False, [{}, {"start": "2", "t_end": "0.05"}], 0.0,
+                {"mixing_width": True, "zones": zones}))
     return out
 
 
