@@ -131,6 +131,14 @@ def golden_cases():
     c, p = cases.chlorine_dissociation_2d(4, eos="ideal")
     c.order = "ThirdOrder"
     out.append(("cl2_4x4_ideal_gs_rk3", c, p, 6, [1, 6]))
+    # 3D: the shear layer of the reacting benchmark (3 species, van der Waals) in a slip-walled
+    # 8^3 box without its reaction (the reference has no periodic patch and no A+B->2C), with the
+    # zero-slope limiter (fused march) and with the linear one (generic path)
+    for lim, tag in (("vanLeer", "vanleer"), ("linear", "linear")):
+        c, p = cases.reacting_shear_3d(n=8, precision="f64", periodic=False)
+        c.chemistry = "no"
+        c.limiter = lim
+        out.append((f"shear3d_8_vdw_{tag}", c, p, 6, [1, 6]))
     return out
 
 
