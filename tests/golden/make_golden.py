@@ -139,6 +139,11 @@ def golden_cases():
         c.chemistry = "no"
         c.limiter = lim
         out.append((f"shear3d_8_vdw_{tag}", c, p, 6, [1, 6]))
+    for order, tag in (("SecondOrderRK", "rk2"), ("ThirdOrderCada", "cada")):
+        c, p = cases.reacting_shear_3d(n=8, precision="f64", periodic=False)
+        c.chemistry = "no"
+        c.order = order
+        out.append((f"shear3d_8_vdw_{tag}", c, p, 4, [1, 4]))
     return out
 
 
