@@ -2,7 +2,7 @@
 
 FP64 mode is compiled without FMA contraction and follows the reference's operation order, so
 it is expected to reproduce the reference bit for bit; the bar written in the tests is the
-north-star tolerance, 1e-12 relative (L-inf over the field, relative to its max magnitude).
+stated FP64 tolerance, 1e-12 relative (L-inf over the field, relative to its max magnitude).
 """
 
 import numpy as np
