@@ -9,7 +9,8 @@ namespace {
 template <int N, int EOS, int D>
 cudaError_t launchT(const StepParams& P, const chem::ChemParams& C, double* U, DevClock* ck, double* blockMax,
                     int blocks, cudaStream_t st) {
-    chem::k_chemistry<N, EOS, D><<<blocks, 256, 0, st>>>(P, C, U, ck, blockMax);
+    if (C.conc) chem::k_chemistry<N, EOS, D, true><<<blocks, 256, 0, st>>>(P, C, U, ck, blockMax);
+    else chem::k_chemistry<N, EOS, D, false><<<blocks, 256, 0, st>>>(P, C, U, ck, blockMax);
     return cudaGetLastError();
 }
 

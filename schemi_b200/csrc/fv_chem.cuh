@@ -416,7 +416,9 @@ __device__ int integrate(const ChemParams& C, const MixParams& mx, double dt, do
 // Chemistry of every cell of U (in place) with the step's dt, then the CFL signal of the result.
 // The register budget is sized for two CTAs of 256 threads per SM (the FP64 arithmetic is
 // latency-bound; the spills this costs stay in L1).
-template <int N, int EOS, int D>
+// CONC: the state keeps its concentrations (C.conc, after a multi-stage average); a separate
+// instantiation so that the single-stage pass carries no extra registers.
+template <int N, int EOS, int D, bool CONC>
 __global__ void __launch_bounds__(256, 2) k_chemistry(const StepParams P, const ChemParams C, double* __restrict__ U,
                                                    DevClock* __restrict__ ck, double* __restrict__ blockMax) {
     __shared__ double red[32];
@@ -437,10 +439,12 @@ __global__ void __launch_bounds__(256, 2) k_chemistry(const StepParams P, const 
         // derived fields after the advection (Advection.cpp:455-479), or the concentrations the
         // multi-stage average left (bunchOfFields::average)
         Cell<N> q;
-        double cIn[N + 1];
-        if (C.conc) {
+        double cIn[CONC ? N + 1 : 1];
+        if constexpr (CONC) {
 #pragma unroll
             for (int k = 0; k <= N; ++k) q.c[k] = C.conc[k * st + i];
+#pragma unroll
+            for (int k = 0; k <= N; ++k) cIn[k] = q.c[k];
         } else {
             q.c[0] = 0;
 #pragma unroll
@@ -449,8 +453,6 @@ __global__ void __launch_bounds__(256, 2) k_chemistry(const StepParams P, const 
                 q.c[0] += q.c[k];
             }
         }
-#pragma unroll
-        for (int k = 0; k <= N; ++k) cIn[k] = q.c[k];
         double v[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) v[d] = m[d] / rho;
@@ -476,7 +478,7 @@ __global__ void __launch_bounds__(256, 2) k_chemistry(const StepParams P, const 
             }
             E = 0.5 * E + 0.5 * E1;
             U[(N + 4) * st + i] = E;
-            if (C.conc) {
+            if constexpr (CONC) {
 #pragma unroll
                 for (int k = 0; k <= N; ++k) {
                     cIn[k] = 0.5 * cIn[k] + 0.5 * q.c[k];
@@ -491,7 +493,7 @@ __global__ void __launch_bounds__(256, 2) k_chemistry(const StepParams P, const 
         ijk[2] = D >= 3 ? (int)(i / ((long long)P.n[0] * P.n[1])) : 0;
         const double ex = extent(P, 0, ijk[0]), ey = extent(P, 1, ijk[1]), ez = extent(P, 2, ijk[2]);
         const double minLS = 1.0 / smin(smin(ex, ey), ez);
-        if (C.conc) {
+        if constexpr (CONC) {
             // the state's own (averaged) concentrations, as main's CFL block reads them
             localMax = smax(localMax, cellSignalC<double, N, EOS, D>(P, cIn, rho, m, E, minLS));
         } else {
