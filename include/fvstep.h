@@ -258,12 +258,14 @@ long long fv_kernels_per_step(const fv_handle* h);
  *   dt                     step to take; dt_next receives main's CFL step of the new state
  *                          (unclamped); cfg->g is the gravity vector of this step
  *   stream                 cudaStream_t or NULL
- * Runs the full MUSCL-Hancock path (any limiter, 1D/2D/3D) on meshes of at most
- * FV_NOALLOC_MAX_CELLS cells; larger meshes, cases with chemistry and SecondOrderRK are rejected with FV_ERR_INIT.  The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress) and should come before any
- * stream capture.  Every call rewrites each part of the array it reads, so no state carries over
- * between calls; calls that overlap on the GPU share the array and race.  Synchronises `stream`
- * before returning. */
+ * Runs the full MUSCL-Hancock path of the SecondOrder step solver (any limiter, 1D/2D/3D, both
+ * precisions) on meshes of at most FV_NOALLOC_MAX_CELLS cells.  Rejected with FV_ERR_INIT: every
+ * configuration fv_create rejects, larger meshes, cases with chemistry, the SecondOrderRK,
+ * ThirdOrder and ThirdOrderCada step solvers, and state_in / state_out arrays that overlap.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress); make
+ * that first call before any stream capture.  Every call rewrites each part of the array it
+ * reads, so no state carries over between calls; calls that overlap on the GPU share the array
+ * and race.  Synchronises `stream` before returning. */
 #define FV_NOALLOC_MAX_CELLS 1024
 #define FV_NOALLOC_SCRATCH_BYTES 2621440
 fv_status fv_step_noalloc(const fv_config* cfg, const double* state_in, double* state_out, double dt,

@@ -17,6 +17,8 @@ Backward: fv_adjoint sweeps the trajectory backwards (recomputing between checkp
 hand-written adjoint kernels and returns dJtot/dU^0; the restart-set-to-conserved conversion
 (phaseInitialization.cpp:1827-1885 for an ideal mixture) is differentiated here in torch.
 The step sizes are frozen at their recorded values (the CFL reduction is not differentiated).
+A handle holds one trajectory: a second forward on the same FVCase replaces it, and the first
+forward's backward then raises instead of sweeping the wrong trajectory.
 """
 
 from __future__ import annotations
@@ -61,6 +63,7 @@ class TimeLoop(torch.autograd.Function):
         UT = torch.empty((g.n_conserved, g.n_cells), dtype=torch.float64, device=prim.device)
         g.state_copy(UT.data_ptr())
         ctx.g = g
+        ctx.record_id = g.records
         ctx.record_stats = st
         ctx.save_for_backward(prim)
         J = torch.tensor(st.objective, dtype=torch.float64, device=prim.device)
@@ -70,6 +73,12 @@ class TimeLoop(torch.autograd.Function):
     def backward(ctx, gJ: Optional[torch.Tensor], gUT: Optional[torch.Tensor]):
         (prim,) = ctx.saved_tensors
         g = ctx.g
+        if g.records != ctx.record_id:
+            # fv_record keeps one trajectory per handle; sweeping a later one would return the
+            # gradient of another forward without any error
+            raise RuntimeError("the handle's trajectory was recorded again by a later TimeLoop.apply "
+                               "before this backward; use one FVCase per forward that is still to be "
+                               "differentiated")
         lam0 = torch.empty((g.n_conserved, g.n_cells), dtype=torch.float64, device=prim.device)
         gain = float(gJ) if gJ is not None else 0.0
         gUT_ptr = None

@@ -18,9 +18,11 @@
 #include <cstring>
 #include <limits>
 #include <mutex>
+#include <string>
 
 #include "../../include/fvstep.h"
 #include "fv_launch.cuh"
+#include "fv_validate.h"
 
 using namespace fv;
 
@@ -128,19 +130,19 @@ __global__ void k_clock(DevClock* ck, double dt, double g0, double g1, double g2
     *ck = c;
 }
 
-bool buildParams(const fv_config& c, StepParams& P) {
-    if (c.dims < 1 || c.dims > 3 || c.n_species < 1 || c.n_species > FV_MAX_SPECIES) return false;
-    if (c.eos != FV_EOS_IDEAL && c.eos != FV_EOS_VAN_DER_WAALS) return false;
-    if (c.flux != FV_FLUX_HLLC && c.flux != FV_FLUX_HLL) return false;
-    if (c.limiter < 0 || c.limiter > FV_LIM_SCHMIDTMANN) return false;
-    if (c.precision != FV_PREC_F64 && c.precision != FV_PREC_F32_FLUX) return false;
-    if (c.order != FV_ORDER_SECOND) return false;  // one MUSCL-Hancock stage only
+// Step parameters of a configuration fv_create accepts (checked by fvValidateConfig first) and
+// that this entry point runs: the SecondOrder step solver, one MUSCL-Hancock stage.
+bool buildParams(const fv_config& c, StepParams& P, std::string& e) {
+    if (!fvValidateConfig(c, e)) return false;
+    if (c.order != FV_ORDER_SECOND) {
+        e = "only the SecondOrder step solver (one MUSCL-Hancock stage) runs without allocation";
+        return false;
+    }
     memset(&P, 0, sizeof(P));
     P.hancock = 1;
     P.dims = c.dims;
     for (int a = 0; a < 3; ++a) {
         P.n[a] = a < c.dims ? c.n[a] : 1;
-        if (P.n[a] < 1 || !(c.L[a] > 0)) return false;
         P.ext[a] = c.L[a];
     }
     P.periodic[0] = c.bc_vel[FV_PATCH_TAIL] == FV_BC_PERIODIC;
@@ -201,14 +203,25 @@ extern "C" fv_status fv_step_noalloc(const fv_config* cfg, const double* state_i
         return FV_ERR_INIT;
     }
     StepParams P;
-    if (!buildParams(*cfg, P)) {
-        fprintf(stderr, "fv_step_noalloc: invalid configuration\n");
+    std::string why;
+    if (!buildParams(*cfg, P, why)) {
+        fprintf(stderr, "fv_step_noalloc: invalid configuration: %s\n", why.c_str());
         return FV_ERR_INIT;
     }
     if (P.ncell > kMaxCells) {
         fprintf(stderr, "fv_step_noalloc: %lld cells exceed the maximum of %lld cells of the static scratch\n",
                 P.ncell, kMaxCells);
         return FV_ERR_INIT;
+    }
+    {
+        // the step reads every cell of state_in while it writes state_out: the two must not overlap
+        const size_t bytes = (size_t)(cfg->n_species + 5) * (size_t)P.ncell * sizeof(double);
+        const char* a = reinterpret_cast<const char*>(state_in);
+        const char* b = reinterpret_cast<const char*>(state_out);
+        if (a < b + bytes && b < a + bytes) {
+            fprintf(stderr, "fv_step_noalloc: state_in and state_out overlap; pass two separate arrays\n");
+            return FV_ERR_INIT;
+        }
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     unsigned char* scratch = nullptr;

@@ -271,6 +271,9 @@ class FVCase:
         mixing-width objective J = sum_n dt_{n-1} W(U^n) in ``.objective``."""
         rc = fv_record_config_t(checkpoint_every, objective, heavy_species, 0)
         s = fv_record_stats_t()
+        # the handle keeps one trajectory: count the recordings so that a caller holding an older
+        # one (TimeLoop's backward) can tell it has been replaced
+        self.records = getattr(self, "records", 0) + 1
         self._check(self.lib.fv_record(self._h, ctypes.byref(rc), t_end, max_steps, ctypes.byref(s)))
         return s
 

@@ -50,27 +50,43 @@ struct Fail : std::runtime_error {
     Fail(const std::string& m, int c = FV_ERR_INIT) : std::runtime_error(m), code(c) {}
 };
 
-// whitespace tokens of a file, read like the reference's operator>> chains
+// A file read by the same stream extractions as the reference's operator>> chains: a string is
+// the next whitespace-delimited word, a number the longest prefix that parses as a double and no
+// more, so "0;" yields 0 and leaves ";" for the next word (zone.cpp:64-65 reads the shipped
+// "1 0 0; 0.5 0.5 0.5" plane this way).
 struct Tokens {
-    std::vector<std::string> t;
-    size_t i = 0;
+    std::istringstream in;
     Tokens(const std::string& path) {
         std::ifstream f(path);
         if (!f.is_open()) throw Fail(path + " not found.", FV_ERR_SYSTEM);
-        std::string w;
-        while (f >> w) t.push_back(w);
+        std::ostringstream all;
+        all << f.rdbuf();
+        in.str(all.str());
     }
-    const std::string& next(const std::string& what) {
-        if (i >= t.size()) throw Fail("unexpected end of file while reading " + what);
-        return t[i++];
+    std::string next(const std::string& what) {
+        std::string w;
+        if (!(in >> w)) throw Fail("unexpected end of file while reading " + what);
+        return w;
     }
     void skip() { next("a label"); }
     double num(const std::string& what) {
-        const std::string& s = next(what);
+        double v;
+        if (!(in >> v)) {
+            in.clear();
+            std::string w;
+            in >> w;
+            throw Fail("not a number for " + what + ": " + (w.empty() ? "end of file" : w));
+        }
+        return v;
+    }
+    // a value the reference reads as a word and converts with std::stod (the species' constants
+    // and the values in zones, phaseInitialization.cpp:272-279,357-359)
+    double word(const std::string& what) {
+        const std::string w = next(what);
         try {
-            return std::stod(s);
+            return std::stod(w);
         } catch (...) {
-            throw Fail("not a number for " + what + ": " + s);
+            throw Fail("not a number for " + what + ": " + w);
         }
     }
 };
@@ -202,7 +218,10 @@ int bcType(const std::string& s) {
     if (s == "slip") return FV_BC_SLIP;
     if (s == "fixedValueCell") return FV_BC_FIXED_CELL;
     if (s == "fixedValueSurface") return FV_BC_FIXED_SURFACE;
-    throw Fail("unknown boundary condition type " + s);
+    // boundaryConditionFromString.cpp:12-32
+    if (s == "innerSurface") throw Fail("<<innerSurface>> can not be boundary surface type.");
+    if (s == "subPatches") throw Fail("subPatches: patches split into sub-patches are not part of this step");
+    throw Fail("Unknown type of boundary condition");
 }
 
 int limiterIndex(const std::string& s) {
@@ -230,15 +249,25 @@ struct Deck {
     std::string path(const std::string& rel) const { return dir + "/" + rel; }
 };
 
-// sub_k / velocity / pressure: six patch conditions, then the values of every zone.
+// sub_k / velocity / pressure: six patch conditions, then the values of every zone.  Only
+// fixedValueCell carries values in the deck (phaseInitialization.cpp:290-299,477-487); they are
+// stream extractions, and when one is not a number the reference's stream fails, the next
+// patch's condition reads as empty ("Unknown type of boundary condition") or, after the last
+// patch, the values label is missed ("Wrong position in file.").
 void readPatches(Tokens& t, int nval, int field, int k, fv_config& c) {
     for (int patch = 0; patch < 6; ++patch) {
         t.skip();  // #<Patch>_boundary_condition
         const std::string type = t.next("boundary condition");
         const int bt = bcType(type);
         double v[3] = {0, 0, 0};
-        if (bt == FV_BC_FIXED_CELL || bt == FV_BC_FIXED_SURFACE)
-            for (int q = 0; q < nval; ++q) v[q] = t.num("boundary value");
+        if (bt == FV_BC_FIXED_CELL)
+            for (int q = 0; q < nval; ++q) {
+                try {
+                    v[q] = t.num("boundary value");
+                } catch (const Fail&) {
+                    throw Fail(patch < 5 ? "Unknown type of boundary condition" : "Wrong position in file.");
+                }
+            }
         if (field == 0) {
             c.bc_conc[patch][k] = bt;
             c.bc_conc_value[patch][k] = v[0];
@@ -252,7 +281,7 @@ void readPatches(Tokens& t, int nval, int field, int k, fv_config& c) {
     }
 }
 
-Deck readDeck(const std::string& dir) {
+Deck readDeck(const std::string& dir, bool createResult) {
     Deck d;
     d.dir = dir;
     fv_config& c = d.cfg;
@@ -338,31 +367,37 @@ Deck readDeck(const std::string& dir) {
     }
     c.precision = FV_PREC_F64;
     if (c.n_species < 1 || c.n_species > FV_MAX_SPECIES) throw Fail("number of components must be 1..4");
+    // Schemi.cpp:312-330: a fresh run recreates result/Time.tsv once main.txt is read, before the
+    // zones and the species' files (so a deck refused there still leaves it behind)
+    if (createResult && (d.readFrom == "no" || d.readFrom == "initialisation")) {
+        std::filesystem::create_directories(d.path("result"));
+        std::ofstream(d.path("result/Time.tsv")).close();
+    }
     d.zones = readZones(d.path("set/zonesDescription.txt"));
     const size_t nzv = d.zones.size();
     for (int k = 0; k < c.n_species; ++k) {
         Tokens t(d.path("set/sub_" + std::to_string(k + 1) + ".txt"));
-        t.skip(); c.M[k] = t.num("molar mass");
-        t.skip(); c.Cv[k] = t.num("Cv");
-        t.skip(); c.Tc[k] = t.num("Tc");
-        t.skip(); c.Pc[k] = t.num("Pc");
+        t.skip(); c.M[k] = t.word("molar mass");
+        t.skip(); c.Cv[k] = t.word("Cv");
+        t.skip(); c.Tc[k] = t.word("Tc");
+        t.skip(); c.Pc[k] = t.word("Pc");
         for (int q = 0; q < 3; ++q) { t.skip(); t.next("transport parameter"); }
         readPatches(t, 1, 0, k, c);
         if (t.next("values label") != "#Values_in_zones") throw Fail("Wrong position in file.");
         d.zoneC.emplace_back();
-        for (size_t z = 0; z < nzv; ++z) d.zoneC[k].push_back(t.num("zone concentration"));
+        for (size_t z = 0; z < nzv; ++z) d.zoneC[k].push_back(t.word("zone concentration"));
     }
     {
         Tokens t(d.path("set/velocity.txt"));
         readPatches(t, 3, 1, 0, c);
         if (t.next("values label") != "#Values_in_zones") throw Fail("Wrong position in file.");
-        for (size_t z = 0; z < 3 * nzv; ++z) d.zoneV.push_back(t.num("zone velocity"));
+        for (size_t z = 0; z < 3 * nzv; ++z) d.zoneV.push_back(t.word("zone velocity"));
     }
     {
         Tokens t(d.path("set/pressure.txt"));
         readPatches(t, 1, 2, 0, c);
         if (t.next("values label") != "#Values_in_zones") throw Fail("Wrong position in file.");
-        for (size_t z = 0; z < nzv; ++z) d.zoneP.push_back(t.num("zone pressure"));
+        for (size_t z = 0; z < nzv; ++z) d.zoneP.push_back(t.word("zone pressure"));
     }
     // chemistry
     {
@@ -839,7 +874,7 @@ int run(const Deck& d) {
             std::clog << fv_last_error(h) << std::endl << "Step number " << nsteps << '.' << std::endl;
             std::clog << "Emergency output." << std::endl;
             writeOutput(d, h, nouts, time, th, sonic);
-            return st;
+            return EXIT_FAILURE;  // Schemi.cpp:774-799
         }
         if (rs.steps == 0) break;
         if (nsteps == nouts * d.freq || time == d.tEnd) {
@@ -882,17 +917,15 @@ int main(int argc, char** argv) {
         } else dir = a;
     }
     try {
-        const Deck d = readDeck(dir);
+        const Deck d = readDeck(dir, !printOnly);
         if (printOnly) {
             printConfig(d.cfg, d);
             return 0;
         }
         return run(d);
-    } catch (const Fail& e) {
-        std::clog << e.what() << std::endl;
-        return e.code ? e.code : 1;
     } catch (const std::exception& e) {
+        // Schemi.cpp:965-973: every error ends the run with its message and EXIT_FAILURE
         std::clog << e.what() << std::endl;
-        return FV_ERR_SYSTEM;
+        return EXIT_FAILURE;
     }
 }

@@ -7,7 +7,8 @@ made in that directory and every file the reference left behind (``golden/make_d
 "Time of ..." label: the run's and each stage's wall time).  Fixtures with a
 non-zero ``tolerance`` (the chemistry deck) are compared value by value to that relative
 tolerance, velocities and momenta on the scale of the largest sonic speed (and density); all
-others byte for byte.
+others byte for byte.  A run the reference refused must end with the same exit code and with
+the message the reference printed.
 """
 
 import os
@@ -116,6 +117,12 @@ def replay(driver, name, d, timeout=600):
             problems.append(f"run {r}: exit {res.returncode}, reference {int(z['rc'][r])}\n"
                             + res.stdout[-1500:] + res.stderr[-1500:])
             return problems
+        if res.returncode != 0 and "log_tails" in z.files:
+            # a refused deck: the driver's message is the one the reference printed
+            said = [x for x in res.stderr.strip().split("\n") if x.strip()]
+            if not said or said[-1].strip() not in str(z["log_tails"][r]):
+                problems.append(f"run {r}: message {said[-1:]!r} not in the reference's output "
+                                f"{str(z['log_tails'][r])[-300:]!r}")
     want = {k[4:].replace("|", os.sep): z[k].tobytes() for k in z.files if k.startswith("out:")}
     got = _tree(d)
     if sorted(got) != sorted(want):

@@ -139,6 +139,23 @@ def deck_cases():
     return out
 
 
+# Task decks shipped with the reference (its tests/TestsTasks directory) whose every stage is in
+# this step: 1D, HLLC, the vanAlbada limiter, ideal gas, diffusion and turbulence off.  Their set/
+# directories are stored unchanged.  Noh_CGS is refused by the reference itself (a parenthesised
+# fixed velocity that its stream reader cannot parse): exit code 1, "Unknown type of boundary
+# condition", and only the empty result/Time.tsv left behind.
+SHIPPED = [
+    ("sod_cgs_1000", "Sod_CGS/Sod_CGS_1000"),
+    ("blastwaves_cgs_3000", "BlastWaves/BlastWaves_CGS_3000"),
+    ("gaussconcentration_cgs_1000", "GaussConcentration_CGS/GaussConcentration_CGS_1000"),
+    ("noh_1_1000", "Noh_1/Noh_1_1000"),
+    ("noh_2_1000", "Noh_2/Noh_2_1000"),
+    ("rarefactions_100_cgs", "Rarefactions_CGS/Rarefactions_100_CGS"),
+    ("noh_cgs_1000", "Noh_CGS/Noh_CGS_1000"),
+]
+SHIPPED_ROOT = "/root/reference/tests/TestsTasks"
+
+
 def _files(d):
     found = {}
     for root, _, names in os.walk(d):
@@ -152,10 +169,46 @@ def _key(prefix, rel):
     return prefix + ":" + rel.replace(os.sep, "|")
 
 
+def _save(name, d, inputs, runs_main, rcs, tol, logs):
+    data = {_key("in", rel): np.frombuffer(b, dtype=np.uint8) for rel, b in inputs.items()}
+    for r, main_txt in enumerate(runs_main):
+        data[f"run{r}:main.txt"] = np.frombuffer(main_txt.encode(), dtype=np.uint8)
+    for rel, b in _files(d).items():
+        if rel.startswith("set" + os.sep):
+            continue
+        data[_key("out", rel)] = np.frombuffer(b, dtype=np.uint8)
+    data["runs"] = np.int64(len(runs_main))
+    data["rc"] = np.asarray(rcs, dtype=np.int64)
+    data["tolerance"] = np.float64(tol)
+    # the end of what the reference printed (a failed run's error message is among its last lines)
+    data["log_tails"] = np.asarray([lg[-600:] for lg in logs])
+    np.savez_compressed(os.path.join(HERE, f"deck_{name}.npz"), **data)
+    outs = sorted(k for k in data if k.startswith("out:result|output_"))
+    print(f"deck_{name}: {len(runs_main)} run(s), exit {rcs}, outputs {[k.split('_')[-1] for k in outs]}")
+
+
+def shipped(binary, only=None):
+    """Fixtures of the reference's own task decks, their set/ directories unchanged."""
+    for name, rel in SHIPPED:
+        if only and name not in only:
+            continue
+        d = tempfile.mkdtemp(prefix="schemi_deck_")
+        try:
+            shutil.copytree(os.path.join(SHIPPED_ROOT, rel, "set"), os.path.join(d, "set"))
+            inputs = _files(d)
+            main_txt = inputs[os.path.join("set", "main.txt")].decode()
+            res = subprocess.run([binary], cwd=d, stdin=subprocess.DEVNULL, stdout=subprocess.PIPE,
+                                 stderr=subprocess.STDOUT, timeout=1800)
+            _save(name, d, inputs, [main_txt], [res.returncode], 0.0, [res.stdout.decode(errors="replace")])
+        finally:
+            shutil.rmtree(d, ignore_errors=True)
+
+
 def main(only=None):
     binary = O.REF_BIN_PATCHED
     if not os.path.exists(binary):
         raise SystemExit(f"{binary} missing: run make -C oracle ref")
+    shipped(binary, only)
     for name, case, prim, freq, restart, runs, tol, *extra in deck_cases():
         if only and name not in only:
             continue

@@ -62,6 +62,14 @@ def golden_cases():
     c, p = cases.shock_tube_1d(n=200)
     c.flux, c.limiter = "HLL", "superbee"
     out.append(("tube_hll_superbee_200", c, p, 30, [30]))
+    # every limiter whose phi acts in 1D MUSCL-Hancock (r > 0 happens only in 1D), on the 200-cell
+    # two-species tube; minmod and superbee are pinned above, UTCDFS and the unlimited linear
+    # reconstruction end in the reference's Riemann failure (step 2 and step 4)
+    for lim in ("vanAlbada", "vanAlbada2", "vanLeer", "vanLeer2", "minmod2", "HQUICK", "Koren", "Koren2",
+                "Sweby", "Schmidtmann"):
+        c, p = cases.shock_tube_1d(n=200)
+        c.limiter = lim
+        out.append((f"tube_{lim.lower()}_200", c, p, 40, [1, 2, 40]))
     # Cl2 <-> 2Cl chemistry (the ClorumTest mechanism and solver, hot mixture)
     c, p = cases.chlorine_dissociation_2d(4)
     out.append(("cl2_4x4_vdw_gs", c, p, 10, [1, 2, 10]))

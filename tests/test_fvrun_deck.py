@@ -125,7 +125,8 @@ def test_missing_deck_file(tmp_path):
 
 
 def test_deck_fixtures_parse(tmp_path):
-    """Every committed deck fixture parses (its inputs written out, then --print-config)."""
+    """Every committed deck fixture parses (its inputs written out, then --print-config), except
+    the reference's refused deck, which fails to parse with the reference's message."""
     names = fixtures()
     assert len(names) >= 6
     for name in names:
@@ -135,7 +136,24 @@ def test_deck_fixtures_parse(tmp_path):
         for r in range(int(z["runs"])):
             (d / "set" / "main.txt").write_bytes(z[f"run{r}:main.txt"].tobytes())
             res = _print_config(str(d))
-            assert res.returncode == 0, (name, res.stderr)
+            if int(z["rc"][r]) == 0:
+                assert res.returncode == 0, (name, res.stderr)
+            else:
+                assert res.returncode != 0, name
+                assert res.stderr.strip().split("\n")[-1] in str(z["log_tails"][r]), (name, res.stderr)
+
+
+SHIPPED = ["sod_cgs_1000", "blastwaves_cgs_3000", "gaussconcentration_cgs_1000", "noh_1_1000", "noh_2_1000",
+           "rarefactions_100_cgs", "noh_cgs_1000"]
+
+
+def test_shipped_decks_are_fixtures():
+    """The reference's own in-scope task decks (1D, HLLC, vanAlbada, ideal gas, no diffusion or
+    turbulence) are among the replayed fixtures, and its refused Noh_CGS deck with them."""
+    assert set(SHIPPED) <= set(fixtures())
+    z = load("noh_cgs_1000")
+    assert int(z["rc"][0]) == 1
+    assert "Unknown type of boundary condition" in str(z["log_tails"][0])
 
 
 ORACLE_DRIVER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "lib",

@@ -241,3 +241,22 @@ def test_adjoint_rejects_unsupported_cases(torch_cuda):
     g2 = fv.FVCase(_rt())
     with pytest.raises(fv.FVError):
         g2.replay()  # nothing recorded
+
+
+def test_second_forward_on_the_handle_invalidates_the_first_backward(torch_cuda):
+    """A handle keeps one recorded trajectory: after a second forward on the same FVCase, the
+    first forward's backward raises instead of returning the gradient of the second."""
+    torch = torch_cuda
+    from schemi_b200 import adjoint, fv
+
+    case = _rt()
+    g = fv.FVCase(case)
+    a = _amplitudes(torch).cuda()
+    a1 = a.clone().requires_grad_(True)
+    J1, _ = adjoint.TimeLoop.apply(adjoint.rayleigh_taylor_primitive(a1, NX, NY), g, T_END, 10, 0)
+    a2 = (2 * a).clone().requires_grad_(True)
+    J2, _ = adjoint.TimeLoop.apply(adjoint.rayleigh_taylor_primitive(a2, NX, NY), g, T_END, 10, 0)
+    with pytest.raises(RuntimeError, match="recorded again"):
+        J1.backward()
+    J2.backward()  # the latest forward still differentiates
+    assert a2.grad is not None and torch.isfinite(a2.grad).all()

@@ -205,14 +205,18 @@ def test_gpu_fp32_flux_march_cases(fv, oracle_mod, name, case, prim):
     print(f"{name}: max rel L1 vs oracle = {worst:.3e}")
 
 
-def test_gpu_riemann_failure_status(fv):
+@pytest.mark.parametrize("limiter,fails_at", [("UTCDFS", 2), ("linear", 4)])
+def test_gpu_riemann_failure_status(fv, limiter, fails_at):
+    """The reference's Riemann failures on the 200-cell tube (UTCDFS at step 2, the unlimited
+    linear reconstruction at step 4) end the same step on the GPU with RiemannSolverError."""
     from schemi_b200 import cases
 
     c, p = cases.shock_tube_1d(n=200)
-    c.limiter = "UTCDFS"
+    c.limiter = limiter
     g = fv.FVCase(c)
     g.upload(p)
-    g.step()
+    for _ in range(fails_at - 1):
+        g.step()
     with pytest.raises(fv.FVError) as ei:
         g.step()
     assert ei.value.status == 1

@@ -38,16 +38,19 @@ def test_oracle_matches_reference(oracle_mod, name, case, prim, data):
     assert done == int(data["n_steps"]) or "full" not in name
 
 
-def test_oracle_riemann_failure_matches_reference(oracle_mod):
-    """UTCDFS on the 200-cell tube makes the HLLC wave speeds NaN at step 2 in the reference
-    (it prints "Fatal error in Riemann solver." and exits); the oracle reports RiemannSolverError."""
+@pytest.mark.parametrize("limiter,fails_at", [("UTCDFS", 2), ("linear", 4)])
+def test_oracle_riemann_failure_matches_reference(oracle_mod, limiter, fails_at):
+    """On the 200-cell tube UTCDFS makes the HLLC wave speeds NaN at step 2 in the reference, and
+    the unlimited linear reconstruction at step 4 (it prints "Fatal error in Riemann solver." and
+    exits); the oracle reports RiemannSolverError at the same step."""
     from schemi_b200 import cases
 
     c, p = cases.shock_tube_1d(n=200)
-    c.limiter = "UTCDFS"
+    c.limiter = limiter
     oc = oracle_mod.OracleCase(c)
     oc.upload(p)
-    oc.step()
+    for _ in range(fails_at - 1):
+        oc.step()
     with pytest.raises(RuntimeError, match="status 1"):
         oc.step()
 
