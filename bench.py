@@ -17,9 +17,18 @@ e2e       the same metric through the C-ABI with host buffers: fv_upload of the 
 roofline  algorithmic bytes per cell-update = 2 * 8 * (N + 1 + D + 1) (conserved FP64 state read
           once and written once; N species densities, mixture density, D momenta, energy)
           over the measured HBM copy bandwidth of this pool (MEASURED_PEAKS.json).
-cpu_baseline / --impl reference: the reference solver compiled from its own sources
-          (oracle/_ref/schemi, as shipped) on the same KH workload at 128 x 128 cells (slip in x:
-          the reference has no periodic patch), steps timed by differencing two runs.
+cpu_baseline / --impl reference: the reference solver compiled from its own sources, with the
+          per-face assignment at HancockStage.cpp:308,313,318 (oracle/_ref/schemi_patched,
+          output byte-identical) as the value and the build as shipped (oracle/_ref/schemi)
+          beside it, on the same KH workload at 128 x 128 cells (slip in x: the reference has no
+          periodic patch), steps timed by differencing two runs.
+accuracy  every section states its relative L1 / L-inf error against the FP64 oracle on the
+          same inputs: KH 1024^2 after 3 steps (FP64 and FP32 flux), 16 sampled ensemble cases
+          (the smallest, the largest and seeded others) after their ensemble steps, the reacting
+          layer at 64^3 after 3 steps, the adjoint against the FP64 tangent oracle on 16 x 48;
+          the oracle runs in spawned worker processes after the timed sections.
+shock_tube_1d  config 1: the 1000-cell two-component tube to t = 0.2 through fv_run, us per step
+          and the final fields against the reference's own output (tests/golden).
 
 batched   512 Richtmyer-Meshkov cases of seeded sizes 128^2..512^2 (FP32 flux) advanced by the
           persistent ensemble kernel, against the same cases one after the other.
@@ -133,6 +142,73 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# ----------------------------------------------------------------------------- accuracy
+# Every GPU result states its relative L1 and L-inf error against the FP64 oracle (the CPU
+# restatement of the reference step, pinned bit for bit to the reference's outputs) on the same
+# inputs.  Groups of conserved fields: each species density, the mixture density, the momentum
+# vector (component errors summed over the components, on the scale of the vector's magnitude)
+# and the total energy.
+def conserved_errors(got: dict, want: dict, n_species: int) -> dict:
+    import numpy as np
+
+    groups = {f"rho{k + 1}": [f"rho{k + 1}"] for k in range(n_species)}
+    groups["rho"] = ["rho"]
+    groups["m"] = [f for f in ("mx", "my", "mz") if f in want and np.any(want[f])]
+    groups["E"] = ["E"]
+    out = {}
+    for name, fields in groups.items():
+        if not fields:
+            continue
+        diff = sum(np.abs(np.asarray(got[f]) - np.asarray(want[f])) for f in fields)
+        mag = sum(np.abs(np.asarray(want[f])) for f in fields)
+        out[name] = {"l1": float(diff.sum() / max(mag.sum(), 1e-300)),
+                     "linf": float(diff.max() / max(mag.max(), 1e-300))}
+    return {"l1": max(v["l1"] for v in out.values()), "linf": max(v["linf"] for v in out.values()),
+            "fields": out}
+
+
+def _oracle_state(case, prim, steps: int) -> dict:
+    """Conserved fields of the FP64 oracle after `steps` steps from the restart set `prim`."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    oc = oracle.OracleCase(case)
+    oc.upload(prim)
+    for _ in range(steps):
+        oc.step()
+    d = oc.download()
+    keep = [f"rho{k + 1}" for k in range(case.n_species)] + ["rho", "mx", "my", "mz", "E"]
+    return {k: d[k] for k in keep}
+
+
+def oracle_job(kind: str, arg: int, steps: int) -> dict:
+    """One oracle run in a worker process (started with spawn before any CUDA call)."""
+    from schemi_b200 import cases
+
+    if kind == "kh":
+        case, prim = cases.kelvin_helmholtz_2d(n=arg)
+    elif kind == "rm":
+        case, prim, _ = cases.richtmyer_meshkov(arg, precision="f64")
+    elif kind == "reacting":
+        case, prim = cases.reacting_shear_3d(n=arg, precision="f64")
+    else:
+        raise ValueError(kind)
+    return _oracle_state(case, prim, steps)
+
+
+def oracle_pool(workers: int):
+    import concurrent.futures as cf
+    import multiprocessing as mp
+
+    return cf.ProcessPoolExecutor(max_workers=max(1, workers), mp_context=mp.get_context("spawn"))
+
+
+def gpu_conserved(g) -> dict:
+    d = g.download()
+    keep = [f"rho{k + 1}" for k in range(g.case.n_species)] + ["rho", "mx", "my", "mz", "E"]
+    return {k: d[k] for k in keep}
+
+
 # ----------------------------------------------------------------------------- reference / CPU
 def _reference_run(binary, case, prim, steps_target, workdir):
     """Run the reference binary to the time reached after `steps_target` steps; return wall s."""
@@ -149,15 +225,17 @@ def _reference_run(binary, case, prim, steps_target, workdir):
     return wall
 
 
-def reference_throughput(n: int = 128, steps: int = 20, steps0: int = 2, processes: int = 1):
-    """Cell-updates/s of the as-shipped reference on KH n x n (slip x), by differencing a run of
+def reference_throughput(n: int = 128, steps: int = 20, steps0: int = 2, processes: int = 1, patched: bool = True):
+    """Cell-updates/s of the reference solver on KH n x n (slip x), by differencing a run of
     `steps` and a run of `steps0` steps (cancels start-up and file I/O); `processes` copies run
-    concurrently and the aggregate rate is reported."""
+    concurrently and the aggregate rate is reported.  patched: the build with the per-face
+    assignment at HancockStage.cpp:308,313,318 (oracle/_ref/schemi_patched, byte-identical
+    output, without the O(faces^2) cost); else the build as shipped (oracle/_ref/schemi)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     from schemi_b200 import cases
 
-    binary = oracle.REF_BIN
+    binary = oracle.REF_BIN_PATCHED if patched else oracle.REF_BIN
     if not os.path.exists(binary):
         raise FileNotFoundError(binary)
     case, prim = cases.kelvin_helmholtz_2d(n=n, periodic=False)
@@ -197,13 +275,15 @@ def run_reference_arm(args):
     procs = max(1, min(cores, 64))
     metric = "cell-updates/s per FV step"
     try:
-        v, info = reference_throughput(n=128, steps=12, steps0=2, processes=procs)
-    except Exception as e:  # the binary is built here from the reference sources
+        v, info = reference_throughput(n=128, steps=12, steps0=2, processes=procs, patched=True)
+        v_shipped, info_s = reference_throughput(n=128, steps=12, steps0=2, processes=procs, patched=False)
+    except Exception as e:  # the binaries are built here from the reference sources
         print(json.dumps({"impl": "reference", "unavailable": f"reference binary could not run: {e}"}))
         return 0
-    sample = (f"{procs} concurrent processes of the as-shipped reference binary (oracle/_ref/schemi), each the KH "
-              f"mixing layer at {info['n']}x{info['n']} with slip x, {info['steps']} steps timed by differencing "
-              f"runs of 12 and 2 steps")
+    sample = (f"{procs} concurrent processes of the reference binary with the per-face assignment at "
+              f"HancockStage.cpp:308,313,318 (oracle/_ref/schemi_patched; output byte-identical to the build as "
+              f"shipped), each the KH mixing layer at {info['n']}x{info['n']} with slip x (the reference has no "
+              f"periodic patch), {info['steps']} steps timed by differencing runs of 12 and 2 steps")
     line = {
         "impl": "reference", "metric": metric, "value": v, "unit": "cell-updates/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
@@ -212,6 +292,12 @@ def run_reference_arm(args):
                    "flux": "HLLC", "limiter": "vanLeer", "species": 2},
         "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": procs, "kind": "reference",
                          "sample": sample},
+        "as_shipped": {"value": v_shipped, "unit": "cell-updates/s", "cores": procs,
+                       "sample": "the same with the reference binary as shipped (oracle/_ref/schemi), whose "
+                                 "per-step cost grows with the square of the face count"},
+        "same_config": False,
+        "config_note": "KH 128x128 sample with slip x: the reference cannot express the periodic x patch of the "
+                       "1024x1024 workload; rates are per cell-update",
         "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -280,12 +366,48 @@ def e2e_run(g, prim_pinned, out_pinned, steps):
     return wall, st, h2d, d2h
 
 
-def batched_vs_plain(n_cases: int, steps: int, torch, rank: int = 0, world: int = 1, dist=None):
+BATCH_WARMUP_STEPS = 16
+
+
+def batch_accuracy_sample(n_cases: int, count: int = 16):
+    """Cases of the ensemble checked against the oracle: the smallest, the largest and seeded
+    others (up to `count`)."""
+    import numpy as np
+
+    from schemi_b200 import cases
+
+    sizes = [cases.richtmyer_meshkov_draws(i)[0] for i in range(n_cases)]
+    pick = [int(np.argmin(sizes)), int(np.argmax(sizes))]
+    rng = np.random.default_rng(4242)
+    for i in rng.permutation(n_cases):
+        if len(pick) >= min(count, n_cases):
+            break
+        if int(i) not in pick:
+            pick.append(int(i))
+    return sorted(pick)
+
+
+def batch_accuracy(kept: dict, fut: dict, steps: int) -> dict:
+    """Relative errors of the sampled ensemble cases against the oracle's states."""
+    worst = {"l1": 0.0, "linf": 0.0}
+    per_case = {}
+    for i, k in sorted(kept.items()):
+        e = conserved_errors(k["state"], fut[("rm", i)].result(), k["n_species"])
+        per_case[str(i)] = {"cells": k["cells"], "l1": e["l1"], "linf": e["linf"]}
+        worst = {q: max(worst[q], e[q]) for q in worst}
+    return {"against": f"FP64 oracle, same restart sets, same step count ({BATCH_WARMUP_STEPS} + {steps} "
+                       f"ensemble steps)", "cases_checked": len(per_case), "max_rel_l1": worst["l1"],
+            "max_rel_linf": worst["linf"], "tolerance_rel_l1": 1e-5, "per_case": per_case}
+
+
+def batched_vs_plain(n_cases: int, steps: int, torch, rank: int = 0, world: int = 1, dist=None, keep=(), kept=None):
     """Config-4 shape: `n_cases` Richtmyer-Meshkov cases of seeded sizes 128^2..512^2 (FP32 flux,
     HLLC + superbee, own end times), advanced `steps` ensemble steps by the batched persistent
     kernel, against the same cases advanced one after the other by the single-case path.  With
     several ranks the cases are sharded by estimated work (schemi_b200.ensemble, no per-step
-    exchange); totals are summed and device times maxed over the ranks."""
+    exchange); totals are summed and device times maxed over the ranks.  keep: case indices
+    whose conserved fields (and step counts) are stored into `kept` after the run, for the
+    comparison with the oracle."""
     from schemi_b200 import cases, ensemble, fv
 
     draws = [cases.richtmyer_meshkov_draws(i) for i in range(n_cases)]
@@ -294,7 +416,7 @@ def batched_vs_plain(n_cases: int, steps: int, torch, rank: int = 0, world: int 
     work = [ensemble.case_work(n * n, tr / ws, 0.5 / (n * 2.5)) for n, _, _, tr in draws]
     shares = ensemble.partition(work, world)
     mine = shares[rank]
-    handles, t_end, cells = [], [], 0
+    handles, t_end, cells, prims = [], [], 0, []
     for i in mine:
         case, prim, te = cases.richtmyer_meshkov(i, precision="f32flux")
         g = fv.FVCase(case)
@@ -302,6 +424,7 @@ def batched_vs_plain(n_cases: int, steps: int, torch, rank: int = 0, world: int 
         g.upload(prim)
         handles.append(g)
         t_end.append(te)
+        prims.append(prim)
         cells += case.n_cells
     torch.cuda.synchronize()
     # plain: each case on its own, `steps` steps through fv_run (device time per case)
@@ -311,19 +434,26 @@ def batched_vs_plain(n_cases: int, steps: int, torch, rank: int = 0, world: int 
         st = g.run(te, max_steps=steps)
         plain_ms += st.device_ms
         plain_updates += st.steps * g.n_cells
+    # the ensemble starts again from the restart sets, so that every case has taken exactly
+    # BATCH_WARMUP_STEPS + steps ensemble steps at the end (the oracle's step count)
+    for g, prim in zip(handles, prims):
+        g.upload(prim)
     batch = fv.FVBatch(handles)
-    batch.run(t_end, max_steps=16)  # warm-up (graph capture, kernel configuration)
+    batch.run(t_end, max_steps=BATCH_WARMUP_STEPS)  # warm-up (graph capture, kernel configuration)
     if dist is not None and world > 1:
         dist.barrier()
     st = batch.run(t_end, max_steps=steps)
-    updates, ms = float(st.cell_updates), float(st.device_ms)
-    if dist is not None and world > 1:
-        t = torch.tensor([updates, float(plain_updates), float(cells)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        updates, plain_updates, cells = float(t[0]), float(t[1]), int(t[2])
-        t = torch.tensor([ms, plain_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, plain_ms = float(t[0]), float(t[1])
+    totals = ensemble.combine_rank_totals(
+        dist if world > 1 else None, "cuda",
+        sums={"updates": float(st.cell_updates), "plain_updates": float(plain_updates), "cells": float(cells)},
+        maxes={"ms": float(st.device_ms), "plain_ms": plain_ms})
+    updates, plain_updates, cells = totals["updates"], totals["plain_updates"], int(totals["cells"])
+    ms, plain_ms = totals["ms"], totals["plain_ms"]
+    if kept is not None:
+        for i, g in zip(mine, handles):
+            if i in keep:
+                kept[i] = {"cells": g.n_cells, "steps": BATCH_WARMUP_STEPS + steps, "state": gpu_conserved(g),
+                           "n_species": g.case.n_species}
     out = {
         "cases": n_cases, "cells": cells, "steps": steps, "arith": "f32flux",
         "value": updates / (ms / 1e3), "unit": "cell-updates/s",
@@ -463,6 +593,112 @@ def adjoint_rt(torch, peak, t_end: float, autotune_shapes: bool):
     return out
 
 
+ACC_STEPS = 3  # steps of the single-case accuracy checks (KH 1024^2, the 3D reacting layer)
+
+
+def kh_accuracy(n: int, prec: str, want) -> dict:
+    """KH n x n in `prec` arithmetic, ACC_STEPS steps through fv_step from the restart set,
+    against the FP64 oracle's state after the same steps (want: a future of oracle_job)."""
+    from schemi_b200 import cases, fv
+
+    case, prim = cases.kelvin_helmholtz_2d(n=n, precision=prec)
+    g = fv.FVCase(case)
+    g.upload(prim)
+    for _ in range(ACC_STEPS):
+        g.step()
+    got = gpu_conserved(g)
+    g.close()
+    e = conserved_errors(got, want.result(), case.n_species)
+    return {"against": f"FP64 oracle, same restart set, {ACC_STEPS} steps", "rel_l1": e["l1"], "rel_linf": e["linf"],
+            "tolerance": {"rel_linf": 1e-12} if prec == "f64" else {"rel_l1": 1e-5}, "fields": e["fields"]}
+
+
+def tube_c1(torch) -> dict:
+    """Config 1: the 1000-cell two-component shock tube (FP64, HLLC + minmod, CFL 0.5,
+    transmissive ends) run to t = 0.2 through fv_run (the device time loop in CUDA graphs):
+    microseconds per step, and the final fields against the reference solver's own output
+    (tests/golden/shock_tube_1d_full.npz, written by the reference binary)."""
+    import numpy as np
+
+    from schemi_b200 import cases, fv
+
+    case, prim = cases.shock_tube_1d()
+    g = fv.FVCase(case)
+    g.upload(prim)
+    g.run(case.t_end)  # warm-up: graph capture and kernel configuration
+    g.upload(prim)
+    t0 = time.perf_counter()
+    st = g.run(case.t_end)
+    wall = time.perf_counter() - t0
+    out = g.download()
+    g.close()
+    ref = np.load(os.path.join(ROOT, "tests", "golden", "shock_tube_1d_full.npz"))
+    last = int(ref["n_steps"])
+    errs = {}
+    for f in ("c1", "c2", "vx", "p", "rho", "E"):
+        key = f"{f}_{last}"
+        if key in ref.files:
+            b = ref[key]
+            errs[f] = float(np.abs(out[f] - b).max() / max(np.abs(b).max(), 1e-300))
+    return {"workload": "shock_tube_1d 1000 cells to t=0.2, FP64, HLLC + minmod", "steps": int(st.steps),
+            "reference_steps": last, "device_us_per_step": 1e3 * st.device_ms / max(st.steps, 1),
+            "wall_us_per_step": 1e6 * wall / max(st.steps, 1), "time": st.time,
+            "rel_linf_vs_reference_output": max(errs.values()) if errs else None, "fields": errs,
+            "tolerance_rel_linf": 1e-12}
+
+
+def reacting_accuracy(n: int, want) -> dict:
+    """The 3D reacting shear layer at n^3 (FP32 flux + FP64 chemistry), ACC_STEPS steps, against
+    the FP64 oracle (flux, van der Waals EOS and the A+B->2C chemistry in FP64)."""
+    from schemi_b200 import cases, fv
+
+    case, prim = cases.reacting_shear_3d(n=n, precision="f32flux")
+    g = fv.FVCase(case)
+    g.upload(prim)
+    for _ in range(ACC_STEPS):
+        g.step()
+    got = gpu_conserved(g)
+    g.close()
+    e = conserved_errors(got, want.result(), case.n_species)
+    return {"against": f"FP64 oracle at {n}^3, same restart set, {ACC_STEPS} steps", "rel_l1": e["l1"],
+            "rel_linf": e["linf"], "tolerance": {"rel_l1": 1e-5}, "fields": e["fields"]}
+
+
+def adjoint_tangent_gap(torch, nx: int = 16, ny: int = 48, t_end: float = 0.5) -> dict:
+    """Gradient of the adjoint against the FP64 CPU tangent oracle (forward-mode derivatives of an
+    independent restatement of the same step) on a reduced Rayleigh-Taylor grid, along seeded
+    directions: the largest gap on the scale of |grad| |d|."""
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import fv_tangent
+    from schemi_b200 import adjoint, cases, fv
+
+    case, _ = cases.rayleigh_taylor_2d(nx, ny, precision="f64", t_end=t_end)
+    a = torch.from_numpy(np.random.default_rng(2029).normal(0.0, 1e-3, size=64))
+    g = fv.FVCase(case)
+    ad = a.clone().cuda().requires_grad_(True)
+    J, _ = adjoint.TimeLoop.apply(adjoint.rayleigh_taylor_primitive(ad, nx, ny), g, t_end, 10, 0)
+    J.backward()
+    grad = ad.grad.detach().cpu()
+    g.close()
+    tc = fv_tangent.TangentCase(case)
+
+    def U0(x):
+        return tc.conserved_from_primitive(list(adjoint.rayleigh_taylor_primitive(x, nx, ny).reshape(6, ny, nx)))
+
+    dts = tc.schedule(U0(a), t_end)
+    f = lambda x: tc.objective(U0(x), dts, 0)  # noqa: E731
+    rng = np.random.default_rng(11)
+    worst = 0.0
+    for _ in range(3):
+        d = torch.from_numpy(rng.normal(size=64))
+        _, dJ = fv_tangent.tangent(f, a, d)
+        worst = max(worst, abs(float(grad @ d) - float(dJ)) / (float(grad.norm()) * float(d.norm())))
+    return {"grid": f"{nx}x{ny} to t={t_end}", "directions": 3, "max_gap_over_grad_scale": worst,
+            "tolerance": 1e-9}
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -556,6 +792,7 @@ def run_ours(args):
         "roofline": {
             "bound": "hbm", "achieved": head["achieved_gbs"], "peak": peak, "unit": "GB/s",
             "frac": head["achieved_gbs"] / peak, "traffic": profile_traffic(f"kh{n}_f64"),
+            "traffic_source": "ncu capture of the step kernel, summarised in profiles/traffic.txt",
             "peak_source": peak_kind, "bytes_per_cell_update": head["bytes_per_cell_update"],
         },
         "fp32_flux": {
@@ -563,12 +800,18 @@ def run_ours(args):
             "e2e": results["f32flux"]["e2e"],
             "roofline": {"bound": "hbm", "achieved": results["f32flux"]["achieved_gbs"], "peak": peak,
                          "unit": "GB/s", "frac": results["f32flux"]["achieved_gbs"] / peak,
-                         "traffic": profile_traffic(f"kh{n}_f32flux")},
+                         "traffic": profile_traffic(f"kh{n}_f32flux"),
+                         "traffic_source": "ncu capture of the step kernel, summarised in profiles/traffic.txt"},
             "clocks": results["f32flux"]["clocks"],
         },
     }
+    if rank == 0 and args.tube:
+        line["shock_tube_1d"] = tube_c1(torch)
+    sample = batch_accuracy_sample(args.batch_cases) if args.batch_cases > 0 and not args.no_accuracy else []
+    kept = {}
     if args.batch_cases > 0:
-        b = batched_vs_plain(args.batch_cases, args.steps, torch, rank, world, dist)
+        b = batched_vs_plain(args.batch_cases, args.steps, torch, rank, world, dist if world > 1 else None,
+                             keep=sample, kept=kept)
         b["roofline_frac"] = b["value"] * b["bytes_per_cell_update"] / 1e9 / peak
         line["batched"] = b
     if args.reacting_n > 0:
@@ -576,23 +819,67 @@ def run_ours(args):
                                           not args.no_autotune)
     if args.adjoint_t_end > 0 and rank == 0:
         line["adjoint"] = adjoint_rt(torch, peak, args.adjoint_t_end, not args.no_autotune)
+
+    # ---- accuracy against the FP64 oracle, after every timed section (the oracle's worker
+    # processes would otherwise share the host cores with the timed host-side work)
+    pool = None
+    if not args.no_accuracy:
+        cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+        pool = oracle_pool(max(1, min(cores // max(world, 1), 24)))
+        fut = {}
+        # largest cases first: they take longest on the host
+        for i in sorted(kept, key=lambda i: -kept[i]["cells"]):
+            fut[("rm", i)] = pool.submit(oracle_job, "rm", i, kept[i]["steps"])
+        if rank == 0:
+            fut["kh"] = pool.submit(oracle_job, "kh", n, ACC_STEPS)
+            if args.reacting_n > 0:
+                fut["reacting"] = pool.submit(oracle_job, "reacting", args.reacting_acc_n, ACC_STEPS)
+            line["accuracy"] = kh_accuracy(n, "f64", fut["kh"])
+            line["fp32_flux"]["accuracy"] = kh_accuracy(n, "f32flux", fut["kh"])
+            if args.reacting_n > 0:
+                line["reacting_3d"]["accuracy"] = reacting_accuracy(args.reacting_acc_n, fut["reacting"])
+            if args.adjoint_t_end > 0:
+                line["adjoint"]["tangent_oracle"] = adjoint_tangent_gap(torch)
+        if args.batch_cases > 0:
+            acc = batch_accuracy(kept, fut, args.steps)
+            if world > 1:
+                # every rank checked its own sampled cases: the job's worst errors
+                tot = ensemble_totals(dist, {"max_rel_l1": acc["max_rel_l1"], "max_rel_linf": acc["max_rel_linf"],
+                                             "cases_checked": float(acc["cases_checked"])})
+                acc.update({"max_rel_l1": tot["max_rel_l1"], "max_rel_linf": tot["max_rel_linf"],
+                            "cases_checked": int(tot["cases_checked"]), "per_case": "rank 0 only"})
+            line["batched"]["accuracy"] = acc
     if rank == 0 and not args.no_cpu_baseline:
         try:
-            v, info = reference_throughput(n=128, steps=12, steps0=2, processes=1)
+            v, info = reference_throughput(n=128, steps=12, steps0=2, processes=1, patched=True)
+            vs, _ = reference_throughput(n=128, steps=12, steps0=2, processes=1, patched=False)
             line["cpu_baseline"] = {
                 "value": v, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
-                "sample": (f"as-shipped reference binary (oracle/_ref/schemi), KH mixing layer {info['n']}x{info['n']} "
-                           f"with slip x, {info['steps']} steps timed by differencing runs of 12 and 2 steps"),
+                "sample": (f"reference binary with the per-face assignment at HancockStage.cpp:308,313,318 "
+                           f"(oracle/_ref/schemi_patched, output byte-identical to the build as shipped), KH mixing "
+                           f"layer {info['n']}x{info['n']} with slip x, {info['steps']} steps timed by differencing "
+                           f"runs of 12 and 2 steps, one process"),
+                "as_shipped": {"value": vs, "unit": "cell-updates/s", "cores": 1,
+                               "sample": "the same with the build as shipped (oracle/_ref/schemi)"},
             }
         except Exception as e:
             line["cpu_baseline"] = {"value": None, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
                                     "sample": f"unavailable: {e}"}
+    if pool is not None:
+        pool.shutdown(wait=True, cancel_futures=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line))
     return 0
+
+
+def ensemble_totals(dist, worst: dict) -> dict:
+    """Largest of per-rank figures over the ranks (the same collectives on every rank)."""
+    from schemi_b200 import ensemble
+
+    return ensemble.combine_rank_totals(dist, "cuda", sums={}, maxes=worst)
 
 
 def main():
@@ -609,12 +896,74 @@ def main():
                     help="cells per axis of the 3D reacting shear layer workload (0: skip)")
     ap.add_argument("--adjoint-t-end", type=float, default=5.0,
                     help="end time of the Rayleigh-Taylor adjoint workload (0: skip)")
+    ap.add_argument("--reacting-acc-n", type=int, default=64,
+                    help="cells per axis of the reacting layer's accuracy check against the oracle")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the checks against the FP64 oracle")
+    ap.add_argument("--no-tube", dest="tube", action="store_false", help="skip the 1000-cell shock tube section")
+    ap.add_argument("--dry-run", action="store_true",
+                    help="multi-rank plumbing only, on the CPU with gloo: launch, sharding, totals, JSON line")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return launch_ranks(args.gpus)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world != args.gpus:
+        print(f"bench.py: --gpus {args.gpus} but WORLD_SIZE is {world}", file=sys.stderr)
+        return 2
+    if args.dry_run:
+        return run_dry(args)
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_ours(args)
+
+
+def torchrun_command(n: int, argv) -> list:
+    """The launch of this script as n ranks on one node (one process per GPU)."""
+    import socket
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+            "--master-addr", "127.0.0.1", f"--master-port={port}", os.path.abspath(__file__), *argv]
+
+
+def launch_ranks(n: int) -> int:
+    """`bench.py --gpus N` outside torchrun: start the N ranks itself and return their status."""
+    return subprocess.run(torchrun_command(n, sys.argv[1:])).returncode
+
+
+def run_dry(args) -> int:
+    """The multi-rank plumbing of the GPU arm without a GPU: every rank takes its share of the
+    ensemble (schemi_b200.ensemble), the totals are combined over gloo, and rank 0 prints the
+    line's rank and sharding fields (no measurement)."""
+    import torch.distributed as dist
+
+    from schemi_b200 import cases, ensemble
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("gloo", timeout=timedelta(seconds=60))
+    ws = 1.2 * math.sqrt(1.4)
+    draws = [cases.richtmyer_meshkov_draws(i) for i in range(args.batch_cases)]
+    work = [ensemble.case_work(nn * nn, tr / ws, 0.5 / (nn * 2.5)) for nn, _, _, tr in draws]
+    shares = ensemble.partition(work, world)
+    cells = sum(draws[i][0] ** 2 for i in shares[rank])
+    tot = ensemble.combine_rank_totals(dist if world > 1 else None, "cpu", sums={"cells": float(cells)},
+                                       maxes={"rank": float(rank)})
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps({"dry_run": True, "n_gpus": world, "value": None,
+                          "batched": {"cases": args.batch_cases, "cells": int(tot["cells"]),
+                                      "sharding": {"ranks": world, "cases_per_rank": [len(x) for x in shares],
+                                                   "estimated_imbalance": ensemble.imbalance(work, shares)}}}))
+    return 0
 
 
 if __name__ == "__main__":

@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define FV_ABI_VERSION 4
+#define FV_ABI_VERSION 5
 #define FV_MAX_SPECIES 4
 
 typedef int fv_status;
@@ -53,8 +53,21 @@ enum fv_error_code {
     FV_ERR_NAN = 12               /* NaNError: non-finite state detected after a step */
 };
 
-/* Equation of state: names of abstractMixtureThermodynamics.cpp:39-43. */
-enum fv_eos { FV_EOS_IDEAL = 0, FV_EOS_VAN_DER_WAALS = 1 };
+/* Equation of state: the five names of abstractMixtureThermodynamics.cpp:39-43 ("ideal",
+ * "vanDerWaals", "RedlichKwong", "stiffened", "Kataoka").  Ideal and van der Waals mixtures run
+ * on every path; the other three on the generic path (fv_step / fv_run), without chemistry.
+ *   REDLICH_KWONG  mixtureRedlichKwong.cpp: a, b from Tc and Pc, T from Uv by the cubic in sqrt(T)
+ *                  of RedlichKwongFluid.cpp:46-127 (the reference solves it in long double; the
+ *                  device in FP64)
+ *   STIFFENED      mixtureStiffened.cpp: stiff_p0 and stiff_gamma per species
+ *                  (set/stiffenedFluidData.txt)
+ *   KATAOKA        mixtureKataokaVanDerWaals.cpp: T from Uv or p by the Newton iteration of
+ *                  NewtonMethod.cpp:13-40 on KataokaVanDerWaalsFluid.cpp's series; lj_eps,
+ *                  lj_sigma and the b rule (set/KataokaVanDerWaalsFluidData.txt) */
+enum fv_eos {
+    FV_EOS_IDEAL = 0, FV_EOS_VAN_DER_WAALS = 1, FV_EOS_REDLICH_KWONG = 2, FV_EOS_STIFFENED = 3,
+    FV_EOS_KATAOKA = 4
+};
 
 /* Flux solver: names of abstractFlowSolver.cpp:29-35 that this build implements. */
 enum fv_flux { FV_FLUX_HLLC = 0, FV_FLUX_HLL = 1 };
@@ -168,6 +181,14 @@ typedef struct fv_config {
     double const_timestep;
     /* #Approximation_order: the step solver (fv_step_solver). */
     int order;
+    /* Equation-of-state data beyond M, Cv, Tc and Pc (ABI version 5). */
+    double stiff_p0[FV_MAX_SPECIES];     /* STIFFENED: p0 of each species */
+    double stiff_gamma[FV_MAX_SPECIES];  /* STIFFENED: gamma of each species */
+    double lj_eps[FV_MAX_SPECIES];       /* KATAOKA: Lennard-Jones epsilon of each species */
+    double lj_sigma[FV_MAX_SPECIES];     /* KATAOKA: Lennard-Jones sigma of each species */
+    int kataoka_b_critical;              /* KATAOKA: 1 "critical": b = coeff R Tc / (8 Pc);
+                                            0 "Kataoka": b = coeff sigma^3 N_A */
+    double kataoka_b_coeff;
 } fv_config;
 
 /* Field indices of fv_download / fv_upload arrays (n_cells doubles each, x fastest).

@@ -178,12 +178,181 @@ struct Cell {
     int nNb;
 };
 
+// ------------------------------------------------------------------ real-gas fluids
+// The cubic of RedlichKwongFluid.cpp in the reference's long-double solver
+// (cubicEquationSolver.cpp:15-113: trigonometric / hyperbolic roots, coefficients divided in
+// double first) and the choice of its single positive root (returnSinglePosValue, :115-152).
+constexpr double kZeroLevel = kStab;         // globalConstants.hpp zeroLevel
+constexpr double kOneThird = 1. / 3., kTwoThirdsC = 2. / 3.;
+const double kPiD = std::acos(-1.0);
+
+int signOf(double v) {  // sign.cpp
+    if (v > kZeroLevel) return 1;
+    if (v < -kZeroLevel) return -1;
+    return 0;
+}
+
+struct Roots {
+    double x[3];
+    bool ok;
+};
+
+Roots cubicRoots(double A, double B, double C, double D) {
+    typedef long double L;
+    constexpr double crit = 1E-9;
+    Roots r{{std::nan("1"), std::nan("2"), std::nan("3")}, true};
+    if ((A > crit) || (A < -crit)) {
+        const L a{B / A}, b{C / A}, c{D / A};
+        const L Q{(a * a - 3 * b) / 9};
+        const L R{(a * (2 * (a * a) - 9 * b) + 27 * c) / 54};
+        const L S{(Q * Q) * Q - R * R};
+        if (S >= kZeroLevel) {
+            const L phi{kOneThird * std::acos(R / std::sqrt(Q * Q * Q))};
+            r.x[0] = -2. * std::sqrt(Q) * std::cos(phi) - a * kOneThird;
+            r.x[1] = -2. * std::sqrt(Q) * std::cos(phi - kTwoThirdsC * kPiD) - a * kOneThird;
+            r.x[2] = -2. * std::sqrt(Q) * std::cos(phi + kTwoThirdsC * kPiD) - a * kOneThird;
+        } else if ((S < kZeroLevel) && (S >= -kZeroLevel)) {
+            r.x[0] = -2. * signOf((double)R) * std::sqrt(Q) - a * kOneThird;
+            r.x[1] = signOf((double)R) * std::sqrt(Q) - a * kOneThird;
+            r.x[2] = r.x[1];
+        } else if (S < -kZeroLevel) {
+            if (Q >= kZeroLevel) {
+                const L phi{kOneThird * std::acosh(std::abs(R) / (std::sqrt((Q * Q) * Q) + kStab))};
+                r.x[0] = -2. * signOf((double)R) * std::sqrt(Q) * std::cosh(phi) - a * kOneThird;
+            } else if ((Q < kZeroLevel) && (Q >= -kZeroLevel)) {
+                r.x[0] = -std::cbrt(c - (a * a) * a / 27) - a * kOneThird;
+            } else if (Q < -kZeroLevel) {
+                const L phi{kOneThird * std::asinh(std::abs(R) / (std::sqrt(std::abs((Q * Q) * Q)) + kStab))};
+                r.x[0] = -2. * signOf((double)R) * std::sqrt(std::abs(Q)) * std::sinh(phi) - a * kOneThird;
+            } else {
+                r.ok = false;  // "Q has unknown value"
+            }
+        } else {
+            r.ok = false;  // "S has unknown value"
+        }
+    } else {
+        const L a{B}, b{C}, c{D};
+        const auto Discr = b * b - 4 * a * c;
+        if (Discr >= 0) {
+            const auto a2 = 0.5 / (a + kStab);
+            r.x[0] = a2 * (-b + std::sqrt(Discr));
+            r.x[1] = a2 * (-b - std::sqrt(Discr));
+        }
+    }
+    return r;
+}
+
+// returnSinglePosValue; `ok` false where the reference throws (positivnessError)
+double singlePositive(Roots r, bool& ok) {
+    int nPositive = 0;
+    for (double& v : r.x) {
+        if (v >= 0) nPositive++;
+        else v = -123.;
+    }
+    ok = r.ok;
+    if (nPositive == 1) return std::max(std::max(r.x[0], r.x[1]), r.x[2]);
+    if (nPositive == 2) {
+        if (((r.x[0] - r.x[1]) < kZeroLevel) && (r.x[2] < 0)) return r.x[0];
+        if (((r.x[1] - r.x[2]) < kZeroLevel) && (r.x[0] < 0)) return r.x[1];
+        if (((r.x[0] - r.x[2]) < kZeroLevel) && (r.x[1] < 0)) return r.x[2];
+    } else if (nPositive == 3 && ((r.x[0] - r.x[1]) < kZeroLevel) && ((r.x[1] - r.x[2]) < kZeroLevel)) {
+        return r.x[0];
+    }
+    ok = false;
+    return std::nan("");
+}
+
+// KataokaVanDerWaalsFluid.cpp: the cluster series with M = 13 terms (its header's constant); the
+// loops written there as "for (J = 2; M < J; ++J)" run no iteration and leave their sums at zero,
+// which the derivatives below keep.
+constexpr double kKataokaM = 13;
+
+double kqa(double c, double T, double V0, double eps, double R) {
+    const double V0c{V0 * c};
+    const double epsRT{0.5 * eps / (R * T)};
+    double series{1.0};
+    for (std::size_t J = 2; J <= kKataokaM; ++J) series += std::pow(V0c, (J - 1.) / 3.) * std::exp((J - 1.) * epsRT);
+    return series;
+}
+double kUvA(double c, double T, double V0, double eps, double R) {
+    const double V0c{V0 * c};
+    const double epsRT{0.5 * eps / (R * T)};
+    double series{0};
+    for (std::size_t J = 2; J <= kKataokaM; ++J)
+        series -= (J - 1.) * std::pow(V0c, (J - 1.) / 3.) * std::exp((J - 1.) * epsRT);
+    return 0.5 * c * eps * series / kqa(c, T, V0, eps, R);
+}
+double kpA(double c, double T, double V0, double eps, double R) {
+    const double V0c{V0 * c};
+    const double epsRT{0.5 * eps / (R * T)};
+    double series{0};
+    for (std::size_t J = 2; J <= kKataokaM; ++J)
+        series -= (J - 1.) / 3. * std::pow(V0c, (J - 1.) / 3.) * std::exp((J - 1.) * epsRT);
+    return c * R * T * series / kqa(c, T, V0, eps, R);
+}
+// the never-running series of the derivatives: 0
+double kEmpty() {
+    double series{0};
+    for (std::size_t J = 2; kKataokaM < J; ++J) series += 1;
+    return series;
+}
+double kdPdC(double c, double T, double V0, double eps, double R, double b) {
+    const double V0c{V0 * c};
+    const double n13 = kEmpty();
+    const double qa1 = kqa(c, T, V0, eps, R);
+    return R * T / (1 - c * b) + c * R * T * b / ((1 - c * b) * (1 - c * b)) +
+           (R * T * n13 + V0c * R * T * (kEmpty() - n13 * kEmpty() / qa1)) / qa1;
+}
+double kdPdT(double c, double T, double V0, double eps, double R, double b) {
+    const double n13 = kEmpty();
+    const double qa1 = kqa(c, T, V0, eps, R);
+    return c * R / (1 - c * b) + (c * R * n13 + 0.5 * c * eps / T * (kEmpty() - n13 * kEmpty() / qa1)) / qa1;
+}
+double kdUvdC(double c, double Cv, double T, double V0, double eps, double R) {
+    const double V0c{V0 * c};
+    const double n13 = kEmpty();
+    const double qa1 = kqa(c, T, V0, eps, R);
+    return Cv * T + (0.5 * eps * n13 + 0.5 * V0c * eps * (kEmpty() - n13 * kEmpty() / qa1)) / qa1;
+}
+double kdUvdT(double c, double Cv, double T, double V0, double eps, double R) {
+    const double qa1 = kqa(c, T, V0, eps, R);
+    const double s2 = kEmpty();
+    return c * Cv + 0.25 * c * (eps * eps) / (R * (T * T)) * kEmpty() / qa1 -
+           0.25 * c * (eps * eps) / (R * (T * T)) * (s2 * s2) / (qa1 * qa1);
+}
+// NewtonMethod.cpp:13-40 (tolerance convergenceToleranceGlobal = 1e-12, at most 100 iterations)
+template <class F, class DF>
+double newton(double start, F f, DF df) {
+    std::size_t it{1};
+    double x1{start};
+    double x2 = x1 - f(x1) / df(x1);
+    if (std::abs(x2 - x1) <= 1E-12) return x2;
+    while ((std::abs(x2 - x1) > 1E-12) && (it <= 100)) {
+        x1 = x2;
+        x2 = x1 - f(x1) / df(x1);
+        it++;
+    }
+    return x2;
+}
+// T of a Kataoka state from its internal energy per volume (pFromUv, TFromUv, dpdrho, dpdUv)
+double kTFromUv(double c, double Cv, double Uv, double V0, double eps, double R) {
+    auto f = [&](double T) { return c * Cv * T + kUvA(c, T, V0, eps, R) - Uv; };
+    auto df = [&](double T) { return kdUvdT(c, Cv, T, V0, eps, R); };
+    const double initT{Uv / ((c + kStab) * Cv)};
+    return newton(initT, f, df);
+}
+
 struct Mix {
     int N;
     int eos;
     double R;
     double M[FV_MAX_SPECIES], Cv[FV_MAX_SPECIES];
+    // pair matrices: van der Waals / Redlich-Kwong a and b, stiffened p0 and gamma, Kataoka V0,
+    // eps and b
     double a[FV_MAX_SPECIES][FV_MAX_SPECIES], b[FV_MAX_SPECIES][FV_MAX_SPECIES];
+    double p0[FV_MAX_SPECIES][FV_MAX_SPECIES], gam[FV_MAX_SPECIES][FV_MAX_SPECIES];
+    double V0[FV_MAX_SPECIES][FV_MAX_SPECIES], eps[FV_MAX_SPECIES][FV_MAX_SPECIES];
+    mutable bool failed = false;  // a cubic without a single positive root (positivnessError)
 
     // calcMolarFrac (fractionCalculation.cpp:36-44) and the mixture sums
     void mixParams(const double* c, double& CvMix, double& aMix, double& bMix, double& MMix) const {
@@ -197,16 +366,64 @@ struct Mix {
         }
         aMix = 0;
         bMix = 0;
-        if (eos == FV_EOS_VAN_DER_WAALS)
+        if (eos == FV_EOS_VAN_DER_WAALS || eos == FV_EOS_REDLICH_KWONG)
             for (int k = 0; k < N; ++k)
                 for (int l = 0; l < N; ++l) {
                     aMix += X[k] * X[l] * a[k][l];
                     bMix += X[k] * X[l] * b[k][l];
                 }
     }
+    // stiffened: p0 and gamma of the mixture (mixtureStiffened.cpp:73-97)
+    void stiffParams(const double* c, double& p0m, double& gm) const {
+        double X[FV_MAX_SPECIES];
+        for (int k = 0; k < N; ++k) X[k] = c[k + 1] / c[0];
+        p0m = 0;
+        gm = 0;
+        for (int k = 0; k < N; ++k)
+            for (int l = 0; l < N; ++l) {
+                p0m += X[k] * X[l] * p0[k][l];
+                gm += X[k] * X[l] * gam[k][l];
+            }
+    }
+    // Kataoka: V0, eps and b of the mixture (mixtureKataokaVanDerWaals.cpp:116-137)
+    void kataokaParams(const double* c, double& V0m, double& em, double& bm) const {
+        double X[FV_MAX_SPECIES];
+        for (int k = 0; k < N; ++k) X[k] = c[k + 1] / c[0];
+        V0m = 0;
+        em = 0;
+        bm = 0;
+        for (int k = 0; k < N; ++k)
+            for (int l = 0; l < N; ++l) {
+                V0m += X[k] * X[l] * V0[k][l];
+                em += X[k] * X[l] * eps[k][l];
+                bm += X[k] * X[l] * b[k][l];
+            }
+    }
+    // sqrt(T) of a Redlich-Kwong state from Uv (RedlichKwongFluid.cpp:46-56, 96-102)
+    double rkSqrtT(double c, double Cvm, double Uv, double am, double bm) const {
+        bool ok;
+        const double r = singlePositive(cubicRoots(c * Cvm, 0, -Uv, -1.5 * am * c / bm * std::log1p(c * bm)), ok);
+        if (!ok) failed = true;
+        return r;
+    }
     double pFromUv(const double* c, double Uv) const {
         double Cvm, am, bm, Mm;
         mixParams(c, Cvm, am, bm, Mm);
+        if (eos == FV_EOS_STIFFENED) {  // stiffenedFluid.cpp:13-17
+            double p0m, gm;
+            stiffParams(c, p0m, gm);
+            return (gm - 1.0) * Uv - p0m * gm;
+        }
+        if (eos == FV_EOS_REDLICH_KWONG) {  // RedlichKwongFluid.cpp:46-56
+            const double sT = rkSqrtT(c[0], Cvm, Uv, am, bm);
+            return c[0] * R * (sT * sT) / (1 - c[0] * bm) - am * (c[0] * c[0]) / (sT * (1 + c[0] * bm));
+        }
+        if (eos == FV_EOS_KATAOKA) {  // KataokaVanDerWaalsFluid.cpp:237-256
+            double V0m, em, bk;
+            kataokaParams(c, V0m, em, bk);
+            const double T = kTFromUv(c[0], Cvm, Uv, V0m, em, R);
+            return c[0] * R * T / (1 - c[0] * bk) + kpA(c[0], T, V0m, em, R);
+        }
         const double g1 = R / Cvm;
         if (eos == FV_EOS_IDEAL) return g1 * Uv;  // idealFluid.cpp:13-17
         const double acc = am * (c[0] * c[0]);   // vanDerWaalsFluid.cpp:14-21
@@ -215,6 +432,29 @@ struct Mix {
     double UvFromp(const double* c, double p) const {
         double Cvm, am, bm, Mm;
         mixParams(c, Cvm, am, bm, Mm);
+        if (eos == FV_EOS_STIFFENED) {  // stiffenedFluid.cpp:19-23
+            double p0m, gm;
+            stiffParams(c, p0m, gm);
+            return (p + p0m * gm) / (gm - 1.0);
+        }
+        if (eos == FV_EOS_REDLICH_KWONG) {  // RedlichKwongFluid.cpp:58-68
+            const double cc = c[0];
+            bool ok;
+            const double sT = singlePositive(
+                cubicRoots(cc * R, 0, -p * (1 - cc * bm), -am * (cc * cc) * (1 - cc * bm) / (1 + cc * bm)), ok);
+            if (!ok) failed = true;
+            return cc * Cvm * (sT * sT) - 1.5 * am * cc / (bm * sT) * std::log1p(cc * bm);
+        }
+        if (eos == FV_EOS_KATAOKA) {  // KataokaVanDerWaalsFluid.cpp:258-277
+            double V0m, em, bk;
+            kataokaParams(c, V0m, em, bk);
+            const double cc = c[0];
+            auto f = [&](double T) { return cc * R * T / (1 - cc * bk) + kpA(cc, T, V0m, em, R) - p; };
+            auto df = [&](double T) { return kdPdT(cc, T, V0m, em, R, bk); };
+            const double initT{p / ((cc + kStab) * R)};
+            const double T = newton(initT, f, df);
+            return cc * Cvm * T + kUvA(cc, T, V0m, em, R);
+        }
         const double g1 = R / Cvm;
         if (eos == FV_EOS_IDEAL) return p / g1;  // idealFluid.cpp:19-23
         const double acc = am * (c[0] * c[0]);   // vanDerWaalsFluid.cpp:23-30
@@ -223,20 +463,87 @@ struct Mix {
     double TFromUv(const double* c, double Uv) const {
         double Cvm, am, bm, Mm;
         mixParams(c, Cvm, am, bm, Mm);
+        if (eos == FV_EOS_STIFFENED) {  // stiffenedFluid.cpp:37-41
+            double p0m, gm;
+            stiffParams(c, p0m, gm);
+            return (Uv - p0m) / ((c[0] + kStab) * Cvm);
+        }
+        if (eos == FV_EOS_REDLICH_KWONG) {  // RedlichKwongFluid.cpp:84-92
+            const double sT = rkSqrtT(c[0], Cvm, Uv, am, bm);
+            return sT * sT;
+        }
+        if (eos == FV_EOS_KATAOKA) {
+            double V0m, em, bk;
+            kataokaParams(c, V0m, em, bk);
+            return kTFromUv(c[0], Cvm, Uv, V0m, em, R);
+        }
         if (eos == FV_EOS_IDEAL) return Uv / ((c[0] + kStab) * Cvm);  // idealFluid.cpp:37-41
         return (Uv + am * (c[0] * c[0])) / ((c[0] + kStab) * Cvm);    // vanDerWaalsFluid.cpp:44-48
     }
-    double dpdUv(const double* c) const {
+    double dpdUv(const double* c, double Uv) const {
         double Cvm, am, bm, Mm;
         mixParams(c, Cvm, am, bm, Mm);
+        if (eos == FV_EOS_STIFFENED) {  // stiffenedFluid.cpp dpdUv: gamma - 1
+            double p0m, gm;
+            stiffParams(c, p0m, gm);
+            return gm - 1.0;
+        }
+        if (eos == FV_EOS_REDLICH_KWONG) {  // RedlichKwongFluid.cpp:120-131
+            const double sT = rkSqrtT(c[0], Cvm, Uv, am, bm);
+            const double T = sT * sT;
+            return rkdPdT(c[0], T, am, bm) / rkdUvdT(c[0], Cvm, T, am, bm);
+        }
+        if (eos == FV_EOS_KATAOKA) {  // KataokaVanDerWaalsFluid.cpp:355-372
+            double V0m, em, bk;
+            kataokaParams(c, V0m, em, bk);
+            const double T = kTFromUv(c[0], Cvm, Uv, V0m, em, R);
+            return kdPdT(c[0], T, V0m, em, R, bk) / kdUvdT(c[0], Cvm, T, V0m, em, R);
+        }
         const double g1 = R / Cvm;
         if (eos == FV_EOS_IDEAL) return g1;
         return g1 / (1 - c[0] * bm);  // vanDerWaalsFluid.cpp:71-75
     }
-    // sqSonicSpeed = dpdrho + dpdUv * (Uv + p) / rho (mixtureIdeal.cpp, mixtureVanDerWaals.cpp:390-397)
+    // RedlichKwongFluid.cpp:14-44
+    double rkdPdC(double c, double T, double am, double bm) const {
+        return R * T / (1 - c * bm) + c * R * T * bm / ((1 - c * bm) * (1 - c * bm)) -
+               2 * am * c / (std::sqrt(T) * (1 + bm * c)) +
+               am * (c * c) * bm / (std::sqrt(T) * ((1 + bm * c) * (1 + bm * c)));
+    }
+    double rkdPdT(double c, double T, double am, double bm) const {
+        const double sT = std::sqrt(T);
+        return c * R / (1 - c * bm) + 0.5 * am * (c * c) / (((sT * sT) * sT) * (1 + c * bm));
+    }
+    double rkdUvdC(double c, double Cvm, double T, double am, double bm) const {
+        return Cvm * T - 1.5 * am * std::log1p(c * bm) / (bm * std::sqrt(T)) - 1.5 * am * c / (std::sqrt(T) * (1 + c * bm));
+    }
+    double rkdUvdT(double c, double Cvm, double T, double am, double bm) const {
+        const double sT = std::sqrt(T);
+        return c * Cvm + 0.75 * am * c * std::log1p(c * bm) / (bm * ((sT * sT) * sT));
+    }
+    // sqSonicSpeed = dpdrho + dpdUv * (Uv + p) / rho (mixtureIdeal.cpp, mixtureVanDerWaals.cpp:390-397,
+    // mixtureRedlichKwong.cpp:418-425, mixtureStiffened.cpp:327-334, mixtureKataokaVanDerWaals.cpp:445-452)
     double sqSonicSpeed(const double* c, double rho, double Uv, double p) const {
         double Cvm, am, bm, Mm;
         mixParams(c, Cvm, am, bm, Mm);
+        if (eos == FV_EOS_STIFFENED) return 0 + dpdUv(c, Uv) * (Uv + p) / rho;
+        if (eos == FV_EOS_REDLICH_KWONG) {  // RedlichKwongFluid.cpp:104-118
+            const double sT = rkSqrtT(c[0], Cvm, Uv, am, bm);
+            const double T = sT * sT;
+            const double dpdrho = (rkdPdC(c[0], T, am, bm) -
+                                   rkdPdT(c[0], T, am, bm) * rkdUvdC(c[0], Cvm, T, am, bm) / rkdUvdT(c[0], Cvm, T, am, bm)) /
+                                  Mm;
+            return dpdrho + dpdUv(c, Uv) * (Uv + p) / rho;
+        }
+        if (eos == FV_EOS_KATAOKA) {  // KataokaVanDerWaalsFluid.cpp:332-353
+            double V0m, em, bk;
+            kataokaParams(c, V0m, em, bk);
+            const double T = kTFromUv(c[0], Cvm, Uv, V0m, em, R);
+            const double dpdrho = (kdPdC(c[0], T, V0m, em, R, bk) -
+                                   kdPdT(c[0], T, V0m, em, R, bk) * kdUvdC(c[0], Cvm, T, V0m, em, R) /
+                                       kdUvdT(c[0], Cvm, T, V0m, em, R)) /
+                                  Mm;
+            return dpdrho + dpdUv(c, Uv) * (Uv + p) / rho;
+        }
         const double g1 = R / Cvm;
         if (eos == FV_EOS_IDEAL) return 0 + g1 * (Uv + p) / rho;
         const double m_cb = 1 - c[0] * bm;  // vanDerWaalsFluid.cpp:57-69
@@ -913,8 +1220,8 @@ struct Flux {
 bool riemann(const fvo_case& cs, const FState& O, const FState& B, const V3& N, Flux& F) {
     const Mix& mx = cs.mix;
     const int NS = mx.N;
-    const double csO = std::sqrt(mx.sqSonicSpeed(O.c, O.rho[0], O.Uv, O.p) + kTwoThirds * 0.0 * (1. + mx.dpdUv(O.c)));
-    const double csN = std::sqrt(mx.sqSonicSpeed(B.c, B.rho[0], B.Uv, B.p) + kTwoThirds * 0.0 * (1. + mx.dpdUv(B.c)));
+    const double csO = std::sqrt(mx.sqSonicSpeed(O.c, O.rho[0], O.Uv, O.p) + kTwoThirds * 0.0 * (1. + mx.dpdUv(O.c, O.Uv)));
+    const double csN = std::sqrt(mx.sqSonicSpeed(B.c, B.rho[0], B.Uv, B.p) + kTwoThirds * 0.0 * (1. + mx.dpdUv(B.c, B.Uv)));
     const double uO = vdot(O.v, N), uN = vdot(B.v, N);
     const double tpO = kTwoThirds * 0.0, tpN = kTwoThirds * 0.0;
     const double SO = std::min(uO - csO, uN - csN);
@@ -1627,12 +1934,16 @@ bool validate(const fv_config& cf, std::string& err) {
     for (int d = 0; d < cf.dims; ++d)
         if (cf.n[d] < 1) { err = "cell counts must be positive"; return false; }
     if (cf.n_species < 1 || cf.n_species > FV_MAX_SPECIES) { err = "n_species out of range"; return false; }
-    if (cf.eos != FV_EOS_IDEAL && cf.eos != FV_EOS_VAN_DER_WAALS) { err = "unknown equation of state"; return false; }
+    if (cf.eos < FV_EOS_IDEAL || cf.eos > FV_EOS_KATAOKA) { err = "unknown equation of state"; return false; }
     if (cf.flux != FV_FLUX_HLLC && cf.flux != FV_FLUX_HLL) { err = "unknown flux solver"; return false; }
     if (cf.limiter < 0 || cf.limiter > FV_LIM_SCHMIDTMANN) { err = "unknown limiter"; return false; }
     if (cf.chemistry == FV_CHEM_CL2 && cf.n_species != 2) { err = "Cl2 dissociation needs 2 species"; return false; }
     if (cf.chemistry == FV_CHEM_A_B_2C && cf.n_species != 3) { err = "A+B->2C needs 3 species"; return false; }
     if (cf.chemistry < FV_CHEM_NONE || cf.chemistry > FV_CHEM_CL2) { err = "unknown chemistry"; return false; }
+    if (cf.chemistry != FV_CHEM_NONE && cf.eos != FV_EOS_IDEAL && cf.eos != FV_EOS_VAN_DER_WAALS) {
+        err = "chemistry runs with ideal and van der Waals mixtures";
+        return false;
+    }
     if (cf.order < FV_ORDER_SECOND || cf.order > FV_ORDER_THIRD_CADA) {
         err = "unknown step solver";
         return false;
@@ -1674,6 +1985,49 @@ fvo_case* fvo_create(const fv_config* cfg, char* err, int err_len) {
                 if (k != l) {
                     mx.b[k][l] = std::pow(0.5 * (std::cbrt(mx.b[k][k]) + std::cbrt(mx.b[l][l])), 3);
                     mx.a[k][l] = std::sqrt(mx.a[k][k] * mx.a[l][l]);
+                }
+    } else if (cfg->eos == FV_EOS_REDLICH_KWONG) {
+        // mixtureRedlichKwong.cpp:34-60 (the constants folded at compile time, as g++ does there)
+        constexpr double chi{std::cbrt(2) - 1.};
+        constexpr double Sigma_a{1. / (9. * chi)}, Sigma_b{chi / 3.};
+        for (int k = 0; k < mx.N; ++k) {
+            mx.b[k][k] = Sigma_b * mx.R * cfg->Tc[k] / cfg->Pc[k];
+            mx.a[k][k] = Sigma_a * mx.R * mx.R * cfg->Tc[k] * cfg->Tc[k] * std::sqrt(cfg->Tc[k]) / cfg->Pc[k];
+        }
+        for (int k = 0; k < mx.N; ++k)
+            for (int l = 0; l < mx.N; ++l)
+                if (k != l) {
+                    mx.b[k][l] = std::pow(0.5 * (std::cbrt(mx.b[k][k]) + std::cbrt(mx.b[l][l])), 3);
+                    mx.a[k][l] = std::sqrt(mx.a[k][k] * mx.a[l][l]);
+                }
+    } else if (cfg->eos == FV_EOS_STIFFENED) {
+        // mixtureStiffened.cpp:19-42
+        for (int k = 0; k < mx.N; ++k) {
+            mx.p0[k][k] = cfg->stiff_p0[k];
+            mx.gam[k][k] = cfg->stiff_gamma[k];
+        }
+        for (int k = 0; k < mx.N; ++k)
+            for (int l = 0; l < mx.N; ++l)
+                if (k != l) {
+                    mx.p0[k][l] = std::sqrt(mx.p0[k][k] * mx.p0[l][l]);
+                    mx.gam[k][l] = std::sqrt(mx.gam[k][k] * mx.gam[l][l]);
+                }
+    } else if (cfg->eos == FV_EOS_KATAOKA) {
+        // mixtureKataokaVanDerWaals.cpp:20-75
+        constexpr double NA = 6.02214076E23;  // globalConstants.hpp NAvogardro
+        for (int k = 0; k < mx.N; ++k) {
+            const double sg = cfg->lj_sigma[k];
+            mx.b[k][k] = cfg->kataoka_b_critical ? cfg->kataoka_b_coeff * mx.R * cfg->Tc[k] / (8 * cfg->Pc[k])
+                                                 : cfg->kataoka_b_coeff * (sg * sg * sg) * NA;
+            mx.V0[k][k] = (sg * sg * sg) / std::sqrt(2) * NA;
+            mx.eps[k][k] = cfg->lj_eps[k];
+        }
+        for (int k = 0; k < mx.N; ++k)
+            for (int l = 0; l < mx.N; ++l)
+                if (k != l) {
+                    mx.b[k][l] = std::pow(0.5 * (std::cbrt(mx.b[k][k]) + std::cbrt(mx.b[l][l])), 3);
+                    mx.V0[k][l] = std::pow(0.5 * (std::cbrt(mx.V0[k][k]) + std::cbrt(mx.V0[l][l])), 3);
+                    mx.eps[k][l] = std::sqrt(mx.eps[k][k] * mx.eps[l][l]);
                 }
     }
     for (int k = 0; k <= cs->N; ++k) {
@@ -1747,6 +2101,11 @@ int fvo_step(fvo_case* cs, double* dt_used, double* dt_next) {
     }
     cs->time += dt;
     cs->dt = cflTimestep(*cs);
+    if (cs->mix.failed) {
+        // cubicEquationSolver.cpp / returnSinglePosValue throw: the run stops
+        cs->mix.failed = false;
+        return FV_ERR_POSITIVENESS;
+    }
     if (dt_used) *dt_used = dt;
     if (dt_next) *dt_next = cs->dt;
     return FV_OK;

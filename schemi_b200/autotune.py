@@ -31,8 +31,8 @@ def _cache_path() -> str:
 
 def _key(case, device: str) -> str:
     n = "x".join(str(v) for v in case.n[: case.dims])
-    # FP32-flux 2D cases run the warp-strip march, whose shapes are timed separately
-    kind = "|warp-strip" if case.dims == 2 and case.precision == "f32flux" else ""
+    # 2D cases run the warp-strip march (FP32 flux or FP64), whose shapes are timed separately
+    kind = ("|warp-strip" if case.precision == "f32flux" else "|warp-strip64") if case.dims == 2 else ""
     return f"{case.dims}d|{n}|ns{case.n_species}|{case.eos}|{case.precision}|{device}{kind}"
 
 

@@ -3,9 +3,10 @@
     python -m schemi_b200.build            # or build() from Python
 
 Translation units (compiled in parallel):
-  csrc/fv_f64_ns<N>.cu  FP64 step kernels for N species, --fmad=false (bit-exact with the reference)
-  csrc/fv_f32_ns<N>.cu  FP32-flux step kernels for N species, fast math
-  csrc/fv_dispatch.cu   selects the unit of a species count
+  csrc/fv_f64_ns<N>_<eos>.cu  FP64 step kernels for N species and one EOS, --fmad=false (bit-exact
+                        with the reference)
+  csrc/fv_f32_ns<N>_<eos>.cu  FP32-flux step kernels for N species and one EOS, fast math
+  csrc/fv_dispatch.cu   selects the unit of a species count and an EOS
   csrc/fv_capi.cu       C-ABI, upload/download/finalize kernels, device time loop (--fmad=false)
   csrc/fv_batch.cu      batched ensemble (--fmad=false)
   csrc/fv_noalloc.cu    the step without device allocation (--fmad=false)
@@ -46,8 +47,9 @@ UNITS = {
     "fv_adjoint_f32.cu": ["-use_fast_math"],
 }
 for _ns in (1, 2, 3, 4):
-    UNITS[f"fv_f64_ns{_ns}.cu"] = ["--fmad=false"]
-    UNITS[f"fv_f32_ns{_ns}.cu"] = ["-use_fast_math"]
+    for _eos in ("ideal", "vdw", "real"):
+        UNITS[f"fv_f64_ns{_ns}_{_eos}.cu"] = ["--fmad=false"]
+        UNITS[f"fv_f32_ns{_ns}_{_eos}.cu"] = ["-use_fast_math"]
 
 
 def nvcc() -> str:
@@ -55,6 +57,11 @@ def nvcc() -> str:
         if cand and os.path.exists(cand):
             return cand
     raise RuntimeError("nvcc not found")
+
+
+def _headers():
+    """Sources every translation unit may include (a .cu file is only its own unit's source)."""
+    return [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".inc", ".h"))]
 
 
 def _sources():
@@ -71,7 +78,7 @@ def _stale(target: str, deps) -> bool:
 def build(verbose: bool = False, force: bool = False, extra_flags=None) -> str:
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
-    deps = _sources() + [os.path.join(HERE, "..", "include", "fvstep.h")]
+    deps = _headers() + [os.path.join(HERE, "..", "include", "fvstep.h")]
     units = dict(UNITS)
     if os.path.exists(os.path.join(CSRC, "fv_noalloc.cu")):
         units["fv_noalloc.cu"] = ["--fmad=false"]
@@ -82,7 +89,7 @@ def build(verbose: bool = False, force: bool = False, extra_flags=None) -> str:
     for unit, flags in units.items():
         obj = os.path.join(BUILD, unit.replace(".cu", ".o"))
         objs.append(obj)
-        if force or _stale(obj, deps):
+        if force or _stale(obj, deps + [os.path.join(CSRC, unit)]):
             cmd = [nvcc(), *ARCH, *COMMON, *flags, *(extra_flags or []), "-c", os.path.join(CSRC, unit), "-o", obj]
             jobs.append(cmd)
     with cf.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 4))) as ex:

@@ -24,7 +24,7 @@ R_SI = 8.31446261815324  # Schemi/headers/globalConstants.hpp:28
 
 GAS_CONSTANT = {"SI": R_SI, "1": 1.0, "CGS": R_SI * 1e7, "CGmS": R_SI * 1e1}
 
-EOS = {"ideal": 0, "vanDerWaals": 1}
+EOS = {"ideal": 0, "vanDerWaals": 1, "RedlichKwong": 2, "stiffened": 3, "Kataoka": 4}
 FLUX = {"HLLC": 0, "HLL": 1}
 LIMITERS = ["zero", "minmod", "vanLeer", "linear", "vanAlbada", "HQUICK", "vanLeer2", "superbee",
             "vanAlbada2", "minmod2", "Sweby", "Koren", "Koren2", "UTCDFS", "Schmidtmann"]
@@ -88,6 +88,12 @@ class fv_config_t(ctypes.Structure):
         ("chem_max_iter", ctypes.c_int),
         ("const_timestep", ctypes.c_double),
         ("order", ctypes.c_int),
+        ("stiff_p0", ctypes.c_double * MAX_SPECIES),
+        ("stiff_gamma", ctypes.c_double * MAX_SPECIES),
+        ("lj_eps", ctypes.c_double * MAX_SPECIES),
+        ("lj_sigma", ctypes.c_double * MAX_SPECIES),
+        ("kataoka_b_critical", ctypes.c_int),
+        ("kataoka_b_coeff", ctypes.c_double),
     ]
 
 
@@ -99,6 +105,10 @@ class Species:
     Cv: float
     Tc: float = 1.0
     Pc: float = 1.0
+    p0: float = 0.0      # stiffened gas (set/stiffenedFluidData.txt)
+    gamma: float = 1.4
+    lj_eps: float = 0.0  # Kataoka (set/KataokaVanDerWaalsFluidData.txt)
+    lj_sigma: float = 0.0
 
 
 @dataclass
@@ -156,6 +166,9 @@ class Case:
     const_timestep: float = 0.0   # > 0: every step takes this dt (#Constant_timestep)
     order: str = "SecondOrder"    # #Approximation_order: a key of ORDERS
     name: str = "case"
+    # Kataoka-van der Waals b rule (set/KataokaVanDerWaalsFluidData.txt): "critical" (b = coeff R Tc
+    # / (8 Pc)) or "Kataoka" (b = coeff sigma^3 N_A), and its coefficient
+    kataoka_b: Tuple[str, float] = ("critical", 1.0)
 
     def __post_init__(self):
         for p in PATCHES_USED[self.dims]:
@@ -208,6 +221,10 @@ class Case:
         c.R = self.R
         for k, s in enumerate(self.species):
             c.M[k], c.Cv[k], c.Tc[k], c.Pc[k] = s.M, s.Cv, s.Tc, s.Pc
+            c.stiff_p0[k], c.stiff_gamma[k] = s.p0, s.gamma
+            c.lj_eps[k], c.lj_sigma[k] = s.lj_eps, s.lj_sigma
+        c.kataoka_b_critical = int(self.kataoka_b[0] == "critical")
+        c.kataoka_b_coeff = float(self.kataoka_b[1])
         c.eos = EOS[self.eos]
         c.flux = FLUX[self.flux]
         c.limiter = LIMITER[self.limiter]

@@ -20,7 +20,7 @@ from typing import List, Sequence, Tuple
 
 import numpy as np
 
-from .case import BC, Case, PatchBC, Species
+from .case import BC, R_SI, Case, PatchBC, Species
 
 
 def _centres(n: int, L: float) -> np.ndarray:
@@ -40,6 +40,37 @@ def shock_tube_1d(n: int = 1000, limiter: str = "minmod", flux: str = "HLLC", pr
     cB = np.where(left, 0.0, 0.125)
     p = np.where(left, 1.0, 0.1)
     z = np.zeros(n)
+    return case, [cA, cB, z, z.copy(), z.copy(), p]
+
+
+def real_gas_tube(eos: str, n: int = 200, limiter: str = "minmod") -> Tuple[Case, list]:
+    """Two-component shock tube for the equations of state beyond ideal and van der Waals
+    (transmissive ends, HLLC).
+    stiffened: R = 1 units, left a stiffened liquid-like species (gamma 2, p0 0.5; rho 1, p 1),
+    right a gas (gamma 1.4, p0 0; rho 0.125, p 0.1).
+    RedlichKwong / Kataoka: SI units on a 1 m tube, nitrogen- and argon-like species (critical
+    points 126.2 K / 3.39 MPa and 150.9 K / 4.9 MPa; Kataoka: Lennard-Jones eps 95 R and 120 R
+    J/mol, sigma 3.7e-10 and 3.4e-10 m, b from the critical point), left 1 MPa at 400 mol/m^3,
+    right 0.1 MPa at 40 mol/m^3."""
+    x = _centres(n, 1.0)
+    left = x < 0.5
+    z = np.zeros(n)
+    if eos == "stiffened":
+        sp = [Species(M=1.0, Cv=1.0, p0=0.5, gamma=2.0), Species(M=1.0, Cv=1.0 / 0.4, p0=0.0, gamma=1.4)]
+        case = Case(dims=1, n=(n, 1, 1), L=(1.0, 1.0, 1.0), species=sp, t_end=0.2, limiter=limiter, eos=eos,
+                    courant=0.5, min_timestep=1e-15, name="stiffened_tube")
+        cA = np.where(left, 1.0, 0.0)
+        cB = np.where(left, 0.0, 0.125)
+        p = np.where(left, 1.0, 0.1)
+        return case, [cA, cB, z, z.copy(), z.copy(), p]
+    R = R_SI
+    sp = [Species(M=0.028, Cv=20.8, Tc=126.2, Pc=3.39e6, lj_eps=95.0 * R, lj_sigma=3.7e-10),
+          Species(M=0.040, Cv=12.5, Tc=150.9, Pc=4.9e6, lj_eps=120.0 * R, lj_sigma=3.4e-10)]
+    case = Case(dims=1, n=(n, 1, 1), L=(1.0, 1.0, 1.0), species=sp, t_end=1e-3, limiter=limiter, eos=eos,
+                R_units="SI", courant=0.5, min_timestep=1e-15, name=f"{eos}_tube")
+    cA = np.where(left, 400.0, 0.0)
+    cB = np.where(left, 0.0, 40.0)
+    p = np.where(left, 1.0e6, 1.0e5)
     return case, [cA, cB, z, z.copy(), z.copy(), p]
 
 

@@ -2,8 +2,9 @@
 // runs one case per process).
 //
 // All cases share dims, species count, EOS, flux, limiter and precision, and use the fused march.
-// One ensemble step = k_march_batch (a persistent grid striding over the tiles of every case)
-// + k_finalize_batch (one CTA per case: its own CFL step, clock and end-time clamp).  Each case
+// One ensemble step = the ensemble kernel (k_warp2d_batch, one CTA per tile, or k_march_batch, a
+// persistent grid striding over the tiles of every case) + k_finalize_batch (one CTA per case: its
+// own CFL step, clock and end-time clamp).  Each case
 // reads and writes the buffer pair selected by the parity of its own step count, so a case that
 // reached its end time simply stops while the others go on.  Ensemble steps are captured in a
 // CUDA graph of `chunk` steps; the host polls the number of active cases once per chunk.
@@ -61,7 +62,8 @@ namespace {
 void layoutTiles(fv_batch* b) {
     bool warp = true, ring = true;
     for (fv_handle* h : b->cases) {
-        warp = warp && warpStripMarch(h->P);
+        // the ensemble kernel has the warp-strip layout in FP32-flux arithmetic only
+        warp = warp && warpStripMarch(h->P) && h->cfg.precision == FV_PREC_F32_FLUX;
         ring = ring && h->P.tma != 0;
     }
     b->shape.warp = warp ? (ring ? 2 : 1) : 0;
@@ -70,6 +72,9 @@ void layoutTiles(fv_batch* b) {
         BatchCase& bc = b->host[i];
         bc.P = b->cases[i]->P;
         bc.P.warp2d = warp ? 1 : 0;
+        // the finalize stays a launch of its own: a ticket per tile (the fused finalize) costs
+        // each of the ensemble's tens of thousands of CTAs an atomic round trip at its end
+        bc.P.fuseFinalize = 0;
         const StepParams& P = bc.P;
         const int cols = marchTileColumns(P, b->shape.bx);
         bc.tiles[0] = (P.n[0] + cols - 1) / cols;

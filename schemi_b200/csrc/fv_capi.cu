@@ -305,22 +305,22 @@ template <template <int, int> class F> struct Dispatch;
 
 void upload(fv_handle* h, const double* primDev) {
     const int ns = h->cfg.n_species;
-    const bool vdw = h->cfg.eos == FV_EOS_VAN_DER_WAALS;
+    const int e = fvEosTemplate(h->cfg.eos);
     switch (ns) {
-    case 1: vdw ? launchUpload<1, 1>(h, primDev) : launchUpload<1, 0>(h, primDev); break;
-    case 2: vdw ? launchUpload<2, 1>(h, primDev) : launchUpload<2, 0>(h, primDev); break;
-    case 3: vdw ? launchUpload<3, 1>(h, primDev) : launchUpload<3, 0>(h, primDev); break;
-    default: vdw ? launchUpload<4, 1>(h, primDev) : launchUpload<4, 0>(h, primDev); break;
+    case 1: e == 0 ? launchUpload<1, 0>(h, primDev) : e == 1 ? launchUpload<1, 1>(h, primDev) : launchUpload<1, kEosGeneral>(h, primDev); break;
+    case 2: e == 0 ? launchUpload<2, 0>(h, primDev) : e == 1 ? launchUpload<2, 1>(h, primDev) : launchUpload<2, kEosGeneral>(h, primDev); break;
+    case 3: e == 0 ? launchUpload<3, 0>(h, primDev) : e == 1 ? launchUpload<3, 1>(h, primDev) : launchUpload<3, kEosGeneral>(h, primDev); break;
+    default: e == 0 ? launchUpload<4, 0>(h, primDev) : e == 1 ? launchUpload<4, 1>(h, primDev) : launchUpload<4, kEosGeneral>(h, primDev); break;
     }
 }
 void download(fv_handle* h) {
     const int ns = h->cfg.n_species;
-    const bool vdw = h->cfg.eos == FV_EOS_VAN_DER_WAALS;
+    const int e = fvEosTemplate(h->cfg.eos);
     switch (ns) {
-    case 1: vdw ? launchDownload<1, 1>(h) : launchDownload<1, 0>(h); break;
-    case 2: vdw ? launchDownload<2, 1>(h) : launchDownload<2, 0>(h); break;
-    case 3: vdw ? launchDownload<3, 1>(h) : launchDownload<3, 0>(h); break;
-    default: vdw ? launchDownload<4, 1>(h) : launchDownload<4, 0>(h); break;
+    case 1: e == 0 ? launchDownload<1, 0>(h) : e == 1 ? launchDownload<1, 1>(h) : launchDownload<1, kEosGeneral>(h); break;
+    case 2: e == 0 ? launchDownload<2, 0>(h) : e == 1 ? launchDownload<2, 1>(h) : launchDownload<2, kEosGeneral>(h); break;
+    case 3: e == 0 ? launchDownload<3, 0>(h) : e == 1 ? launchDownload<3, 1>(h) : launchDownload<3, kEosGeneral>(h); break;
+    default: e == 0 ? launchDownload<4, 0>(h) : e == 1 ? launchDownload<4, 1>(h) : launchDownload<4, kEosGeneral>(h); break;
     }
 }
 
@@ -367,13 +367,18 @@ void launchAverage(fv_handle* h, int from, const double* concIn, double* concOut
 
 void average(fv_handle* h, int from, const double* concIn, double* concOut, double ownWeight) {
     const int ns = h->cfg.n_species;
-    const bool vdw = h->cfg.eos == FV_EOS_VAN_DER_WAALS;
+    const int e = fvEosTemplate(h->cfg.eos);
+#define FV_AVG(N)                                                                                           \
+    (e == 0 ? launchAverage<N, 0>(h, from, concIn, concOut, ownWeight)                                      \
+            : e == 1 ? launchAverage<N, 1>(h, from, concIn, concOut, ownWeight)                             \
+                     : launchAverage<N, kEosGeneral>(h, from, concIn, concOut, ownWeight))
     switch (ns) {
-    case 1: vdw ? launchAverage<1, 1>(h, from, concIn, concOut, ownWeight) : launchAverage<1, 0>(h, from, concIn, concOut, ownWeight); break;
-    case 2: vdw ? launchAverage<2, 1>(h, from, concIn, concOut, ownWeight) : launchAverage<2, 0>(h, from, concIn, concOut, ownWeight); break;
-    case 3: vdw ? launchAverage<3, 1>(h, from, concIn, concOut, ownWeight) : launchAverage<3, 0>(h, from, concIn, concOut, ownWeight); break;
-    default: vdw ? launchAverage<4, 1>(h, from, concIn, concOut, ownWeight) : launchAverage<4, 0>(h, from, concIn, concOut, ownWeight); break;
+    case 1: FV_AVG(1); break;
+    case 2: FV_AVG(2); break;
+    case 3: FV_AVG(3); break;
+    default: FV_AVG(4); break;
     }
+#undef FV_AVG
 }
 
 // The chemistry pass after a multi-stage average (secondOrderStepSolverRK.cpp:114-118,
@@ -446,6 +451,14 @@ cudaError_t enqueueStep(fv_handle* h, int from) {
     if (h->cfg.order == FV_ORDER_SECOND_RK) return enqueueRk2(h, from);
     if (h->cfg.order == FV_ORDER_THIRD || h->cfg.order == FV_ORDER_THIRD_CADA) return enqueueRk3(h, from);
     const StepBuffers B = buffersFor(h, from);
+    if (h->cfg.chemistry == FV_CHEM_NONE) {
+        // the step kernel's last CTA reduces the CFL partials and advances the clock
+        StepParams Pf = h->P;
+        Pf.fuseFinalize = 1;
+        cudaError_t e = h->cfg.precision == FV_PREC_F64 ? launchStepF64(Pf, B, h->path, h->shape, h->stream)
+                                                         : launchStepF32(Pf, B, h->path, h->shape, h->stream);
+        return e != cudaSuccess ? e : cudaGetLastError();
+    }
     cudaError_t e = h->cfg.precision == FV_PREC_F64 ? launchStepF64(h->P, B, h->path, h->shape, h->stream)
                                                      : launchStepF32(h->P, B, h->path, h->shape, h->stream);
     if (e != cudaSuccess) return e;
@@ -496,6 +509,7 @@ fv_status ensureScratch(fv_handle* h) {
 
 int choosePath(const fv_config& c) {
     if (c.dims < 2) return PATH_GENERIC;
+    if (c.eos != FV_EOS_IDEAL && c.eos != FV_EOS_VAN_DER_WAALS) return PATH_GENERIC;  // real-gas mixtures
     if (c.order == FV_ORDER_THIRD || c.order == FV_ORDER_THIRD_CADA) return PATH_GENERIC;  // directional slopes: k_faces3
     for (int a = 0; a < c.dims; ++a)
         if (c.n[a] < 2) return PATH_GENERIC;
@@ -568,28 +582,7 @@ fv_status fv_create(const fv_config* cfg, fv_handle** out) {
     P.courant = cfg->courant;
     P.min_dt = cfg->min_timestep;
     P.const_dt = cfg->const_timestep;
-    MixParams& mp = P.mix;
-    mp.ns = cfg->n_species;
-    mp.eos_kind = cfg->eos;
-    mp.R = cfg->R;
-    for (int k = 0; k < cfg->n_species; ++k) {
-        mp.M[k] = cfg->M[k];
-        mp.invM[k] = 1.0 / cfg->M[k];
-        mp.Cv[k] = cfg->Cv[k];
-    }
-    if (cfg->eos == FV_EOS_VAN_DER_WAALS) {
-        // mixtureVanDerWaals.cpp:33-52
-        for (int k = 0; k < cfg->n_species; ++k) {
-            mp.b[k][k] = cfg->Tc[k] * mp.R / (8 * cfg->Pc[k]);
-            mp.a[k][k] = cfg->Pc[k] * mp.b[k][k] * mp.b[k][k] * 27;
-        }
-        for (int k = 0; k < cfg->n_species; ++k)
-            for (int l = 0; l < cfg->n_species; ++l)
-                if (k != l) {
-                    mp.b[k][l] = std::pow(0.5 * (std::cbrt(mp.b[k][k]) + std::cbrt(mp.b[l][l])), 3);
-                    mp.a[k][l] = std::sqrt(mp.a[k][k] * mp.a[l][l]);
-                }
-    }
+    fvMixParams(*cfg, P.mix);
     for (int p = 0; p < 6; ++p) {
         for (int k = 0; k < FV_MAX_SPECIES; ++k) {
             P.bc.conc[p][k] = cfg->bc_conc[p][k];
@@ -604,10 +597,12 @@ fv_status fv_create(const fv_config* cfg, fv_handle** out) {
     P.nmom = cfg->dims;
     // rows are staged with 16-byte aligned bulk copies: field and row pitches must be even
     P.tma = (P.n[0] % 2 == 0) ? 1 : 0;
-    // the warp-strip march addresses fields with 32-bit offsets
-    P.warp2d = (cfg->precision == FV_PREC_F32_FLUX && cfg->dims == 2 &&
-                P.ncell * (cfg->n_species + 5) < (1LL << 31)) ? 1 : 0;
-    if (P.warp2d) P.tma = 1;
+    // 2D steps of the fused march run the warp-strip layout (FP32 flux: fv_warp2d.cuh, whose
+    // fields are addressed with 32-bit offsets; FP64: fv_warp2d64.cuh); the FP32 one stages rows
+    // by 8-byte copies, so its staging needs no even row length
+    P.warp2d = (cfg->dims == 2 && (cfg->precision == FV_PREC_F64 || P.ncell * (cfg->n_species + 5) < (1LL << 31)))
+                   ? 1 : 0;
+    if (P.warp2d && cfg->precision == FV_PREC_F32_FLUX) P.tma = 1;
     P.hancock = cfg->order == FV_ORDER_SECOND ? 1 : 0;
     P.third = (cfg->order == FV_ORDER_THIRD || cfg->order == FV_ORDER_THIRD_CADA) ? 1 : 0;
     P.cada = cfg->order == FV_ORDER_THIRD_CADA ? 1 : 0;
@@ -728,12 +723,12 @@ void fv_destroy(fv_handle* h) {
 static fv_status setMomentumComponents(fv_handle* h) {
     int nmom = h->cfg.dims;
     if (h->cfg.dims < 3) {
-        FV_CUDA(h, cudaMemsetAsync(&h->ck->pad, 0, sizeof(int), h->stream));
+        FV_CUDA(h, cudaMemsetAsync(&h->ck->flag, 0, sizeof(int), h->stream));
         const unsigned g = (unsigned)((h->P.ncell + 255) / 256);
-        k_transverse<<<g, 256, 0, h->stream>>>(h->P, h->prim0, &h->ck->pad);
+        k_transverse<<<g, 256, 0, h->stream>>>(h->P, h->prim0, &h->ck->flag);
         FV_CUDA(h, cudaGetLastError());
         int flag = 0;
-        FV_CUDA(h, cudaMemcpyAsync(&flag, &h->ck->pad, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        FV_CUDA(h, cudaMemcpyAsync(&flag, &h->ck->flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
         FV_CUDA(h, cudaStreamSynchronize(h->stream));
         if (flag) nmom = 3;
         // a fixed-value patch velocity with a transverse component feeds the transverse momentum
@@ -747,6 +742,8 @@ static fv_status setMomentumComponents(fv_handle* h) {
     if (nmom != h->P.nmom) {
         h->P.nmom = nmom;
         destroyGraphs(h);
+        // the kernel choice depends on the carried momenta (warp strip with two): configure it
+        return ensureScratch(h);
     }
     return FV_OK;
 }
@@ -978,7 +975,7 @@ long long fv_kernels_per_step(const fv_handle* h) {
     if (h->cfg.order == FV_ORDER_SECOND_RK) return 2 * stage + 2 + chem;  // two stages, average, finalize
     if (h->cfg.order == FV_ORDER_THIRD || h->cfg.order == FV_ORDER_THIRD_CADA)
         return 3 * stage + 3 + chem;  // three stages, two averages, finalize
-    return stage + 1 + chem;
+    return chem ? stage + 2 : stage;  // without chemistry the step kernel finalizes itself
 }
 
 // ---- introspection used by the tests and the bench (no reference counterpart)
@@ -999,7 +996,7 @@ fv_status fv_set_staging(fv_handle* h, int on) {
     if (!h) return FV_ERR_INIT;
     // the CTA march stages rows by 16-byte bulk copies (nx even); the warp-strip march copies
     // 8 bytes per lane
-    const int want = (on && (h->P.n[0] % 2 == 0 || h->P.warp2d)) ? 1 : 0;
+    const int want = (on && (h->P.n[0] % 2 == 0 || (h->P.warp2d && h->cfg.precision == FV_PREC_F32_FLUX))) ? 1 : 0;
     if (want != h->P.tma) {
         h->P.tma = want;
         destroyGraphs(h);

@@ -17,6 +17,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <math_constants.h>
 #include <stdint.h>
 
 #include "../../include/fvstep.h"
@@ -71,9 +72,17 @@ struct MixParams {
     double M[MAXS];
     double invM[MAXS];  // 1 / M (FP32-flux arithmetic only)
     double Cv[MAXS];
-    double a[MAXS][MAXS];
-    double b[MAXS][MAXS];
+    double a[MAXS][MAXS];   // van der Waals / Redlich-Kwong a
+    double b[MAXS][MAXS];   // van der Waals / Redlich-Kwong / Kataoka b
+    double p0[MAXS][MAXS];  // stiffened p0
+    double g[MAXS][MAXS];   // stiffened gamma
+    double V0[MAXS][MAXS];  // Kataoka V0
+    double ep[MAXS][MAXS];  // Kataoka eps
 };
+
+// Template value of the EOS parameter for the three real-gas mixtures chosen at run time by
+// MixParams::eos_kind (Redlich-Kwong, stiffened, Kataoka): they run on the generic path only.
+constexpr int kEosGeneral = 9;
 
 template <typename T, int NS, int EOS>
 struct Mixture {
@@ -102,19 +111,32 @@ struct Mixture {
                 }
         }
     }
-    __device__ __forceinline__ static T pFromUv(const MixParams& mp, const T* c, T Uv) {
+    // The mixture coefficients of one set of concentrations.  The reference recomputes them in
+    // every EOS call; computing them once per state and passing them on gives the same bits (the
+    // same operations on the same values) with fewer divisions.
+    struct Coef {
         T g1, am, bm, Mm;
-        params(mp, c, g1, am, bm, Mm);
-        if (EOS == FV_EOS_IDEAL) return g1 * Uv;
-        const T acc = am * (c[0] * c[0]);
-        return g1 * (Uv + acc) / (T(1) - c[0] * bm) - acc;
+    };
+    __device__ __forceinline__ static Coef coef(const MixParams& mp, const T* c) {
+        Coef k;
+        params(mp, c, k.g1, k.am, k.bm, k.Mm);
+        return k;
+    }
+    __device__ __forceinline__ static T pFromUv(const Coef& k, const T* c, T Uv) {
+        if (EOS == FV_EOS_IDEAL) return k.g1 * Uv;
+        const T acc = k.am * (c[0] * c[0]);
+        return k.g1 * (Uv + acc) / (T(1) - c[0] * k.bm) - acc;
+    }
+    __device__ __forceinline__ static T UvFromp(const Coef& k, const T* c, T p) {
+        if (EOS == FV_EOS_IDEAL) return p / k.g1;
+        const T acc = k.am * (c[0] * c[0]);
+        return (p + acc) * (T(1) - c[0] * k.bm) / k.g1 - acc;
+    }
+    __device__ __forceinline__ static T pFromUv(const MixParams& mp, const T* c, T Uv) {
+        return pFromUv(coef(mp, c), c, Uv);
     }
     __device__ __forceinline__ static T UvFromp(const MixParams& mp, const T* c, T p) {
-        T g1, am, bm, Mm;
-        params(mp, c, g1, am, bm, Mm);
-        if (EOS == FV_EOS_IDEAL) return p / g1;
-        const T acc = am * (c[0] * c[0]);
-        return (p + acc) * (T(1) - c[0] * bm) / g1 - acc;
+        return UvFromp(coef(mp, c), c, p);
     }
     // idealFluid.cpp:37-41, vanDerWaalsFluid.cpp:44-48 with Cv_mix = sum X_k Cv_k
     __device__ __forceinline__ static T TFromUv(const MixParams& mp, const T* c, T Uv) {
@@ -133,15 +155,286 @@ struct Mixture {
         return (Uv + am * (c[0] * c[0])) / ((c[0] + Num<T>::stab()) * Cvm);
     }
     // sqSonicSpeed = dpdrho + dpdUv * (Uv + p) / rho
-    __device__ __forceinline__ static T sqSonic(const MixParams& mp, const T* c, T rho, T Uv, T p) {
-        T g1, am, bm, Mm;
-        params(mp, c, g1, am, bm, Mm);
-        if (EOS == FV_EOS_IDEAL) return T(0) + g1 * (Uv + p) / rho;
-        const T m_cb = T(1) - c[0] * bm;
-        const T ac = am * c[0];
-        const T dpdrho = (g1 * (T(2) * ac / m_cb - bm * (Uv + ac * c[0]) / (m_cb * m_cb)) - T(2) * ac) / Mm;
-        const T dUv = g1 / m_cb;
+    __device__ __forceinline__ static T sqSonic(const Coef& k, const T* c, T rho, T Uv, T p) {
+        if (EOS == FV_EOS_IDEAL) return T(0) + k.g1 * (Uv + p) / rho;
+        const T m_cb = T(1) - c[0] * k.bm;
+        const T ac = k.am * c[0];
+        const T dpdrho = (k.g1 * (T(2) * ac / m_cb - k.bm * (Uv + ac * c[0]) / (m_cb * m_cb)) - T(2) * ac) / k.Mm;
+        const T dUv = k.g1 / m_cb;
         return dpdrho + dUv * (Uv + p) / rho;
+    }
+    __device__ __forceinline__ static T sqSonic(const MixParams& mp, const T* c, T rho, T Uv, T p) {
+        return sqSonic(coef(mp, c), c, rho, Uv, p);
+    }
+};
+
+// ------------------------------------------------------------------ real-gas mixtures
+// Redlich-Kwong (mixtureRedlichKwong.cpp, RedlichKwongFluid.cpp), stiffened (mixtureStiffened.cpp,
+// stiffenedFluid.cpp) and Kataoka-van der Waals (mixtureKataokaVanDerWaals.cpp,
+// KataokaVanDerWaalsFluid.cpp) in FP64 whatever the step's arithmetic, each expression in the
+// reference's operation order.  The Redlich-Kwong cubic is solved in FP64 where the reference uses
+// long double (cubicEquationSolver.cpp), and the device's transcendental functions round their
+// last bit differently from the host's, so these agree with the reference to rounding, not bit
+// for bit.  A cubic without a single positive root (the reference's positivnessError) gives NaN,
+// which the flux reports as a Riemann solver error.
+namespace realgas {
+
+__device__ __forceinline__ int signOf(double v) {  // sign.cpp
+    const double z = kStabD();
+    if (v > z) return 1;
+    if (v < -z) return -1;
+    return 0;
+}
+
+// cubicEquationSolver + returnSinglePosValue: the single positive root of A x^3 + B x^2 + C x + D
+__device__ inline double cubicPositiveRoot(double A, double B, double C, double D) {
+    const double z = kStabD();
+    const double third = 1. / 3., twoThirds = 2. / 3.;
+    const double pi = 3.141592653589793;  // acos(-1)
+    double x[3] = {CUDART_NAN, CUDART_NAN, CUDART_NAN};
+    if ((A > 1E-9) || (A < -1E-9)) {
+        const double a = B / A, b = C / A, c = D / A;
+        const double Q = (a * a - 3 * b) / 9;
+        const double R = (a * (2 * (a * a) - 9 * b) + 27 * c) / 54;
+        const double S = (Q * Q) * Q - R * R;
+        if (S >= z) {
+            const double phi = third * acos(R / sqrt(Q * Q * Q));
+            x[0] = -2. * sqrt(Q) * cos(phi) - a * third;
+            x[1] = -2. * sqrt(Q) * cos(phi - twoThirds * pi) - a * third;
+            x[2] = -2. * sqrt(Q) * cos(phi + twoThirds * pi) - a * third;
+        } else if ((S < z) && (S >= -z)) {
+            x[0] = -2. * signOf(R) * sqrt(Q) - a * third;
+            x[1] = signOf(R) * sqrt(Q) - a * third;
+            x[2] = x[1];
+        } else if (S < -z) {
+            if (Q >= z) {
+                const double phi = third * acosh(fabs(R) / (sqrt((Q * Q) * Q) + z));
+                x[0] = -2. * signOf(R) * sqrt(Q) * cosh(phi) - a * third;
+            } else if ((Q < z) && (Q >= -z)) {
+                x[0] = -cbrt(c - (a * a) * a / 27) - a * third;
+            } else if (Q < -z) {
+                const double phi = third * asinh(fabs(R) / (sqrt(fabs((Q * Q) * Q)) + z));
+                x[0] = -2. * signOf(R) * sqrt(fabs(Q)) * sinh(phi) - a * third;
+            }
+        }
+    } else {
+        const double a = B, b = C, c = D;
+        const double Discr = b * b - 4 * a * c;
+        if (Discr >= 0) {
+            const double a2 = 0.5 / (a + z);
+            x[0] = a2 * (-b + sqrt(Discr));
+            x[1] = a2 * (-b - sqrt(Discr));
+        }
+    }
+    int nPositive = 0;
+    for (int i = 0; i < 3; ++i) {
+        if (x[i] >= 0) nPositive++;
+        else x[i] = -123.;
+    }
+    if (nPositive == 1) return fmax(fmax(x[0], x[1]), x[2]);
+    if (nPositive == 2) {
+        if (((x[0] - x[1]) < z) && (x[2] < 0)) return x[0];
+        if (((x[1] - x[2]) < z) && (x[0] < 0)) return x[1];
+        if (((x[0] - x[2]) < z) && (x[1] < 0)) return x[2];
+    } else if (nPositive == 3 && ((x[0] - x[1]) < z) && ((x[1] - x[2]) < z)) {
+        return x[0];
+    }
+    return CUDART_NAN;
+}
+
+// Kataoka cluster series, M = 13 terms; the derivative series of the reference run no term
+constexpr double kKataokaTerms = 13;
+__device__ inline double kqa(double c, double T, double V0, double eps, double R) {
+    const double V0c = V0 * c, epsRT = 0.5 * eps / (R * T);
+    double series = 1.0;
+    for (int J = 2; J <= (int)kKataokaTerms; ++J) series += pow(V0c, (J - 1.) / 3.) * exp((J - 1.) * epsRT);
+    return series;
+}
+__device__ inline double kUvA(double c, double T, double V0, double eps, double R) {
+    const double V0c = V0 * c, epsRT = 0.5 * eps / (R * T);
+    double series = 0;
+    for (int J = 2; J <= (int)kKataokaTerms; ++J) series -= (J - 1.) * pow(V0c, (J - 1.) / 3.) * exp((J - 1.) * epsRT);
+    return 0.5 * c * eps * series / kqa(c, T, V0, eps, R);
+}
+__device__ inline double kpA(double c, double T, double V0, double eps, double R) {
+    const double V0c = V0 * c, epsRT = 0.5 * eps / (R * T);
+    double series = 0;
+    for (int J = 2; J <= (int)kKataokaTerms; ++J)
+        series -= (J - 1.) / 3. * pow(V0c, (J - 1.) / 3.) * exp((J - 1.) * epsRT);
+    return c * R * T * series / kqa(c, T, V0, eps, R);
+}
+__device__ inline double kdPdC(double c, double T, double V0, double eps, double R, double b) {
+    const double V0c = V0 * c, n13 = 0.0, qa1 = kqa(c, T, V0, eps, R);
+    return R * T / (1 - c * b) + c * R * T * b / ((1 - c * b) * (1 - c * b)) +
+           (R * T * n13 + V0c * R * T * (0.0 - n13 * 0.0 / qa1)) / qa1;
+}
+__device__ inline double kdPdT(double c, double T, double V0, double eps, double R, double b) {
+    const double n13 = 0.0, qa1 = kqa(c, T, V0, eps, R);
+    return c * R / (1 - c * b) + (c * R * n13 + 0.5 * c * eps / T * (0.0 - n13 * 0.0 / qa1)) / qa1;
+}
+__device__ inline double kdUvdC(double c, double Cv, double T, double V0, double eps, double R) {
+    const double V0c = V0 * c, n13 = 0.0, qa1 = kqa(c, T, V0, eps, R);
+    return Cv * T + (0.5 * eps * n13 + 0.5 * V0c * eps * (0.0 - n13 * 0.0 / qa1)) / qa1;
+}
+__device__ inline double kdUvdT(double c, double Cv, double T, double V0, double eps, double R) {
+    const double qa1 = kqa(c, T, V0, eps, R), s2 = 0.0;
+    return c * Cv + 0.25 * c * (eps * eps) / (R * (T * T)) * 0.0 / qa1 -
+           0.25 * c * (eps * eps) / (R * (T * T)) * (s2 * s2) / (qa1 * qa1);
+}
+// NewtonMethod.cpp:13-40 on T (tolerance 1e-12, at most 100 further iterations)
+template <class F, class DF> __device__ inline double newton(double x1, F f, DF df) {
+    double x2 = x1 - f(x1) / df(x1);
+    if (fabs(x2 - x1) <= 1E-12) return x2;
+    for (int it = 1; fabs(x2 - x1) > 1E-12 && it <= 100; ++it) {
+        x1 = x2;
+        x2 = x1 - f(x1) / df(x1);
+    }
+    return x2;
+}
+__device__ inline double kTFromUv(double c, double Cv, double Uv, double V0, double eps, double R) {
+    auto f = [&](double T) { return c * Cv * T + kUvA(c, T, V0, eps, R) - Uv; };
+    auto df = [&](double T) { return kdUvdT(c, Cv, T, V0, eps, R); };
+    return newton(Uv / ((c + kStabD()) * Cv), f, df);
+}
+// Redlich-Kwong derivatives (RedlichKwongFluid.cpp:14-44)
+__device__ inline double rkdPdC(double c, double T, double a, double b, double R) {
+    return R * T / (1 - c * b) + c * R * T * b / ((1 - c * b) * (1 - c * b)) - 2 * a * c / (sqrt(T) * (1 + b * c)) +
+           a * (c * c) * b / (sqrt(T) * ((1 + b * c) * (1 + b * c)));
+}
+__device__ inline double rkdPdT(double c, double T, double a, double b, double R) {
+    const double sT = sqrt(T);
+    return c * R / (1 - c * b) + 0.5 * a * (c * c) / (((sT * sT) * sT) * (1 + c * b));
+}
+__device__ inline double rkdUvdC(double c, double Cv, double T, double a, double b) {
+    return Cv * T - 1.5 * a * log1p(c * b) / (b * sqrt(T)) - 1.5 * a * c / (sqrt(T) * (1 + c * b));
+}
+__device__ inline double rkdUvdT(double c, double Cv, double T, double a, double b) {
+    const double sT = sqrt(T);
+    return c * Cv + 0.75 * a * c * log1p(c * b) / (b * ((sT * sT) * sT));
+}
+__device__ inline double rkSqrtT(double c, double Cv, double Uv, double a, double b) {
+    return cubicPositiveRoot(c * Cv, 0, -Uv, -1.5 * a * c / b * log1p(c * b));
+}
+
+}  // namespace realgas
+
+template <typename T, int NS>
+struct Mixture<T, NS, kEosGeneral> {
+    // the mixture sums of one set of concentrations (X_k = c_k / c_0), with the EOS kind and R
+    struct Coef {
+        int kind;
+        double R, c0, Cvm, Mm;  // gas constant, total concentration, Cv and M of the mixture
+        double a, b;            // Redlich-Kwong a and b; Kataoka b
+        double p0, g;           // stiffened p0 and gamma
+        double V0, ep;          // Kataoka V0 and eps
+    };
+    __device__ __forceinline__ static Coef coef(const MixParams& mp, const T* c) {
+        Coef k{};
+        k.kind = mp.eos_kind;
+        k.R = mp.R;
+        k.c0 = double(c[0]);
+        double X[NS];
+#pragma unroll
+        for (int q = 0; q < NS; ++q) X[q] = double(c[q + 1]) / double(c[0]);
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+            k.Cvm += X[q] * mp.Cv[q];
+            k.Mm += X[q] * mp.M[q];
+        }
+#pragma unroll
+        for (int q = 0; q < NS; ++q)
+#pragma unroll
+            for (int l = 0; l < NS; ++l) {
+                if (k.kind == FV_EOS_STIFFENED) {
+                    k.p0 += X[q] * X[l] * mp.p0[q][l];
+                    k.g += X[q] * X[l] * mp.g[q][l];
+                } else if (k.kind == FV_EOS_KATAOKA) {
+                    k.V0 += X[q] * X[l] * mp.V0[q][l];
+                    k.ep += X[q] * X[l] * mp.ep[q][l];
+                    k.b += X[q] * X[l] * mp.b[q][l];
+                } else {
+                    k.a += X[q] * X[l] * mp.a[q][l];
+                    k.b += X[q] * X[l] * mp.b[q][l];
+                }
+            }
+        return k;
+    }
+    // stiffenedFluid.cpp:13-17, RedlichKwongFluid.cpp:46-56, KataokaVanDerWaalsFluid.cpp:237-256
+    __device__ __noinline__ static double pFromUvD(const Coef& k, double Uv) {
+        const double c = k.c0;
+        if (k.kind == FV_EOS_STIFFENED) return (k.g - 1.0) * Uv - k.p0 * k.g;
+        if (k.kind == FV_EOS_KATAOKA) {
+            const double Tk = realgas::kTFromUv(c, k.Cvm, Uv, k.V0, k.ep, k.R);
+            return c * k.R * Tk / (1 - c * k.b) + realgas::kpA(c, Tk, k.V0, k.ep, k.R);
+        }
+        const double sT = realgas::rkSqrtT(c, k.Cvm, Uv, k.a, k.b);
+        return c * k.R * (sT * sT) / (1 - c * k.b) - k.a * (c * c) / (sT * (1 + c * k.b));
+    }
+    // stiffenedFluid.cpp:19-23, RedlichKwongFluid.cpp:58-68, KataokaVanDerWaalsFluid.cpp:258-277
+    __device__ __noinline__ static double UvFrompD(const Coef& k, double p) {
+        const double c = k.c0;
+        if (k.kind == FV_EOS_STIFFENED) return (p + k.p0 * k.g) / (k.g - 1.0);
+        if (k.kind == FV_EOS_KATAOKA) {
+            const double V0 = k.V0, ep = k.ep, R = k.R, b = k.b;
+            auto f = [&](double Tk) { return c * R * Tk / (1 - c * b) + realgas::kpA(c, Tk, V0, ep, R) - p; };
+            auto df = [&](double Tk) { return realgas::kdPdT(c, Tk, V0, ep, R, b); };
+            const double Tk = realgas::newton(p / ((c + kStabD()) * R), f, df);
+            return c * k.Cvm * Tk + realgas::kUvA(c, Tk, V0, ep, R);
+        }
+        const double sT = realgas::cubicPositiveRoot(c * k.R, 0, -p * (1 - c * k.b),
+                                                     -k.a * (c * c) * (1 - c * k.b) / (1 + c * k.b));
+        return c * k.Cvm * (sT * sT) - 1.5 * k.a * c / (k.b * sT) * log1p(c * k.b);
+    }
+    // sqSonicSpeed = dpdrho + dpdUv (Uv + p) / rho
+    __device__ __noinline__ static double sqSonicD(const Coef& k, double rho, double Uv, double p) {
+        const double c = k.c0;
+        if (k.kind == FV_EOS_STIFFENED) return 0 + (k.g - 1.0) * (Uv + p) / rho;
+        if (k.kind == FV_EOS_KATAOKA) {  // KataokaVanDerWaalsFluid.cpp:332-372
+            const double Tk = realgas::kTFromUv(c, k.Cvm, Uv, k.V0, k.ep, k.R);
+            const double dpdrho = (realgas::kdPdC(c, Tk, k.V0, k.ep, k.R, k.b) -
+                                   realgas::kdPdT(c, Tk, k.V0, k.ep, k.R, k.b) *
+                                       realgas::kdUvdC(c, k.Cvm, Tk, k.V0, k.ep, k.R) /
+                                       realgas::kdUvdT(c, k.Cvm, Tk, k.V0, k.ep, k.R)) /
+                                  k.Mm;
+            const double dpdUv =
+                realgas::kdPdT(c, Tk, k.V0, k.ep, k.R, k.b) / realgas::kdUvdT(c, k.Cvm, Tk, k.V0, k.ep, k.R);
+            return dpdrho + dpdUv * (Uv + p) / rho;
+        }
+        // RedlichKwongFluid.cpp:104-131
+        const double sT = realgas::rkSqrtT(c, k.Cvm, Uv, k.a, k.b);
+        const double Tr = sT * sT;
+        const double dpdrho = (realgas::rkdPdC(c, Tr, k.a, k.b, k.R) -
+                               realgas::rkdPdT(c, Tr, k.a, k.b, k.R) * realgas::rkdUvdC(c, k.Cvm, Tr, k.a, k.b) /
+                                   realgas::rkdUvdT(c, k.Cvm, Tr, k.a, k.b)) /
+                              k.Mm;
+        const double dpdUv = realgas::rkdPdT(c, Tr, k.a, k.b, k.R) / realgas::rkdUvdT(c, k.Cvm, Tr, k.a, k.b);
+        return dpdrho + dpdUv * (Uv + p) / rho;
+    }
+    // stiffenedFluid.cpp:37-41, RedlichKwongFluid.cpp:84-92, KataokaVanDerWaalsFluid.cpp:291-306
+    __device__ __noinline__ static double TFromUvD(const Coef& k, double Uv) {
+        const double c = k.c0;
+        if (k.kind == FV_EOS_STIFFENED) return (Uv - k.p0) / ((c + kStabD()) * k.Cvm);
+        if (k.kind == FV_EOS_KATAOKA) return realgas::kTFromUv(c, k.Cvm, Uv, k.V0, k.ep, k.R);
+        const double sT = realgas::rkSqrtT(c, k.Cvm, Uv, k.a, k.b);
+        return sT * sT;
+    }
+
+    __device__ __forceinline__ static T pFromUv(const Coef& k, const T*, T Uv) { return T(pFromUvD(k, double(Uv))); }
+    __device__ __forceinline__ static T UvFromp(const Coef& k, const T*, T p) { return T(UvFrompD(k, double(p))); }
+    __device__ __forceinline__ static T sqSonic(const Coef& k, const T*, T rho, T Uv, T p) {
+        return T(sqSonicD(k, double(rho), double(Uv), double(p)));
+    }
+    __device__ __forceinline__ static T pFromUv(const MixParams& mp, const T* c, T Uv) {
+        return pFromUv(coef(mp, c), c, Uv);
+    }
+    __device__ __forceinline__ static T UvFromp(const MixParams& mp, const T* c, T p) {
+        return UvFromp(coef(mp, c), c, p);
+    }
+    __device__ __forceinline__ static T sqSonic(const MixParams& mp, const T* c, T rho, T Uv, T p) {
+        return sqSonic(coef(mp, c), c, rho, Uv, p);
+    }
+    __device__ __forceinline__ static T TFromUv(const MixParams& mp, const T* c, T Uv) {
+        return T(TFromUvD(coef(mp, c), double(Uv)));
     }
 };
 
@@ -230,8 +523,10 @@ struct FaceState {
 };
 
 // Closure of a reconstructed primitive state (Advection.cpp:238-303 / :305-387).
+// `known`: the mixture coefficients of these concentrations when the caller has them already.
 template <typename T, int NS, int EOS>
-__device__ __forceinline__ void closeFromPrimitive(const MixParams& mp, FaceState<T, NS>& s) {
+__device__ __forceinline__ void closeFromPrimitive(const MixParams& mp, FaceState<T, NS>& s,
+                                                   const typename Mixture<T, NS, EOS>::Coef* known = nullptr) {
     s.c[0] = 0;
     s.rho[0] = 0;
 #pragma unroll
@@ -240,7 +535,7 @@ __device__ __forceinline__ void closeFromPrimitive(const MixParams& mp, FaceStat
         s.rho[k] = s.c[k] * T(mp.M[k - 1]);
         s.rho[0] += s.rho[k];
     }
-    s.Uv = Mixture<T, NS, EOS>::UvFromp(mp, s.c, s.p);
+    s.Uv = known ? Mixture<T, NS, EOS>::UvFromp(*known, s.c, s.p) : Mixture<T, NS, EOS>::UvFromp(mp, s.c, s.p);
 #pragma unroll
     for (int d = 0; d < 3; ++d) s.m[d] = s.v[d] * s.rho[0];
     T v2 = 0;
@@ -253,8 +548,10 @@ __device__ __forceinline__ void closeFromPrimitive(const MixParams& mp, FaceStat
 // Recalculation from conserved face values (HancockStage.cpp:177-224, Advection.cpp:455-479).
 // `nmom` momentum components are carried; the others are exactly zero and so is their
 // velocity (0 / rho = +0 for a positive density).
+// `out`: receives the mixture coefficients of the new concentrations (for soundSpeed).
 template <typename T, int NS, int EOS>
-__device__ __forceinline__ void closeFromConserved(const MixParams& mp, FaceState<T, NS>& s, int nmom = 3) {
+__device__ __forceinline__ void closeFromConserved(const MixParams& mp, FaceState<T, NS>& s, int nmom = 3,
+                                                   typename Mixture<T, NS, EOS>::Coef* out = nullptr) {
     s.c[0] = 0;
 #pragma unroll
     for (int k = 1; k <= NS; ++k) {
@@ -268,13 +565,19 @@ __device__ __forceinline__ void closeFromConserved(const MixParams& mp, FaceStat
     v2 += s.v[1] * s.v[1];
     v2 += s.v[2] * s.v[2];
     s.Uv = s.E - s.rho[0] * v2 * T(0.5) - T(0);
-    s.p = Mixture<T, NS, EOS>::pFromUv(mp, s.c, s.Uv);
+    const typename Mixture<T, NS, EOS>::Coef k = Mixture<T, NS, EOS>::coef(mp, s.c);
+    s.p = Mixture<T, NS, EOS>::pFromUv(k, s.c, s.Uv);
+    if (out) *out = k;
 }
 
 // Sound speed of HLLCSolver.cpp:26-50 with zero turbulent energy.
 template <typename T, int NS, int EOS>
 __device__ __forceinline__ void soundSpeed(const MixParams& mp, FaceState<T, NS>& s) {
     s.cs = Num<T>::sqrt_(Mixture<T, NS, EOS>::sqSonic(mp, s.c, s.rho[0], s.Uv, s.p) + T(0));
+}
+template <typename T, int NS, int EOS>
+__device__ __forceinline__ void soundSpeed(const typename Mixture<T, NS, EOS>::Coef& k, FaceState<T, NS>& s) {
+    s.cs = Num<T>::sqrt_(Mixture<T, NS, EOS>::sqSonic(k, s.c, s.rho[0], s.Uv, s.p) + T(0));
 }
 
 // ------------------------------------------------------------------ boundary conditions

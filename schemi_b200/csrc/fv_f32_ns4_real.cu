@@ -1,7 +1,8 @@
-// FP32-flux step kernels for 4 species: reconstruction, closures and fluxes in FP32 (fast
+// FP32-flux step kernels for 4 species, the real-gas mixtures (Redlich-Kwong, stiffened, Kataoka; generic path): reconstruction, closures and fluxes in FP32 (fast
 // math), conserved variables read, accumulated and stored in FP64.
 #define FV_T float
 #define FV_NS 4
+#define FV_EOS 9
 #define FV_LAUNCH_NAME launchStepF32
 #define FV_BATCH_NAME launchBatchF32
 #define FV_SMEM_NAME marchSmemF32

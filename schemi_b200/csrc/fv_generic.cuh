@@ -948,6 +948,7 @@ __global__ void k_update(const StepParams P, const GenericLayout L, const double
     }
     const T bm = blockMaxReduce<T>(localMax, red);
     if (threadIdx.x == 0) blockMax[blockIdx.x] = double(bm);
+    if (P.fuseFinalize) finalizeIfLast(P, ck, blockMax, (int)gridDim.x, gridDim.x);
 }
 
 }  // namespace fv

@@ -60,6 +60,8 @@ struct StepParams {
     double min_dt;
     double const_dt;     // > 0: constant time step (main skips its CFL block)
     double ext[3];          // parallelepiped extents (the transverse sizes of 1D / 2D cells)
+    int fuseFinalize;       // 1: the step kernel's last CTA runs the CFL finalize (no k_finalize launch)
+    int pad0;
     MixParams mix;
     BCParams bc;
     Geometry geo;
@@ -78,6 +80,9 @@ struct DevClock {
     int done;           // time >= t_end: further steps are no-ops
     int err;            // fv_error_code raised by a kernel
     int first;          // 1 until the first step: primitives come from the uploaded restart set
+    unsigned ticket;    // CTAs of the running step that have written their CFL partials (fused
+                        // finalize); the last one resets it to 0
+    int flag;           // scratch word of host-side checks (the transverse-velocity test of an upload)
     int pad;
 };
 
@@ -117,9 +122,14 @@ __device__ __forceinline__ Src globalSrc(const StepParams& P, const double* __re
 
 // Primitive recovery of a cell from its conserved state (Advection.cpp:455-479), or the
 // uploaded restart primitives before the first step (phaseInitialization keeps them as read).
+// `kc` (optional) receives the mixture coefficients of c when c is computed here from the
+// densities (its c_0 then being the sum that closeFromPrimitive forms again); *haveK says so.
 template <typename T, int NS, int EOS, int D>
 __device__ __forceinline__ void cellPrimitive(const StepParams& P, const Src& sc, const double* __restrict__ prim,
-                                              long long i, T* c, T* v, T& p, T& rho0, T* rho, T* m, T& E) {
+                                              long long i, T* c, T* v, T& p, T& rho0, T* rho, T* m, T& E,
+                                              typename Mixture<T, NS, EOS>::Coef* kc = nullptr,
+                                              bool* haveK = nullptr) {
+    if (haveK) *haveK = false;
     const long long s = P.stride;
 #pragma unroll
     for (int k = 1; k <= NS; ++k) rho[k] = T(sc.p[(k - 1) * sc.fs]);
@@ -159,7 +169,12 @@ __device__ __forceinline__ void cellPrimitive(const StepParams& P, const Src& sc
     v2 += v[1] * v[1];
     v2 += v[2] * v[2];
     const T Uv = E - rho0 * v2 * T(0.5) - T(0);
-    p = Mixture<T, NS, EOS>::pFromUv(P.mix, c, Uv);
+    const typename Mixture<T, NS, EOS>::Coef k = Mixture<T, NS, EOS>::coef(P.mix, c);
+    p = Mixture<T, NS, EOS>::pFromUv(k, c, Uv);
+    if (kc && !P.conc) {
+        *kc = k;
+        *haveK = true;
+    }
 }
 
 template <typename T, int NS, int EOS, int D>
@@ -171,17 +186,26 @@ __device__ __forceinline__ void cellPrimitive(const StepParams& P, const double*
 
 // Face state of a cell whose slopes vanish: closure, then (MUSCL-Hancock) the zero Hancock
 // divergence and the recalculation from conserved values, sound speed.
+// known: the mixture coefficients of c (with c_0 the sum of c_1..c_N), when the caller has them.
 template <typename T, int NS, int EOS>
 __device__ __forceinline__ void cellFaceState(const MixParams& mp, const T* c, const T* v, T p, FaceState<T, NS>& W,
-                                              int nmom = 3, bool hancock = true) {
+                                              int nmom = 3, bool hancock = true,
+                                              const typename Mixture<T, NS, EOS>::Coef* known = nullptr) {
 #pragma unroll
     for (int k = 1; k <= NS; ++k) W.c[k] = c[k];
 #pragma unroll
     for (int d = 0; d < 3; ++d) W.v[d] = v[d];
     W.p = p;
-    closeFromPrimitive<T, NS, EOS>(mp, W);
-    if (hancock) closeFromConserved<T, NS, EOS>(mp, W, nmom);
-    soundSpeed<T, NS, EOS>(mp, W);
+    closeFromPrimitive<T, NS, EOS>(mp, W, known);
+    if (hancock) {
+        typename Mixture<T, NS, EOS>::Coef k2;
+        closeFromConserved<T, NS, EOS>(mp, W, nmom, &k2);
+        soundSpeed<T, NS, EOS>(k2, W);
+    } else if (known) {
+        soundSpeed<T, NS, EOS>(*known, W);
+    } else {
+        soundSpeed<T, NS, EOS>(mp, W);
+    }
 }
 
 // FP32-flux predicted state: the closure / Hancock round trip is an identity up to rounding, so
@@ -351,8 +375,9 @@ __device__ __forceinline__ T cellSignalC(const StepParams& P, const T* c, T rho0
     v2 += v[1] * v[1];
     v2 += v[2] * v[2];
     const T Uv = E - rho0 * v2 * T(0.5) - T(0);
-    const T p = Mixture<T, NS, EOS>::pFromUv(P.mix, c, Uv);
-    const T sonic = Num<T>::sqrt_(Mixture<T, NS, EOS>::sqSonic(P.mix, c, rho0, Uv, p));
+    const typename Mixture<T, NS, EOS>::Coef k = Mixture<T, NS, EOS>::coef(P.mix, c);
+    const T p = Mixture<T, NS, EOS>::pFromUv(k, c, Uv);
+    const T sonic = Num<T>::sqrt_(Mixture<T, NS, EOS>::sqSonic(k, c, rho0, Uv, p));
     T s = (P.nmom == 3 ? mag3<T>(v[0], v[1], v[2]) : mag2z<T>(v[0], v[1])) + sonic;
     s *= minLS;
     return s;
@@ -369,6 +394,59 @@ __device__ __forceinline__ T cellSignal(const StepParams& P, const T* rho, T rho
         c[0] += c[k];
     }
     return cellSignalC<T, NS, EOS, D>(P, c, rho0, m, E, minLS);
+}
+
+// ============================================================================ finalize
+// dt = Courant / max signal; dt = min(dt, dtSource) unless Courant-only; dt = max(dt, minTime);
+// time += dt_used; g += g_delta * dt_used; clamp to t_end (Schemi.cpp:802-835, 933-935).
+// Executed by one CTA.
+__device__ __forceinline__ void finalizeCase(const StepParams& P, DevClock* ck, const double* __restrict__ blockMax,
+                                             int nblocks) {
+    __shared__ double red[32];
+    if (ck->done) return;
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+    const int nthr = blockDim.x * blockDim.y;
+    double m = -1;
+    // L2 loads: the partials may have been written by other CTAs of the same launch
+    for (int b = tid; b < nblocks; b += nthr) m = smax(m, __ldcg(blockMax + b));
+    m = blockMaxReduce<double>(m, red);
+    if (tid != 0) return;
+    const double dtUsed = ck->dt;
+    double dtn = P.courant / m;
+    if (!P.courant_only) dtn = smin(dtn, kVeryBigD());
+    dtn = smax(dtn, P.min_dt);
+    if (P.const_dt > 0) dtn = P.const_dt;  // Schemi.cpp:807: no CFL block with a constant step
+    if (P.gravity) {
+        for (int d = 0; d < 3; ++d) ck->g[d] += ck->g_delta[d] * dtUsed;
+    }
+    ck->time += dtUsed;
+    ck->steps += 1;
+    ck->first = 0;
+    ck->dt_used = dtUsed;
+    ck->dt_free = dtn;
+    if ((ck->time + dtn) > ck->t_end) dtn = ck->t_end - ck->time;
+    ck->dt = dtn;
+    if (!(ck->time < ck->t_end) || ck->err) ck->done = 1;
+}
+
+// Fused finalize at the end of a step kernel (all threads of the CTA, after its CFL partials are
+// written): each CTA takes a ticket; the CTA that takes the last of `nCtas` has every partial
+// of the step visible and runs finalizeCase, then returns the ticket counter to zero for the
+// next step.  Every CTA has read the clock before it takes its ticket, so the last one may
+// advance it.
+__device__ __forceinline__ void finalizeIfLast(const StepParams& P, DevClock* ck, const double* __restrict__ blockMax,
+                                               int nPartials, unsigned nCtas) {
+    __shared__ int isLast;
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        __threadfence();
+        isLast = atomicAdd(&ck->ticket, 1u) == nCtas - 1u;
+    }
+    __syncthreads();
+    if (!isLast) return;
+    __threadfence();
+    finalizeCase(P, ck, blockMax, nPartials);
+    if (threadIdx.x == 0 && threadIdx.y == 0) ck->ticket = 0u;
 }
 
 // ============================================================================ bulk async copies
@@ -570,8 +648,10 @@ __device__ __forceinline__ void marchTile(const StepParams& P, const double* __r
             for (int d = 0; d < 3; ++d) vp[d] = W.v[d];
         } else {
             T c[NS + 1], v[3], p, r0, rr2[NS + 1], mm[3], EE;
-            cellPrimitive<T, NS, EOS, D>(P, sc, prim, cell, c, v, p, r0, rr2, mm, EE);
-            cellFaceState<T, NS, EOS>(P.mix, c, v, p, W, nmom, P.hancock != 0);
+            typename Mixture<T, NS, EOS>::Coef kc;
+            bool haveK;
+            cellPrimitive<T, NS, EOS, D>(P, sc, prim, cell, c, v, p, r0, rr2, mm, EE, &kc, &haveK);
+            cellFaceState<T, NS, EOS>(P.mix, c, v, p, W, nmom, P.hancock != 0, haveK ? &kc : nullptr);
 #pragma unroll
             for (int d = 0; d < 3; ++d) vp[d] = v[d];
         }
@@ -815,11 +895,16 @@ __global__ void __launch_bounds__(BX* BY, MINB) k_march(const StepParams P, cons
                                                         double* __restrict__ Un, const double* __restrict__ prim0,
                                                         DevClock* __restrict__ ck, double* __restrict__ blockMax,
                                                         int rows) {
+    if (ck->done) return;  // uniform over the grid
     const long long b = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
     if (D == 2)
         marchTile<T, NS, EOS, D, BX, BY>(P, U, Un, prim0, ck, blockMax + b, rows, blockIdx.x, 0, blockIdx.y);
     else
         marchTile<T, NS, EOS, D, BX, BY>(P, U, Un, prim0, ck, blockMax + b, rows, blockIdx.x, blockIdx.y, blockIdx.z);
+    if (P.fuseFinalize) {
+        const unsigned n = gridDim.x * gridDim.y * gridDim.z;
+        finalizeIfLast(P, ck, blockMax, (int)n, n);
+    }
 }
 
 // One case of a batched ensemble (device-side case table).
@@ -863,42 +948,13 @@ __global__ void __launch_bounds__(BX* BY, MINB) k_march_batch(const BatchCase* _
         double* Uout = odd ? const_cast<double*>(C.U0) : C.U1;
         marchTile<T, NS, EOS, D, BX, BY>(C.P, Uin, Uout, C.prim0, C.ck, C.blockMax + local, rows, tx, tyy, tz);
         __syncthreads();  // shared memory is reused by the next tile
+        if (C.P.fuseFinalize) finalizeIfLast(C.P, C.ck, C.blockMax, C.nPartials, (unsigned)C.nTiles);
     }
 }
 
 // CTAs per SM the register budget of k_march is sized for.
 template <typename T, int BX, int BY> constexpr int marchMinBlocks() {
     return sizeof(T) == 8 ? (384 / (BX * BY) > 0 ? 384 / (BX * BY) : 1) : (512 / (BX * BY) > 0 ? 512 / (BX * BY) : 1);
-}
-
-// ============================================================================ finalize
-// dt = Courant / max signal; dt = min(dt, dtSource) unless Courant-only; dt = max(dt, minTime);
-// time += dt_used; g += g_delta * dt_used; clamp to t_end (Schemi.cpp:802-835, 933-935).
-// Executed by one CTA.
-__device__ __forceinline__ void finalizeCase(const StepParams& P, DevClock* ck, const double* __restrict__ blockMax,
-                                             int nblocks) {
-    __shared__ double red[32];
-    if (ck->done) return;
-    double m = -1;
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) m = smax(m, blockMax[b]);
-    m = blockMaxReduce<double>(m, red);
-    if (threadIdx.x != 0) return;
-    const double dtUsed = ck->dt;
-    double dtn = P.courant / m;
-    if (!P.courant_only) dtn = smin(dtn, kVeryBigD());
-    dtn = smax(dtn, P.min_dt);
-    if (P.const_dt > 0) dtn = P.const_dt;  // Schemi.cpp:807: no CFL block with a constant step
-    if (P.gravity) {
-        for (int d = 0; d < 3; ++d) ck->g[d] += ck->g_delta[d] * dtUsed;
-    }
-    ck->time += dtUsed;
-    ck->steps += 1;
-    ck->first = 0;
-    ck->dt_used = dtUsed;
-    ck->dt_free = dtn;
-    if ((ck->time + dtn) > ck->t_end) dtn = ck->t_end - ck->time;
-    ck->dt = dtn;
-    if (!(ck->time < ck->t_end) || ck->err) ck->done = 1;
 }
 
 __global__ void k_finalize(const StepParams P, DevClock* ck, const double* __restrict__ blockMax, int nblocks);

@@ -4,6 +4,7 @@
 
 #include "fv_generic.cuh"
 #include "fv_warp2d.cuh"
+#include "fv_warp2d64.cuh"
 
 namespace fv {
 

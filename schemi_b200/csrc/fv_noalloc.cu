@@ -158,28 +158,7 @@ bool buildParams(const fv_config& c, StepParams& P, std::string& e) {
     P.courant = c.courant;
     P.min_dt = c.min_timestep;
     P.const_dt = c.const_timestep;
-    MixParams& mp = P.mix;
-    mp.ns = c.n_species;
-    mp.eos_kind = c.eos;
-    mp.R = c.R;
-    for (int k = 0; k < c.n_species; ++k) {
-        mp.M[k] = c.M[k];
-        mp.invM[k] = 1.0 / c.M[k];
-        mp.Cv[k] = c.Cv[k];
-    }
-    if (c.eos == FV_EOS_VAN_DER_WAALS) {
-        // mixtureVanDerWaals.cpp:33-52
-        for (int k = 0; k < c.n_species; ++k) {
-            mp.b[k][k] = c.Tc[k] * mp.R / (8 * c.Pc[k]);
-            mp.a[k][k] = c.Pc[k] * mp.b[k][k] * mp.b[k][k] * 27;
-        }
-        for (int k = 0; k < c.n_species; ++k)
-            for (int l = 0; l < c.n_species; ++l)
-                if (k != l) {
-                    mp.b[k][l] = std::pow(0.5 * (std::cbrt(mp.b[k][k]) + std::cbrt(mp.b[l][l])), 3);
-                    mp.a[k][l] = std::sqrt(mp.a[k][k] * mp.a[l][l]);
-                }
-    }
+    fvMixParams(c, P.mix);
     for (int p = 0; p < 6; ++p) {
         for (int k = 0; k < FV_MAX_SPECIES; ++k) {
             P.bc.conc[p][k] = c.bc_conc[p][k];

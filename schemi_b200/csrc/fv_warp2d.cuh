@@ -667,6 +667,10 @@ __global__ void __launch_bounds__(32 * NW, MINB) k_warp2d(const StepParams P, co
     if (ck->done) return;  // uniform over the grid
     warpTile<NS, EOS, RING>(P, U, Un, ck, blockMax + (blockIdx.x + (long long)gridDim.x * blockIdx.y) * NW, rows,
                             blockIdx.x, blockIdx.y);
+    if (P.fuseFinalize) {
+        const unsigned n = gridDim.x * gridDim.y;
+        finalizeIfLast(P, ck, blockMax, (int)(n * NW), n);
+    }
 }
 
 // Ensemble version: one CTA per tile of any case (the tile list of all cases in order).
@@ -699,6 +703,7 @@ __global__ void __launch_bounds__(32 * NW, MINB) k_warp2d_batch(const BatchCase*
     }
     __syncthreads();
     warpTile<NS, EOS, RING>(sP, Uin, Uout, C.ck, C.blockMax + local * NW, rows, tx, tz);
+    if (sP.fuseFinalize) finalizeIfLast(sP, C.ck, C.blockMax, C.nPartials, (unsigned)C.nTiles);
 }
 
 }  // namespace fv

@@ -234,6 +234,15 @@ def write_deck(case: Case, directory: str, prim: Sequence[np.ndarray], frequency
     _write(sdir, "epsilon.txt", free + "\n#Values_in_zones\n" + " ".join(["0.0"] * nzv))
     _write(sdir, "a.txt", free + "\n#Values_in_zones\n" + " ".join(["0.0 0.0 0.0"] * nzv))
     _write(sdir, "b.txt", free + "\n#Values_in_zones\n" + " ".join(["0"] * nzv))
+    if case.eos == "stiffened":
+        # abstractMixtureThermodynamics.cpp:71-95: "<label> p0 gamma" per species
+        _write(sdir, "stiffenedFluidData.txt",
+               "\n".join(f"#sub_{k + 1} {_f(sp.p0)} {_f(sp.gamma)}" for k, sp in enumerate(case.species)))
+    elif case.eos == "Kataoka":
+        # abstractMixtureThermodynamics.cpp:96-143: "<label> eps sigma" per species, then the b rule
+        _write(sdir, "KataokaVanDerWaalsFluidData.txt",
+               "\n".join(f"#sub_{k + 1} {_f(sp.lj_eps)} {_f(sp.lj_sigma)}" for k, sp in enumerate(case.species))
+               + f"\n#b_calculation {case.kataoka_b[0]} {_f(case.kataoka_b[1])}")
     _write(sdir, "chemicalKinetics.txt", _chemistry_block(case))
     _write(sdir, "transportCoefficients.txt", _TRANSPORT)
     _write(sdir, "turbulentParameters.txt", _TURB_PARAMS)

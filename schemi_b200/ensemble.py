@@ -36,3 +36,25 @@ def imbalance(work: Sequence[float], shares: Sequence[Sequence[int]]) -> float:
     loads = [sum(work[i] for i in s) for s in shares]
     mean = sum(loads) / len(loads)
     return max(loads) / mean if mean > 0 else 1.0
+
+
+def combine_rank_totals(dist, device, sums: dict, maxes: dict) -> dict:
+    """Job totals of per-rank figures: `sums` (cell updates, cells) summed and `maxes` (device
+    times) maxed over the ranks of the process group `dist` (torch.distributed; None for one
+    rank).  Every rank takes the same two collectives in the same order."""
+    out = dict(sums)
+    out.update(maxes)
+    if dist is None:
+        return out
+    import torch
+
+    ks, km = sorted(sums), sorted(maxes)
+    if ks:
+        t = torch.tensor([float(sums[k]) for k in ks], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        out.update({k: float(v) for k, v in zip(ks, t.tolist())})
+    if km:
+        m = torch.tensor([float(maxes[k]) for k in km], device=device, dtype=torch.float64)
+        dist.all_reduce(m, op=dist.ReduceOp.MAX)
+        out.update({k: float(v) for k, v in zip(km, m.tolist())})
+    return out

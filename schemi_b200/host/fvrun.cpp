@@ -344,9 +344,13 @@ Deck readDeck(const std::string& dir, bool createResult) {
     if (flux == "HLLC") c.flux = FV_FLUX_HLLC;
     else if (flux == "HLL") c.flux = FV_FLUX_HLL;
     else throw Fail("#Type_of_flow_solver " + flux + ": HLLC and HLL are implemented");
+    // abstractMixtureThermodynamics.cpp:39-51
     if (d.eos == "ideal") c.eos = FV_EOS_IDEAL;
     else if (d.eos == "vanDerWaals") c.eos = FV_EOS_VAN_DER_WAALS;
-    else throw Fail("#Equation_of_state " + d.eos + ": ideal and vanDerWaals are implemented");
+    else if (d.eos == "RedlichKwong") c.eos = FV_EOS_REDLICH_KWONG;
+    else if (d.eos == "stiffened") c.eos = FV_EOS_STIFFENED;
+    else if (d.eos == "Kataoka") c.eos = FV_EOS_KATAOKA;
+    else throw Fail("Unknown type of equation of state.");
     // phaseInitialization.cpp:418-435
     if (d.units == "SI") { c.R = kRSI; d.hPlanck = kPlanckSI; }
     else if (d.units == "1") { c.R = 1; d.hPlanck = kPlanckSI / kRSI; }
@@ -386,6 +390,28 @@ Deck readDeck(const std::string& dir, bool createResult) {
         if (t.next("values label") != "#Values_in_zones") throw Fail("Wrong position in file.");
         d.zoneC.emplace_back();
         for (size_t z = 0; z < nzv; ++z) d.zoneC[k].push_back(t.word("zone concentration"));
+    }
+    // the EOS data files of createThermodynamics (abstractMixtureThermodynamics.cpp:71-143)
+    if (c.eos == FV_EOS_STIFFENED) {
+        Tokens t(d.path("set/stiffenedFluidData.txt"));
+        for (int k = 0; k < c.n_species; ++k) {
+            t.next("species label");
+            c.stiff_p0[k] = t.num("p0");
+            c.stiff_gamma[k] = t.num("gamma");
+        }
+    } else if (c.eos == FV_EOS_KATAOKA) {
+        Tokens t(d.path("set/KataokaVanDerWaalsFluidData.txt"));
+        for (int k = 0; k < c.n_species; ++k) {
+            t.next("species label");
+            c.lj_eps[k] = t.num("Lennard-Jones epsilon");
+            c.lj_sigma[k] = t.num("Lennard-Jones sigma");
+        }
+        t.skip();
+        const std::string rule = t.next("b calculation");
+        c.kataoka_b_coeff = t.num("b coefficient");
+        if (rule == "critical") c.kataoka_b_critical = 1;
+        else if (rule == "Kataoka") c.kataoka_b_critical = 0;
+        else throw Fail("Wrong type of Kataoka-van der Waals b coefficient calculation");
     }
     {
         Tokens t(d.path("set/velocity.txt"));
@@ -494,30 +520,65 @@ void initialFields(const Deck& d, const fv_config& c, std::vector<std::vector<do
 // ---------------------------------------------------------------- Helmholtz energy and entropy
 // mixtureIdeal::Fv/Sv (mixtureIdeal.cpp:300-354), mixtureVanDerWaals::Fv/Sv (:461-537) with
 // idealFluid::Fmx/Smx (idealFluid.cpp:90-116) and vanDerWaalsFluid::Fmx/Smx (:122-151).
+// With the mixtures of mixtureRedlichKwong::Fv/Sv (:459-530, RedlichKwongFluid::Fmx/Smx :175-211),
+// mixtureStiffened::Fv/Sv (:390-470, stiffenedFluid::Fmx/Smx :91-120) and
+// mixtureKataokaVanDerWaals::Fv/Sv (KataokaVanDerWaalsFluid::Fmx/Smx :430-496).
 struct Thermo {
     int N, eos;
     double R, kB, h;
     double molecMass[FV_MAX_SPECIES];
-    double aMolec[FV_MAX_SPECIES][FV_MAX_SPECIES], bMolec[FV_MAX_SPECIES][FV_MAX_SPECIES];
+    // per molecule: van der Waals / Redlich-Kwong a and b, Kataoka V0, eps and b; stiffened p0
+    double aMolec[FV_MAX_SPECIES][FV_MAX_SPECIES] = {}, bMolec[FV_MAX_SPECIES][FV_MAX_SPECIES] = {};
+    double V0Molec[FV_MAX_SPECIES][FV_MAX_SPECIES] = {}, epsMolec[FV_MAX_SPECIES][FV_MAX_SPECIES] = {};
+    double p0[FV_MAX_SPECIES][FV_MAX_SPECIES] = {};
 
     Thermo(const fv_config& c, double hPlanck) : N(c.n_species), eos(c.eos), R(c.R), kB(c.R / kNA), h(hPlanck) {
         double a[FV_MAX_SPECIES][FV_MAX_SPECIES] = {}, b[FV_MAX_SPECIES][FV_MAX_SPECIES] = {};
+        double V0[FV_MAX_SPECIES][FV_MAX_SPECIES] = {}, ep[FV_MAX_SPECIES][FV_MAX_SPECIES] = {};
+        constexpr double chi{std::cbrt(2) - 1.};  // mixtureRedlichKwong.cpp:34-37
+        constexpr double Sigma_a{1. / (9. * chi)}, Sigma_b{chi / 3.};
         for (int k = 0; k < N; ++k) {
             molecMass[k] = c.M[k] / kNA;
-            b[k][k] = c.Tc[k] * R / (8 * c.Pc[k]);
-            a[k][k] = c.Pc[k] * b[k][k] * b[k][k] * 27;
+            if (eos == FV_EOS_REDLICH_KWONG) {
+                b[k][k] = Sigma_b * R * c.Tc[k] / c.Pc[k];
+                a[k][k] = Sigma_a * R * R * c.Tc[k] * c.Tc[k] * std::sqrt(c.Tc[k]) / c.Pc[k];
+            } else if (eos == FV_EOS_KATAOKA) {
+                const double sg = c.lj_sigma[k];
+                b[k][k] = c.kataoka_b_critical ? c.kataoka_b_coeff * R * c.Tc[k] / (8 * c.Pc[k])
+                                               : c.kataoka_b_coeff * (sg * sg * sg) * kNA;
+                V0[k][k] = (sg * sg * sg) / std::sqrt(2) * kNA;
+                ep[k][k] = c.lj_eps[k];
+            } else {
+                b[k][k] = c.Tc[k] * R / (8 * c.Pc[k]);
+                a[k][k] = c.Pc[k] * b[k][k] * b[k][k] * 27;
+            }
+            p0[k][k] = c.stiff_p0[k];
         }
         for (int k = 0; k < N; ++k)
             for (int l = 0; l < N; ++l)
                 if (k != l) {
                     b[k][l] = std::pow(0.5 * (std::cbrt(b[k][k]) + std::cbrt(b[l][l])), 3);
                     a[k][l] = std::sqrt(a[k][k] * a[l][l]);
+                    V0[k][l] = std::pow(0.5 * (std::cbrt(V0[k][k]) + std::cbrt(V0[l][l])), 3);
+                    ep[k][l] = std::sqrt(ep[k][k] * ep[l][l]);
+                    p0[k][l] = std::sqrt(p0[k][k] * p0[l][l]);
                 }
         for (int k = 0; k < N; ++k)
             for (int l = 0; l < N; ++l) {
                 bMolec[k][l] = b[k][l] / kNA;
                 aMolec[k][l] = a[k][l] / (kNA * kNA);
+                V0Molec[k][l] = V0[k][l] / kNA;
+                epsMolec[k][l] = ep[k][l] / kNA;
             }
+    }
+
+    // KataokaVanDerWaalsFluid::qa with the molecular constants (M = 13 terms)
+    static double qa(double c, double T, double V0, double eps, double R) {
+        const double V0c{V0 * c};
+        const double epsRT{0.5 * eps / (R * T)};
+        double series{1.0};
+        for (std::size_t J = 2; J <= 13; ++J) series += std::pow(V0c, (J - 1.) / 3.) * std::exp((J - 1.) * epsRT);
+        return series;
     }
 
     // Sum over the species of a valarray expression, in the order libstdc++'s _Expr::sum() takes:
@@ -541,10 +602,50 @@ struct Thermo {
         }
         const double A = speciesSum([&](int k) { return x[k] * std::log(x[k] + kStab); });
         const double C = speciesSum([&](int k) { return -x[k] * std::log(x[k] + kStab); });
-        if (eos == FV_EOS_IDEAL) {
+        if (eos == FV_EOS_IDEAL || eos == FV_EOS_STIFFENED) {
             const double B = speciesSum([&](int k) { return x[k] * std::log(Vm / lam3[k]); });
-            F = kB * T * (A - 1 - B) * molecConc;
+            if (eos == FV_EOS_IDEAL) {
+                F = kB * T * (A - 1 - B) * molecConc;
+            } else {
+                double p0m = 0;
+                for (int k = 0; k < N; ++k)
+                    for (int l = 0; l < N; ++l) p0m += x[k] * x[l] * p0[k][l];
+                F = (kB * T * (A - 1 - B) + p0m * Vm) * molecConc;
+            }
             S = kB * (C + B + 5. / 2.) * molecConc;
+            return;
+        }
+        if (eos == FV_EOS_REDLICH_KWONG || eos == FV_EOS_KATAOKA) {
+            double am = 0, bm = 0, V0m = 0, em = 0;
+            for (int k = 0; k < N; ++k)
+                for (int l = 0; l < N; ++l) {
+                    if (eos == FV_EOS_KATAOKA) {
+                        V0m += x[k] * x[l] * V0Molec[k][l];
+                        em += x[k] * x[l] * epsMolec[k][l];
+                    } else {
+                        am += x[k] * x[l] * aMolec[k][l];
+                    }
+                    bm += x[k] * x[l] * bMolec[k][l];
+                }
+            const double mixS = -A;
+            const double trans = speciesSum([&](int k) { return x[k] * std::log((Vm - bm) / lam3[k]); });
+            if (eos == FV_EOS_REDLICH_KWONG) {
+                const double potF = am / (bm * std::sqrt(T)) * std::log1p(bm / Vm);
+                const double potS = 0.5 * am / (bm * T * std::sqrt(T)) * std::log1p(bm / Vm);
+                F = (kB * T * (A - 1 - trans) - potF) * molecConc;
+                S = (kB * (mixS + 5. / 2. + trans) - potS) * molecConc;
+                return;
+            }
+            const double q = qa(1 / Vm, T, V0m, em, kB);
+            const double potF = std::log(q);
+            const double V0c{V0m / Vm};
+            const double epsRT{0.5 * em / (kB * T)};
+            double series{0.0};
+            for (std::size_t J = 2; J <= 13; ++J)
+                series -= 0.5 * (J - 1) * std::pow(V0c, (J - 1) / 3.) * std::exp(0.5 * (J - 1.) * epsRT);
+            const double potS = std::log(q) + em / (kB * T) * series / q;
+            F = kB * T * ((A - 1 - trans) - potF) * molecConc;
+            S = kB * ((mixS + 5. / 2. + trans) - potS) * molecConc;
             return;
         }
         // mixture a and b accumulate cell by cell from zero, k outer, l inner

@@ -104,9 +104,11 @@ def _first_difference(a: bytes, b: bytes, rel: str):
     return f"{rel}: {len(la)} lines, reference {len(lb)}"
 
 
-def replay(driver, name, d, timeout=600):
+def replay(driver, name, d, timeout=600, gpu=False):
     """Runs every run of fixture ``name`` in directory ``d`` with ``driver``; returns a list of
-    differences from the reference's files (empty when they agree)."""
+    differences from the reference's files (empty when they agree).  ``gpu``: the driver runs the
+    CUDA library, and a fixture's ``gpu_tolerance`` (the real-gas mixtures whose transcendental
+    functions round differently on the device) replaces its ``tolerance``."""
     z = load(name)
     unpack_inputs(z, d)
     problems = []
@@ -128,6 +130,8 @@ def replay(driver, name, d, timeout=600):
     if sorted(got) != sorted(want):
         problems.append(f"files: extra {sorted(set(got) - set(want))}, missing {sorted(set(want) - set(got))}")
     tol = float(z["tolerance"])
+    if gpu and "gpu_tolerance" in z.files:
+        tol = float(z["gpu_tolerance"])
     scale = _velocity_scale(want) if tol > 0 else None
     for rel, data in sorted(want.items()):
         if rel not in got:

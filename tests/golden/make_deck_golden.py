@@ -136,6 +136,14 @@ def deck_cases():
     c.t_end = 0.03
     out.append(("tube60_zones_width", c, p, 4, False, [{}, {"start": "2", "t_end": "0.05"}], 0.0,
                 {"mixing_width": True, "zones": zones}))
+    # the equations of state beyond ideal and van der Waals, with their data files
+    # (set/stiffenedFluidData.txt, set/KataokaVanDerWaalsFluidData.txt) and the Helmholtz energy and
+    # entropy of each mixture in the outputs
+    for eos in ("stiffened", "RedlichKwong", "Kataoka"):
+        c, p = cases.real_gas_tube(eos, n=60)
+        c.t_end = _t_after(c, p, 10, 0.4)
+        out.append((f"tube60_{eos.lower()}", c, p, 4, True, [{}], 0.0,
+                    {} if eos == "stiffened" else {"gpu_tolerance": 1e-11}))
     return out
 
 
@@ -213,8 +221,10 @@ def main(only=None):
         if only and name not in only:
             continue
         d = tempfile.mkdtemp(prefix="schemi_deck_")
+        extra = dict(extra[0]) if extra else {}
+        gpu_tol = extra.pop("gpu_tolerance", None)
         try:
-            write_deck(case, d, prim, frequency_of_output=freq, restart=restart, **(extra[0] if extra else {}))
+            write_deck(case, d, prim, frequency_of_output=freq, restart=restart, **extra)
             inputs = _files(d)
             base = inputs[os.path.join("set", "main.txt")].decode()
             data = {_key("in", rel): np.frombuffer(b, dtype=np.uint8) for rel, b in inputs.items()}
@@ -237,6 +247,8 @@ def main(only=None):
             data["runs"] = np.int64(len(runs))
             data["rc"] = np.asarray(rcs, dtype=np.int64)
             data["tolerance"] = np.float64(tol)
+            if gpu_tol is not None:
+                data["gpu_tolerance"] = np.float64(gpu_tol)
             np.savez_compressed(os.path.join(HERE, f"deck_{name}.npz"), **data)
             outs = sorted(k for k in data if k.startswith("out:result|output_"))
             print(f"deck_{name}: {len(runs)} run(s), outputs {[k.split('_')[-1] for k in outs]}")

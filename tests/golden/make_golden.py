@@ -70,6 +70,10 @@ def golden_cases():
         c, p = cases.shock_tube_1d(n=200)
         c.limiter = lim
         out.append((f"tube_{lim.lower()}_200", c, p, 40, [1, 2, 40]))
+    # the equations of state beyond ideal and van der Waals (abstractMixtureThermodynamics.cpp:39-43)
+    for eos in ("stiffened", "RedlichKwong", "Kataoka"):
+        c, p = cases.real_gas_tube(eos)
+        out.append((f"tube_{eos.lower()}_200", c, p, 40, [1, 2, 40]))
     # Cl2 <-> 2Cl chemistry (the ClorumTest mechanism and solver, hot mixture)
     c, p = cases.chlorine_dissociation_2d(4)
     out.append(("cl2_4x4_vdw_gs", c, p, 10, [1, 2, 10]))

@@ -46,7 +46,6 @@ def _free_port():
 
 
 def _rank_main(rank, world, port, out):
-    import torch
     import torch.distributed as dist
 
     from schemi_b200 import ensemble
@@ -58,13 +57,11 @@ def _rank_main(rank, world, port, out):
         mine = shares[rank]
         # what every rank reports: its cell updates and a device time; the job value uses the
         # sum of updates and the max of times
-        updates = torch.tensor([sum(work[i] for i in mine)], dtype=torch.float64)
-        ms = torch.tensor([1.0 + rank], dtype=torch.float64)
-        dist.all_reduce(updates, op=dist.ReduceOp.SUM)
-        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+        tot = ensemble.combine_rank_totals(dist, "cpu", sums={"updates": sum(work[i] for i in mine)},
+                                           maxes={"ms": 1.0 + rank})
         gathered = [None] * world
         dist.all_gather_object(gathered, mine)
-        out[rank] = (gathered, float(updates), float(ms))
+        out[rank] = (gathered, tot["updates"], tot["ms"])
     finally:
         dist.destroy_process_group()
 

@@ -105,6 +105,9 @@ def _edit(path, key, value):
     ("main.txt", "#Source_timestep_correction", "Implicit=0.25,0.5", "Unknown source time-step flag."),
     ("main.txt", "#Defines_universal_gas_constant", "Planck", "Unknown type of universal gas constant."),
     ("main.txt", "#Reconstruction", "cubic", "Unknown reconstruction flag."),
+    ("main.txt", "#Equation_of_state", "BenedictWebbRubin", "Unknown type of equation of state."),
+    ("main.txt", "#Equation_of_state", "stiffened", "stiffenedFluidData.txt not found."),
+    ("main.txt", "#Equation_of_state", "Kataoka", "KataokaVanDerWaalsFluidData.txt not found."),
     ("zonesDescription.txt", "#Number_of_zones", "1", "end of file"),
     ("g.txt", "#Free_fall_acceleration_flag", "maybe", "Unknown gravitation flag."),
     ("chemicalKinetics.txt", "#Type_of_chemical_reaction", "H2Cl2Combustion", "not implemented"),

@@ -13,6 +13,9 @@ from golden_cases import golden_steps, load_cases, rel_err
 pytestmark = pytest.mark.gpu
 
 FP64_TOL = 1e-12
+# Redlich-Kwong and Kataoka mixtures: the device solves the cubic in FP64 where the reference uses
+# long double, and its pow / exp / acos ... round their last bit differently from the host's
+REAL_GAS_TOL = 1e-11
 COMPARE = ["c1", "c2", "c3", "vx", "vy", "p", "rho", "E", "mx", "my"]
 # the fixtures with chemistry are checked by test_gpu_chemistry.py (exp/pow round differently on
 # the GPU, and velocities that start from rest are compared on the flow's speed scale there)
@@ -41,6 +44,7 @@ def _advance(g, n, t_end):
 
 @pytest.mark.parametrize("name,case,prim,data", CASES, ids=[c[0] for c in CASES])
 def test_gpu_fp64_matches_reference(fv, name, case, prim, data):
+    tol = REAL_GAS_TOL if case.eos in ("RedlichKwong", "Kataoka") else FP64_TOL
     g = fv.FVCase(case)
     g.upload(prim)
     t_end = float(data["t_end"])
@@ -57,7 +61,7 @@ def test_gpu_fp64_matches_reference(fv, name, case, prim, data):
             if key in data and f in out:
                 linf, l1 = rel_err(out[f], data[key])
                 worst = max(worst, linf)
-                assert linf <= FP64_TOL, f"{name} step {target} {f}: rel Linf {linf:.3e} L1 {l1:.3e}"
+                assert linf <= tol, f"{name} step {target} {f}: rel Linf {linf:.3e} L1 {l1:.3e}"
     print(f"{name}: max rel Linf vs reference = {worst:.3e}")
 
 
@@ -245,3 +249,52 @@ def test_gpu_download_into_pinned_buffers(fv):
     outs["p"] = np.zeros(g.n_cells - 1)
     with pytest.raises(ValueError):
         g.download(outs)
+
+
+def test_step_kernel_finalizes_itself(fv, oracle_mod):
+    """Without chemistry the step kernel's last CTA runs the CFL finalize: one launch per step on
+    the fused march (four on the generic path), and a run of steps through fv_run still matches
+    the oracle step for step (the clock, the step sizes and the state)."""
+    from schemi_b200 import cases
+
+    case, prim = cases.kelvin_helmholtz_2d(n=64)
+    g = fv.FVCase(case)
+    assert g.path == fv.PATH_MARCH and g.kernels_per_step == 1
+    g.upload(prim)
+    st = g.run(1.0, max_steps=25)
+    oc = oracle_mod.OracleCase(case)
+    oc.upload(prim)
+    for _ in range(25):
+        oc.step()
+    assert st.steps == 25
+    assert g.time() == oc.time()
+    a, b = g.download(), oc.download()
+    for f in COMPARE:
+        if f in a and f in b:
+            linf, _ = rel_err(a[f], b[f])
+            assert linf <= FP64_TOL, f
+    t, _ = cases.shock_tube_1d(n=100)
+    assert fv.FVCase(t).kernels_per_step == 4
+
+
+@pytest.mark.parametrize("eos", ["stiffened", "RedlichKwong", "Kataoka"])
+def test_gpu_real_gas_2d_and_f32flux_against_oracle(fv, oracle_mod, eos):
+    """The real-gas mixtures on a 2D mesh (generic path, periodic in x) against the FP64 oracle,
+    in FP64 and in FP32-flux arithmetic (their EOS stays FP64 in both)."""
+    import numpy as np
+
+    from schemi_b200 import cases
+    from schemi_b200.case import PatchBC
+
+    tube, tprim = cases.real_gas_tube(eos, n=24)
+    for prec, tol, l1 in (("f64", REAL_GAS_TOL if eos != "stiffened" else FP64_TOL, False), ("f32flux", 1e-5, True)):
+        case = tube.__class__(**{**tube.__dict__})
+        case.dims, case.n, case.precision = 2, (24, 24, 1), prec
+        case.bc = {"tail": PatchBC.uniform("periodic", 2), "point": PatchBC.uniform("periodic", 2),
+                   "right": PatchBC.uniform("slip", 2), "left": PatchBC.uniform("slip", 2)}
+        # the tube's jump along y, a small shear along x
+        prim = [np.repeat(a, 24) for a in tprim]
+        prim[2] = 0.01 * np.sqrt(np.abs(prim[5]) / np.maximum(prim[0] + prim[1], 1e-30)) * np.tile(
+            np.sin(np.linspace(0, 2 * np.pi, 24, endpoint=False)), 24)
+        g, worst = _oracle_compare(fv, oracle_mod, case, prim, 8, tol, l1=l1)
+        assert g.path == fv.PATH_GENERIC
