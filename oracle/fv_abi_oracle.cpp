@@ -1,11 +1,13 @@
 // fv_abi_oracle.cpp -- TEST INFRASTRUCTURE, not part of the product.
 //
 // The subset of the C-ABI of include/fvstep.h that the task-deck driver (schemi_b200/host/
-// fvrun.cpp) calls -- fv_create, fv_destroy, fv_last_error, fv_upload, fv_run, fv_download,
+// fvrun.cpp) and the reference-side step solver (schemi_b200/host/schemi_adapter) call --
+// fv_create, fv_destroy, fv_last_error, fv_upload, fv_run, fv_step, fv_download, fv_get_time,
 // fv_set_time -- implemented over the FP64 CPU oracle (fv_oracle.cpp).  Linking the driver
 // against this library instead of libschemi_fv.so gives lib/fvrun_oracle, with which the CPU
 // tests check the driver's deck reader, time loop, restart and file writer against the
-// reference's own result files without a GPU.  The shipped driver never loads it.
+// reference's own result files without a GPU; linking the reference's main with the step
+// solver against it checks the step solver the same way.  Neither shipped binary loads it.
 #include <cstdio>
 #include <string>
 
@@ -59,9 +61,28 @@ fv_status fv_run(fv_handle* h, double t_end, long long max_steps, fv_run_stats* 
     return (fv_status)st;
 }
 
+fv_status fv_step(fv_handle* h, double* dt_used, double* dt_next) {
+    if (!h) return FV_ERR_INIT;
+    double used = 0, next = 0;
+    const int st = fvo_step(h->c, &used, &next);
+    if (st != FV_OK) h->err = "oracle step failed with status " + std::to_string(st);
+    if (dt_used) *dt_used = used;
+    if (dt_next) *dt_next = next;
+    return (fv_status)st;
+}
+
 fv_status fv_download(fv_handle* h, double* const* out) {
     if (!h || !out) return FV_ERR_INIT;
     return (fv_status)fvo_download(h->c, out);
+}
+
+fv_status fv_get_time(const fv_handle* h, double* time, double* dt) {
+    if (!h) return FV_ERR_INIT;
+    double t = 0, d = 0;
+    fvo_get_time(h->c, &t, &d);
+    if (time) *time = t;
+    if (dt) *dt = d;
+    return FV_OK;
 }
 
 fv_status fv_set_time(fv_handle* h, double time, double dt) {

@@ -111,7 +111,7 @@ def build(verbose: bool = False, force: bool = False, extra_flags=None) -> str:
 
 def build_driver(force: bool = False) -> str:
     """Compile the task-deck driver against the built library."""
-    deps = [DRIVER_SRC, LIB, os.path.join(HERE, "..", "include", "fvstep.h")]
+    deps = [DRIVER_SRC, os.path.join(HERE, "host", "deck.hpp"), LIB, os.path.join(HERE, "..", "include", "fvstep.h")]
     if force or _stale(DRIVER, deps):
         cmd = [os.environ.get("CXX", "g++"), "-std=c++17", "-O2", "-Wall", "-I", os.path.join(HERE, "..", "include"),
                DRIVER_SRC, "-o", DRIVER, "-L", LIBDIR, "-lschemi_fv", "-Wl,-rpath,$ORIGIN"]

@@ -12,6 +12,7 @@ the message the reference printed.
 """
 
 import os
+import re
 import subprocess
 
 import numpy as np
@@ -104,17 +105,37 @@ def _first_difference(a: bytes, b: bytes, rel: str):
     return f"{rel}: {len(la)} lines, reference {len(lb)}"
 
 
-def replay(driver, name, d, timeout=600, gpu=False):
+ORDER = re.compile(rb"(#Approximation_order\r?\n)(SecondOrder|SecondOrderRK|ThirdOrder|ThirdOrderCada)(\r?\n)")
+
+
+def step_order(name):
+    """The fixture's approximation order (its first run's set/main.txt)."""
+    m = ORDER.search(load(name)["run0:main.txt"].tobytes())
+    return m.group(2).decode() if m else None
+
+
+def replay(driver, name, d, timeout=600, gpu=False, reference_main=False):
     """Runs every run of fixture ``name`` in directory ``d`` with ``driver``; returns a list of
     differences from the reference's files (empty when they agree).  ``gpu``: the driver runs the
     CUDA library, and a fixture's ``gpu_tolerance`` (the real-gas mixtures whose transcendental
-    functions round differently on the device) replaces its ``tolerance``."""
+    functions round differently on the device) replaces its ``tolerance``.  ``reference_main``:
+    the driver is the reference's own main with the step-solver adapter registered (it reads
+    ./set from its working directory); every run's approximation order X becomes "GpuX", the
+    name under which the adapter runs the library's step."""
     z = load(name)
     unpack_inputs(z, d)
     problems = []
     for r in range(int(z["runs"])):
-        _write(d, os.path.join("set", "main.txt"), z[f"run{r}:main.txt"].tobytes())
-        res = subprocess.run([driver, d], capture_output=True, text=True, timeout=timeout)
+        main_txt = z[f"run{r}:main.txt"].tobytes()
+        if reference_main:
+            main_txt, n = ORDER.subn(rb"\1Gpu\2\3", main_txt)
+            assert n == 1, f"{name}: no approximation order to redirect"
+        _write(d, os.path.join("set", "main.txt"), main_txt)
+        if reference_main:
+            res = subprocess.run([driver], cwd=d, stdin=subprocess.DEVNULL, capture_output=True,
+                                 text=True, timeout=timeout)
+        else:
+            res = subprocess.run([driver, d], capture_output=True, text=True, timeout=timeout)
         if res.returncode != int(z["rc"][r]):
             problems.append(f"run {r}: exit {res.returncode}, reference {int(z['rc'][r])}\n"
                             + res.stdout[-1500:] + res.stderr[-1500:])
