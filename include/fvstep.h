@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define FV_ABI_VERSION 5
+#define FV_ABI_VERSION 6
 #define FV_MAX_SPECIES 4
 
 typedef int fv_status;
@@ -137,6 +137,19 @@ enum fv_chem_solver {
     FV_CHEM_CONJUGATE_GRADIENT = 3, FV_CHEM_JACOBI_CONJUGATE_GRADIENT = 4
 };
 
+/* Linear solver of the diffusion stage (#Type_of_SLE_solver_flag, abstractMatrixSolver.cpp:51-70):
+ * "explicit" (the stage's fields advance explicitly, Diffusion.cpp:437-441,787-797,818-825) or
+ * "GaussSeidel". */
+enum fv_sle_solver { FV_SLE_EXPLICIT = 0, FV_SLE_GAUSS_SEIDEL = 1 };
+
+/* Transport-coefficient model (transportCoefficients.txt #Transport_coefficient_model,
+ * phaseInitialization.cpp:211-222); "constant": mu, D and kappa as given
+ * (abstractTransportModel.cpp:52-187). */
+enum fv_transport { FV_TRANSPORT_CONSTANT = 0 };
+
+/* transportCoefficients.txt #Flag_for_enthalpy_flow_solution (phaseInitialization.cpp:224-235). */
+enum fv_enthalpy_flow { FV_ENTHALPY_NO = 0, FV_ENTHALPY_EXPLICIT = 1, FV_ENTHALPY_IMPLICIT = 2 };
+
 /* Arrhenius rate constant k = A * T^n * exp(-E / (R T)), E in J/mol (R units of the case). */
 typedef struct fv_arrhenius {
     double A, n, E;
@@ -189,6 +202,24 @@ typedef struct fv_config {
     int kataoka_b_critical;              /* KATAOKA: 1 "critical": b = coeff R Tc / (8 Pc);
                                             0 "Kataoka": b = coeff sigma^3 N_A */
     double kataoka_b_coeff;
+    /* Diffusion stage (ABI version 6): #Diffusion_flag on runs Diffusion.cpp:20-1061 after each
+     * advection (secondOrderStepSolver.cpp:69-80), with the gas's molecular transport and no
+     * turbulence. */
+    int diffusion;            /* 1: #Diffusion_flag on */
+    int sle_solver;           /* fv_sle_solver */
+    int sle_max_iter;         /* #Number_of_iterations_of_SLE_matrix_solver */
+    int transport;            /* fv_transport */
+    double mu_const;          /* #Viscosity_coefficient (the constant model's mu) */
+    double D_const;           /* #Diffusion_coefficient */
+    double kappa_const;       /* #Heat_conduction_coefficient */
+    int enthalpy_flow;        /* fv_enthalpy_flow */
+    int molmass_diffusion;    /* #Flag_for_molar_mass_diffusion_correction on */
+    int linear_reconstruction;  /* #Reconstruction "linear" (1) or "star" (0): the stage's velocity
+                                   gradient from the cells or from the Riemann star states */
+    int diffusion_timestep;   /* 1: #Source_timestep_correction "Courant-Source-Diffusion" (the
+                                 stage limits the next step, Diffusion.cpp:1036-1049) */
+    double dt_coeff_source;   /* the flag's first coefficient (explicit enthalpy flow limit) */
+    double dt_coeff_diffusion;  /* its second (diffusion limit) */
 } fv_config;
 
 /* Field indices of fv_download / fv_upload arrays (n_cells doubles each, x fastest).
@@ -246,9 +277,17 @@ fv_status fv_download(fv_handle* h, double* const* out);
 fv_status fv_get_time(const fv_handle* h, double* time, double* dt);
 fv_status fv_set_time(fv_handle* h, double time, double dt);
 
+/* The source time step the last step's diffusion stage set (mesh::timestepSource after
+ * Diffusion.cpp:688-706,1036-1049; 1e-3 * DBL_MAX, the reference's veryBig, when no stage
+ * limited it): the limit main's CFL block applies to the next step unless #Source_timestep_correction
+ * is "Courant".  A host that runs its own CFL block (the step-solver adapter) hands it on. */
+fv_status fv_get_source_timestep(const fv_handle* h, double* dt_source);
+
 /* Conserved state (rho_1..rho_N, rho, m_x, m_y, m_z, E) as device pointers, SoA, n_cells each.
  * A 1D/2D case whose restart set has no transverse velocity leaves the transverse momentum
- * fields untouched (they stay zero). */
+ * fields untouched (they stay zero).  The arrays are for reading: the step keeps data derived
+ * from the current state between steps, so a new state goes in through fv_upload or
+ * fv_upload_device. */
 fv_status fv_state_device(fv_handle* h, double** fields, int* n_fields, long long* n_cells);
 
 /* Synchronises the handle's stream. */

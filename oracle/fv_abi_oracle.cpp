@@ -3,7 +3,7 @@
 // The subset of the C-ABI of include/fvstep.h that the task-deck driver (schemi_b200/host/
 // fvrun.cpp) and the reference-side step solver (schemi_b200/host/schemi_adapter) call --
 // fv_create, fv_destroy, fv_last_error, fv_upload, fv_run, fv_step, fv_download, fv_get_time,
-// fv_set_time -- implemented over the FP64 CPU oracle (fv_oracle.cpp).  Linking the driver
+// fv_set_time, fv_get_source_timestep -- implemented over the FP64 CPU oracle (fv_oracle.cpp).  Linking the driver
 // against this library instead of libschemi_fv.so gives lib/fvrun_oracle, with which the CPU
 // tests check the driver's deck reader, time loop, restart and file writer against the
 // reference's own result files without a GPU; linking the reference's main with the step
@@ -83,6 +83,11 @@ fv_status fv_get_time(const fv_handle* h, double* time, double* dt) {
     if (time) *time = t;
     if (dt) *dt = d;
     return FV_OK;
+}
+
+fv_status fv_get_source_timestep(const fv_handle* h, double* dt_source) {
+    if (!h) return FV_ERR_INIT;
+    return (fv_status)fvo_get_source_timestep(h->c, dt_source);
 }
 
 fv_status fv_set_time(fv_handle* h, double time, double dt) {

@@ -582,6 +582,16 @@ struct fvo_case {
     // loop (1), or per cell (0)
     int chemCarry = 1;
     std::string err;
+    // diffusion stage: the Riemann star velocity of the last advection (starFields::v) and the
+    // source time step the stage sets for the next step (mesh::timestepSource, reset by main's
+    // CFL block, Schemi.cpp:829-833)
+    std::vector<V3> starV;
+    double dtSource = kVeryBig;
+    double dtSourceLast = kVeryBig;  // the limit the last CFL block took
+    // the temperature a diffusion stage leaves (gasPhase.temperature = the stage's new T,
+    // Diffusion.cpp:981, not TFromUv of the recomputed energy); the next advection replaces it
+    std::vector<double> Tstate;
+    bool Tvalid = false;
 };
 
 namespace {
@@ -1216,8 +1226,10 @@ struct Flux {
 };
 
 // HLLC (HLLCSolver.cpp:13-406) and HLL (HLLSolver.cpp:13-318) for one face; returns false
-// when no branch applies (NaN wave speeds).
-bool riemann(const fvo_case& cs, const FState& O, const FState& B, const V3& N, Flux& F) {
+// when no branch applies (NaN wave speeds).  starV (HLLC): the face velocity the solver hands
+// the diffusion stage (starValues.v, HLLCSolver.cpp:399): the side's velocity outside the star
+// region, the star momentum over the star density inside it.
+bool riemann(const fvo_case& cs, const FState& O, const FState& B, const V3& N, Flux& F, V3* starV = nullptr) {
     const Mix& mx = cs.mix;
     const int NS = mx.N;
     const double csO = std::sqrt(mx.sqSonicSpeed(O.c, O.rho[0], O.Uv, O.p) + kTwoThirds * 0.0 * (1. + mx.dpdUv(O.c, O.Uv)));
@@ -1239,6 +1251,7 @@ bool riemann(const fvo_case& cs, const FState& O, const FState& B, const V3& N, 
             for (int k = 0; k <= NS; ++k) F.rho[k] = vmul(vmul(N, uO), O.rho[k]);
             F.m = outer(vadd(vmul(O.m, uO), vmul(INe, O.p + tpO)), N);
             F.E = vmul(N, uO * (O.E + O.p + tpO));
+            if (starV) *starV = O.v;
         } else if (Sc >= 0) {
             const double factor = SO - uO;
             const double den = 1 / (SO - Sc);
@@ -1249,6 +1262,7 @@ bool riemann(const fvo_case& cs, const FState& O, const FState& B, const V3& N, 
             for (int k = 0; k <= NS; ++k) F.rho[k] = vmul(N, O.rho[k] * uO + SO * (rs[k] - O.rho[k]));
             F.m = outer(vadd(vadd(vmul(O.m, uO), vmul(INe, O.p + tpO)), vmul(vsub(ms, O.m), SO)), N);
             F.E = vmul(N, (O.E + O.p + tpO) * uO + SO * (Es - O.E));
+            if (starV) *starV = vdiv(ms, rs[0]);
         } else if (SN > 0) {
             const double factor = SN - uN;
             const double den = 1 / (SN - Sc);
@@ -1259,10 +1273,12 @@ bool riemann(const fvo_case& cs, const FState& O, const FState& B, const V3& N, 
             for (int k = 0; k <= NS; ++k) F.rho[k] = vmul(N, B.rho[k] * uN + SN * (rs[k] - B.rho[k]));
             F.m = outer(vadd(vadd(vmul(B.m, uN), vmul(INe, B.p + tpN)), vmul(vsub(ms, B.m), SN)), N);
             F.E = vmul(N, (B.E + B.p + tpN) * uN + SN * (Es - B.E));
+            if (starV) *starV = vdiv(ms, rs[0]);
         } else if (SN <= 0) {
             for (int k = 0; k <= NS; ++k) F.rho[k] = vmul(vmul(N, uN), B.rho[k]);
             F.m = outer(vadd(vmul(B.m, uN), vmul(INe, B.p + tpN)), N);
             F.E = vmul(N, uN * (B.E + B.p + tpN));
+            if (starV) *starV = B.v;
         } else {
             return false;
         }
@@ -1314,6 +1330,7 @@ void cellPrimitivesFromConserved(fvo_case& cs, long long i) {
 // third = true reconstructs with the per-face limited surface gradients of Advection3dOrder.cpp
 // (no predictor either), cada = true with those of Advection3dOrderCada.cpp.
 int doStep(fvo_case& cs, double dt, bool hancock = true, bool third = false, bool cada = false) {
+    cs.Tvalid = false;  // the advection's temperature is TFromUv of its energy (Advection.cpp:478)
     const Mix& mx = cs.mix;
     const int NS = mx.N;
     const long long nc = cs.nCells;
@@ -1455,8 +1472,9 @@ int doStep(fvo_case& cs, double dt, bool hancock = true, bool third = false, boo
 
     // 4. fluxes
     std::vector<Flux> flux(nf);
+    if (cs.cfg.diffusion) cs.starV.assign(nf, v3(0, 0, 0));
     for (size_t f = 0; f < nf; ++f)
-        if (!riemann(cs, own[f], nei[f], cs.faces[f].N, flux[f])) {
+        if (!riemann(cs, own[f], nei[f], cs.faces[f].N, flux[f], cs.cfg.diffusion ? &cs.starV[f] : nullptr)) {
             cs.err = "Fatal error in Riemann solver.";
             return FV_ERR_RIEMANN;
         }
@@ -1561,6 +1579,551 @@ int rk3Step(fvo_case& cs, double dt, bool cada) {
     st = doStep(cs, dt, false, true, cada);
     if (st != FV_OK) return st;
     averageWith(cs, u, kTwoThirds);
+    return FV_OK;
+}
+
+// ---------------------------------------------------------------- diffusion stage
+// Diffusion.cpp:20-1061 for the molecular transport of a constant-coefficient gas
+// (abstractTransportModel.cpp:52-187), no turbulence, the explicit solver (noMatrixSolver: each
+// field advances as (explOldTime + freeTerm dt) / centralDiagonale, Diffusion.cpp:437-441,
+// 787-797,818-825), one pass of its non-linearity loop (with turbulence off its convergence
+// measure is 0 and it stops after the first pass, Diffusion.cpp:937-946), ideal and van der
+// Waals mixtures.
+
+// mixture functions of the stage (mixtureIdeal.cpp / mixtureVanDerWaals.cpp with
+// idealFluid.cpp / vanDerWaalsFluid.cpp)
+double dCv(const Mix& mx, const double* c) {  // Cv(concentrations): sum X_k Cv_k
+    double Cvm, am, bm, Mm;
+    mx.mixParams(c, Cvm, am, bm, Mm);
+    return Cvm;
+}
+double dNonIdeality(const Mix& mx, const double* c) {  // ideal 0; vdW -a c^2
+    if (mx.eos == FV_EOS_IDEAL) return 0;
+    double Cvm, am, bm, Mm;
+    mx.mixParams(c, Cvm, am, bm, Mm);
+    return -am * (c[0] * c[0]);
+}
+double dUvcFromT(const Mix& mx, const double* c, double T) {  // ideal Cv T; vdW Cv T - a c
+    double Cvm, am, bm, Mm;
+    mx.mixParams(c, Cvm, am, bm, Mm);
+    if (mx.eos == FV_EOS_IDEAL) return Cvm * T;
+    return Cvm * T - am * c[0];
+}
+// hkT (mixtureIdeal.cpp:291-298, mixtureVanDerWaals.cpp:452-459): (UvcFromTk + pcFromTk) / T of
+// species k alone at concentration ck
+double dhkT(const Mix& mx, double ck, double T, int k) {
+    if (mx.eos == FV_EOS_IDEAL) return (mx.Cv[k] * T + mx.R * T) / T;
+    const double a = mx.a[k][k], b = mx.b[k][k];
+    return ((mx.Cv[k] * T - a * ck) + (mx.R * T / (1 - ck * b) - a * ck)) / T;
+}
+
+// boundary concentrations of a patch from the owner cell (c_0 their sum in species order), the
+// surface (boundaryConditionValueSurface) or the cell (boundaryConditionValueCell) variant
+void dBoundaryConc(const fvo_case& cs, long long own, int patch, bool cellVariant, double* cB, bool& bad) {
+    cB[0] = 0;
+    for (int k = 1; k <= cs.N; ++k) {
+        cB[k] = cellVariant ? bcCellS(cs, cs.c[k][own], 0, k - 1, patch, bad)
+                            : bcSurfaceS(cs, cs.c[k][own], 0, k - 1, patch);
+        cB[0] += cB[k];
+    }
+}
+// calculatedTemperature (boundaryConditionValue.hpp:89-108 / 326-345)
+double dBoundaryT(const fvo_case& cs, long long own, int patch, bool cellVariant, bool& bad) {
+    double cB[FV_MAX_SPECIES + 1];
+    dBoundaryConc(cs, own, patch, cellVariant, cB, bad);
+    const double pB = cellVariant ? bcCellS(cs, cs.p[own], 2, 0, patch, bad) : bcSurfaceS(cs, cs.p[own], 2, 0, patch);
+    return cs.mix.TFromUv(cB, cs.mix.UvFromp(cB, pB));
+}
+
+// surfGrad of a scalar cell field with a ghost value per boundary face (gradient.hpp:96-168)
+template <class Ghost>
+void dSurfGrad(const fvo_case& cs, const std::vector<double>& phi, Ghost ghost, std::vector<V3>& sg) {
+    const size_t nf = cs.faces.size();
+    sg.assign(nf, v3(0, 0, 0));
+    for (size_t f = 0; f < nf; ++f) {
+        const Face& F = cs.faces[f];
+        const V3& rO = cs.cells[F.own].rC;
+        if (F.nei >= 0) {
+            const V3 d = vsub(vadd(cs.cells[F.nei].rC, F.neiShift), rO);
+            const double m = mag3(d);
+            const double q = (phi[F.nei] - phi[F.own]) / (m * m);
+            sg[f] = v3(q * d.x[0], q * d.x[1], q * d.x[2]);
+        } else {
+            const double b = ghost(f);
+            const V3 dR = vmul(vsub(F.rC, rO), 2.);
+            const double dm = mag3(dR);
+            const V3 dn = vdiv(dR, dm);
+            const double q = (b - phi[F.own]) / dm;
+            sg[f] = v3(q * dn.x[0], q * dn.x[1], q * dn.x[2]);
+        }
+    }
+}
+// linearInterpolate of a scalar cell field with a boundary face value (linearInterpolate.hpp:43-80)
+template <class Bnd>
+void dInterp(const fvo_case& cs, const std::vector<double>& phi, Bnd bnd, std::vector<double>& out) {
+    const size_t nf = cs.faces.size();
+    out.assign(nf, 0);
+    for (size_t f = 0; f < nf; ++f) {
+        const Face& F = cs.faces[f];
+        out[f] = F.nei >= 0 ? phi[F.own] * F.wOwn + phi[F.nei] * F.wNei : bnd(f);
+    }
+}
+// divergence of a surface vector field (divergence.hpp:58-88)
+void dDivV(const fvo_case& cs, const std::vector<V3>& sf, std::vector<double>& out) {
+    out.assign(cs.nCells, 0);
+    for (long long i = 0; i < cs.nCells; ++i) {
+        const Cell& c = cs.cells[i];
+        double acc = 0;
+        for (int j = 0; j < c.nFaces; ++j) {
+            const Face& F = cs.faces[c.faces[j]];
+            const V3 n = (F.own == i) ? F.N : vmul(F.N, -1);
+            acc += vdot(sf[c.faces[j]], n) * F.S;
+        }
+        out[i] = acc / c.V;
+    }
+}
+// divergence of a surface tensor field: sum (T & n) S / V
+void dDivT(const fvo_case& cs, const std::vector<T9>& sf, std::vector<V3>& out) {
+    out.assign(cs.nCells, v3(0, 0, 0));
+    for (long long i = 0; i < cs.nCells; ++i) {
+        const Cell& c = cs.cells[i];
+        V3 acc = v3(0, 0, 0);
+        for (int j = 0; j < c.nFaces; ++j) {
+            const Face& F = cs.faces[c.faces[j]];
+            const V3 n = (F.own == i) ? F.N : vmul(F.N, -1);
+            const V3 t = vmul(tdot(sf[c.faces[j]], n), F.S);
+            acc.x[0] += t.x[0]; acc.x[1] += t.x[1]; acc.x[2] += t.x[2];
+        }
+        out[i] = vdiv(acc, c.V);
+    }
+}
+inline T9 ttrans(const T9& t) {  // tensor::transpose (tensor.cpp:57-69)
+    T9 r = t;
+    r.x[1] = t.x[3]; r.x[2] = t.x[6]; r.x[3] = t.x[1]; r.x[5] = t.x[7]; r.x[6] = t.x[2]; r.x[7] = t.x[5];
+    return r;
+}
+inline T9 tadd(const T9& a, const T9& b) {
+    T9 r;
+    for (int q = 0; q < 9; ++q) r.x[q] = b.x[q] + a.x[q];
+    return r;
+}
+
+// effectiveTransportCoefficients::caclulateDFluxes without turbulence (transportCoefficients.hpp:
+// 256-325) for one face and one direction: the Maxwell-Stefan system of the molar-fraction
+// gradients, the row of the least concentration replaced by sum N_k M_k J_k = 0, solved by the
+// pivoting Gauss elimination of transportCoefficients.hpp:413-456, scaled by M_k c_k.
+void dMaxwellStefan(int NS, const double* Nc, const double* M, double D, const double* gradXf, double* out) {
+    double c[FV_MAX_SPECIES];
+    for (int k = 1; k <= NS; ++k) c[k - 1] = Nc[k];
+    double cmin = c[0];
+    for (int k = 1; k < NS; ++k) cmin = std::min(cmin, c[k]);
+    int replaceIndex = 0;
+    for (int k = 0; k < NS; ++k)
+        if (cmin == c[k]) { replaceIndex = k + 1; break; }
+    double A[FV_MAX_SPECIES][FV_MAX_SPECIES] = {};
+    double b[FV_MAX_SPECIES] = {};
+    for (int k = 0; k < NS; ++k) b[k] = -gradXf[k];
+    for (int k1 = 1; k1 <= NS; ++k1) {
+        if (k1 != replaceIndex) {
+            for (int k2 = 1; k2 <= NS; ++k2) {
+                if (k1 == k2) continue;
+                const double Aij = Nc[k1] * Nc[k2] / (Nc[0] * Nc[0] * D);
+                A[k1 - 1][k2 - 1] = -Aij;
+                A[k1 - 1][k1 - 1] += Aij;
+            }
+        } else {
+            b[k1 - 1] = 0;
+            for (int k2 = 1; k2 <= NS; ++k2) A[k1 - 1][k2 - 1] = Nc[k2] * M[k2 - 1];
+        }
+    }
+    // pivoting: each row k takes the row below with the largest (signed) entry of column k
+    for (int k = 0; k < NS - 1; ++k) {
+        double mv = A[k][k];
+        int mi = k;
+        for (int r = k + 1; r < NS; ++r)
+            if (A[r][k] > mv) { mv = A[r][k]; mi = r; }
+        if (mi != k) {
+            for (int q = 0; q < NS; ++q) std::swap(A[mi][q], A[k][q]);
+            std::swap(b[mi], b[k]);
+        }
+    }
+    for (int k = 0; k < NS - 1; ++k)
+        for (int i = k + 1; i < NS; ++i) {
+            const double ratio = A[i][k] / (A[k][k] + kStab);
+            for (int j = k + 1; j < NS; ++j) A[i][j] = A[i][j] - ratio * A[k][j];
+            b[i] = b[i] - ratio * b[k];
+        }
+    double phi[FV_MAX_SPECIES];
+    phi[NS - 1] = b[NS - 1] / (A[NS - 1][NS - 1] + kStab);
+    for (int i = NS - 2; i >= 0; --i) {
+        double term = 0.0;
+        for (int j = i + 1; j < NS; ++j) term += A[i][j] * phi[j];
+        phi[i] = (b[i] - term) / (A[i][i] + kStab);
+    }
+    for (int k = 0; k < NS; ++k) {
+        if (std::fabs(phi[k]) < std::numeric_limits<double>::epsilon()) phi[k] = 0;  // normalize
+        out[k] = phi[k] * M[k] * c[k];
+    }
+}
+
+int diffusionStage(fvo_case& cs, double dt) {
+    const Mix& mx = cs.mix;
+    const int NS = cs.N;
+    const long long nc = cs.nCells;
+    const size_t nf = cs.faces.size();
+    const fv_config& cf = cs.cfg;
+    bool bad = false;
+    auto conc = [&](long long i, double* c) { for (int k = 0; k <= NS; ++k) c[k] = cs.c[k][i]; };
+
+    // the phase after the advection: temperature (Advection.cpp:478), mass fractions
+    // (diffusiveFields.cpp:24-46), velocity
+    std::vector<double> T(nc);
+    std::vector<std::vector<double>> w(NS, std::vector<double>(nc));
+    for (long long i = 0; i < nc; ++i) {
+        double cc[FV_MAX_SPECIES + 1];
+        conc(i, cc);
+        T[i] = mx.TFromUv(cc, cs.Uv[i]);
+        double sum = 0.0;
+        for (int k = 0; k < NS; ++k) {
+            w[k][i] = cs.rho[k + 1][i] / cs.rho[0][i];
+            sum += w[k][i];
+        }
+        for (int k = 0; k < NS; ++k) w[k][i] /= sum;
+    }
+    const std::vector<V3>& v = cs.v;
+    const double mu = cf.mu_const, Dc = cf.D_const, kappa = cf.kappa_const;
+
+    // Diffusion.cpp:136-176
+    std::vector<double> nonIdOld(nc), CVOld(nc), CvM(nc), CCVOld(nc), NonIdRho(nc);
+    for (long long i = 0; i < nc; ++i) {
+        double cc[FV_MAX_SPECIES + 1];
+        conc(i, cc);
+        nonIdOld[i] = dNonIdeality(mx, cc);
+        const double avMolMass = cs.rho[0][i] / cs.c[0][i];
+        CVOld[i] = dCv(mx, cc);
+        CvM[i] = CVOld[i] / avMolMass;
+        CCVOld[i] = cs.c[0][i] * CVOld[i];
+        NonIdRho[i] = nonIdOld[i] / cs.rho[0][i];
+    }
+    std::vector<double> surfaceCv;
+    dInterp(cs, CVOld, [&](size_t f) {  // calculatedCv
+        double cB[FV_MAX_SPECIES + 1];
+        dBoundaryConc(cs, cs.faces[f].own, cs.faces[f].patch, false, cB, bad);
+        return dCv(mx, cB);
+    }, surfaceCv);
+    std::vector<std::vector<double>> sc(NS + 1, std::vector<double>(nf, 0.0));
+    std::vector<double> surfaceRho(nf, 0.0);
+    for (int k = 1; k <= NS; ++k) {
+        std::vector<double> sk;
+        dInterp(cs, cs.c[k], [&](size_t f) {
+            return bcSurfaceS(cs, cs.c[k][cs.faces[f].own], 0, k - 1, cs.faces[f].patch);
+        }, sk);
+        for (size_t f = 0; f < nf; ++f) {
+            sc[k][f] = sk[f];
+            sc[0][f] += sk[f];
+            surfaceRho[f] += sk[f] * mx.M[k - 1];
+        }
+    }
+    std::vector<V3> gradNonIdRho, gradCvM;
+    dSurfGrad(cs, NonIdRho, [&](size_t f) {  // calculatedNonidealityCorrectionPerDensity (cell)
+        const long long o = cs.faces[f].own;
+        const int pt = cs.faces[f].patch;
+        double cB[FV_MAX_SPECIES + 1];
+        dBoundaryConc(cs, o, pt, true, cB, bad);
+        double dens = 0;
+        for (int k = 1; k <= NS; ++k) dens += cB[k] * mx.M[k - 1];
+        const double Tb = dBoundaryT(cs, o, pt, false, bad);
+        (void)Tb;  // the ideal and van der Waals corrections do not depend on T
+        return dNonIdeality(mx, cB) / dens;
+    }, gradNonIdRho);
+    dSurfGrad(cs, CvM, [&](size_t f) {  // calculatedCvM (cell)
+        double cB[FV_MAX_SPECIES + 1];
+        dBoundaryConc(cs, cs.faces[f].own, cs.faces[f].patch, true, cB, bad);
+        double dens = 0;
+        for (int k = 1; k <= NS; ++k) dens += cB[k] * mx.M[k - 1];
+        return dCv(mx, cB) * cB[0] / dens;
+    }, gradCvM);
+
+    // velocity gradients (Diffusion.cpp:178-229): the cell gradient from the Riemann star
+    // velocities ("star"; under gravity the interpolated cell velocities, secondOrderStepSolver.cpp:
+    // 71-73) or from the cells ("linear")
+    std::vector<V3> starV = cs.starV;
+    if (cf.gravity || cf.linear_reconstruction)
+        for (size_t f = 0; f < nf; ++f) {
+            const Face& F = cs.faces[f];
+            starV[f] = F.nei >= 0 ? vadd(vmul(v[F.own], F.wOwn), vmul(v[F.nei], F.wNei))
+                                  : bcSurfaceV(cs, v[F.own], F.patch, F.N);
+        }
+    std::vector<T9> gradV(nc);
+    std::vector<double> divV;
+    for (long long i = 0; i < nc; ++i) {
+        const Cell& c = cs.cells[i];
+        T9 acc{};
+        for (int j = 0; j < c.nFaces; ++j) {
+            const Face& F = cs.faces[c.faces[j]];
+            const V3 n = (F.own == i) ? F.N : vmul(F.N, -1);
+            const T9 term = tmul(outer(starV[c.faces[j]], n), F.S);
+            for (int q = 0; q < 9; ++q) acc.x[q] += term.x[q];
+        }
+        for (int q = 0; q < 9; ++q) gradV[i].x[q] = acc.x[q] / c.V;
+    }
+    dDivV(cs, starV, divV);
+    std::vector<T9> gradVs;
+    surfGradVector(cs, v, gradVs, bad);
+    std::vector<double> divVs(nf);
+    for (size_t f = 0; f < nf; ++f) {  // surfDivergence (divergence.hpp:90-150)
+        const Face& F = cs.faces[f];
+        const V3& rO = cs.cells[F.own].rC;
+        if (F.nei >= 0) {
+            const V3 d = vsub(vadd(cs.cells[F.nei].rC, F.neiShift), rO);
+            const double m = mag3(d);
+            divVs[f] = vdot(vdiv(vsub(v[F.nei], v[F.own]), m * m), d);
+        } else {
+            const V3 b = bcCellV(cs, v[F.own], F.patch, F.N, bad);
+            const V3 dR = vmul(vsub(F.rC, rO), 2.);
+            const double dm = mag3(dR);
+            divVs[f] = vdot(vdiv(vsub(b, v[F.own]), dm), vdiv(dR, dm));
+        }
+    }
+    std::vector<double> surfaceT;
+    dInterp(cs, T, [&](size_t f) { return dBoundaryT(cs, cs.faces[f].own, cs.faces[f].patch, false, bad); }, surfaceT);
+    std::vector<T9> strainVol(nc), strainSurf1(nf);
+    for (long long i = 0; i < nc; ++i) {
+        strainVol[i] = tadd(gradV[i], ttrans(gradV[i]));
+        const double l = kTwoThirds * divV[i];
+        strainVol[i].x[0] -= l; strainVol[i].x[4] -= l; strainVol[i].x[8] -= l;
+    }
+    for (size_t f = 0; f < nf; ++f) {
+        strainSurf1[f] = ttrans(gradVs[f]);
+        const double l = kTwoThirds * divVs[f];
+        strainSurf1[f].x[0] -= l; strainSurf1[f].x[4] -= l; strainSurf1[f].x[8] -= l;
+    }
+
+    // effective coefficients without turbulence (transportCoefficients.hpp:222-232)
+    std::vector<std::vector<double>> rhoD(NS, std::vector<double>(nf));
+    for (int k = 0; k < NS; ++k)
+        for (size_t f = 0; f < nf; ++f) rhoD[k][f] = surfaceRho[f] * Dc;
+
+    // mass-fraction matrices (Diffusion.cpp:321-339; SLEMatrix.cpp:2054-2078)
+    std::vector<std::vector<V3>> gradW(NS);
+    std::vector<std::vector<double>> diagW(NS, std::vector<double>(nc)), oldW(NS, std::vector<double>(nc)),
+        freeW(NS, std::vector<double>(nc, 0.0));
+    for (int k = 0; k < NS; ++k) {
+        dSurfGrad(cs, w[k], [&](size_t f) {  // calculatedMassFraction (cell), component k + 1
+            double cB[FV_MAX_SPECIES + 1];
+            dBoundaryConc(cs, cs.faces[f].own, cs.faces[f].patch, true, cB, bad);
+            const double dens = cB[k + 1] * mx.M[k];
+            double sum = 0;
+            for (int q = 1; q <= NS; ++q) sum += cB[q] * mx.M[q - 1];
+            return dens / sum;
+        }, gradW[k]);
+        std::vector<V3> flow(nf);
+        for (size_t f = 0; f < nf; ++f) flow[f] = vmul(vmul(gradW[k][f], rhoD[k][f]), -1.);
+        std::vector<double> div;
+        dDivV(cs, flow, div);
+        for (long long i = 0; i < nc; ++i) {
+            diagW[k][i] = cs.rho[0][i];
+            oldW[k][i] = w[k][i] * cs.rho[0][i];
+            freeW[k][i] -= div[i];
+        }
+    }
+
+    // molar-mass correction and explicit enthalpy flow (Diffusion.cpp:341-422)
+    std::vector<V3> entFlow(nf, v3(0, 0, 0));
+    if (cf.molmass_diffusion || cf.enthalpy_flow != FV_ENTHALPY_NO) {
+        std::vector<std::vector<V3>> gradX(NS);
+        std::vector<std::vector<V3>> DFlux(NS, std::vector<V3>(nf, v3(0, 0, 0)));
+        if (cf.molmass_diffusion) {
+            for (int k = 0; k < NS; ++k) {
+                std::vector<double> X(nc);
+                for (long long i = 0; i < nc; ++i) X[i] = cs.c[k + 1][i] / cs.c[0][i];
+                dSurfGrad(cs, X, [&](size_t f) {  // calculatedMolarFraction (cell), component k + 1
+                    double cB[FV_MAX_SPECIES + 1];
+                    dBoundaryConc(cs, cs.faces[f].own, cs.faces[f].patch, true, cB, bad);
+                    double sum = 0;
+                    for (int q = 1; q <= NS; ++q) sum += cB[q];
+                    return cB[k + 1] / sum;
+                }, gradX[k]);
+            }
+            for (size_t f = 0; f < nf; ++f) {
+                if (NS > 1) {
+                    double Nc[FV_MAX_SPECIES + 1];
+                    for (int k = 0; k <= NS; ++k) Nc[k] = sc[k][f];
+                    for (int d = 0; d < 3; ++d) {
+                        double g[FV_MAX_SPECIES], out[FV_MAX_SPECIES];
+                        for (int k = 0; k < NS; ++k) g[k] = gradX[k][f].x[d];
+                        dMaxwellStefan(NS, Nc, mx.M, Dc, g, out);
+                        for (int k = 0; k < NS; ++k) DFlux[k][f].x[d] = out[k];
+                    }
+                }
+            }
+        }
+        for (int k = 0; k < NS; ++k) {
+            std::vector<V3> flowW(nf), corr(nf, v3(0, 0, 0));
+            for (size_t f = 0; f < nf; ++f) flowW[f] = vmul(gradW[k][f], -1 * rhoD[k][f]);
+            if (cf.molmass_diffusion) {
+                for (size_t f = 0; f < nf; ++f) corr[f] = vsub(DFlux[k][f], flowW[f]);
+                std::vector<double> div;
+                dDivV(cs, corr, div);
+                for (long long i = 0; i < nc; ++i) {  // distributeSourceTerm (SLEMatrix.cpp:2166-2175)
+                    const double s = div[i] * (-1.0);
+                    if (s >= 0.) freeW[k][i] += s;
+                    else diagW[k][i] -= s / (w[k][i] + kStab);
+                }
+            }
+            if (cf.enthalpy_flow != FV_ENTHALPY_NO)
+                for (size_t f = 0; f < nf; ++f) {
+                    const double h = dhkT(mx, sc[k + 1][f], surfaceT[f], k);
+                    const V3 t = vdiv(vmul(vadd(corr[f], flowW[f]), h), mx.M[k]);
+                    entFlow[f] = vadd(entFlow[f], t);
+                }
+        }
+    }
+
+    // non-ideality correction (Diffusion.cpp:424-428; tLambda is zero without turbulence)
+    std::vector<V3> nonIdLap(nf);
+    for (size_t f = 0; f < nf; ++f) {
+        const V3 nonIdFlow = vmul(vadd(vmul(gradCvM[f], surfaceT[f]), gradNonIdRho[f]), -1.);
+        nonIdLap[f] = vmul(vmul(nonIdFlow, surfaceRho[f]), 0.0);
+    }
+
+    // new mass fractions and concentrations (Diffusion.cpp:430-476)
+    std::vector<std::vector<double>> wNew(NS, std::vector<double>(nc));
+    std::vector<std::vector<double>> cN(NS + 1, std::vector<double>(nc));
+    for (long long i = 0; i < nc; ++i) {
+        double sum = 0.;
+        for (int k = 0; k < NS; ++k) {
+            double x = (oldW[k][i] + freeW[k][i] * dt) / diagW[k][i];
+            if (x < 0.) x = 0.0;
+            wNew[k][i] = x;
+            sum += x;
+        }
+        for (int k = 0; k < NS; ++k) wNew[k][i] /= sum;
+        cN[0][i] = 0;
+        for (int k = 1; k <= NS; ++k) {
+            cN[k][i] = wNew[k - 1][i] * cs.rho[0][i] / mx.M[k - 1];
+            cN[0][i] += cN[k][i];
+        }
+    }
+    std::vector<double> CCVNew(nc), oldEnergy(nc);
+    for (long long i = 0; i < nc; ++i) {
+        double cc[FV_MAX_SPECIES + 1];
+        for (int k = 0; k <= NS; ++k) cc[k] = cN[k][i];
+        CCVNew[i] = dCv(mx, cc) * cN[0][i];
+        const double nonIdNew = dNonIdeality(mx, cc);
+        oldEnergy[i] = CCVOld[i] * T[i] + nonIdOld[i] - nonIdNew;
+    }
+
+    // velocity and temperature matrices (Diffusion.cpp:480-500; SLEMatrix.cpp:2054-2110)
+    std::vector<V3> freeV(nc, v3(0, 0, 0)), oldV(nc);
+    {
+        std::vector<T9> flow(nf);
+        for (size_t f = 0; f < nf; ++f) flow[f] = tmul(tmul(gradVs[f], mu), -1.);
+        std::vector<V3> div;
+        dDivT(cs, flow, div);
+        for (long long i = 0; i < nc; ++i) {
+            oldV[i] = vmul(v[i], cs.rho[0][i]);
+            for (int d = 0; d < 3; ++d) freeV[i].x[d] -= div[i].x[d];
+        }
+    }
+    std::vector<double> freeT(nc, 0.0), diagT(CCVNew);
+    {
+        std::vector<V3> gT;
+        dSurfGrad(cs, T, [&](size_t f) { return dBoundaryT(cs, cs.faces[f].own, cs.faces[f].patch, true, bad); }, gT);
+        std::vector<V3> flow(nf);
+        for (size_t f = 0; f < nf; ++f) flow[f] = vmul(vmul(gT[f], kappa), -1.);
+        std::vector<double> div;
+        dDivV(cs, flow, div);
+        for (long long i = 0; i < nc; ++i) freeT[i] -= div[i];
+    }
+    // explicit deviatoric viscous stress on the velocity (Diffusion.cpp:503-506,600-605)
+    {
+        std::vector<T9> dev1(nf);
+        for (size_t f = 0; f < nf; ++f) dev1[f] = tmul(strainSurf1[f], mu);
+        std::vector<V3> div;
+        dDivT(cs, dev1, div);
+        for (long long i = 0; i < nc; ++i)
+            for (int d = 0; d < 3; ++d) freeV[i].x[d] += div[i].x[d];
+    }
+    {
+        std::vector<double> div;
+        dDivV(cs, nonIdLap, div);
+        for (long long i = 0; i < nc; ++i) {
+            const double s = div[i] * (-1.0);
+            if (s >= 0.) freeT[i] += s;
+            else diagT[i] -= s / (T[i] + kStab);
+        }
+    }
+    if (cf.enthalpy_flow == FV_ENTHALPY_EXPLICIT) {  // Diffusion.cpp:688-706
+        for (size_t f = 0; f < nf; ++f) entFlow[f] = vmul(entFlow[f], surfaceT[f]);
+        std::vector<double> div;
+        dDivV(cs, entFlow, div);
+        double mn = std::numeric_limits<double>::infinity();
+        for (long long i = 0; i < nc; ++i) mn = std::min(mn, CCVOld[i] * T[i] / std::fabs(div[i] + kStab));
+        cs.dtSource = cf.dt_coeff_source * mn;
+        for (long long i = 0; i < nc; ++i) {
+            const double s = div[i] * -1;
+            if (s >= 0.) freeT[i] += s;
+            else diagT[i] -= s / (T[i] + kStab);
+        }
+    }
+    for (long long i = 0; i < nc; ++i) {  // viscous heating: devPhysVisc && gradV
+        const T9 dev = tmul(strainVol[i], mu);
+        double dd = 0;
+        for (int q = 0; q < 9; ++q) dd += dev.x[q] * gradV[i].x[q];
+        freeT[i] += dd;
+    }
+    if (bad) {
+        cs.err = "fixedValueSurface is not a valid cell boundary value";
+        return FV_ERR_BOUNDARY;
+    }
+
+    // the phase after the stage (Diffusion.cpp:965-1034)
+    double Tmin = std::numeric_limits<double>::infinity();
+    cs.Tstate.assign(nc, 0.0);
+    cs.Tvalid = true;
+    for (long long i = 0; i < nc; ++i) {
+        V3 vn;
+        for (int d = 0; d < 3; ++d) vn.x[d] = (oldV[i].x[d] + freeV[i].x[d] * dt) / cs.rho[0][i];
+        const double Tn = (oldEnergy[i] + freeT[i] * dt) / diagT[i];
+        Tmin = std::min(Tmin, Tn);
+        cs.Tstate[i] = Tn;
+        double cc[FV_MAX_SPECIES + 1];
+        for (int k = 0; k <= NS; ++k) cc[k] = cN[k][i];
+        cs.c[0][i] = cN[0][i];
+        for (int k = 1; k <= NS; ++k) {
+            cs.c[k][i] = cN[k][i];
+            cs.rho[k][i] = cs.c[k][i] * mx.M[k - 1];
+        }
+        cs.v[i] = vn;
+        cs.m[i] = vmul(vn, cs.rho[0][i]);
+        cs.Uv[i] = dUvcFromT(mx, cc, Tn) * cs.c[0][i];
+        cs.p[i] = mx.pFromUv(cc, cs.Uv[i]);
+        const double v2 = vdot(vn, vn);
+        cs.E[i] = cs.Uv[i] + cs.rho[0][i] * v2 * 0.5 + 0.0;
+    }
+    if (cf.diffusion_timestep) {  // Diffusion.cpp:1036-1049
+        std::vector<double> maxVal(nf);
+        for (size_t f = 0; f < nf; ++f) maxVal[f] = std::max(std::max(kappa, surfaceRho[f] * Dc), mu);
+        double mn = std::numeric_limits<double>::infinity();
+        for (long long i = 0; i < nc; ++i) {
+            const Cell& c = cs.cells[i];
+            double sumDist = 0;
+            double dist[6];
+            for (int j = 0; j < c.nFaces; ++j) {
+                dist[j] = mag3(vsub(faceCentreFrom(i, cs.faces[c.faces[j]]), c.rC));
+                sumDist += dist[j];
+            }
+            double vol = 0;
+            for (int j = 0; j < c.nFaces; ++j) vol += maxVal[c.faces[j]] * (1 - dist[j] / sumDist);
+            mn = std::min(mn, vol * c.minLS * c.minLS);
+        }
+        cs.dtSource = std::min(cs.dtSource, 0.5 * cf.dt_coeff_diffusion / mn);
+    }
+    if (Tmin < 0.) {
+        cs.err = "Negative temperature after diffusion.";
+        return FV_ERR_NEGATIVE_T;
+    }
     return FV_OK;
 }
 
@@ -1911,8 +2474,8 @@ int chemistryStep(fvo_case& cs, double dt) {
     return FV_OK;
 }
 
-// main's CFL block (Schemi.cpp:807-833)
-double cflTimestep(const fvo_case& cs) {
+// main's CFL block (Schemi.cpp:807-833); it consumes the source time step a diffusion stage set
+double cflTimestep(fvo_case& cs) {
     double maxS = -std::numeric_limits<double>::infinity();
     for (long long i = 0; i < cs.nCells; ++i) {
         double cc[FV_MAX_SPECIES + 1];
@@ -1923,8 +2486,10 @@ double cflTimestep(const fvo_case& cs) {
         maxS = std::max(maxS, s);
     }
     double dt = cs.cfg.courant / maxS;
-    if (!cs.cfg.courant_only) dt = std::min(dt, kVeryBig);
+    cs.dtSourceLast = cs.dtSource;
+    if (!cs.cfg.courant_only) dt = std::min(dt, cs.dtSource);
     dt = std::max(dt, cs.cfg.min_timestep);
+    if (cs.cfg.const_timestep <= 0) cs.dtSource = kVeryBig;
     if (cs.cfg.const_timestep > 0) dt = cs.cfg.const_timestep;  // no CFL block (Schemi.cpp:807)
     return dt;
 }
@@ -1947,6 +2512,21 @@ bool validate(const fv_config& cf, std::string& err) {
     if (cf.order < FV_ORDER_SECOND || cf.order > FV_ORDER_THIRD_CADA) {
         err = "unknown step solver";
         return false;
+    }
+    if (cf.diffusion) {
+        if (cf.order != FV_ORDER_SECOND) { err = "the diffusion stage runs with the SecondOrder step"; return false; }
+        if (cf.flux != FV_FLUX_HLLC) { err = "the diffusion stage runs with the HLLC flux"; return false; }
+        if (cf.eos != FV_EOS_IDEAL && cf.eos != FV_EOS_VAN_DER_WAALS) {
+            err = "the diffusion stage runs with ideal and van der Waals mixtures";
+            return false;
+        }
+        if (cf.sle_solver != FV_SLE_EXPLICIT) { err = "the diffusion stage runs with the explicit solver"; return false; }
+        if (cf.transport != FV_TRANSPORT_CONSTANT) { err = "the diffusion stage runs with constant transport coefficients"; return false; }
+        if (cf.chemistry != FV_CHEM_NONE) { err = "the diffusion stage runs without chemistry"; return false; }
+        if (cf.enthalpy_flow < FV_ENTHALPY_NO || cf.enthalpy_flow > FV_ENTHALPY_EXPLICIT) {
+            err = "the explicit diffusion stage takes no or explicit enthalpy flow";
+            return false;
+        }
     }
     return true;
 }
@@ -2055,6 +2635,7 @@ int fvo_set_chem_carry(fvo_case* c, int carry) {
 }
 
 int fvo_upload(fvo_case* cs, const double* const* prim) {
+    cs->Tvalid = false;
     const int NS = cs->N;
     const Mix& mx = cs->mix;
     for (long long i = 0; i < cs->nCells; ++i) {
@@ -2089,6 +2670,11 @@ int fvo_step(fvo_case* cs, double* dt_used, double* dt_next) {
              : (order == FV_ORDER_THIRD || order == FV_ORDER_THIRD_CADA) ? rk3Step(*cs, dt, order == FV_ORDER_THIRD_CADA)
                                                                          : doStep(*cs, dt);
     if (st != FV_OK) return st;
+    if (cs->cfg.diffusion) {
+        // the diffusion stage after the advection (secondOrderStepSolver.cpp:69-80)
+        st = diffusionStage(*cs, dt);
+        if (st != FV_OK) return st;
+    }
     if (cs->cfg.chemistry != FV_CHEM_NONE) {
         // chemistry after the advection (and after the multi-stage average), same dt:
         // secondOrderStepSolver.cpp:87-91, secondOrderStepSolverRK.cpp:114-118,
@@ -2147,7 +2733,7 @@ int fvo_download(fvo_case* cs, double* const* out) {
         if (out[FV_F_MZ]) out[FV_F_MZ][i] = cs->m[i].x[2];
         if (out[FV_F_E]) out[FV_F_E][i] = cs->E[i];
         if (out[FV_F_UV]) out[FV_F_UV][i] = cs->Uv[i];
-        if (out[FV_F_T]) out[FV_F_T][i] = mx.TFromUv(cc, cs->Uv[i]);
+        if (out[FV_F_T]) out[FV_F_T][i] = cs->Tvalid ? cs->Tstate[i] : mx.TFromUv(cc, cs->Uv[i]);
         if (out[FV_F_SONIC]) out[FV_F_SONIC][i] = std::sqrt(mx.sqSonicSpeed(cc, cs->rho[0][i], cs->Uv[i], cs->p[i]));
         if (out[FV_F_CONC0]) out[FV_F_CONC0][i] = cs->c[0][i];
     }
@@ -2157,6 +2743,11 @@ int fvo_download(fvo_case* cs, double* const* out) {
 int fvo_get_time(const fvo_case* cs, double* time, double* dt) {
     if (time) *time = cs->time;
     if (dt) *dt = cs->dt;
+    return FV_OK;
+}
+
+int fvo_get_source_timestep(const fvo_case* cs, double* dt_source) {
+    if (dt_source) *dt_source = cs->dtSourceLast;
     return FV_OK;
 }
 
@@ -2178,6 +2769,7 @@ int fvo_get_conserved(const fvo_case* cs, double* const* out) {
 }
 
 int fvo_set_conserved(fvo_case* cs, const double* const* in) {
+    cs->Tvalid = false;
     const int NS = cs->N;
     for (long long i = 0; i < cs->nCells; ++i) {
         for (int k = 0; k < NS; ++k) cs->rho[k + 1][i] = in[k][i];

@@ -33,6 +33,7 @@ int fvo_download(fvo_case* c, double* const* out);
 
 int fvo_get_time(const fvo_case* c, double* time, double* dt);
 int fvo_set_time(fvo_case* c, double time, double dt);
+int fvo_get_source_timestep(const fvo_case* c, double* dt_source);
 
 /* Conserved state rho_1..rho_N, rho, m_x, m_y, m_z, E (n_cells each): get / set. */
 int fvo_get_conserved(const fvo_case* c, double* const* out);

@@ -11,6 +11,7 @@ Translation units (compiled in parallel):
   csrc/fv_batch.cu      batched ensemble (--fmad=false)
   csrc/fv_noalloc.cu    the step without device allocation (--fmad=false)
   csrc/fv_chem.cu       chemistry pass (Cl2, A+B->2C), FP64 (--fmad=false)
+  csrc/fv_diffusion.cu  diffusion stage (explicit, constant coefficients), FP64 (--fmad=false)
   csrc/fv_adjoint.cu    recorded trajectories, checkpoints and the adjoint sweep
   csrc/fv_adjoint_f64.cu / fv_adjoint_f32.cu  adjoint step kernels per arithmetic
 nvcc cross-compiles for sm_100a without a GPU.
@@ -23,6 +24,7 @@ from __future__ import annotations
 
 import concurrent.futures as cf
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -42,6 +44,7 @@ UNITS = {
     "fv_capi.cu": ["--fmad=false"],
     "fv_dispatch.cu": [],
     "fv_chem.cu": ["--fmad=false"],
+    "fv_diffusion.cu": ["--fmad=false"],
     "fv_adjoint.cu": [],
     "fv_adjoint_f64.cu": [],
     "fv_adjoint_f32.cu": ["-use_fast_math"],
@@ -59,9 +62,26 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
-def _headers():
-    """Sources every translation unit may include (a .cu file is only its own unit's source)."""
-    return [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".inc", ".h"))]
+_INCLUDE = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
+
+
+def _closure(path: str, seen=None) -> set:
+    """The file and every local header it includes, directly or through other headers (quoted
+    includes resolved beside the including file, then in csrc/ and include/)."""
+    seen = set() if seen is None else seen
+    path = os.path.normpath(path)
+    if path in seen or not os.path.exists(path):
+        return seen
+    seen.add(path)
+    with open(path, encoding="utf-8", errors="replace") as f:
+        text = f.read()
+    for name in _INCLUDE.findall(text):
+        for base in (os.path.dirname(path), CSRC, os.path.join(HERE, "..", "include")):
+            cand = os.path.join(base, name)
+            if os.path.exists(cand):
+                _closure(cand, seen)
+                break
+    return seen
 
 
 def _sources():
@@ -78,7 +98,6 @@ def _stale(target: str, deps) -> bool:
 def build(verbose: bool = False, force: bool = False, extra_flags=None) -> str:
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
-    deps = _headers() + [os.path.join(HERE, "..", "include", "fvstep.h")]
     units = dict(UNITS)
     if os.path.exists(os.path.join(CSRC, "fv_noalloc.cu")):
         units["fv_noalloc.cu"] = ["--fmad=false"]
@@ -89,7 +108,7 @@ def build(verbose: bool = False, force: bool = False, extra_flags=None) -> str:
     for unit, flags in units.items():
         obj = os.path.join(BUILD, unit.replace(".cu", ".o"))
         objs.append(obj)
-        if force or _stale(obj, deps + [os.path.join(CSRC, unit)]):
+        if force or _stale(obj, sorted(_closure(os.path.join(CSRC, unit)))):
             cmd = [nvcc(), *ARCH, *COMMON, *flags, *(extra_flags or []), "-c", os.path.join(CSRC, unit), "-o", obj]
             jobs.append(cmd)
     with cf.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 4))) as ex:

@@ -37,6 +37,9 @@ CHEM_SOLVERS = {"Gauss-Seidel": 0, "Jacobi": 1, "GaussElimination": 2, "conjugat
                 "JacobiConjugateGradient": 4}
 # #Approximation_order values with a GPU step (abstractStepSolver.cpp:56-146)
 ORDERS = {"SecondOrder": 0, "SecondOrderRK": 1, "ThirdOrder": 2, "ThirdOrderCada": 3}
+SLE_SOLVERS = {"explicit": 0, "GaussSeidel": 1}
+TRANSPORT_MODELS = {"constant": 0}
+ENTHALPY_FLOWS = {"no": 0, "explicit": 1, "implicit": 2}
 
 # patch order of the task files: #Tail, #Point, #Bottom, #Right, #Left, #Top
 PATCHES = ["tail", "point", "bottom", "right", "left", "top"]
@@ -94,6 +97,19 @@ class fv_config_t(ctypes.Structure):
         ("lj_sigma", ctypes.c_double * MAX_SPECIES),
         ("kataoka_b_critical", ctypes.c_int),
         ("kataoka_b_coeff", ctypes.c_double),
+        ("diffusion", ctypes.c_int),
+        ("sle_solver", ctypes.c_int),
+        ("sle_max_iter", ctypes.c_int),
+        ("transport", ctypes.c_int),
+        ("mu_const", ctypes.c_double),
+        ("D_const", ctypes.c_double),
+        ("kappa_const", ctypes.c_double),
+        ("enthalpy_flow", ctypes.c_int),
+        ("molmass_diffusion", ctypes.c_int),
+        ("linear_reconstruction", ctypes.c_int),
+        ("diffusion_timestep", ctypes.c_int),
+        ("dt_coeff_source", ctypes.c_double),
+        ("dt_coeff_diffusion", ctypes.c_double),
     ]
 
 
@@ -169,6 +185,20 @@ class Case:
     # Kataoka-van der Waals b rule (set/KataokaVanDerWaalsFluidData.txt): "critical" (b = coeff R Tc
     # / (8 Pc)) or "Kataoka" (b = coeff sigma^3 N_A), and its coefficient
     kataoka_b: Tuple[str, float] = ("critical", 1.0)
+    # diffusion stage (#Diffusion_flag, #Type_of_SLE_solver_flag, set/transportCoefficients.txt,
+    # #Reconstruction, #Source_timestep_correction "Courant-Source-Diffusion=<source>,<diffusion>")
+    diffusion: bool = False
+    sle_solver: str = "explicit"          # a key of SLE_SOLVERS
+    sle_max_iter: int = 2000
+    transport: str = "constant"           # a key of TRANSPORT_MODELS
+    mu: float = 0.0                       # #Viscosity_coefficient
+    D: float = 0.0                        # #Diffusion_coefficient
+    kappa: float = 0.0                    # #Heat_conduction_coefficient
+    enthalpy_flow: str = "explicit"       # a key of ENTHALPY_FLOWS
+    molmass_diffusion: bool = True
+    reconstruction: str = "star"          # "star" or "linear"
+    diffusion_timestep: bool = False
+    dt_coeffs: Tuple[float, float] = (0.25, 0.5)
 
     def __post_init__(self):
         for p in PATCHES_USED[self.dims]:
@@ -225,6 +255,16 @@ class Case:
             c.lj_eps[k], c.lj_sigma[k] = s.lj_eps, s.lj_sigma
         c.kataoka_b_critical = int(self.kataoka_b[0] == "critical")
         c.kataoka_b_coeff = float(self.kataoka_b[1])
+        c.diffusion = int(self.diffusion)
+        c.sle_solver = SLE_SOLVERS[self.sle_solver]
+        c.sle_max_iter = int(self.sle_max_iter)
+        c.transport = TRANSPORT_MODELS[self.transport]
+        c.mu_const, c.D_const, c.kappa_const = float(self.mu), float(self.D), float(self.kappa)
+        c.enthalpy_flow = ENTHALPY_FLOWS[self.enthalpy_flow]
+        c.molmass_diffusion = int(self.molmass_diffusion)
+        c.linear_reconstruction = int(self.reconstruction == "linear")
+        c.diffusion_timestep = int(self.diffusion_timestep)
+        c.dt_coeff_source, c.dt_coeff_diffusion = float(self.dt_coeffs[0]), float(self.dt_coeffs[1])
         c.eos = EOS[self.eos]
         c.flux = FLUX[self.flux]
         c.limiter = LIMITER[self.limiter]

@@ -246,6 +246,7 @@ fv_status checkSupported(fv_handle* h) {
                                     "limiter with zero multi-dimensional slopes); this case uses the generic path");
     if (h->cfg.eos != FV_EOS_IDEAL) return fail(h, FV_ERR_INIT, "the adjoint supports ideal-gas mixtures only");
     if (h->cfg.chemistry != FV_CHEM_NONE) return fail(h, FV_ERR_INIT, "the adjoint does not differentiate chemistry");
+    if (h->cfg.diffusion) return fail(h, FV_ERR_INIT, "the adjoint does not differentiate the diffusion stage");
     if (h->cfg.order != FV_ORDER_SECOND)
         return fail(h, FV_ERR_INIT, "the adjoint differentiates the SecondOrder (MUSCL-Hancock) step");
     return FV_OK;

@@ -135,6 +135,10 @@ fv_status fv_batch_create(fv_handle* const* handles, int n_cases, fv_batch** out
             fprintf(stderr, "fv_batch_create: case %d has chemistry (the ensemble kernel advances the flow only)\n", i);
             return FV_ERR_INIT;
         }
+        if (c.diffusion) {
+            fprintf(stderr, "fv_batch_create: case %d has diffusion (the ensemble kernel advances the flow only)\n", i);
+            return FV_ERR_INIT;
+        }
         if (c.order != FV_ORDER_SECOND) {
             fprintf(stderr, "fv_batch_create: case %d uses SecondOrderRK (the ensemble kernel runs SecondOrder)\n", i);
             return FV_ERR_INIT;

@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../include/fvstep.h"
+#include "fv_diffusion_launch.h"
 #include "fv_launch.cuh"
 #include "fv_validate.h"
 
@@ -64,14 +65,19 @@ __global__ void k_download(const StepParams P, const double* __restrict__ U, con
     if (i >= P.ncell) return;
     const long long n = P.ncell, s = P.stride;
     double c[NS + 1], v[3], p, rho0, rho[NS + 1], m[3], E;
-    const double* prim = ck->first ? prim0 : nullptr;
+    // the restart set before the first step; after a diffusion stage the primitives, energy and
+    // temperature it set (Diffusion.cpp:965-1025: the phase's T is the stage's, not TFromUv)
+    const bool stage = !ck->first && ck->stagePrim;
+    const double* prim = ck->first ? prim0 : (stage ? P.stagePrim : nullptr);
     switch (P.dims) {
     case 1: cellPrimitive<double, NS, EOS, 1>(P, U, prim, i, c, v, p, rho0, rho, m, E); break;
     case 2: cellPrimitive<double, NS, EOS, 2>(P, U, prim, i, c, v, p, rho0, rho, m, E); break;
     default: cellPrimitive<double, NS, EOS, 3>(P, U, prim, i, c, v, p, rho0, rho, m, E); break;
     }
     double Uv;
-    if (prim) {
+    if (stage) {
+        Uv = P.stagePrim[(NS + 4) * s + i];
+    } else if (prim) {
         Uv = Mixture<double, NS, EOS>::UvFromp(P.mix, c, p);
     } else {
         double v2 = 0;
@@ -92,7 +98,7 @@ __global__ void k_download(const StepParams P, const double* __restrict__ U, con
     out[FV_F_MZ * n + i] = m[2];
     out[FV_F_E * n + i] = E;
     out[FV_F_UV * n + i] = Uv;
-    out[FV_F_T * n + i] = Mixture<double, NS, EOS>::TFromUv(P.mix, c, Uv);
+    out[FV_F_T * n + i] = stage ? P.stagePrim[(NS + 5) * s + i] : Mixture<double, NS, EOS>::TFromUv(P.mix, c, Uv);
     out[FV_F_SONIC * n + i] = sqrt(Mixture<double, NS, EOS>::sqSonic(P.mix, c, rho0, Uv, p));
     out[FV_F_CONC0 * n + i] = c[0];
 }
@@ -345,6 +351,8 @@ StepBuffers buffersFor(fv_handle* h, int from) {
     B.FS = h->FS;
     B.FL = h->FL;
     B.L = h->L;
+    B.pcIn = h->pc[from];
+    B.pcOut = h->pc[from ^ 1];
     return B;
 }
 
@@ -402,6 +410,8 @@ cudaError_t chemistryAndFinalize(fv_handle* h, int from) {
 // U[from ^ 1] -> Ustage, average (Ustage, U[from]) -> U[from ^ 1] with the CFL partials.
 cudaError_t enqueueRk2(fv_handle* h, int from) {
     StepBuffers B1 = buffersFor(h, from);
+    B1.pcIn = nullptr;  // the stages do not use the primitive cache
+    B1.pcOut = nullptr;
     StepParams P2 = h->P;
     P2.conc = nullptr;  // stage 2 reads the first stage's own rho_k / M_k
     StepBuffers B2 = B1;
@@ -428,6 +438,8 @@ cudaError_t enqueueRk3(fv_handle* h, int from) {
     const bool f64 = h->cfg.precision == FV_PREC_F64;
     auto stage = [&](const StepParams& Ps, const double* in, double* out, const double* prim) {
         StepBuffers B = buffersFor(h, from);
+        B.pcIn = nullptr;  // the stages do not use the primitive cache
+        B.pcOut = nullptr;
         B.U = in;
         B.Un = out;
         B.prim0 = prim;
@@ -451,6 +463,17 @@ cudaError_t enqueueStep(fv_handle* h, int from) {
     if (h->cfg.order == FV_ORDER_SECOND_RK) return enqueueRk2(h, from);
     if (h->cfg.order == FV_ORDER_THIRD || h->cfg.order == FV_ORDER_THIRD_CADA) return enqueueRk3(h, from);
     const StepBuffers B = buffersFor(h, from);
+    if (h->cfg.diffusion) {
+        // secondOrderStepSolver::calculateStep: the advection, then the diffusion stage of the
+        // advected state with the same dt; main's CFL block reads the state after the stage
+        cudaError_t e = launchStepF64(h->P, B, h->path, h->shape, h->stream);
+        if (e != cudaSuccess) return e;
+        e = launchDiffusion(h->cfg.n_species, h->cfg.eos, h->cfg.dims, h->P, h->L, h->diff, h->U[from ^ 1], h->ck,
+                            h->blockMax, h->stream);
+        if (e != cudaSuccess) return e;
+        k_finalize<<<1, 1024, 0, h->stream>>>(h->P, h->ck, h->blockMax, diffusionBlocks(h->P));
+        return cudaGetLastError();
+    }
     if (h->cfg.chemistry == FV_CHEM_NONE) {
         // the step kernel's last CTA reduces the CFL partials and advances the clock
         StepParams Pf = h->P;
@@ -489,12 +512,34 @@ fv_status configureKernels(fv_handle* h) {
 fv_status ensureScratch(fv_handle* h) {
     long long nb = std::max(marchBlocks(h->P, h->shape), genericBlocks(h->P));
     if (h->cfg.chemistry != FV_CHEM_NONE) nb = std::max<long long>(nb, chemistryBlocks(h->P));
+    if (h->cfg.diffusion) nb = std::max<long long>(nb, diffusionBlocks(h->P));
     if (nb > h->blockMaxCap) {
         if (h->blockMax) cudaFree(h->blockMax);
         FV_CUDA(h, cudaMalloc(&h->blockMax, sizeof(double) * nb));
         h->blockMaxCap = nb;
     }
     if (configureKernels(h) != FV_OK) return FV_ERR_SYSTEM;
+    if (h->cfg.precision == FV_PREC_F64 && h->path == PATH_MARCH && warpStripMarch(h->P) && !h->pc[0]) {
+        // the FP64 warp strip's primitive cache: c_1..c_N, v_x, v_y, p and the 4 mixture
+        // coefficients of each cell, one array per state buffer
+        const size_t bytes = sizeof(double) * (size_t)(h->cfg.n_species + 7) * (size_t)h->P.ncell;
+        FV_CUDA(h, cudaMalloc(&h->pc[0], bytes));
+        FV_CUDA(h, cudaMalloc(&h->pc[1], bytes));
+    }
+    if (h->cfg.diffusion && !h->diff.face) {
+        // the stage's buffers: star velocities and face quantities per face, the advected
+        // primitives, the stage's primitives and the partial minima of its limits
+        const int ns = h->cfg.n_species;
+        const size_t nf = (size_t)h->L.nfaces, st = (size_t)h->P.stride;
+        diff::DiffParams& X = h->diff;
+        FV_CUDA(h, cudaMalloc(&X.starV, sizeof(double) * 3 * nf));
+        FV_CUDA(h, cudaMalloc(&X.face, sizeof(double) * (2 * ns + 9) * nf));
+        FV_CUDA(h, cudaMalloc(&X.cellPrim, sizeof(double) * (2 * ns + 5) * st));
+        FV_CUDA(h, cudaMalloc(&X.stagePrim, sizeof(double) * (ns + 6) * st));
+        FV_CUDA(h, cudaMalloc(&X.partMin, sizeof(double) * 2 * (size_t)diffusionBlocks(h->P)));
+        h->P.starV = X.starV;
+        h->P.stagePrim = X.stagePrim;
+    }
     if (h->path == PATH_GENERIC && !h->FS) {
         const size_t tsz = h->cfg.precision == FV_PREC_F64 ? sizeof(double) : sizeof(float);
         const int ns = h->cfg.n_species;
@@ -509,6 +554,7 @@ fv_status ensureScratch(fv_handle* h) {
 
 int choosePath(const fv_config& c) {
     if (c.dims < 2) return PATH_GENERIC;
+    if (c.diffusion) return PATH_GENERIC;  // the stage reads the generic path's Riemann star velocities
     if (c.eos != FV_EOS_IDEAL && c.eos != FV_EOS_VAN_DER_WAALS) return PATH_GENERIC;  // real-gas mixtures
     if (c.order == FV_ORDER_THIRD || c.order == FV_ORDER_THIRD_CADA) return PATH_GENERIC;  // directional slopes: k_faces3
     for (int a = 0; a < c.dims; ++a)
@@ -618,6 +664,20 @@ fv_status fv_create(const fv_config* cfg, fv_handle** out) {
     h->chem.Eb = cfg->chem_backward.E;
     h->chem.q = cfg->chem_q;
     h->chem.conc = nullptr;  // the multi-stage enqueues pass the stored concentrations
+    if (cfg->diffusion) {
+        diff::DiffParams& X = h->diff;
+        X.mu = cfg->mu_const;
+        X.D = cfg->D_const;
+        X.kappa = cfg->kappa_const;
+        X.enthalpy = cfg->enthalpy_flow == FV_ENTHALPY_EXPLICIT;
+        X.molmass = cfg->molmass_diffusion != 0;
+        // gravity invalidates the star velocities (secondOrderStepSolver.cpp:71-73); the
+        // "linear" reconstruction takes the cell velocities' gradient (Diffusion.cpp:178-184)
+        X.interpV = cfg->gravity || cfg->linear_reconstruction;
+        X.dtDiff = cfg->diffusion_timestep != 0;
+        X.coeffSource = cfg->dt_coeff_source;
+        X.coeffDiff = cfg->dt_coeff_diffusion;
+    }
     h->shape = defaultShape(*cfg);
 
     // generic face layout
@@ -708,11 +768,15 @@ void fv_destroy(fv_handle* h) {
     if (h->ck) cudaFree(h->ck);
     if (h->ckHost) cudaFreeHost(h->ckHost);
     if (h->blockMax) cudaFree(h->blockMax);
+    for (double* q : h->pc)
+        if (q) cudaFree(q);
     if (h->geo) cudaFree(h->geo);
     if (h->Pc) cudaFree(h->Pc);
     if (h->FS) cudaFree(h->FS);
     if (h->FL) cudaFree(h->FL);
     if (h->outBuf) cudaFree(h->outBuf);
+    for (double* q : {h->diff.starV, h->diff.face, h->diff.cellPrim, h->diff.stagePrim, h->diff.partMin})
+        if (q) cudaFree(q);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -914,6 +978,15 @@ fv_status fv_get_time(const fv_handle* hc, double* time, double* dt) {
     return FV_OK;
 }
 
+fv_status fv_get_source_timestep(const fv_handle* hc, double* dt_source) {
+    fv_handle* h = const_cast<fv_handle*>(hc);
+    if (!h) return FV_ERR_INIT;
+    fv_status st = readClock(h);
+    if (st != FV_OK) return st;
+    if (dt_source) *dt_source = h->ckHost->dtSourceLast > 0 ? h->ckHost->dtSourceLast : kVeryBigD();
+    return FV_OK;
+}
+
 fv_status fv_set_time(fv_handle* h, double time, double dt) {
     if (!h) return FV_ERR_INIT;
     fv_status st = readClock(h);
@@ -972,6 +1045,7 @@ long long fv_kernels_per_step(const fv_handle* h) {
     if (!h) return 0;
     const int stage = h->path == PATH_MARCH ? 1 : 4;
     const int chem = h->cfg.chemistry != FV_CHEM_NONE ? 1 : 0;
+    if (h->cfg.diffusion) return stage + 5;  // the stage's 4 kernels, finalize
     if (h->cfg.order == FV_ORDER_SECOND_RK) return 2 * stage + 2 + chem;  // two stages, average, finalize
     if (h->cfg.order == FV_ORDER_THIRD || h->cfg.order == FV_ORDER_THIRD_CADA)
         return 3 * stage + 3 + chem;  // three stages, two averages, finalize

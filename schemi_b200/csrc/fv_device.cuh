@@ -662,7 +662,10 @@ struct FaceFlux {
 // applies (NaN wave speeds), which the reference reports as RiemannSolverError.
 template <typename T, int NS>
 __device__ __forceinline__ bool riemann(int flux, int axis, int sign, const FaceState<T, NS>& O,
-                                        const FaceState<T, NS>& B, FaceFlux<T, NS>& F) {
+                                        const FaceState<T, NS>& B, FaceFlux<T, NS>& F, T* sv = nullptr) {
+    // sv (HLLC, not null): the face velocity the solver hands the diffusion stage (starValues.v,
+    // HLLCSolver.cpp:399): the side's velocity outside the star region, the star momentum over
+    // the star density inside it
     const T sg = T(sign);
     const T uO = O.v[axis] * sg, uN = B.v[axis] * sg;
     const T SO = smin(uO - O.cs, uN - B.cs);
@@ -679,6 +682,10 @@ __device__ __forceinline__ bool riemann(int flux, int axis, int sign, const Face
 #pragma unroll
             for (int d = 0; d < 3; ++d) F.m[d] = O.m[d] * uO + (d == axis ? sg : T(0)) * (O.p + T(0));
             F.E = uO * (O.E + O.p + T(0));
+            if (sv) {
+#pragma unroll
+                for (int d = 0; d < 3; ++d) sv[d] = O.v[d];
+            }
         } else if (Sc >= T(0) || SN > T(0)) {
             // star flux of the side the contact leaves (owner when Sc >= 0): the reference's two
             // branches are the same expression on (O, uO, SO) or (B, uN, SN)
@@ -690,10 +697,12 @@ __device__ __forceinline__ bool riemann(int flux, int axis, int sign, const Face
                     const T rs = rw[k] * factor * den;
                     F.rho[k] = rw[k] * u + S * (rs - rw[k]);
                 }
+                const T rs0 = rw[0] * factor * den;
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     const T ms = (mw[d] * factor - (d == axis ? sg : T(0)) * (pw + T(0) - PON)) * den;
                     F.m[d] = mw[d] * u + (d == axis ? sg : T(0)) * (pw + T(0)) + (ms - mw[d]) * S;
+                    if (sv) sv[d] = ms / rs0;
                 }
                 const T Es = (Ew * factor - (pw + T(0)) * u + PON * Sc) * den;
                 F.E = (Ew + pw + T(0)) * u + S * (Es - Ew);
@@ -719,6 +728,10 @@ __device__ __forceinline__ bool riemann(int flux, int axis, int sign, const Face
 #pragma unroll
             for (int d = 0; d < 3; ++d) F.m[d] = B.m[d] * uN + (d == axis ? sg : T(0)) * (B.p + T(0));
             F.E = uN * (B.E + B.p + T(0));
+            if (sv) {
+#pragma unroll
+                for (int d = 0; d < 3; ++d) sv[d] = B.v[d];
+            }
         } else {
             return false;
         }

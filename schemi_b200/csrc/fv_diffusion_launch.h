@@ -1,0 +1,40 @@
+// fv_diffusion_launch.h -- launcher of the diffusion stage (fv_diffusion.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "fv_kernels.cuh"
+
+namespace fv {
+
+struct GenericLayout;
+namespace diff {
+
+// Coefficients and buffers of the stage (allocated by the handle when cfg.diffusion is on).
+struct DiffParams {
+    double mu, D, kappa;       // constant transport coefficients
+    int enthalpy;              // 1: explicit enthalpy flow
+    int molmass;               // 1: molar-mass diffusion correction
+    int interpV;               // 1: cell velocity gradient from interpolated cell velocities
+                               //    ("linear" reconstruction, or gravity), else the star velocities
+    int dtDiff;                // 1: "Courant-Source-Diffusion" (the diffusion limit)
+    double coeffSource, coeffDiff;
+    double* starV;             // [3][faces] Riemann star velocity of the advection (replaced by
+                               //    the interpolated cell velocity when interpV)
+    double* cellPrim;          // [2N + 5][stride]: c_1..c_N, v_x, v_y, v_z, p, T, w_1..w_N
+    double* face;              // [2N + 9][faces] face quantities (see faceSlots)
+    double* stagePrim;         // [N + 6][stride]: c_1..c_N, v, p, Uv, T after the stage
+    double* partMin;           // [2][blocks] per-CTA minima of the enthalpy and diffusion limits
+};
+
+}  // namespace diff
+
+// CTAs of the stage's cell kernel (= blockMax entries it writes, and the partial minima per limit).
+int diffusionBlocks(const StepParams& P);
+
+// Enqueue the diffusion stage of the advected state U (in place) with the clock's dt: the new
+// state, its primitives (P.stagePrim), the CFL block maxima and the clock's source time step.
+cudaError_t launchDiffusion(int ns, int eos, int dims, const StepParams& P, const GenericLayout& L,
+                            const diff::DiffParams& X, double* U, DevClock* ck, double* blockMax, cudaStream_t st);
+
+}  // namespace fv

@@ -147,7 +147,8 @@ template <typename T, int NS, int EOS, int D>
 __global__ void k_prim(const StepParams P, const double* __restrict__ U, const double* __restrict__ prim0,
                        DevClock* __restrict__ ck, T* __restrict__ Pc) {
     if (ck->done) return;
-    const double* prim = ck->first ? prim0 : nullptr;
+    // the restart set at the first step, the primitives of a diffusion stage after one
+    const double* prim = ck->first ? prim0 : (ck->stagePrim ? P.stagePrim : nullptr);
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= P.ncell) return;
     T c[NS + 1], v[3], p, r0, rr[NS + 1], mm[3], EE;
@@ -851,18 +852,24 @@ __global__ void k_fluxes(const StepParams P, const GenericLayout L, const T* __r
     const bool boundary = !P.periodic[a] && (fi == 0 || fi == n);
     FaceFlux<T, NS> F;
     bool ok;
+    T sv[3];
+    T* svp = P.starV ? sv : nullptr;
     if (boundary) {
         const int sign = fi == 0 ? -1 : 1;
         const int patch = a == 0 ? (fi == 0 ? FV_PATCH_TAIL : FV_PATCH_POINT)
                                  : a == 1 ? (fi == 0 ? FV_PATCH_RIGHT : FV_PATCH_LEFT)
                                           : (fi == 0 ? FV_PATCH_BOTTOM : FV_PATCH_TOP);
         ghostState<T, NS, EOS>(P.mix, P.bc, patch, a, sign, O, B);
-        ok = riemann<T, NS>(P.flux, a, sign, O, B, F);
+        ok = riemann<T, NS>(P.flux, a, sign, O, B, F, svp);
     } else {
         loadFace<T, NS>(FS, nf, 1, f, B);
-        ok = riemann<T, NS>(P.flux, a, 1, O, B, F);
+        ok = riemann<T, NS>(P.flux, a, 1, O, B, F, svp);
     }
     if (!ok) raise(ck, FV_ERR_RIEMANN);
+    if (P.starV) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) P.starV[d * nf + f] = double(sv[d]);
+    }
     int q = 0;
 #pragma unroll
     for (int k = 0; k <= NS; ++k) FL[(q++) * nf + f] = F.rho[k];
@@ -948,6 +955,9 @@ __global__ void k_update(const StepParams P, const GenericLayout L, const double
     }
     const T bm = blockMaxReduce<T>(localMax, red);
     if (threadIdx.x == 0) blockMax[blockIdx.x] = double(bm);
+    // the advected state's primitives follow from its conserved variables again (k_prim of this
+    // step has read the flag)
+    if (i == 0) ck->stagePrim = 0;
     if (P.fuseFinalize) finalizeIfLast(P, ck, blockMax, (int)gridDim.x, gridDim.x);
 }
 

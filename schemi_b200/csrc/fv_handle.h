@@ -7,6 +7,7 @@
 
 #include "../../include/fvstep.h"
 #include "fv_chem_launch.h"
+#include "fv_diffusion_launch.h"
 #include "fv_launch.cuh"
 
 using namespace fv;
@@ -32,6 +33,7 @@ struct fv_handle {
     DevClock* ckHost = nullptr;    // pinned mirror
     double* blockMax = nullptr;
     long long blockMaxCap = 0;
+    double* pc[2] = {nullptr, nullptr};  // FP64 warp strip: primitive cache of U[0] / U[1]
     double* geo = nullptr;         // all geometry tables
     void* Pc = nullptr;            // generic scratch
     void* FS = nullptr;
@@ -40,6 +42,7 @@ struct fv_handle {
     double* outBuf = nullptr;      // download staging
     int path = PATH_GENERIC;
     chem::ChemParams chem{};       // chemistry pass (cfg.chemistry != FV_CHEM_NONE)
+    diff::DiffParams diff{};       // diffusion stage (cfg.diffusion): its buffers and coefficients
     MarchShape shape{128, 1, 32};
     int nConserved = 0;
     // graphs of step chunks, one per start buffer

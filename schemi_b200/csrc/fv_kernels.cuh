@@ -62,6 +62,10 @@ struct StepParams {
     double ext[3];          // parallelepiped extents (the transverse sizes of 1D / 2D cells)
     int fuseFinalize;       // 1: the step kernel's last CTA runs the CFL finalize (no k_finalize launch)
     int pad0;
+    double* starV;          // not null: k_fluxes stores each face's Riemann star velocity here
+                            // ([3][faces], HLLCSolver.cpp:399) for the diffusion stage
+    const double* stagePrim;  // primitives a diffusion stage left (c_1..c_N, v, p, Uv, T; stride
+                              // apart): the next step reads them when the clock's stagePrim is set
     MixParams mix;
     BCParams bc;
     Geometry geo;
@@ -83,8 +87,19 @@ struct DevClock {
     unsigned ticket;    // CTAs of the running step that have written their CFL partials (fused
                         // finalize); the last one resets it to 0
     int flag;           // scratch word of host-side checks (the transverse-velocity test of an upload)
-    int pad;
+    int pcValid;        // 1: the primitive cache of the buffer to read holds this state's primitives
+                        // (written by the last FP64 warp-strip step; every other writer clears it)
+    int stagePrim;      // 1: the state's primitives are those a diffusion stage set (P.stagePrim),
+                        // not the ones its conserved variables give; cleared by the next advection
+    double dtSource;    // mesh::timestepSource: the limit a diffusion stage sets for the next step;
+                        // 0 stands for the reference's initial and reset value (veryBig), so that a
+                        // zeroed clock holds it; main's CFL block takes it and resets it
+    double dtSourceLast;  // the limit the last CFL block took (same encoding)
 };
+
+__host__ __device__ inline double sourceTimestep(const DevClock* ck) {
+    return ck->dtSource > 0 ? ck->dtSource : kVeryBigD();
+}
 
 __device__ __forceinline__ void raise(DevClock* ck, int code) { atomicCAS(&ck->err, 0, code); }
 
@@ -383,6 +398,33 @@ __device__ __forceinline__ T cellSignalC(const StepParams& P, const T* c, T rho0
     return s;
 }
 
+// CFL signal of a cell from its conserved values (c_k = rho_k / M_k) that also returns the
+// primitives it recovers on the way (c, v, p and the mixture coefficients of c): exactly what
+// cellPrimitive computes from the same state.
+template <typename T, int NS, int EOS>
+__device__ __forceinline__ T cellSignalPrim(const StepParams& P, const T* rho, T rho0, const T* m, T E, T minLS,
+                                            T* c, T* v, T& p, typename Mixture<T, NS, EOS>::Coef& k) {
+    c[0] = 0;
+#pragma unroll
+    for (int q = 1; q <= NS; ++q) {
+        c[q] = rho[q] / T(P.mix.M[q - 1]);
+        c[0] += c[q];
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) v[d] = d < P.nmom ? m[d] / rho0 : T(0);
+    T v2 = 0;
+    v2 += v[0] * v[0];
+    v2 += v[1] * v[1];
+    v2 += v[2] * v[2];
+    const T Uv = E - rho0 * v2 * T(0.5) - T(0);
+    k = Mixture<T, NS, EOS>::coef(P.mix, c);
+    p = Mixture<T, NS, EOS>::pFromUv(k, c, Uv);
+    const T sonic = Num<T>::sqrt_(Mixture<T, NS, EOS>::sqSonic(k, c, rho0, Uv, p));
+    T s = (P.nmom == 3 ? mag3<T>(v[0], v[1], v[2]) : mag2z<T>(v[0], v[1])) + sonic;
+    s *= minLS;
+    return s;
+}
+
 // The same from conserved values (c_k = rho_k / M_k).
 template <typename T, int NS, int EOS, int D>
 __device__ __forceinline__ T cellSignal(const StepParams& P, const T* rho, T rho0, const T* m, T E, T minLS) {
@@ -401,7 +443,7 @@ __device__ __forceinline__ T cellSignal(const StepParams& P, const T* rho, T rho
 // time += dt_used; g += g_delta * dt_used; clamp to t_end (Schemi.cpp:802-835, 933-935).
 // Executed by one CTA.
 __device__ __forceinline__ void finalizeCase(const StepParams& P, DevClock* ck, const double* __restrict__ blockMax,
-                                             int nblocks) {
+                                             int nblocks, int pcValidAfter = 0) {
     __shared__ double red[32];
     if (ck->done) return;
     const int tid = threadIdx.x + threadIdx.y * blockDim.x;
@@ -413,9 +455,11 @@ __device__ __forceinline__ void finalizeCase(const StepParams& P, DevClock* ck, 
     if (tid != 0) return;
     const double dtUsed = ck->dt;
     double dtn = P.courant / m;
-    if (!P.courant_only) dtn = smin(dtn, kVeryBigD());
+    ck->dtSourceLast = ck->dtSource;
+    if (!P.courant_only) dtn = smin(dtn, sourceTimestep(ck));
     dtn = smax(dtn, P.min_dt);
     if (P.const_dt > 0) dtn = P.const_dt;  // Schemi.cpp:807: no CFL block with a constant step
+    else ck->dtSource = 0;                  // Schemi.cpp:833 (veryBig)
     if (P.gravity) {
         for (int d = 0; d < 3; ++d) ck->g[d] += ck->g_delta[d] * dtUsed;
     }
@@ -426,6 +470,7 @@ __device__ __forceinline__ void finalizeCase(const StepParams& P, DevClock* ck, 
     ck->dt_free = dtn;
     if ((ck->time + dtn) > ck->t_end) dtn = ck->t_end - ck->time;
     ck->dt = dtn;
+    ck->pcValid = pcValidAfter;
     if (!(ck->time < ck->t_end) || ck->err) ck->done = 1;
 }
 
@@ -435,7 +480,7 @@ __device__ __forceinline__ void finalizeCase(const StepParams& P, DevClock* ck, 
 // next step.  Every CTA has read the clock before it takes its ticket, so the last one may
 // advance it.
 __device__ __forceinline__ void finalizeIfLast(const StepParams& P, DevClock* ck, const double* __restrict__ blockMax,
-                                               int nPartials, unsigned nCtas) {
+                                               int nPartials, unsigned nCtas, int pcValidAfter = 0) {
     __shared__ int isLast;
     __syncthreads();
     if (threadIdx.x == 0 && threadIdx.y == 0) {
@@ -445,7 +490,7 @@ __device__ __forceinline__ void finalizeIfLast(const StepParams& P, DevClock* ck
     __syncthreads();
     if (!isLast) return;
     __threadfence();
-    finalizeCase(P, ck, blockMax, nPartials);
+    finalizeCase(P, ck, blockMax, nPartials, pcValidAfter);
     if (threadIdx.x == 0 && threadIdx.y == 0) ck->ticket = 0u;
 }
 

@@ -28,6 +28,8 @@ struct StepBuffers {
     void* FS;            // generic path: face states (T)
     void* FL;            // generic path: face fluxes (T)
     GenericLayout L;
+    const double* pcIn;  // FP64 warp strip: primitive cache of U (null: none)
+    double* pcOut;       // FP64 warp strip: primitive cache of Un, written by a fused step
 };
 
 enum StepPath { PATH_MARCH = 0, PATH_GENERIC = 1 };

@@ -181,6 +181,10 @@ extern "C" fv_status fv_step_noalloc(const fv_config* cfg, const double* state_i
         fprintf(stderr, "fv_step_noalloc: the step without device allocation has no chemistry pass\n");
         return FV_ERR_INIT;
     }
+    if (cfg->diffusion) {
+        fprintf(stderr, "fv_step_noalloc: the step without device allocation has no diffusion stage\n");
+        return FV_ERR_INIT;
+    }
     StepParams P;
     std::string why;
     if (!buildParams(*cfg, P, why)) {

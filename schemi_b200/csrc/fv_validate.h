@@ -22,12 +22,6 @@ inline bool fvValidateConfig(const fv_config& c, std::string& e) {
                 e = "stiffened gas needs gamma > 1 and p0 >= 0 for every species";
                 return false;
             }
-    if (c.eos == FV_EOS_REDLICH_KWONG || c.eos == FV_EOS_KATAOKA || c.eos == FV_EOS_VAN_DER_WAALS)
-        for (int k = 0; k < c.n_species; ++k)
-            if (!(c.Tc[k] > 0) || !(c.Pc[k] > 0)) {
-                e = "the critical temperature and pressure of every species must be positive";
-                return false;
-            }
     if (c.eos == FV_EOS_KATAOKA) {
         for (int k = 0; k < c.n_species; ++k)
             if (!(c.lj_sigma[k] > 0) || !(c.lj_eps[k] >= 0)) {
@@ -35,6 +29,28 @@ inline bool fvValidateConfig(const fv_config& c, std::string& e) {
                 return false;
             }
         if (!(c.kataoka_b_coeff > 0)) { e = "Kataoka needs a positive b coefficient"; return false; }
+    }
+    if (c.diffusion) {
+        // the diffusion stage (Diffusion.cpp) this build runs: after the SecondOrder advection, HLLC
+        // star velocities, FP64, ideal or van der Waals, constant coefficients, the explicit
+        // solver, no or explicit enthalpy flow, no chemistry
+        if (c.order != FV_ORDER_SECOND) { e = "the diffusion stage runs with the SecondOrder step"; return false; }
+        if (c.flux != FV_FLUX_HLLC) { e = "the diffusion stage runs with the HLLC flux"; return false; }
+        if (c.precision != FV_PREC_F64) { e = "the diffusion stage runs in FP64"; return false; }
+        if (c.eos != FV_EOS_IDEAL && c.eos != FV_EOS_VAN_DER_WAALS) {
+            e = "the diffusion stage runs with ideal and van der Waals mixtures";
+            return false;
+        }
+        if (c.chemistry != FV_CHEM_NONE) { e = "the diffusion stage runs without chemistry"; return false; }
+        if (c.sle_solver != FV_SLE_EXPLICIT) { e = "the diffusion stage runs with the explicit solver"; return false; }
+        if (c.transport != FV_TRANSPORT_CONSTANT) {
+            e = "the diffusion stage runs with constant transport coefficients";
+            return false;
+        }
+        if (c.enthalpy_flow != FV_ENTHALPY_NO && c.enthalpy_flow != FV_ENTHALPY_EXPLICIT) {
+            e = "the explicit diffusion stage takes no or explicit enthalpy flow";
+            return false;
+        }
     }
     if (c.flux != FV_FLUX_HLLC && c.flux != FV_FLUX_HLL) { e = "unknown flux solver"; return false; }
     if (c.limiter < 0 || c.limiter > FV_LIM_SCHMIDTMANN) { e = "unknown limiter"; return false; }

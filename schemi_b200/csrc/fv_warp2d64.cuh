@@ -52,11 +52,18 @@ template <int NS> __device__ __forceinline__ void shflDownF(const FaceFlux<doubl
 
 // One strip of the FP64 march: columns xs .. xs + 29 (lanes 1..30), rows z0 .. z0 + rows - 1.
 // Returns the lane's CFL signal maximum (-1 when it updated nothing).
+//
+// Primitive cache (pcIn / pcOut, one array per state buffer, N + 7 fields of n_cells doubles:
+// c_1..c_N, v_x, v_y, p and the mixture coefficients g1, a, b, M): the epilogue recovers c, v, p and
+// the coefficients of the updated cell for its CFL signal, which are exactly what the next step's
+// closure recovers again from the same FP64 state (same operations on the same values).  A fused
+// step writes them to pcOut and its finalize marks the clock's cache valid; the next step then
+// reads them (pcIn) instead of recomputing them.  Any other writer of the state clears the mark.
 template <int NS, int EOS>
 __device__ __forceinline__ double warpStrip64(const StepParams& P, const double* __restrict__ U,
                                               double* __restrict__ Un, const double* __restrict__ prim,
                                               DevClock* __restrict__ ck, double dt, const double* g, int xs, int z0,
-                                              int rows) {
+                                              int rows, const double* __restrict__ pcIn, double* __restrict__ pcOut) {
     constexpr int NF = NS + 4;  // rho_1..rho_N, rho, m_x, m_y, E
     const int lane = threadIdx.x & 31;
     const int nx = P.n[0], ny = P.n[1];
@@ -112,8 +119,27 @@ __device__ __forceinline__ double warpStrip64(const StepParams& P, const double*
         double c[NS + 1], v[3], p, r0, rr[NS + 1], mm[3], EE;
         typename Mixture<double, NS, EOS>::Coef kc;
         bool haveK;
-        cellPrimitive<double, NS, EOS, 2>(P, sc, (has && ok) ? prim : nullptr, i, c, v, p, r0, rr, mm, EE, &kc,
-                                          &haveK);
+        if (pcIn && has && ok) {
+            const double* q = pcIn + i;
+            c[0] = 0;
+#pragma unroll
+            for (int k = 1; k <= NS; ++k) {
+                c[k] = __ldg(q + (k - 1) * st);
+                c[0] += c[k];
+            }
+            v[0] = __ldg(q + NS * st);
+            v[1] = __ldg(q + (NS + 1) * st);
+            v[2] = 0.0;
+            p = __ldg(q + (NS + 2) * st);
+            kc.g1 = __ldg(q + (NS + 3) * st);
+            kc.am = __ldg(q + (NS + 4) * st);
+            kc.bm = __ldg(q + (NS + 5) * st);
+            kc.Mm = __ldg(q + (NS + 6) * st);
+            haveK = true;
+        } else {
+            cellPrimitive<double, NS, EOS, 2>(P, sc, (has && ok) ? prim : nullptr, i, c, v, p, r0, rr, mm, EE, &kc,
+                                              &haveK);
+        }
         cellFaceState<double, NS, EOS>(P.mix, c, v, p, W, 2, P.hancock != 0, haveK ? &kc : nullptr);
         vp[0] = v[0];
         vp[1] = v[1];
@@ -222,7 +248,22 @@ __device__ __forceinline__ double warpStrip64(const StepParams& P, const double*
             Un[(NS + 1) * st + ic] = mNew[0];
             Un[(NS + 2) * st + ic] = mNew[1];
             Un[(NS + 4) * st + ic] = Enew;
-            localMax = smax(localMax, cellSignal<double, NS, EOS, 2>(P, rNew, rNew[0], mNew, Enew, minLS));
+            double cN[NS + 1], vN[3], pN;
+            typename Mixture<double, NS, EOS>::Coef kN;
+            localMax = smax(localMax,
+                            cellSignalPrim<double, NS, EOS>(P, rNew, rNew[0], mNew, Enew, minLS, cN, vN, pN, kN));
+            if (pcOut) {
+                double* q = pcOut + ic;
+#pragma unroll
+                for (int k = 1; k <= NS; ++k) q[(k - 1) * st] = cN[k];
+                q[NS * st] = vN[0];
+                q[(NS + 1) * st] = vN[1];
+                q[(NS + 2) * st] = pN;
+                q[(NS + 3) * st] = kN.g1;
+                q[(NS + 4) * st] = kN.am;
+                q[(NS + 5) * st] = kN.bm;
+                q[(NS + 6) * st] = kN.Mm;
+            }
         }
         // roll the marching window
         Gprev = Gnext;
@@ -246,22 +287,27 @@ __global__ void __launch_bounds__(32 * NW, MINB) k_warp2d64(const StepParams P, 
                                                             double* __restrict__ Un,
                                                             const double* __restrict__ prim0,
                                                             DevClock* __restrict__ ck, double* __restrict__ blockMax,
-                                                            int rows) {
+                                                            int rows, const double* __restrict__ pcIn,
+                                                            double* __restrict__ pcOut) {
     if (ck->done) return;  // uniform over the grid
     const int w = threadIdx.x >> 5;
     const double* prim = ck->first ? prim0 : nullptr;
+    // the cache is read when the clock marks it valid (never before the first step, which reads
+    // the restart set) and written only by a step that finalizes itself (and so marks it)
+    const double* pcUse = (pcIn && ck->pcValid && !ck->first) ? pcIn : nullptr;
+    double* pcWrite = P.fuseFinalize ? pcOut : nullptr;
     const int strip = blockIdx.x * NW + w;
     const int xs = strip * kWarpStripCols;
     double m = -1;
     if (xs < P.n[0])
-        m = warpStrip64<NS, EOS>(P, U, Un, prim, ck, ck->dt, ck->g, xs, blockIdx.y * rows, rows);
+        m = warpStrip64<NS, EOS>(P, U, Un, prim, ck, ck->dt, ck->g, xs, blockIdx.y * rows, rows, pcUse, pcWrite);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = smax(m, __shfl_xor_sync(0xffffffffu, m, o));
     const long long part = (blockIdx.x + (long long)gridDim.x * blockIdx.y) * NW + w;
     if ((threadIdx.x & 31) == 0) blockMax[part] = m;
     if (P.fuseFinalize) {
         const unsigned n = gridDim.x * gridDim.y;
-        finalizeIfLast(P, ck, blockMax, (int)(n * NW), n);
+        finalizeIfLast(P, ck, blockMax, (int)(n * NW), n, pcWrite ? 1 : 0);
     }
 }
 

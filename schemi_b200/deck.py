@@ -41,6 +41,18 @@ explicit
 #Flag_for_molar_mass_diffusion_correction
 on"""
 
+def _transport_block(case):
+    """set/transportCoefficients.txt of a diffusion deck (phaseInitialization.cpp:193-243)."""
+    return "\n".join([
+        "#Transport_coefficient_model", case.transport,
+        "#Viscosity_coefficient", _f(case.mu),
+        "#Diffusion_coefficient", _f(case.D),
+        "#Heat_conduction_coefficient", _f(case.kappa),
+        "#Flag_for_enthalpy_flow_solution", case.enthalpy_flow,
+        "#Flag_for_molar_mass_diffusion_correction", "on" if case.molmass_diffusion else "off",
+    ])
+
+
 _TURB_PARAMS = """#Cmu
 0.09
 #Turbulent_Schmidt
@@ -170,7 +182,9 @@ def write_deck(case: Case, directory: str, prim: Sequence[np.ndarray], frequency
     dims_name = {1: "1D", 2: "2D", 3: "3D"}[case.dims]
     ncell = [nx, ny if case.dims >= 2 else 1, nz if case.dims >= 3 else 1]
     # "<type>=<source coefficient>,<diffusion coefficient>" (Schemi.cpp:180-243)
-    src_ts = ("Courant" if case.courant_only else "Courant-Source") + "=0.25,0.5"
+    src_ts = ("Courant" if case.courant_only else
+              "Courant-Source-Diffusion" if case.diffusion_timestep else "Courant-Source") + \
+        f"={_f(case.dt_coeffs[0])},{_f(case.dt_coeffs[1])}"
     main = [
         ("#Radius-vector_of_system's_parallelepiped", " ".join(_f(x) for x in case.L)),
         ("#Number_of_cells_in_direction", " ".join(str(x) for x in ncell)),
@@ -182,16 +196,16 @@ def write_deck(case: Case, directory: str, prim: Sequence[np.ndarray], frequency
         ("#Defines_universal_gas_constant", case.R_units),
         ("#Equation_of_state", case.eos),
         ("#TVD_limiter_type", case.limiter),
-        ("#Number_of_iterations_of_SLE_matrix_solver", "2000"),
-        ("#Diffusion_flag", "off"),
+        ("#Number_of_iterations_of_SLE_matrix_solver", str(case.sle_max_iter)),
+        ("#Diffusion_flag", "on" if case.diffusion else "off"),
         ("#Turbulence_flag", "off"),
-        ("#Type_of_SLE_solver_flag", "GaussSeidel"),
+        ("#Type_of_SLE_solver_flag", case.sle_solver if case.diffusion else "GaussSeidel"),
         ("#Type_of_source_flag", "BHR"),
         ("#Type_of_flow_solver", case.flux),
         ("#Dimensions_of_the_task", dims_name),
         ("#Constant_timestep", _f(case.const_timestep) if case.const_timestep > 0 else "-1E-8"),
         ("#Source_timestep_correction", src_ts),
-        ("#Reconstruction", "star"),
+        ("#Reconstruction", case.reconstruction),
         ("#Approximation_order", case.order),
         ("#Start_From_Time-Step", "1" if restart else "no"),
         ("#Calculation_of_mixing_zone_width", "on" if mixing_width else "off"),
@@ -244,7 +258,7 @@ def write_deck(case: Case, directory: str, prim: Sequence[np.ndarray], frequency
                "\n".join(f"#sub_{k + 1} {_f(sp.lj_eps)} {_f(sp.lj_sigma)}" for k, sp in enumerate(case.species))
                + f"\n#b_calculation {case.kataoka_b[0]} {_f(case.kataoka_b[1])}")
     _write(sdir, "chemicalKinetics.txt", _chemistry_block(case))
-    _write(sdir, "transportCoefficients.txt", _TRANSPORT)
+    _write(sdir, "transportCoefficients.txt", _transport_block(case) if case.diffusion else _TRANSPORT)
     _write(sdir, "turbulentParameters.txt", _TURB_PARAMS)
     _write(sdir, "turbPeak.txt", _TURB_PEAK)
     _write(sdir, "GoncharovModel.txt", _GONCHAROV)

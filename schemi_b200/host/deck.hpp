@@ -282,7 +282,7 @@ inline Deck readDeck(const std::string& dir, bool createResult) {
         c.gravity = onOff(on, "gravitation");
     }
     // main.txt
-    std::string limiter, diffusion, turbulence, flux, dims, sourceTime, reconstruction, order, width;
+    std::string limiter, diffusion, turbulence, flux, dims, sourceTime, reconstruction, order, width, sle;
     {
         Tokens t(d.path("set/main.txt"));
         t.skip();
@@ -297,10 +297,10 @@ inline Deck readDeck(const std::string& dir, bool createResult) {
         t.skip(); d.units = t.next("gas constant");
         t.skip(); d.eos = t.next("equation of state");
         t.skip(); limiter = t.next("limiter");
-        t.skip(); t.next("iterations");
+        t.skip(); c.sle_max_iter = (int)t.num("iterations");
         t.skip(); diffusion = t.next("diffusion flag");
         t.skip(); turbulence = t.next("turbulence flag");
-        t.skip(); t.next("matrix solver");
+        t.skip(); sle = t.next("matrix solver");
         t.skip(); t.next("source type");
         t.skip(); flux = t.next("flow solver");
         t.skip(); dims = t.next("dimensions");
@@ -312,10 +312,20 @@ inline Deck readDeck(const std::string& dir, bool createResult) {
         t.skip(); width = t.next("mixing zone width flag");
         t.skip(); t.next("nonlinearity iterations");
     }
-    if (onOff(diffusion, "diffusion")) throw Fail("#Diffusion_flag on: implicit diffusion is not part of this step");
+    c.diffusion = onOff(diffusion, "diffusion");
     if (onOff(turbulence, "turbulence"))
         throw Fail("#Turbulence_flag on: turbulence models are not part of this step");
     if (reconstruction != "linear" && reconstruction != "star") throw Fail("Unknown reconstruction flag.");
+    c.linear_reconstruction = reconstruction == "linear";
+    // abstractMatrixSolver.cpp:51-70
+    if (sle == "explicit") c.sle_solver = FV_SLE_EXPLICIT;
+    else if (sle == "GaussSeidel") c.sle_solver = FV_SLE_GAUSS_SEIDEL;
+    else if (sle == "Thomas" || sle == "noSolver" || sle == "conjugateGradient" || sle == "JacobiConjugateGradient" ||
+             sle == "Jacobi" || sle == "biConjugateGradient") {
+        if (c.diffusion) throw Fail("#Type_of_SLE_solver_flag " + sle + ": the diffusion stage implements explicit");
+    } else throw Fail("Unknown or inappropriate matrix solver flag.");
+    if (c.diffusion && c.sle_solver != FV_SLE_EXPLICIT)
+        throw Fail("#Type_of_SLE_solver_flag " + sle + ": the diffusion stage implements explicit");
     // "Gpu" + an order name: the factory string under which the step-solver adapter runs the
     // step inside the reference's main (schemi_adapter/gpuStepSolver.hpp)
     if (order.rfind("Gpu", 0) == 0) order = order.substr(3);
@@ -353,9 +363,20 @@ inline Deck readDeck(const std::string& dir, bool createResult) {
         if ((count('=') != 1 && count(',') != 1) || eq > com)
             throw Fail("Wrong format of time-step parameters settings");
         const std::string type = sourceTime.substr(0, eq == std::string::npos ? 0 : eq);
+        // the two coefficients: between '=' and ',', and after ',' (std::stod, Schemi.cpp:219-226)
+        const auto coeff = [&](const std::string& txt) {
+            try {
+                return std::stod(txt);
+            } catch (const std::exception&) {
+                throw Fail("Wrong format of time-step parameters settings");
+            }
+        };
+        c.dt_coeff_source = coeff(sourceTime.substr(eq + 1, com - eq - 1));
+        c.dt_coeff_diffusion = coeff(sourceTime.substr(com + 1));
         if (type != "Courant" && type != "Courant-Source" && type != "Courant-Source-Diffusion")
             throw Fail("Unknown source time-step flag.");
         c.courant_only = type == "Courant";
+        c.diffusion_timestep = type == "Courant-Source-Diffusion";
     }
     c.precision = FV_PREC_F64;
     if (c.n_species < 1 || c.n_species > FV_MAX_SPECIES) throw Fail("number of components must be 1..4");
@@ -366,6 +387,34 @@ inline Deck readDeck(const std::string& dir, bool createResult) {
         std::ofstream(d.path("result/Time.tsv")).close();
     }
     d.zones = readZones(d.path("set/zonesDescription.txt"));
+    if (c.diffusion) {
+        // phaseInitialization.cpp:193-243: model, mu, D, kappa, enthalpy-flow flag, molar-mass flag
+        if (!std::filesystem::exists(d.path("set/transportCoefficients.txt")))
+            throw Fail("./set/transportCoefficients.txt not found.");
+        Tokens t(d.path("set/transportCoefficients.txt"));
+        t.skip(); const std::string model = t.next("transport model");
+        t.skip(); c.mu_const = t.num("viscosity coefficient");
+        t.skip(); c.D_const = t.num("diffusion coefficient");
+        t.skip(); c.kappa_const = t.num("heat conduction coefficient");
+        t.skip(); const std::string enthalpy = t.next("enthalpy flow flag");
+        t.skip(); const std::string molMass = t.next("molar mass diffusion flag");
+        if (model == "hardSpheres" || model == "LennardJones")
+            throw Fail("#Transport_coefficient_model " + model + ": the diffusion stage implements constant");
+        if (model != "constant") throw Fail("Unknown flag for transport model.");
+        c.transport = FV_TRANSPORT_CONSTANT;
+        if (enthalpy == "no") c.enthalpy_flow = FV_ENTHALPY_NO;
+        else if (enthalpy == "explicit") c.enthalpy_flow = FV_ENTHALPY_EXPLICIT;
+        else if (enthalpy == "implicit")
+            throw Fail("#Flag_for_enthalpy_flow_solution implicit: the explicit diffusion stage takes no or explicit");
+        else throw Fail("Unknown flag for enthalpy flow calculation.");
+        if (molMass != "on" && molMass != "off" && molMass != "yes" && molMass != "no")
+            throw Fail("Unknown flag for molar mass diffusion correction.");
+        c.molmass_diffusion = onOff(molMass, "molar mass diffusion correction");
+        if (c.order != FV_ORDER_SECOND) throw Fail("#Diffusion_flag on: the diffusion stage runs with SecondOrder");
+        if (c.flux != FV_FLUX_HLLC) throw Fail("#Diffusion_flag on: the diffusion stage runs with HLLC");
+        if (c.eos != FV_EOS_IDEAL && c.eos != FV_EOS_VAN_DER_WAALS)
+            throw Fail("#Diffusion_flag on: the diffusion stage runs with ideal and vanDerWaals mixtures");
+    }
     const size_t nzv = d.zones.size();
     for (int k = 0; k < c.n_species; ++k) {
         Tokens t(d.path("set/sub_" + std::to_string(k + 1) + ".txt"));
@@ -441,6 +490,8 @@ inline Deck readDeck(const std::string& dir, bool createResult) {
             throw Fail("chemical mechanism " + name + " is not implemented (no, Cl2)");
         }
     }
+    if (c.diffusion && c.chemistry != FV_CHEM_NONE)
+        throw Fail("#Diffusion_flag on: the diffusion stage runs without a chemical mechanism");
     return d;
 }
 

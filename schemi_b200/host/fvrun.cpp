@@ -378,7 +378,15 @@ void printConfig(const fv_config& c, const Deck& d) {
     for (int p = 0; p < 6; ++p) std::cout << (p ? ", " : "") << c.bc_p[p];
     std::cout << "], \"chemistry\": " << c.chemistry << ", \"const_timestep\": " << c.const_timestep
               << ", \"t_end\": " << d.tEnd << ", \"frequency\": " << d.freq << ", \"start\": \"" << d.readFrom
-              << "\", \"order\": " << c.order << "}" << std::endl;
+              << "\", \"order\": " << c.order << ", \"diffusion\": " << c.diffusion
+              << ", \"sle_solver\": " << c.sle_solver << ", \"transport\": " << c.transport
+              << ", \"mu_const\": " << c.mu_const << ", \"D_const\": " << c.D_const
+              << ", \"kappa_const\": " << c.kappa_const << ", \"enthalpy_flow\": " << c.enthalpy_flow
+              << ", \"molmass_diffusion\": " << c.molmass_diffusion
+              << ", \"linear_reconstruction\": " << c.linear_reconstruction
+              << ", \"diffusion_timestep\": " << c.diffusion_timestep
+              << ", \"dt_coeff_source\": " << c.dt_coeff_source
+              << ", \"dt_coeff_diffusion\": " << c.dt_coeff_diffusion << "}" << std::endl;
 }
 
 // output::mixedZoneWidth1D (src/service/output.cpp:310-391): the distance between the first
@@ -555,7 +563,10 @@ int run(const Deck& d) {
         nsteps += rs.steps;
         time = rs.time;
         if (st != FV_OK) {
-            std::clog << fv_last_error(h) << std::endl << "Step number " << nsteps << '.' << std::endl;
+            // the failing step is the one after the last completed step; its time step is the one
+            // the run would have taken next
+            std::clog << fv_last_error(h) << std::endl << "Step number " << nsteps + 1 << '.' << std::endl;
+            std::clog << "Time-step " << rs.dt_next << '.' << std::endl;
             std::clog << "Emergency output." << std::endl;
             writeOutput(d, h, nouts, time, th, sonic);
             return EXIT_FAILURE;  // Schemi.cpp:774-799

@@ -102,6 +102,12 @@ void schemi::gpuStepSolver::calculateStep()
 	const fv_status st = fv_step(h, &dtUsed, &dtNext);
 	if (st != FV_OK)
 		throw exception(fv_last_error(h), static_cast<errors>(st));
+	// the source time step the step's diffusion stage set (Diffusion.cpp:688-706,1036-1049 set it
+	// on the mesh), which main's CFL block takes into the next step
+	double dtSource = 0;
+	if (fv_get_source_timestep(h, &dtSource) != FV_OK)
+		throw exception(fv_last_error(h), errors::systemError);
+	const_cast<mesh&>(gasPhase.pressure.meshRef()).timestepSourceRef() = dtSource;
 	writeBack();
 }
 

@@ -22,8 +22,9 @@
 //     src/solverStages/secondOrderStepSolver.cpp, over Advection.cpp:20-513), and writes the new
 //     state back into the phase: concentrations, densities, velocity, pressure, momentum, total
 //     and internal energy, temperature, and the Helmholtz energy and entropy from the phase's own
-//     thermodynamics (as Advection.cpp:455-486 does), so main's CFL block and outputs read what
-//     they read after the reference's step;
+//     thermodynamics (as Advection.cpp:455-486 does), and the source time step a diffusion stage
+//     set on the mesh (fv_get_source_timestep), so main's CFL block and outputs read what they
+//     read after the reference's step;
 //   * a failed step throws schemi::exception with the library's message and the reference's errors
 //     value (fv_status numbers them alike), which main turns into its emergency output.
 // The device state is kept between steps; main changes the phase only through this solver.

@@ -54,9 +54,12 @@ def _tree(d):
 
 
 def _velocity_scale(want):
-    """Largest sonic speed and density of the reference's outputs: velocities and momenta are
-    compared on these scales, since a flow at rest carries only rounding-level velocities."""
-    c_max, rho_max = 0.0, 0.0
+    """Largest sonic speed, density and total concentration of the reference's outputs:
+    velocities and momenta are compared on the first two, since a flow at rest carries only
+    rounding-level velocities, and species concentrations, densities and fractions on the
+    mixture's, since a species that is nearly absent carries values far below any rounding of
+    the mixture (1e-44 and less in the real-gas tubes)."""
+    c_max, rho_max, conc_max = 0.0, 0.0, 0.0
     for rel, data in want.items():
         if os.path.basename(rel).startswith("output_") and rel.endswith(".tsv"):
             lines = data.decode().strip("\n").split("\n")
@@ -64,23 +67,32 @@ def _velocity_scale(want):
             rows = np.array([[float(x) for x in ln.split("\t")] for ln in lines[1:]])
             c_max = max(c_max, float(np.abs(rows[:, head.index("sonic_speed")]).max()))
             rho_max = max(rho_max, float(np.abs(rows[:, head.index("density")]).max()))
-    return c_max, rho_max
+            conc_max = max(conc_max, float(np.abs(rows[:, head.index("concentration")]).max()))
+    return c_max, rho_max, conc_max
 
 
 def _numbers_close(a: bytes, b: bytes, tol: float, rel: str, scale):
     la, lb = a.decode().split("\n"), b.decode().split("\n")
     if len(la) != len(lb):
         return f"{rel}: {len(la)} lines, reference {len(lb)}"
-    c_max, rho_max = scale
+    c_max, rho_max, conc_max = scale
     floors = {}
     if os.path.basename(rel) == "velocity.dat":
         floors = {0: c_max, 1: c_max, 2: c_max}
+    elif os.path.basename(rel).startswith("sub_"):
+        floors = {0: conc_max}
     elif rel.endswith(".tsv") and la:
         for j, name in enumerate(lb[0].split("\t")):
             if name.startswith("velocity_"):
                 floors[j] = c_max
             elif name.startswith("momentum_"):
                 floors[j] = c_max * rho_max
+            elif name.startswith("concentration_"):
+                floors[j] = conc_max
+            elif name.startswith("density_"):
+                floors[j] = rho_max
+            elif name.startswith(("x_", "w_")):
+                floors[j] = 1.0
     for i, (x, y) in enumerate(zip(la, lb)):
         tx, ty = x.split("\t"), y.split("\t")
         if len(tx) != len(ty):

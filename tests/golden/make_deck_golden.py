@@ -144,11 +144,50 @@ def deck_cases():
         c.t_end = _t_after(c, p, 10, 0.4)
         out.append((f"tube60_{eos.lower()}", c, p, 4, True, [{}], 0.0,
                     {} if eos == "stiffened" else {"gpu_tolerance": 1e-11}))
+    # the diffusion stage (explicit solver, constant coefficients): a tube with the explicit
+    # enthalpy flow, the molar-mass correction and the diffusion time-step limit; a tube with the
+    # "linear" reconstruction and neither; a three-species van der Waals box; a Rayleigh-Taylor
+    # box under growing gravity (the interpolated face velocities); a 3D van der Waals box
+    c, p = cases.shock_tube_1d(n=60)
+    c.diffusion, c.mu, c.D, c.kappa = True, 1e-4, 1e-3, 1e-4
+    c.enthalpy_flow, c.molmass_diffusion, c.diffusion_timestep = "explicit", True, True
+    c.t_end = _t_after(c, p, 20, 0.4)
+    out.append(("tube60_diffusion", c, p, 6, True, [{}], 0.0))
+    c, p = cases.shock_tube_1d(n=60)
+    c.diffusion, c.mu, c.D, c.kappa = True, 2e-4, 5e-4, 2e-4
+    c.enthalpy_flow, c.molmass_diffusion, c.reconstruction = "no", False, "linear"
+    c.t_end = _t_after(c, p, 20, 0.4)
+    out.append(("tube60_diffusion_linear", c, p, 6, True, [{}], 0.0))
+    c3, p3 = cases.reacting_shear_3d(n=6, periodic=False)
+    c = Case(dims=2, n=(6, 6, 1), L=(1.0, 1.0, 1.0), species=c3.species, t_end=1.0, R_units="SI",
+             eos="vanDerWaals", limiter="vanLeer", name="vdw2d")
+    for k in ("tail", "point", "right", "left"):
+        c.bc[k] = PatchBC.uniform("slip", 3)
+    p = [a.reshape(6, 6, 6)[0].ravel() for a in p3]
+    c.diffusion, c.mu, c.D, c.kappa = True, 1e-5, 1e-5, 1e-3
+    c.enthalpy_flow, c.molmass_diffusion, c.diffusion_timestep = "explicit", False, True
+    c.t_end = _t_after(c, p, 8, 0.5)
+    out.append(("vdw3_6x6_diffusion", c, p, 3, True, [{}], 0.0))
+    c, p = cases.rayleigh_taylor_2d(nx=8, ny=16, modes=2)
+    c.g_delta = (0.0, -0.05, 0.0)
+    c.diffusion, c.mu, c.D, c.kappa = True, 1e-3, 1e-3, 1e-3
+    c.enthalpy_flow, c.molmass_diffusion = "explicit", True
+    c.t_end = _t_after(c, p, 12, 0.5)
+    out.append(("rt8x16_gravity_diffusion", c, p, 5, True, [{}], 0.0))
+    c, p = cases.reacting_shear_3d(n=6, periodic=False, precision="f64")
+    c.chemistry = "no"
+    for k in list(c.bc):
+        c.bc[k] = PatchBC.uniform("slip", 3)
+    c.diffusion, c.mu, c.D, c.kappa = True, 1e-5, 1e-5, 1e-3
+    c.enthalpy_flow, c.molmass_diffusion, c.diffusion_timestep = "explicit", False, True
+    c.t_end = _t_after(c, p, 6, 0.5)
+    out.append(("vdw3_6x6x6_diffusion", c, p, 3, True, [{}], 0.0))
     return out
 
 
 # Task decks shipped with the reference (its tests/TestsTasks directory) whose every stage is in
-# this step: 1D, HLLC, the vanAlbada limiter, ideal gas, diffusion and turbulence off.  Their set/
+# this step: 1D, HLLC, the vanAlbada limiter, ideal gas, turbulence off; diffusion off, or (the
+# Diffusion deck) explicit with constant coefficients.  Their set/
 # directories are stored unchanged.  Noh_CGS is refused by the reference itself (a parenthesised
 # fixed velocity that its stream reader cannot parse): exit code 1, "Unknown type of boundary
 # condition", and only the empty result/Time.tsv left behind.
@@ -160,6 +199,7 @@ SHIPPED = [
     ("noh_2_1000", "Noh_2/Noh_2_1000"),
     ("rarefactions_100_cgs", "Rarefactions_CGS/Rarefactions_100_CGS"),
     ("noh_cgs_1000", "Noh_CGS/Noh_CGS_1000"),
+    ("diffusion_1000", "Diffusion/Diffusion_1000"),
 ]
 SHIPPED_ROOT = "/root/reference/tests/TestsTasks"
 

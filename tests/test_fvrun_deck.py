@@ -96,7 +96,7 @@ def _edit(path, key, value):
 
 
 @pytest.mark.parametrize("file,key,value,message", [
-    ("main.txt", "#Diffusion_flag", "on", "Diffusion"),
+    ("main.txt", "#Diffusion_flag", "on", "the diffusion stage implements explicit"),
     ("main.txt", "#Turbulence_flag", "yes", "Turbulence"),
     ("main.txt", "#Approximation_order", "FourthOrder", "Unknown gas dynamics approximation order."),
     ("main.txt", "#TVD_limiter_type", "vanLeer3", "limiter"),
@@ -114,6 +114,52 @@ def _edit(path, key, value):
 ])
 def test_unsupported_deck_refused(tmp_path, file, key, value, message):
     c, p = cases.kelvin_helmholtz_2d(n=8, periodic=False)
+    write_deck(c, str(tmp_path), p, restart=True)
+    _edit(os.path.join(tmp_path, "set", file), key, value)
+    res = _print_config(str(tmp_path))
+    assert res.returncode != 0
+    assert message in res.stderr
+
+
+def _diffusion_case():
+    c, p = cases.shock_tube_1d(n=40)
+    c.diffusion, c.mu, c.D, c.kappa = True, 1e-4, 1e-3, 1e-4
+    c.enthalpy_flow, c.molmass_diffusion, c.diffusion_timestep = "explicit", True, True
+    return c, p
+
+
+def test_print_config_diffusion(tmp_path):
+    """A diffusion deck: the stage's settings from main.txt and set/transportCoefficients.txt."""
+    c, p = _diffusion_case()
+    c.dt_coeffs = (0.3, 0.45)
+    c.reconstruction = "linear"
+    write_deck(c, str(tmp_path), p, restart=True)
+    res = _print_config(str(tmp_path))
+    assert res.returncode == 0, res.stderr
+    got = json.loads(res.stdout.strip().splitlines()[-1])
+    want = c.fv_config()
+    for key in ("diffusion", "sle_solver", "transport", "enthalpy_flow", "molmass_diffusion",
+                "linear_reconstruction", "diffusion_timestep"):
+        assert got[key] == getattr(want, key), key
+    for key in ("mu_const", "D_const", "kappa_const", "dt_coeff_source", "dt_coeff_diffusion"):
+        assert got[key] == getattr(want, key), key
+
+
+@pytest.mark.parametrize("file,key,value,message", [
+    ("main.txt", "#Type_of_SLE_solver_flag", "Jacobi", "the diffusion stage implements explicit"),
+    ("main.txt", "#Type_of_SLE_solver_flag", "LU", "Unknown or inappropriate matrix solver flag."),
+    ("main.txt", "#Type_of_flow_solver", "HLL", "the diffusion stage runs with HLLC"),
+    ("main.txt", "#Approximation_order", "SecondOrderRK", "the diffusion stage runs with SecondOrder"),
+    ("transportCoefficients.txt", "#Transport_coefficient_model", "hardSpheres", "implements constant"),
+    ("transportCoefficients.txt", "#Transport_coefficient_model", "Sutherland", "Unknown flag for transport model."),
+    ("transportCoefficients.txt", "#Flag_for_enthalpy_flow_solution", "implicit", "takes no or explicit"),
+    ("transportCoefficients.txt", "#Flag_for_enthalpy_flow_solution", "maybe",
+     "Unknown flag for enthalpy flow calculation."),
+    ("transportCoefficients.txt", "#Flag_for_molar_mass_diffusion_correction", "maybe",
+     "Unknown flag for molar mass diffusion correction."),
+])
+def test_unsupported_diffusion_deck_refused(tmp_path, file, key, value, message):
+    c, p = _diffusion_case()
     write_deck(c, str(tmp_path), p, restart=True)
     _edit(os.path.join(tmp_path, "set", file), key, value)
     res = _print_config(str(tmp_path))

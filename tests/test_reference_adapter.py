@@ -57,7 +57,8 @@ def test_unknown_gpu_order_is_refused_by_the_factory(tmp_path):
 
 
 def test_deck_outside_the_step_is_refused_before_the_first_step(tmp_path):
-    """Implicit diffusion on: the adapter refuses at the factory, with the deck reader's message."""
+    """Diffusion with the Gauss-Seidel (implicit) solver: the adapter refuses at the factory, with
+    the deck reader's message."""
     from deck_replay import ORDER, load, unpack_inputs
 
     z = load("tube40_fresh")
@@ -70,5 +71,5 @@ def test_deck_outside_the_step_is_refused_before_the_first_step(tmp_path):
     res = subprocess.run([_binary()], cwd=tmp_path, stdin=subprocess.DEVNULL, capture_output=True,
                          text=True, timeout=120)
     assert res.returncode != 0
-    assert "implicit diffusion is not part of this step" in res.stderr + res.stdout
+    assert "the diffusion stage implements explicit" in res.stderr + res.stdout
     assert not (tmp_path / "result" / "output_000001.tsv").exists()
