@@ -29,6 +29,9 @@ accuracy  every section states its relative L1 / L-inf error against the FP64 or
           the oracle runs in spawned worker processes after the timed sections.
 shock_tube_1d  config 1: the 1000-cell two-component tube to t = 0.2 through fv_run, us per step
           and the final fields against the reference's own output (tests/golden).
+diffusion_deck  the reference's Diffusion_1000 deck (the diffusion stage after every advection,
+          34,561 steps to t = 0.3) through fv_run: us per step, the final fields against the
+          reference's output of that deck, and the reference binary's us per step on it.
 
 batched   512 Richtmyer-Meshkov cases of seeded sizes 128^2..512^2 (FP32 flux) advanced by the
           persistent ensemble kernel, against the same cases one after the other.
@@ -647,6 +650,71 @@ def tube_c1(torch) -> dict:
             "tolerance_rel_linf": 1e-12}
 
 
+def diffusion_deck(torch, ref_steps: int = 300, ref_steps0: int = 20) -> dict:
+    """The reference's Diffusion_1000 deck (1000 cells, the diffusion stage with the explicit
+    solver after every advection, 34,561 steps to t = 0.3) through fv_run: microseconds per step
+    on the device, and the final fields against the reference's own output of that deck
+    (tests/golden/deck_diffusion_1000.npz).  cpu_baseline: the reference binary (patched build)
+    on the same deck, per step by differencing runs of ref_steps and ref_steps0 steps."""
+    import numpy as np
+
+    from schemi_b200 import cases, fv
+
+    case, prim = cases.diffusion_tube_1d()
+    g = fv.FVCase(case)
+    g.upload(prim)
+    g.run(case.t_end, 2000)  # warm-up: graph capture and kernel configuration
+    g.upload(prim)
+    t0 = time.perf_counter()
+    st = g.run(case.t_end)
+    wall = time.perf_counter() - t0
+    out = g.download()
+    g.close()
+    z = np.load(os.path.join(ROOT, "tests", "golden", "deck_diffusion_1000.npz"))
+    txt = z["out:result|output_000001.tsv"].tobytes().decode().strip().split("\n")
+    head = txt[0].split("\t")
+    rows = np.array([[float(x) for x in ln.split("\t")] for ln in txt[1:]])
+    errs = {}
+    for f, col in (("c1", "concentration_1"), ("c2", "concentration_2"), ("vx", "velocity_x"), ("p", "pressure"),
+                   ("T", "temperature")):
+        b = rows[:, head.index(col)]
+        errs[f] = float(np.abs(out[f] - b).max() / max(np.abs(b).max(), 1e-300))
+    res = {"workload": "diffusion_tube_1d (the reference's Diffusion_1000 deck) to t=0.3, FP64, HLLC + vanAlbada, "
+                       "explicit diffusion with the molar-mass correction and the explicit enthalpy flow",
+           "steps": int(st.steps), "time": st.time, "device_us_per_step": 1e3 * st.device_ms / max(st.steps, 1),
+           "wall_us_per_step": 1e6 * wall / max(st.steps, 1), "kernels_per_step": 9,
+           "rel_linf_vs_reference_output": max(errs.values()), "fields": errs, "tolerance_rel_linf": 1e-12}
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+
+        oc = oracle.OracleCase(case)
+        oc.upload(prim)
+        t_at = {}
+        for s in range(1, ref_steps + 1):
+            oc.step()
+            t_at[s] = oc.time()[0]
+        import copy
+
+        base = tempfile.mkdtemp(prefix="schemi_refdiff_")
+        walls = {}
+        for nst in (ref_steps0, ref_steps):
+            c = copy.deepcopy(case)
+            c.t_end = t_at[nst]
+            walls[nst] = _reference_run(oracle.REF_BIN_PATCHED, c, prim, nst, os.path.join(base, str(nst)))
+        import shutil
+
+        shutil.rmtree(base, ignore_errors=True)
+        us = 1e6 * (walls[ref_steps] - walls[ref_steps0]) / (ref_steps - ref_steps0)
+        res["cpu_baseline"] = {"value": us, "unit": "us/step", "cores": 1, "kind": "reference",
+                               "sample": f"oracle/_ref/schemi_patched on the same deck, steps {ref_steps0}..{ref_steps} "
+                                         "by differencing two runs"}
+        res["speedup_device_vs_reference"] = us / res["device_us_per_step"]
+    except Exception as e:  # noqa: BLE001 -- the reference build may be absent
+        res["cpu_baseline"] = {"unavailable": str(e)}
+    return res
+
+
 def reacting_accuracy(n: int, want) -> dict:
     """The 3D reacting shear layer at n^3 (FP32 flux + FP64 chemistry), ACC_STEPS steps, against
     the FP64 oracle (flux, van der Waals EOS and the A+B->2C chemistry in FP64)."""
@@ -807,6 +875,7 @@ def run_ours(args):
     }
     if rank == 0 and args.tube:
         line["shock_tube_1d"] = tube_c1(torch)
+        line["diffusion_deck"] = diffusion_deck(torch)
     sample = batch_accuracy_sample(args.batch_cases) if args.batch_cases > 0 and not args.no_accuracy else []
     kept = {}
     if args.batch_cases > 0:

@@ -55,6 +55,7 @@ def load():
         lib.fvo_download.argtypes = [P, ctypes.POINTER(DP)]
         lib.fvo_get_time.argtypes = [P, DP, DP]
         lib.fvo_set_time.argtypes = [P, D, D]
+        lib.fvo_get_source_timestep.argtypes = [P, DP]
         lib.fvo_get_conserved.argtypes = [P, ctypes.POINTER(DP)]
         lib.fvo_set_conserved.argtypes = [P, ctypes.POINTER(DP)]
         lib.fvo_n_cells.restype = ctypes.c_longlong
@@ -112,6 +113,11 @@ class OracleCase:
 
     def set_time(self, t: float, dt: float) -> None:
         load().fvo_set_time(self._h, t, dt)
+
+    def source_timestep(self) -> float:
+        d = ctypes.c_double()
+        load().fvo_get_source_timestep(self._h, ctypes.byref(d))
+        return d.value
 
     def download(self) -> Dict[str, np.ndarray]:
         out = [np.empty(self.n_cells) for _ in range(FV_F_COUNT)]

@@ -43,6 +43,26 @@ def shock_tube_1d(n: int = 1000, limiter: str = "minmod", flux: str = "HLLC", pr
     return case, [cA, cB, z, z.copy(), z.copy(), p]
 
 
+def diffusion_tube_1d(n: int = 1000, t_end: float = 0.3) -> Tuple[Case, list]:
+    """Interdiffusion of two ideal gases of equal molar mass at rest: c_1 = 0.05 mol/m^3 for
+    x < 0.5, c_2 = 0.05 beyond, p = 100 Pa, slip ends, SI units (M = 28.8, Cv = 20.78615655),
+    vanAlbada, HLLC, Courant 0.47; the diffusion stage with the explicit solver, mu = 2e-7,
+    D = 2e-2, kappa = 2e-4, the explicit enthalpy flow, the molar-mass correction and the
+    Courant-Source-Diffusion=0.25,0.5 limit -- the parameters of the reference's
+    tests/TestsTasks/Diffusion/Diffusion_1000 deck."""
+    sp = [Species(M=28.8, Cv=20.78615655, Tc=1.0, Pc=1.0) for _ in range(2)]
+    case = Case(dims=1, n=(n, 1, 1), L=(1.0, 1.0, 1.0), species=sp, t_end=t_end, R_units="SI",
+                limiter="vanAlbada", courant=0.47, min_timestep=1e-15, name="diffusion_tube_1d")
+    case.bc["tail"] = PatchBC.uniform("slip", 2)
+    case.bc["point"] = PatchBC.uniform("slip", 2)
+    case.diffusion, case.mu, case.D, case.kappa = True, 2e-7, 2e-2, 2e-4
+    case.enthalpy_flow, case.molmass_diffusion, case.diffusion_timestep = "explicit", True, True
+    x = _centres(n, 1.0)
+    left = x < 0.5
+    z = np.zeros(n)
+    return case, [np.where(left, 0.05, 0.0), np.where(left, 0.0, 0.05), z, z.copy(), z.copy(), np.full(n, 100.0)]
+
+
 def real_gas_tube(eos: str, n: int = 200, limiter: str = "minmod") -> Tuple[Case, list]:
     """Two-component shock tube for the equations of state beyond ideal and van der Waals
     (transmissive ends, HLLC).

@@ -208,6 +208,21 @@ __device__ __forceinline__ int cellAxisCoords(const StepParams& P, long long i, 
     return 0;
 }
 
+// minimum over the CTA (all threads pass a value; +inf pads the missing warps); valid in thread 0
+__device__ __forceinline__ double blockMinReduce(double v, double* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = smin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        v = lane < nw ? red[lane] : 1.0 / 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = smin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    }
+    return v;
+}
+
 // ----------------------------------------------------------------------------- k_diff_prim
 template <int NS, int EOS, int D>
 __global__ void k_diff_prim(const StepParams P, const DiffParams X, const double* __restrict__ U,
@@ -680,9 +695,9 @@ __global__ void k_diff_cells(const StepParams P, const GenericLayout L, const Di
     }
     const double bm = blockMaxReduce<double>(localMax, red);
     __syncthreads();
-    const double bE = -blockMaxReduce<double>(-minE, red);
+    const double bE = blockMinReduce(minE, red);
     __syncthreads();
-    const double bD = -blockMaxReduce<double>(-minD, red);
+    const double bD = blockMinReduce(minD, red);
     if (threadIdx.x == 0) {
         blockMax[blockIdx.x] = bm;
         X.partMin[blockIdx.x] = bE;
@@ -701,9 +716,9 @@ __global__ void k_diff_source(const DiffParams X, DevClock* __restrict__ ck, int
         mE = smin(mE, X.partMin[b]);
         mD = smin(mD, X.partMin[nblocks + b]);
     }
-    mE = -blockMaxReduce<double>(-mE, red);
+    mE = blockMinReduce(mE, red);
     __syncthreads();
-    mD = -blockMaxReduce<double>(-mD, red);
+    mD = blockMinReduce(mD, red);
     if (threadIdx.x != 0) return;
     double src = sourceTimestep(ck);
     if (X.enthalpy) src = X.coeffSource * mE;

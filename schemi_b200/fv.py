@@ -87,6 +87,7 @@ def load():
     lib.fv_download.argtypes = [P, ctypes.POINTER(DP)]
     lib.fv_get_time.argtypes = [P, DP, DP]
     lib.fv_set_time.argtypes = [P, D, D]
+    lib.fv_get_source_timestep.argtypes = [P, DP]
     lib.fv_state_device.argtypes = [P, ctypes.POINTER(DP), ctypes.POINTER(I), ctypes.POINTER(LL)]
     lib.fv_sync.argtypes = [P]
     lib.fv_step_path.argtypes = [P]
@@ -188,6 +189,12 @@ class FVCase:
 
     def set_time(self, t: float, dt: float) -> None:
         self._check(self.lib.fv_set_time(self._h, t, dt))
+
+    def source_timestep(self) -> float:
+        """The limit the last step's diffusion stage set for the next step (fv_get_source_timestep)."""
+        d = ctypes.c_double()
+        self._check(self.lib.fv_get_source_timestep(self._h, ctypes.byref(d)))
+        return d.value
 
     def download_fields(self) -> Dict[str, int]:
         """Names of the fields fv_download writes for this case, with their fv_download index."""

@@ -1,0 +1,143 @@
+"""The diffusion stage on the GPU (Diffusion.cpp through fv_step / fv_run) against the FP64 oracle.
+
+Both follow the reference's operation order in FP64 without contraction, so the device state,
+its temperature (the stage's own, not TFromUv of the energy), the CFL step and the source time
+step the stage sets must agree bit for bit.  The oracle itself is byte-identical to the
+reference on the diffusion deck fixtures (tests/test_reference_adapter.py, test_fvrun_deck.py);
+tests/test_gpu_fvrun.py and test_gpu_adapter.py replay those decks on the GPU.
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ["c1", "c2", "c3", "vx", "vy", "vz", "p", "rho", "rho1", "rho2", "mx", "my", "E", "Uv", "T", "sonic"]
+
+
+@pytest.fixture(scope="module")
+def fv():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from schemi_b200 import fv as fvmod
+
+    fvmod.load()
+    return fvmod
+
+
+def _tube(**kw):
+    from schemi_b200 import cases
+
+    c, p = cases.shock_tube_1d(n=60)
+    c.diffusion, c.mu, c.D, c.kappa = True, 1e-4, 1e-3, 1e-4
+    c.enthalpy_flow, c.molmass_diffusion, c.diffusion_timestep = "explicit", True, True
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c, p
+
+
+def _vdw_box(dims):
+    from schemi_b200 import cases
+    from schemi_b200.case import Case, PatchBC
+
+    c3, p3 = cases.reacting_shear_3d(n=6, periodic=False, precision="f64")
+    if dims == 3:
+        c, p = c3, p3
+        c.chemistry = "no"
+        for k in list(c.bc):
+            c.bc[k] = PatchBC.uniform("slip", 3)
+    else:
+        c = Case(dims=2, n=(6, 6, 1), L=(1.0, 1.0, 1.0), species=c3.species, t_end=1.0, R_units="SI",
+                 eos="vanDerWaals", limiter="vanLeer", name="vdw2d")
+        for k in ("tail", "point", "right", "left"):
+            c.bc[k] = PatchBC.uniform("slip", 3)
+        p = [a.reshape(6, 6, 6)[0].ravel() for a in p3]
+    c.diffusion, c.mu, c.D, c.kappa = True, 1e-5, 1e-5, 1e-3
+    c.enthalpy_flow, c.molmass_diffusion, c.diffusion_timestep = "explicit", False, True
+    return c, p
+
+
+def _rt_gravity():
+    from schemi_b200 import cases
+
+    c, p = cases.rayleigh_taylor_2d(nx=8, ny=16, modes=2)
+    c.g_delta = (0.0, -0.05, 0.0)
+    c.diffusion, c.mu, c.D, c.kappa = True, 1e-3, 1e-3, 1e-3
+    c.enthalpy_flow, c.molmass_diffusion = "explicit", True
+    return c, p
+
+
+def _kh_periodic():
+    """A periodic axis (no reference counterpart; the oracle's periodic faces) with diffusion."""
+    from schemi_b200 import cases
+
+    c, p = cases.kelvin_helmholtz_2d(n=24)
+    c.diffusion, c.mu, c.D, c.kappa = True, 1e-4, 1e-4, 1e-4
+    c.enthalpy_flow, c.molmass_diffusion, c.diffusion_timestep = "explicit", True, True
+    c.reconstruction = "linear"
+    return c, p
+
+
+CASES = [
+    ("tube_enthalpy_molmass", lambda: _tube(), 25),
+    ("tube_linear_plain", lambda: _tube(enthalpy_flow="no", molmass_diffusion=False, reconstruction="linear",
+                                        diffusion_timestep=False), 25),
+    ("vdw3_2d", lambda: _vdw_box(2), 10),
+    ("vdw3_3d", lambda: _vdw_box(3), 8),
+    ("rt_gravity", _rt_gravity, 14),
+    ("kh_periodic", _kh_periodic, 12),
+]
+
+
+@pytest.mark.parametrize("name,make,steps", CASES, ids=[c[0] for c in CASES])
+def test_gpu_diffusion_step_matches_oracle_bitwise(fv, oracle_mod, name, make, steps):
+    case, prim = make()
+    g = fv.FVCase(case)
+    g.upload(prim)
+    assert g.path == fv.PATH_GENERIC
+    oc = oracle_mod.OracleCase(case)
+    oc.upload(prim)
+    for s in range(steps):
+        g.step()
+        oc.step()
+        assert g.time() == oc.time(), f"{name} step {s + 1}: clock {g.time()} vs {oc.time()}"
+        assert g.source_timestep() == oc.source_timestep(), f"{name} step {s + 1}: source time step"
+    a, b = g.download(), oc.download()
+    for f in FIELDS:
+        if f in a and f in b:
+            bad = np.flatnonzero(a[f] != b[f])
+            assert bad.size == 0, f"{name} {f}: {bad.size} cells differ, first {bad[0]}: {a[f][bad[0]]!r} vs {b[f][bad[0]]!r}"
+
+
+def test_gpu_diffusion_run_matches_oracle(fv, oracle_mod):
+    """fv_run (CUDA graphs of step chunks) with the stage: the same state and step count."""
+    case, prim = _tube()
+    g = fv.FVCase(case)
+    g.upload(prim)
+    st = g.run(0.02)
+    oc = oracle_mod.OracleCase(case)
+    oc.upload(prim)
+    t, n = oc.run(0.02, 10**6)
+    assert st.steps == n and st.time == t
+    a, b = g.download(), oc.download()
+    for f in FIELDS:
+        if f in a and f in b:
+            assert np.array_equal(a[f], b[f]), f
+
+
+def test_gpu_diffusion_kernel_count(fv):
+    case, prim = _tube()
+    g = fv.FVCase(case)
+    assert g.kernels_per_step == 4 + 5  # the generic step's 4, the stage's 4, the finalize
+
+
+def test_gpu_diffusion_refusals(fv):
+    """Configurations outside the stage are refused at fv_create with initialisationError."""
+    for kw in ({"precision": "f32flux"}, {"order": "SecondOrderRK"}, {"flux": "HLL"}, {"sle_solver": "GaussSeidel"},
+               {"enthalpy_flow": "implicit"}):
+        case, _ = _tube(**kw)
+        with pytest.raises(fv.FVError) as e:
+            fv.FVCase(case)
+        assert e.value.status == 11, kw
