@@ -1766,6 +1766,98 @@ void dMaxwellStefan(int NS, const double* Nc, const double* M, double D, const d
     }
 }
 
+// ---- the implicit solver of the stage: SLEMatrix::generateDTimeLaplacian (SLEMatrix.cpp:410-546
+// for a scalar, :706-907 for a vector, whose three components share the coefficients) and
+// GaussSeidelSolver::algorithm (GaussSeidelSolver.cpp:12-82)
+struct SLE1 {
+    std::vector<double> diag, free;
+    std::vector<std::vector<std::pair<double, long long>>> lower, upper;  // (coefficient, cell), face order
+};
+// rNew / dt + the faces' D / |d| (n S / V & d / |d|) on the diagonal; rOld / dt and each patch's
+// coefficient times the ghost value in the free term; the neighbours' negated coefficients
+template <class Ghost>
+void dLaplacian(const fvo_case& cs, Ghost ghost, const std::vector<double>& rOld, const std::vector<double>& rNew,
+                const std::vector<double>& Dface, double dt, SLE1& M) {
+    const long long nc = cs.nCells;
+    const double rt = 1 / dt;
+    M.diag.assign(nc, 0.0);
+    M.free.assign(nc, 0.0);
+    M.lower.assign(nc, {});
+    M.upper.assign(nc, {});
+    for (long long i = 0; i < nc; ++i) {
+        M.diag[i] = rNew[i] * rt;
+        M.free[i] = rOld[i] * rt;
+    }
+    for (long long i = 0; i < nc; ++i) {
+        const Cell& c = cs.cells[i];
+        for (int j = 0; j < c.nFaces; ++j) {
+            const int fi = c.faces[j];
+            const Face& F = cs.faces[fi];
+            if (F.nei >= 0) {
+                long long o;
+                V3 outerN, dR;
+                if (F.own == i) {
+                    o = F.nei;
+                    outerN = vdiv(vmul(F.N, F.S), c.V);
+                    dR = vsub(vadd(cs.cells[o].rC, F.neiShift), c.rC);
+                } else {
+                    o = F.own;
+                    outerN = vmul(vdiv(vmul(F.N, F.S), c.V), -1);
+                    dR = vsub(vsub(cs.cells[o].rC, F.neiShift), c.rC);  // the owner one period back
+                }
+                const double m = mag3(dR);
+                const V3 dn = vdiv(dR, m);
+                M.diag[i] += Dface[fi] / m * vdot(outerN, dn);
+                const double off = -Dface[fi] / m * vdot(outerN, dn);
+                if (o < i) M.lower[i].emplace_back(off, o);
+                else M.upper[i].emplace_back(off, o);
+            } else {
+                const double b = ghost(i, fi);
+                const V3 dR = vmul(vsub(F.rC, c.rC), 2);
+                const double m = mag3(dR);
+                const V3 dn = vdiv(dR, m);
+                const V3 outerN = vdiv(vmul(F.N, F.S), c.V);
+                M.diag[i] += Dface[fi] / m * vdot(outerN, dn);
+                M.free[i] += Dface[fi] / m * vdot(outerN, dn) * b;
+            }
+        }
+    }
+}
+// a forward sweep, then a backward one, until 100 max |(new - old) / (|new| + eps)| is below
+// convergenceToleranceGlobal (1e-12) or maxIt sweeps ran; normalize (|x| < DBL_EPSILON -> 0)
+std::vector<double> dGaussSeidel(const SLE1& M, const std::vector<double>& start, long long maxIt) {
+    const long long n = (long long)start.size();
+    std::vector<double> oldI(start), newI(start);
+    long long it = 0;
+    while (true) {
+        ++it;
+        for (long long i = 0; i < n; ++i) {
+            const double aii = 1. / M.diag[i];
+            newI[i] = M.free[i] * aii;
+            for (const auto& e : M.lower[i]) newI[i] -= e.first * newI[e.second] * aii;
+            for (const auto& e : M.upper[i]) newI[i] -= e.first * oldI[e.second] * aii;
+        }
+        for (long long i = n - 1; i >= 0; --i) {
+            const double aii = 1. / M.diag[i];
+            newI[i] = M.free[i] * aii;
+            for (size_t j = M.lower[i].size(); j-- > 0;) newI[i] -= M.lower[i][j].first * oldI[M.lower[i][j].second] * aii;
+            for (size_t j = M.upper[i].size(); j-- > 0;) newI[i] -= M.upper[i][j].first * newI[M.upper[i][j].second] * aii;
+        }
+        double mx = 0;
+        for (long long i = 0; i < n; ++i) {
+            const double r = std::fabs((newI[i] - oldI[i]) / (std::fabs(newI[i]) + kStab));
+            if (i == 0 || r > mx) mx = r;
+        }
+        const double diff = 100. * mx;
+        if (diff < 1e-12 || it >= maxIt) {
+            for (auto& x : newI)
+                if (std::fabs(x) < std::numeric_limits<double>::epsilon()) x = 0;
+            return newI;
+        }
+        oldI = newI;
+    }
+}
+
 int diffusionStage(fvo_case& cs, double dt) {
     const Mix& mx = cs.mix;
     const int NS = cs.N;
@@ -1904,26 +1996,36 @@ int diffusionStage(fvo_case& cs, double dt) {
     for (int k = 0; k < NS; ++k)
         for (size_t f = 0; f < nf; ++f) rhoD[k][f] = surfaceRho[f] * Dc;
 
-    // mass-fraction matrices (Diffusion.cpp:321-339; SLEMatrix.cpp:2054-2078)
+    // mass-fraction matrices (Diffusion.cpp:321-339; SLEMatrix.cpp:2054-2078 explicit,
+    // :410-546 implicit)
+    const bool gs = cf.sle_solver == FV_SLE_GAUSS_SEIDEL;
     std::vector<std::vector<V3>> gradW(NS);
     std::vector<std::vector<double>> diagW(NS, std::vector<double>(nc)), oldW(NS, std::vector<double>(nc)),
         freeW(NS, std::vector<double>(nc, 0.0));
+    std::vector<SLE1> MW(gs ? NS : 0);
     for (int k = 0; k < NS; ++k) {
-        dSurfGrad(cs, w[k], [&](size_t f) {  // calculatedMassFraction (cell), component k + 1
+        auto ghostW = [&, k](size_t f) {  // calculatedMassFraction (cell), component k + 1
             double cB[FV_MAX_SPECIES + 1];
             dBoundaryConc(cs, cs.faces[f].own, cs.faces[f].patch, true, cB, bad);
             const double dens = cB[k + 1] * mx.M[k];
             double sum = 0;
             for (int q = 1; q <= NS; ++q) sum += cB[q] * mx.M[q - 1];
             return dens / sum;
-        }, gradW[k]);
+        };
+        dSurfGrad(cs, w[k], ghostW, gradW[k]);
+        for (long long i = 0; i < nc; ++i) oldW[k][i] = w[k][i] * cs.rho[0][i];
+        if (gs) {
+            dLaplacian(cs, [&](long long, int fi) { return ghostW(fi); }, oldW[k], cs.rho[0], rhoD[k], dt, MW[k]);
+            diagW[k] = MW[k].diag;
+            freeW[k] = MW[k].free;
+            continue;
+        }
         std::vector<V3> flow(nf);
         for (size_t f = 0; f < nf; ++f) flow[f] = vmul(vmul(gradW[k][f], rhoD[k][f]), -1.);
         std::vector<double> div;
         dDivV(cs, flow, div);
         for (long long i = 0; i < nc; ++i) {
             diagW[k][i] = cs.rho[0][i];
-            oldW[k][i] = w[k][i] * cs.rho[0][i];
             freeW[k][i] -= div[i];
         }
     }
@@ -1988,12 +2090,18 @@ int diffusionStage(fvo_case& cs, double dt) {
     }
 
     // new mass fractions and concentrations (Diffusion.cpp:430-476)
+    std::vector<std::vector<double>> wSol(gs ? NS : 0);
+    for (int k = 0; k < (gs ? NS : 0); ++k) {
+        MW[k].diag = diagW[k];
+        MW[k].free = freeW[k];
+        wSol[k] = dGaussSeidel(MW[k], w[k], cf.sle_max_iter);
+    }
     std::vector<std::vector<double>> wNew(NS, std::vector<double>(nc));
     std::vector<std::vector<double>> cN(NS + 1, std::vector<double>(nc));
     for (long long i = 0; i < nc; ++i) {
         double sum = 0.;
         for (int k = 0; k < NS; ++k) {
-            double x = (oldW[k][i] + freeW[k][i] * dt) / diagW[k][i];
+            double x = gs ? wSol[k][i] : (oldW[k][i] + freeW[k][i] * dt) / diagW[k][i];
             if (x < 0.) x = 0.0;
             wNew[k][i] = x;
             sum += x;
@@ -2014,27 +2122,97 @@ int diffusionStage(fvo_case& cs, double dt) {
         oldEnergy[i] = CCVOld[i] * T[i] + nonIdOld[i] - nonIdNew;
     }
 
-    // velocity and temperature matrices (Diffusion.cpp:480-500; SLEMatrix.cpp:2054-2110)
+    // the implicit solver with an enthalpy flow: the flow again with the new concentrations, and
+    // its 0.5 average with the first (Diffusion.cpp:618-686)
+    if (gs && cf.enthalpy_flow != FV_ENTHALPY_NO) {
+        std::vector<std::vector<double>> scN(NS + 1, std::vector<double>(nf, 0.0));
+        for (int k = 1; k <= NS; ++k) {
+            std::vector<double> sk;
+            dInterp(cs, cN[k], [&](size_t f) {
+                return bcSurfaceS(cs, cN[k][cs.faces[f].own], 0, k - 1, cs.faces[f].patch);
+            }, sk);
+            for (size_t f = 0; f < nf; ++f) {
+                scN[k][f] = sk[f];
+                scN[0][f] += sk[f];
+            }
+        }
+        std::vector<std::vector<V3>> DFluxN(NS, std::vector<V3>(nf, v3(0, 0, 0)));
+        if (cf.molmass_diffusion && NS > 1) {
+            std::vector<std::vector<V3>> gradXN(NS);
+            for (int k = 0; k < NS; ++k) {
+                std::vector<double> X(nc);
+                for (long long i = 0; i < nc; ++i) X[i] = cN[k + 1][i] / cN[0][i];
+                dSurfGrad(cs, X, [&](size_t f) {  // calculatedMolarFraction of the phase (cell)
+                    double cB[FV_MAX_SPECIES + 1];
+                    dBoundaryConc(cs, cs.faces[f].own, cs.faces[f].patch, true, cB, bad);
+                    double sum = 0;
+                    for (int q = 1; q <= NS; ++q) sum += cB[q];
+                    return cB[k + 1] / sum;
+                }, gradXN[k]);
+            }
+            for (size_t f = 0; f < nf; ++f) {
+                double Nc[FV_MAX_SPECIES + 1];
+                for (int k = 0; k <= NS; ++k) Nc[k] = scN[k][f];
+                for (int d = 0; d < 3; ++d) {
+                    double g[FV_MAX_SPECIES], out[FV_MAX_SPECIES];
+                    for (int k = 0; k < NS; ++k) g[k] = gradXN[k][f].x[d];
+                    dMaxwellStefan(NS, Nc, mx.M, Dc, g, out);
+                    for (int k = 0; k < NS; ++k) DFluxN[k][f].x[d] = out[k];
+                }
+            }
+        }
+        std::vector<V3> afDif(nf, v3(0, 0, 0));
+        for (int k = 0; k < NS; ++k)
+            for (size_t f = 0; f < nf; ++f) {
+                const V3 flowW = vmul(gradW[k][f], -1 * rhoD[k][f]);
+                const V3 corr = cf.molmass_diffusion ? vsub(DFluxN[k][f], flowW) : v3(0, 0, 0);
+                const double h = dhkT(mx, scN[k + 1][f], surfaceT[f], k);
+                afDif[f] = vadd(afDif[f], vdiv(vmul(vadd(corr, flowW), h), mx.M[k]));
+            }
+        for (size_t f = 0; f < nf; ++f) entFlow[f] = vadd(vmul(afDif[f], 0.5), vmul(entFlow[f], 1 - 0.5));
+    }
+
+    // velocity and temperature matrices (Diffusion.cpp:480-500; SLEMatrix.cpp:2054-2110
+    // explicit, :410-546 and :706-907 implicit)
     std::vector<V3> freeV(nc, v3(0, 0, 0)), oldV(nc);
-    {
+    SLE1 MV[3];
+    for (long long i = 0; i < nc; ++i) oldV[i] = vmul(v[i], cs.rho[0][i]);
+    if (gs) {
+        for (int d = 0; d < 3; ++d) {
+            std::vector<double> rOld(nc);
+            for (long long i = 0; i < nc; ++i) rOld[i] = oldV[i].x[d];
+            std::vector<double> muF(nf, mu);
+            dLaplacian(cs, [&, d](long long i, int fi) {
+                return bcCellV(cs, v[i], cs.faces[fi].patch, cs.faces[fi].N, bad).x[d];
+            }, rOld, cs.rho[0], muF, dt, MV[d]);
+            for (long long i = 0; i < nc; ++i) freeV[i].x[d] = MV[d].free[i];
+        }
+    } else {
         std::vector<T9> flow(nf);
         for (size_t f = 0; f < nf; ++f) flow[f] = tmul(tmul(gradVs[f], mu), -1.);
         std::vector<V3> div;
         dDivT(cs, flow, div);
-        for (long long i = 0; i < nc; ++i) {
-            oldV[i] = vmul(v[i], cs.rho[0][i]);
+        for (long long i = 0; i < nc; ++i)
             for (int d = 0; d < 3; ++d) freeV[i].x[d] -= div[i].x[d];
-        }
     }
     std::vector<double> freeT(nc, 0.0), diagT(CCVNew);
+    SLE1 MT;
     {
-        std::vector<V3> gT;
-        dSurfGrad(cs, T, [&](size_t f) { return dBoundaryT(cs, cs.faces[f].own, cs.faces[f].patch, true, bad); }, gT);
-        std::vector<V3> flow(nf);
-        for (size_t f = 0; f < nf; ++f) flow[f] = vmul(vmul(gT[f], kappa), -1.);
-        std::vector<double> div;
-        dDivV(cs, flow, div);
-        for (long long i = 0; i < nc; ++i) freeT[i] -= div[i];
+        auto ghostT = [&](size_t f) { return dBoundaryT(cs, cs.faces[f].own, cs.faces[f].patch, true, bad); };
+        if (gs) {
+            std::vector<double> kF(nf, kappa);
+            dLaplacian(cs, [&](long long, int fi) { return ghostT(fi); }, oldEnergy, CCVNew, kF, dt, MT);
+            diagT = MT.diag;
+            freeT = MT.free;
+        } else {
+            std::vector<V3> gT;
+            dSurfGrad(cs, T, ghostT, gT);
+            std::vector<V3> flow(nf);
+            for (size_t f = 0; f < nf; ++f) flow[f] = vmul(vmul(gT[f], kappa), -1.);
+            std::vector<double> div;
+            dDivV(cs, flow, div);
+            for (long long i = 0; i < nc; ++i) freeT[i] -= div[i];
+        }
     }
     // explicit deviatoric viscous stress on the velocity (Diffusion.cpp:503-506,600-605)
     {
@@ -2078,14 +2256,30 @@ int diffusionStage(fvo_case& cs, double dt) {
         return FV_ERR_BOUNDARY;
     }
 
+    // the implicit solves: velocity by components, then temperature (Diffusion.cpp:786-826)
+    std::vector<double> vSol[3], TSol;
+    if (gs) {
+        for (int d = 0; d < 3; ++d) {
+            std::vector<double> start(nc);
+            for (long long i = 0; i < nc; ++i) {
+                start[i] = v[i].x[d];
+                MV[d].free[i] = freeV[i].x[d];
+            }
+            vSol[d] = dGaussSeidel(MV[d], start, cf.sle_max_iter);
+        }
+        MT.diag = diagT;
+        MT.free = freeT;
+        TSol = dGaussSeidel(MT, T, cf.sle_max_iter);
+    }
+
     // the phase after the stage (Diffusion.cpp:965-1034)
     double Tmin = std::numeric_limits<double>::infinity();
     cs.Tstate.assign(nc, 0.0);
     cs.Tvalid = true;
     for (long long i = 0; i < nc; ++i) {
         V3 vn;
-        for (int d = 0; d < 3; ++d) vn.x[d] = (oldV[i].x[d] + freeV[i].x[d] * dt) / cs.rho[0][i];
-        const double Tn = (oldEnergy[i] + freeT[i] * dt) / diagT[i];
+        for (int d = 0; d < 3; ++d) vn.x[d] = gs ? vSol[d][i] : (oldV[i].x[d] + freeV[i].x[d] * dt) / cs.rho[0][i];
+        const double Tn = gs ? TSol[i] : (oldEnergy[i] + freeT[i] * dt) / diagT[i];
         Tmin = std::min(Tmin, Tn);
         cs.Tstate[i] = Tn;
         double cc[FV_MAX_SPECIES + 1];
@@ -2520,11 +2714,14 @@ bool validate(const fv_config& cf, std::string& err) {
             err = "the diffusion stage runs with ideal and van der Waals mixtures";
             return false;
         }
-        if (cf.sle_solver != FV_SLE_EXPLICIT) { err = "the diffusion stage runs with the explicit solver"; return false; }
+        if (cf.sle_solver != FV_SLE_EXPLICIT && cf.sle_solver != FV_SLE_GAUSS_SEIDEL) {
+            err = "the diffusion stage runs with the explicit and Gauss-Seidel solvers";
+            return false;
+        }
         if (cf.transport != FV_TRANSPORT_CONSTANT) { err = "the diffusion stage runs with constant transport coefficients"; return false; }
         if (cf.chemistry != FV_CHEM_NONE) { err = "the diffusion stage runs without chemistry"; return false; }
         if (cf.enthalpy_flow < FV_ENTHALPY_NO || cf.enthalpy_flow > FV_ENTHALPY_EXPLICIT) {
-            err = "the explicit diffusion stage takes no or explicit enthalpy flow";
+            err = "the diffusion stage takes no or explicit enthalpy flow";
             return false;
         }
     }

@@ -537,6 +537,20 @@ fv_status ensureScratch(fv_handle* h) {
         FV_CUDA(h, cudaMalloc(&X.cellPrim, sizeof(double) * (2 * ns + 5) * st));
         FV_CUDA(h, cudaMalloc(&X.stagePrim, sizeof(double) * (ns + 6) * st));
         FV_CUDA(h, cudaMalloc(&X.partMin, sizeof(double) * 2 * (size_t)diffusionBlocks(h->P)));
+        if (X.gs) {
+            FV_CUDA(h, cudaMalloc(&X.wDiag, sizeof(double) * ns * st));
+            FV_CUDA(h, cudaMalloc(&X.wFree, sizeof(double) * ns * st));
+            FV_CUDA(h, cudaMalloc(&X.wOff, sizeof(double) * 6 * st));
+            FV_CUDA(h, cudaMalloc(&X.vDiag, sizeof(double) * st));
+            FV_CUDA(h, cudaMalloc(&X.vFree, sizeof(double) * 3 * st));
+            FV_CUDA(h, cudaMalloc(&X.vOff, sizeof(double) * 6 * st));
+            FV_CUDA(h, cudaMalloc(&X.tDiag, sizeof(double) * st));
+            FV_CUDA(h, cudaMalloc(&X.tFree, sizeof(double) * st));
+            FV_CUDA(h, cudaMalloc(&X.tOff, sizeof(double) * 6 * st));
+            FV_CUDA(h, cudaMalloc(&X.sol, sizeof(double) * (ns + 4) * st));
+            FV_CUDA(h, cudaMalloc(&X.work, sizeof(double) * 2 * st));
+            FV_CUDA(h, cudaMalloc(&X.cNew, sizeof(double) * (ns + 3) * st));
+        }
         h->P.starV = X.starV;
         h->P.stagePrim = X.stagePrim;
     }
@@ -675,6 +689,8 @@ fv_status fv_create(const fv_config* cfg, fv_handle** out) {
         // "linear" reconstruction takes the cell velocities' gradient (Diffusion.cpp:178-184)
         X.interpV = cfg->gravity || cfg->linear_reconstruction;
         X.dtDiff = cfg->diffusion_timestep != 0;
+        X.gs = cfg->sle_solver == FV_SLE_GAUSS_SEIDEL;
+        X.maxIter = cfg->sle_max_iter;
         X.coeffSource = cfg->dt_coeff_source;
         X.coeffDiff = cfg->dt_coeff_diffusion;
     }
@@ -775,7 +791,9 @@ void fv_destroy(fv_handle* h) {
     if (h->FS) cudaFree(h->FS);
     if (h->FL) cudaFree(h->FL);
     if (h->outBuf) cudaFree(h->outBuf);
-    for (double* q : {h->diff.starV, h->diff.face, h->diff.cellPrim, h->diff.stagePrim, h->diff.partMin})
+    for (double* q : {h->diff.starV, h->diff.face, h->diff.cellPrim, h->diff.stagePrim, h->diff.partMin, h->diff.wDiag,
+                      h->diff.wFree, h->diff.wOff, h->diff.vDiag, h->diff.vFree, h->diff.vOff, h->diff.tDiag,
+                      h->diff.tFree, h->diff.tOff, h->diff.sol, h->diff.work, h->diff.cNew})
         if (q) cudaFree(q);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
@@ -1045,6 +1063,10 @@ long long fv_kernels_per_step(const fv_handle* h) {
     if (!h) return 0;
     const int stage = h->path == PATH_MARCH ? 1 : 4;
     const int chem = h->cfg.chemistry != FV_CHEM_NONE ? 1 : 0;
+    if (h->cfg.diffusion && h->diff.gs)
+        // prim, faces, the mass-fraction matrices and N solves, concentrations, the averaged
+        // enthalpy flow, velocity / temperature matrices and nmom + 1 solves, phase, source, finalize
+        return stage + 2 + 1 + h->cfg.n_species + 1 + (h->diff.enthalpy ? 1 : 0) + 1 + h->P.nmom + 1 + 1 + 1 + 1;
     if (h->cfg.diffusion) return stage + 5;  // the stage's 4 kernels, finalize
     if (h->cfg.order == FV_ORDER_SECOND_RK) return 2 * stage + 2 + chem;  // two stages, average, finalize
     if (h->cfg.order == FV_ORDER_THIRD || h->cfg.order == FV_ORDER_THIRD_CADA)

@@ -1,6 +1,7 @@
 // fv_diffusion.cu -- instantiations and launcher of the diffusion stage (fv_diffusion.cuh), FP64
 // with --fmad=false like the reference's arithmetic.
 #include "fv_diffusion.cuh"
+#include "fv_diffusion_gs.cuh"
 #include "fv_diffusion_launch.h"
 
 namespace fv {
@@ -15,7 +16,26 @@ cudaError_t launchT(const StepParams& P, const GenericLayout& L, const diff::Dif
     const unsigned gf = (unsigned)((L.nfaces + kDiffThreads - 1) / kDiffThreads);
     diff::k_diff_prim<NS, EOS, D><<<gc, kDiffThreads, 0, st>>>(P, X, U, ck);
     diff::k_diff_faces<NS, EOS, D><<<gf, kDiffThreads, 0, st>>>(P, L, X, ck);
-    diff::k_diff_cells<NS, EOS, D><<<gc, kDiffThreads, 0, st>>>(P, L, X, U, ck, blockMax);
+    if (!X.gs) {
+        diff::k_diff_cells<NS, EOS, D><<<gc, kDiffThreads, 0, st>>>(P, L, X, U, ck, blockMax);
+    } else {
+        // the implicit solver: mass-fraction matrices and solves, new concentrations, the
+        // averaged enthalpy flow, velocity and temperature matrices and solves, the phase
+        const long long s = P.stride;
+        diff::k_gs_wmat<NS, EOS, D><<<gc, kDiffThreads, 0, st>>>(P, L, X, U, ck);
+        for (int k = 0; k < NS; ++k)
+            diff::k_gs_solve<D><<<1, diff::kGsThreads, 0, st>>>(P, X.wDiag + k * s, X.wFree + k * s, X.wOff,
+                                                               X.sol + k * s, X.work, X.maxIter, ck);
+        diff::k_gs_post1<NS, EOS, D><<<gc, kDiffThreads, 0, st>>>(P, X, U, ck);
+        if (X.enthalpy) diff::k_gs_afdif<NS, EOS, D><<<gf, kDiffThreads, 0, st>>>(P, L, X, ck);
+        diff::k_gs_vtmat<NS, EOS, D><<<gc, kDiffThreads, 0, st>>>(P, L, X, U, ck);
+        for (int d = 0; d < P.nmom; ++d)
+            diff::k_gs_solve<D><<<1, diff::kGsThreads, 0, st>>>(P, X.vDiag, X.vFree + d * s, X.vOff,
+                                                               X.sol + (NS + d) * s, X.work, X.maxIter, ck);
+        diff::k_gs_solve<D><<<1, diff::kGsThreads, 0, st>>>(P, X.tDiag, X.tFree, X.tOff, X.sol + (NS + 3) * s,
+                                                           X.work, X.maxIter, ck);
+        diff::k_gs_final<NS, EOS, D><<<gc, kDiffThreads, 0, st>>>(P, L, X, U, ck, blockMax);
+    }
     diff::k_diff_source<<<1, 1024, 0, st>>>(X, ck, (int)gc);
     return cudaGetLastError();
 }

@@ -43,8 +43,9 @@ namespace diff {
 
 
 // face quantity slots: flowW_k, corr_k (k < N), enthalpy flow, velocity Laplacian flow (3),
-// deviatoric stress (3), temperature Laplacian flow, maximal coefficient
-template <int NS> __host__ __device__ constexpr int faceSlots() { return 2 * NS + 9; }
+// deviatoric stress (3), temperature Laplacian flow, maximal coefficient; for the implicit
+// solver also the interpolated density and temperature
+template <int NS> __host__ __device__ constexpr int faceSlots() { return 2 * NS + 11; }
 template <int NS> __device__ __forceinline__ int slotW(int k) { return k; }
 template <int NS> __device__ __forceinline__ int slotCorr(int k) { return NS + k; }
 template <int NS> __device__ __forceinline__ int slotEnt() { return 2 * NS; }
@@ -52,6 +53,8 @@ template <int NS> __device__ __forceinline__ int slotV(int d) { return 2 * NS + 
 template <int NS> __device__ __forceinline__ int slotDev(int d) { return 2 * NS + 4 + d; }
 template <int NS> __device__ __forceinline__ int slotT() { return 2 * NS + 7; }
 template <int NS> __device__ __forceinline__ int slotMax() { return 2 * NS + 8; }
+template <int NS> __device__ __forceinline__ int slotRho() { return 2 * NS + 9; }
+template <int NS> __device__ __forceinline__ int slotTs() { return 2 * NS + 10; }
 
 // ----------------------------------------------------------------------------- mixture functions
 // mixtureIdeal.cpp / mixtureVanDerWaals.cpp with idealFluid.cpp / vanDerWaalsFluid.cpp
@@ -440,7 +443,9 @@ __global__ void k_diff_faces(const StepParams P, const GenericLayout L, const Di
             const double h = hkT<EOS>(P.mix, sc[k + 1], sT, k);
             ent = ent + (corr[k] + flowW[k]) * h / P.mix.M[k];
         }
-        F[slotEnt<NS>() * nf + f] = ent * sT;
+        // the implicit solver averages the flow with the one of the new concentrations before the
+        // product with T (Diffusion.cpp:618-690)
+        F[slotEnt<NS>() * nf + f] = X.gs ? ent : ent * sT;
     }
     // velocity: surfGrad column a (dv_i / |d|^2) d_a, surfDivergence, the Laplacian flow and the
     // deviatoric stress (gradient transposed, 2/3 div off the diagonal) of the face
@@ -477,6 +482,10 @@ __global__ void k_diff_faces(const StepParams P, const GenericLayout L, const Di
     const double Tother = boundary ? boundaryT<NS, EOS>(P, g.patch, cO, pO, true, bad) : TN;
     F[slotT<NS>() * nf + f] = sgrad(TO, Tother) * X.kappa * -1.;
     if (X.dtDiff) F[slotMax<NS>() * nf + f] = smax(smax(X.kappa, sRho * X.D), X.mu);
+    if (X.gs) {
+        F[slotRho<NS>() * nf + f] = sRho;
+        F[slotTs<NS>() * nf + f] = sT;
+    }
     if (X.interpV) {
         // star.v = linearInterpolate(velocity) (secondOrderStepSolver.cpp:71-73, or the
         // "linear" reconstruction's grad(velocity), Diffusion.cpp:178-184)

@@ -1,0 +1,614 @@
+// fv_diffusion_gs.cuh -- the diffusion stage with the Gauss-Seidel solver (#Type_of_SLE_solver_flag
+// GaussSeidel): the implicit matrices of SLEMatrix::generateDTimeLaplacian (SLEMatrix.cpp:410-546,
+// 706-907) and GaussSeidelSolver::algorithm (GaussSeidelSolver.cpp:12-82), FP64 in the
+// reference's operation order.
+//
+// Matrix of a field phi with face coefficient D_f: diagonal rNew / dt + sum over the cell's faces
+// (in its face order) of D_f / |d| (n S / V & d / |d|), free term rOld / dt plus, on a patch, that
+// coefficient times the ghost value; the neighbour of an inner face gets -D_f / |d| (...).  On
+// this mesh n = +-e_a and an inner face's d lies along a, so the product is n_a S / V d_a / |d|
+// (the other terms add zeros); a patch's d = 2 (r_f - r_C) enters through |d| and d_a / |d|.
+//
+// The solver sweeps forward, then backward, until 100 max |(new - old) / (|new| + eps)| < 1e-12 or
+// the iteration limit.  The backward sweep recomputes every cell from the old iterate of its lower
+// neighbours and the new one of its upper neighbours, so the forward sweep's values are never
+// read and the iterate is the backward sweep's alone.  Cells with the same i + j + k depend on
+// none of each other in that sweep: k_gs_solve runs it as wavefronts of decreasing i + j + k in
+// one CTA (the order of every cell's own operations is the reference's), a 1D mesh on one thread.
+// Without a periodic axis the lower neighbours of cell (i, j, k) in its face order are x-, y-, z-
+// and the upper ones x+, y+, z+.
+#pragma once
+
+#include "fv_diffusion.cuh"
+
+namespace fv {
+namespace diff {
+
+// geometry of face slot s of cell ijk: the neighbour (or -1 on a patch), |d| and (n S / V)_a d_a / |d|
+struct FaceCoef {
+    long long nb;
+    double m, dot;
+    FaceGeo g;
+};
+template <int D>
+__device__ __forceinline__ FaceCoef faceCoef(const StepParams& P, const GenericLayout& L, const int* ijk, int a, int hi,
+                                             const double* rc, double V) {
+    FaceCoef c;
+    c.g = faceOf(P, L, ijk, a, hi);
+    double dR[3];
+    double onA;
+    if (!c.g.boundary) {
+        int nbc[3];
+        double sh;
+        neighbourOf(P, ijk, a, hi, nbc, sh);
+        c.nb = cellIndex(P, nbc[0], nbc[1], nbc[2]);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double cn = P.geo.cc[d][nbc[d]];
+            dR[d] = (d == a ? cn + sh : cn) - rc[d];
+        }
+        onA = c.g.own ? (1.0 * c.g.S) / V : ((1.0 * c.g.S) / V) * -1;
+    } else {
+        c.nb = -1;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) dR[d] = (c.g.rc[d] - rc[d]) * 2;
+        onA = (double(c.g.sign) * c.g.S) / V;
+    }
+    c.m = mag3<double>(dR[0], dR[1], dR[2]);
+    c.dot = onA * (dR[a] / c.m);
+    return c;
+}
+
+template <int D> __device__ __forceinline__ void faceOrder(int* fa, int* fh) {
+    int q = 0;
+    fa[q] = 0; fh[q++] = 0;
+    fa[q] = 0; fh[q++] = 1;
+    if (D >= 2) { fa[q] = 1; fh[q++] = 1; fa[q] = 1; fh[q++] = 0; }
+    if (D >= 3) { fa[q] = 2; fh[q++] = 0; fa[q] = 2; fh[q++] = 1; }
+}
+
+// ----------------------------------------------------------------------------- k_gs_wmat
+// the mass fractions' matrices (their coefficient rho D is the same for every species) and the
+// molar-mass correction distributed into them (Diffusion.cpp:321-339, 396-412)
+template <int NS, int EOS, int D>
+__global__ void k_gs_wmat(const StepParams P, const GenericLayout L, const DiffParams X, const double* __restrict__ U,
+                          DevClock* __restrict__ ck) {
+    if (ck->done) return;
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= P.ncell) return;
+    const long long st = P.stride, nf = L.nfaces;
+    const double rt = 1 / ck->dt;
+    int ijk[3];
+    cellAxisCoords(P, i, D, ijk);
+    const double ex = extent(P, 0, ijk[0]), ey = extent(P, 1, ijk[1]), ez = extent(P, 2, ijk[2]);
+    const double V = ex * ey * ez;
+    const double rc[3] = {P.geo.cc[0][ijk[0]], P.geo.cc[1][ijk[1]], P.geo.cc[2][ijk[2]]};
+    const double* cp = X.cellPrim;
+    const double* F = X.face;
+    const double rho0 = U[NS * st + i];
+    double c[NS + 1], w[NS];
+    c[0] = 0;
+#pragma unroll
+    for (int k = 1; k <= NS; ++k) {
+        c[k] = cp[(k - 1) * st + i];
+        c[0] += c[k];
+    }
+#pragma unroll
+    for (int k = 0; k < NS; ++k) w[k] = cp[(NS + 5 + k) * st + i];
+    // the patch's concentrations as cell values (calculatedMassFraction's ghosts)
+    double diag = rho0 * rt, free[NS], divC[NS];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        free[k] = (w[k] * rho0) * rt;
+        divC[k] = 0;
+    }
+    bool bad = false;
+    constexpr int NFC = 2 * D;
+    int fa[NFC], fh[NFC];
+    faceOrder<D>(fa, fh);
+#pragma unroll
+    for (int s = 0; s < NFC; ++s) {
+        const FaceCoef fc = faceCoef<D>(P, L, ijk, fa[s], fh[s], rc, V);
+        const long long f = fc.g.f;
+        const double rhoD = F[slotRho<NS>() * nf + f] * X.D;
+        const double coef = rhoD / fc.m * fc.dot;
+        diag += coef;
+        if (fc.nb >= 0) {
+            X.wOff[s * st + i] = -rhoD / fc.m * fc.dot;
+        } else {
+            X.wOff[s * st + i] = 0;
+            double cB[NS + 1];
+            cB[0] = 0;
+#pragma unroll
+            for (int k = 1; k <= NS; ++k) {
+                cB[k] = cellGhostScalar<double, NS>(P, fc.g.patch, k - 1, c[k], bad);
+                cB[0] += cB[k];
+            }
+            double sum = 0;
+#pragma unroll
+            for (int q = 1; q <= NS; ++q) sum += cB[q] * P.mix.M[q - 1];
+#pragma unroll
+            for (int k = 0; k < NS; ++k) free[k] += coef * ((cB[k + 1] * P.mix.M[k]) / sum);
+        }
+        if (X.molmass) {
+            const double nsg = fc.g.own ? double(fc.g.sign) : double(-fc.g.sign);
+#pragma unroll
+            for (int k = 0; k < NS; ++k) divC[k] += F[slotCorr<NS>(k) * nf + f] * nsg * fc.g.S;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        double dk = diag, fk = free[k];
+        if (X.molmass) {
+            const double s = (divC[k] / V) * (-1.0);
+            if (s >= 0.) fk += s;
+            else dk -= s / (w[k] + Num<double>::stab());
+        }
+        X.wDiag[k * st + i] = dk;
+        X.wFree[k * st + i] = fk;
+        X.sol[k * st + i] = w[k];  // the solve's start: the current mass fraction
+    }
+    if (bad) raise(ck, FV_ERR_BOUNDARY);
+}
+
+
+// ----------------------------------------------------------------------------- k_gs_solve
+// One CTA solves diag x + off x = free for the field in x (start in, solution out): backward
+// sweeps as wavefronts, the convergence measure reduced over the CTA after each sweep.
+constexpr int kGsThreads = 1024;
+
+template <int D>
+__device__ __forceinline__ double gsCell(const StepParams& P, long long i, const int* ijk, const double* __restrict__ diag,
+                                         const double* __restrict__ free, const double* __restrict__ off,
+                                         const double* oldI, const double* newI) {
+    // (the iterates are written by other threads of the CTA between wavefronts: plain loads)
+    const long long st = P.stride;
+    const double aii = 1. / diag[i];
+    double x = free[i] * aii;
+    // lower neighbours in reverse face order: z-, y-, x-; then upper: z+, y+, x+
+    if (D >= 3 && ijk[2] > 0) x -= off[4 * st + i] * oldI[i - (long long)P.n[0] * P.n[1]] * aii;
+    if (D >= 2 && ijk[1] > 0) x -= off[3 * st + i] * oldI[i - P.n[0]] * aii;
+    if (ijk[0] > 0) x -= off[0 * st + i] * oldI[i - 1] * aii;
+    if (D >= 3 && ijk[2] < P.n[2] - 1) x -= off[5 * st + i] * newI[i + (long long)P.n[0] * P.n[1]] * aii;
+    if (D >= 2 && ijk[1] < P.n[1] - 1) x -= off[2 * st + i] * newI[i + P.n[0]] * aii;
+    if (ijk[0] < P.n[0] - 1) x -= off[1 * st + i] * newI[i + 1] * aii;
+    return x;
+}
+
+template <int D>
+__global__ void __launch_bounds__(kGsThreads) k_gs_solve(const StepParams P, const double* __restrict__ diag,
+                                                          const double* __restrict__ free,
+                                                          const double* __restrict__ off, double* __restrict__ x,
+                                                          double* __restrict__ work, int maxIt,
+                                                          DevClock* __restrict__ ck) {
+    __shared__ double red[32];
+    __shared__ int stop;
+    if (ck->done) return;
+    const long long n = P.ncell;
+    const int nx = P.n[0], ny = P.n[1], nz = P.n[2];
+    double* bufA = x;       // the old iterate
+    double* bufB = work;    // the new one
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) bufB[i] = x[i];
+    __syncthreads();
+    for (int it = 1;; ++it) {
+        if (D == 1) {
+            if (threadIdx.x == 0)
+                for (long long i = n - 1; i >= 0; --i) {
+                    const int ijk[3] = {(int)i, 0, 0};
+                    bufB[i] = gsCell<D>(P, i, ijk, diag, free, off, bufA, bufB);
+                }
+        } else {
+            const int smax = (nx - 1) + (ny - 1) + (D >= 3 ? nz - 1 : 0);
+            for (int sw = smax; sw >= 0; --sw) {
+                // the cells with i + j (+ k) = sw
+                const long long cand = D >= 3 ? (long long)nx * ny : (long long)nx;
+                for (long long q = threadIdx.x; q < cand; q += blockDim.x) {
+                    int ijk[3];
+                    ijk[0] = (int)(q % nx);
+                    ijk[1] = D >= 3 ? (int)(q / nx) : sw - ijk[0];
+                    ijk[2] = D >= 3 ? sw - ijk[0] - ijk[1] : 0;
+                    if (ijk[1] < 0 || ijk[1] >= ny || ijk[2] < 0 || ijk[2] >= nz) continue;
+                    const long long i = ijk[0] + (long long)nx * (ijk[1] + (long long)ny * ijk[2]);
+                    bufB[i] = gsCell<D>(P, i, ijk, diag, free, off, bufA, bufB);
+                }
+                __syncthreads();
+            }
+        }
+        __syncthreads();
+        double mx = 0;
+        for (long long i = threadIdx.x; i < n; i += blockDim.x)
+            mx = smax(mx, fabs((bufB[i] - bufA[i]) / (fabs(bufB[i]) + Num<double>::stab())));
+        mx = blockMaxReduce<double>(mx, red);
+        if (threadIdx.x == 0) stop = (100. * mx < 1e-12) || it >= maxIt;
+        __syncthreads();
+        if (stop) break;
+        double* t = bufA;  // old = new
+        bufA = bufB;
+        bufB = t;
+        __syncthreads();
+    }
+    // normalize, and the solution into x
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+        double v = bufB[i];
+        if (fabs(v) < 2.220446049250313e-16) v = 0;
+        x[i] = v;
+    }
+}
+
+
+// ----------------------------------------------------------------------------- k_gs_post1
+// new mass fractions (clipped at 0, renormalised), concentrations, CCV and the old energy
+// (Diffusion.cpp:443-478)
+template <int NS, int EOS, int D>
+__global__ void k_gs_post1(const StepParams P, const DiffParams X, const double* __restrict__ U,
+                           DevClock* __restrict__ ck) {
+    if (ck->done) return;
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= P.ncell) return;
+    const long long st = P.stride;
+    const double* cp = X.cellPrim;
+    const double rho0 = U[NS * st + i];
+    double wNew[NS], sum = 0.;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        double x = X.sol[k * st + i];
+        if (x < 0.) x = 0.0;
+        wNew[k] = x;
+        sum += x;
+    }
+    double c[NS + 1], cN[NS + 1];
+    c[0] = 0;
+    cN[0] = 0;
+#pragma unroll
+    for (int k = 1; k <= NS; ++k) {
+        c[k] = cp[(k - 1) * st + i];
+        c[0] += c[k];
+        cN[k] = wNew[k - 1] / sum * rho0 / P.mix.M[k - 1];
+        cN[0] += cN[k];
+    }
+    const double T = cp[(NS + 4) * st + i];
+    const double CCVOld = c[0] * mixCv<NS, EOS>(P.mix, c);
+    const double CCVNew = mixCv<NS, EOS>(P.mix, cN) * cN[0];
+    const double oldEnergy = CCVOld * T + nonIdeality<NS, EOS>(P.mix, c) - nonIdeality<NS, EOS>(P.mix, cN);
+#pragma unroll
+    for (int k = 0; k <= NS; ++k) X.cNew[k * st + i] = cN[k];
+    X.cNew[(NS + 1) * st + i] = CCVNew;
+    X.cNew[(NS + 2) * st + i] = oldEnergy;
+}
+
+// ----------------------------------------------------------------------------- k_gs_afdif
+// the enthalpy flow again with the new concentrations (their interpolation, molar fractions and
+// Maxwell-Stefan fluxes; the patches' molar fractions still those of the phase) and its 0.5
+// average with the first, then the product with the face temperature (Diffusion.cpp:618-690)
+template <int NS, int EOS, int D>
+__global__ void k_gs_afdif(const StepParams P, const GenericLayout L, const DiffParams X, DevClock* __restrict__ ck) {
+    if (ck->done) return;
+    const long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (f >= L.nfaces) return;
+    int a = 0;
+    while (a + 1 < D && f >= L.faceBase[a + 1]) ++a;
+    const long long local = f - L.faceBase[a];
+    const int n = P.n[a];
+    const int fi = (int)(local % (n + 1));
+    if (P.periodic[a] && fi == 0) return;
+    const long long tr = local / (n + 1);
+    int ijk[3];
+    if (a == 0) { ijk[1] = D >= 2 ? (int)(tr % P.n[1]) : 0; ijk[2] = D >= 3 ? (int)(tr / P.n[1]) : 0; }
+    else if (a == 1) { ijk[0] = (int)(tr % P.n[0]); ijk[2] = D >= 3 ? (int)(tr / P.n[0]) : 0; }
+    else { ijk[0] = (int)(tr % P.n[0]); ijk[1] = (int)(tr / P.n[0]); }
+    const bool boundary = !P.periodic[a] && (fi == 0 || fi == n);
+    ijk[a] = fi == 0 ? 0 : fi - 1;
+    const int hi = (boundary && fi == 0) ? 0 : 1;
+    const FaceGeo g = faceOf(P, L, ijk, a, hi);
+    const long long o = cellIndex(P, ijk[0], ijk[1], ijk[2]);
+    const long long st = P.stride, nf = L.nfaces;
+    const double rO[3] = {P.geo.cc[0][ijk[0]], P.geo.cc[1][ijk[1]], P.geo.cc[2][ijk[2]]};
+    bool bad = false;
+    long long nb = -1;
+    double dA = 0, m2 = 0, dnA = 0, dmag = 0, wOwn = 0, wNei = 0;
+    if (!boundary) {
+        int nbc[3];
+        double sh;
+        neighbourOf(P, ijk, a, 1, nbc, sh);
+        nb = cellIndex(P, nbc[0], nbc[1], nbc[2]);
+        double dv[3], dOwn[3], dNei[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double cnb = P.geo.cc[d][nbc[d]];
+            const double neiP = d == a ? cnb + sh : cnb;
+            dv[d] = neiP - rO[d];
+            dOwn[d] = g.rc[d] - rO[d];
+            dNei[d] = g.rc[d] - neiP;
+        }
+        const double mg = mag3<double>(dv[0], dv[1], dv[2]);
+        m2 = mg * mg;
+        dA = dv[a];
+        const double ownR = mag3<double>(dOwn[0], dOwn[1], dOwn[2]);
+        const double neiR = mag3<double>(dNei[0], dNei[1], dNei[2]);
+        const double sumR = ownR + neiR;
+        wOwn = neiR / sumR;
+        wNei = ownR / sumR;
+    } else {
+        double dR[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) dR[d] = (g.rc[d] - rO[d]) * 2.;
+        dmag = mag3<double>(dR[0], dR[1], dR[2]);
+        dnA = dR[a] / dmag;
+    }
+    auto sgrad = [&](double phiO, double other) {
+        if (!boundary) return ((other - phiO) / m2) * dA;
+        return ((other - phiO) / dmag) * dnA;
+    };
+    const double* cn = X.cNew;
+    double cO[NS + 1], cNb[NS + 1], sc[NS + 1];
+    sc[0] = 0.0;
+#pragma unroll
+    for (int k = 0; k <= NS; ++k) {
+        cO[k] = cn[k * st + o];
+        cNb[k] = boundary ? 0.0 : cn[k * st + nb];
+    }
+#pragma unroll
+    for (int k = 1; k <= NS; ++k) {
+        sc[k] = boundary ? surfaceScalar<double, NS>(P, g.patch, k - 1, cO[k]) : cO[k] * wOwn + cNb[k] * wNei;
+        sc[0] += sc[k];
+    }
+    const double* F = X.face;
+    const double sT = F[slotTs<NS>() * nf + f];
+    double flowW[NS], corr[NS];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        flowW[k] = F[slotW<NS>(k) * nf + f];
+        corr[k] = 0;
+    }
+    if (X.molmass && NS == 1) corr[0] = 0 - flowW[0];  // no Maxwell-Stefan flux for one species
+    if (X.molmass && NS > 1) {
+        // the patch's molar fractions from the phase's concentrations (calculatedMolarFraction)
+        double cB[NS + 1];
+        if (boundary) {
+            const double* cp = X.cellPrim;
+            cB[0] = 0;
+#pragma unroll
+            for (int k = 1; k <= NS; ++k) {
+                cB[k] = cellGhostScalar<double, NS>(P, g.patch, k - 1, cp[(k - 1) * st + o], bad);
+                cB[0] += cB[k];
+            }
+        }
+        double gX[NS];
+#pragma unroll
+        for (int k = 0; k < NS; ++k) {
+            const double xO = cO[k + 1] / cO[0];
+            double other;
+            if (boundary) {
+                double sum = 0;
+#pragma unroll
+                for (int q = 1; q <= NS; ++q) sum += cB[q];
+                other = cB[k + 1] / sum;
+            } else {
+                other = cNb[k + 1] / cNb[0];
+            }
+            gX[k] = sgrad(xO, other);
+        }
+        double DF[NS];
+        maxwellStefan<NS>(sc, P.mix.M, X.D, gX, DF);
+#pragma unroll
+        for (int k = 0; k < NS; ++k) corr[k] = DF[k] - flowW[k];
+    }
+    double af = 0;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        const double h = hkT<EOS>(P.mix, sc[k + 1], sT, k);
+        af = af + (corr[k] + flowW[k]) * h / P.mix.M[k];
+    }
+    const double raw = F[slotEnt<NS>() * nf + f];
+    X.face[slotEnt<NS>() * nf + f] = (af * 0.5 + raw * (1 - 0.5)) * sT;
+    if (bad) raise(ck, FV_ERR_BOUNDARY);
+}
+
+
+// ----------------------------------------------------------------------------- k_gs_vtmat
+// the velocity matrices (coefficient mu; the explicit deviatoric stress in their free terms) and
+// the temperature matrix (coefficient kappa; the explicit enthalpy flow distributed into it, its
+// time-step limit's partial minima, the viscous heating) (Diffusion.cpp:480-500, 600-709)
+template <int NS, int EOS, int D>
+__global__ void k_gs_vtmat(const StepParams P, const GenericLayout L, const DiffParams X, const double* __restrict__ U,
+                           DevClock* __restrict__ ck) {
+    __shared__ double red[32];
+    if (ck->done) return;
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    double minE = 1.0 / 0.0;
+    if (i < P.ncell) {
+        const long long st = P.stride, nf = L.nfaces;
+        const double rt = 1 / ck->dt;
+        int ijk[3];
+        cellAxisCoords(P, i, D, ijk);
+        const double ex = extent(P, 0, ijk[0]), ey = extent(P, 1, ijk[1]), ez = extent(P, 2, ijk[2]);
+        const double V = ex * ey * ez;
+        const double rc[3] = {P.geo.cc[0][ijk[0]], P.geo.cc[1][ijk[1]], P.geo.cc[2][ijk[2]]};
+        const double* cp = X.cellPrim;
+        const double* F = X.face;
+        const double rho0 = U[NS * st + i];
+        double c[NS + 1], v[3];
+        c[0] = 0;
+#pragma unroll
+        for (int k = 1; k <= NS; ++k) {
+            c[k] = cp[(k - 1) * st + i];
+            c[0] += c[k];
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) v[d] = cp[(NS + d) * st + i];
+        const double p = cp[(NS + 3) * st + i], T = cp[(NS + 4) * st + i];
+        const double CCVNew = X.cNew[(NS + 1) * st + i], oldEnergy = X.cNew[(NS + 2) * st + i];
+        double vdiag = rho0 * rt, vfree[3], tdiag = CCVNew * rt, tfree = oldEnergy * rt;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) vfree[d] = (v[d] * rho0) * rt;
+        double divDev[3] = {0, 0, 0}, divE = 0, gradV[9], divV = 0;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) gradV[q] = 0;
+        bool bad = false;
+        constexpr int NFC = 2 * D;
+        int fa[NFC], fh[NFC];
+        faceOrder<D>(fa, fh);
+#pragma unroll
+        for (int s = 0; s < NFC; ++s) {
+            const int a = fa[s];
+            const FaceCoef fc = faceCoef<D>(P, L, ijk, a, fh[s], rc, V);
+            const long long f = fc.g.f;
+            const double coefV = X.mu / fc.m * fc.dot, coefT = X.kappa / fc.m * fc.dot;
+            vdiag += coefV;
+            tdiag += coefT;
+            if (fc.nb >= 0) {
+                X.vOff[s * st + i] = -X.mu / fc.m * fc.dot;
+                X.tOff[s * st + i] = -X.kappa / fc.m * fc.dot;
+            } else {
+                X.vOff[s * st + i] = 0;
+                X.tOff[s * st + i] = 0;
+                double gv[3];
+                if (P.bc.vel[fc.g.patch] == FV_BC_FIXED_SURFACE) bad = true;
+                ghostVelocity<double>(P.bc.vel[fc.g.patch], P.bc.vel_value[fc.g.patch], a, fc.g.sign, v, gv);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) vfree[d] += coefV * gv[d];
+                tfree += coefT * boundaryT<NS, EOS>(P, fc.g.patch, c, p, true, bad);
+            }
+            const double nsg = fc.g.own ? double(fc.g.sign) : double(-fc.g.sign);
+            const double S = fc.g.S;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) divDev[d] += F[slotDev<NS>(d) * nf + f] * nsg * S;
+            if (X.enthalpy) divE += F[slotEnt<NS>() * nf + f] * nsg * S;
+            double sv[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) sv[d] = X.starV[d * nf + f];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) gradV[3 * d + a] += sv[d] * nsg * S;
+            divV += sv[a] * nsg * S;
+        }
+        divE /= V;
+        divV /= V;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            divDev[d] /= V;
+            vfree[d] += divDev[d];
+        }
+#pragma unroll
+        for (int q = 0; q < 9; ++q) gradV[q] /= V;
+        if (X.enthalpy) {
+            const double CCVOld = c[0] * mixCv<NS, EOS>(P.mix, c);
+            minE = CCVOld * T / fabs(divE + Num<double>::stab());
+            const double s = divE * -1;
+            if (s >= 0.) tfree += s;
+            else tdiag -= s / (T + Num<double>::stab());
+        }
+        {
+            const double l = (2. / 3.) * divV;
+            double dd = 0;
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    double sv = gradV[3 * q + r] + gradV[3 * r + q];
+                    if (r == q) sv -= l;
+                    dd += sv * X.mu * gradV[3 * r + q];
+                }
+            tfree += dd;
+        }
+        X.vDiag[i] = vdiag;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            X.vFree[d * st + i] = vfree[d];
+            X.sol[(NS + d) * st + i] = v[d];
+        }
+        X.tDiag[i] = tdiag;
+        X.tFree[i] = tfree;
+        X.sol[(NS + 3) * st + i] = T;
+        if (bad) raise(ck, FV_ERR_BOUNDARY);
+    }
+    const double bE = blockMinReduce(minE, red);
+    if (threadIdx.x == 0) X.partMin[blockIdx.x] = bE;
+}
+
+
+// ----------------------------------------------------------------------------- k_gs_final
+// the recomputed phase from the solved velocity and temperature (Diffusion.cpp:965-1025), its CFL
+// signal and the diffusion limit's partial minima (as k_diff_cells)
+template <int NS, int EOS, int D>
+__global__ void k_gs_final(const StepParams P, const GenericLayout L, const DiffParams X, double* __restrict__ U,
+                           DevClock* __restrict__ ck, double* __restrict__ blockMax) {
+    __shared__ double red[32];
+    if (ck->done) return;
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    double localMax = -1, minD = 1.0 / 0.0;
+    if (i < P.ncell) {
+        const long long st = P.stride, nf = L.nfaces;
+        int ijk[3];
+        cellAxisCoords(P, i, D, ijk);
+        const double ex = extent(P, 0, ijk[0]), ey = extent(P, 1, ijk[1]), ez = extent(P, 2, ijk[2]);
+        const double minLS = 1.0 / smin(smin(ex, ey), ez);
+        const double rc[3] = {P.geo.cc[0][ijk[0]], P.geo.cc[1][ijk[1]], P.geo.cc[2][ijk[2]]};
+        const double rho0 = U[NS * st + i];
+        double cNew[NS + 1], vNew[3];
+#pragma unroll
+        for (int k = 0; k <= NS; ++k) cNew[k] = X.cNew[k * st + i];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) vNew[d] = d < P.nmom ? X.sol[(NS + d) * st + i] : 0.0;
+        const double Tn = X.sol[(NS + 3) * st + i];
+        if (Tn < 0.) raise(ck, FV_ERR_NEGATIVE_T);
+        const double Uv = UvcFromT<NS, EOS>(P.mix, cNew, Tn) * cNew[0];
+        const double p = Mixture<double, NS, EOS>::pFromUv(P.mix, cNew, Uv);
+        double v2 = 0;
+        v2 += vNew[0] * vNew[0];
+        v2 += vNew[1] * vNew[1];
+        v2 += vNew[2] * vNew[2];
+#pragma unroll
+        for (int k = 1; k <= NS; ++k) U[(k - 1) * st + i] = cNew[k] * P.mix.M[k - 1];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            if (d < P.nmom) U[(NS + 1 + d) * st + i] = vNew[d] * rho0;
+        U[(NS + 4) * st + i] = Uv + rho0 * v2 * 0.5 + 0.0;
+        double* sp = X.stagePrim;
+#pragma unroll
+        for (int k = 1; k <= NS; ++k) sp[(k - 1) * st + i] = cNew[k];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) sp[(NS + d) * st + i] = vNew[d];
+        sp[(NS + 3) * st + i] = p;
+        sp[(NS + 4) * st + i] = Uv;
+        sp[(NS + 5) * st + i] = Tn;
+        const double sonic = sqrt(Mixture<double, NS, EOS>::sqSonic(Mixture<double, NS, EOS>::coef(P.mix, cNew), cNew,
+                                                                     rho0, Uv, p));
+        localMax = (mag3<double>(vNew[0], vNew[1], vNew[2]) + sonic) * minLS;
+        if (X.dtDiff) {
+            constexpr int NFC = 2 * D;
+            int fa[NFC], fh[NFC];
+            faceOrder<D>(fa, fh);
+            double dist[NFC], sumDist = 0, vol = 0;
+#pragma unroll
+            for (int s = 0; s < NFC; ++s) {
+                const FaceGeo g = faceOf(P, L, ijk, fa[s], fh[s]);
+                double dr[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    double fc = g.rc[d];
+                    if (d == fa[s] && !g.own && !g.boundary && ijk[fa[s]] == 0) fc -= P.ext[fa[s]];
+                    dr[d] = fc - rc[d];
+                }
+                dist[s] = mag3<double>(dr[0], dr[1], dr[2]);
+                sumDist += dist[s];
+            }
+#pragma unroll
+            for (int s = 0; s < NFC; ++s) {
+                const FaceGeo g = faceOf(P, L, ijk, fa[s], fh[s]);
+                vol += X.face[slotMax<NS>() * nf + g.f] * (1 - dist[s] / sumDist);
+            }
+            minD = vol * minLS * minLS;
+        }
+    }
+    const double bm = blockMaxReduce<double>(localMax, red);
+    __syncthreads();
+    const double bD = blockMinReduce(minD, red);
+    if (threadIdx.x == 0) {
+        blockMax[blockIdx.x] = bm;
+        X.partMin[gridDim.x + blockIdx.x] = bD;
+    }
+    if (i == 0) ck->stagePrim = 1;
+}
+
+}  // namespace diff
+}  // namespace fv

@@ -18,6 +18,8 @@ struct DiffParams {
     int interpV;               // 1: cell velocity gradient from interpolated cell velocities
                                //    ("linear" reconstruction, or gravity), else the star velocities
     int dtDiff;                // 1: "Courant-Source-Diffusion" (the diffusion limit)
+    int gs;                    // 1: the Gauss-Seidel (implicit) solver
+    int maxIter;               // its iteration limit (#Number_of_iterations_of_SLE_matrix_solver)
     double coeffSource, coeffDiff;
     double* starV;             // [3][faces] Riemann star velocity of the advection (replaced by
                                //    the interpolated cell velocity when interpV)
@@ -25,6 +27,20 @@ struct DiffParams {
     double* face;              // [2N + 9][faces] face quantities (see faceSlots)
     double* stagePrim;         // [N + 6][stride]: c_1..c_N, v, p, Uv, T after the stage
     double* partMin;           // [2][blocks] per-CTA minima of the enthalpy and diffusion limits
+    // the implicit solver's matrices and solutions (null with the explicit solver); face slots s
+    // in the cell's face order [x-, x+, y+, y-, z-, z+]
+    double* wDiag;             // [N][stride] mass fractions: diagonal, free term
+    double* wFree;
+    double* wOff;              // [6][stride] their off-diagonal coefficient per face slot (shared)
+    double* vDiag;             // [stride] velocity: diagonal (shared by the components)
+    double* vFree;             // [3][stride]
+    double* vOff;              // [6][stride]
+    double* tDiag;             // [stride] temperature
+    double* tFree;
+    double* tOff;              // [6][stride]
+    double* sol;               // [N + 4][stride] solutions: w_1..w_N, v_x, v_y, v_z, T
+    double* work;              // [2][stride] Gauss-Seidel iterates
+    double* cNew;              // [N + 3][stride] concentrations c_0..c_N, CCVNew, old energy
 };
 
 }  // namespace diff

@@ -42,13 +42,25 @@ inline bool fvValidateConfig(const fv_config& c, std::string& e) {
             return false;
         }
         if (c.chemistry != FV_CHEM_NONE) { e = "the diffusion stage runs without chemistry"; return false; }
-        if (c.sle_solver != FV_SLE_EXPLICIT) { e = "the diffusion stage runs with the explicit solver"; return false; }
+        if (c.sle_solver != FV_SLE_EXPLICIT && c.sle_solver != FV_SLE_GAUSS_SEIDEL) {
+            e = "the diffusion stage runs with the explicit and Gauss-Seidel solvers";
+            return false;
+        }
+        if (c.sle_solver == FV_SLE_GAUSS_SEIDEL) {
+            // the wavefront sweep orders neighbours by index: no wrap-around
+            for (int p = 0; p < 6; ++p)
+                if (c.bc_vel[p] == FV_BC_PERIODIC) {
+                    e = "the Gauss-Seidel diffusion stage runs without periodic axes";
+                    return false;
+                }
+            if (c.sle_max_iter < 1) { e = "the Gauss-Seidel solver needs at least one iteration"; return false; }
+        }
         if (c.transport != FV_TRANSPORT_CONSTANT) {
             e = "the diffusion stage runs with constant transport coefficients";
             return false;
         }
         if (c.enthalpy_flow != FV_ENTHALPY_NO && c.enthalpy_flow != FV_ENTHALPY_EXPLICIT) {
-            e = "the explicit diffusion stage takes no or explicit enthalpy flow";
+            e = "the diffusion stage takes no or explicit enthalpy flow";
             return false;
         }
     }

@@ -322,10 +322,9 @@ inline Deck readDeck(const std::string& dir, bool createResult) {
     else if (sle == "GaussSeidel") c.sle_solver = FV_SLE_GAUSS_SEIDEL;
     else if (sle == "Thomas" || sle == "noSolver" || sle == "conjugateGradient" || sle == "JacobiConjugateGradient" ||
              sle == "Jacobi" || sle == "biConjugateGradient") {
-        if (c.diffusion) throw Fail("#Type_of_SLE_solver_flag " + sle + ": the diffusion stage implements explicit");
+        if (c.diffusion)
+            throw Fail("#Type_of_SLE_solver_flag " + sle + ": the diffusion stage implements explicit and GaussSeidel");
     } else throw Fail("Unknown or inappropriate matrix solver flag.");
-    if (c.diffusion && c.sle_solver != FV_SLE_EXPLICIT)
-        throw Fail("#Type_of_SLE_solver_flag " + sle + ": the diffusion stage implements explicit");
     // "Gpu" + an order name: the factory string under which the step-solver adapter runs the
     // step inside the reference's main (schemi_adapter/gpuStepSolver.hpp)
     if (order.rfind("Gpu", 0) == 0) order = order.substr(3);
@@ -405,7 +404,7 @@ inline Deck readDeck(const std::string& dir, bool createResult) {
         if (enthalpy == "no") c.enthalpy_flow = FV_ENTHALPY_NO;
         else if (enthalpy == "explicit") c.enthalpy_flow = FV_ENTHALPY_EXPLICIT;
         else if (enthalpy == "implicit")
-            throw Fail("#Flag_for_enthalpy_flow_solution implicit: the explicit diffusion stage takes no or explicit");
+            throw Fail("#Flag_for_enthalpy_flow_solution implicit: the diffusion stage takes no or explicit");
         else throw Fail("Unknown flag for enthalpy flow calculation.");
         if (molMass != "on" && molMass != "off" && molMass != "yes" && molMass != "no")
             throw Fail("Unknown flag for molar mass diffusion correction.");

@@ -182,6 +182,36 @@ def deck_cases():
     c.enthalpy_flow, c.molmass_diffusion, c.diffusion_timestep = "explicit", False, True
     c.t_end = _t_after(c, p, 6, 0.5)
     out.append(("vdw3_6x6x6_diffusion", c, p, 3, True, [{}], 0.0))
+    # the same stage with the Gauss-Seidel solver (implicit matrices, the averaged enthalpy flow)
+    c, p = cases.shock_tube_1d(n=60)
+    c.diffusion, c.mu, c.D, c.kappa, c.sle_solver = True, 1e-4, 1e-3, 1e-4, "GaussSeidel"
+    c.enthalpy_flow, c.molmass_diffusion, c.diffusion_timestep = "explicit", True, True
+    c.t_end = _t_after(c, p, 20, 0.4)
+    out.append(("tube60_diffusion_gs", c, p, 6, True, [{}], 0.0))
+    c3, p3 = cases.reacting_shear_3d(n=6, periodic=False)
+    c = Case(dims=2, n=(6, 6, 1), L=(1.0, 1.0, 1.0), species=c3.species, t_end=1.0, R_units="SI",
+             eos="vanDerWaals", limiter="vanLeer", name="vdw2d")
+    for k in ("tail", "point", "right", "left"):
+        c.bc[k] = PatchBC.uniform("slip", 3)
+    p = [a.reshape(6, 6, 6)[0].ravel() for a in p3]
+    c.diffusion, c.mu, c.D, c.kappa, c.sle_solver = True, 1e-5, 1e-5, 1e-3, "GaussSeidel"
+    c.enthalpy_flow, c.molmass_diffusion, c.diffusion_timestep = "explicit", False, True
+    c.t_end = _t_after(c, p, 8, 0.5)
+    out.append(("vdw3_6x6_diffusion_gs", c, p, 3, True, [{}], 0.0))
+    c, p = cases.rayleigh_taylor_2d(nx=8, ny=16, modes=2)
+    c.g_delta = (0.0, -0.05, 0.0)
+    c.diffusion, c.mu, c.D, c.kappa, c.sle_solver = True, 1e-3, 1e-3, 1e-3, "GaussSeidel"
+    c.enthalpy_flow, c.molmass_diffusion = "explicit", True
+    c.t_end = _t_after(c, p, 12, 0.5)
+    out.append(("rt8x16_gravity_diffusion_gs", c, p, 5, True, [{}], 0.0))
+    c, p = cases.reacting_shear_3d(n=6, periodic=False, precision="f64")
+    c.chemistry = "no"
+    for k in list(c.bc):
+        c.bc[k] = PatchBC.uniform("slip", 3)
+    c.diffusion, c.mu, c.D, c.kappa, c.sle_solver = True, 1e-5, 1e-5, 1e-3, "GaussSeidel"
+    c.enthalpy_flow, c.molmass_diffusion = "no", True
+    c.t_end = _t_after(c, p, 6, 0.5)
+    out.append(("vdw3_6x6x6_diffusion_gs", c, p, 3, True, [{}], 0.0))
     return out
 
 
@@ -200,6 +230,9 @@ SHIPPED = [
     ("rarefactions_100_cgs", "Rarefactions_CGS/Rarefactions_100_CGS"),
     ("noh_cgs_1000", "Noh_CGS/Noh_CGS_1000"),
     ("diffusion_1000", "Diffusion/Diffusion_1000"),
+    # Gauss-Seidel diffusion of a van der Waals mixture between fixed walls, 100 x 100; to
+    # t = 2e-3 (320 steps) instead of 2.0 (about 330,000)
+    ("poiseuille_100x100_short", "PoiseuilleFlow/PoiseuilleFlow_SI_100x100", "2E-3"),
 ]
 SHIPPED_ROOT = "/root/reference/tests/TestsTasks"
 
@@ -235,14 +268,30 @@ def _save(name, d, inputs, runs_main, rcs, tol, logs):
     print(f"deck_{name}: {len(runs_main)} run(s), exit {rcs}, outputs {[k.split('_')[-1] for k in outs]}")
 
 
+def _shorten(main_txt: str, t_end: str) -> str:
+    """main.txt with #Time_of_calculation replaced, line endings kept."""
+    i = main_txt.index(END_KEY)
+    j = main_txt.index("\n", i)
+    k = main_txt.index("\n", j + 1)
+    cr = "\r" if main_txt[k - 1] == "\r" else ""
+    return main_txt[:j + 1] + t_end + cr + main_txt[k:]
+
+
 def shipped(binary, only=None):
-    """Fixtures of the reference's own task decks, their set/ directories unchanged."""
-    for name, rel in SHIPPED:
+    """Fixtures of the reference's own task decks, their set/ directories unchanged (a long deck
+    with only its #Time_of_calculation shortened)."""
+    for name, rel, *t_end in SHIPPED:
         if only and name not in only:
             continue
         d = tempfile.mkdtemp(prefix="schemi_deck_")
         try:
             shutil.copytree(os.path.join(SHIPPED_ROOT, rel, "set"), os.path.join(d, "set"))
+            if t_end:
+                path = os.path.join(d, "set", "main.txt")
+                with open(path, newline="") as f:
+                    txt = f.read()
+                with open(path, "w", newline="") as f:
+                    f.write(_shorten(txt, t_end[0]))
             inputs = _files(d)
             main_txt = inputs[os.path.join("set", "main.txt")].decode()
             res = subprocess.run([binary], cwd=d, stdin=subprocess.DEVNULL, stdout=subprocess.PIPE,

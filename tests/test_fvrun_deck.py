@@ -96,7 +96,6 @@ def _edit(path, key, value):
 
 
 @pytest.mark.parametrize("file,key,value,message", [
-    ("main.txt", "#Diffusion_flag", "on", "the diffusion stage implements explicit"),
     ("main.txt", "#Turbulence_flag", "yes", "Turbulence"),
     ("main.txt", "#Approximation_order", "FourthOrder", "Unknown gas dynamics approximation order."),
     ("main.txt", "#TVD_limiter_type", "vanLeer3", "limiter"),
@@ -146,7 +145,7 @@ def test_print_config_diffusion(tmp_path):
 
 
 @pytest.mark.parametrize("file,key,value,message", [
-    ("main.txt", "#Type_of_SLE_solver_flag", "Jacobi", "the diffusion stage implements explicit"),
+    ("main.txt", "#Type_of_SLE_solver_flag", "Jacobi", "the diffusion stage implements explicit and GaussSeidel"),
     ("main.txt", "#Type_of_SLE_solver_flag", "LU", "Unknown or inappropriate matrix solver flag."),
     ("main.txt", "#Type_of_flow_solver", "HLL", "the diffusion stage runs with HLLC"),
     ("main.txt", "#Approximation_order", "SecondOrderRK", "the diffusion stage runs with SecondOrder"),

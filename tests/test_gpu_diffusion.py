@@ -1,4 +1,5 @@
-"""The diffusion stage on the GPU (Diffusion.cpp through fv_step / fv_run) against the FP64 oracle.
+"""The diffusion stage on the GPU (Diffusion.cpp through fv_step / fv_run), with the explicit and
+the Gauss-Seidel solvers, against the FP64 oracle.
 
 Both follow the reference's operation order in FP64 without contraction, so the device state,
 its temperature (the stage's own, not TFromUv of the energy), the CFL step and the source time
@@ -80,8 +81,23 @@ def _kh_periodic():
     return c, p
 
 
+def _gs(make):
+    """The same case with the Gauss-Seidel (implicit) solver."""
+    def f():
+        c, p = make()
+        c.sle_solver = "GaussSeidel"
+        return c, p
+    return f
+
+
 CASES = [
     ("tube_enthalpy_molmass", lambda: _tube(), 25),
+    ("tube_gs", _gs(lambda: _tube()), 25),
+    ("tube_gs_plain", _gs(lambda: _tube(enthalpy_flow="no", molmass_diffusion=False, reconstruction="linear",
+                                        diffusion_timestep=False)), 25),
+    ("vdw3_2d_gs", _gs(lambda: _vdw_box(2)), 10),
+    ("vdw3_3d_gs", _gs(lambda: _vdw_box(3)), 6),
+    ("rt_gravity_gs", _gs(_rt_gravity), 12),
     ("tube_linear_plain", lambda: _tube(enthalpy_flow="no", molmass_diffusion=False, reconstruction="linear",
                                         diffusion_timestep=False), 25),
     ("vdw3_2d", lambda: _vdw_box(2), 10),
@@ -131,13 +147,22 @@ def test_gpu_diffusion_kernel_count(fv):
     case, prim = _tube()
     g = fv.FVCase(case)
     assert g.kernels_per_step == 4 + 5  # the generic step's 4, the stage's 4, the finalize
+    case.sle_solver = "GaussSeidel"
+    g = fv.FVCase(case)
+    # step 4; prim, faces, matrices, 2 solves, concentrations, averaged enthalpy flow, matrices,
+    # 1 + 1 solves (1D: one momentum component), phase, source, finalize
+    assert g.kernels_per_step == 4 + 2 + 1 + 2 + 1 + 1 + 1 + 2 + 1 + 1 + 1
 
 
 def test_gpu_diffusion_refusals(fv):
     """Configurations outside the stage are refused at fv_create with initialisationError."""
-    for kw in ({"precision": "f32flux"}, {"order": "SecondOrderRK"}, {"flux": "HLL"}, {"sle_solver": "GaussSeidel"},
-               {"enthalpy_flow": "implicit"}):
+    for kw in ({"precision": "f32flux"}, {"order": "SecondOrderRK"}, {"flux": "HLL"}, {"enthalpy_flow": "implicit"}):
         case, _ = _tube(**kw)
         with pytest.raises(fv.FVError) as e:
             fv.FVCase(case)
         assert e.value.status == 11, kw
+    case, _ = _kh_periodic()
+    case.sle_solver = "GaussSeidel"
+    with pytest.raises(fv.FVError) as e:
+        fv.FVCase(case)
+    assert e.value.status == 11
