@@ -533,7 +533,7 @@ fv_status ensureScratch(fv_handle* h) {
         const size_t nf = (size_t)h->L.nfaces, st = (size_t)h->P.stride;
         diff::DiffParams& X = h->diff;
         FV_CUDA(h, cudaMalloc(&X.starV, sizeof(double) * 3 * nf));
-        FV_CUDA(h, cudaMalloc(&X.face, sizeof(double) * (2 * ns + 9) * nf));
+        FV_CUDA(h, cudaMalloc(&X.face, sizeof(double) * diff::faceSlotCount(ns) * nf));
         FV_CUDA(h, cudaMalloc(&X.cellPrim, sizeof(double) * (2 * ns + 5) * st));
         FV_CUDA(h, cudaMalloc(&X.stagePrim, sizeof(double) * (ns + 6) * st));
         FV_CUDA(h, cudaMalloc(&X.partMin, sizeof(double) * 2 * (size_t)diffusionBlocks(h->P)));

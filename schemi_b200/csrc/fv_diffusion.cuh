@@ -45,7 +45,7 @@ namespace diff {
 // face quantity slots: flowW_k, corr_k (k < N), enthalpy flow, velocity Laplacian flow (3),
 // deviatoric stress (3), temperature Laplacian flow, maximal coefficient; for the implicit
 // solver also the interpolated density and temperature
-template <int NS> __host__ __device__ constexpr int faceSlots() { return 2 * NS + 11; }
+template <int NS> __host__ __device__ constexpr int faceSlots() { return faceSlotCount(NS); }
 template <int NS> __device__ __forceinline__ int slotW(int k) { return k; }
 template <int NS> __device__ __forceinline__ int slotCorr(int k) { return NS + k; }
 template <int NS> __device__ __forceinline__ int slotEnt() { return 2 * NS; }
@@ -55,6 +55,7 @@ template <int NS> __device__ __forceinline__ int slotT() { return 2 * NS + 7; }
 template <int NS> __device__ __forceinline__ int slotMax() { return 2 * NS + 8; }
 template <int NS> __device__ __forceinline__ int slotRho() { return 2 * NS + 9; }
 template <int NS> __device__ __forceinline__ int slotTs() { return 2 * NS + 10; }
+static_assert(faceSlotCount(1) == 2 * 1 + 11 && faceSlotCount(4) == 2 * 4 + 11, "slots 0 .. 2N + 10");
 
 // ----------------------------------------------------------------------------- mixture functions
 // mixtureIdeal.cpp / mixtureVanDerWaals.cpp with idealFluid.cpp / vanDerWaalsFluid.cpp

@@ -24,7 +24,7 @@ struct DiffParams {
     double* starV;             // [3][faces] Riemann star velocity of the advection (replaced by
                                //    the interpolated cell velocity when interpV)
     double* cellPrim;          // [2N + 5][stride]: c_1..c_N, v_x, v_y, v_z, p, T, w_1..w_N
-    double* face;              // [2N + 9][faces] face quantities (see faceSlots)
+    double* face;              // [faceSlotCount(N)][faces] face quantities (see faceSlots)
     double* stagePrim;         // [N + 6][stride]: c_1..c_N, v, p, Uv, T after the stage
     double* partMin;           // [2][blocks] per-CTA minima of the enthalpy and diffusion limits
     // the implicit solver's matrices and solutions (null with the explicit solver); face slots s
@@ -42,6 +42,9 @@ struct DiffParams {
     double* work;              // [2][stride] Gauss-Seidel iterates
     double* cNew;              // [N + 3][stride] concentrations c_0..c_N, CCVNew, old energy
 };
+
+// face quantity slots per face (fv_diffusion.cuh: faceSlots<N>() is the same count)
+__host__ __device__ constexpr int faceSlotCount(int ns) { return 2 * ns + 11; }
 
 }  // namespace diff
 
