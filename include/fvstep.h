@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define FV_ABI_VERSION 6
+#define FV_ABI_VERSION 7
 #define FV_MAX_SPECIES 4
 
 typedef int fv_status;
@@ -143,9 +143,19 @@ enum fv_chem_solver {
 enum fv_sle_solver { FV_SLE_EXPLICIT = 0, FV_SLE_GAUSS_SEIDEL = 1 };
 
 /* Transport-coefficient model (transportCoefficients.txt #Transport_coefficient_model,
- * phaseInitialization.cpp:211-222); "constant": mu, D and kappa as given
- * (abstractTransportModel.cpp:52-187). */
-enum fv_transport { FV_TRANSPORT_CONSTANT = 0 };
+ * phaseInitialization.cpp:211-222, abstractTransportModel.cpp:37-80):
+ *   CONSTANT        "constant": mu, D and kappa as given (abstractTransportModel.cpp:82-187);
+ *   HARD_SPHERES    "hardSpheres": the constants plus the hard-sphere kinetic-theory values of
+ *                   each species (transport_diameter, sub_k.txt #Kinetic_diameter_(A)), mixed by
+ *                   Wilke's rule (hardSpheresTransportModel.cpp);
+ *   LENNARD_JONES   "LennardJones": the same with the collision integrals of the Lennard-Jones
+ *                   potential (transport_lj_eps, transport_lj_sigma: sub_k.txt
+ *                   #Lennard_Jones_eps/kB_(K), #Lennard_Jones_sigma_(A);
+ *                   LennardJonesTransportModel.cpp).
+ * The coefficients of a face follow from its interpolated temperature and concentrations and the
+ * Riemann star pressure; the cell viscosity of the viscous heating from the cell's
+ * (Diffusion.cpp:130-132,238-240,506). */
+enum fv_transport { FV_TRANSPORT_CONSTANT = 0, FV_TRANSPORT_HARD_SPHERES = 1, FV_TRANSPORT_LENNARD_JONES = 2 };
 
 /* transportCoefficients.txt #Flag_for_enthalpy_flow_solution (phaseInitialization.cpp:224-235). */
 enum fv_enthalpy_flow { FV_ENTHALPY_NO = 0, FV_ENTHALPY_EXPLICIT = 1, FV_ENTHALPY_IMPLICIT = 2 };
@@ -220,6 +230,10 @@ typedef struct fv_config {
                                  stage limits the next step, Diffusion.cpp:1036-1049) */
     double dt_coeff_source;   /* the flag's first coefficient (explicit enthalpy flow limit) */
     double dt_coeff_diffusion;  /* its second (diffusion limit) */
+    /* Species data of the transport models (ABI version 7). */
+    double transport_diameter[FV_MAX_SPECIES];  /* HARD_SPHERES: kinetic diameter (angstrom) */
+    double transport_lj_eps[FV_MAX_SPECIES];    /* LENNARD_JONES: eps / k_B (K) */
+    double transport_lj_sigma[FV_MAX_SPECIES];  /* LENNARD_JONES: sigma (angstrom) */
 } fv_config;
 
 /* Field indices of fv_download / fv_upload arrays (n_cells doubles each, x fastest).

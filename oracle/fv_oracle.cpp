@@ -586,6 +586,7 @@ struct fvo_case {
     // source time step the stage sets for the next step (mesh::timestepSource, reset by main's
     // CFL block, Schemi.cpp:829-833)
     std::vector<V3> starV;
+    std::vector<double> starP;  // the star pressure (starFields::p, HLLCSolver.cpp:400)
     double dtSource = kVeryBig;
     double dtSourceLast = kVeryBig;  // the limit the last CFL block took
     // the temperature a diffusion stage leaves (gasPhase.temperature = the stage's new T,
@@ -1228,8 +1229,11 @@ struct Flux {
 // HLLC (HLLCSolver.cpp:13-406) and HLL (HLLSolver.cpp:13-318) for one face; returns false
 // when no branch applies (NaN wave speeds).  starV (HLLC): the face velocity the solver hands
 // the diffusion stage (starValues.v, HLLCSolver.cpp:399): the side's velocity outside the star
-// region, the star momentum over the star density inside it.
-bool riemann(const fvo_case& cs, const FState& O, const FState& B, const V3& N, Flux& F, V3* starV = nullptr) {
+// region, the star momentum over the star density inside it.  starP: the pressure beside it
+// (starValues.p, :400): the side's pressure outside the star region, inside it pressureStar of
+// the star state (pressureStarClass.cpp:12-36).
+bool riemann(const fvo_case& cs, const FState& O, const FState& B, const V3& N, Flux& F, V3* starV = nullptr,
+             double* starP = nullptr) {
     const Mix& mx = cs.mix;
     const int NS = mx.N;
     const double csO = std::sqrt(mx.sqSonicSpeed(O.c, O.rho[0], O.Uv, O.p) + kTwoThirds * 0.0 * (1. + mx.dpdUv(O.c, O.Uv)));
@@ -1242,6 +1246,17 @@ bool riemann(const fvo_case& cs, const FState& O, const FState& B, const V3& N, 
     const V3 INe = v3(1 * N.x[0] + 0 * N.x[1] + 0 * N.x[2], 0 * N.x[0] + 1 * N.x[1] + 0 * N.x[2],
                       0 * N.x[0] + 0 * N.x[1] + 1 * N.x[2]);
     (void)IN;
+    // pressureStar: c_k = rho_k / M_k, Uv = E - 0.5 (m & m) / rho - rho k
+    auto pStar = [&](const double* rs, const V3& ms, double Es) {
+        const double kin = 0.5 * vdot(ms, ms) / rs[0];
+        const double Uv = Es - kin - 0.0;
+        double cst[FV_MAX_SPECIES + 1] = {};
+        for (int k = 1; k <= NS; ++k) {
+            cst[k] = rs[k] / mx.M[k - 1];
+            cst[0] += cst[k];
+        }
+        return mx.pFromUv(cst, Uv);
+    };
     if (cs.cfg.flux == FV_FLUX_HLLC) {
         const double Sc = ((B.p + tpN) - (O.p + tpO) + O.rho[0] * uO * (SO - uO) - B.rho[0] * uN * (SN - uN)) /
                           (O.rho[0] * (SO - uO) - B.rho[0] * (SN - uN));
@@ -1252,6 +1267,7 @@ bool riemann(const fvo_case& cs, const FState& O, const FState& B, const V3& N, 
             F.m = outer(vadd(vmul(O.m, uO), vmul(INe, O.p + tpO)), N);
             F.E = vmul(N, uO * (O.E + O.p + tpO));
             if (starV) *starV = O.v;
+            if (starP) *starP = O.p;
         } else if (Sc >= 0) {
             const double factor = SO - uO;
             const double den = 1 / (SO - Sc);
@@ -1263,6 +1279,7 @@ bool riemann(const fvo_case& cs, const FState& O, const FState& B, const V3& N, 
             F.m = outer(vadd(vadd(vmul(O.m, uO), vmul(INe, O.p + tpO)), vmul(vsub(ms, O.m), SO)), N);
             F.E = vmul(N, (O.E + O.p + tpO) * uO + SO * (Es - O.E));
             if (starV) *starV = vdiv(ms, rs[0]);
+            if (starP) *starP = pStar(rs, ms, Es);
         } else if (SN > 0) {
             const double factor = SN - uN;
             const double den = 1 / (SN - Sc);
@@ -1274,11 +1291,13 @@ bool riemann(const fvo_case& cs, const FState& O, const FState& B, const V3& N, 
             F.m = outer(vadd(vadd(vmul(B.m, uN), vmul(INe, B.p + tpN)), vmul(vsub(ms, B.m), SN)), N);
             F.E = vmul(N, (B.E + B.p + tpN) * uN + SN * (Es - B.E));
             if (starV) *starV = vdiv(ms, rs[0]);
+            if (starP) *starP = pStar(rs, ms, Es);
         } else if (SN <= 0) {
             for (int k = 0; k <= NS; ++k) F.rho[k] = vmul(vmul(N, uN), B.rho[k]);
             F.m = outer(vadd(vmul(B.m, uN), vmul(INe, B.p + tpN)), N);
             F.E = vmul(N, uN * (B.E + B.p + tpN));
             if (starV) *starV = B.v;
+            if (starP) *starP = B.p;
         } else {
             return false;
         }
@@ -1472,9 +1491,13 @@ int doStep(fvo_case& cs, double dt, bool hancock = true, bool third = false, boo
 
     // 4. fluxes
     std::vector<Flux> flux(nf);
-    if (cs.cfg.diffusion) cs.starV.assign(nf, v3(0, 0, 0));
+    if (cs.cfg.diffusion) {
+        cs.starV.assign(nf, v3(0, 0, 0));
+        cs.starP.assign(nf, 0.0);
+    }
     for (size_t f = 0; f < nf; ++f)
-        if (!riemann(cs, own[f], nei[f], cs.faces[f].N, flux[f], cs.cfg.diffusion ? &cs.starV[f] : nullptr)) {
+        if (!riemann(cs, own[f], nei[f], cs.faces[f].N, flux[f], cs.cfg.diffusion ? &cs.starV[f] : nullptr,
+                     cs.cfg.diffusion ? &cs.starP[f] : nullptr)) {
             cs.err = "Fatal error in Riemann solver.";
             return FV_ERR_RIEMANN;
         }
@@ -1712,7 +1735,8 @@ inline T9 tadd(const T9& a, const T9& b) {
 // 256-325) for one face and one direction: the Maxwell-Stefan system of the molar-fraction
 // gradients, the row of the least concentration replaced by sum N_k M_k J_k = 0, solved by the
 // pivoting Gauss elimination of transportCoefficients.hpp:413-456, scaled by M_k c_k.
-void dMaxwellStefan(int NS, const double* Nc, const double* M, double D, const double* gradXf, double* out) {
+void dMaxwellStefan(int NS, const double* Nc, const double* M, const double (*Dm)[FV_MAX_SPECIES],
+                    const double* gradXf, double* out) {
     double c[FV_MAX_SPECIES];
     for (int k = 1; k <= NS; ++k) c[k - 1] = Nc[k];
     double cmin = c[0];
@@ -1727,7 +1751,7 @@ void dMaxwellStefan(int NS, const double* Nc, const double* M, double D, const d
         if (k1 != replaceIndex) {
             for (int k2 = 1; k2 <= NS; ++k2) {
                 if (k1 == k2) continue;
-                const double Aij = Nc[k1] * Nc[k2] / (Nc[0] * Nc[0] * D);
+                const double Aij = Nc[k1] * Nc[k2] / (Nc[0] * Nc[0] * Dm[k1 - 1][k2 - 1]);
                 A[k1 - 1][k2 - 1] = -Aij;
                 A[k1 - 1][k1 - 1] += Aij;
             }
@@ -1858,6 +1882,138 @@ std::vector<double> dGaussSeidel(const SLE1& M, const std::vector<double>& start
     }
 }
 
+// ---------------------------------------------------------------- transport models
+// Molecular transport coefficients of one point from its temperature T, pressure p and
+// concentrations c[0..N] (c[0] the total): transportCoefficients::calculateCoefficients
+// (templates/transportCoefficients.hpp:124-133) over the model's calculateMu, calculateDm,
+// calculateDs and calculateKappa.
+struct Transport {
+    double mu = 0, kappa = 0;
+    double Dm[FV_MAX_SPECIES][FV_MAX_SPECIES] = {};  // binary coefficients (off the diagonal)
+    double Ds[FV_MAX_SPECIES] = {};                  // coefficient of each species in the mixture
+};
+
+// Collision integrals of the Lennard-Jones potential at the reduced temperature Ts
+// (LennardJonesTransportModel.cpp:10-29): Omega(2,2) for mu and kappa, Omega(1,1) for D.
+double ljOmegaMuKappa(double Ts) {
+    constexpr double Ac = 1.16145, Bc = 0.14874, Cc = 0.52487, Dc = 0.77320, Ec = 2.16178, Fc = 2.4378;
+    return Ac * std::pow(Ts, -Bc) + Cc * std::exp(-Dc * Ts) + Ec * std::exp(-Fc * Ts);
+}
+double ljOmegaD(double Ts) {
+    constexpr double Ac = 1.06036, Bc = 0.1561, Cc = 0.19300, Dc = 0.47635, Ec = 1.03587, Fc = 1.52996,
+                     Gc = 1.76474, Hc = 3.89411;
+    return Ac * std::pow(Ts, -Bc) + Cc * std::exp(-Dc * Ts) + Ec * std::exp(-Fc * Ts) + Gc * std::exp(-Hc * Ts);
+}
+
+// Kinetic-theory values of one species or pair (hardSpheresTransportModel.cpp:11-38 with
+// Omega = 1; LennardJonesTransportModel.cpp:31-60): M in kg/mol, sigma in angstrom, each added
+// to the model's constant.
+double ktMu(const fv_config& cf, double M, double T, double Omega, double sigma) {
+    const double v = 2.6693E-6 * std::sqrt(1E3) * std::sqrt(M * T) / Omega / (sigma * sigma);
+    return cf.mu_const + v;
+}
+double ktD(const fv_config& cf, double M, double T, double p, double Omega, double sigma) {
+    const double v = 2.6280E-7 / std::sqrt(1E3) / Omega * std::sqrt(T * T * T / M) / (p / 101325. * (sigma * sigma));
+    return cf.D_const + v;
+}
+double ktKappa(const fv_config& cf, double M, double T, double Omega, double sigma) {
+    const double v = 4.184 * 1.9891E-2 / std::sqrt(1E3) * std::sqrt(T / M) / Omega / (sigma * sigma);
+    return cf.kappa_const + v;
+}
+// the hard-sphere forms carry no Omega: the same expressions without the division
+double hsMu(const fv_config& cf, double M, double T, double sigma) {
+    const double v = 2.6693E-6 * std::sqrt(1E3) * std::sqrt(M * T) / (sigma * sigma);
+    return cf.mu_const + v;
+}
+double hsD(const fv_config& cf, double M, double T, double p, double sigma) {
+    const double v = 2.6280E-7 / std::sqrt(1E3) * std::sqrt(T * T * T / M) / (p / 101325. * (sigma * sigma));
+    return cf.D_const + v;
+}
+double hsKappa(const fv_config& cf, double M, double T, double sigma) {
+    const double v = 4.184 * 1.9891E-2 / std::sqrt(1E3) * std::sqrt(T / M) / (sigma * sigma);
+    return cf.kappa_const + v;
+}
+
+// Wilke's mixing rule of the species' values q_k (hardSpheresTransportModel.cpp:55-77 for mu,
+// :189-210 for kappa with the factor 0.85 on Phi)
+double wilke(int N, const double* x, const double* q, const double* M, double phiScale) {
+    double Phi[FV_MAX_SPECIES][FV_MAX_SPECIES];
+    for (int k1 = 0; k1 < N; ++k1)
+        for (int k2 = 0; k2 < N; ++k2) {
+            const double num = 1 + std::sqrt(q[k1] / q[k2]) * std::sqrt(std::sqrt(M[k2] / M[k1]));
+            const double dem = 8 * (1 + M[k1] / M[k2]);
+            Phi[k1][k2] = phiScale == 1.0 ? num * num / std::sqrt(dem) : phiScale * num * num / std::sqrt(dem);
+        }
+    double mix = 0;
+    for (int k1 = 0; k1 < N; ++k1) {
+        double Phi_k1 = 0;
+        for (int k2 = 0; k2 < N; ++k2) Phi_k1 += x[k2] * Phi[k1][k2];
+        mix += x[k1] * q[k1] / Phi_k1;
+    }
+    return mix;
+}
+
+// The coefficients of one point.  surface = true: a face's, whose Ds guards the inverse sum with
+// the stabilizator (hardSpheresTransportModel.cpp:360-388); the cells' Ds (:133-170) is not used
+// by the stage and is not formed.
+void transportPoint(const fv_config& cf, const Mix& mx, double T, double p, const double* c, bool surface,
+                    Transport& out) {
+    const int N = mx.N;
+    out = Transport();
+    if (cf.transport == FV_TRANSPORT_CONSTANT) {  // abstractTransportModel.cpp:82-187
+        out.mu = cf.mu_const;
+        out.kappa = cf.kappa_const;
+        for (int k1 = 0; k1 < N; ++k1) {
+            out.Ds[k1] = cf.D_const;
+            for (int k2 = 0; k2 < N; ++k2)
+                if (k1 != k2) out.Dm[k1][k2] = cf.D_const;
+        }
+        return;
+    }
+    const bool lj = cf.transport == FV_TRANSPORT_LENNARD_JONES;
+    double x[FV_MAX_SPECIES] = {}, muk[FV_MAX_SPECIES] = {}, kk[FV_MAX_SPECIES] = {};
+    for (int k = 0; k < N; ++k) x[k] = c[k + 1] / c[0];
+    for (int k = 0; k < N; ++k) {
+        if (lj) {
+            const double Om = ljOmegaMuKappa(T / cf.transport_lj_eps[k]);
+            muk[k] = ktMu(cf, mx.M[k], T, Om, cf.transport_lj_sigma[k]);
+            kk[k] = ktKappa(cf, mx.M[k], T, Om, cf.transport_lj_sigma[k]);
+        } else {
+            muk[k] = hsMu(cf, mx.M[k], T, cf.transport_diameter[k]);
+            kk[k] = hsKappa(cf, mx.M[k], T, cf.transport_diameter[k]);
+        }
+    }
+    out.mu = wilke(N, x, muk, mx.M, 1.0);
+    out.kappa = wilke(N, x, kk, mx.M, 0.85);
+    for (int k1 = 0; k1 < N; ++k1)
+        for (int k2 = 0; k2 < N; ++k2) {
+            if (k1 == k2) continue;
+            const double M12 = 2 * mx.M[k1] * mx.M[k2] / (mx.M[k1] + mx.M[k2]);
+            if (lj) {
+                const double Om = ljOmegaD(T / std::sqrt(cf.transport_lj_eps[k1] * cf.transport_lj_eps[k2]));
+                const double s12 = 0.5 * (cf.transport_lj_sigma[k1] + cf.transport_lj_sigma[k2]);
+                out.Dm[k1][k2] = ktD(cf, M12, T, p, Om, s12);
+            } else {
+                const double d12 = 0.5 * (cf.transport_diameter[k1] + cf.transport_diameter[k2]);
+                out.Dm[k1][k2] = hsD(cf, M12, T, p, d12);
+            }
+        }
+    if (!surface) return;
+    for (int k1 = 0; k1 < N; ++k1) {
+        double rDk = 0;
+        for (int k2 = 0; k2 < N; ++k2) {
+            if (k1 == k2) continue;
+            rDk += x[k2] / out.Dm[k1][k2];
+        }
+        if (rDk >= kStab) {
+            rDk *= 1.0 / (1.0 - x[k1] + kStab);
+            out.Ds[k1] = 1 / rDk;
+        } else {
+            out.Ds[k1] = kStab;
+        }
+    }
+}
+
 int diffusionStage(fvo_case& cs, double dt) {
     const Mix& mx = cs.mix;
     const int NS = cs.N;
@@ -1883,7 +2039,6 @@ int diffusionStage(fvo_case& cs, double dt) {
         for (int k = 0; k < NS; ++k) w[k][i] /= sum;
     }
     const std::vector<V3>& v = cs.v;
-    const double mu = cf.mu_const, Dc = cf.D_const, kappa = cf.kappa_const;
 
     // Diffusion.cpp:136-176
     std::vector<double> nonIdOld(nc), CVOld(nc), CvM(nc), CCVOld(nc), NonIdRho(nc);
@@ -1979,6 +2134,24 @@ int diffusionStage(fvo_case& cs, double dt) {
     }
     std::vector<double> surfaceT;
     dInterp(cs, T, [&](size_t f) { return dBoundaryT(cs, cs.faces[f].own, cs.faces[f].patch, false, bad); }, surfaceT);
+
+    // transport coefficients: the cells' of the phase (its viscosity enters the viscous heating)
+    // and the faces' of the interpolated temperature and concentrations and the star pressure
+    // (Diffusion.cpp:130-132,238-240)
+    std::vector<double> muC(nc);
+    for (long long i = 0; i < nc; ++i) {
+        double cc[FV_MAX_SPECIES + 1];
+        conc(i, cc);
+        Transport t;
+        transportPoint(cf, mx, T[i], cs.p[i], cc, false, t);
+        muC[i] = t.mu;
+    }
+    std::vector<Transport> trF(nf);
+    for (size_t f = 0; f < nf; ++f) {
+        double Nc[FV_MAX_SPECIES + 1];
+        for (int k = 0; k <= NS; ++k) Nc[k] = sc[k][f];
+        transportPoint(cf, mx, surfaceT[f], cs.starP[f], Nc, true, trF[f]);
+    }
     std::vector<T9> strainVol(nc), strainSurf1(nf);
     for (long long i = 0; i < nc; ++i) {
         strainVol[i] = tadd(gradV[i], ttrans(gradV[i]));
@@ -1994,7 +2167,7 @@ int diffusionStage(fvo_case& cs, double dt) {
     // effective coefficients without turbulence (transportCoefficients.hpp:222-232)
     std::vector<std::vector<double>> rhoD(NS, std::vector<double>(nf));
     for (int k = 0; k < NS; ++k)
-        for (size_t f = 0; f < nf; ++f) rhoD[k][f] = surfaceRho[f] * Dc;
+        for (size_t f = 0; f < nf; ++f) rhoD[k][f] = surfaceRho[f] * trF[f].Ds[k];
 
     // mass-fraction matrices (Diffusion.cpp:321-339; SLEMatrix.cpp:2054-2078 explicit,
     // :410-546 implicit)
@@ -2054,7 +2227,7 @@ int diffusionStage(fvo_case& cs, double dt) {
                     for (int d = 0; d < 3; ++d) {
                         double g[FV_MAX_SPECIES], out[FV_MAX_SPECIES];
                         for (int k = 0; k < NS; ++k) g[k] = gradX[k][f].x[d];
-                        dMaxwellStefan(NS, Nc, mx.M, Dc, g, out);
+                        dMaxwellStefan(NS, Nc, mx.M, trF[f].Dm, g, out);
                         for (int k = 0; k < NS; ++k) DFlux[k][f].x[d] = out[k];
                     }
                 }
@@ -2156,7 +2329,7 @@ int diffusionStage(fvo_case& cs, double dt) {
                 for (int d = 0; d < 3; ++d) {
                     double g[FV_MAX_SPECIES], out[FV_MAX_SPECIES];
                     for (int k = 0; k < NS; ++k) g[k] = gradXN[k][f].x[d];
-                    dMaxwellStefan(NS, Nc, mx.M, Dc, g, out);
+                    dMaxwellStefan(NS, Nc, mx.M, trF[f].Dm, g, out);
                     for (int k = 0; k < NS; ++k) DFluxN[k][f].x[d] = out[k];
                 }
             }
@@ -2181,7 +2354,8 @@ int diffusionStage(fvo_case& cs, double dt) {
         for (int d = 0; d < 3; ++d) {
             std::vector<double> rOld(nc);
             for (long long i = 0; i < nc; ++i) rOld[i] = oldV[i].x[d];
-            std::vector<double> muF(nf, mu);
+            std::vector<double> muF(nf);
+            for (size_t f = 0; f < nf; ++f) muF[f] = trF[f].mu;
             dLaplacian(cs, [&, d](long long i, int fi) {
                 return bcCellV(cs, v[i], cs.faces[fi].patch, cs.faces[fi].N, bad).x[d];
             }, rOld, cs.rho[0], muF, dt, MV[d]);
@@ -2189,7 +2363,7 @@ int diffusionStage(fvo_case& cs, double dt) {
         }
     } else {
         std::vector<T9> flow(nf);
-        for (size_t f = 0; f < nf; ++f) flow[f] = tmul(tmul(gradVs[f], mu), -1.);
+        for (size_t f = 0; f < nf; ++f) flow[f] = tmul(tmul(gradVs[f], trF[f].mu), -1.);
         std::vector<V3> div;
         dDivT(cs, flow, div);
         for (long long i = 0; i < nc; ++i)
@@ -2200,7 +2374,8 @@ int diffusionStage(fvo_case& cs, double dt) {
     {
         auto ghostT = [&](size_t f) { return dBoundaryT(cs, cs.faces[f].own, cs.faces[f].patch, true, bad); };
         if (gs) {
-            std::vector<double> kF(nf, kappa);
+            std::vector<double> kF(nf);
+            for (size_t f = 0; f < nf; ++f) kF[f] = trF[f].kappa;
             dLaplacian(cs, [&](long long, int fi) { return ghostT(fi); }, oldEnergy, CCVNew, kF, dt, MT);
             diagT = MT.diag;
             freeT = MT.free;
@@ -2208,7 +2383,7 @@ int diffusionStage(fvo_case& cs, double dt) {
             std::vector<V3> gT;
             dSurfGrad(cs, T, ghostT, gT);
             std::vector<V3> flow(nf);
-            for (size_t f = 0; f < nf; ++f) flow[f] = vmul(vmul(gT[f], kappa), -1.);
+            for (size_t f = 0; f < nf; ++f) flow[f] = vmul(vmul(gT[f], trF[f].kappa), -1.);
             std::vector<double> div;
             dDivV(cs, flow, div);
             for (long long i = 0; i < nc; ++i) freeT[i] -= div[i];
@@ -2217,7 +2392,7 @@ int diffusionStage(fvo_case& cs, double dt) {
     // explicit deviatoric viscous stress on the velocity (Diffusion.cpp:503-506,600-605)
     {
         std::vector<T9> dev1(nf);
-        for (size_t f = 0; f < nf; ++f) dev1[f] = tmul(strainSurf1[f], mu);
+        for (size_t f = 0; f < nf; ++f) dev1[f] = tmul(strainSurf1[f], trF[f].mu);
         std::vector<V3> div;
         dDivT(cs, dev1, div);
         for (long long i = 0; i < nc; ++i)
@@ -2246,7 +2421,7 @@ int diffusionStage(fvo_case& cs, double dt) {
         }
     }
     for (long long i = 0; i < nc; ++i) {  // viscous heating: devPhysVisc && gradV
-        const T9 dev = tmul(strainVol[i], mu);
+        const T9 dev = tmul(strainVol[i], muC[i]);
         double dd = 0;
         for (int q = 0; q < 9; ++q) dd += dev.x[q] * gradV[i].x[q];
         freeT[i] += dd;
@@ -2298,7 +2473,11 @@ int diffusionStage(fvo_case& cs, double dt) {
     }
     if (cf.diffusion_timestep) {  // Diffusion.cpp:1036-1049
         std::vector<double> maxVal(nf);
-        for (size_t f = 0; f < nf; ++f) maxVal[f] = std::max(std::max(kappa, surfaceRho[f] * Dc), mu);
+        for (size_t f = 0; f < nf; ++f) {  // effectiveTransportCoefficients::maxValue (:172-184)
+            double Dmax = trF[f].Ds[0];
+            for (int k = 1; k < NS; ++k) Dmax = std::max(Dmax, trF[f].Ds[k]);
+            maxVal[f] = std::max(std::max(trF[f].kappa, surfaceRho[f] * Dmax), trF[f].mu);
+        }
         double mn = std::numeric_limits<double>::infinity();
         for (long long i = 0; i < nc; ++i) {
             const Cell& c = cs.cells[i];
@@ -2636,7 +2815,9 @@ int chemistryStep(fvo_case& cs, double dt) {
         for (int k = 0; k <= N; ++k) q.c[k] = cs.c[k][i];
         for (int k = 0; k < N; ++k) q.dens[k] = cs.rho[k + 1][i];
         q.Uv = cs.Uv[i];
-        q.T = mx.TFromUv(q.c, q.Uv);
+        // the phase's temperature: the diffusion stage's when it ran (secondOrderStepSolver.cpp:
+        // 69-91), else TFromUv of the advected energy
+        q.T = cs.Tvalid ? cs.Tstate[i] : mx.TFromUv(q.c, q.Uv);
     }
     for (int pass = 0; pass < 2; ++pass) {
         long long subIt = 1;
@@ -2665,6 +2846,7 @@ int chemistryStep(fvo_case& cs, double dt) {
         for (int k = 0; k <= N; ++k) cc[k] = cs.c[k][i];
         cs.p[i] = mx.pFromUv(cc, cs.Uv[i]);
     }
+    cs.Tvalid = false;  // bunchOfFields::average: T = TFromUv (bunchOfFields.hpp:197-198)
     return FV_OK;
 }
 
@@ -2718,8 +2900,21 @@ bool validate(const fv_config& cf, std::string& err) {
             err = "the diffusion stage runs with the explicit and Gauss-Seidel solvers";
             return false;
         }
-        if (cf.transport != FV_TRANSPORT_CONSTANT) { err = "the diffusion stage runs with constant transport coefficients"; return false; }
-        if (cf.chemistry != FV_CHEM_NONE) { err = "the diffusion stage runs without chemistry"; return false; }
+        if (cf.transport < FV_TRANSPORT_CONSTANT || cf.transport > FV_TRANSPORT_LENNARD_JONES) {
+            err = "unknown transport model";
+            return false;
+        }
+        for (int k = 0; k < cf.n_species; ++k) {
+            if (cf.transport == FV_TRANSPORT_HARD_SPHERES && !(cf.transport_diameter[k] > 0)) {
+                err = "hard-sphere diameters must be positive";
+                return false;
+            }
+            if (cf.transport == FV_TRANSPORT_LENNARD_JONES &&
+                !(cf.transport_lj_eps[k] > 0 && cf.transport_lj_sigma[k] > 0)) {
+                err = "Lennard-Jones parameters must be positive";
+                return false;
+            }
+        }
         if (cf.enthalpy_flow < FV_ENTHALPY_NO || cf.enthalpy_flow > FV_ENTHALPY_EXPLICIT) {
             err = "the diffusion stage takes no or explicit enthalpy flow";
             return false;

@@ -38,7 +38,7 @@ CHEM_SOLVERS = {"Gauss-Seidel": 0, "Jacobi": 1, "GaussElimination": 2, "conjugat
 # #Approximation_order values with a GPU step (abstractStepSolver.cpp:56-146)
 ORDERS = {"SecondOrder": 0, "SecondOrderRK": 1, "ThirdOrder": 2, "ThirdOrderCada": 3}
 SLE_SOLVERS = {"explicit": 0, "GaussSeidel": 1}
-TRANSPORT_MODELS = {"constant": 0}
+TRANSPORT_MODELS = {"constant": 0, "hardSpheres": 1, "LennardJones": 2}
 ENTHALPY_FLOWS = {"no": 0, "explicit": 1, "implicit": 2}
 
 # patch order of the task files: #Tail, #Point, #Bottom, #Right, #Left, #Top
@@ -110,6 +110,9 @@ class fv_config_t(ctypes.Structure):
         ("diffusion_timestep", ctypes.c_int),
         ("dt_coeff_source", ctypes.c_double),
         ("dt_coeff_diffusion", ctypes.c_double),
+        ("transport_diameter", ctypes.c_double * MAX_SPECIES),
+        ("transport_lj_eps", ctypes.c_double * MAX_SPECIES),
+        ("transport_lj_sigma", ctypes.c_double * MAX_SPECIES),
     ]
 
 
@@ -125,6 +128,11 @@ class Species:
     gamma: float = 1.4
     lj_eps: float = 0.0  # Kataoka (set/KataokaVanDerWaalsFluidData.txt)
     lj_sigma: float = 0.0
+    # transport models (sub_k.txt #Kinetic_diameter_(A), #Lennard_Jones_eps/kB_(K),
+    # #Lennard_Jones_sigma_(A))
+    diameter: float = 1.0
+    tr_eps: float = 1.0
+    tr_sigma: float = 1.0
 
 
 @dataclass
@@ -253,6 +261,8 @@ class Case:
             c.M[k], c.Cv[k], c.Tc[k], c.Pc[k] = s.M, s.Cv, s.Tc, s.Pc
             c.stiff_p0[k], c.stiff_gamma[k] = s.p0, s.gamma
             c.lj_eps[k], c.lj_sigma[k] = s.lj_eps, s.lj_sigma
+            c.transport_diameter[k] = s.diameter
+            c.transport_lj_eps[k], c.transport_lj_sigma[k] = s.tr_eps, s.tr_sigma
         c.kataoka_b_critical = int(self.kataoka_b[0] == "critical")
         c.kataoka_b_coeff = float(self.kataoka_b[1])
         c.diffusion = int(self.diffusion)

@@ -471,7 +471,17 @@ cudaError_t enqueueStep(fv_handle* h, int from) {
         e = launchDiffusion(h->cfg.n_species, h->cfg.eos, h->cfg.dims, h->P, h->L, h->diff, h->U[from ^ 1], h->ck,
                             h->blockMax, h->stream);
         if (e != cudaSuccess) return e;
-        k_finalize<<<1, 1024, 0, h->stream>>>(h->P, h->ck, h->blockMax, diffusionBlocks(h->P));
+        int blocks = diffusionBlocks(h->P);
+        if (h->cfg.chemistry != FV_CHEM_NONE) {
+            // then the chemistry of the phase the stage left (secondOrderStepSolver.cpp:87-91)
+            chem::ChemParams C = h->chem;
+            C.stage = h->diff.stagePrim;
+            e = launchChemistry(h->cfg.n_species, h->cfg.eos, h->cfg.dims, h->P, C, h->U[from ^ 1], h->ck,
+                                h->blockMax, h->stream);
+            if (e != cudaSuccess) return e;
+            blocks = chemistryBlocks(h->P);
+        }
+        k_finalize<<<1, 1024, 0, h->stream>>>(h->P, h->ck, h->blockMax, blocks);
         return cudaGetLastError();
     }
     if (h->cfg.chemistry == FV_CHEM_NONE) {
@@ -533,6 +543,7 @@ fv_status ensureScratch(fv_handle* h) {
         const size_t nf = (size_t)h->L.nfaces, st = (size_t)h->P.stride;
         diff::DiffParams& X = h->diff;
         FV_CUDA(h, cudaMalloc(&X.starV, sizeof(double) * 3 * nf));
+        FV_CUDA(h, cudaMalloc(&X.starP, sizeof(double) * nf));
         FV_CUDA(h, cudaMalloc(&X.face, sizeof(double) * diff::faceSlotCount(ns) * nf));
         FV_CUDA(h, cudaMalloc(&X.cellPrim, sizeof(double) * (2 * ns + 5) * st));
         FV_CUDA(h, cudaMalloc(&X.stagePrim, sizeof(double) * (ns + 6) * st));
@@ -540,7 +551,7 @@ fv_status ensureScratch(fv_handle* h) {
         if (X.gs) {
             FV_CUDA(h, cudaMalloc(&X.wDiag, sizeof(double) * ns * st));
             FV_CUDA(h, cudaMalloc(&X.wFree, sizeof(double) * ns * st));
-            FV_CUDA(h, cudaMalloc(&X.wOff, sizeof(double) * 6 * st));
+            FV_CUDA(h, cudaMalloc(&X.wOff, sizeof(double) * ns * 6 * st));
             FV_CUDA(h, cudaMalloc(&X.vDiag, sizeof(double) * st));
             FV_CUDA(h, cudaMalloc(&X.vFree, sizeof(double) * 3 * st));
             FV_CUDA(h, cudaMalloc(&X.vOff, sizeof(double) * 6 * st));
@@ -552,6 +563,7 @@ fv_status ensureScratch(fv_handle* h) {
             FV_CUDA(h, cudaMalloc(&X.cNew, sizeof(double) * (ns + 3) * st));
         }
         h->P.starV = X.starV;
+        h->P.starP = X.starP;
         h->P.stagePrim = X.stagePrim;
     }
     if (h->path == PATH_GENERIC && !h->FS) {
@@ -678,11 +690,18 @@ fv_status fv_create(const fv_config* cfg, fv_handle** out) {
     h->chem.Eb = cfg->chem_backward.E;
     h->chem.q = cfg->chem_q;
     h->chem.conc = nullptr;  // the multi-stage enqueues pass the stored concentrations
+    h->chem.stage = nullptr;  // the diffusion enqueue passes the stage's primitives
     if (cfg->diffusion) {
         diff::DiffParams& X = h->diff;
         X.mu = cfg->mu_const;
         X.D = cfg->D_const;
         X.kappa = cfg->kappa_const;
+        X.transport = cfg->transport;
+        for (int k = 0; k < FV_MAX_SPECIES; ++k) {
+            X.diam[k] = cfg->transport_diameter[k];
+            X.ljEps[k] = cfg->transport_lj_eps[k];
+            X.ljSig[k] = cfg->transport_lj_sigma[k];
+        }
         X.enthalpy = cfg->enthalpy_flow == FV_ENTHALPY_EXPLICIT;
         X.molmass = cfg->molmass_diffusion != 0;
         // gravity invalidates the star velocities (secondOrderStepSolver.cpp:71-73); the
@@ -791,7 +810,7 @@ void fv_destroy(fv_handle* h) {
     if (h->FS) cudaFree(h->FS);
     if (h->FL) cudaFree(h->FL);
     if (h->outBuf) cudaFree(h->outBuf);
-    for (double* q : {h->diff.starV, h->diff.face, h->diff.cellPrim, h->diff.stagePrim, h->diff.partMin, h->diff.wDiag,
+    for (double* q : {h->diff.starV, h->diff.starP, h->diff.face, h->diff.cellPrim, h->diff.stagePrim, h->diff.partMin, h->diff.wDiag,
                       h->diff.wFree, h->diff.wOff, h->diff.vDiag, h->diff.vFree, h->diff.vOff, h->diff.tDiag,
                       h->diff.tFree, h->diff.tOff, h->diff.sol, h->diff.work, h->diff.cNew})
         if (q) cudaFree(q);
@@ -1066,8 +1085,9 @@ long long fv_kernels_per_step(const fv_handle* h) {
     if (h->cfg.diffusion && h->diff.gs)
         // prim, faces, the mass-fraction matrices and N solves, concentrations, the averaged
         // enthalpy flow, velocity / temperature matrices and nmom + 1 solves, phase, source, finalize
-        return stage + 2 + 1 + h->cfg.n_species + 1 + (h->diff.enthalpy ? 1 : 0) + 1 + h->P.nmom + 1 + 1 + 1 + 1;
-    if (h->cfg.diffusion) return stage + 5;  // the stage's 4 kernels, finalize
+        return stage + 2 + 1 + h->cfg.n_species + 1 + (h->diff.enthalpy ? 1 : 0) + 1 + h->P.nmom + 1 + 1 + 1 + 1 +
+               chem;
+    if (h->cfg.diffusion) return stage + 5 + chem;  // the stage's 4 kernels, [chemistry,] finalize
     if (h->cfg.order == FV_ORDER_SECOND_RK) return 2 * stage + 2 + chem;  // two stages, average, finalize
     if (h->cfg.order == FV_ORDER_THIRD || h->cfg.order == FV_ORDER_THIRD_CADA)
         return 3 * stage + 3 + chem;  // three stages, two averages, finalize

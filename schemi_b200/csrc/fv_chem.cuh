@@ -445,6 +445,13 @@ __global__ void __launch_bounds__(256, 2) k_chemistry(const StepParams P, const 
             for (int k = 0; k <= N; ++k) q.c[k] = C.conc[k * st + i];
 #pragma unroll
             for (int k = 0; k <= N; ++k) cIn[k] = q.c[k];
+        } else if (C.stage) {
+            q.c[0] = 0;
+#pragma unroll
+            for (int k = 1; k <= N; ++k) {
+                q.c[k] = C.stage[(k - 1) * st + i];
+                q.c[0] += q.c[k];
+            }
         } else {
             q.c[0] = 0;
 #pragma unroll
@@ -455,13 +462,19 @@ __global__ void __launch_bounds__(256, 2) k_chemistry(const StepParams P, const 
         }
         double v[3];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) v[d] = m[d] / rho;
+        for (int d = 0; d < 3; ++d) v[d] = C.stage ? C.stage[(N + d) * st + i] : m[d] / rho;
         double v2 = 0;
         v2 += v[0] * v[0];
         v2 += v[1] * v[1];
         v2 += v[2] * v[2];
-        q.Uv = E - rho * v2 * 0.5 - 0.0;
-        q.T = TFromUv<N, EOS>(mx, q.c, q.Uv);
+        if (C.stage) {
+            // the stage's internal energy and temperature (Diffusion.cpp:965-1025)
+            q.Uv = C.stage[(N + 4) * st + i];
+            q.T = C.stage[(N + 5) * st + i];
+        } else {
+            q.Uv = E - rho * v2 * 0.5 - 0.0;
+            q.T = TFromUv<N, EOS>(mx, q.c, q.Uv);
+        }
 #pragma unroll
         for (int k = 0; k < N; ++k) q.dens[k] = rhoS[k];
         int status = integrate<N, EOS>(C, mx, dt, P.min_dt, rho, q);
@@ -506,6 +519,10 @@ __global__ void __launch_bounds__(256, 2) k_chemistry(const StepParams P, const 
     }
     const double bm = blockMaxReduce<double>(localMax, red);
     if (threadIdx.x == 0) blockMax[blockIdx.x] = bm;
+    // the averaged phase is the state's (bunchOfFields::average recomputes p and T from it): the
+    // next step and the download derive the primitives from the state again (nothing in this
+    // kernel reads the flag)
+    if (C.stage && blockIdx.x == 0 && threadIdx.x == 0) ck->stagePrim = 0;
 }
 
 }  // namespace chem

@@ -18,6 +18,10 @@ struct ChemParams {
     double* conc;     // concentrations c_0..c_N kept as state (stride apart) after a multi-stage
                       // average: read as the pass's input and replaced by their 0.5 average with
                       // the integrated ones; null: c_k = rho_k / M_k
+    const double* stage;  // primitives a diffusion stage left (c_1..c_N, v, p, Uv, T; stride
+                          // apart): the pass's input concentrations, velocity, internal energy and
+                          // temperature (the phase after Diffusion, secondOrderStepSolver.cpp:69-91);
+                          // null: from the state
 };
 
 }  // namespace chem

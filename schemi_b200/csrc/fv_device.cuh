@@ -658,14 +658,36 @@ struct FaceFlux {
     T E;
 };
 
+// pressureStar (pressureStarClass.cpp:12-36) of a star state: c_k = rho_k / M_k,
+// Uv = E - 0.5 (m & m) / rho - rho k, p = pFromUv(c, Uv)
+template <typename T, int NS, int EOS>
+__device__ __forceinline__ T starPressure(const MixParams& mp, const T* rs, const T* ms, T Es) {
+    T m2 = 0;
+    m2 += ms[0] * ms[0];
+    m2 += ms[1] * ms[1];
+    m2 += ms[2] * ms[2];
+    const T kin = T(0.5) * m2 / rs[0];
+    const T Uv = Es - kin - T(0);
+    T c[NS + 1];
+    c[0] = 0;
+#pragma unroll
+    for (int k = 1; k <= NS; ++k) {
+        c[k] = rs[k] / T(mp.M[k - 1]);
+        c[0] += c[k];
+    }
+    return Mixture<T, NS, EOS>::pFromUv(mp, c, Uv);
+}
+
 // HLLC (HLLCSolver.cpp:52-403) or HLL (HLLSolver.cpp:52-300); returns false when no branch
 // applies (NaN wave speeds), which the reference reports as RiemannSolverError.
-template <typename T, int NS>
+template <typename T, int NS, int EOS = -1>
 __device__ __forceinline__ bool riemann(int flux, int axis, int sign, const FaceState<T, NS>& O,
-                                        const FaceState<T, NS>& B, FaceFlux<T, NS>& F, T* sv = nullptr) {
+                                        const FaceState<T, NS>& B, FaceFlux<T, NS>& F, T* sv = nullptr,
+                                        T* sp = nullptr, const MixParams* mp = nullptr) {
     // sv (HLLC, not null): the face velocity the solver hands the diffusion stage (starValues.v,
     // HLLCSolver.cpp:399): the side's velocity outside the star region, the star momentum over
-    // the star density inside it
+    // the star density inside it; sp (EOS given, not null): the pressure beside it (starValues.p,
+    // :400), the side's outside the star region, pressureStar of the star state inside it
     const T sg = T(sign);
     const T uO = O.v[axis] * sg, uN = B.v[axis] * sg;
     const T SO = smin(uO - O.cs, uN - B.cs);
@@ -686,26 +708,35 @@ __device__ __forceinline__ bool riemann(int flux, int axis, int sign, const Face
 #pragma unroll
                 for (int d = 0; d < 3; ++d) sv[d] = O.v[d];
             }
+            if (sp) *sp = O.p;
         } else if (Sc >= T(0) || SN > T(0)) {
             // star flux of the side the contact leaves (owner when Sc >= 0): the reference's two
             // branches are the same expression on (O, uO, SO) or (B, uN, SN)
             auto star = [&](const T* rw, const T* mw, T Ew, T pw, T u, T S) {
                 const T factor = S - u;
                 const T den = T(1) / (S - Sc);
+                T rsa[NS + 1], msa[3];
 #pragma unroll
                 for (int k = 0; k <= NS; ++k) {
                     const T rs = rw[k] * factor * den;
+                    rsa[k] = rs;
                     F.rho[k] = rw[k] * u + S * (rs - rw[k]);
                 }
                 const T rs0 = rw[0] * factor * den;
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     const T ms = (mw[d] * factor - (d == axis ? sg : T(0)) * (pw + T(0) - PON)) * den;
+                    msa[d] = ms;
                     F.m[d] = mw[d] * u + (d == axis ? sg : T(0)) * (pw + T(0)) + (ms - mw[d]) * S;
                     if (sv) sv[d] = ms / rs0;
                 }
                 const T Es = (Ew * factor - (pw + T(0)) * u + PON * Sc) * den;
                 F.E = (Ew + pw + T(0)) * u + S * (Es - Ew);
+                if constexpr (EOS >= 0) {
+                    if (sp) *sp = starPressure<T, NS, EOS>(*mp, rsa, msa, Es);
+                }
+                (void)rsa;
+                (void)msa;
             };
             const bool own = Sc >= T(0);
             if constexpr (sizeof(T) == 8) {
@@ -732,6 +763,7 @@ __device__ __forceinline__ bool riemann(int flux, int axis, int sign, const Face
 #pragma unroll
                 for (int d = 0; d < 3; ++d) sv[d] = B.v[d];
             }
+            if (sp) *sp = B.p;
         } else {
             return false;
         }

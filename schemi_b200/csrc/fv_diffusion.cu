@@ -24,7 +24,7 @@ cudaError_t launchT(const StepParams& P, const GenericLayout& L, const diff::Dif
         const long long s = P.stride;
         diff::k_gs_wmat<NS, EOS, D><<<gc, kDiffThreads, 0, st>>>(P, L, X, U, ck);
         for (int k = 0; k < NS; ++k)
-            diff::k_gs_solve<D><<<1, diff::kGsThreads, 0, st>>>(P, X.wDiag + k * s, X.wFree + k * s, X.wOff,
+            diff::k_gs_solve<D><<<1, diff::kGsThreads, 0, st>>>(P, X.wDiag + k * s, X.wFree + k * s, X.wOff + k * 6 * s,
                                                                X.sol + k * s, X.work, X.maxIter, ck);
         diff::k_gs_post1<NS, EOS, D><<<gc, kDiffThreads, 0, st>>>(P, X, U, ck);
         if (X.enthalpy) diff::k_gs_afdif<NS, EOS, D><<<gf, kDiffThreads, 0, st>>>(P, L, X, ck);

@@ -44,7 +44,8 @@ namespace diff {
 
 // face quantity slots: flowW_k, corr_k (k < N), enthalpy flow, velocity Laplacian flow (3),
 // deviatoric stress (3), temperature Laplacian flow, maximal coefficient; for the implicit
-// solver also the interpolated density and temperature
+// solver also the interpolated density and temperature and the face's transport coefficients
+// mu, kappa and D_k
 template <int NS> __host__ __device__ constexpr int faceSlots() { return faceSlotCount(NS); }
 template <int NS> __device__ __forceinline__ int slotW(int k) { return k; }
 template <int NS> __device__ __forceinline__ int slotCorr(int k) { return NS + k; }
@@ -55,7 +56,10 @@ template <int NS> __device__ __forceinline__ int slotT() { return 2 * NS + 7; }
 template <int NS> __device__ __forceinline__ int slotMax() { return 2 * NS + 8; }
 template <int NS> __device__ __forceinline__ int slotRho() { return 2 * NS + 9; }
 template <int NS> __device__ __forceinline__ int slotTs() { return 2 * NS + 10; }
-static_assert(faceSlotCount(1) == 2 * 1 + 11 && faceSlotCount(4) == 2 * 4 + 11, "slots 0 .. 2N + 10");
+template <int NS> __device__ __forceinline__ int slotMu() { return 2 * NS + 11; }
+template <int NS> __device__ __forceinline__ int slotKappa() { return 2 * NS + 12; }
+template <int NS> __device__ __forceinline__ int slotDs(int k) { return 2 * NS + 13 + k; }
+static_assert(faceSlotCount(1) == 3 * 1 + 13 && faceSlotCount(4) == 3 * 4 + 13, "slots 0 .. 3N + 12");
 
 // ----------------------------------------------------------------------------- mixture functions
 // mixtureIdeal.cpp / mixtureVanDerWaals.cpp with idealFluid.cpp / vanDerWaalsFluid.cpp
@@ -104,6 +108,120 @@ __device__ __forceinline__ double hkT(const MixParams& mp, double ck, double T, 
     return ((mp.Cv[k] * T - a * ck) + (mp.R * T / (1 - ck * b) - a * ck)) / T;
 }
 
+// ----------------------------------------------------------------------------- transport models
+// transportCoefficients::calculateCoefficients (transportCoefficients.hpp:124-133) of one point
+// from its temperature T, pressure p and concentrations c[0..N]: the constants
+// (abstractTransportModel.cpp:82-187), the hard-sphere kinetic theory
+// (hardSpheresTransportModel.cpp) or the Lennard-Jones collision integrals
+// (LennardJonesTransportModel.cpp), each species' value added to the constant, mixed by Wilke's
+// rule.  The hard-sphere forms use only sqrt and division (correctly rounded here as in the
+// reference); the Lennard-Jones integrals call pow and exp, whose last bit may differ from the
+// host library's.
+__device__ __forceinline__ double ljOmegaMuKappa(double Ts) {
+    return 1.16145 * pow(Ts, -0.14874) + 0.52487 * exp(-0.77320 * Ts) + 2.16178 * exp(-2.4378 * Ts);
+}
+__device__ __forceinline__ double ljOmegaD(double Ts) {
+    return 1.06036 * pow(Ts, -0.1561) + 0.19300 * exp(-0.47635 * Ts) + 1.03587 * exp(-1.52996 * Ts) +
+           1.76474 * exp(-3.89411 * Ts);
+}
+// a species' viscosity and conductivity (hardSpheresTransportModel.cpp:11-38,
+// LennardJonesTransportModel.cpp:31-60)
+__device__ __forceinline__ void speciesMuKappa(const DiffParams& X, double M, double T, int k, double& mu,
+                                               double& kappa) {
+    if (X.transport == FV_TRANSPORT_LENNARD_JONES) {
+        const double Om = ljOmegaMuKappa(T / X.ljEps[k]);
+        const double s = X.ljSig[k];
+        mu = X.mu + 2.6693E-6 * sqrt(1E3) * sqrt(M * T) / Om / (s * s);
+        kappa = X.kappa + 4.184 * 1.9891E-2 / sqrt(1E3) * sqrt(T / M) / Om / (s * s);
+    } else {
+        const double s = X.diam[k];
+        mu = X.mu + 2.6693E-6 * sqrt(1E3) * sqrt(M * T) / (s * s);
+        kappa = X.kappa + 4.184 * 1.9891E-2 / sqrt(1E3) * sqrt(T / M) / (s * s);
+    }
+}
+// binary coefficient of the pair (k1, k2) (calculateDm)
+__device__ __forceinline__ double binaryD(const DiffParams& X, const double* M, int k1, int k2, double T, double p) {
+    const double M12 = 2 * M[k1] * M[k2] / (M[k1] + M[k2]);
+    if (X.transport == FV_TRANSPORT_LENNARD_JONES) {
+        const double Om = ljOmegaD(T / sqrt(X.ljEps[k1] * X.ljEps[k2]));
+        const double s = 0.5 * (X.ljSig[k1] + X.ljSig[k2]);
+        return X.D + 2.6280E-7 / sqrt(1E3) / Om * sqrt(T * T * T / M12) / (p / 101325. * (s * s));
+    }
+    const double s = 0.5 * (X.diam[k1] + X.diam[k2]);
+    return X.D + 2.6280E-7 / sqrt(1E3) * sqrt(T * T * T / M12) / (p / 101325. * (s * s));
+}
+// Wilke's mixing rule (hardSpheresTransportModel.cpp:55-77; kappa: 0.85 on Phi, :189-210)
+template <int NS>
+__device__ __forceinline__ double wilke(const double* x, const double* q, const double* M, bool kappa) {
+    double mix = 0;
+#pragma unroll
+    for (int k1 = 0; k1 < NS; ++k1) {
+        double Phi_k1 = 0;
+#pragma unroll
+        for (int k2 = 0; k2 < NS; ++k2) {
+            const double num = 1 + sqrt(q[k1] / q[k2]) * sqrt(sqrt(M[k2] / M[k1]));
+            const double dem = 8 * (1 + M[k1] / M[k2]);
+            const double Phi = kappa ? 0.85 * num * num / sqrt(dem) : num * num / sqrt(dem);
+            Phi_k1 += x[k2] * Phi;
+        }
+        mix += x[k1] * q[k1] / Phi_k1;
+    }
+    return mix;
+}
+// the viscosity and conductivity of a point
+template <int NS>
+__device__ __forceinline__ void pointMuKappa(const DiffParams& X, const double* M, double T, const double* c,
+                                             double& mu, double& kappa) {
+    if (X.transport == FV_TRANSPORT_CONSTANT) {
+        mu = X.mu;
+        kappa = X.kappa;
+        return;
+    }
+    double x[NS], muk[NS], kk[NS];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) {
+        x[k] = c[k + 1] / c[0];
+        speciesMuKappa(X, M[k], T, k, muk[k], kk[k]);
+    }
+    mu = wilke<NS>(x, muk, M, false);
+    kappa = wilke<NS>(x, kk, M, true);
+}
+// the binary matrix of a point (the diagonal unused)
+template <int NS>
+__device__ __forceinline__ void pointDm(const DiffParams& X, const double* M, double T, double p, double (*Dm)[NS]) {
+#pragma unroll
+    for (int k1 = 0; k1 < NS; ++k1)
+#pragma unroll
+        for (int k2 = 0; k2 < NS; ++k2)
+            Dm[k1][k2] = (k1 == k2) ? 0.0 : (X.transport == FV_TRANSPORT_CONSTANT ? X.D : binaryD(X, M, k1, k2, T, p));
+}
+// a face's coefficient of each species in the mixture (calculateDs, surface variant,
+// hardSpheresTransportModel.cpp:360-388: the inverse sum guarded by the stabilizator)
+template <int NS>
+__device__ __forceinline__ void faceDs(const DiffParams& X, const double* c, const double (*Dm)[NS], double* Ds) {
+    if (X.transport == FV_TRANSPORT_CONSTANT) {
+#pragma unroll
+        for (int k = 0; k < NS; ++k) Ds[k] = X.D;
+        return;
+    }
+    double x[NS];
+#pragma unroll
+    for (int k = 0; k < NS; ++k) x[k] = c[k + 1] / c[0];
+#pragma unroll
+    for (int k1 = 0; k1 < NS; ++k1) {
+        double rDk = 0;
+#pragma unroll
+        for (int k2 = 0; k2 < NS; ++k2)
+            if (k1 != k2) rDk += x[k2] / Dm[k1][k2];
+        if (rDk >= Num<double>::stab()) {
+            rDk *= 1.0 / (1.0 - x[k1] + Num<double>::stab());
+            Ds[k1] = 1 / rDk;
+        } else {
+            Ds[k1] = Num<double>::stab();
+        }
+    }
+}
+
 // calculatedTemperature (boundaryConditionValue.hpp:89-108, 326-345): the temperature of the
 // patch's concentrations and pressure, surface or cell variant
 template <int NS, int EOS>
@@ -127,8 +245,8 @@ __device__ __forceinline__ double boundaryT(const StepParams& P, int patch, cons
 // :413-456, with normalize, :544-550): the row of the least concentration replaced by
 // sum N_k M_k J_k = 0, the result scaled by M_k c_k.
 template <int NS>
-__device__ __forceinline__ void maxwellStefan(const double* Nc, const double* M, double D, const double* gX,
-                                              double* out) {
+__device__ __forceinline__ void maxwellStefan(const double* Nc, const double* M, const double (*Dm)[NS],
+                                              const double* gX, double* out) {
     double c[NS];
 #pragma unroll
     for (int k = 1; k <= NS; ++k) c[k - 1] = Nc[k];
@@ -151,7 +269,7 @@ __device__ __forceinline__ void maxwellStefan(const double* Nc, const double* M,
 #pragma unroll
             for (int k2 = 1; k2 <= NS; ++k2) {
                 if (k1 == k2) continue;
-                const double Aij = Nc[k1] * Nc[k2] / (Nc[0] * Nc[0] * D);
+                const double Aij = Nc[k1] * Nc[k2] / (Nc[0] * Nc[0] * Dm[k1 - 1][k2 - 1]);
                 A[k1 - 1][k2 - 1] = -Aij;
                 A[k1 - 1][k1 - 1] += Aij;
             }
@@ -383,7 +501,12 @@ __global__ void k_diff_faces(const StepParams P, const GenericLayout L, const Di
         }
     }
 
-    const double rhoD = sRho * X.D;
+    // the face's transport coefficients: its interpolated temperature and concentrations and the
+    // Riemann star pressure (Diffusion.cpp:238-240)
+    double muF, kappaF, DmF[NS][NS], DsF[NS];
+    pointMuKappa<NS>(X, P.mix.M, sT, sc, muF, kappaF);
+    pointDm<NS>(X, P.mix.M, sT, X.starP[f], DmF);
+    faceDs<NS>(X, sc, DmF, DsF);
     double* F = X.face;
     double flowW[NS];
 #pragma unroll
@@ -401,6 +524,7 @@ __global__ void k_diff_faces(const StepParams P, const GenericLayout L, const Di
             other = prim(NS + 5 + k, nb);
         }
         const double gW = sgrad(wO, other);
+        const double rhoD = sRho * DsF[k];  // effectiveTransportCoefficients::rhoD (:228-230)
         flowW[k] = gW * (-1 * rhoD);
         F[slotW<NS>(k) * nf + f] = flowW[k];
     }
@@ -426,7 +550,7 @@ __global__ void k_diff_faces(const StepParams P, const GenericLayout L, const Di
         }
         double DF[NS];
         if (NS > 1) {
-            maxwellStefan<NS>(sc, P.mix.M, X.D, gX, DF);
+            maxwellStefan<NS>(sc, P.mix.M, DmF, gX, DF);
         } else {
 #pragma unroll
             for (int k = 0; k < NS; ++k) DF[k] = 0;
@@ -464,7 +588,7 @@ __global__ void k_diff_faces(const StepParams P, const GenericLayout L, const Di
     for (int d = 0; d < 3; ++d) {
         qv[d] = (vOther[d] - vO[d]) / (boundary ? dmag : m2);
         // row d of (grad_s v mu (-1)) & n: column a
-        F[slotV<NS>(d) * nf + f] = qv[d] * dir[a] * X.mu * -1.;
+        F[slotV<NS>(d) * nf + f] = qv[d] * dir[a] * muF * -1.;
     }
     double divVs = 0;  // q & dir
     divVs += qv[0] * dir[0];
@@ -477,15 +601,25 @@ __global__ void k_diff_faces(const StepParams P, const GenericLayout L, const Di
     for (int d = 0; d < 3; ++d) {
         double e = qv[a] * dir[d];
         if (d == a) e -= lam;
-        F[slotDev<NS>(d) * nf + f] = e * X.mu;
+        F[slotDev<NS>(d) * nf + f] = e * muF;
     }
     // temperature: calculatedTemperature ghost
     const double Tother = boundary ? boundaryT<NS, EOS>(P, g.patch, cO, pO, true, bad) : TN;
-    F[slotT<NS>() * nf + f] = sgrad(TO, Tother) * X.kappa * -1.;
-    if (X.dtDiff) F[slotMax<NS>() * nf + f] = smax(smax(X.kappa, sRho * X.D), X.mu);
+    F[slotT<NS>() * nf + f] = sgrad(TO, Tother) * kappaF * -1.;
+    if (X.dtDiff) {
+        // effectiveTransportCoefficients::maxValue (transportCoefficients.hpp:172-184)
+        double Dmax = DsF[0];
+#pragma unroll
+        for (int k = 1; k < NS; ++k) Dmax = smax(Dmax, DsF[k]);
+        F[slotMax<NS>() * nf + f] = smax(smax(kappaF, sRho * Dmax), muF);
+    }
     if (X.gs) {
         F[slotRho<NS>() * nf + f] = sRho;
         F[slotTs<NS>() * nf + f] = sT;
+        F[slotMu<NS>() * nf + f] = muF;
+        F[slotKappa<NS>() * nf + f] = kappaF;
+#pragma unroll
+        for (int k = 0; k < NS; ++k) F[slotDs<NS>(k) * nf + f] = DsF[k];
     }
     if (X.interpV) {
         // star.v = linearInterpolate(velocity) (secondOrderStepSolver.cpp:71-73, or the
@@ -652,7 +786,10 @@ __global__ void k_diff_cells(const StepParams P, const GenericLayout L, const Di
             else diagT -= s / (T + Num<double>::stab());
         }
         {
-            // devPhysVisc && gradV with devPhysVisc = (gradV + gradV^T - 2/3 div I) mu
+            // devPhysVisc && gradV with devPhysVisc = (gradV + gradV^T - 2/3 div I) mu, mu the
+            // cell's (Diffusion.cpp:130-132,506)
+            double muC, kappaC;
+            pointMuKappa<NS>(X, P.mix.M, T, c, muC, kappaC);
             const double l = (2. / 3.) * divV;
             double dd = 0;
 #pragma unroll
@@ -661,7 +798,7 @@ __global__ void k_diff_cells(const StepParams P, const GenericLayout L, const Di
                 for (int q = 0; q < 3; ++q) {
                     double sv = gradV[3 * q + r] + gradV[3 * r + q];
                     if (r == q) sv -= l;
-                    dd += sv * X.mu * gradV[3 * r + q];
+                    dd += sv * muC * gradV[3 * r + q];
                 }
             freeT += dd;
         }

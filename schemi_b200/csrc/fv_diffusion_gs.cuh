@@ -68,8 +68,8 @@ template <int D> __device__ __forceinline__ void faceOrder(int* fa, int* fh) {
 }
 
 // ----------------------------------------------------------------------------- k_gs_wmat
-// the mass fractions' matrices (their coefficient rho D is the same for every species) and the
-// molar-mass correction distributed into them (Diffusion.cpp:321-339, 396-412)
+// the mass fractions' matrices (coefficient rho D_k of the face) and the molar-mass correction
+// distributed into them (Diffusion.cpp:321-339, 396-412)
 template <int NS, int EOS, int D>
 __global__ void k_gs_wmat(const StepParams P, const GenericLayout L, const DiffParams X, const double* __restrict__ U,
                           DevClock* __restrict__ ck) {
@@ -96,9 +96,10 @@ __global__ void k_gs_wmat(const StepParams P, const GenericLayout L, const DiffP
 #pragma unroll
     for (int k = 0; k < NS; ++k) w[k] = cp[(NS + 5 + k) * st + i];
     // the patch's concentrations as cell values (calculatedMassFraction's ghosts)
-    double diag = rho0 * rt, free[NS], divC[NS];
+    double diag[NS], free[NS], divC[NS];
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
+        diag[k] = rho0 * rt;
         free[k] = (w[k] * rho0) * rt;
         divC[k] = 0;
     }
@@ -110,25 +111,29 @@ __global__ void k_gs_wmat(const StepParams P, const GenericLayout L, const DiffP
     for (int s = 0; s < NFC; ++s) {
         const FaceCoef fc = faceCoef<D>(P, L, ijk, fa[s], fh[s], rc, V);
         const long long f = fc.g.f;
-        const double rhoD = F[slotRho<NS>() * nf + f] * X.D;
-        const double coef = rhoD / fc.m * fc.dot;
-        diag += coef;
-        if (fc.nb >= 0) {
-            X.wOff[s * st + i] = -rhoD / fc.m * fc.dot;
-        } else {
-            X.wOff[s * st + i] = 0;
-            double cB[NS + 1];
+        const double sRho = F[slotRho<NS>() * nf + f];
+        double cB[NS + 1], sum = 0;
+        if (fc.nb < 0) {
             cB[0] = 0;
 #pragma unroll
             for (int k = 1; k <= NS; ++k) {
                 cB[k] = cellGhostScalar<double, NS>(P, fc.g.patch, k - 1, c[k], bad);
                 cB[0] += cB[k];
             }
-            double sum = 0;
 #pragma unroll
             for (int q = 1; q <= NS; ++q) sum += cB[q] * P.mix.M[q - 1];
+        }
 #pragma unroll
-            for (int k = 0; k < NS; ++k) free[k] += coef * ((cB[k + 1] * P.mix.M[k]) / sum);
+        for (int k = 0; k < NS; ++k) {
+            const double rhoD = sRho * F[slotDs<NS>(k) * nf + f];
+            const double coef = rhoD / fc.m * fc.dot;
+            diag[k] += coef;
+            if (fc.nb >= 0) {
+                X.wOff[(k * 6 + s) * st + i] = -rhoD / fc.m * fc.dot;
+            } else {
+                X.wOff[(k * 6 + s) * st + i] = 0;
+                free[k] += coef * ((cB[k + 1] * P.mix.M[k]) / sum);
+            }
         }
         if (X.molmass) {
             const double nsg = fc.g.own ? double(fc.g.sign) : double(-fc.g.sign);
@@ -138,7 +143,7 @@ __global__ void k_gs_wmat(const StepParams P, const GenericLayout L, const DiffP
     }
 #pragma unroll
     for (int k = 0; k < NS; ++k) {
-        double dk = diag, fk = free[k];
+        double dk = diag[k], fk = free[k];
         if (X.molmass) {
             const double s = (divC[k] / V) * (-1.0);
             if (s >= 0.) fk += s;
@@ -388,8 +393,10 @@ __global__ void k_gs_afdif(const StepParams P, const GenericLayout L, const Diff
             }
             gX[k] = sgrad(xO, other);
         }
-        double DF[NS];
-        maxwellStefan<NS>(sc, P.mix.M, X.D, gX, DF);
+        // the face's binary coefficients of the first pass (they depend on T and p alone)
+        double Dm[NS][NS], DF[NS];
+        pointDm<NS>(X, P.mix.M, sT, X.starP[f], Dm);
+        maxwellStefan<NS>(sc, P.mix.M, Dm, gX, DF);
 #pragma unroll
         for (int k = 0; k < NS; ++k) corr[k] = DF[k] - flowW[k];
     }
@@ -453,12 +460,13 @@ __global__ void k_gs_vtmat(const StepParams P, const GenericLayout L, const Diff
             const int a = fa[s];
             const FaceCoef fc = faceCoef<D>(P, L, ijk, a, fh[s], rc, V);
             const long long f = fc.g.f;
-            const double coefV = X.mu / fc.m * fc.dot, coefT = X.kappa / fc.m * fc.dot;
+            const double muF = F[slotMu<NS>() * nf + f], kappaF = F[slotKappa<NS>() * nf + f];
+            const double coefV = muF / fc.m * fc.dot, coefT = kappaF / fc.m * fc.dot;
             vdiag += coefV;
             tdiag += coefT;
             if (fc.nb >= 0) {
-                X.vOff[s * st + i] = -X.mu / fc.m * fc.dot;
-                X.tOff[s * st + i] = -X.kappa / fc.m * fc.dot;
+                X.vOff[s * st + i] = -muF / fc.m * fc.dot;
+                X.tOff[s * st + i] = -kappaF / fc.m * fc.dot;
             } else {
                 X.vOff[s * st + i] = 0;
                 X.tOff[s * st + i] = 0;
@@ -498,6 +506,9 @@ __global__ void k_gs_vtmat(const StepParams P, const GenericLayout L, const Diff
             else tdiag -= s / (T + Num<double>::stab());
         }
         {
+            // the viscous heating with the cell's viscosity (Diffusion.cpp:130-132,506)
+            double muC, kappaC;
+            pointMuKappa<NS>(X, P.mix.M, T, c, muC, kappaC);
             const double l = (2. / 3.) * divV;
             double dd = 0;
 #pragma unroll
@@ -506,7 +517,7 @@ __global__ void k_gs_vtmat(const StepParams P, const GenericLayout L, const Diff
                 for (int q = 0; q < 3; ++q) {
                     double sv = gradV[3 * q + r] + gradV[3 * r + q];
                     if (r == q) sv -= l;
-                    dd += sv * X.mu * gradV[3 * r + q];
+                    dd += sv * muC * gradV[3 * r + q];
                 }
             tfree += dd;
         }

@@ -12,7 +12,12 @@ namespace diff {
 
 // Coefficients and buffers of the stage (allocated by the handle when cfg.diffusion is on).
 struct DiffParams {
-    double mu, D, kappa;       // constant transport coefficients
+    double mu, D, kappa;       // the transport model's constants (fv_config mu/D/kappa_const)
+    int transport;             // fv_transport
+    int pad0;
+    double diam[FV_MAX_SPECIES];   // HARD_SPHERES: kinetic diameters (angstrom)
+    double ljEps[FV_MAX_SPECIES];  // LENNARD_JONES: eps / k_B (K)
+    double ljSig[FV_MAX_SPECIES];  // LENNARD_JONES: sigma (angstrom)
     int enthalpy;              // 1: explicit enthalpy flow
     int molmass;               // 1: molar-mass diffusion correction
     int interpV;               // 1: cell velocity gradient from interpolated cell velocities
@@ -23,6 +28,7 @@ struct DiffParams {
     double coeffSource, coeffDiff;
     double* starV;             // [3][faces] Riemann star velocity of the advection (replaced by
                                //    the interpolated cell velocity when interpV)
+    double* starP;             // [faces] its star pressure (the face coefficients' pressure)
     double* cellPrim;          // [2N + 5][stride]: c_1..c_N, v_x, v_y, v_z, p, T, w_1..w_N
     double* face;              // [faceSlotCount(N)][faces] face quantities (see faceSlots)
     double* stagePrim;         // [N + 6][stride]: c_1..c_N, v, p, Uv, T after the stage
@@ -31,7 +37,7 @@ struct DiffParams {
     // in the cell's face order [x-, x+, y+, y-, z-, z+]
     double* wDiag;             // [N][stride] mass fractions: diagonal, free term
     double* wFree;
-    double* wOff;              // [6][stride] their off-diagonal coefficient per face slot (shared)
+    double* wOff;              // [N][6][stride] their off-diagonal coefficient per face slot
     double* vDiag;             // [stride] velocity: diagonal (shared by the components)
     double* vFree;             // [3][stride]
     double* vOff;              // [6][stride]
@@ -44,7 +50,7 @@ struct DiffParams {
 };
 
 // face quantity slots per face (fv_diffusion.cuh: faceSlots<N>() is the same count)
-__host__ __device__ constexpr int faceSlotCount(int ns) { return 2 * ns + 11; }
+__host__ __device__ constexpr int faceSlotCount(int ns) { return 3 * ns + 13; }
 
 }  // namespace diff
 

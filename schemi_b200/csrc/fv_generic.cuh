@@ -852,24 +852,26 @@ __global__ void k_fluxes(const StepParams P, const GenericLayout L, const T* __r
     const bool boundary = !P.periodic[a] && (fi == 0 || fi == n);
     FaceFlux<T, NS> F;
     bool ok;
-    T sv[3];
+    T sv[3], sp = T(0);
     T* svp = P.starV ? sv : nullptr;
+    T* spp = P.starP ? &sp : nullptr;
     if (boundary) {
         const int sign = fi == 0 ? -1 : 1;
         const int patch = a == 0 ? (fi == 0 ? FV_PATCH_TAIL : FV_PATCH_POINT)
                                  : a == 1 ? (fi == 0 ? FV_PATCH_RIGHT : FV_PATCH_LEFT)
                                           : (fi == 0 ? FV_PATCH_BOTTOM : FV_PATCH_TOP);
         ghostState<T, NS, EOS>(P.mix, P.bc, patch, a, sign, O, B);
-        ok = riemann<T, NS>(P.flux, a, sign, O, B, F, svp);
+        ok = riemann<T, NS, EOS>(P.flux, a, sign, O, B, F, svp, spp, &P.mix);
     } else {
         loadFace<T, NS>(FS, nf, 1, f, B);
-        ok = riemann<T, NS>(P.flux, a, 1, O, B, F, svp);
+        ok = riemann<T, NS, EOS>(P.flux, a, 1, O, B, F, svp, spp, &P.mix);
     }
     if (!ok) raise(ck, FV_ERR_RIEMANN);
     if (P.starV) {
 #pragma unroll
         for (int d = 0; d < 3; ++d) P.starV[d * nf + f] = double(sv[d]);
     }
+    if (P.starP) P.starP[f] = double(sp);
     int q = 0;
 #pragma unroll
     for (int k = 0; k <= NS; ++k) FL[(q++) * nf + f] = F.rho[k];

@@ -64,6 +64,8 @@ struct StepParams {
     int pad0;
     double* starV;          // not null: k_fluxes stores each face's Riemann star velocity here
                             // ([3][faces], HLLCSolver.cpp:399) for the diffusion stage
+    double* starP;          // not null: and its star pressure ([faces], :400), which the transport
+                            // models' face coefficients read
     const double* stagePrim;  // primitives a diffusion stage left (c_1..c_N, v, p, Uv, T; stride
                               // apart): the next step reads them when the clock's stagePrim is set
     MixParams mix;

@@ -32,8 +32,9 @@ inline bool fvValidateConfig(const fv_config& c, std::string& e) {
     }
     if (c.diffusion) {
         // the diffusion stage (Diffusion.cpp) this build runs: after the SecondOrder advection, HLLC
-        // star velocities, FP64, ideal or van der Waals, constant coefficients, the explicit
-        // solver, no or explicit enthalpy flow, no chemistry
+        // star states, FP64, ideal or van der Waals, the constant, hard-sphere or Lennard-Jones
+        // coefficients, the explicit or Gauss-Seidel solver, no or explicit enthalpy flow; a
+        // chemical mechanism follows the stage
         if (c.order != FV_ORDER_SECOND) { e = "the diffusion stage runs with the SecondOrder step"; return false; }
         if (c.flux != FV_FLUX_HLLC) { e = "the diffusion stage runs with the HLLC flux"; return false; }
         if (c.precision != FV_PREC_F64) { e = "the diffusion stage runs in FP64"; return false; }
@@ -41,7 +42,6 @@ inline bool fvValidateConfig(const fv_config& c, std::string& e) {
             e = "the diffusion stage runs with ideal and van der Waals mixtures";
             return false;
         }
-        if (c.chemistry != FV_CHEM_NONE) { e = "the diffusion stage runs without chemistry"; return false; }
         if (c.sle_solver != FV_SLE_EXPLICIT && c.sle_solver != FV_SLE_GAUSS_SEIDEL) {
             e = "the diffusion stage runs with the explicit and Gauss-Seidel solvers";
             return false;
@@ -55,9 +55,19 @@ inline bool fvValidateConfig(const fv_config& c, std::string& e) {
                 }
             if (c.sle_max_iter < 1) { e = "the Gauss-Seidel solver needs at least one iteration"; return false; }
         }
-        if (c.transport != FV_TRANSPORT_CONSTANT) {
-            e = "the diffusion stage runs with constant transport coefficients";
+        if (c.transport < FV_TRANSPORT_CONSTANT || c.transport > FV_TRANSPORT_LENNARD_JONES) {
+            e = "unknown transport model";
             return false;
+        }
+        for (int k = 0; k < c.n_species; ++k) {
+            if (c.transport == FV_TRANSPORT_HARD_SPHERES && !(c.transport_diameter[k] > 0)) {
+                e = "hard-sphere diameters must be positive";
+                return false;
+            }
+            if (c.transport == FV_TRANSPORT_LENNARD_JONES && !(c.transport_lj_eps[k] > 0 && c.transport_lj_sigma[k] > 0)) {
+                e = "Lennard-Jones parameters must be positive";
+                return false;
+            }
         }
         if (c.enthalpy_flow != FV_ENTHALPY_NO && c.enthalpy_flow != FV_ENTHALPY_EXPLICIT) {
             e = "the diffusion stage takes no or explicit enthalpy flow";

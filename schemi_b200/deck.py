@@ -230,9 +230,9 @@ def write_deck(case: Case, directory: str, prim: Sequence[np.ndarray], frequency
             "#Molar_isohoric_heat_capacity_(J/T/mol)", _f(sp.Cv),
             "#Critical_temperature_(K)", _f(sp.Tc),
             "#Critical_pressure_(Pa)", _f(sp.Pc),
-            "#Kinetic_diameter_(A)", "1",
-            "#Lennard_Jones_eps/kB_(K)", "1",
-            "#Lennard_Jones_sigma_(A)", "1",
+            "#Kinetic_diameter_(A)", _f(sp.diameter),
+            "#Lennard_Jones_eps/kB_(K)", _f(sp.tr_eps),
+            "#Lennard_Jones_sigma_(A)", _f(sp.tr_sigma),
             _bc_block(case, lambda pb, k=k: pb.conc[k], False),
             "#Values_in_zones", " ".join(zone_c[k]),
         ]

@@ -397,10 +397,10 @@ inline Deck readDeck(const std::string& dir, bool createResult) {
         t.skip(); c.kappa_const = t.num("heat conduction coefficient");
         t.skip(); const std::string enthalpy = t.next("enthalpy flow flag");
         t.skip(); const std::string molMass = t.next("molar mass diffusion flag");
-        if (model == "hardSpheres" || model == "LennardJones")
-            throw Fail("#Transport_coefficient_model " + model + ": the diffusion stage implements constant");
-        if (model != "constant") throw Fail("Unknown flag for transport model.");
-        c.transport = FV_TRANSPORT_CONSTANT;
+        if (model == "constant") c.transport = FV_TRANSPORT_CONSTANT;
+        else if (model == "hardSpheres") c.transport = FV_TRANSPORT_HARD_SPHERES;
+        else if (model == "LennardJones") c.transport = FV_TRANSPORT_LENNARD_JONES;
+        else throw Fail("Unknown flag for transport model.");
         if (enthalpy == "no") c.enthalpy_flow = FV_ENTHALPY_NO;
         else if (enthalpy == "explicit") c.enthalpy_flow = FV_ENTHALPY_EXPLICIT;
         else if (enthalpy == "implicit")
@@ -421,7 +421,24 @@ inline Deck readDeck(const std::string& dir, bool createResult) {
         t.skip(); c.Cv[k] = t.word("Cv");
         t.skip(); c.Tc[k] = t.word("Tc");
         t.skip(); c.Pc[k] = t.word("Pc");
-        for (int q = 0; q < 3; ++q) { t.skip(); t.next("transport parameter"); }
+        // #Kinetic_diameter_(A), #Lennard_Jones_eps/kB_(K), #Lennard_Jones_sigma_(A): the
+        // species data of the transport models, converted (std::stod) only by the model that
+        // reads them (abstractTransportModel.cpp:44-75)
+        std::string tr[3];
+        for (int q = 0; q < 3; ++q) { t.skip(); tr[q] = t.next("transport parameter"); }
+        auto conv = [&](const std::string& w, const char* what) {
+            try {
+                return std::stod(w);
+            } catch (...) {
+                throw Fail(std::string("not a number for ") + what + ": " + w);
+            }
+        };
+        if (c.diffusion && c.transport == FV_TRANSPORT_HARD_SPHERES)
+            c.transport_diameter[k] = conv(tr[0], "kinetic diameter");
+        if (c.diffusion && c.transport == FV_TRANSPORT_LENNARD_JONES) {
+            c.transport_lj_eps[k] = conv(tr[1], "Lennard-Jones eps/kB");
+            c.transport_lj_sigma[k] = conv(tr[2], "Lennard-Jones sigma");
+        }
         readPatches(t, 1, 0, k, c);
         if (t.next("values label") != "#Values_in_zones") throw Fail("Wrong position in file.");
         d.zoneC.emplace_back();
@@ -489,8 +506,6 @@ inline Deck readDeck(const std::string& dir, bool createResult) {
             throw Fail("chemical mechanism " + name + " is not implemented (no, Cl2)");
         }
     }
-    if (c.diffusion && c.chemistry != FV_CHEM_NONE)
-        throw Fail("#Diffusion_flag on: the diffusion stage runs without a chemical mechanism");
     return d;
 }
 

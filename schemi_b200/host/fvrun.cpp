@@ -386,7 +386,13 @@ void printConfig(const fv_config& c, const Deck& d) {
               << ", \"linear_reconstruction\": " << c.linear_reconstruction
               << ", \"diffusion_timestep\": " << c.diffusion_timestep
               << ", \"dt_coeff_source\": " << c.dt_coeff_source
-              << ", \"dt_coeff_diffusion\": " << c.dt_coeff_diffusion << "}" << std::endl;
+              << ", \"dt_coeff_diffusion\": " << c.dt_coeff_diffusion << ", \"transport_diameter\": [";
+    for (int k = 0; k < c.n_species; ++k) std::cout << (k ? ", " : "") << c.transport_diameter[k];
+    std::cout << "], \"transport_lj_eps\": [";
+    for (int k = 0; k < c.n_species; ++k) std::cout << (k ? ", " : "") << c.transport_lj_eps[k];
+    std::cout << "], \"transport_lj_sigma\": [";
+    for (int k = 0; k < c.n_species; ++k) std::cout << (k ? ", " : "") << c.transport_lj_sigma[k];
+    std::cout << "]}" << std::endl;
 }
 
 // output::mixedZoneWidth1D (src/service/output.cpp:310-391): the distance between the first

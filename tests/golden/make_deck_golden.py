@@ -28,7 +28,7 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 from schemi_b200 import cases  # noqa: E402
-from schemi_b200.case import BC, Case, PatchBC  # noqa: E402
+from schemi_b200.case import BC, Case, PatchBC, Species  # noqa: E402
 from schemi_b200.deck import write_deck  # noqa: E402
 import oracle as O  # noqa: E402
 
@@ -212,6 +212,58 @@ def deck_cases():
     c.enthalpy_flow, c.molmass_diffusion = "no", True
     c.t_end = _t_after(c, p, 6, 0.5)
     out.append(("vdw3_6x6x6_diffusion_gs", c, p, 3, True, [{}], 0.0))
+    # the transport models: hard spheres (kinetic diameters) and Lennard-Jones (eps / k_B, sigma)
+    # with both solvers; their face coefficients read the interpolated temperature and
+    # concentrations and the Riemann star pressure, the viscous heating the cells' viscosity.  The
+    # Lennard-Jones collision integrals call pow and exp, whose last bit the GPU's libm may set
+    # otherwise than the host's.
+    for solver, tag in (("explicit", ""), ("GaussSeidel", "_gs")):
+        c, p = cases.shock_tube_1d(n=60)
+        c.diffusion, c.transport, c.sle_solver = True, "hardSpheres", solver
+        c.mu, c.D, c.kappa = 1e-6, 0.0, 1e-6
+        c.species[0].diameter, c.species[1].diameter = 1.0, 1.3
+        # (the explicit solver with the molar-mass correction: see the van der Waals box below)
+        c.enthalpy_flow, c.molmass_diffusion, c.diffusion_timestep = "explicit", solver != "explicit", True
+        c.t_end = _t_after(c, p, 20, 0.4)
+        out.append((f"tube60_hardspheres{tag}", c, p, 6, True, [{}], 0.0))
+    c3, p3 = cases.reacting_shear_3d(n=6, periodic=False)
+    for model, solver, name in (("hardSpheres", "GaussSeidel", "vdw3_6x6_hardspheres_gs"),
+                                ("LennardJones", "explicit", "vdw3_6x6_lennardjones")):
+        c = Case(dims=2, n=(6, 6, 1), L=(1.0, 1.0, 1.0), species=[Species(**vars(s)) for s in c3.species],
+                 t_end=1.0, R_units="SI", eos="vanDerWaals", limiter="vanLeer", name="vdw2d")
+        for k in ("tail", "point", "right", "left"):
+            c.bc[k] = PatchBC.uniform("slip", 3)
+        p = [a.reshape(6, 6, 6)[0].ravel() for a in p3]
+        c.diffusion, c.transport, c.sle_solver = True, model, solver
+        c.mu, c.D, c.kappa = 0.0, 0.0, 0.0
+        for sp, d, e, sg in zip(c.species, (3.64, 3.46, 3.80), (98.0, 107.0, 71.4), (3.68, 3.43, 3.80)):
+            sp.diameter, sp.tr_eps, sp.tr_sigma = d, e, sg
+        # (the explicit solver takes the enthalpy flow's negative source into its diagonal without
+        # the time step, SLEMatrix.cpp:2166-2175: with the molar-mass correction the first 1e-15 s
+        # step cools this box to 15 K; the explicit deck runs without that correction)
+        c.enthalpy_flow, c.molmass_diffusion, c.diffusion_timestep = "explicit", solver != "explicit", True
+        c.t_end = _t_after(c, p, 8, 0.5)
+        out.append((name, c, p, 3, True, [{}], 0.0, {} if model == "hardSpheres" else {"gpu_tolerance": 1e-11}))
+    c, p = cases.shock_tube_1d(n=60)
+    c.diffusion, c.transport, c.sle_solver = True, "LennardJones", "GaussSeidel"
+    c.mu, c.D, c.kappa = 0.0, 1e-6, 0.0
+    for sp, e, sg in zip(c.species, (0.8, 1.1), (1.0, 1.2)):
+        sp.tr_eps, sp.tr_sigma = e, sg
+    # (without the molar-mass correction: with it this tube is ill conditioned, a one-ulp change of
+    # its input moving the state by 1e-4 within six steps, and the GPU's collision integrals may
+    # differ from the host's in the last bit)
+    c.enthalpy_flow, c.molmass_diffusion = "explicit", False
+    c.t_end = _t_after(c, p, 20, 0.4)
+    out.append(("tube60_lennardjones_gs", c, p, 6, True, [{}], 0.0, {"gpu_tolerance": 1e-11}))
+    # the Cl2 mechanism after a Gauss-Seidel hard-sphere diffusion stage (secondOrderStepSolver.cpp:
+    # 69-91) on a hot, non-uniform mixture, with the ClorumTest deck's transport data
+    c, p = cases.chlorine_dissociation_2d(n=4)
+    c.diffusion, c.transport, c.sle_solver = True, "hardSpheres", "GaussSeidel"
+    c.mu, c.D, c.kappa = 2e-8, 2e-8, 2e-5
+    c.species[0].diameter, c.species[1].diameter = 3.2, 1.6
+    c.enthalpy_flow, c.molmass_diffusion = "explicit", True
+    c.t_end = _t_after(c, p, 12, 0.5)
+    out.append(("cl2_4x4_diffusion_gs", c, p, 4, True, [{}], 0.0, {"gpu_tolerance": 1e-11}))
     return out
 
 
@@ -222,19 +274,25 @@ def deck_cases():
 # fixed velocity that its stream reader cannot parse): exit code 1, "Unknown type of boundary
 # condition", and only the empty result/Time.tsv left behind.
 SHIPPED = [
-    ("sod_cgs_1000", "Sod_CGS/Sod_CGS_1000"),
-    ("blastwaves_cgs_3000", "BlastWaves/BlastWaves_CGS_3000"),
-    ("gaussconcentration_cgs_1000", "GaussConcentration_CGS/GaussConcentration_CGS_1000"),
-    ("noh_1_1000", "Noh_1/Noh_1_1000"),
-    ("noh_2_1000", "Noh_2/Noh_2_1000"),
-    ("rarefactions_100_cgs", "Rarefactions_CGS/Rarefactions_100_CGS"),
-    ("noh_cgs_1000", "Noh_CGS/Noh_CGS_1000"),
-    ("diffusion_1000", "Diffusion/Diffusion_1000"),
+    ("sod_cgs_1000", "TestsTasks/Sod_CGS/Sod_CGS_1000"),
+    ("blastwaves_cgs_3000", "TestsTasks/BlastWaves/BlastWaves_CGS_3000"),
+    ("gaussconcentration_cgs_1000", "TestsTasks/GaussConcentration_CGS/GaussConcentration_CGS_1000"),
+    ("noh_1_1000", "TestsTasks/Noh_1/Noh_1_1000"),
+    ("noh_2_1000", "TestsTasks/Noh_2/Noh_2_1000"),
+    ("rarefactions_100_cgs", "TestsTasks/Rarefactions_CGS/Rarefactions_100_CGS"),
+    ("noh_cgs_1000", "TestsTasks/Noh_CGS/Noh_CGS_1000"),
+    ("diffusion_1000", "TestsTasks/Diffusion/Diffusion_1000"),
     # Gauss-Seidel diffusion of a van der Waals mixture between fixed walls, 100 x 100; to
     # t = 2e-3 (320 steps) instead of 2.0 (about 330,000)
-    ("poiseuille_100x100_short", "PoiseuilleFlow/PoiseuilleFlow_SI_100x100", "2E-3"),
+    ("poiseuille_100x100_short", "TestsTasks/PoiseuilleFlow/PoiseuilleFlow_SI_100x100", "2E-3"),
+    # the chemistry integrator's deck: Cl2 dissociation after a Gauss-Seidel hard-sphere diffusion
+    # stage, van der Waals, 2 x 2 at a constant 1e-8 s step (the GPU's exp may differ in the
+    # last bit: compared numerically there)
+    ("chlorum_2x2", "Chemical Reactions/ClorumTest/Chlorum"),
 ]
-SHIPPED_ROOT = "/root/reference/tests/TestsTasks"
+SHIPPED_ROOT = "/root/reference/tests"
+# decks whose GPU replay is compared numerically (relative to each column's scale)
+SHIPPED_GPU_TOLERANCE = {"chlorum_2x2": 1e-11}
 
 
 def _files(d):
@@ -250,7 +308,7 @@ def _key(prefix, rel):
     return prefix + ":" + rel.replace(os.sep, "|")
 
 
-def _save(name, d, inputs, runs_main, rcs, tol, logs):
+def _save(name, d, inputs, runs_main, rcs, tol, logs, gpu_tol=None):
     data = {_key("in", rel): np.frombuffer(b, dtype=np.uint8) for rel, b in inputs.items()}
     for r, main_txt in enumerate(runs_main):
         data[f"run{r}:main.txt"] = np.frombuffer(main_txt.encode(), dtype=np.uint8)
@@ -261,6 +319,8 @@ def _save(name, d, inputs, runs_main, rcs, tol, logs):
     data["runs"] = np.int64(len(runs_main))
     data["rc"] = np.asarray(rcs, dtype=np.int64)
     data["tolerance"] = np.float64(tol)
+    if gpu_tol is not None:
+        data["gpu_tolerance"] = np.float64(gpu_tol)
     # the end of what the reference printed (a failed run's error message is among its last lines)
     data["log_tails"] = np.asarray([lg[-600:] for lg in logs])
     np.savez_compressed(os.path.join(HERE, f"deck_{name}.npz"), **data)
@@ -296,7 +356,8 @@ def shipped(binary, only=None):
             main_txt = inputs[os.path.join("set", "main.txt")].decode()
             res = subprocess.run([binary], cwd=d, stdin=subprocess.DEVNULL, stdout=subprocess.PIPE,
                                  stderr=subprocess.STDOUT, timeout=1800)
-            _save(name, d, inputs, [main_txt], [res.returncode], 0.0, [res.stdout.decode(errors="replace")])
+            _save(name, d, inputs, [main_txt], [res.returncode], 0.0, [res.stdout.decode(errors="replace")],
+                  SHIPPED_GPU_TOLERANCE.get(name))
         finally:
             shutil.rmtree(d, ignore_errors=True)
 

@@ -144,12 +144,32 @@ def test_print_config_diffusion(tmp_path):
         assert got[key] == getattr(want, key), key
 
 
+@pytest.mark.parametrize("model", ["hardSpheres", "LennardJones"])
+def test_print_config_transport_models(tmp_path, model):
+    """The transport model of set/transportCoefficients.txt and its species data from sub_k.txt
+    (#Kinetic_diameter_(A), #Lennard_Jones_eps/kB_(K), #Lennard_Jones_sigma_(A)); the data a
+    model does not read is left at zero."""
+    c, p = _diffusion_case()
+    c.transport = model
+    for sp, d, e, sg in zip(c.species, (3.2, 1.6), (316.0, 130.0), (4.217, 3.0)):
+        sp.diameter, sp.tr_eps, sp.tr_sigma = d, e, sg
+    write_deck(c, str(tmp_path), p, restart=True)
+    res = _print_config(str(tmp_path))
+    assert res.returncode == 0, res.stderr
+    got = json.loads(res.stdout.strip().splitlines()[-1])
+    assert got["transport"] == {"hardSpheres": 1, "LennardJones": 2}[model]
+    hs = model == "hardSpheres"
+    assert got["transport_diameter"] == ([3.2, 1.6] if hs else [0, 0])
+    assert got["transport_lj_eps"] == ([0, 0] if hs else [316.0, 130.0])
+    assert got["transport_lj_sigma"] == ([0, 0] if hs else [4.217, 3.0])
+
+
 @pytest.mark.parametrize("file,key,value,message", [
     ("main.txt", "#Type_of_SLE_solver_flag", "Jacobi", "the diffusion stage implements explicit and GaussSeidel"),
     ("main.txt", "#Type_of_SLE_solver_flag", "LU", "Unknown or inappropriate matrix solver flag."),
     ("main.txt", "#Type_of_flow_solver", "HLL", "the diffusion stage runs with HLLC"),
     ("main.txt", "#Approximation_order", "SecondOrderRK", "the diffusion stage runs with SecondOrder"),
-    ("transportCoefficients.txt", "#Transport_coefficient_model", "hardSpheres", "implements constant"),
+    ("sub_1.txt", "#Kinetic_diameter_(A)", "wide", "not a number for kinetic diameter"),
     ("transportCoefficients.txt", "#Transport_coefficient_model", "Sutherland", "Unknown flag for transport model."),
     ("transportCoefficients.txt", "#Flag_for_enthalpy_flow_solution", "implicit", "takes no or explicit"),
     ("transportCoefficients.txt", "#Flag_for_enthalpy_flow_solution", "maybe",
@@ -159,6 +179,7 @@ def test_print_config_diffusion(tmp_path):
 ])
 def test_unsupported_diffusion_deck_refused(tmp_path, file, key, value, message):
     c, p = _diffusion_case()
+    c.transport = "hardSpheres"
     write_deck(c, str(tmp_path), p, restart=True)
     _edit(os.path.join(tmp_path, "set", file), key, value)
     res = _print_config(str(tmp_path))
