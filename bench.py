@@ -32,6 +32,8 @@ shock_tube_1d  config 1: the 1000-cell two-component tube to t = 0.2 through fv_
 diffusion_deck  the reference's Diffusion_1000 deck (the diffusion stage after every advection,
           34,561 steps to t = 0.3) through fv_run: us per step, the final fields against the
           reference's output of that deck, and the reference binary's us per step on it.
+gauss_seidel_deck  the same for the reference's PoiseuilleFlow_SI_100x100 deck (Gauss-Seidel
+          diffusion of a van der Waals channel flow, 100 x 100) shortened to t = 2e-3.
 
 batched   512 Richtmyer-Meshkov cases of seeded sizes 128^2..512^2 (FP32 flux) advanced by the
           persistent ensemble kernel, against the same cases one after the other.
@@ -650,39 +652,38 @@ def tube_c1(torch) -> dict:
             "tolerance_rel_linf": 1e-12}
 
 
-def diffusion_deck(torch, ref_steps: int = 300, ref_steps0: int = 20) -> dict:
-    """The reference's Diffusion_1000 deck (1000 cells, the diffusion stage with the explicit
-    solver after every advection, 34,561 steps to t = 0.3) through fv_run: microseconds per step
-    on the device, and the final fields against the reference's own output of that deck
-    (tests/golden/deck_diffusion_1000.npz).  cpu_baseline: the reference binary (patched build)
-    on the same deck, per step by differencing runs of ref_steps and ref_steps0 steps."""
+def _deck_section(torch, case, prim, fixture: str, workload: str, ref_steps: int, ref_steps0: int) -> dict:
+    """A restated deck of the reference through fv_run: microseconds per step on the device, the
+    final fields against the reference's own output of that deck (tests/golden/<fixture>), and
+    cpu_baseline: the reference binary (patched build) on the same deck, per step by differencing
+    runs of ref_steps and ref_steps0 steps (the oracle finds their end times)."""
     import numpy as np
 
-    from schemi_b200 import cases, fv
+    from schemi_b200 import fv
 
-    case, prim = cases.diffusion_tube_1d()
     g = fv.FVCase(case)
     g.upload(prim)
-    g.run(case.t_end, 2000)  # warm-up: graph capture and kernel configuration
+    g.run(case.t_end, 20)  # warm-up: graph capture and kernel configuration
     g.upload(prim)
     t0 = time.perf_counter()
     st = g.run(case.t_end)
     wall = time.perf_counter() - t0
     out = g.download()
+    kernels = g.kernels_per_step
     g.close()
-    z = np.load(os.path.join(ROOT, "tests", "golden", "deck_diffusion_1000.npz"))
+    z = np.load(os.path.join(ROOT, "tests", "golden", fixture))
     txt = z["out:result|output_000001.tsv"].tobytes().decode().strip().split("\n")
     head = txt[0].split("\t")
     rows = np.array([[float(x) for x in ln.split("\t")] for ln in txt[1:]])
     errs = {}
-    for f, col in (("c1", "concentration_1"), ("c2", "concentration_2"), ("vx", "velocity_x"), ("p", "pressure"),
-                   ("T", "temperature")):
-        b = rows[:, head.index(col)]
-        errs[f] = float(np.abs(out[f] - b).max() / max(np.abs(b).max(), 1e-300))
-    res = {"workload": "diffusion_tube_1d (the reference's Diffusion_1000 deck) to t=0.3, FP64, HLLC + vanAlbada, "
-                       "explicit diffusion with the molar-mass correction and the explicit enthalpy flow",
-           "steps": int(st.steps), "time": st.time, "device_us_per_step": 1e3 * st.device_ms / max(st.steps, 1),
-           "wall_us_per_step": 1e6 * wall / max(st.steps, 1), "kernels_per_step": 9,
+    for f, col in (("c1", "concentration_1"), ("c2", "concentration_2"), ("vx", "velocity_x"),
+                   ("vy", "velocity_y"), ("p", "pressure"), ("T", "temperature")):
+        if f in out and col in head:
+            b = rows[:, head.index(col)]
+            errs[f] = float(np.abs(out[f] - b).max() / max(np.abs(b).max(), 1e-300))
+    res = {"workload": workload, "steps": int(st.steps), "time": st.time,
+           "device_us_per_step": 1e3 * st.device_ms / max(st.steps, 1),
+           "wall_us_per_step": 1e6 * wall / max(st.steps, 1), "kernels_per_step": kernels,
            "rel_linf_vs_reference_output": max(errs.values()), "fields": errs, "tolerance_rel_linf": 1e-12}
     try:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -713,6 +714,31 @@ def diffusion_deck(torch, ref_steps: int = 300, ref_steps0: int = 20) -> dict:
     except Exception as e:  # noqa: BLE001 -- the reference build may be absent
         res["cpu_baseline"] = {"unavailable": str(e)}
     return res
+
+
+def diffusion_deck(torch, ref_steps: int = 300, ref_steps0: int = 20) -> dict:
+    """The reference's Diffusion_1000 deck (1000 cells, the diffusion stage with the explicit
+    solver after every advection, 34,561 steps to t = 0.3)."""
+    from schemi_b200 import cases
+
+    case, prim = cases.diffusion_tube_1d()
+    return _deck_section(torch, case, prim, "deck_diffusion_1000.npz",
+                         "diffusion_tube_1d (the reference's Diffusion_1000 deck) to t=0.3, FP64, HLLC + vanAlbada, "
+                         "explicit diffusion with the molar-mass correction and the explicit enthalpy flow",
+                         ref_steps, ref_steps0)
+
+
+def gauss_seidel_deck(torch, ref_steps: int = 60, ref_steps0: int = 10) -> dict:
+    """The reference's PoiseuilleFlow_SI_100x100 deck (van der Waals channel flow, 100 x 100, the
+    diffusion stage with the Gauss-Seidel solver after every advection) shortened to t = 2e-3
+    (309 steps)."""
+    from schemi_b200 import cases
+
+    case, prim = cases.poiseuille_2d()
+    return _deck_section(torch, case, prim, "deck_poiseuille_100x100_short.npz",
+                         "poiseuille_2d (the reference's PoiseuilleFlow_SI_100x100 deck) to t=2e-3, FP64, HLLC + "
+                         "vanAlbada, van der Waals, Gauss-Seidel diffusion with the molar-mass correction and the "
+                         "explicit enthalpy flow", ref_steps, ref_steps0)
 
 
 def reacting_accuracy(n: int, want) -> dict:
@@ -876,6 +902,7 @@ def run_ours(args):
     if rank == 0 and args.tube:
         line["shock_tube_1d"] = tube_c1(torch)
         line["diffusion_deck"] = diffusion_deck(torch)
+        line["gauss_seidel_deck"] = gauss_seidel_deck(torch)
     sample = batch_accuracy_sample(args.batch_cases) if args.batch_cases > 0 and not args.no_accuracy else []
     kept = {}
     if args.batch_cases > 0:

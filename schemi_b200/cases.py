@@ -63,6 +63,29 @@ def diffusion_tube_1d(n: int = 1000, t_end: float = 0.3) -> Tuple[Case, list]:
     return case, [np.where(left, 0.05, 0.0), np.where(left, 0.0, 0.05), z, z.copy(), z.copy(), np.full(n, 100.0)]
 
 
+def poiseuille_2d(n: int = 100, t_end: float = 2e-3) -> Tuple[Case, list]:
+    """A van der Waals gas (M = 0.0288, Cv = 20.8572, Tc = 131.523 K, Pc = 4.108e6 Pa) at rest in
+    a channel [0, 1] x [0, 0.5] m, c = 37.615 mol/m^3, p = 101317 Pa, driven by p = 101325 Pa held
+    at the inlet (fixedValueCell) and a free outlet, walls with v = 0 (fixedValueCell) and slip
+    concentration and pressure, SI units, vanAlbada, HLLC, Courant 0.47; the diffusion stage with
+    the Gauss-Seidel solver (2000 iterations), mu = D = 2e-3, kappa = 2, the explicit enthalpy
+    flow and the molar-mass correction, Courant-Source=0.25,0.5 -- the parameters of the
+    reference's tests/TestsTasks/PoiseuilleFlow/PoiseuilleFlow_SI_100x100 deck (whose 2.0 s this
+    shortens to t_end)."""
+    sp = [Species(M=0.0288, Cv=20.8572, Tc=131.523, Pc=4.108e6)]
+    case = Case(dims=2, n=(n, n, 1), L=(1.0, 0.5, 1.0), species=sp, t_end=t_end, R_units="SI",
+                eos="vanDerWaals", limiter="vanAlbada", courant=0.47, min_timestep=1e-15, name="poiseuille_2d")
+    case.bc["tail"] = PatchBC([BC("freeBoundary")], BC("freeBoundary"), BC("fixedValueCell", 101325.0))
+    case.bc["point"] = PatchBC.uniform("freeBoundary", 1)
+    for wall in ("right", "left"):
+        case.bc[wall] = PatchBC([BC("slip")], BC("fixedValueCell", (0.0, 0.0, 0.0)), BC("slip"))
+    case.diffusion, case.sle_solver, case.sle_max_iter = True, "GaussSeidel", 2000
+    case.mu, case.D, case.kappa = 2e-3, 2e-3, 2.0
+    case.enthalpy_flow, case.molmass_diffusion, case.diffusion_timestep = "explicit", True, False
+    z = np.zeros(n * n)
+    return case, [np.full(n * n, 37.615), z, z.copy(), z.copy(), np.full(n * n, 101317.0)]
+
+
 def real_gas_tube(eos: str, n: int = 200, limiter: str = "minmod") -> Tuple[Case, list]:
     """Two-component shock tube for the equations of state beyond ideal and van der Waals
     (transmissive ends, HLLC).

@@ -559,12 +559,13 @@ fv_status ensureScratch(fv_handle* h) {
             FV_CUDA(h, cudaMalloc(&X.tFree, sizeof(double) * st));
             FV_CUDA(h, cudaMalloc(&X.tOff, sizeof(double) * 6 * st));
             FV_CUDA(h, cudaMalloc(&X.sol, sizeof(double) * (ns + 4) * st));
-            FV_CUDA(h, cudaMalloc(&X.work, sizeof(double) * 2 * st));
+            FV_CUDA(h, cudaMalloc(&X.work, sizeof(double) * 3 * st));
             FV_CUDA(h, cudaMalloc(&X.cNew, sizeof(double) * (ns + 3) * st));
         }
         h->P.starV = X.starV;
         h->P.starP = X.starP;
         h->P.stagePrim = X.stagePrim;
+        if (X.gs) FV_CUDA(h, configureDiffusion(h->cfg.dims, h->P));
     }
     if (h->path == PATH_GENERIC && !h->FS) {
         const size_t tsz = h->cfg.precision == FV_PREC_F64 ? sizeof(double) : sizeof(float);

@@ -9,6 +9,18 @@ namespace fv {
 namespace {
 constexpr int kDiffThreads = 256;
 
+// dynamic shared memory of the Gauss-Seidel solve: both iterates when they fit, else none (the
+// iterates then live in the work buffer)
+int gsSmemBytes(const StepParams& P) {
+    const long long b = 2 * P.ncell * (long long)sizeof(double);
+    return b <= diff::kGsSmemBytes ? (int)b : 0;
+}
+// threads of the solve: one per column of a wavefront (whole warps), or the CTA's maximum
+int gsThreads(const StepParams& P, int D) {
+    const long long ncol = D == 1 ? 1 : (D == 2 ? (long long)P.n[0] : (long long)P.n[0] * P.n[1]);
+    return ncol >= diff::kGsThreads ? diff::kGsThreads : (int)((ncol + 31) / 32 * 32);
+}
+
 template <int NS, int EOS, int D>
 cudaError_t launchT(const StepParams& P, const GenericLayout& L, const diff::DiffParams& X, double* U, DevClock* ck,
                     double* blockMax, cudaStream_t st) {
@@ -22,18 +34,20 @@ cudaError_t launchT(const StepParams& P, const GenericLayout& L, const diff::Dif
         // the implicit solver: mass-fraction matrices and solves, new concentrations, the
         // averaged enthalpy flow, velocity and temperature matrices and solves, the phase
         const long long s = P.stride;
+        const int sm = gsSmemBytes(P);
+        const int gt = gsThreads(P, D);
         diff::k_gs_wmat<NS, EOS, D><<<gc, kDiffThreads, 0, st>>>(P, L, X, U, ck);
         for (int k = 0; k < NS; ++k)
-            diff::k_gs_solve<D><<<1, diff::kGsThreads, 0, st>>>(P, X.wDiag + k * s, X.wFree + k * s, X.wOff + k * 6 * s,
-                                                               X.sol + k * s, X.work, X.maxIter, ck);
+            diff::k_gs_solve<D><<<1, gt, sm, st>>>(P, X.wDiag + k * s, X.wFree + k * s, X.wOff + k * 6 * s,
+                                                                X.sol + k * s, X.work, X.maxIter, sm > 0, ck);
         diff::k_gs_post1<NS, EOS, D><<<gc, kDiffThreads, 0, st>>>(P, X, U, ck);
         if (X.enthalpy) diff::k_gs_afdif<NS, EOS, D><<<gf, kDiffThreads, 0, st>>>(P, L, X, ck);
         diff::k_gs_vtmat<NS, EOS, D><<<gc, kDiffThreads, 0, st>>>(P, L, X, U, ck);
         for (int d = 0; d < P.nmom; ++d)
-            diff::k_gs_solve<D><<<1, diff::kGsThreads, 0, st>>>(P, X.vDiag, X.vFree + d * s, X.vOff,
-                                                               X.sol + (NS + d) * s, X.work, X.maxIter, ck);
-        diff::k_gs_solve<D><<<1, diff::kGsThreads, 0, st>>>(P, X.tDiag, X.tFree, X.tOff, X.sol + (NS + 3) * s,
-                                                           X.work, X.maxIter, ck);
+            diff::k_gs_solve<D><<<1, gt, sm, st>>>(P, X.vDiag, X.vFree + d * s, X.vOff,
+                                                                X.sol + (NS + d) * s, X.work, X.maxIter, sm > 0, ck);
+        diff::k_gs_solve<D><<<1, gt, sm, st>>>(P, X.tDiag, X.tFree, X.tOff, X.sol + (NS + 3) * s,
+                                                            X.work, X.maxIter, sm > 0, ck);
         diff::k_gs_final<NS, EOS, D><<<gc, kDiffThreads, 0, st>>>(P, L, X, U, ck, blockMax);
     }
     diff::k_diff_source<<<1, 1024, 0, st>>>(X, ck, (int)gc);
@@ -57,6 +71,14 @@ cudaError_t byEos(int eos, int dims, const StepParams& P, const GenericLayout& L
 }  // namespace
 
 int diffusionBlocks(const StepParams& P) { return (int)((P.ncell + kDiffThreads - 1) / kDiffThreads); }
+
+cudaError_t configureDiffusion(int dims, const StepParams& P) {
+    const int sm = gsSmemBytes(P);
+    if (sm <= 48 * 1024) return cudaSuccess;
+    if (dims == 1) return cudaFuncSetAttribute(diff::k_gs_solve<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (dims == 2) return cudaFuncSetAttribute(diff::k_gs_solve<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    return cudaFuncSetAttribute(diff::k_gs_solve<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+}
 
 cudaError_t launchDiffusion(int ns, int eos, int dims, const StepParams& P, const GenericLayout& L,
                             const diff::DiffParams& X, double* U, DevClock* ck, double* blockMax, cudaStream_t st) {

@@ -159,82 +159,192 @@ __global__ void k_gs_wmat(const StepParams P, const GenericLayout L, const DiffP
 
 // ----------------------------------------------------------------------------- k_gs_solve
 // One CTA solves diag x + off x = free for the field in x (start in, solution out): backward
-// sweeps as wavefronts, the convergence measure reduced over the CTA after each sweep.
+// sweeps as wavefronts of decreasing i + j (+ k), the convergence test of each sweep over all
+// cells.  Each cell computes, in the reference's order, x = free / diag - sum of off x / diag over
+// the lower neighbours in reverse face order (z-, y-, x-: the old iterate) and then the upper ones
+// (z+, y+, x+: this sweep's new values).
 constexpr int kGsThreads = 1024;
+// the two iterates in shared memory up to this many bytes (else in global memory)
+constexpr int kGsSmemBytes = 200 * 1024;
 
+// one cell's coefficients: 1 / diag (the same value each sweep, formed once per solve), free, the
+// off-diagonal per face slot
+struct GsCoef {
+    double aii, free, o[6];
+};
 template <int D>
-__device__ __forceinline__ double gsCell(const StepParams& P, long long i, const int* ijk, const double* __restrict__ diag,
-                                         const double* __restrict__ free, const double* __restrict__ off,
-                                         const double* oldI, const double* newI) {
-    // (the iterates are written by other threads of the CTA between wavefronts: plain loads)
+__device__ __forceinline__ void gsLoad(const StepParams& P, long long i, const double* aiiI,
+                                       const double* __restrict__ free, const double* __restrict__ off, GsCoef& c) {
     const long long st = P.stride;
-    const double aii = 1. / diag[i];
-    double x = free[i] * aii;
-    // lower neighbours in reverse face order: z-, y-, x-; then upper: z+, y+, x+
-    if (D >= 3 && ijk[2] > 0) x -= off[4 * st + i] * oldI[i - (long long)P.n[0] * P.n[1]] * aii;
-    if (D >= 2 && ijk[1] > 0) x -= off[3 * st + i] * oldI[i - P.n[0]] * aii;
-    if (ijk[0] > 0) x -= off[0 * st + i] * oldI[i - 1] * aii;
-    if (D >= 3 && ijk[2] < P.n[2] - 1) x -= off[5 * st + i] * newI[i + (long long)P.n[0] * P.n[1]] * aii;
-    if (D >= 2 && ijk[1] < P.n[1] - 1) x -= off[2 * st + i] * newI[i + P.n[0]] * aii;
-    if (ijk[0] < P.n[0] - 1) x -= off[1 * st + i] * newI[i + 1] * aii;
+    c.aii = aiiI[i];
+    c.free = free[i];
+#pragma unroll
+    for (int s = 0; s < 2 * D; ++s) c.o[s] = off[s * st + i];
+}
+// free / diag less the lower neighbours' terms (the old iterate: known before the sweep reaches
+// the cell), then the upper neighbours' (this sweep's new values)
+template <int D>
+__device__ __forceinline__ double gsLower(const StepParams& P, long long i, const int* ijk, const GsCoef& c,
+                                          const double* oldI) {
+    const double aii = c.aii;
+    double x = c.free * aii;
+    const long long sy = P.n[0], sz = (long long)P.n[0] * P.n[1];
+    if (D >= 3 && ijk[2] > 0) x -= c.o[4] * oldI[i - sz] * aii;
+    if (D >= 2 && ijk[1] > 0) x -= c.o[3] * oldI[i - sy] * aii;
+    if (ijk[0] > 0) x -= c.o[0] * oldI[i - 1] * aii;
     return x;
 }
+template <int D>
+__device__ __forceinline__ double gsUpper(const StepParams& P, long long i, const int* ijk, const GsCoef& c,
+                                          double x, const double* newI) {
+    const double aii = c.aii;
+    const long long sy = P.n[0], sz = (long long)P.n[0] * P.n[1];
+    if (D >= 3 && ijk[2] < P.n[2] - 1) x -= c.o[5] * newI[i + sz] * aii;
+    if (D >= 2 && ijk[1] < P.n[1] - 1) x -= c.o[2] * newI[i + sy] * aii;
+    if (ijk[0] < P.n[0] - 1) x -= c.o[1] * newI[i + 1] * aii;
+    return x;
+}
+template <int D>
+__device__ __forceinline__ double gsUpdate(const StepParams& P, long long i, const int* ijk, const GsCoef& c,
+                                           const double* oldI, const double* newI) {
+    return gsUpper<D>(P, i, ijk, c, gsLower<D>(P, i, ijk, c, oldI), newI);
+}
+// the reference loop's convergence measure of one cell, as a test: 100 max_i r_i < 1e-12 holds
+// exactly when no cell has 100 r_i >= 1e-12 (the rounded product is monotone in r), a NaN at the
+// first cell failing it (its value is taken as it is) and elsewhere passed over (taken only when
+// larger)
+__device__ __forceinline__ bool gsFails(long long i, double v, double old) {
+    const double r = fabs((v - old) / (fabs(v) + Num<double>::stab()));
+    return i == 0 ? !(100. * r < 1e-12) : (100. * r >= 1e-12);
+}
 
+// The sweep's cells of one wavefront are one per column (2D: the cells of one x; 3D: of one
+// (x, y)), so a thread keeps its columns over the whole solve and walks down each.  With at most
+// one column per thread the work between two barriers is pipelined: the thread applies to its
+// cell only the upper neighbours' terms (the values of the wavefront just computed), and then
+// forms its next cell's lower part (free / diag and the old iterate's terms, whose coefficients
+// it loaded a wavefront earlier) and loads the coefficients of the cell after that; the
+// convergence test runs over all cells after the sweep.  The iterates live in shared memory when
+// both fit (useSmem), else in work[0..2); 1 / diag in work[2] (work[0] with useSmem).
 template <int D>
 __global__ void __launch_bounds__(kGsThreads) k_gs_solve(const StepParams P, const double* __restrict__ diag,
                                                           const double* __restrict__ free,
                                                           const double* __restrict__ off, double* __restrict__ x,
-                                                          double* __restrict__ work, int maxIt,
+                                                          double* __restrict__ work, int maxIt, int useSmem,
                                                           DevClock* __restrict__ ck) {
-    __shared__ double red[32];
-    __shared__ int stop;
+    extern __shared__ double gsSmem[];
     if (ck->done) return;
-    const long long n = P.ncell;
-    const int nx = P.n[0], ny = P.n[1], nz = P.n[2];
-    double* bufA = x;       // the old iterate
-    double* bufB = work;    // the new one
-    for (long long i = threadIdx.x; i < n; i += blockDim.x) bufB[i] = x[i];
+    const long long n = P.ncell, rs = P.stride;
+    double* oldI = useSmem ? gsSmem : work;
+    double* newI = useSmem ? gsSmem + n : work + rs;
+    double* aiiI = useSmem ? work : work + 2 * rs;
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) aiiI[i] = 1. / diag[i];
     __syncthreads();
-    for (int it = 1;; ++it) {
-        if (D == 1) {
-            if (threadIdx.x == 0)
+    if constexpr (D == 1) {
+        // a 1D wavefront is one cell: one thread sweeps
+        if (threadIdx.x == 0) {
+            for (long long i = 0; i < n; ++i) oldI[i] = x[i];
+            for (int it = 1;; ++it) {
+                bool failed = false;
+                GsCoef c;
+                gsLoad<D>(P, n - 1, aiiI, free, off, c);
                 for (long long i = n - 1; i >= 0; --i) {
+                    GsCoef cn;
+                    if (i > 0) gsLoad<D>(P, i - 1, aiiI, free, off, cn);
                     const int ijk[3] = {(int)i, 0, 0};
-                    bufB[i] = gsCell<D>(P, i, ijk, diag, free, off, bufA, bufB);
+                    const double v = gsUpdate<D>(P, i, ijk, c, oldI, newI);
+                    newI[i] = v;
+                    failed |= gsFails(i, v, oldI[i]);
+                    c = cn;
                 }
-        } else {
-            const int smax = (nx - 1) + (ny - 1) + (D >= 3 ? nz - 1 : 0);
-            for (int sw = smax; sw >= 0; --sw) {
-                // the cells with i + j (+ k) = sw
-                const long long cand = D >= 3 ? (long long)nx * ny : (long long)nx;
-                for (long long q = threadIdx.x; q < cand; q += blockDim.x) {
-                    int ijk[3];
-                    ijk[0] = (int)(q % nx);
-                    ijk[1] = D >= 3 ? (int)(q / nx) : sw - ijk[0];
-                    ijk[2] = D >= 3 ? sw - ijk[0] - ijk[1] : 0;
-                    if (ijk[1] < 0 || ijk[1] >= ny || ijk[2] < 0 || ijk[2] >= nz) continue;
-                    const long long i = ijk[0] + (long long)nx * (ijk[1] + (long long)ny * ijk[2]);
-                    bufB[i] = gsCell<D>(P, i, ijk, diag, free, off, bufA, bufB);
-                }
-                __syncthreads();
+                if (!failed || it >= maxIt) break;
+                double* t = oldI;
+                oldI = newI;
+                newI = t;
+            }
+            for (long long i = 0; i < n; ++i) {
+                double v = newI[i];
+                if (fabs(v) < 2.220446049250313e-16) v = 0;
+                x[i] = v;
             }
         }
-        __syncthreads();
-        double mx = 0;
-        for (long long i = threadIdx.x; i < n; i += blockDim.x)
-            mx = smax(mx, fabs((bufB[i] - bufA[i]) / (fabs(bufB[i]) + Num<double>::stab())));
-        mx = blockMaxReduce<double>(mx, red);
-        if (threadIdx.x == 0) stop = (100. * mx < 1e-12) || it >= maxIt;
-        __syncthreads();
-        if (stop) break;
-        double* t = bufA;  // old = new
-        bufA = bufB;
-        bufB = t;
-        __syncthreads();
+        return;
+    }
+    const int nx = P.n[0], ny = P.n[1], nz = P.n[2];
+    const int dmax = (nx - 1) + (ny - 1) + (D >= 3 ? nz - 1 : 0);
+    const int ncol = D == 2 ? nx : nx * ny;
+    const int hmax = D == 2 ? ny : nz;  // cells per column
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) oldI[i] = x[i];
+    __syncthreads();
+    const bool single = ncol <= (int)blockDim.x;
+    // this thread's column (single): its x (and y) and the wavefront index of its lowest cell
+    const int col = threadIdx.x;
+    const int cx = D == 2 ? col : col % nx, cy = D == 2 ? 0 : col / nx;
+    const int base = D == 2 ? cx : cx + cy;  // d of the column's cell at height 0
+    const bool mine = single && col < ncol;
+    auto cellOf = [&](int hh) -> long long {
+        return D == 2 ? cx + (long long)nx * hh : cx + (long long)nx * (cy + (long long)ny * hh);
+    };
+    auto ijkOf = [&](int hh, int* ijk) {
+        ijk[0] = cx;
+        ijk[1] = D == 2 ? hh : cy;
+        ijk[2] = D == 2 ? 0 : hh;
+    };
+    for (int it = 1;; ++it) {
+        bool failed = false;
+        int h = hmax - 1;  // height of this thread's next cell (y in 2D, z in 3D)
+        GsCoef c{}, cn{};  // the coefficients of cells h and h - 1
+        double lower = 0;  // the lower part of cell h
+        if (mine) {
+            int ijk[3];
+            ijkOf(h, ijk);
+            gsLoad<D>(P, cellOf(h), aiiI, free, off, c);
+            lower = gsLower<D>(P, cellOf(h), ijk, c, oldI);
+            if (h > 0) gsLoad<D>(P, cellOf(h - 1), aiiI, free, off, cn);
+        }
+        for (int d = dmax; d >= 0; --d) {
+            if (single) {
+                if (mine && h >= 0 && d == base + h) {
+                    const long long i = cellOf(h);
+                    int ijk[3];
+                    ijkOf(h, ijk);
+                    const double v = gsUpper<D>(P, i, ijk, c, lower, newI);
+                    newI[i] = v;
+                    // off the path to the next barrier's readers: the next cell's lower part and
+                    // the loads of the one after it
+                    if (h > 0) {
+                        int ijn[3];
+                        ijkOf(h - 1, ijn);
+                        c = cn;
+                        lower = gsLower<D>(P, cellOf(h - 1), ijn, c, oldI);
+                        if (h > 1) gsLoad<D>(P, cellOf(h - 2), aiiI, free, off, cn);
+                    }
+                    --h;
+                }
+            } else {
+                for (int q = threadIdx.x; q < ncol; q += blockDim.x) {
+                    const int qx = D == 2 ? q : q % nx, qy = D == 2 ? 0 : q / nx;
+                    const int hh = d - (D == 2 ? qx : qx + qy);
+                    if (hh < 0 || hh >= hmax) continue;
+                    const long long i = D == 2 ? qx + (long long)nx * hh : qx + (long long)nx * (qy + (long long)ny * hh);
+                    GsCoef cq;
+                    gsLoad<D>(P, i, aiiI, free, off, cq);
+                    const int ijk[3] = {qx, D == 2 ? hh : qy, D == 2 ? 0 : hh};
+                    newI[i] = gsUpdate<D>(P, i, ijk, cq, oldI, newI);
+                }
+            }
+            __syncthreads();
+        }
+        for (long long i = threadIdx.x; i < n; i += blockDim.x) failed |= gsFails(i, newI[i], oldI[i]);
+        const int anyFailed = __syncthreads_or(failed);
+        if (!anyFailed || it >= maxIt) break;
+        double* t = oldI;
+        oldI = newI;
+        newI = t;
     }
     // normalize, and the solution into x
     for (long long i = threadIdx.x; i < n; i += blockDim.x) {
-        double v = bufB[i];
+        double v = newI[i];
         if (fabs(v) < 2.220446049250313e-16) v = 0;
         x[i] = v;
     }

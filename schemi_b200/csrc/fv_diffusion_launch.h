@@ -45,7 +45,8 @@ struct DiffParams {
     double* tFree;
     double* tOff;              // [6][stride]
     double* sol;               // [N + 4][stride] solutions: w_1..w_N, v_x, v_y, v_z, T
-    double* work;              // [2][stride] Gauss-Seidel iterates
+    double* work;              // [3][stride] Gauss-Seidel scratch: the iterates (when they exceed
+                               //    shared memory) and 1 / diag
     double* cNew;              // [N + 3][stride] concentrations c_0..c_N, CCVNew, old energy
 };
 
@@ -56,6 +57,9 @@ __host__ __device__ constexpr int faceSlotCount(int ns) { return 3 * ns + 13; }
 
 // CTAs of the stage's cell kernel (= blockMax entries it writes, and the partial minima per limit).
 int diffusionBlocks(const StepParams& P);
+
+// Opt the Gauss-Seidel solve in to the shared memory its iterates need (outside any capture).
+cudaError_t configureDiffusion(int dims, const StepParams& P);
 
 // Enqueue the diffusion stage of the advected state U (in place) with the clock's dt: the new
 // state, its primitives (P.stagePrim), the CFL block maxima and the clock's source time step.
