@@ -55,15 +55,32 @@ __device__ __forceinline__ void normalize(double* x) {
         if (fabs(x[i]) < kEps) x[i] = 0;
 }
 
+// The solvers' convergence test 100 max_i d_i < kTol, d_i = |new_i - old_i| / (|new_i| + stab)
+// (the first component's d taken as it is, later ones when larger).  It holds exactly when no
+// component has 100 d_i >= kTol (the rounded product is monotone in d), a NaN d_0 failing it and a
+// NaN elsewhere passed over.  Each d_i = a / b is compared without the division where the quotient
+// is far from the threshold: fl(a 1e14) < b bounds a / b below 1e-14 (1 + eps), so 100 d_i stays
+// below 1e-12 (1 + eps)^3 < kTol; fl(b 1e-9) < a bounds it above 1e-9 (1 - eps), so 100 d_i
+// exceeds 1e-7 (1 - eps)^2 > kTol (b >= stab, so b 1e-9 does not underflow).  In between, and
+// for NaN operands, the quotient is formed as in the reference.
 template <int N>
-__device__ __forceinline__ double relDiff(const double* nw, const double* old) {
-    double mx = 0;
+__device__ __forceinline__ bool converged(const double* nw, const double* old) {
+    bool ok = true;
 #pragma unroll
     for (int i = 0; i < N; ++i) {
-        const double d = fabs((nw[i] - old[i]) / (fabs(nw[i]) + stab()));
-        if (i == 0 || d > mx) mx = d;
+        const double a = fabs(nw[i] - old[i]), b = fabs(nw[i]) + stab();
+        bool fails;
+        if (a * 1e14 < b) {
+            fails = false;
+        } else if (a > b * 1e-9) {
+            fails = true;
+        } else {
+            const double d = a / b;
+            fails = i == 0 ? !(100. * d < kTol) : (100. * d >= kTol);
+        }
+        ok = ok && !fails;
     }
-    return 100. * mx;
+    return ok;
 }
 
 template <int N>
@@ -105,7 +122,7 @@ __device__ bool solveGS(const System<N>& m, const double* init, int maxIter, dou
 #pragma unroll
             for (int q = nRight<N>(i) - 1; q >= 0; --q) nw[i] -= m.A[i][right<N>(i, q)] * nw[right<N>(i, q)] * aii[i];
         }
-        if (relDiff<N>(nw, old) < kTol) {
+        if (converged<N>(nw, old)) {
             normalize<N>(nw);
 #pragma unroll
             for (int i = 0; i < N; ++i) out[i] = nw[i];
@@ -145,7 +162,7 @@ __device__ bool solveJ(const System<N>& m, const double* init, int maxIter, doub
             for (int q = nRight<N>(i) - 1; q >= 0; --q) rs -= m.A[i][right<N>(i, q)] * old[right<N>(i, q)];
             nw[i] = (m.B[i] + rs) * aii[i];
         }
-        if (relDiff<N>(nw, old) < kTol) {
+        if (converged<N>(nw, old)) {
             normalize<N>(nw);
 #pragma unroll
             for (int i = 0; i < N; ++i) out[i] = nw[i];
