@@ -138,9 +138,14 @@ enum fv_chem_solver {
 };
 
 /* Linear solver of the diffusion stage (#Type_of_SLE_solver_flag, abstractMatrixSolver.cpp:51-70):
- * "explicit" (the stage's fields advance explicitly, Diffusion.cpp:437-441,787-797,818-825) or
- * "GaussSeidel". */
-enum fv_sle_solver { FV_SLE_EXPLICIT = 0, FV_SLE_GAUSS_SEIDEL = 1 };
+ * "explicit" (the stage's fields advance explicitly, Diffusion.cpp:437-441,787-797,818-825),
+ * "GaussSeidel" (GaussSeidelSolver.cpp), "Jacobi" (JacobiSolver.cpp), on 1D meshes "Thomas"
+ * (ThomasSolver.cpp, the tridiagonal sweep), each solving the matrices of
+ * SLEMatrix::generateDTimeLaplacian, or "noSolver" (noMatrixSolver.cpp: the stage takes the
+ * implicit branch and every solve returns its start field). */
+enum fv_sle_solver {
+    FV_SLE_EXPLICIT = 0, FV_SLE_GAUSS_SEIDEL = 1, FV_SLE_JACOBI = 2, FV_SLE_THOMAS = 3, FV_SLE_NO_SOLVER = 4
+};
 
 /* Transport-coefficient model (transportCoefficients.txt #Transport_coefficient_model,
  * phaseInitialization.cpp:211-222, abstractTransportModel.cpp:37-80):

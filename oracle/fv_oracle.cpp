@@ -1882,6 +1882,87 @@ std::vector<double> dGaussSeidel(const SLE1& M, const std::vector<double>& start
     }
 }
 
+// The matrix solvers' convergence measure (abstractMatrixSolver::relativeIterationDifference,
+// src/interfaces/abstractMatrixSolver.cpp:22-29): 100 max |(new - old) / (|new| + eps)|, the
+// valarray's max taking the first element as it is and later ones when larger.
+double dRelDiff(const std::vector<double>& oldI, const std::vector<double>& newI) {
+    double mx = 0;
+    for (size_t i = 0; i < newI.size(); ++i) {
+        const double r = std::fabs((newI[i] - oldI[i]) / (std::fabs(newI[i]) + kStab));
+        if (i == 0 || r > mx) mx = r;
+    }
+    return 100. * mx;
+}
+void dNormalize(std::vector<double>& x) {  // abstractMatrixSolver::normalize (:31-38)
+    for (auto& v : x)
+        if (std::fabs(v) < std::numeric_limits<double>::epsilon()) v = 0;
+}
+
+// JacobiSolver::algorithm (src/SLE/JacobiSolver.cpp:9-86): a forward and a backward pass per
+// iteration, each row from the old iterate alone, (b + rowSum) / diag with rowSum the negated
+// lower then upper terms, each list in reverse in the backward pass (whose values are the
+// iterate); stop below the tolerance or at the iteration limit.
+std::vector<double> dJacobi(const SLE1& M, const std::vector<double>& start, long long maxIt) {
+    const long long n = (long long)start.size();
+    std::vector<double> oldI(start), newI(start);
+    long long it = 0;
+    while (true) {
+        ++it;
+        for (long long i = 0; i < n; ++i) {
+            const double aii = 1. / M.diag[i];
+            double rowSum = 0;
+            for (const auto& e : M.lower[i]) rowSum -= e.first * oldI[e.second];
+            for (const auto& e : M.upper[i]) rowSum -= e.first * oldI[e.second];
+            newI[i] = (M.free[i] + rowSum) * aii;
+        }
+        for (long long i = n - 1; i >= 0; --i) {
+            const double aii = 1. / M.diag[i];
+            double rowSum = 0;
+            for (size_t j = M.lower[i].size(); j-- > 0;) rowSum -= M.lower[i][j].first * oldI[M.lower[i][j].second];
+            for (size_t j = M.upper[i].size(); j-- > 0;) rowSum -= M.upper[i][j].first * oldI[M.upper[i][j].second];
+            newI[i] = (M.free[i] + rowSum) * aii;
+        }
+        const double diff = dRelDiff(oldI, newI);
+        if (diff < 1e-12 || it >= maxIt) {
+            dNormalize(newI);
+            return newI;
+        }
+        oldI = newI;
+    }
+}
+
+// ThomasSolver::algorithm (src/SLE/ThomasSolver.cpp:9-52): the tridiagonal sweep of a 1D mesh,
+// P_i = -u_i / (d_i + l_i P_{i-1}), Q_i = (f_i - l_i Q_{i-1}) / (d_i + l_i P_{i-1}), then
+// x_i = P_i x_{i+1} + Q_i from the last row down.
+std::vector<double> dThomas(const SLE1& M) {
+    const long long N = (long long)M.diag.size();
+    std::vector<double> x(N), P(N), Q(N);
+    P[0] = -M.upper[0][0].first / M.diag[0];
+    Q[0] = M.free[0] / M.diag[0];
+    for (long long i = 1; i < N - 1; ++i) {
+        const double l = M.lower[i][0].first;
+        P[i] = -M.upper[i][0].first / (M.diag[i] + l * P[i - 1]);
+        Q[i] = (M.free[i] - l * Q[i - 1]) / (M.diag[i] + l * P[i - 1]);
+    }
+    P[N - 1] = 0;
+    {
+        const double l = M.lower[N - 1][0].first;
+        Q[N - 1] = (M.free[N - 1] - l * Q[N - 2]) / (M.diag[N - 1] + l * P[N - 2]);
+    }
+    x[N - 1] = Q[N - 1];
+    for (long long i = N - 2; i >= 0; --i) x[i] = P[i] * x[i + 1] + Q[i];
+    dNormalize(x);
+    return x;
+}
+
+// the stage's implicit solver (abstractMatrixSolver::createMatrixSolver, :50-120)
+std::vector<double> dSolve(const fv_config& cf, const SLE1& M, const std::vector<double>& start) {
+    if (cf.sle_solver == FV_SLE_JACOBI) return dJacobi(M, start, cf.sle_max_iter);
+    if (cf.sle_solver == FV_SLE_THOMAS) return dThomas(M);
+    if (cf.sle_solver == FV_SLE_NO_SOLVER) return start;  // noMatrixSolver::solve
+    return dGaussSeidel(M, start, cf.sle_max_iter);
+}
+
 // ---------------------------------------------------------------- transport models
 // Molecular transport coefficients of one point from its temperature T, pressure p and
 // concentrations c[0..N] (c[0] the total): transportCoefficients::calculateCoefficients
@@ -2171,7 +2252,7 @@ int diffusionStage(fvo_case& cs, double dt) {
 
     // mass-fraction matrices (Diffusion.cpp:321-339; SLEMatrix.cpp:2054-2078 explicit,
     // :410-546 implicit)
-    const bool gs = cf.sle_solver == FV_SLE_GAUSS_SEIDEL;
+    const bool gs = cf.sle_solver != FV_SLE_EXPLICIT;  // the implicit branch: Gauss-Seidel, Jacobi, Thomas, noSolver
     std::vector<std::vector<V3>> gradW(NS);
     std::vector<std::vector<double>> diagW(NS, std::vector<double>(nc)), oldW(NS, std::vector<double>(nc)),
         freeW(NS, std::vector<double>(nc, 0.0));
@@ -2267,7 +2348,7 @@ int diffusionStage(fvo_case& cs, double dt) {
     for (int k = 0; k < (gs ? NS : 0); ++k) {
         MW[k].diag = diagW[k];
         MW[k].free = freeW[k];
-        wSol[k] = dGaussSeidel(MW[k], w[k], cf.sle_max_iter);
+        wSol[k] = dSolve(cf, MW[k], w[k]);
     }
     std::vector<std::vector<double>> wNew(NS, std::vector<double>(nc));
     std::vector<std::vector<double>> cN(NS + 1, std::vector<double>(nc));
@@ -2440,11 +2521,11 @@ int diffusionStage(fvo_case& cs, double dt) {
                 start[i] = v[i].x[d];
                 MV[d].free[i] = freeV[i].x[d];
             }
-            vSol[d] = dGaussSeidel(MV[d], start, cf.sle_max_iter);
+            vSol[d] = dSolve(cf, MV[d], start);
         }
         MT.diag = diagT;
         MT.free = freeT;
-        TSol = dGaussSeidel(MT, T, cf.sle_max_iter);
+        TSol = dSolve(cf, MT, T);
     }
 
     // the phase after the stage (Diffusion.cpp:965-1034)
@@ -2896,8 +2977,12 @@ bool validate(const fv_config& cf, std::string& err) {
             err = "the diffusion stage runs with ideal and van der Waals mixtures";
             return false;
         }
-        if (cf.sle_solver != FV_SLE_EXPLICIT && cf.sle_solver != FV_SLE_GAUSS_SEIDEL) {
-            err = "the diffusion stage runs with the explicit and Gauss-Seidel solvers";
+        if (cf.sle_solver < FV_SLE_EXPLICIT || cf.sle_solver > FV_SLE_NO_SOLVER) {
+            err = "unknown matrix solver";
+            return false;
+        }
+        if (cf.sle_solver == FV_SLE_THOMAS && (cf.dims != 1 || cf.n[0] < 2)) {
+            err = "the Thomas solver runs on 1D meshes of at least 2 cells";
             return false;
         }
         if (cf.transport < FV_TRANSPORT_CONSTANT || cf.transport > FV_TRANSPORT_LENNARD_JONES) {

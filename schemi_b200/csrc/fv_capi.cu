@@ -709,7 +709,8 @@ fv_status fv_create(const fv_config* cfg, fv_handle** out) {
         // "linear" reconstruction takes the cell velocities' gradient (Diffusion.cpp:178-184)
         X.interpV = cfg->gravity || cfg->linear_reconstruction;
         X.dtDiff = cfg->diffusion_timestep != 0;
-        X.gs = cfg->sle_solver == FV_SLE_GAUSS_SEIDEL;
+        X.gs = cfg->sle_solver != FV_SLE_EXPLICIT;
+        X.sle = cfg->sle_solver;
         X.maxIter = cfg->sle_max_iter;
         X.coeffSource = cfg->dt_coeff_source;
         X.coeffDiff = cfg->dt_coeff_diffusion;
@@ -1086,8 +1087,8 @@ long long fv_kernels_per_step(const fv_handle* h) {
     if (h->cfg.diffusion && h->diff.gs)
         // prim, faces, the mass-fraction matrices and N solves, concentrations, the averaged
         // enthalpy flow, velocity / temperature matrices and nmom + 1 solves, phase, source, finalize
-        return stage + 2 + 1 + h->cfg.n_species + 1 + (h->diff.enthalpy ? 1 : 0) + 1 + h->P.nmom + 1 + 1 + 1 + 1 +
-               chem;
+        return stage + 2 + 1 + (h->diff.sle == FV_SLE_NO_SOLVER ? 0 : h->cfg.n_species + h->P.nmom + 1) + 1 +
+               (h->diff.enthalpy ? 1 : 0) + 1 + 1 + 1 + 1 + chem;
     if (h->cfg.diffusion) return stage + 5 + chem;  // the stage's 4 kernels, [chemistry,] finalize
     if (h->cfg.order == FV_ORDER_SECOND_RK) return 2 * stage + 2 + chem;  // two stages, average, finalize
     if (h->cfg.order == FV_ORDER_THIRD || h->cfg.order == FV_ORDER_THIRD_CADA)

@@ -36,18 +36,24 @@ cudaError_t launchT(const StepParams& P, const GenericLayout& L, const diff::Dif
         const long long s = P.stride;
         const int sm = gsSmemBytes(P);
         const int gt = gsThreads(P, D);
+        // one solve of diag x + off x = free (x: the start in, the solution out) by the deck's solver
+        auto solve = [&](const double* dg, const double* fr, const double* of, double* xs) {
+            if (X.sle == FV_SLE_JACOBI)
+                diff::k_jacobi_solve<D><<<1, diff::kGsThreads, sm, st>>>(P, dg, fr, of, xs, X.work, X.maxIter, sm > 0, ck);
+            else if (X.sle == FV_SLE_THOMAS)
+                diff::k_thomas_solve<<<1, 32, 0, st>>>(P, dg, fr, of, xs, X.work, ck);
+            else if (X.sle == FV_SLE_NO_SOLVER)
+                return;  // noMatrixSolver::solve: the start field is the solution
+            else
+                diff::k_gs_solve<D><<<1, gt, sm, st>>>(P, dg, fr, of, xs, X.work, X.maxIter, sm > 0, ck);
+        };
         diff::k_gs_wmat<NS, EOS, D><<<gc, kDiffThreads, 0, st>>>(P, L, X, U, ck);
-        for (int k = 0; k < NS; ++k)
-            diff::k_gs_solve<D><<<1, gt, sm, st>>>(P, X.wDiag + k * s, X.wFree + k * s, X.wOff + k * 6 * s,
-                                                                X.sol + k * s, X.work, X.maxIter, sm > 0, ck);
+        for (int k = 0; k < NS; ++k) solve(X.wDiag + k * s, X.wFree + k * s, X.wOff + k * 6 * s, X.sol + k * s);
         diff::k_gs_post1<NS, EOS, D><<<gc, kDiffThreads, 0, st>>>(P, X, U, ck);
         if (X.enthalpy) diff::k_gs_afdif<NS, EOS, D><<<gf, kDiffThreads, 0, st>>>(P, L, X, ck);
         diff::k_gs_vtmat<NS, EOS, D><<<gc, kDiffThreads, 0, st>>>(P, L, X, U, ck);
-        for (int d = 0; d < P.nmom; ++d)
-            diff::k_gs_solve<D><<<1, gt, sm, st>>>(P, X.vDiag, X.vFree + d * s, X.vOff,
-                                                                X.sol + (NS + d) * s, X.work, X.maxIter, sm > 0, ck);
-        diff::k_gs_solve<D><<<1, gt, sm, st>>>(P, X.tDiag, X.tFree, X.tOff, X.sol + (NS + 3) * s,
-                                                            X.work, X.maxIter, sm > 0, ck);
+        for (int d = 0; d < P.nmom; ++d) solve(X.vDiag, X.vFree + d * s, X.vOff, X.sol + (NS + d) * s);
+        solve(X.tDiag, X.tFree, X.tOff, X.sol + (NS + 3) * s);
         diff::k_gs_final<NS, EOS, D><<<gc, kDiffThreads, 0, st>>>(P, L, X, U, ck, blockMax);
     }
     diff::k_diff_source<<<1, 1024, 0, st>>>(X, ck, (int)gc);
@@ -75,9 +81,18 @@ int diffusionBlocks(const StepParams& P) { return (int)((P.ncell + kDiffThreads 
 cudaError_t configureDiffusion(int dims, const StepParams& P) {
     const int sm = gsSmemBytes(P);
     if (sm <= 48 * 1024) return cudaSuccess;
-    if (dims == 1) return cudaFuncSetAttribute(diff::k_gs_solve<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    if (dims == 2) return cudaFuncSetAttribute(diff::k_gs_solve<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    return cudaFuncSetAttribute(diff::k_gs_solve<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    cudaError_t e;
+    if (dims == 1) {
+        e = cudaFuncSetAttribute(diff::k_gs_solve<1>, a, sm);
+        return e != cudaSuccess ? e : cudaFuncSetAttribute(diff::k_jacobi_solve<1>, a, sm);
+    }
+    if (dims == 2) {
+        e = cudaFuncSetAttribute(diff::k_gs_solve<2>, a, sm);
+        return e != cudaSuccess ? e : cudaFuncSetAttribute(diff::k_jacobi_solve<2>, a, sm);
+    }
+    e = cudaFuncSetAttribute(diff::k_gs_solve<3>, a, sm);
+    return e != cudaSuccess ? e : cudaFuncSetAttribute(diff::k_jacobi_solve<3>, a, sm);
 }
 
 cudaError_t launchDiffusion(int ns, int eos, int dims, const StepParams& P, const GenericLayout& L,

@@ -351,6 +351,92 @@ __global__ void __launch_bounds__(kGsThreads) k_gs_solve(const StepParams P, con
 }
 
 
+// ----------------------------------------------------------------------------- k_jacobi_solve
+// JacobiSolver::algorithm (JacobiSolver.cpp:9-86) in one CTA: every row from the old iterate
+// alone, (free + rowSum) / diag with rowSum the negated terms of the lower then the upper
+// neighbours, each list in reverse (z-, y-, x-, then z+, y+, x+: the backward pass, whose values
+// are the reference's iterate), all cells of an iteration at once; the convergence test over all
+// cells after each iteration (gsFails).  Iterates in shared memory when they fit, else in work.
+template <int D>
+__global__ void __launch_bounds__(kGsThreads) k_jacobi_solve(const StepParams P, const double* __restrict__ diag,
+                                                              const double* __restrict__ free,
+                                                              const double* __restrict__ off, double* __restrict__ x,
+                                                              double* __restrict__ work, int maxIt, int useSmem,
+                                                              DevClock* __restrict__ ck) {
+    extern __shared__ double gsSmem[];
+    if (ck->done) return;
+    const long long n = P.ncell, rs = P.stride;
+    double* oldI = useSmem ? gsSmem : work;
+    double* newI = useSmem ? gsSmem + n : work + rs;
+    const int nx = P.n[0], ny = P.n[1], nz = P.n[2];
+    const long long sy = nx, sz = (long long)nx * ny;
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) oldI[i] = x[i];
+    __syncthreads();
+    for (int it = 1;; ++it) {
+        bool failed = false;
+        for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+            const int cx = (int)(i % nx);
+            const int cy = D >= 2 ? (int)((i / nx) % ny) : 0;
+            const int cz = D >= 3 ? (int)(i / sz) : 0;
+            const double aii = 1. / diag[i];
+            double rowSum = 0;
+            if (D >= 3 && cz > 0) rowSum -= off[4 * rs + i] * oldI[i - sz];
+            if (D >= 2 && cy > 0) rowSum -= off[3 * rs + i] * oldI[i - sy];
+            if (cx > 0) rowSum -= off[0 * rs + i] * oldI[i - 1];
+            if (D >= 3 && cz < nz - 1) rowSum -= off[5 * rs + i] * oldI[i + sz];
+            if (D >= 2 && cy < ny - 1) rowSum -= off[2 * rs + i] * oldI[i + sy];
+            if (cx < nx - 1) rowSum -= off[1 * rs + i] * oldI[i + 1];
+            const double v = (free[i] + rowSum) * aii;
+            newI[i] = v;
+            failed |= gsFails(i, v, oldI[i]);
+        }
+        const int anyFailed = __syncthreads_or(failed);
+        if (!anyFailed || it >= maxIt) break;
+        double* t = oldI;
+        oldI = newI;
+        newI = t;
+    }
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+        double v = newI[i];
+        if (fabs(v) < 2.220446049250313e-16) v = 0;
+        x[i] = v;
+    }
+}
+
+// ----------------------------------------------------------------------------- k_thomas_solve
+// ThomasSolver::algorithm (ThomasSolver.cpp:9-52), a 1D mesh on one thread: P_i = -u_i / (d_i +
+// l_i P_{i-1}), Q_i = (f_i - l_i Q_{i-1}) / (the same denominator), x from the last row down as
+// P_i x_{i+1} + Q_i, then normalize.  l_i, u_i are the x- and x+ slots of the off-diagonal.
+__global__ void k_thomas_solve(const StepParams P, const double* __restrict__ diag, const double* __restrict__ free,
+                               const double* __restrict__ off, double* __restrict__ x, double* __restrict__ work,
+                               DevClock* __restrict__ ck) {
+    if (ck->done || threadIdx.x != 0) return;
+    const long long N = P.ncell, rs = P.stride;
+    double* Pp = work;
+    double* Qq = work + rs;
+    Pp[0] = -off[1 * rs + 0] / diag[0];
+    Qq[0] = free[0] / diag[0];
+    for (long long i = 1; i < N - 1; ++i) {
+        const double l = off[0 * rs + i];
+        const double den = diag[i] + l * Pp[i - 1];
+        Pp[i] = -off[1 * rs + i] / den;
+        Qq[i] = (free[i] - l * Qq[i - 1]) / den;
+    }
+    Pp[N - 1] = 0;
+    {
+        const double l = off[0 * rs + N - 1];
+        Qq[N - 1] = (free[N - 1] - l * Qq[N - 2]) / (diag[N - 1] + l * Pp[N - 2]);
+    }
+    double xn = Qq[N - 1];
+    x[N - 1] = fabs(xn) < 2.220446049250313e-16 ? 0.0 : xn;
+    for (long long i = N - 2; i >= 0; --i) {
+        const double v = Pp[i] * xn + Qq[i];  // from the unnormalized x_{i+1}
+        xn = v;
+        x[i] = fabs(v) < 2.220446049250313e-16 ? 0.0 : v;
+    }
+}
+
+
 // ----------------------------------------------------------------------------- k_gs_post1
 // new mass fractions (clipped at 0, renormalised), concentrations, CCV and the old energy
 // (Diffusion.cpp:443-478)

@@ -23,7 +23,8 @@ struct DiffParams {
     int interpV;               // 1: cell velocity gradient from interpolated cell velocities
                                //    ("linear" reconstruction, or gravity), else the star velocities
     int dtDiff;                // 1: "Courant-Source-Diffusion" (the diffusion limit)
-    int gs;                    // 1: the Gauss-Seidel (implicit) solver
+    int gs;                    // 1: an implicit solver (the stage's matrices; fv_sle_solver in sle)
+    int sle;                   // fv_sle_solver: Gauss-Seidel, Jacobi, Thomas or noSolver when gs
     int maxIter;               // its iteration limit (#Number_of_iterations_of_SLE_matrix_solver)
     double coeffSource, coeffDiff;
     double* starV;             // [3][faces] Riemann star velocity of the advection (replaced by

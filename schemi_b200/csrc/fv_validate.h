@@ -42,18 +42,22 @@ inline bool fvValidateConfig(const fv_config& c, std::string& e) {
             e = "the diffusion stage runs with ideal and van der Waals mixtures";
             return false;
         }
-        if (c.sle_solver != FV_SLE_EXPLICIT && c.sle_solver != FV_SLE_GAUSS_SEIDEL) {
-            e = "the diffusion stage runs with the explicit and Gauss-Seidel solvers";
+        if (c.sle_solver < FV_SLE_EXPLICIT || c.sle_solver > FV_SLE_NO_SOLVER) {
+            e = "unknown matrix solver";
             return false;
         }
-        if (c.sle_solver == FV_SLE_GAUSS_SEIDEL) {
-            // the wavefront sweep orders neighbours by index: no wrap-around
+        if (c.sle_solver != FV_SLE_EXPLICIT) {
+            // the implicit solvers index a cell's neighbours without wrap-around
             for (int p = 0; p < 6; ++p)
                 if (c.bc_vel[p] == FV_BC_PERIODIC) {
-                    e = "the Gauss-Seidel diffusion stage runs without periodic axes";
+                    e = "the implicit diffusion solvers run without periodic axes";
                     return false;
                 }
-            if (c.sle_max_iter < 1) { e = "the Gauss-Seidel solver needs at least one iteration"; return false; }
+            if (c.sle_max_iter < 1) { e = "the iterative solvers need at least one iteration"; return false; }
+        }
+        if (c.sle_solver == FV_SLE_THOMAS && (c.dims != 1 || c.n[0] < 2)) {
+            e = "the Thomas solver runs on 1D meshes of at least 2 cells";
+            return false;
         }
         if (c.transport < FV_TRANSPORT_CONSTANT || c.transport > FV_TRANSPORT_LENNARD_JONES) {
             e = "unknown transport model";

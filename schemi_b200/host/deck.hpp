@@ -319,11 +319,14 @@ inline Deck readDeck(const std::string& dir, bool createResult) {
     c.linear_reconstruction = reconstruction == "linear";
     // abstractMatrixSolver.cpp:51-70
     if (sle == "explicit") c.sle_solver = FV_SLE_EXPLICIT;
+    else if (sle == "noSolver") c.sle_solver = FV_SLE_NO_SOLVER;
     else if (sle == "GaussSeidel") c.sle_solver = FV_SLE_GAUSS_SEIDEL;
-    else if (sle == "Thomas" || sle == "noSolver" || sle == "conjugateGradient" || sle == "JacobiConjugateGradient" ||
-             sle == "Jacobi" || sle == "biConjugateGradient") {
+    else if (sle == "Jacobi") c.sle_solver = FV_SLE_JACOBI;
+    else if (sle == "Thomas" && dims == "1D") c.sle_solver = FV_SLE_THOMAS;
+    else if (sle == "conjugateGradient" || sle == "JacobiConjugateGradient" || sle == "biConjugateGradient") {
         if (c.diffusion)
-            throw Fail("#Type_of_SLE_solver_flag " + sle + ": the diffusion stage implements explicit and GaussSeidel");
+            throw Fail("#Type_of_SLE_solver_flag " + sle +
+                       ": the diffusion stage implements explicit, noSolver, GaussSeidel, Jacobi and Thomas");
     } else throw Fail("Unknown or inappropriate matrix solver flag.");
     // "Gpu" + an order name: the factory string under which the step-solver adapter runs the
     // step inside the reference's main (schemi_adapter/gpuStepSolver.hpp)

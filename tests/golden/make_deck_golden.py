@@ -212,6 +212,28 @@ def deck_cases():
     c.enthalpy_flow, c.molmass_diffusion = "no", True
     c.t_end = _t_after(c, p, 6, 0.5)
     out.append(("vdw3_6x6x6_diffusion_gs", c, p, 3, True, [{}], 0.0))
+    # the other matrix solvers of the stage: Jacobi (1D, 2D under gravity, 3D), Thomas (the 1D
+    # tridiagonal sweep) and noSolver (the implicit branch, its solves returning the start field)
+    for solver, tag in (("Jacobi", "jacobi"), ("Thomas", "thomas"), ("noSolver", "nosolver")):
+        c, p = cases.shock_tube_1d(n=60)
+        c.diffusion, c.mu, c.D, c.kappa, c.sle_solver = True, 1e-4, 1e-3, 1e-4, solver
+        c.enthalpy_flow, c.molmass_diffusion, c.diffusion_timestep = "explicit", True, True
+        c.t_end = _t_after(c, p, 20, 0.4)
+        out.append((f"tube60_diffusion_{tag}", c, p, 6, True, [{}], 0.0))
+    c, p = cases.rayleigh_taylor_2d(nx=8, ny=16, modes=2)
+    c.g_delta = (0.0, -0.05, 0.0)
+    c.diffusion, c.mu, c.D, c.kappa, c.sle_solver = True, 1e-3, 1e-3, 1e-3, "Jacobi"
+    c.enthalpy_flow, c.molmass_diffusion = "explicit", True
+    c.t_end = _t_after(c, p, 12, 0.5)
+    out.append(("rt8x16_gravity_diffusion_jacobi", c, p, 5, True, [{}], 0.0))
+    c, p = cases.reacting_shear_3d(n=6, periodic=False, precision="f64")
+    c.chemistry = "no"
+    for k in list(c.bc):
+        c.bc[k] = PatchBC.uniform("slip", 3)
+    c.diffusion, c.mu, c.D, c.kappa, c.sle_solver = True, 1e-5, 1e-5, 1e-3, "Jacobi"
+    c.enthalpy_flow, c.molmass_diffusion = "explicit", False
+    c.t_end = _t_after(c, p, 6, 0.5)
+    out.append(("vdw3_6x6x6_diffusion_jacobi", c, p, 3, True, [{}], 0.0))
     # the transport models: hard spheres (kinetic diameters) and Lennard-Jones (eps / k_B, sigma)
     # with both solvers; their face coefficients read the interpolated temperature and
     # concentrations and the Riemann star pressure, the viscous heating the cells' viscosity.  The

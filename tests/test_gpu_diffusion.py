@@ -129,11 +129,11 @@ def _kh_periodic_plain():
     return c, p
 
 
-def _gs(make):
-    """The same case with the Gauss-Seidel (implicit) solver."""
+def _gs(make, solver="GaussSeidel"):
+    """The same case with an implicit solver (Gauss-Seidel unless named)."""
     def f():
         c, p = make()
-        c.sle_solver = "GaussSeidel"
+        c.sle_solver = solver
         return c, p
     return f
 
@@ -162,6 +162,16 @@ CASES = [
     ("rt_gravity_hs_gs", _gs(_hard_spheres(_rt_gravity)), 10),
     ("kh_periodic_hs", _hard_spheres(lambda: _kh_periodic_plain(), molmass=False), 8),
     ("vdw3_3d_hs_gs_molmass", _gs(_hard_spheres(lambda: _vdw_box(3), molmass=True)), 6),
+    # the other solvers of the stage's matrices: Jacobi, Thomas (1D), noSolver
+    ("tube_jacobi", _gs(lambda: _tube(), "Jacobi"), 25),
+    ("vdw3_2d_jacobi", _gs(lambda: _vdw_box(2), "Jacobi"), 10),
+    ("vdw3_3d_jacobi", _gs(lambda: _vdw_box(3), "Jacobi"), 6),
+    ("rt_gravity_jacobi", _gs(_rt_gravity, "Jacobi"), 10),
+    ("tube_thomas", _gs(lambda: _tube(), "Thomas"), 25),
+    ("tube_thomas_plain", _gs(lambda: _tube(enthalpy_flow="no", molmass_diffusion=False, reconstruction="linear",
+                                            diffusion_timestep=False), "Thomas"), 25),
+    ("tube_nosolver", _gs(lambda: _tube(), "noSolver"), 25),
+    ("vdw3_2d_nosolver", _gs(lambda: _vdw_box(2), "noSolver"), 10),
 ]
 
 # cases whose arithmetic calls pow / exp: (name, make, steps, relative tolerance).  Each is
@@ -253,6 +263,9 @@ def test_gpu_diffusion_kernel_count(fv):
     case, _ = _cl2_diffusion()
     g = fv.FVCase(case)
     assert g.kernels_per_step == 4 + 2 + 1 + 2 + 1 + 1 + 1 + 3 + 1 + 1 + 1 + 1
+    # noSolver: the implicit branch without its 1 + 1 + 1 solves
+    case, _ = _gs(lambda: _tube(), "noSolver")()
+    assert fv.FVCase(case).kernels_per_step == 4 + 2 + 1 + 1 + 1 + 1 + 1 + 1 + 1
 
 
 def test_gpu_diffusion_refusals(fv):
@@ -267,8 +280,14 @@ def test_gpu_diffusion_refusals(fv):
     with pytest.raises(fv.FVError) as e:
         fv.FVCase(case)
     assert e.value.status == 11
-    case, _ = _kh_periodic()
-    case.sle_solver = "GaussSeidel"
+    for solver in ("GaussSeidel", "Jacobi", "noSolver"):  # the implicit branch without wrap-around
+        case, _ = _kh_periodic()
+        case.sle_solver = solver
+        with pytest.raises(fv.FVError) as e:
+            fv.FVCase(case)
+        assert e.value.status == 11, solver
+    case, _ = _vdw_box(2)
+    case.sle_solver = "Thomas"  # 1D only
     with pytest.raises(fv.FVError) as e:
         fv.FVCase(case)
     assert e.value.status == 11
