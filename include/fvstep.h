@@ -142,9 +142,14 @@ enum fv_chem_solver {
  * "GaussSeidel" (GaussSeidelSolver.cpp), "Jacobi" (JacobiSolver.cpp), on 1D meshes "Thomas"
  * (ThomasSolver.cpp, the tridiagonal sweep), each solving the matrices of
  * SLEMatrix::generateDTimeLaplacian, or "noSolver" (noMatrixSolver.cpp: the stage takes the
- * implicit branch and every solve returns its start field). */
+ * implicit branch and every solve returns its start field), or the conjugate-gradient solvers
+ * "conjugateGradient", "JacobiConjugateGradient" and "biConjugateGradient"
+ * (conjugateGradientSolver.cpp, JacobiConjugateGradientSolver.cpp, biConjugateGradientSolver.cpp;
+ * on the device their dot products are block sums, not the reference's serial order, and agree
+ * with it to rounding). */
 enum fv_sle_solver {
-    FV_SLE_EXPLICIT = 0, FV_SLE_GAUSS_SEIDEL = 1, FV_SLE_JACOBI = 2, FV_SLE_THOMAS = 3, FV_SLE_NO_SOLVER = 4
+    FV_SLE_EXPLICIT = 0, FV_SLE_GAUSS_SEIDEL = 1, FV_SLE_JACOBI = 2, FV_SLE_THOMAS = 3, FV_SLE_NO_SOLVER = 4,
+    FV_SLE_CG = 5, FV_SLE_JACOBI_CG = 6, FV_SLE_BICG = 7
 };
 
 /* Transport-coefficient model (transportCoefficients.txt #Transport_coefficient_model,

@@ -1955,11 +1955,140 @@ std::vector<double> dThomas(const SLE1& M) {
     return x;
 }
 
+// operator& of a matrix and a vector (src/SLE/SLEMatrixDotProduct.cpp:9-31): diag v_i plus the
+// lower then the upper entries, each list in order
+std::vector<double> dMatVec(const SLE1& M, const std::vector<double>& v) {
+    std::vector<double> r(v.size());
+    for (size_t i = 0; i < v.size(); ++i) {
+        double acc = M.diag[i] * v[i];
+        for (const auto& e : M.lower[i]) acc += e.first * v[e.second];
+        for (const auto& e : M.upper[i]) acc += e.first * v[e.second];
+        r[i] = acc;
+    }
+    return r;
+}
+// sum() of a valarray expression such as (r * r).sum() (libstdc++ bits/valarray_after.h,
+// _Expr::sum: from the last element down, a_{n-1} + a_{n-2} + ... + a_0) and the max of |a| (the
+// first as it is, later ones when larger)
+double dSum(const std::vector<double>& a) {
+    if (a.empty()) return 0;
+    size_t n = a.size();
+    double s = a[--n];
+    while (n != 0) s += a[--n];
+    return s;
+}
+double dAbsMax(const std::vector<double>& a) {
+    double m = std::fabs(a[0]);
+    for (size_t i = 1; i < a.size(); ++i)
+        if (std::fabs(a[i]) > m) m = std::fabs(a[i]);
+    return m;
+}
+std::vector<double> dMul(const std::vector<double>& a, const std::vector<double>& b) {
+    std::vector<double> r(a.size());
+    for (size_t i = 0; i < a.size(); ++i) r[i] = a[i] * b[i];
+    return r;
+}
+// SLEMatrixStorage::transpose (src/SLE/SLEMatrix.cpp:32-64): row i's lower entry (a, j) becomes
+// row j's upper entry (a, i) and the reverse, rows appended in the order of i
+SLE1 dTranspose(const SLE1& M) {
+    SLE1 T;
+    T.diag = M.diag;
+    T.free = M.free;
+    T.lower.assign(M.diag.size(), {});
+    T.upper.assign(M.diag.size(), {});
+    for (size_t i = 0; i < M.diag.size(); ++i) {
+        for (const auto& e : M.lower[i]) T.upper[e.second].push_back({e.first, (long long)i});
+        for (const auto& e : M.upper[i]) T.lower[e.second].push_back({e.first, (long long)i});
+    }
+    return T;
+}
+// The Jacobi preconditioner's product (JacobiConjugateGradientSolver.cpp:14-24: 1 / diag on the
+// diagonal, the off-diagonal entries kept as zeros, so each adds 0 v_j)
+std::vector<double> dPrecond(const SLE1& M, const std::vector<double>& v) {
+    std::vector<double> r(v.size());
+    for (size_t i = 0; i < v.size(); ++i) {
+        double acc = (1. / M.diag[i]) * v[i];
+        for (const auto& e : M.lower[i]) acc += 0 * v[e.second];
+        for (const auto& e : M.upper[i]) acc += 0 * v[e.second];
+        r[i] = acc;
+    }
+    return r;
+}
+
+// conjugateGradientSovler::algorithm (src/SLE/conjugateGradientSolver.cpp:10-53) and, with the
+// Jacobi preconditioner, JacobiConjugateGradientSolver::algorithm (JacobiConjugateGradientSolver.
+// cpp:10-83): the absolute residual max |r| below the tolerance after the first iteration, or the
+// iteration limit.
+std::vector<double> dCG(const SLE1& M, const std::vector<double>& start, long long maxIt, bool jacobi) {
+    const size_t n = start.size();
+    std::vector<double> x(start);
+    std::vector<double> r = dMatVec(M, start);
+    for (size_t i = 0; i < n; ++i) r[i] = M.free[i] - r[i];
+    std::vector<double> d = jacobi ? dPrecond(M, r) : r;
+    long long it = 0;
+    while (true) {
+        ++it;
+        const double diff = dAbsMax(r);
+        if ((diff < 1e-12 && it > 1) || it >= maxIt) {
+            dNormalize(x);
+            return x;
+        }
+        const std::vector<double> Ad = dMatVec(M, d);
+        const double rz = jacobi ? dSum(dMul(r, dPrecond(M, r))) : dSum(dMul(r, r));
+        const double alpha = rz / (dSum(dMul(d, Ad)) + kStab);
+        for (size_t i = 0; i < n; ++i) x[i] += alpha * d[i];
+        std::vector<double> r1(n);
+        for (size_t i = 0; i < n; ++i) r1[i] = r[i] - alpha * Ad[i];
+        const std::vector<double> z1 = jacobi ? dPrecond(M, r1) : r1;
+        const double beta = dSum(dMul(r1, z1)) / (rz + kStab);
+        for (size_t i = 0; i < n; ++i) d[i] = z1[i] + beta * d[i];
+        r = r1;
+    }
+}
+
+// biConjugateGradientSovler::algorithm (src/SLE/biConjugateGradientSolver.cpp:10-75): the shadow
+// residual and direction through the transposed matrix
+std::vector<double> dBiCG(const SLE1& M, const std::vector<double>& start, long long maxIt) {
+    const size_t n = start.size();
+    const SLE1 MT = dTranspose(M);
+    std::vector<double> x(start);
+    std::vector<double> r = dMatVec(M, start);
+    for (size_t i = 0; i < n; ++i) r[i] = M.free[i] - r[i];
+    std::vector<double> d = r, ro = r, dO = r;
+    long long it = 0;
+    while (true) {
+        ++it;
+        const double diff = dAbsMax(r);
+        if ((diff < 1e-12 && it > 1) || it >= maxIt) {
+            dNormalize(x);
+            return x;
+        }
+        const std::vector<double> Ad = dMatVec(M, d);
+        const double rr = dSum(dMul(ro, r));
+        const double alpha = rr / (dSum(dMul(dO, Ad)) + kStab);
+        for (size_t i = 0; i < n; ++i) x[i] += alpha * d[i];
+        std::vector<double> r1(n), ro1(n);
+        for (size_t i = 0; i < n; ++i) r1[i] = r[i] - alpha * Ad[i];
+        const std::vector<double> ATdo = dMatVec(MT, dO);
+        for (size_t i = 0; i < n; ++i) ro1[i] = ro[i] - alpha * ATdo[i];
+        const double beta = dSum(dMul(ro1, r1)) / (rr + kStab);
+        for (size_t i = 0; i < n; ++i) {
+            d[i] = r1[i] + beta * d[i];
+            dO[i] = ro1[i] + beta * dO[i];
+        }
+        r = r1;
+        ro = ro1;
+    }
+}
+
 // the stage's implicit solver (abstractMatrixSolver::createMatrixSolver, :50-120)
 std::vector<double> dSolve(const fv_config& cf, const SLE1& M, const std::vector<double>& start) {
     if (cf.sle_solver == FV_SLE_JACOBI) return dJacobi(M, start, cf.sle_max_iter);
     if (cf.sle_solver == FV_SLE_THOMAS) return dThomas(M);
     if (cf.sle_solver == FV_SLE_NO_SOLVER) return start;  // noMatrixSolver::solve
+    if (cf.sle_solver == FV_SLE_CG) return dCG(M, start, cf.sle_max_iter, false);
+    if (cf.sle_solver == FV_SLE_JACOBI_CG) return dCG(M, start, cf.sle_max_iter, true);
+    if (cf.sle_solver == FV_SLE_BICG) return dBiCG(M, start, cf.sle_max_iter);
     return dGaussSeidel(M, start, cf.sle_max_iter);
 }
 
@@ -2977,7 +3106,7 @@ bool validate(const fv_config& cf, std::string& err) {
             err = "the diffusion stage runs with ideal and van der Waals mixtures";
             return false;
         }
-        if (cf.sle_solver < FV_SLE_EXPLICIT || cf.sle_solver > FV_SLE_NO_SOLVER) {
+        if (cf.sle_solver < FV_SLE_EXPLICIT || cf.sle_solver > FV_SLE_BICG) {
             err = "unknown matrix solver";
             return false;
         }

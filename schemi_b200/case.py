@@ -37,7 +37,8 @@ CHEM_SOLVERS = {"Gauss-Seidel": 0, "Jacobi": 1, "GaussElimination": 2, "conjugat
                 "JacobiConjugateGradient": 4}
 # #Approximation_order values with a GPU step (abstractStepSolver.cpp:56-146)
 ORDERS = {"SecondOrder": 0, "SecondOrderRK": 1, "ThirdOrder": 2, "ThirdOrderCada": 3}
-SLE_SOLVERS = {"explicit": 0, "GaussSeidel": 1, "Jacobi": 2, "Thomas": 3, "noSolver": 4}
+SLE_SOLVERS = {"explicit": 0, "GaussSeidel": 1, "Jacobi": 2, "Thomas": 3, "noSolver": 4, "conjugateGradient": 5,
+               "JacobiConjugateGradient": 6, "biConjugateGradient": 7}
 TRANSPORT_MODELS = {"constant": 0, "hardSpheres": 1, "LennardJones": 2}
 ENTHALPY_FLOWS = {"no": 0, "explicit": 1, "implicit": 2}
 

@@ -559,7 +559,7 @@ fv_status ensureScratch(fv_handle* h) {
             FV_CUDA(h, cudaMalloc(&X.tFree, sizeof(double) * st));
             FV_CUDA(h, cudaMalloc(&X.tOff, sizeof(double) * 6 * st));
             FV_CUDA(h, cudaMalloc(&X.sol, sizeof(double) * (ns + 4) * st));
-            FV_CUDA(h, cudaMalloc(&X.work, sizeof(double) * 3 * st));
+            FV_CUDA(h, cudaMalloc(&X.work, sizeof(double) * 7 * st));
             FV_CUDA(h, cudaMalloc(&X.cNew, sizeof(double) * (ns + 3) * st));
         }
         h->P.starV = X.starV;

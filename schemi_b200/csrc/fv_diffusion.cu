@@ -44,6 +44,12 @@ cudaError_t launchT(const StepParams& P, const GenericLayout& L, const diff::Dif
                 diff::k_thomas_solve<<<1, 32, 0, st>>>(P, dg, fr, of, xs, X.work, ck);
             else if (X.sle == FV_SLE_NO_SOLVER)
                 return;  // noMatrixSolver::solve: the start field is the solution
+            else if (X.sle == FV_SLE_CG)
+                diff::k_cg_solve<D, 0><<<1, diff::kGsThreads, 0, st>>>(P, dg, fr, of, xs, X.work, X.maxIter, ck);
+            else if (X.sle == FV_SLE_JACOBI_CG)
+                diff::k_cg_solve<D, 1><<<1, diff::kGsThreads, 0, st>>>(P, dg, fr, of, xs, X.work, X.maxIter, ck);
+            else if (X.sle == FV_SLE_BICG)
+                diff::k_cg_solve<D, 2><<<1, diff::kGsThreads, 0, st>>>(P, dg, fr, of, xs, X.work, X.maxIter, ck);
             else
                 diff::k_gs_solve<D><<<1, gt, sm, st>>>(P, dg, fr, of, xs, X.work, X.maxIter, sm > 0, ck);
         };

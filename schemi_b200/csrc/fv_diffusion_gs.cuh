@@ -437,6 +437,157 @@ __global__ void k_thomas_solve(const StepParams P, const double* __restrict__ di
 }
 
 
+// ----------------------------------------------------------------------------- k_cg_solve
+// conjugateGradientSovler / JacobiConjugateGradientSolver / biConjugateGradientSovler::algorithm
+// (conjugateGradientSolver.cpp:10-53, JacobiConjugateGradientSolver.cpp:10-83,
+// biConjugateGradientSolver.cpp:10-75) in one CTA.  The matrix products take each row's terms in
+// the reference's order (diag v_i, the lower entries x-, y-, z-, the upper x+, y+, z+; the
+// transposed matrix's rows as SLEMatrixStorage::transpose leaves them: z-, y-, x-, then x+, y+,
+// z+, each entry the transposed row's); the dot products are sums over the CTA in a fixed order,
+// not the reference's serial order, so the iterates agree with it to rounding.  Stop when the
+// absolute residual max |r| is below 1e-12 after the first iteration, or at the limit.
+// KIND: 0 CG, 1 Jacobi-preconditioned CG, 2 BiCG.  work holds [7][stride] vectors.
+__device__ __forceinline__ double blockSum(double v, double* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double s = 0;
+    for (int w = 0; w < nw; ++w) s += red[w];  // every thread, in warp order
+    return s;
+}
+
+template <int D, bool TRANSPOSED>
+__device__ __forceinline__ double cgRow(const StepParams& P, long long i, const double* __restrict__ diag,
+                                        const double* __restrict__ off, const double* v) {
+    const long long rs = P.stride;
+    const int nx = P.n[0], ny = P.n[1], nz = P.n[2];
+    const long long sy = nx, sz = (long long)nx * ny;
+    const int cx = (int)(i % nx);
+    const int cy = D >= 2 ? (int)((i / nx) % ny) : 0;
+    const int cz = D >= 3 ? (int)(i / sz) : 0;
+    double acc = diag[i] * v[i];
+    if (!TRANSPOSED) {
+        // row i's own entries: off slots [x-, x+, y+, y-, z-, z+] = 0, 1, 2, 3, 4, 5
+        if (cx > 0) acc += off[0 * rs + i] * v[i - 1];
+        if (D >= 2 && cy > 0) acc += off[3 * rs + i] * v[i - sy];
+        if (D >= 3 && cz > 0) acc += off[4 * rs + i] * v[i - sz];
+        if (cx < nx - 1) acc += off[1 * rs + i] * v[i + 1];
+        if (D >= 2 && cy < ny - 1) acc += off[2 * rs + i] * v[i + sy];
+        if (D >= 3 && cz < nz - 1) acc += off[5 * rs + i] * v[i + sz];
+    } else {
+        // column i: the entries of the rows that reach cell i, lower ones from the lowest row up
+        if (D >= 3 && cz > 0) acc += off[5 * rs + i - sz] * v[i - sz];
+        if (D >= 2 && cy > 0) acc += off[2 * rs + i - sy] * v[i - sy];
+        if (cx > 0) acc += off[1 * rs + i - 1] * v[i - 1];
+        if (cx < nx - 1) acc += off[0 * rs + i + 1] * v[i + 1];
+        if (D >= 2 && cy < ny - 1) acc += off[3 * rs + i + sy] * v[i + sy];
+        if (D >= 3 && cz < nz - 1) acc += off[4 * rs + i + sz] * v[i + sz];
+    }
+    return acc;
+}
+
+// the Jacobi preconditioner's product: (1 / diag) v plus a zero for each off-diagonal entry
+template <int D>
+__device__ __forceinline__ double cgPrecond(const StepParams& P, long long i, const double* __restrict__ diag,
+                                            const double* v) {
+    const int nx = P.n[0], ny = P.n[1], nz = P.n[2];
+    const long long sy = nx, sz = (long long)nx * ny;
+    const int cx = (int)(i % nx);
+    const int cy = D >= 2 ? (int)((i / nx) % ny) : 0;
+    const int cz = D >= 3 ? (int)(i / sz) : 0;
+    double acc = (1. / diag[i]) * v[i];
+    if (cx > 0) acc += 0 * v[i - 1];
+    if (D >= 2 && cy > 0) acc += 0 * v[i - sy];
+    if (D >= 3 && cz > 0) acc += 0 * v[i - sz];
+    if (cx < nx - 1) acc += 0 * v[i + 1];
+    if (D >= 2 && cy < ny - 1) acc += 0 * v[i + sy];
+    if (D >= 3 && cz < nz - 1) acc += 0 * v[i + sz];
+    return acc;
+}
+
+template <int D, int KIND>
+__global__ void __launch_bounds__(kGsThreads) k_cg_solve(const StepParams P, const double* __restrict__ diag,
+                                                          const double* __restrict__ free,
+                                                          const double* __restrict__ off, double* __restrict__ x,
+                                                          double* __restrict__ work, int maxIt,
+                                                          DevClock* __restrict__ ck) {
+    __shared__ double red[32];
+    if (ck->done) return;
+    const long long n = P.ncell, rs = P.stride;
+    double* r = work;
+    double* d = work + rs;
+    double* Ad = work + 2 * rs;
+    double* z = work + 3 * rs;   // JCG: the preconditioned residual
+    double* ro = work + 4 * rs;  // BiCG: the shadow residual and direction, A^T do
+    double* dO = work + 5 * rs;
+    double* ATd = work + 6 * rs;
+    const int tid = threadIdx.x, bd = blockDim.x;
+    for (long long i = tid; i < n; i += bd) r[i] = free[i] - cgRow<D, false>(P, i, diag, off, x);
+    __syncthreads();
+    for (long long i = tid; i < n; i += bd) {
+        d[i] = KIND == 1 ? cgPrecond<D>(P, i, diag, r) : r[i];
+        if (KIND == 2) ro[i] = dO[i] = r[i];
+    }
+    __syncthreads();
+    for (int it = 1;; ++it) {
+        double mx = -1.0;  // max |r| (a NaN passed over)
+        for (long long i = tid; i < n; i += bd) mx = smax(mx, fabs(r[i]));
+        mx = blockMaxReduce<double>(mx, red);
+        __syncthreads();
+        if (tid == 0) red[0] = mx;
+        __syncthreads();
+        mx = red[0];
+        if ((mx < 1e-12 && it > 1) || it >= maxIt) break;
+        double p1 = 0, p2 = 0;
+        for (long long i = tid; i < n; i += bd) {
+            const double a = cgRow<D, false>(P, i, diag, off, d);
+            Ad[i] = a;
+            if (KIND == 0) p1 += r[i] * r[i];
+            else if (KIND == 1) p1 += r[i] * cgPrecond<D>(P, i, diag, r);
+            else p1 += ro[i] * r[i];
+            p2 += (KIND == 2 ? dO[i] : d[i]) * a;
+        }
+        const double rz = blockSum(p1, red);
+        const double alpha = rz / (blockSum(p2, red) + Num<double>::stab());
+        __syncthreads();
+        if (KIND == 2)
+            for (long long i = tid; i < n; i += bd) ATd[i] = cgRow<D, true>(P, i, diag, off, dO);
+        double p3 = 0;
+        for (long long i = tid; i < n; i += bd) {
+            x[i] += alpha * d[i];
+            const double r1 = r[i] - alpha * Ad[i];
+            r[i] = r1;
+            if (KIND == 2) {
+                const double ro1 = ro[i] - alpha * ATd[i];
+                ro[i] = ro1;
+                p3 += ro1 * r1;
+            } else if (KIND == 0) {
+                p3 += r1 * r1;
+            }
+        }
+        __syncthreads();
+        if (KIND == 1) {
+            for (long long i = tid; i < n; i += bd) {
+                const double z1 = cgPrecond<D>(P, i, diag, r);
+                z[i] = z1;
+                p3 += r[i] * z1;
+            }
+        }
+        const double beta = blockSum(p3, red) / (rz + Num<double>::stab());
+        for (long long i = tid; i < n; i += bd) {
+            d[i] = (KIND == 1 ? z[i] : r[i]) + beta * d[i];
+            if (KIND == 2) dO[i] = ro[i] + beta * dO[i];
+        }
+        __syncthreads();
+    }
+    for (long long i = tid; i < n; i += bd)
+        if (fabs(x[i]) < 2.220446049250313e-16) x[i] = 0;
+}
+
+
 // ----------------------------------------------------------------------------- k_gs_post1
 // new mass fractions (clipped at 0, renormalised), concentrations, CCV and the old energy
 // (Diffusion.cpp:443-478)

@@ -24,7 +24,7 @@ struct DiffParams {
                                //    ("linear" reconstruction, or gravity), else the star velocities
     int dtDiff;                // 1: "Courant-Source-Diffusion" (the diffusion limit)
     int gs;                    // 1: an implicit solver (the stage's matrices; fv_sle_solver in sle)
-    int sle;                   // fv_sle_solver: Gauss-Seidel, Jacobi, Thomas or noSolver when gs
+    int sle;                   // fv_sle_solver of the implicit branch (gs)
     int maxIter;               // its iteration limit (#Number_of_iterations_of_SLE_matrix_solver)
     double coeffSource, coeffDiff;
     double* starV;             // [3][faces] Riemann star velocity of the advection (replaced by
@@ -46,8 +46,9 @@ struct DiffParams {
     double* tFree;
     double* tOff;              // [6][stride]
     double* sol;               // [N + 4][stride] solutions: w_1..w_N, v_x, v_y, v_z, T
-    double* work;              // [3][stride] Gauss-Seidel scratch: the iterates (when they exceed
-                               //    shared memory) and 1 / diag
+    double* work;              // [7][stride] solver scratch: the Gauss-Seidel and Jacobi iterates
+                               //    (when they exceed shared memory) and 1 / diag; the
+                               //    conjugate-gradient vectors
     double* cNew;              // [N + 3][stride] concentrations c_0..c_N, CCVNew, old energy
 };
 

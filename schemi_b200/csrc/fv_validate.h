@@ -42,7 +42,7 @@ inline bool fvValidateConfig(const fv_config& c, std::string& e) {
             e = "the diffusion stage runs with ideal and van der Waals mixtures";
             return false;
         }
-        if (c.sle_solver < FV_SLE_EXPLICIT || c.sle_solver > FV_SLE_NO_SOLVER) {
+        if (c.sle_solver < FV_SLE_EXPLICIT || c.sle_solver > FV_SLE_BICG) {
             e = "unknown matrix solver";
             return false;
         }

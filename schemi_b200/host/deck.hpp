@@ -323,11 +323,10 @@ inline Deck readDeck(const std::string& dir, bool createResult) {
     else if (sle == "GaussSeidel") c.sle_solver = FV_SLE_GAUSS_SEIDEL;
     else if (sle == "Jacobi") c.sle_solver = FV_SLE_JACOBI;
     else if (sle == "Thomas" && dims == "1D") c.sle_solver = FV_SLE_THOMAS;
-    else if (sle == "conjugateGradient" || sle == "JacobiConjugateGradient" || sle == "biConjugateGradient") {
-        if (c.diffusion)
-            throw Fail("#Type_of_SLE_solver_flag " + sle +
-                       ": the diffusion stage implements explicit, noSolver, GaussSeidel, Jacobi and Thomas");
-    } else throw Fail("Unknown or inappropriate matrix solver flag.");
+    else if (sle == "conjugateGradient") c.sle_solver = FV_SLE_CG;
+    else if (sle == "JacobiConjugateGradient") c.sle_solver = FV_SLE_JACOBI_CG;
+    else if (sle == "biConjugateGradient") c.sle_solver = FV_SLE_BICG;
+    else throw Fail("Unknown or inappropriate matrix solver flag.");
     // "Gpu" + an order name: the factory string under which the step-solver adapter runs the
     // step inside the reference's main (schemi_adapter/gpuStepSolver.hpp)
     if (order.rfind("Gpu", 0) == 0) order = order.substr(3);

@@ -213,13 +213,19 @@ def deck_cases():
     c.t_end = _t_after(c, p, 6, 0.5)
     out.append(("vdw3_6x6x6_diffusion_gs", c, p, 3, True, [{}], 0.0))
     # the other matrix solvers of the stage: Jacobi (1D, 2D under gravity, 3D), Thomas (the 1D
-    # tridiagonal sweep) and noSolver (the implicit branch, its solves returning the start field)
-    for solver, tag in (("Jacobi", "jacobi"), ("Thomas", "thomas"), ("noSolver", "nosolver")):
+    # tridiagonal sweep), noSolver (the implicit branch, its solves returning the start field) and
+    # the conjugate-gradient three (on the GPU their dot products are block sums: compared there to
+    # a tolerance)
+    for solver, tag in (("Jacobi", "jacobi"), ("Thomas", "thomas"), ("noSolver", "nosolver"), ("conjugateGradient", "cg"),
+                        ("JacobiConjugateGradient", "jcg"), ("biConjugateGradient", "bicg")):
         c, p = cases.shock_tube_1d(n=60)
         c.diffusion, c.mu, c.D, c.kappa, c.sle_solver = True, 1e-4, 1e-3, 1e-4, solver
-        c.enthalpy_flow, c.molmass_diffusion, c.diffusion_timestep = "explicit", True, True
+        # (the conjugate-gradient decks without the molar-mass correction: with it the tube is ill
+        # conditioned, a one-ulp change of the input moving the state by 1e-5 within six steps)
+        c.enthalpy_flow, c.molmass_diffusion, c.diffusion_timestep = "explicit", "Gradient" not in solver, True
         c.t_end = _t_after(c, p, 20, 0.4)
-        out.append((f"tube60_diffusion_{tag}", c, p, 6, True, [{}], 0.0))
+        out.append((f"tube60_diffusion_{tag}", c, p, 6, True, [{}], 0.0,
+                    {"gpu_tolerance": 1e-10} if "Gradient" in solver else {}))
     c, p = cases.rayleigh_taylor_2d(nx=8, ny=16, modes=2)
     c.g_delta = (0.0, -0.05, 0.0)
     c.diffusion, c.mu, c.D, c.kappa, c.sle_solver = True, 1e-3, 1e-3, 1e-3, "Jacobi"

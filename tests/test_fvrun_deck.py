@@ -168,8 +168,6 @@ def test_print_config_transport_models(tmp_path, model):
 
 
 @pytest.mark.parametrize("file,key,value,message", [
-    ("main.txt", "#Type_of_SLE_solver_flag", "conjugateGradient",
-     "the diffusion stage implements explicit, noSolver, GaussSeidel, Jacobi and Thomas"),
     ("main.txt", "#Type_of_SLE_solver_flag", "LU", "Unknown or inappropriate matrix solver flag."),
     ("main.txt", "#Type_of_flow_solver", "HLL", "the diffusion stage runs with HLLC"),
     ("main.txt", "#Approximation_order", "SecondOrderRK", "the diffusion stage runs with SecondOrder"),

@@ -186,6 +186,12 @@ TOLERANT = [
     ("vdw3_2d_lj", _lennard_jones(lambda: _vdw_box(2)), 10, 1e-11),
     ("vdw3_3d_lj_gs", _gs(_lennard_jones(lambda: _vdw_box(3), molmass=False)), 6, 1e-11),
     ("cl2_4x4_diffusion_gs", _cl2_diffusion, 12, 1e-11),
+    # the conjugate-gradient solvers: block sums for the reference's serial dot products
+    ("tube_cg", _gs(lambda: _tube(molmass_diffusion=False), "conjugateGradient"), 20, 1e-10),
+    ("tube_bicg", _gs(lambda: _tube(molmass_diffusion=False), "biConjugateGradient"), 20, 1e-10),
+    ("vdw3_2d_jcg", _gs(lambda: _vdw_box(2), "JacobiConjugateGradient"), 8, 1e-10),
+    ("vdw3_2d_bicg", _gs(lambda: _vdw_box(2), "biConjugateGradient"), 8, 1e-10),
+    ("vdw3_3d_cg", _gs(lambda: _vdw_box(3), "conjugateGradient"), 5, 1e-10),
 ]
 
 
