@@ -167,7 +167,10 @@ enum fv_sle_solver {
  * (Diffusion.cpp:130-132,238-240,506). */
 enum fv_transport { FV_TRANSPORT_CONSTANT = 0, FV_TRANSPORT_HARD_SPHERES = 1, FV_TRANSPORT_LENNARD_JONES = 2 };
 
-/* transportCoefficients.txt #Flag_for_enthalpy_flow_solution (phaseInitialization.cpp:224-235). */
+/* transportCoefficients.txt #Flag_for_enthalpy_flow_solution (phaseInitialization.cpp:224-235):
+ * the species' enthalpy flow explicit in the temperature's free term and diagonal (with its
+ * source time-step limit), or implicit as the upwind term of SLEMatrix::addNabla in the
+ * temperature matrix (Diffusion.cpp:820-826; with the explicit solver the temperature stays). */
 enum fv_enthalpy_flow { FV_ENTHALPY_NO = 0, FV_ENTHALPY_EXPLICIT = 1, FV_ENTHALPY_IMPLICIT = 2 };
 
 /* Arrhenius rate constant k = A * T^n * exp(-E / (R T)), E in J/mol (R units of the case). */

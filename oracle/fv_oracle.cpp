@@ -1847,6 +1847,44 @@ void dLaplacian(const fvo_case& cs, Ghost ghost, const std::vector<double>& rOld
         }
     }
 }
+
+// SLEMatrix::addNabla (src/SLE/SLEMatrix.cpp:291-401): the upwind term of the flow F across each
+// face of each cell (its faces in order), F & (n S / V) with n outward: outgoing onto the
+// diagonal, incoming onto the neighbour's entry (added to it, or appended) or, on a patch, times
+// the field's cell-variant boundary value off the free term.
+template <class Ghost>
+void dAddNabla(const fvo_case& cs, Ghost ghost, const std::vector<V3>& Fface, SLE1& M) {
+    for (long long i = 0; i < cs.nCells; ++i) {
+        const Cell& c = cs.cells[i];
+        for (int j = 0; j < c.nFaces; ++j) {
+            const int fi = c.faces[j];
+            const Face& F = cs.faces[fi];
+            if (F.nei >= 0) {
+                long long o;
+                V3 outerN;
+                if (F.own == i) {
+                    o = F.nei;
+                    outerN = vdiv(vmul(F.N, F.S), c.V);
+                } else {
+                    o = F.own;
+                    outerN = vmul(vdiv(vmul(F.N, F.S), c.V), -1);
+                }
+                if (vdot(outerN, Fface[fi]) > 0) {
+                    M.diag[i] += vdot(Fface[fi], outerN);
+                } else {
+                    auto& row = o < i ? M.lower[i] : M.upper[i];
+                    auto it = std::find_if(row.begin(), row.end(), [o](const auto& p) { return p.second == o; });
+                    if (it != row.end()) it->first += vdot(Fface[fi], outerN);
+                    else row.emplace_back(vdot(Fface[fi], outerN), o);
+                }
+            } else {
+                const V3 outerN = vdiv(vmul(F.N, F.S), c.V);
+                if (vdot(outerN, Fface[fi]) > 0) M.diag[i] += vdot(Fface[fi], outerN);
+                else M.free[i] -= vdot(Fface[fi], outerN) * ghost(i, fi);
+            }
+        }
+    }
+}
 // a forward sweep, then a backward one, until 100 max |(new - old) / (|new| + eps)| is below
 // convergenceToleranceGlobal (1e-12) or maxIt sweeps ran; normalize (|x| < DBL_EPSILON -> 0)
 std::vector<double> dGaussSeidel(const SLE1& M, const std::vector<double>& start, long long maxIt) {
@@ -2654,6 +2692,9 @@ int diffusionStage(fvo_case& cs, double dt) {
         }
         MT.diag = diagT;
         MT.free = freeT;
+        if (cf.enthalpy_flow == FV_ENTHALPY_IMPLICIT)  // Diffusion.cpp:820-826
+            dAddNabla(cs, [&](long long, int fi) { return dBoundaryT(cs, cs.faces[fi].own, cs.faces[fi].patch, true, bad); },
+                      entFlow, MT);
         TSol = dSolve(cf, MT, T);
     }
 
@@ -2664,7 +2705,10 @@ int diffusionStage(fvo_case& cs, double dt) {
     for (long long i = 0; i < nc; ++i) {
         V3 vn;
         for (int d = 0; d < 3; ++d) vn.x[d] = gs ? vSol[d][i] : (oldV[i].x[d] + freeV[i].x[d] * dt) / cs.rho[0][i];
-        const double Tn = gs ? TSol[i] : (oldEnergy[i] + freeT[i] * dt) / diagT[i];
+        // (the explicit solver with the implicit enthalpy flow solves the temperature with the
+        // factory's second solver, a noMatrixSolver: the temperature stays)
+        const double Tn = gs ? TSol[i]
+                             : (cf.enthalpy_flow == FV_ENTHALPY_IMPLICIT ? T[i] : (oldEnergy[i] + freeT[i] * dt) / diagT[i]);
         Tmin = std::min(Tmin, Tn);
         cs.Tstate[i] = Tn;
         double cc[FV_MAX_SPECIES + 1];
@@ -3129,8 +3173,8 @@ bool validate(const fv_config& cf, std::string& err) {
                 return false;
             }
         }
-        if (cf.enthalpy_flow < FV_ENTHALPY_NO || cf.enthalpy_flow > FV_ENTHALPY_EXPLICIT) {
-            err = "the diffusion stage takes no or explicit enthalpy flow";
+        if (cf.enthalpy_flow < FV_ENTHALPY_NO || cf.enthalpy_flow > FV_ENTHALPY_IMPLICIT) {
+            err = "unknown enthalpy flow flag";
             return false;
         }
     }

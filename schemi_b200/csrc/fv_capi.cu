@@ -703,7 +703,8 @@ fv_status fv_create(const fv_config* cfg, fv_handle** out) {
             X.ljEps[k] = cfg->transport_lj_eps[k];
             X.ljSig[k] = cfg->transport_lj_sigma[k];
         }
-        X.enthalpy = cfg->enthalpy_flow == FV_ENTHALPY_EXPLICIT;
+        X.enthalpy = cfg->enthalpy_flow != FV_ENTHALPY_NO;
+        X.enthImplicit = cfg->enthalpy_flow == FV_ENTHALPY_IMPLICIT;
         X.molmass = cfg->molmass_diffusion != 0;
         // gravity invalidates the star velocities (secondOrderStepSolver.cpp:71-73); the
         // "linear" reconstruction takes the cell velocities' gradient (Diffusion.cpp:178-184)

@@ -684,7 +684,7 @@ __global__ void k_diff_cells(const StepParams P, const GenericLayout L, const Di
                 divW[k] += F[slotW<NS>(k) * nf + f] * nsg * S;
                 if (X.molmass) divC[k] += F[slotCorr<NS>(k) * nf + f] * nsg * S;
             }
-            if (X.enthalpy) divE += F[slotEnt<NS>() * nf + f] * nsg * S;
+            if (X.enthalpy && !X.enthImplicit) divE += F[slotEnt<NS>() * nf + f] * nsg * S;
 #pragma unroll
             for (int d = 0; d < 3; ++d) divFV[d] += F[slotV<NS>(d) * nf + f] * nsg * S;
 #pragma unroll
@@ -779,7 +779,7 @@ __global__ void k_diff_cells(const StepParams P, const GenericLayout L, const Di
         }
         // temperature (Diffusion.cpp:491-500,688-709,818-825)
         double freeT = 0.0 - divT, diagT = CCVNew;
-        if (X.enthalpy) {
+        if (X.enthalpy && !X.enthImplicit) {
             minE = CCVOld * T / fabs(divE + Num<double>::stab());
             const double s = divE * -1;
             if (s >= 0.) freeT += s;
@@ -805,7 +805,9 @@ __global__ void k_diff_cells(const StepParams P, const GenericLayout L, const Di
         double vNew[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) vNew[d] = (rho0 * v[d] + freeV[d] * dt) / rho0;
-        const double Tn = (oldEnergy + freeT * dt) / diagT;
+        // (with the implicit enthalpy flow this solver's temperature is the factory's second
+        // solver's, a noMatrixSolver: it stays, Diffusion.cpp:820-826)
+        const double Tn = X.enthImplicit ? T : (oldEnergy + freeT * dt) / diagT;
         if (Tn < 0.) raise(ck, FV_ERR_NEGATIVE_T);
         // the recomputed phase (Diffusion.cpp:965-1025)
         const double Uv = UvcFromT<NS, EOS>(P.mix, cNew, Tn) * cNew[0];
@@ -868,7 +870,7 @@ __global__ void k_diff_source(const DiffParams X, DevClock* __restrict__ ck, int
     mD = blockMinReduce(mD, red);
     if (threadIdx.x != 0) return;
     double src = sourceTimestep(ck);
-    if (X.enthalpy) src = X.coeffSource * mE;
+    if (X.enthalpy && !X.enthImplicit) src = X.coeffSource * mE;
     if (X.dtDiff) src = smin(src, 0.5 * X.coeffDiff / mD);
     ck->dtSource = src;
 }

@@ -754,7 +754,8 @@ __global__ void k_gs_afdif(const StepParams P, const GenericLayout L, const Diff
         af = af + (corr[k] + flowW[k]) * h / P.mix.M[k];
     }
     const double raw = F[slotEnt<NS>() * nf + f];
-    X.face[slotEnt<NS>() * nf + f] = (af * 0.5 + raw * (1 - 0.5)) * sT;
+    const double avg = af * 0.5 + raw * (1 - 0.5);
+    X.face[slotEnt<NS>() * nf + f] = X.enthImplicit ? avg : avg * sT;  // the implicit flow enters without T
     if (bad) raise(ck, FV_ERR_BOUNDARY);
 }
 
@@ -828,7 +829,7 @@ __global__ void k_gs_vtmat(const StepParams P, const GenericLayout L, const Diff
             const double S = fc.g.S;
 #pragma unroll
             for (int d = 0; d < 3; ++d) divDev[d] += F[slotDev<NS>(d) * nf + f] * nsg * S;
-            if (X.enthalpy) divE += F[slotEnt<NS>() * nf + f] * nsg * S;
+            if (X.enthalpy && !X.enthImplicit) divE += F[slotEnt<NS>() * nf + f] * nsg * S;
             double sv[3];
 #pragma unroll
             for (int d = 0; d < 3; ++d) sv[d] = X.starV[d * nf + f];
@@ -845,7 +846,7 @@ __global__ void k_gs_vtmat(const StepParams P, const GenericLayout L, const Diff
         }
 #pragma unroll
         for (int q = 0; q < 9; ++q) gradV[q] /= V;
-        if (X.enthalpy) {
+        if (X.enthalpy && !X.enthImplicit) {
             const double CCVOld = c[0] * mixCv<NS, EOS>(P.mix, c);
             minE = CCVOld * T / fabs(divE + Num<double>::stab());
             const double s = divE * -1;
@@ -867,6 +868,22 @@ __global__ void k_gs_vtmat(const StepParams P, const GenericLayout L, const Diff
                     dd += sv * muC * gradV[3 * r + q];
                 }
             tfree += dd;
+        }
+        if (X.enthImplicit) {
+            // SLEMatrix::addNabla (SLEMatrix.cpp:291-401) of the enthalpy flow, after every other
+            // term (Diffusion.cpp:820-822): F & (n S / V), n outward, onto the diagonal when
+            // outgoing, else onto the neighbour's entry or, on a patch, times the temperature's
+            // cell-variant ghost off the free term (the flow's other components meet zeros of n)
+#pragma unroll
+            for (int s = 0; s < NFC; ++s) {
+                const FaceGeo g = faceOf(P, L, ijk, fa[s], fh[s]);
+                const double on = g.boundary ? (double(g.sign) * g.S) / V
+                                             : (g.own ? (1.0 * g.S) / V : ((1.0 * g.S) / V) * -1);
+                const double val = F[slotEnt<NS>() * nf + g.f] * on;
+                if (val > 0) tdiag += val;
+                else if (!g.boundary) X.tOff[s * st + i] += val;
+                else tfree -= val * boundaryT<NS, EOS>(P, g.patch, c, p, true, bad);
+            }
         }
         X.vDiag[i] = vdiag;
 #pragma unroll

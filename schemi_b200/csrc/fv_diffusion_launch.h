@@ -18,7 +18,8 @@ struct DiffParams {
     double diam[FV_MAX_SPECIES];   // HARD_SPHERES: kinetic diameters (angstrom)
     double ljEps[FV_MAX_SPECIES];  // LENNARD_JONES: eps / k_B (K)
     double ljSig[FV_MAX_SPECIES];  // LENNARD_JONES: sigma (angstrom)
-    int enthalpy;              // 1: explicit enthalpy flow
+    int enthalpy;              // 1: an enthalpy flow (explicit or implicit)
+    int enthImplicit;          // 1: the implicit one (the upwind term in the temperature matrix)
     int molmass;               // 1: molar-mass diffusion correction
     int interpV;               // 1: cell velocity gradient from interpolated cell velocities
                                //    ("linear" reconstruction, or gravity), else the star velocities

@@ -73,8 +73,8 @@ inline bool fvValidateConfig(const fv_config& c, std::string& e) {
                 return false;
             }
         }
-        if (c.enthalpy_flow != FV_ENTHALPY_NO && c.enthalpy_flow != FV_ENTHALPY_EXPLICIT) {
-            e = "the diffusion stage takes no or explicit enthalpy flow";
+        if (c.enthalpy_flow < FV_ENTHALPY_NO || c.enthalpy_flow > FV_ENTHALPY_IMPLICIT) {
+            e = "unknown enthalpy flow flag";
             return false;
         }
     }

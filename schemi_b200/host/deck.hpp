@@ -405,8 +405,7 @@ inline Deck readDeck(const std::string& dir, bool createResult) {
         else throw Fail("Unknown flag for transport model.");
         if (enthalpy == "no") c.enthalpy_flow = FV_ENTHALPY_NO;
         else if (enthalpy == "explicit") c.enthalpy_flow = FV_ENTHALPY_EXPLICIT;
-        else if (enthalpy == "implicit")
-            throw Fail("#Flag_for_enthalpy_flow_solution implicit: the diffusion stage takes no or explicit");
+        else if (enthalpy == "implicit") c.enthalpy_flow = FV_ENTHALPY_IMPLICIT;
         else throw Fail("Unknown flag for enthalpy flow calculation.");
         if (molMass != "on" && molMass != "off" && molMass != "yes" && molMass != "no")
             throw Fail("Unknown flag for molar mass diffusion correction.");

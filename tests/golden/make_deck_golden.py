@@ -240,6 +240,26 @@ def deck_cases():
     c.enthalpy_flow, c.molmass_diffusion = "explicit", False
     c.t_end = _t_after(c, p, 6, 0.5)
     out.append(("vdw3_6x6x6_diffusion_jacobi", c, p, 3, True, [{}], 0.0))
+    # the implicit enthalpy flow (the upwind term of SLEMatrix::addNabla in the temperature matrix;
+    # with the explicit solver the temperature keeps its value, the factory's second solver being a
+    # noMatrixSolver): a tube with Gauss-Seidel, with Jacobi and with the explicit solver, and a
+    # three-species van der Waals box with Gauss-Seidel
+    for solver, tag in (("GaussSeidel", "gs"), ("Jacobi", "jacobi"), ("explicit", "explicit")):
+        c, p = cases.shock_tube_1d(n=60)
+        c.diffusion, c.mu, c.D, c.kappa, c.sle_solver = True, 1e-4, 1e-3, 1e-4, solver
+        c.enthalpy_flow, c.molmass_diffusion, c.diffusion_timestep = "implicit", True, True
+        c.t_end = _t_after(c, p, 20, 0.4)
+        out.append((f"tube60_enthalpy_implicit_{tag}", c, p, 6, True, [{}], 0.0))
+    c3, p3 = cases.reacting_shear_3d(n=6, periodic=False)
+    c = Case(dims=2, n=(6, 6, 1), L=(1.0, 1.0, 1.0), species=[Species(**vars(s)) for s in c3.species], t_end=1.0,
+             R_units="SI", eos="vanDerWaals", limiter="vanLeer", name="vdw2d")
+    for k in ("tail", "point", "right", "left"):
+        c.bc[k] = PatchBC.uniform("slip", 3)
+    p = [a.reshape(6, 6, 6)[0].ravel() for a in p3]
+    c.diffusion, c.mu, c.D, c.kappa, c.sle_solver = True, 1e-5, 1e-5, 1e-3, "GaussSeidel"
+    c.enthalpy_flow, c.molmass_diffusion, c.diffusion_timestep = "implicit", False, True
+    c.t_end = _t_after(c, p, 8, 0.5)
+    out.append(("vdw3_6x6_enthalpy_implicit_gs", c, p, 3, True, [{}], 0.0))
     # the transport models: hard spheres (kinetic diameters) and Lennard-Jones (eps / k_B, sigma)
     # with both solvers; their face coefficients read the interpolated temperature and
     # concentrations and the Riemann star pressure, the viscous heating the cells' viscosity.  The

@@ -173,7 +173,6 @@ def test_print_config_transport_models(tmp_path, model):
     ("main.txt", "#Approximation_order", "SecondOrderRK", "the diffusion stage runs with SecondOrder"),
     ("sub_1.txt", "#Kinetic_diameter_(A)", "wide", "not a number for kinetic diameter"),
     ("transportCoefficients.txt", "#Transport_coefficient_model", "Sutherland", "Unknown flag for transport model."),
-    ("transportCoefficients.txt", "#Flag_for_enthalpy_flow_solution", "implicit", "takes no or explicit"),
     ("transportCoefficients.txt", "#Flag_for_enthalpy_flow_solution", "maybe",
      "Unknown flag for enthalpy flow calculation."),
     ("transportCoefficients.txt", "#Flag_for_molar_mass_diffusion_correction", "maybe",

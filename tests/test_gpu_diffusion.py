@@ -172,6 +172,16 @@ CASES = [
                                             diffusion_timestep=False), "Thomas"), 25),
     ("tube_nosolver", _gs(lambda: _tube(), "noSolver"), 25),
     ("vdw3_2d_nosolver", _gs(lambda: _vdw_box(2), "noSolver"), 10),
+    # the implicit enthalpy flow: the upwind term in the temperature matrix (explicit solver: the
+    # temperature stays)
+    ("tube_enth_implicit_gs", _gs(lambda: _tube(enthalpy_flow="implicit")), 25),
+    ("tube_enth_implicit_jacobi", _gs(lambda: _tube(enthalpy_flow="implicit"), "Jacobi"), 25),
+    ("tube_enth_implicit_thomas", _gs(lambda: _tube(enthalpy_flow="implicit"), "Thomas"), 25),
+    ("tube_enth_implicit_explicit", lambda: _tube(enthalpy_flow="implicit"), 25),
+    ("vdw3_2d_enth_implicit_gs", _gs(lambda: (lambda cp: (setattr(cp[0], "enthalpy_flow", "implicit"), cp)[1])(
+        _vdw_box(2))), 10),
+    ("vdw3_3d_enth_implicit_gs", _gs(lambda: (lambda cp: (setattr(cp[0], "enthalpy_flow", "implicit"), cp)[1])(
+        _vdw_box(3))), 6),
 ]
 
 # cases whose arithmetic calls pow / exp: (name, make, steps, relative tolerance).  Each is
@@ -276,7 +286,7 @@ def test_gpu_diffusion_kernel_count(fv):
 
 def test_gpu_diffusion_refusals(fv):
     """Configurations outside the stage are refused at fv_create with initialisationError."""
-    for kw in ({"precision": "f32flux"}, {"order": "SecondOrderRK"}, {"flux": "HLL"}, {"enthalpy_flow": "implicit"}):
+    for kw in ({"precision": "f32flux"}, {"order": "SecondOrderRK"}, {"flux": "HLL"}):
         case, _ = _tube(**kw)
         with pytest.raises(fv.FVError) as e:
             fv.FVCase(case)

@@ -57,23 +57,18 @@ def test_unknown_gpu_order_is_refused_by_the_factory(tmp_path):
 
 
 def test_deck_outside_the_step_is_refused_before_the_first_step(tmp_path):
-    """Diffusion with the implicit enthalpy flow: the adapter refuses at the factory, with the deck
-    reader's message."""
+    """A deck with turbulence: the adapter refuses at the factory, with the deck reader's message."""
     from deck_replay import ORDER, load, unpack_inputs
 
     z = load("tube40_fresh")
     unpack_inputs(z, str(tmp_path))
     main_txt = ORDER.sub(rb"\1Gpu\2\3", z["run0:main.txt"].tobytes())
     lines = main_txt.split(b"\n")
-    i = lines.index(b"#Diffusion_flag")
+    i = lines.index(b"#Turbulence_flag")
     lines[i + 1] = b"on"
     (tmp_path / "set" / "main.txt").write_bytes(b"\n".join(lines))
-    tc = (tmp_path / "set" / "transportCoefficients.txt").read_bytes().split(b"\n")
-    i = tc.index(b"#Flag_for_enthalpy_flow_solution")
-    tc[i + 1] = b"implicit"
-    (tmp_path / "set" / "transportCoefficients.txt").write_bytes(b"\n".join(tc))
     res = subprocess.run([_binary()], cwd=tmp_path, stdin=subprocess.DEVNULL, capture_output=True,
                          text=True, timeout=120)
     assert res.returncode != 0
-    assert "the diffusion stage takes no or explicit" in res.stderr + res.stdout
+    assert "turbulence models are not part of this step" in res.stderr + res.stdout
     assert not (tmp_path / "result" / "output_000001.tsv").exists()
