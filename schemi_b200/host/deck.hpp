@@ -310,7 +310,10 @@ inline Deck readDeck(const std::string& dir, bool createResult) {
         t.skip(); order = t.next("approximation order");
         t.skip(); d.readFrom = t.next("start point");
         t.skip(); width = t.next("mixing zone width flag");
-        t.skip(); t.next("nonlinearity iterations");
+        // #Nonlinearity_iterations (Schemi.cpp:304, on / off): without turbulence the stage's
+        // non-linearity loop ends after its first pass either way (its measure is the change of
+        // epsilon, 0)
+        t.skip(); onOff(t.next("nonlinearity iterations"), "nonlinearity iterations");
     }
     c.diffusion = onOff(diffusion, "diffusion");
     if (onOff(turbulence, "turbulence"))
