@@ -2,10 +2,11 @@
 // (secondOrderStepSolver.cpp:69-80, Diffusion.cpp:20-1061) on the generic path, FP64 in the
 // reference's operation order.
 //
-// Scope: molecular transport with constant coefficients (abstractTransportModel.cpp:52-187), no
-// turbulence, the explicit solver (noMatrixSolver: each field advances as (explOldTime +
-// freeTerm dt) / centralDiagonale), ideal and van der Waals mixtures, the enthalpy flow off or
-// explicit, the molar-mass (Maxwell-Stefan) correction on or off.  With turbulence off the
+// Scope: molecular transport with the constant, hard-sphere or Lennard-Jones coefficients, no
+// turbulence, the explicit solver (each field advances as (explOldTime + freeTerm dt) /
+// centralDiagonale; this file) or the implicit matrices and their solvers
+// (fv_diffusion_gs.cuh), ideal and van der Waals mixtures, the enthalpy flow off, explicit or
+// implicit, the molar-mass (Maxwell-Stefan) correction on or off.  With turbulence off the
 // stage's non-linearity loop stops after one pass (its convergence measure is the change of
 // epsilon, 0), and its non-ideality term is multiplied by the turbulent tLambda, 0: that term
 // (Diffusion.cpp:424-428, 608-617) adds signed zeros to the temperature's free term, which
