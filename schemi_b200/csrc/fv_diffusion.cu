@@ -9,16 +9,29 @@ namespace fv {
 namespace {
 constexpr int kDiffThreads = 256;
 
-// dynamic shared memory of the Gauss-Seidel solve: both iterates when they fit, else none (the
-// iterates then live in the work buffer)
-int gsSmemBytes(const StepParams& P) {
+// Launch shape of the Gauss-Seidel solve (k_gs_solve): up to 512 columns (2D / 3D) the split
+// mode, two threads per column rounded to warps; else one per column (whole warps) or the CTA's
+// maximum.  Its dynamic shared memory: the split mode's slots, then both iterates when they fit
+// (itersInSmem), else the iterates live in the work buffer.  The Jacobi solve's: the iterates
+// alone when they fit.
+struct GsShape {
+    int threads, smem, itersInSmem;
+};
+GsShape gsShape(const StepParams& P, int D) {
+    const long long ncol = D == 1 ? 1 : (D == 2 ? (long long)P.n[0] : (long long)P.n[0] * P.n[1]);
+    const long long W = (ncol + 31) / 32 * 32;
+    const bool split = D >= 2 && ncol <= 512;
+    GsShape g;
+    g.threads = split ? (int)(2 * W) : (ncol >= diff::kGsThreads ? diff::kGsThreads : (int)W);
+    const long long role = split ? diff::kGsRoleDoubles * W * (long long)sizeof(double) : 0;
+    const long long iters = 2 * P.ncell * (long long)sizeof(double);
+    g.itersInSmem = role + iters <= diff::kGsSmemBytes;
+    g.smem = (int)(role + (g.itersInSmem ? iters : 0));
+    return g;
+}
+int jacobiSmemBytes(const StepParams& P) {
     const long long b = 2 * P.ncell * (long long)sizeof(double);
     return b <= diff::kGsSmemBytes ? (int)b : 0;
-}
-// threads of the solve: one per column of a wavefront (whole warps), or the CTA's maximum
-int gsThreads(const StepParams& P, int D) {
-    const long long ncol = D == 1 ? 1 : (D == 2 ? (long long)P.n[0] : (long long)P.n[0] * P.n[1]);
-    return ncol >= diff::kGsThreads ? diff::kGsThreads : (int)((ncol + 31) / 32 * 32);
 }
 
 template <int NS, int EOS, int D>
@@ -34,8 +47,8 @@ cudaError_t launchT(const StepParams& P, const GenericLayout& L, const diff::Dif
         // the implicit solver: mass-fraction matrices and solves, new concentrations, the
         // averaged enthalpy flow, velocity and temperature matrices and solves, the phase
         const long long s = P.stride;
-        const int sm = gsSmemBytes(P);
-        const int gt = gsThreads(P, D);
+        const GsShape gs = gsShape(P, D);
+        const int sm = jacobiSmemBytes(P);
         // one solve of diag x + off x = free (x: the start in, the solution out) by the deck's solver
         auto solve = [&](const double* dg, const double* fr, const double* of, double* xs) {
             if (X.sle == FV_SLE_JACOBI)
@@ -51,7 +64,8 @@ cudaError_t launchT(const StepParams& P, const GenericLayout& L, const diff::Dif
             else if (X.sle == FV_SLE_BICG)
                 diff::k_cg_solve<D, 2><<<1, diff::kGsThreads, 0, st>>>(P, dg, fr, of, xs, X.work, X.maxIter, ck);
             else
-                diff::k_gs_solve<D><<<1, gt, sm, st>>>(P, dg, fr, of, xs, X.work, X.maxIter, sm > 0, ck);
+                diff::k_gs_solve<D><<<1, gs.threads, gs.smem, st>>>(P, dg, fr, of, xs, X.work, X.maxIter, gs.itersInSmem,
+                                                                    ck);
         };
         diff::k_gs_wmat<NS, EOS, D><<<gc, kDiffThreads, 0, st>>>(P, L, X, U, ck);
         for (int k = 0; k < NS; ++k) solve(X.wDiag + k * s, X.wFree + k * s, X.wOff + k * 6 * s, X.sol + k * s);
@@ -85,20 +99,20 @@ cudaError_t byEos(int eos, int dims, const StepParams& P, const GenericLayout& L
 int diffusionBlocks(const StepParams& P) { return (int)((P.ncell + kDiffThreads - 1) / kDiffThreads); }
 
 cudaError_t configureDiffusion(int dims, const StepParams& P) {
-    const int sm = gsSmemBytes(P);
-    if (sm <= 48 * 1024) return cudaSuccess;
+    const int sg = gsShape(P, dims).smem, sj = jacobiSmemBytes(P);
     const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    cudaError_t e;
+    cudaError_t e = cudaSuccess;
     if (dims == 1) {
-        e = cudaFuncSetAttribute(diff::k_gs_solve<1>, a, sm);
-        return e != cudaSuccess ? e : cudaFuncSetAttribute(diff::k_jacobi_solve<1>, a, sm);
+        if (sg > 48 * 1024) e = cudaFuncSetAttribute(diff::k_gs_solve<1>, a, sg);
+        if (e == cudaSuccess && sj > 48 * 1024) e = cudaFuncSetAttribute(diff::k_jacobi_solve<1>, a, sj);
+    } else if (dims == 2) {
+        if (sg > 48 * 1024) e = cudaFuncSetAttribute(diff::k_gs_solve<2>, a, sg);
+        if (e == cudaSuccess && sj > 48 * 1024) e = cudaFuncSetAttribute(diff::k_jacobi_solve<2>, a, sj);
+    } else {
+        if (sg > 48 * 1024) e = cudaFuncSetAttribute(diff::k_gs_solve<3>, a, sg);
+        if (e == cudaSuccess && sj > 48 * 1024) e = cudaFuncSetAttribute(diff::k_jacobi_solve<3>, a, sj);
     }
-    if (dims == 2) {
-        e = cudaFuncSetAttribute(diff::k_gs_solve<2>, a, sm);
-        return e != cudaSuccess ? e : cudaFuncSetAttribute(diff::k_jacobi_solve<2>, a, sm);
-    }
-    e = cudaFuncSetAttribute(diff::k_gs_solve<3>, a, sm);
-    return e != cudaSuccess ? e : cudaFuncSetAttribute(diff::k_jacobi_solve<3>, a, sm);
+    return e;
 }
 
 cudaError_t launchDiffusion(int ns, int eos, int dims, const StepParams& P, const GenericLayout& L,

@@ -164,8 +164,11 @@ __global__ void k_gs_wmat(const StepParams P, const GenericLayout L, const DiffP
 // the lower neighbours in reverse face order (z-, y-, x-: the old iterate) and then the upper ones
 // (z+, y+, x+: this sweep's new values).
 constexpr int kGsThreads = 1024;
-// the two iterates in shared memory up to this many bytes (else in global memory)
+// the two iterates (and in split mode the helpers' slots) in shared memory up to this many bytes
+// (else the iterates in global memory)
 constexpr int kGsSmemBytes = 200 * 1024;
+// split mode: per column 2 slots of the lower part and 2 x 4 coefficients
+constexpr int kGsRoleDoubles = 2 + 8;
 
 // one cell's coefficients: 1 / diag (the same value each sweep, formed once per solve), free, the
 // off-diagonal per face slot
@@ -235,8 +238,15 @@ __global__ void __launch_bounds__(kGsThreads) k_gs_solve(const StepParams P, con
     extern __shared__ double gsSmem[];
     if (ck->done) return;
     const long long n = P.ncell, rs = P.stride;
-    double* oldI = useSmem ? gsSmem : work;
-    double* newI = useSmem ? gsSmem + n : work + rs;
+    // split mode (2D / 3D, at most 512 columns, launched with two threads per column rounded to
+    // warps): the first W threads apply each column's upper terms, the other W prepare the next
+    // cell's lower part and coefficients, in shared memory ahead of the iterates
+    const int ncolAll = D == 1 ? 1 : (D == 2 ? P.n[0] : P.n[0] * P.n[1]);
+    const int W = (ncolAll + 31) / 32 * 32;
+    const bool split = D >= 2 && (int)blockDim.x == 2 * W;
+    const int roleOff = split ? kGsRoleDoubles * W : 0;
+    double* oldI = useSmem ? gsSmem + roleOff : work;
+    double* newI = useSmem ? gsSmem + roleOff + n : work + rs;
     double* aiiI = useSmem ? work : work + 2 * rs;
     for (long long i = threadIdx.x; i < n; i += blockDim.x) aiiI[i] = 1. / diag[i];
     __syncthreads();
@@ -276,6 +286,78 @@ __global__ void __launch_bounds__(kGsThreads) k_gs_solve(const StepParams P, con
     const int hmax = D == 2 ? ny : nz;  // cells per column
     for (long long i = threadIdx.x; i < n; i += blockDim.x) oldI[i] = x[i];
     __syncthreads();
+    if (split) {
+        // slot (phase & 1): lowerS[slot][col], coefS[slot][q][col] with q = 1/diag, z+, y+, x+
+        double* lowerS = gsSmem;
+        double* coefS = gsSmem + 2 * W;
+        const bool helper = (int)threadIdx.x >= W;
+        const int col = helper ? (int)threadIdx.x - W : (int)threadIdx.x;
+        const bool has = col < ncol;
+        const int cx = D == 2 ? col : col % nx, cy = D == 2 ? 0 : col / nx;
+        const int base = D == 2 ? cx : cx + cy;
+        const long long sy = nx, sz = (long long)nx * ny;
+        auto cellOf = [&](int hh) -> long long {
+            return D == 2 ? cx + (long long)nx * hh : cx + (long long)nx * (cy + (long long)ny * hh);
+        };
+        // the helper's preparation of its column's cell at wavefront dd into slot sl, from the
+        // coefficients cq already loaded
+        auto prepare = [&](int dd, int sl, const GsCoef& cq) {
+            const int h = dd - base;
+            int ijk[3] = {cx, D == 2 ? h : cy, D == 2 ? 0 : h};
+            lowerS[sl * W + col] = gsLower<D>(P, cellOf(h), ijk, cq, oldI);
+            coefS[(sl * 4 + 0) * W + col] = cq.aii;
+            coefS[(sl * 4 + 1) * W + col] = cq.o[5];
+            coefS[(sl * 4 + 2) * W + col] = cq.o[2];
+            coefS[(sl * 4 + 3) * W + col] = cq.o[1];
+        };
+        auto valid = [&](int dd) { return has && dd - base >= 0 && dd - base < hmax; };
+        for (int it = 1;; ++it) {
+            GsCoef cpre{};  // helper: the coefficients of its next cell to prepare
+            if (helper) {
+                if (valid(dmax)) {
+                    GsCoef c0{};
+                    gsLoad<D>(P, cellOf(dmax - base), aiiI, free, off, c0);
+                    prepare(dmax, 0, c0);
+                }
+                if (valid(dmax - 1)) gsLoad<D>(P, cellOf(dmax - 1 - base), aiiI, free, off, cpre);
+            }
+            __syncthreads();
+            for (int d = dmax; d >= 0; --d) {
+                const int p = dmax - d, sl = p & 1;
+                if (!helper) {
+                    if (valid(d)) {
+                        const int h = d - base;
+                        const long long i = cellOf(h);
+                        const double aii = coefS[(sl * 4 + 0) * W + col];
+                        double v = lowerS[sl * W + col];
+                        if (D >= 3 && h < nz - 1) v -= coefS[(sl * 4 + 1) * W + col] * newI[i + sz] * aii;
+                        if (D >= 2 && (D == 2 ? h : cy) < ny - 1) v -= coefS[(sl * 4 + 2) * W + col] * newI[i + sy] * aii;
+                        if (cx < nx - 1) v -= coefS[(sl * 4 + 3) * W + col] * newI[i + 1] * aii;
+                        newI[i] = v;
+                    }
+                } else {
+                    // the cell of the next wavefront from the coefficients loaded a wavefront ago,
+                    // then the load for the one after (a column's first cell included)
+                    if (valid(d - 1)) prepare(d - 1, sl ^ 1, cpre);
+                    if (valid(d - 2)) gsLoad<D>(P, cellOf(d - 2 - base), aiiI, free, off, cpre);
+                }
+                __syncthreads();
+            }
+            bool failed = false;
+            for (long long i = threadIdx.x; i < n; i += blockDim.x) failed |= gsFails(i, newI[i], oldI[i]);
+            const int anyFailed = __syncthreads_or(failed);
+            if (!anyFailed || it >= maxIt) break;
+            double* t = oldI;
+            oldI = newI;
+            newI = t;
+        }
+        for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+            double v = newI[i];
+            if (fabs(v) < 2.220446049250313e-16) v = 0;
+            x[i] = v;
+        }
+        return;
+    }
     const bool single = ncol <= (int)blockDim.x;
     // this thread's column (single): its x (and y) and the wavefront index of its lowest cell
     const int col = threadIdx.x;
