@@ -331,7 +331,8 @@ fv_status fv_check(fv_handle* h);
 /* The handle's CUDA stream (cudaStream_t), for event timing and interop. */
 void* fv_stream(fv_handle* h);
 
-/* Kernel launches one step issues (fused march: 2, generic path: 5). */
+/* Kernel launches one step issues (the fused march: 1, the generic path: 4, each finalizing the
+ * CFL block in its last CTA; more with chemistry, a diffusion stage or a multi-stage step). */
 long long fv_kernels_per_step(const fv_handle* h);
 
 /* ---- One step that allocates no device memory (no counterpart in the reference) ----
@@ -348,11 +349,12 @@ long long fv_kernels_per_step(const fv_handle* h);
  * Runs the full MUSCL-Hancock path of the SecondOrder step solver (any limiter, 1D/2D/3D, both
  * precisions) on meshes of at most FV_NOALLOC_MAX_CELLS cells.  Rejected with FV_ERR_INIT: every
  * configuration fv_create rejects, larger meshes, cases with chemistry, the SecondOrderRK,
- * ThirdOrder and ThirdOrderCada step solvers, and state_in / state_out arrays that overlap.
- * The first call on a device looks up the array's device address (cudaGetSymbolAddress); make
- * that first call before any stream capture.  Every call rewrites each part of the array it
- * reads, so no state carries over between calls; calls that overlap on the GPU share the array
- * and race.  Synchronises `stream` before returning. */
+ * ThirdOrder and ThirdOrderCada step solvers, the diffusion stage, and state_in / state_out arrays
+ * that overlap.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress).  Every call rewrites each part of the array it reads, so no state
+ * carries over between calls; calls that overlap on the GPU share the array and race.  The call
+ * synchronises `stream` before returning (it reads the new time step back), so it cannot be
+ * captured in a CUDA graph. */
 #define FV_NOALLOC_MAX_CELLS 1024
 #define FV_NOALLOC_SCRATCH_BYTES 2621440
 fv_status fv_step_noalloc(const fv_config* cfg, const double* state_in, double* state_out, double dt,
